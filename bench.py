@@ -1,0 +1,327 @@
+"""Benchmark: multigrid solves/s to 1e-10 relative residual, plain FP64, on the
+1024x1024 stretched mapped grid (x = xi + 0.1 sin(2 pi xi) sin(2 pi eta),
+y = (e^{beta eta} - 1)/(e^beta - 1) with a 64:1 first-cell aspect ratio; Dirichlet
+x sides, Neumann y sides; seeded 16-mode Fourier rhs, J-weighted mean removed).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one full solve (V-cycles until |r|/|r0| <= 1e-10) of that problem.
+Under torchrun every rank solves its own copy (replicas; the solve does not
+shard) and rank 0 prints one JSON line.
+
+--impl reference times the CPU restatement of the reference algorithm (the
+reference is Fortran and no Fortran compiler exists on these hosts) on all
+host cores, on a bounded sample of V-cycles of the same solve.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+N_GRID = 1024
+TOL = 1e-10
+MAXITERS = 4000
+NU = (8, 8, 8)            # smooth_down, smooth_up, smooth_bottom (the reference test setting, test.f90:2546-2548)
+METRIC = "solves/s @1e-10 rel resid (plain FP64)"
+WORKLOAD = "wavy_stretched_1024"
+# words moved per cell by one smoothing sweep: read phi, rhs, invdiag, 4 Jgup; write phi
+SWEEP_WORDS = 8
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n", type=int, default=N_GRID)
+    p.add_argument("--cpu-vcycles", type=int, default=2, help="V-cycles in the bounded CPU sample")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def workload(n):
+    from mgpoisson2d_b200 import workloads as W
+    return W.wavy_stretched(n)
+
+
+# --------------------------------------------------------------------------- #
+# clocks sampled during the timed region
+# --------------------------------------------------------------------------- #
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if not self.proc:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return out
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        out.update(sm_mhz=sm[len(sm) // 2] if sm else None, sm_max_mhz=max(mx) if mx else None, reasons=reasons,
+                   samples=len(rows))
+        return out
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """DRAM bytes per smoothing sweep from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        d = json.load(open(path))
+        return d
+    except Exception:
+        return None
+
+
+# --------------------------------------------------------------------------- #
+# CPU legs
+# --------------------------------------------------------------------------- #
+def cpu_sample(n, vcycles):
+    """Time `vcycles` V-cycles of the oracle (lexicographic, as the reference)
+    on this workload, single thread.  Returns seconds per V-cycle."""
+    import ctypes
+    from mgpoisson2d_b200.types import BoxData
+    from oracle import oracle as O
+    O.lib().or_set_dirichlet_coupled_diagonal.argtypes = [ctypes.c_int]
+    O.lib().or_set_dirichlet_coupled_diagonal(1)
+    v, geo, rhs, bc, _ = workload(n)
+    phi = BoxData(v, 1, 1)
+    t0 = time.perf_counter()
+    rep = O.vcycle(phi, rhs, geo, bc, True, TOL, vcycles, smooth_down=NU[0], smooth_up=NU[1], smooth_bottom=NU[2],
+                   gs_order=0)
+    dt = time.perf_counter() - t0
+    return dt / max(rep.iterations, 1), rep.iterations
+
+
+def _ref_worker(args):
+    n, vc = args
+    return cpu_sample(n, vc)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    iters = solve_vcycles_estimate(args.n)
+    ctx = mp.get_context("spawn")
+    times = []
+    with ctx.Pool(cores) as pool:
+        for step in range(args.warmup + args.steps):
+            res = pool.map(_ref_worker, [(args.n, args.cpu_vcycles)] * cores)
+            if step >= args.warmup:
+                times.append(res)
+    per_vc = [t for step in times for (t, _) in step]
+    tvc = sum(per_vc) / len(per_vc)
+    value = cores / (tvc * iters)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tvc * iters * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": args.n, "tol": TOL, "nu": list(NU), "solver": "vcycle",
+                   "vcycles_per_solve": iters},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
+                         "sample": f"{args.cpu_vcycles} V-cycles per core per step of the {args.n}^2 solve "
+                                   f"(oracle, lexicographic Gauss-Seidel); solves/s = cores / "
+                                   f"(s per V-cycle x {iters} V-cycles per solve)"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# V-cycles the 1e-10 solve of this workload takes (the device solve reports
+# its own count in every bench line; the CPU legs cannot afford a full solve).
+_VCYCLES = {}
+
+
+def solve_vcycles_estimate(n):
+    path = os.path.join(ROOT, "profiles", "vcycles.json")
+    try:
+        return int(json.load(open(path))[str(n)])
+    except Exception:
+        return _VCYCLES.get(n, 1000)
+
+
+# --------------------------------------------------------------------------- #
+# GPU arm
+# --------------------------------------------------------------------------- #
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    import mgpoisson2d_b200.api as M
+    from mgpoisson2d_b200.types import BoxData
+
+    v, geo, rhs, bc, _ = workload(args.n)
+    flags = M.FLAG_DIRICHLET_COUPLED_DIAG
+    solver = M.Solver(v, geo, bc, M.KIND_MG, flags)
+    phi_d = BoxData(v, 1, 1).to_device()
+    rhs_d = rhs.to_device()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def solve():
+        phi_d.data.zero_()
+        return solver.vcycle(phi_d, rhs_d, bc, True, TOL, MAXITERS, 1, *NU)
+
+    reps = []
+    for _ in range(args.warmup):
+        reps.append(solve())
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = M.kernel_launch_count()
+    sampler = ClockSampler(local)
+    sampler.start()
+    step_ms = []
+    t_wall = time.perf_counter()
+    for _ in range(args.steps):
+        flush.fill_(1.0)   # L2 flush between steps; outside the per-step events
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rep = solve()
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        reps.append(rep)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    wall = time.perf_counter() - t_wall
+    clocks = sampler.stop()
+    launches = M.kernel_launch_count() - launches0
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.steps / (total_ms * 1e-3)
+    last = reps[-1]
+    assert last.relres[-1] <= TOL and not last.diverged, "solve did not converge"
+
+    # live roofline of the dominant kernel: one more solve with the finest
+    # level's smoothing bracketed by events
+    prof = M.Solver(v, geo, bc, M.KIND_MG, flags | M.FLAG_TIME_SMOOTHER)
+    phi_d.data.zero_()
+    flush.fill_(1.0)
+    prep = prof.vcycle(phi_d, rhs_d, bc, True, TOL, MAXITERS, 1, *NU)
+    prof.close()
+    sweep_s = prep.smooth0_seconds / max(prep.smooth0_sweeps, 1)
+    alg_bytes = SWEEP_WORDS * 8 * v.nx * v.ny
+    peak, peak_kind = measured_peak()
+    achieved = alg_bytes / sweep_s / 1e9
+    tr = committed_traffic()
+    roofline = {"bound": "hbm", "kernel": "gs_sweep level 0 (ghost fill + 4 colour passes)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "traffic": (tr or {}).get("bytes_per_sweep"),
+                "alg_bytes_per_sweep": alg_bytes, "sweep_us": sweep_s * 1e6}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": args.n, "tol": TOL, "nu": list(NU), "solver": "vcycle",
+                   "flags": "dirichlet_coupled_diag", "vcycles_per_solve": last.iterations,
+                   "maxdepth": last.maxdepth, "l2": "flushed between steps (256 MiB write, outside step events)",
+                   "parallelism": f"replicas{world}"},
+        "roofline": roofline, "clocks": clocks, "gpu_launches": launches,
+        "unknowns_vcycles_per_s": value * last.iterations * v.nx * v.ny,
+        "wall_s": wall,
+    }
+
+    if rank == 0 and not args.no_e2e:
+        # end to end through the reference-facing call: host arrays, hierarchy
+        # built inside the call (mgp_vcycle has the Fortran argument list)
+        phi_h = BoxData(v, 1, 1)
+        M.set_flags(flags)
+        t0 = time.perf_counter()
+        erep = M.vcycle(phi_h, rhs, geo, bc, True, TOL, MAXITERS, -1, 1, *NU)
+        e2e_s = time.perf_counter() - t0
+        M.set_flags(0)
+        h2d = 8 * (phi_h.data.size + rhs.data.size + v.nx * v.ny + 4 * (v.nx + 1) * v.ny)
+        line["e2e"] = {"value": 1.0 / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                       "d2h_bytes_per_step": 8 * phi_h.data.size, "api": "mgp_vcycle (host arrays)",
+                       "vcycles": erep.iterations}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        tvc, nvc = cpu_sample(args.n, args.cpu_vcycles)
+        iters = last.iterations
+        line["cpu_baseline"] = {"value": 1.0 / (tvc * iters), "unit": "solves/s", "cores": 1, "kind": "port",
+                                "sample": f"{nvc} V-cycles of the {args.n}^2 solve on the oracle (lexicographic "
+                                          f"Gauss-Seidel), {tvc:.2f} s per V-cycle x {iters} V-cycles per solve"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

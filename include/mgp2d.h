@@ -1,0 +1,257 @@
+/*
+ * mgp2d.h -- C ABI of the B200 multigrid solver for the 2-D mapped-grid,
+ * variable-coefficient Poisson operator  L[phi] = d_xi(J g^{xi xi} d_xi phi + J g^{xi eta} d_eta phi)
+ *                                               + d_eta(J g^{eta xi} d_xi phi + J g^{eta eta} d_eta phi).
+ *
+ * Every entry point replaces one module procedure of the Fortran library
+ * MGPoisson2D (src/libMGPoisson, src/libBaseTools).  The citation beside each
+ * declaration names the routine it replaces (file:line).  Argument meaning,
+ * defaults and numerical behaviour follow that routine; differences are listed
+ * in the comment.
+ *
+ * Conventions
+ *  - Arrays are Fortran column-major (i / x fastest), exactly the memory of
+ *    box_data%data (arrayutils.f90:83-96).  An mgp_array names the first
+ *    element of the allocation (bx%ilo, bx%jlo) plus its leading dimension and
+ *    ghost counts, so a Fortran caller passes c_loc(bd%data) without a copy.
+ *  - Pointers may be host or device memory; the library asks the CUDA driver
+ *    which one each pointer is (cudaPointerGetAttributes).  Host arrays are
+ *    staged through device buffers inside the call.
+ *  - All arithmetic is IEEE FP64 without fused multiply-add, in the same
+ *    operation order as the Fortran routines.
+ *  - Every function returns an mgp_status (0 = MGP_OK).  Nothing calls exit();
+ *    where the Fortran library prints and stops, this library returns an
+ *    error code and records a message readable through mgp_last_error().
+ */
+#ifndef MGP2D_H
+#define MGP2D_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- BC types and modes: same values as arrayutils.f90:27-49 ---- */
+#define MGP_BCTYPE_UNDEFINED (-2)
+#define MGP_BCTYPE_NONE      (-1)
+#define MGP_BCTYPE_NEUM        0
+#define MGP_BCTYPE_DIRI        1
+#define MGP_BCTYPE_PERIODIC    2
+#define MGP_BCTYPE_CF          3
+#define MGP_BCTYPE_EXTRAP0     4
+#define MGP_BCTYPE_EXTRAP1     5
+#define MGP_BCTYPE_EXTRAP2     6
+
+#define MGP_BCMODE_UNIFORM     0
+#define MGP_BCMODE_NONUNIFORM  1
+#define MGP_BCMODE_LAH         2
+
+/* Sides, in the order of the bdry_data components (arrayutils.f90:55-70). */
+#define MGP_XLO 0
+#define MGP_XHI 1
+#define MGP_YLO 2
+#define MGP_YHI 3
+
+/* The sentinel the Fortran library writes into corner ghosts (precision.f90:53). */
+#define MGP_BOGUS_VAL 1.2345e300
+
+typedef enum mgp_status {
+    MGP_OK        = 0,
+    MGP_EINVAL    = 1,  /* bad argument: the Fortran code would print and stop  */
+    MGP_ENOMEM    = 2,  /* device or host allocation failed                     */
+    MGP_EDIVERGED = 3,  /* non-finite residual (NaN/Inf in the data)            */
+    MGP_EMAXITER  = 4,  /* reserved: iteration cap reached (solves return OK)    */
+    MGP_ETIMEOUT  = 5,  /* a bounded device wait ran out                         */
+    MGP_ECUDA     = 6,  /* a CUDA runtime call failed                            */
+    MGP_ENOTSUP   = 7   /* a path the Fortran library also stops on              */
+} mgp_status;
+
+/* type(box), arrayutils.f90:10-15.  nx = ihi-ilo+1, ny = jhi-jlo+1. */
+typedef struct mgp_box {
+    int ilo, ihi, jlo, jhi;
+    int nx, ny;
+    double dx, dy;
+} mgp_box;
+
+/* box_data%data seen from C.  Valid element (i,j), counted from the valid
+ * region's lower corner (0 <= i < nx of the centring), lives at
+ *     data[(i + ngx) + (j + ngy) * ld].
+ * ld = 0 means the natural leading dimension (valid extent + 2*ngx). */
+typedef struct mgp_array {
+    double *data;
+    int ld;
+    int ngx, ngy;
+} mgp_array;
+
+/* type(bdry_data), arrayutils.f90:55-70.  data[s] points at 1 value (UNIFORM,
+ * LAH) or at the side length of values (NONUNIFORM: ny for x sides, nx for y
+ * sides), indexed from the valid region's lower corner. */
+typedef struct mgp_bdry {
+    int type[4];
+    int mode[4];
+    const double *data[4];
+} mgp_bdry;
+
+/* type(geo_data), arrayutils.f90:109-116.  J is cell-centred; Jgup_xx and
+ * Jgup_xy live on x-faces ((nx+1) x ny valid); Jgup_yx and Jgup_yy on y-faces
+ * (nx x (ny+1) valid). */
+typedef struct mgp_geo {
+    mgp_array J, Jgup_xx, Jgup_xy, Jgup_yx, Jgup_yy;
+    double dx, dy;
+} mgp_geo;
+
+/* Per-solve record, filled by the solve entry points when non-NULL.  relres
+ * (optional, caller-owned, maxiters+1 doubles) receives the relative residual
+ * history that the Fortran drivers print at verbosity >= 1. */
+typedef struct mgp_report {
+    int status;
+    int iterations;      /* outer iterations performed                        */
+    int maxdepth;        /* multigrid depth used (levels 0..maxdepth)         */
+    int diverged;        /* 1 if the last correction was undone (MG:630-639)  */
+    double rscale;       /* |r0|_2 (1 if it was zero)                          */
+    double final_relres;
+    double *relres;      /* in: caller array or NULL; out: history            */
+    double seconds;      /* wall time of the solve on the device              */
+    /* With MGP_FLAG_TIME_SMOOTHER: device time of the level-0 smoothing calls
+     * and the number of level-0 sweeps they ran. */
+    double smooth0_seconds;
+    long long smooth0_sweeps;
+} mgp_report;
+
+/* Solver flags (mgp_solver_create; mgp_set_flags for the Fortran-signature
+ * drivers and operator calls).  0 reproduces the Fortran library exactly. */
+/* compute_invdiags adds the order-3 Dirichlet ghost's dependence on the cell
+ * (the ghost moves by -3 per unit change of the cell, arrayutils.f90:1162-1166).
+ * The Fortran routine leaves it out (poisson2d.f90:29-33); with that diagonal
+ * the Gauss-Seidel sweep amplifies errors at Dirichlet corners and the V-cycle
+ * diverges on every problem with two adjacent Dirichlet sides. */
+#define MGP_FLAG_DIRICHLET_COUPLED_DIAG 1
+/* Time the finest level's smoothing with CUDA events (reported in
+ * mgp_report.smooth0_seconds); the events are read after the solve. */
+#define MGP_FLAG_TIME_SMOOTHER 2
+
+/* Solver kinds for the resident-hierarchy handle. */
+#define MGP_KIND_MG 0   /* module MGPoisson2D (vcycle, fmg)                  */
+#define MGP_KIND_DD 1   /* module DeferredMGPoisson2D (vcycle)               */
+
+typedef struct mgp_solver mgp_solver;
+
+/* ------------------------------------------------------------------------ */
+/* Library                                                                    */
+/* ------------------------------------------------------------------------ */
+const char *mgp_version(void);
+const char *mgp_last_error(void);
+/* Process-wide flags used by the calls that carry no flags argument.  Returns
+ * the previous value. */
+int mgp_set_flags(int flags);
+/* Number of CUDA kernels this process has launched through the library. */
+long long mgp_kernel_launch_count(void);
+
+/* ------------------------------------------------------------------------ */
+/* Schedule (MGPoisson2D.f90:38-129)                                          */
+/* ------------------------------------------------------------------------ */
+/* estimate_maxdepth, MGPoisson2D.f90:38-62. */
+int mgp_estimate_maxdepth(int *maxdepth, const mgp_box *valid);
+/* create_mgschedule, MGPoisson2D.f90:67-129.  refx/refy hold maxdepth ints. */
+int mgp_create_mgschedule(int *refx, int *refy, int *maxdepth, const mgp_box *valid);
+
+/* ------------------------------------------------------------------------ */
+/* Operator-level calls (module Poisson2D and arrayutils)                     */
+/* ------------------------------------------------------------------------ */
+/* fill_ghosts, arrayutils.f90:1277-1492 (do_neum is the optional do_neum_opt). */
+int mgp_fill_ghosts(const mgp_box *valid, mgp_array *phi, const mgp_bdry *bc,
+                    const mgp_geo *geo, int homog, int do_neum);
+/* extrapolate_ghosts, arrayutils.f90:1497-1566. */
+int mgp_extrapolate_ghosts(const mgp_box *valid, mgp_array *phi, int order);
+/* compute_invdiags, poisson2d.f90:16-388. */
+int mgp_compute_invdiags(const mgp_box *valid, mgp_array *invdiags,
+                         const mgp_geo *geo, const mgp_bdry *bc, int homog);
+/* compute_laplacian, poisson2d.f90:886-1319 (jscale = opt_jscale). */
+int mgp_compute_laplacian(const mgp_box *valid, mgp_array *lap, mgp_array *phi,
+                          const mgp_geo *geo, const mgp_bdry *bc, int homog, int jscale);
+/* compute_residual, poisson2d.f90:1327-1353. */
+int mgp_compute_residual(const mgp_box *valid, mgp_array *res, const mgp_array *rhs,
+                         mgp_array *phi, const mgp_geo *geo, const mgp_bdry *bc,
+                         int homog, int jscale);
+/* relax_gs, poisson2d.f90:1460-1988.  The device sweep visits the four
+ * colours (i mod 2, j mod 2) = (0,0),(1,1),(1,0),(0,1) in turn instead of the
+ * lexicographic order; ghosts are refreshed once per sweep as in P2:1556. */
+int mgp_relax_gs(const mgp_box *valid, mgp_array *phi, const mgp_array *rhs,
+                 const mgp_geo *geo, const mgp_bdry *bc, int homog,
+                 const mgp_array *invdiags, double omega, double tol, int maxiters,
+                 int zerophi, int verbosity);
+/* solve_bicgstab2, poisson2d.f90:2253-2477. */
+int mgp_solve_bicgstab2(const mgp_box *valid, mgp_array *phi, const mgp_array *rhs,
+                        const mgp_geo *geo, const mgp_bdry *bc, int homog,
+                        const mgp_array *invdiags, double tol, int max_iters,
+                        int max_restarts, int zerophi, int verbosity);
+/* restrict, MGPoisson2D.f90:135-257.  offi/offj: 0 = node, 1 = cell
+ * (BD_NODE/BD_CELL, arrayutils.f90:76-77); crse/fine give the cell-centred
+ * valid boxes of the two levels. */
+int mgp_restrict(const mgp_box *fine_valid, const mgp_array *fine,
+                 const mgp_box *crse_valid, mgp_array *crse, int offi, int offj);
+/* prolong, MGPoisson2D.f90:262-394.  Adds the interpolated correction to fine.
+ * Ratios (2,2) follow the Fortran routine; (2,1) and (1,2), where the Fortran
+ * routine stops, use the same constant + linear form in the coarsened
+ * direction only. */
+int mgp_prolong(const mgp_box *fine_valid, mgp_array *fine, const mgp_box *crse_valid,
+                mgp_array *crse, const mgp_geo *fine_geo, const mgp_geo *crse_geo,
+                const mgp_bdry *crse_bc, int order);
+/* pnorm, arrayutils.f90:753-796 (p = 0 max, 1, 2, other p). */
+int mgp_pnorm(const mgp_box *valid, const mgp_array *bd, int p, double *out);
+/* inner_prod, arrayutils.f90:637-661. */
+int mgp_inner_prod(const mgp_box *valid, const mgp_array *a, const mgp_array *b, double *out);
+
+/* ------------------------------------------------------------------------ */
+/* Drivers with the Fortran argument lists (the hierarchy is built and freed  */
+/* inside every call, as the Fortran drivers do)                              */
+/* ------------------------------------------------------------------------ */
+/* MGPoisson2D::vcycle, MGPoisson2D.f90:400-670. */
+int mgp_vcycle(const mgp_box *valid, mgp_array *phi, mgp_array *rhs, const mgp_geo *geo,
+               const mgp_bdry *bc, int homog, int amrrefx, int amrrefy, double tol,
+               int maxiters, int maxdepth_user, int numcycles, int smooth_down,
+               int smooth_up, int smooth_bottom, int zerophi, int verbosity,
+               mgp_report *report);
+/* MGPoisson2D::fmg, MGPoisson2D.f90:860-1122. */
+int mgp_fmg(const mgp_box *valid, mgp_array *phi, mgp_array *rhs, const mgp_geo *geo,
+            const mgp_bdry *bc, int homog, int amrrefx, int amrrefy, double tol,
+            int maxiters, int maxdepth_user, int numcycles, int smooth_down,
+            int smooth_up, int smooth_bottom, int zerophi, int verbosity,
+            mgp_report *report);
+/* DeferredMGPoisson2D::vcycle, MGPoisson2D_DD.f90:589-862.  rhs is scaled by
+ * J on entry and divided by J on exit, as in DD:772-773 and DD:837-838. */
+int mgp_dc_vcycle(const mgp_box *valid, mgp_array *phi, mgp_array *rhs, const mgp_geo *geo,
+                  const mgp_bdry *bc, int homog, int amrrefx, int amrrefy, double tol,
+                  int maxiters, int maxdepth_user, int numcycles, int smooth_down,
+                  int smooth_up, int smooth_bottom, int zerophi, int verbosity,
+                  mgp_report *report);
+
+/* ------------------------------------------------------------------------ */
+/* Resident hierarchy.  The set-up half of the drivers above (schedule,       */
+/* geometry restriction, inverse diagonals; MG:432-562, DD:622-761) runs once */
+/* in mgp_solver_create and stays in HBM; each solve call then runs only the  */
+/* iteration half (MG:565-645, MG:1010-1096, DD:765-839).                     */
+/* ------------------------------------------------------------------------ */
+/* bc supplies the BC types; values are taken per solve call. */
+int mgp_solver_create(const mgp_box *valid, const mgp_geo *geo, const mgp_bdry *bc,
+                      int kind, int flags, int maxdepth_user, mgp_solver **out);
+int mgp_solver_destroy(mgp_solver *s);
+/* CUDA stream (cudaStream_t) the solver's work is queued on; NULL = default. */
+int mgp_solver_set_stream(mgp_solver *s, void *stream);
+int mgp_solver_maxdepth(const mgp_solver *s, int *maxdepth);
+int mgp_solver_vcycle(mgp_solver *s, mgp_array *phi, mgp_array *rhs, const mgp_bdry *bc,
+                      int homog, double tol, int maxiters, int numcycles, int smooth_down,
+                      int smooth_up, int smooth_bottom, int zerophi, int verbosity,
+                      mgp_report *report);
+int mgp_solver_fmg(mgp_solver *s, mgp_array *phi, mgp_array *rhs, const mgp_bdry *bc,
+                   int homog, double tol, int maxiters, int numcycles, int smooth_down,
+                   int smooth_up, int smooth_bottom, int zerophi, int verbosity,
+                   mgp_report *report);
+int mgp_solver_dc_vcycle(mgp_solver *s, mgp_array *phi, mgp_array *rhs, const mgp_bdry *bc,
+                         int homog, double tol, int maxiters, int numcycles, int smooth_down,
+                         int smooth_up, int smooth_bottom, int zerophi, int verbosity,
+                         mgp_report *report);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MGP2D_H */

@@ -1,0 +1,297 @@
+"""Python binding of the C ABI (include/mgp2d.h) with the call shapes of the
+Fortran module procedures it replaces.
+
+    from mgpoisson2d_b200 import vcycle, fmg, dc_vcycle, Solver
+    report = vcycle(phi, rhs, geo, bc, homog, tol=1e-10, maxiters=100)
+
+Arrays are ``BoxData`` (host NumPy or device torch); the library stages host
+arrays through device memory itself.  Every call raises ``MGPError`` on a
+non-zero status.  The library file must have been built
+(``python -m mgpoisson2d_b200.build``); importing this module raises
+ImportError otherwise -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from .types import (KIND_DD, KIND_MG, STATUS_NAMES, BdryData, Box, BoxData, GeoData, MgpArray, MgpBdry, MgpBox,
+                    MgpGeo, MgpReport, Report, make_report, read_report)
+
+FLAG_DIRICHLET_COUPLED_DIAG = 1
+FLAG_TIME_SMOOTHER = 2
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libmgp2d.so")
+
+if not os.path.exists(_LIB_PATH):
+    raise ImportError(f"mgpoisson2d_b200: CUDA library {_LIB_PATH} is missing; "
+                      "build it with `python -m mgpoisson2d_b200.build`")
+
+_lib = C.CDLL(_LIB_PATH)
+
+_P = C.POINTER
+_B, _A, _BC, _G, _R = _P(MgpBox), _P(MgpArray), _P(MgpBdry), _P(MgpGeo), _P(MgpReport)
+_i, _d, _vp = C.c_int, C.c_double, C.c_void_p
+
+_SIGS = {
+    "mgp_set_flags": [_i],
+    "mgp_estimate_maxdepth": [_P(_i), _B],
+    "mgp_create_mgschedule": [_P(_i), _P(_i), _P(_i), _B],
+    "mgp_fill_ghosts": [_B, _A, _BC, _G, _i, _i],
+    "mgp_extrapolate_ghosts": [_B, _A, _i],
+    "mgp_compute_invdiags": [_B, _A, _G, _BC, _i],
+    "mgp_compute_laplacian": [_B, _A, _A, _G, _BC, _i, _i],
+    "mgp_compute_residual": [_B, _A, _A, _A, _G, _BC, _i, _i],
+    "mgp_relax_gs": [_B, _A, _A, _G, _BC, _i, _A, _d, _d, _i, _i, _i],
+    "mgp_solve_bicgstab2": [_B, _A, _A, _G, _BC, _i, _A, _d, _i, _i, _i, _i],
+    "mgp_restrict": [_B, _A, _B, _A, _i, _i],
+    "mgp_prolong": [_B, _A, _B, _A, _G, _G, _BC, _i],
+    "mgp_pnorm": [_B, _A, _i, _P(_d)],
+    "mgp_inner_prod": [_B, _A, _A, _P(_d)],
+    "mgp_vcycle": [_B, _A, _A, _G, _BC, _i, _i, _i, _d, _i, _i, _i, _i, _i, _i, _i, _i, _R],
+    "mgp_fmg": [_B, _A, _A, _G, _BC, _i, _i, _i, _d, _i, _i, _i, _i, _i, _i, _i, _i, _R],
+    "mgp_dc_vcycle": [_B, _A, _A, _G, _BC, _i, _i, _i, _d, _i, _i, _i, _i, _i, _i, _i, _i, _R],
+    "mgp_solver_create": [_B, _G, _BC, _i, _i, _i, _P(_vp)],
+    "mgp_solver_destroy": [_vp],
+    "mgp_solver_set_stream": [_vp, _vp],
+    "mgp_solver_maxdepth": [_vp, _P(_i)],
+    "mgp_solver_vcycle": [_vp, _A, _A, _BC, _i, _d, _i, _i, _i, _i, _i, _i, _i, _R],
+    "mgp_solver_fmg": [_vp, _A, _A, _BC, _i, _d, _i, _i, _i, _i, _i, _i, _i, _R],
+    "mgp_solver_dc_vcycle": [_vp, _A, _A, _BC, _i, _d, _i, _i, _i, _i, _i, _i, _i, _R],
+}
+for _name, _args in _SIGS.items():
+    _f = getattr(_lib, _name)
+    _f.argtypes = _args
+    _f.restype = _i
+_lib.mgp_version.restype = C.c_char_p
+_lib.mgp_last_error.restype = C.c_char_p
+_lib.mgp_kernel_launch_count.restype = C.c_longlong
+
+#: every symbol include/mgp2d.h declares
+EXPORTS = sorted(list(_SIGS) + ["mgp_version", "mgp_last_error", "mgp_kernel_launch_count"])
+
+
+class MGPError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = _lib.mgp_last_error().decode(errors="replace")
+        super().__init__(f"{where}: {STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _ck(rc: int, where: str):
+    if rc != 0:
+        raise MGPError(rc, where)
+
+
+def _r(x):
+    return C.byref(x)
+
+
+def library_path() -> str:
+    return _LIB_PATH
+
+
+def kernel_launch_count() -> int:
+    return int(_lib.mgp_kernel_launch_count())
+
+
+def set_flags(flags: int) -> int:
+    """Process-wide flags for the calls without a flags argument (mgp_set_flags)."""
+    return int(_lib.mgp_set_flags(flags))
+
+
+# ---- schedule (MG:38-129) -------------------------------------------------- #
+def estimate_maxdepth(maxdepth: int, valid: Box) -> int:
+    m = C.c_int(maxdepth)
+    _ck(_lib.mgp_estimate_maxdepth(_r(m), _r(valid.c())), "estimate_maxdepth")
+    return m.value
+
+
+def create_mgschedule(maxdepth: int, valid: Box):
+    m = C.c_int(maxdepth)
+    rx = (C.c_int * max(maxdepth, 1))()
+    ry = (C.c_int * max(maxdepth, 1))()
+    _ck(_lib.mgp_create_mgschedule(rx, ry, _r(m), _r(valid.c())), "create_mgschedule")
+    return list(rx)[:m.value], list(ry)[:m.value], m.value
+
+
+# ---- operator-level calls --------------------------------------------------- #
+def fill_ghosts(phi: BoxData, bc: BdryData, geo: GeoData, homog: bool, do_neum: bool = True):
+    """fill_ghosts, arrayutils.f90:1277-1492."""
+    a, b, g = phi.c(), bc.c(), geo.c()
+    _ck(_lib.mgp_fill_ghosts(_r(phi.valid.c()), _r(a), _r(b), _r(g), int(homog), int(do_neum)), "fill_ghosts")
+
+
+def extrapolate_ghosts(phi: BoxData, order: int):
+    """extrapolate_ghosts, arrayutils.f90:1497-1566."""
+    a = phi.c()
+    _ck(_lib.mgp_extrapolate_ghosts(_r(phi.valid.c()), _r(a), order), "extrapolate_ghosts")
+
+
+def compute_invdiags(invdiags: BoxData, geo: GeoData, bc: BdryData, homog: bool):
+    """compute_invdiags, poisson2d.f90:16-388."""
+    a, b, g = invdiags.c(), bc.c(), geo.c()
+    _ck(_lib.mgp_compute_invdiags(_r(invdiags.valid.c()), _r(a), _r(g), _r(b), int(homog)), "compute_invdiags")
+
+
+def compute_laplacian(lap: BoxData, phi: BoxData, geo: GeoData, bc: BdryData, homog: bool, jscale: bool = False):
+    """compute_laplacian, poisson2d.f90:886-1319."""
+    l, p, b, g = lap.c(), phi.c(), bc.c(), geo.c()
+    _ck(_lib.mgp_compute_laplacian(_r(lap.valid.c()), _r(l), _r(p), _r(g), _r(b), int(homog), int(jscale)),
+        "compute_laplacian")
+
+
+def compute_residual(res: BoxData, rhs: BoxData, phi: BoxData, geo: GeoData, bc: BdryData, homog: bool,
+                     jscale: bool = False):
+    """compute_residual, poisson2d.f90:1327-1353."""
+    r, f, p, b, g = res.c(), rhs.c(), phi.c(), bc.c(), geo.c()
+    _ck(_lib.mgp_compute_residual(_r(res.valid.c()), _r(r), _r(f), _r(p), _r(g), _r(b), int(homog), int(jscale)),
+        "compute_residual")
+
+
+def relax_gs(phi: BoxData, rhs: BoxData, geo: GeoData, bc: BdryData, homog: bool, invdiags: BoxData, omega: float,
+             tol: float, maxiters: int, zerophi: bool, verbosity: int = 0):
+    """relax_gs, poisson2d.f90:1460-1988 (4-colour order on the device)."""
+    p, f, b, g, d = phi.c(), rhs.c(), bc.c(), geo.c(), invdiags.c()
+    _ck(_lib.mgp_relax_gs(_r(phi.valid.c()), _r(p), _r(f), _r(g), _r(b), int(homog), _r(d), omega, tol, maxiters,
+                          int(zerophi), verbosity), "relax_gs")
+
+
+def solve_bicgstab2(phi: BoxData, rhs: BoxData, geo: GeoData, bc: BdryData, homog: bool, invdiags: BoxData,
+                    tol: float, max_iters: int, max_restarts: int, zerophi: bool, verbosity: int = 0):
+    """solve_bicgstab2, poisson2d.f90:2253-2477."""
+    p, f, b, g, d = phi.c(), rhs.c(), bc.c(), geo.c(), invdiags.c()
+    _ck(_lib.mgp_solve_bicgstab2(_r(phi.valid.c()), _r(p), _r(f), _r(g), _r(b), int(homog), _r(d), tol, max_iters,
+                                 max_restarts, int(zerophi), verbosity), "solve_bicgstab2")
+
+
+def restrict(fine: BoxData, crse: BoxData):
+    """restrict, MGPoisson2D.f90:135-257."""
+    f, c = fine.c(), crse.c()
+    _ck(_lib.mgp_restrict(_r(fine.valid.c()), _r(f), _r(crse.valid.c()), _r(c), fine.offi, fine.offj), "restrict")
+
+
+def prolong(fine: BoxData, crse: BoxData, fine_geo: GeoData, crse_geo: GeoData, crse_bc: BdryData, order: int):
+    """prolong, MGPoisson2D.f90:262-394."""
+    f, c, fg, cg, b = fine.c(), crse.c(), fine_geo.c(), crse_geo.c(), crse_bc.c()
+    _ck(_lib.mgp_prolong(_r(fine.valid.c()), _r(f), _r(crse.valid.c()), _r(c), _r(fg), _r(cg), _r(b), order),
+        "prolong")
+
+
+def pnorm(bd: BoxData, p: int) -> float:
+    """pnorm, arrayutils.f90:753-796 (p = 0, 1, 2)."""
+    out = C.c_double()
+    a = bd.c()
+    _ck(_lib.mgp_pnorm(_r(bd.valid.c()), _r(a), p, _r(out)), "pnorm")
+    return out.value
+
+
+def inner_prod(a: BoxData, b: BoxData) -> float:
+    """inner_prod, arrayutils.f90:637-661."""
+    out = C.c_double()
+    x, y = a.c(), b.c()
+    _ck(_lib.mgp_inner_prod(_r(a.valid.c()), _r(x), _r(y), _r(out)), "inner_prod")
+    return out.value
+
+
+# ---- drivers with the Fortran argument lists ------------------------------- #
+def _driver(fn, name, phi, rhs, geo, bc, homog, tol, maxiters, maxdepth_user, numcycles, smooth_down, smooth_up,
+            smooth_bottom, zerophi, verbosity) -> Report:
+    rep, buf = make_report(maxiters)
+    p, f, b, g = phi.c(), rhs.c(), bc.c(), geo.c()
+    rc = fn(_r(rhs.valid.c()), _r(p), _r(f), _r(g), _r(b), int(homog), 0, 0, tol, maxiters, maxdepth_user, numcycles,
+            smooth_down, smooth_up, smooth_bottom, int(zerophi), verbosity, _r(rep))
+    _ck(rc, name)
+    return read_report(rep, buf)
+
+
+def vcycle(phi, rhs, geo, bc, homog, tol, maxiters, maxdepth_user=-1, numcycles=1, smooth_down=8, smooth_up=8,
+           smooth_bottom=8, zerophi=False, verbosity=0) -> Report:
+    """MGPoisson2D::vcycle, MGPoisson2D.f90:400-670."""
+    return _driver(_lib.mgp_vcycle, "vcycle", phi, rhs, geo, bc, homog, tol, maxiters, maxdepth_user, numcycles,
+                   smooth_down, smooth_up, smooth_bottom, zerophi, verbosity)
+
+
+def fmg(phi, rhs, geo, bc, homog, tol, maxiters, maxdepth_user=-1, numcycles=1, smooth_down=8, smooth_up=8,
+        smooth_bottom=8, zerophi=False, verbosity=0) -> Report:
+    """MGPoisson2D::fmg, MGPoisson2D.f90:860-1122."""
+    return _driver(_lib.mgp_fmg, "fmg", phi, rhs, geo, bc, homog, tol, maxiters, maxdepth_user, numcycles,
+                   smooth_down, smooth_up, smooth_bottom, zerophi, verbosity)
+
+
+def dc_vcycle(phi, rhs, geo, bc, homog, tol, maxiters, maxdepth_user=-1, numcycles=1, smooth_down=1, smooth_up=1,
+              smooth_bottom=1, zerophi=False, verbosity=0) -> Report:
+    """DeferredMGPoisson2D::vcycle, MGPoisson2D_DD.f90:589-862."""
+    return _driver(_lib.mgp_dc_vcycle, "dc_vcycle", phi, rhs, geo, bc, homog, tol, maxiters, maxdepth_user,
+                   numcycles, smooth_down, smooth_up, smooth_bottom, zerophi, verbosity)
+
+
+class Solver:
+    """A hierarchy built once and kept in HBM (mgp_solver_create).
+
+    ``kind`` is KIND_MG (vcycle / fmg) or KIND_DD (deferred-correction vcycle);
+    ``flags`` e.g. FLAG_DIRICHLET_COUPLED_DIAG.
+    """
+
+    def __init__(self, valid: Box, geo: GeoData, bc: BdryData, kind: int = KIND_MG, flags: int = 0,
+                 maxdepth_user: int = -1):
+        self._h = C.c_void_p()
+        b, g = bc.c(), geo.c()
+        _ck(_lib.mgp_solver_create(_r(valid.c()), _r(g), _r(b), kind, flags, maxdepth_user, _r(self._h)),
+            "solver_create")
+        self.valid, self.kind, self.flags = valid, kind, flags
+        md = C.c_int()
+        _lib.mgp_solver_maxdepth(self._h, _r(md))
+        self.maxdepth = md.value
+
+    def close(self):
+        if self._h:
+            _lib.mgp_solver_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_stream(self, stream_handle: int):
+        _ck(_lib.mgp_solver_set_stream(self._h, C.c_void_p(stream_handle)), "solver_set_stream")
+
+    def _solve(self, fn, name, phi, rhs, bc, homog, tol, maxiters, numcycles, nd, nu, nb, zerophi, verbosity):
+        rep, buf = make_report(maxiters)
+        p, f, b = phi.c(), rhs.c(), bc.c()
+        _ck(fn(self._h, _r(p), _r(f), _r(b), int(homog), tol, maxiters, numcycles, nd, nu, nb, int(zerophi),
+               verbosity, _r(rep)), name)
+        return read_report(rep, buf)
+
+    def vcycle(self, phi, rhs, bc, homog, tol, maxiters, numcycles=1, smooth_down=8, smooth_up=8, smooth_bottom=8,
+               zerophi=False, verbosity=0) -> Report:
+        return self._solve(_lib.mgp_solver_vcycle, "solver_vcycle", phi, rhs, bc, homog, tol, maxiters, numcycles,
+                           smooth_down, smooth_up, smooth_bottom, zerophi, verbosity)
+
+    def fmg(self, phi, rhs, bc, homog, tol, maxiters, numcycles=1, smooth_down=8, smooth_up=8, smooth_bottom=8,
+            zerophi=False, verbosity=0) -> Report:
+        return self._solve(_lib.mgp_solver_fmg, "solver_fmg", phi, rhs, bc, homog, tol, maxiters, numcycles,
+                           smooth_down, smooth_up, smooth_bottom, zerophi, verbosity)
+
+    def dc_vcycle(self, phi, rhs, bc, homog, tol, maxiters, numcycles=1, smooth_down=1, smooth_up=1, smooth_bottom=1,
+                  zerophi=False, verbosity=0) -> Report:
+        return self._solve(_lib.mgp_solver_dc_vcycle, "solver_dc_vcycle", phi, rhs, bc, homog, tol, maxiters,
+                           numcycles, smooth_down, smooth_up, smooth_bottom, zerophi, verbosity)
+
+
+__all__ = ["vcycle", "fmg", "dc_vcycle", "Solver", "fill_ghosts", "extrapolate_ghosts", "compute_invdiags",
+           "compute_laplacian", "compute_residual", "relax_gs", "solve_bicgstab2", "restrict", "prolong", "pnorm",
+           "inner_prod", "estimate_maxdepth", "create_mgschedule", "MGPError", "library_path", "kernel_launch_count",
+           "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "EXPORTS", "KIND_MG", "KIND_DD"]

@@ -1,0 +1,465 @@
+// mgp_core.cuh -- device-side building blocks of the B200 multigrid solver.
+//
+// Everything here is FP64 and is compiled with -fmad=false, so each product
+// and sum is rounded on its own in the order the Fortran routines write them:
+// a cell computed here is bit-identical to the same cell computed by the
+// Fortran code (and by the CPU oracle).
+//
+// Citations: AU = arrayutils.f90, P2 = poisson2d.f90, MG = MGPoisson2D.f90,
+// DD = MGPoisson2D_DD.f90 (EdSantilli/MGPoisson2D, src/).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mgp {
+
+constexpr double kBogus = 1.2345e300;   // precision.f90:53
+enum { RLO = 0, RMID = 1, RHI = 2 };
+enum { T_NONE = -1, T_NEUM = 0, T_DIRI = 1, T_PERIODIC = 2, T_CF = 3, T_EX0 = 4, T_EX1 = 5, T_EX2 = 6 };
+enum { M_UNIFORM = 0, M_NONUNIFORM = 1, M_LAH = 2 };
+enum { S_XLO = 0, S_XHI = 1, S_YLO = 2, S_YHI = 3 };
+
+// A 2-D FP64 field; p points at valid element (0,0), ld is the row pitch.
+struct DF {
+    double* p;
+    int ld;
+};
+#define AT(f, i, j) ((f).p[(long)(i) + (long)(j) * (long)(f).ld])
+
+struct Geo {
+    DF J, xx, xy, yx, yy;   // J cell-centred; xx, xy on x-faces; yx, yy on y-faces
+    double dx, dy, idx, idy;
+};
+
+// Boundary conditions of one level (type(bdry_data), AU:55-70).
+struct BCd {
+    int type[4];
+    int mode[4];
+    const double* d[4];   // NONUNIFORM values in device memory, else nullptr
+    double u[4];          // UNIFORM values
+    int kyhi;             // index of the north-face Neumann value the operator reads (P2: data_yhi(j), j = jhi)
+    int koffy;            // offset of y-side NONUNIFORM Dirichlet values (AU:1224: bcd(jlo:jhi))
+};
+
+// One multigrid level as the kernels see it.
+struct Lv {
+    int nx, ny;
+    Geo g;
+    BCd bc;
+    DF e;      // correction, 1 ghost layer
+    DF r;      // right-hand side of the residual equation
+    DF w;      // work (residual before restriction)
+    DF invd;   // inverse diagonal
+    DF ea;     // extra arrays for the bottom solver (1 ghost): e_loc, p_tilde, s_tilde
+    DF pt, st;
+    DF rr, rt, pp, tt, vv;   // bottom solver, no ghosts
+};
+
+__device__ __forceinline__ int region(int i, int n, bool per_lo, bool per_hi) {
+    if (i == 0 && !per_lo) return RLO;
+    if (i == n - 1 && !per_hi) return RHI;
+    return RMID;
+}
+
+// ---------------------------------------------------------------------------
+// The mapped 9-point operator, P2:886-1319
+// ---------------------------------------------------------------------------
+struct St9 {
+    double p, pe, pw, pn, ps, ee, ew, en, es, ene, enw, ese, esw;
+};
+
+// Reads phi around the cell from global memory.
+struct GLoad {
+    const double* c;
+    long ld;
+    __device__ __forceinline__ double operator()(int di, int dj) const { return c[di + (long)dj * ld]; }
+};
+
+// A unit impulse at the cell, zero elsewhere; the four own-row/column ghosts
+// may carry the Dirichlet coupling (-3) for the coupled diagonal.
+struct DeltaLoad {
+    double gw, ge, gs, gn;
+    __device__ __forceinline__ double operator()(int di, int dj) const {
+        if (di == 0 && dj == 0) return 1.0;
+        if (dj == 0 && di == -1) return gw;
+        if (dj == 0 && di == 1) return ge;
+        if (di == 0 && dj == -1) return gs;
+        if (di == 0 && dj == 1) return gn;
+        return 0.0;
+    }
+};
+
+// The transverse values of the nine region blocks of compute_laplacian.
+template <class L>
+__device__ __forceinline__ void gather9(const L& P, int xr, int yr, St9& s) {
+    const double p = P(0, 0), pe = P(1, 0), pw = P(-1, 0), pn = P(0, 1), ps = P(0, -1);
+    double ee, ew, en, es, ene, enw, ese, esw;
+    s.p = p; s.pe = pe; s.pw = pw; s.pn = pn; s.ps = ps;
+    if (yr == RLO) {
+        if (xr == RLO) {              // P2:937-958
+            ee = P(1, 0); en = P(0, 1);
+            ew = 3.0 * (p - ee) + P(2, 0);
+            es = 3.0 * (p - en) + P(0, 2);
+            ene = P(1, 1);
+            enw = 3.0 * (en - ene) + P(2, 1);
+            ese = 3.0 * (ee - ene) + P(1, 2);
+            esw = 0.5 * ((3.0 * (es - ese) + P(2, -1)) + (3.0 * (ew - enw) + P(-1, 2)));
+        } else if (xr == RMID) {      // P2:986-1002
+            ee = P(1, 0); ew = P(-1, 0); en = P(0, 1);
+            es = 3.0 * (p - en) + P(0, 2);
+            ene = P(1, 1); enw = P(-1, 1);
+            ese = 3.0 * (ee - ene) + P(1, 2);
+            esw = 3.0 * (ew - enw) + P(-1, 2);
+        } else {                      // P2:1021-1039
+            ew = P(-1, 0); en = P(0, 1);
+            ee = 3.0 * (p - ew) + P(-2, 0);
+            es = 3.0 * (p - en) + P(0, 2);
+            enw = P(-1, 1);
+            ene = 3.0 * (pn - enw) + P(-2, 1);
+            esw = 3.0 * (pw - enw) + P(-1, 2);
+            ese = 0.5 * ((3.0 * (es - esw) + P(-2, -1)) + (3.0 * (ee - ene) + P(1, 2)));
+        }
+    } else if (yr == RMID) {
+        if (xr == RLO) {              // P2:1068-1085
+            ee = P(1, 0); en = P(0, 1); es = P(0, -1);
+            ew = 3.0 * (p - ee) + P(2, 0);
+            ene = P(1, 1); ese = P(1, -1);
+            enw = 3.0 * (en - ene) + P(2, 1);
+            esw = 3.0 * (es - ese) + P(2, -1);
+        } else if (xr == RMID) {      // P2:1103-1125
+            ee = P(1, 0); ew = P(-1, 0); en = P(0, 1); es = P(0, -1);
+            ene = P(1, 1); enw = P(-1, 1); ese = P(1, -1); esw = P(-1, -1);
+        } else {                      // P2:1128-1147
+            ew = P(-1, 0); en = P(0, 1); es = P(0, -1);
+            ee = 3.0 * (p - ew) + P(-2, 0);
+            enw = P(-1, 1); esw = P(-1, -1);
+            ene = 3.0 * (en - enw) + P(-2, 1);
+            ese = 3.0 * (es - esw) + P(-2, -1);
+        }
+    } else {
+        if (xr == RLO) {              // P2:1176-1194
+            ee = P(1, 0); es = P(0, -1);
+            ew = 3.0 * (p - ee) + P(2, 0);
+            en = 3.0 * (p - es) + P(0, -2);
+            ese = P(1, -1);
+            ene = 3.0 * (ee - ese) + P(1, -2);
+            esw = 3.0 * (es - ese) + P(2, -1);
+            enw = 0.5 * ((3.0 * (ew - esw) + P(-1, -2)) + (3.0 * (en - ene) + P(2, 1)));
+        } else if (xr == RMID) {      // P2:1223-1239
+            ee = P(1, 0); ew = P(-1, 0); es = P(0, -1);
+            en = 3.0 * (p - es) + P(0, -2);
+            ese = P(1, -1); esw = P(-1, -1);
+            ene = 3.0 * (ee - ese) + P(1, -2);
+            enw = 3.0 * (ew - esw) + P(-1, -2);
+        } else {                      // P2:1258-1276
+            ew = P(-1, 0); es = P(0, -1);
+            ee = 3.0 * (p - ew) + P(-2, 0);
+            en = 3.0 * (p - es) + P(0, -2);
+            esw = P(-1, -1);
+            enw = 3.0 * (ew - esw) + P(-1, -2);
+            ese = 3.0 * (es - esw) + P(-2, -1);
+            ene = 0.5 * ((3.0 * (en - enw) + P(-2, 1)) + (3.0 * (ee - ese) + P(1, -2)));
+        }
+    }
+    s.ee = ee; s.ew = ew; s.en = en; s.es = es;
+    s.ene = ene; s.enw = enw; s.ese = ese; s.esw = esw;
+}
+
+__device__ __forceinline__ double nbval(const BCd& b, int homog, int s, int k) {
+    if (homog) return 0.0;
+    if (b.mode[s] == M_UNIFORM) return b.u[s];
+    return b.d[s][k];
+}
+
+// (xfe - xfw)/dx + (yfn - yfs)/dy with Neumann faces replaced by the BC flux.
+__device__ __forceinline__ double lap9(const St9& s, const Geo& g, int i, int j, int xr, int yr,
+                                       const BCd& b, int homog) {
+    const double idx = g.idx, idy = g.idy;
+    double xfe = AT(g.xx, i + 1, j) * (s.pe - s.p) * idx + AT(g.xy, i + 1, j) * 0.25 * (s.ene - s.ese + s.en - s.es) * idy;
+    double xfw = AT(g.xx, i, j) * (s.p - s.pw) * idx + AT(g.xy, i, j) * 0.25 * (s.en - s.es + s.enw - s.esw) * idy;
+    double yfn = AT(g.yy, i, j + 1) * (s.pn - s.p) * idy + AT(g.yx, i, j + 1) * 0.25 * (s.ene - s.enw + s.ee - s.ew) * idx;
+    double yfs = AT(g.yy, i, j) * (s.p - s.ps) * idy + AT(g.yx, i, j) * 0.25 * (s.ee - s.ew + s.ese - s.esw) * idx;
+    if (xr == RLO && b.type[S_XLO] == T_NEUM) xfw = nbval(b, homog, S_XLO, j);
+    if (yr == RLO && b.type[S_YLO] == T_NEUM) yfs = nbval(b, homog, S_YLO, i);
+    if (xr == RHI && b.type[S_XHI] == T_NEUM) xfe = nbval(b, homog, S_XHI, j);
+    if (yr == RHI && b.type[S_YHI] == T_NEUM) yfn = nbval(b, homog, S_YHI, b.kyhi);
+    return (xfe - xfw) * idx + (yfn - yfs) * idy;
+}
+
+struct Per {
+    bool xl, xh, yl, yh;
+};
+__device__ __forceinline__ Per periodic_of(const BCd& b) {
+    Per p;
+    p.xl = b.type[S_XLO] == T_PERIODIC; p.xh = b.type[S_XHI] == T_PERIODIC;
+    p.yl = b.type[S_YLO] == T_PERIODIC; p.yh = b.type[S_YHI] == T_PERIODIC;
+    return p;
+}
+
+// L[phi] at (i,j); phi's ghosts must be set.
+__device__ __forceinline__ double apply9(const DF& phi, const Geo& g, const BCd& b, int homog, int nx, int ny,
+                                         int i, int j) {
+    const Per pr = periodic_of(b);
+    const int xr = region(i, nx, pr.xl, pr.xh), yr = region(j, ny, pr.yl, pr.yh);
+    St9 s;
+    gather9(GLoad{&AT(phi, i, j), phi.ld}, xr, yr, s);
+    return lap9(s, g, i, j, xr, yr, b, homog);
+}
+
+// Diagonal of the operator at (i,j) (compute_invdiags, P2:16-388), before inversion.
+__device__ __forceinline__ double diag9(const Geo& g, const BCd& b, int homog, int nx, int ny, int i, int j,
+                                        bool diri_coupled) {
+    const Per pr = periodic_of(b);
+    const int xr = region(i, nx, pr.xl, pr.xh), yr = region(j, ny, pr.yl, pr.yh);
+    DeltaLoad D{0.0, 0.0, 0.0, 0.0};
+    if (diri_coupled) {
+        if (xr == RLO && b.type[S_XLO] == T_DIRI) D.gw = -3.0;
+        if (xr == RHI && b.type[S_XHI] == T_DIRI) D.ge = -3.0;
+        if (yr == RLO && b.type[S_YLO] == T_DIRI) D.gs = -3.0;
+        if (yr == RHI && b.type[S_YHI] == T_DIRI) D.gn = -3.0;
+    }
+    St9 s;
+    gather9(D, xr, yr, s);
+    return lap9(s, g, i, j, xr, yr, b, homog);
+}
+
+// One Gauss-Seidel update of (i,j) (P2:1768-1771).
+__device__ __forceinline__ void gs9(const DF& phi, const DF& rhs, const DF& invd, const Geo& g, const BCd& b,
+                                    int homog, int nx, int ny, int i, int j, double omega) {
+    const double lphi = apply9(phi, g, b, homog, nx, ny, i, j);
+    const double p = AT(phi, i, j);
+    const double newphi = p + (AT(rhs, i, j) - lphi) * AT(invd, i, j);
+    AT(phi, i, j) = omega * newphi + (1.0 - omega) * p;
+}
+
+// Colour c of the 4-colour sweep: (i mod 2, j mod 2) = (0,0), (1,1), (1,0), (0,1).
+__device__ __forceinline__ int colour_ci(int c) { return (c == 1 || c == 2) ? 1 : 0; }
+__device__ __forceinline__ int colour_cj(int c) { return (c == 1 || c == 3) ? 1 : 0; }
+
+// ---------------------------------------------------------------------------
+// Ghost fills, AU:871-1492.  Each function returns the final value of one
+// ghost cell of one side, given the array state the Fortran loop sees.
+// ---------------------------------------------------------------------------
+
+// Dirichlet, order 3 (AU:1161-1177, AU:1215-1231).  k = index along the side.
+__device__ __forceinline__ double ghost_diri(const BCd& b, int homog, int s, int k, double p0, double p1, double p2) {
+    const double sixteenfifth = 16.0 / 5.0, fifth = 1.0 / 5.0;
+    if (b.mode[s] == M_LAH) return -p0;
+    if (homog) return -(3.0 * p0) + p1 - fifth * p2;
+    if (b.mode[s] == M_UNIFORM) return sixteenfifth * b.u[s] - 3.0 * p0 + p1 - fifth * p2;
+    const double g = (s < 2) ? b.d[s][k] : b.d[s][b.koffy + k];
+    return sixteenfifth * g - 3.0 * p0 + p1 - fifth * p2;
+}
+
+// Neumann on an x side (AU:926-985), ghost of row j.  Which formula last wrote
+// row j depends on homog: homogeneous fills are one-sided at both ends;
+// inhomogeneous fills rewrite jlo with the centred formula (which reads the y
+// ghosts at jlo-1).
+__device__ __forceinline__ double ghost_neum_x(const DF& p, const Geo& g, const BCd& b, int homog, int s, int nx,
+                                               int ny, int j) {
+    const bool lo = (s == S_XLO);
+    const int e = lo ? -1 : 1, i = lo ? 0 : nx - 1;
+    const double dx = lo ? -g.dx : g.dx, dy = g.dy;
+    if (b.mode[s] == M_LAH) return AT(p, i, j);
+    double dpn, dpf, cross;
+    const bool onesided_lo = (j == 0) && homog;
+    const bool onesided_hi = (j == ny - 1);
+    if (onesided_lo) {
+        dpn = -((3.0 * AT(p, i, j) - 4.0 * AT(p, i, j + 1) + AT(p, i, j + 2)) * 0.5 / dy);
+        dpf = -((3.0 * AT(p, i - e, j) - 4.0 * AT(p, i - e, j + 1) + AT(p, i - e, j + 2)) * 0.5 / dy);
+        cross = 0.5 * (3.0 * dpn - dpf) * AT(g.xy, i, j);
+    } else if (onesided_hi) {
+        dpn = (3.0 * AT(p, i, j) - 4.0 * AT(p, i, j - 1) + AT(p, i, j - 2)) * 0.5 / dy;
+        dpf = (3.0 * AT(p, i - e, j) - 4.0 * AT(p, i - e, j - 1) + AT(p, i - e, j - 2)) * 0.5 / dy;
+        cross = 0.5 * (3.0 * dpn - dpf) * AT(g.xy, i, j);
+    } else {
+        dpn = (AT(p, i, j + 1) - AT(p, i, j - 1)) * 0.5 / dy;
+        dpf = (AT(p, i - e, j + 1) - AT(p, i - e, j - 1)) * 0.5 / dy;
+        cross = (1.5 * dpn - 0.5 * dpf) * AT(g.xy, i, j);
+    }
+    if (homog) return AT(p, i, j) - (-cross) * dx / AT(g.xx, i, j);
+    const double bv = (b.mode[s] == M_UNIFORM) ? b.u[s] : b.d[s][j];
+    return AT(p, i, j) - (bv - cross) * dx / AT(g.xx, i, j);
+}
+
+// Neumann on a y side (AU:990-1062), ghost of column i.  Column ilo always
+// ends with the centred formula (it reads the x ghosts), ihi one-sided.
+__device__ __forceinline__ double ghost_neum_y(const DF& p, const Geo& g, const BCd& b, int homog, int s, int nx,
+                                               int ny, int i) {
+    const bool lo = (s == S_YLO);
+    const int e = lo ? -1 : 1, j = lo ? 0 : ny - 1;
+    const double dy = lo ? -g.dy : g.dy, dx = g.dx;
+    if (b.mode[s] == M_LAH) return AT(p, i, j);
+    double dpn, dpf, cross;
+    if (i == nx - 1) {
+        dpn = (3.0 * AT(p, i, j) - 4.0 * AT(p, i - 1, j) + AT(p, i - 2, j)) * 0.5 / dx;
+        dpf = (3.0 * AT(p, i, j - e) - 4.0 * AT(p, i - 1, j - e) + AT(p, i - 2, j - e)) * 0.5 / dx;
+        cross = 0.5 * (3.0 * dpn - dpf) * AT(g.yx, i, j);
+    } else {
+        dpn = (AT(p, i + 1, j) - AT(p, i - 1, j)) * 0.5 / dx;
+        dpf = (AT(p, i + 1, j - e) - AT(p, i - 1, j - e)) * 0.5 / dx;
+        cross = (1.5 * dpn - 0.5 * dpf) * AT(g.yx, i, j);
+    }
+    if (homog) return AT(p, i, j) - (-cross) * dy / AT(g.yy, i, j);
+    const double bv = (b.mode[s] == M_UNIFORM) ? b.u[s] : b.d[s][i];
+    return AT(p, i, j) - (bv - cross) * dy / AT(g.yy, i, j);
+}
+
+// Number of ghost cells a side's fill writes, and the first index.
+__device__ __forceinline__ void side_range(const BCd& b, int s, int nx, int ny, int do_neum, int& lo, int& cnt) {
+    const int t = b.type[s];
+    const int n = (s < 2) ? ny : nx;
+    lo = 0;
+    cnt = 0;
+    if (t == T_NEUM) { if (do_neum) cnt = n; }
+    else if (t == T_DIRI || t == T_PERIODIC) cnt = n;
+    else if (t == T_EX0 || t == T_EX1 || t == T_EX2) { lo = -1; cnt = n + 2; }   // whole column/row incl. ghosts
+}
+
+// Ghost k of side s (k counted from `lo` of side_range).  Returns false if the
+// side writes nothing there.  Writes the value.
+__device__ __forceinline__ void fill_side_elem(const DF& p, const Geo& g, const BCd& b, int homog, int s, int nx,
+                                               int ny, int k) {
+    const int t = b.type[s];
+    if (s < 2) {
+        const bool lo = (s == S_XLO);
+        const int i = lo ? 0 : nx - 1, e = lo ? -1 : 1;
+        double v;
+        if (t == T_NEUM) v = ghost_neum_x(p, g, b, homog, s, nx, ny, k);
+        else if (t == T_DIRI) v = ghost_diri(b, homog, s, k, AT(p, i, k), AT(p, i - e, k), AT(p, i - 2 * e, k));
+        else if (t == T_PERIODIC) v = lo ? AT(p, nx - 1, k) : AT(p, 0, k);
+        else {
+            const double v0 = AT(p, i, k), v1 = AT(p, i - e, k), v2 = AT(p, i - 2 * e, k);
+            v = (t == T_EX0) ? v0 : (t == T_EX1) ? 2.0 * v0 - v1 : 3.0 * (v0 - v1) + v2;
+        }
+        AT(p, i + e, k) = v;
+    } else {
+        const bool lo = (s == S_YLO);
+        const int j = lo ? 0 : ny - 1, e = lo ? -1 : 1;
+        double v;
+        if (t == T_NEUM) v = ghost_neum_y(p, g, b, homog, s, nx, ny, k);
+        else if (t == T_DIRI) v = ghost_diri(b, homog, s, k, AT(p, k, j), AT(p, k, j - e), AT(p, k, j - 2 * e));
+        else if (t == T_PERIODIC) v = lo ? AT(p, k, ny - 1) : AT(p, k, 0);
+        else {
+            const double v0 = AT(p, k, j), v1 = AT(p, k, j - e), v2 = AT(p, k, j - 2 * e);
+            v = (t == T_EX0) ? v0 : (t == T_EX1) ? 2.0 * v0 - v1 : 3.0 * (v0 - v1) + v2;
+        }
+        AT(p, k, j + e) = v;
+    }
+}
+
+// Corner ghosts, AU:1460-1490.  Corner c = 0..3: (-1,-1), (-1,ny), (nx,-1), (nx,ny).
+__device__ __forceinline__ void fill_corner(const DF& p, const BCd& b, int nx, int ny, int c) {
+    const bool px = b.type[S_XLO] == T_PERIODIC, py = b.type[S_YLO] == T_PERIODIC;
+    const int ci = (c >= 2) ? nx : -1, cj = (c & 1) ? ny : -1;
+    double v;
+    if (!px && !py) v = kBogus;
+    else if (px && py) v = AT(p, ci < 0 ? nx - 1 : 0, cj < 0 ? ny - 1 : 0);
+    else if (px) v = AT(p, ci < 0 ? nx - 1 : 0, cj);
+    else v = AT(p, ci, cj < 0 ? ny - 1 : 0);
+    AT(p, ci, cj) = v;
+}
+
+// extrapolate_ghosts value for an x-ghost column (lo/hi) at row a, AU:1497-1566.
+__device__ __forceinline__ double extrap_val(int order, double v0, double v1, double v2, double v3) {
+    switch (order) {
+        case 0: return v0;
+        case 1: return 2.0 * v0 - v1;
+        case 2: return 3.0 * (v0 - v1) + v2;
+        default: return 4.0 * (v0 + v2) - 6.0 * v1 - v3;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Transfers, MG:135-394
+// ---------------------------------------------------------------------------
+// Cell-centred restriction (MG:145-158): sum in the Fortran loop order.
+__device__ __forceinline__ double restrict_cc(const DF& f, int ci, int cj, int refx, int refy, double scale) {
+    double acc = 0.0;
+    for (int a = 0; a < refy; ++a)
+        for (int c = 0; c < refx; ++c) acc = acc + scale * AT(f, ci * refx + c, cj * refy + a);
+    return acc;
+}
+
+// ---------------------------------------------------------------------------
+// Deferred-correction operators, DD:45-334
+// ---------------------------------------------------------------------------
+// Value of phi at (i,j) after extrapolate_ghosts(phi, 0): indices clamped to the valid region.
+__device__ __forceinline__ double clampv(const DF& p, int nx, int ny, int i, int j) {
+    i = i < 0 ? 0 : (i > nx - 1 ? nx - 1 : i);
+    j = j < 0 ? 0 : (j > ny - 1 ? ny - 1 : j);
+    return AT(p, i, j);
+}
+
+// Value of phi at a neighbour after fill_ghosts with LAH BCs (AU:935-936, AU:1135-1136):
+// Dirichlet ghost = -cell, Neumann ghost = cell, periodic = wrapped.  (i,j) is a
+// valid cell and (di,dj) a unit step.
+__device__ __forceinline__ double lahv(const DF& p, const BCd& b, int nx, int ny, int i, int j, int di, int dj) {
+    const int ii = i + di, jj = j + dj;
+    int s = -1;
+    if (ii < 0) s = S_XLO;
+    else if (ii >= nx) s = S_XHI;
+    else if (jj < 0) s = S_YLO;
+    else if (jj >= ny) s = S_YHI;
+    if (s < 0) return AT(p, ii, jj);
+    const int t = b.type[s];
+    if (t == T_PERIODIC) {
+        const int wi = (ii + nx) % nx, wj = (jj + ny) % ny;
+        return AT(p, wi, wj);
+    }
+    if (t == T_DIRI) return -AT(p, i, j);
+    if (t == T_NEUM) return AT(p, i, j);
+    return AT(p, ii, jj);   // other types leave the ghost as stored
+}
+
+// Lagged corner cross terms of the DD smoother's modified rhs (DD:226-250).
+__device__ __forceinline__ double dd_modrhs(const DF& phi, const DF& rhs, const Geo& g, int nx, int ny, int i, int j) {
+    const double xyscale = 0.5 * g.idx * g.idy;
+    const double pne = clampv(phi, nx, ny, i + 1, j + 1), pnw = clampv(phi, nx, ny, i - 1, j + 1);
+    const double psw = clampv(phi, nx, ny, i - 1, j - 1), pse = clampv(phi, nx, ny, i + 1, j - 1);
+    const double gxye = AT(g.xy, i + 1, j) * (pne - pse);
+    const double gxyw = AT(g.xy, i, j) * (pnw - psw);
+    const double gyxn = AT(g.yx, i, j + 1) * (pne - pnw);
+    const double gyxs = AT(g.yx, i, j) * (pse - psw);
+    return AT(rhs, i, j) - (gxye - gxyw + gyxn - gyxs) * xyscale;
+}
+
+// DD compute_laplacian (DD:45-119) at (i,j), reading phi's valid cells only.
+__device__ __forceinline__ double dd_apply(const DF& phi, const Geo& g, const BCd& b, int nx, int ny, int i, int j) {
+    const double xyscale = 0.25 * g.idx * g.idy;
+    double pe = clampv(phi, nx, ny, i + 1, j), pw = clampv(phi, nx, ny, i - 1, j);
+    double pn = clampv(phi, nx, ny, i, j + 1), ps = clampv(phi, nx, ny, i, j - 1);
+    const double pne = clampv(phi, nx, ny, i + 1, j + 1), pnw = clampv(phi, nx, ny, i - 1, j + 1);
+    const double psw = clampv(phi, nx, ny, i - 1, j - 1), pse = clampv(phi, nx, ny, i + 1, j - 1);
+    const double gxye = AT(g.xy, i + 1, j) * (pne - pse + pn - ps);
+    const double gxyw = AT(g.xy, i, j) * (pn - ps + pnw - psw);
+    const double gyxn = AT(g.yx, i, j + 1) * (pne - pnw + pe - pw);
+    const double gyxs = AT(g.yx, i, j) * (pe - pw + pse - psw);
+    const double cross = (gxye - gxyw + gyxn - gyxs) * xyscale;
+    const double p = AT(phi, i, j);
+    pe = lahv(phi, b, nx, ny, i, j, 1, 0);
+    pw = lahv(phi, b, nx, ny, i, j, -1, 0);
+    pn = lahv(phi, b, nx, ny, i, j, 0, 1);
+    ps = lahv(phi, b, nx, ny, i, j, 0, -1);
+    const double xfe = AT(g.xx, i + 1, j) * (pe - p) * g.idx;
+    const double xfw = AT(g.xx, i, j) * (p - pw) * g.idx;
+    const double yfn = AT(g.yy, i, j + 1) * (pn - p) * g.idy;
+    const double yfs = AT(g.yy, i, j) * (p - ps) * g.idy;
+    return cross + (xfe - xfw) * g.idx + (yfn - yfs) * g.idy;
+}
+
+// One DD Gauss-Seidel update (DD:288-306); phi's ghosts hold the LAH fill.
+__device__ __forceinline__ void dd_gs(const DF& phi, const DF& modrhs, const DF& invd, const Geo& g, int i, int j,
+                                      double omega) {
+    const double p = AT(phi, i, j), pe = AT(phi, i + 1, j), pw = AT(phi, i - 1, j);
+    const double pn = AT(phi, i, j + 1), ps = AT(phi, i, j - 1);
+    const double xfe = AT(g.xx, i + 1, j) * (pe - p) * g.idx;
+    const double xfw = AT(g.xx, i, j) * (p - pw) * g.idx;
+    const double yfn = AT(g.yy, i, j + 1) * (pn - p) * g.idy;
+    const double yfs = AT(g.yy, i, j) * (p - ps) * g.idy;
+    const double lphi = (xfe - xfw) * g.idx + (yfn - yfs) * g.idy;
+    const double newphi = p + (AT(modrhs, i, j) - lphi) * AT(invd, i, j);
+    AT(phi, i, j) = omega * newphi + (1.0 - omega) * p;
+}
+
+}  // namespace mgp

@@ -1,0 +1,1124 @@
+// mgp_host.cu -- host side of the B200 multigrid solver: hierarchy set-up,
+// the V-cycle / FMG / deferred-correction drivers, array staging and the C ABI
+// declared in include/mgp2d.h.
+//
+// The drivers follow MGPoisson2D.f90 (vcycle MG:400-670, vcycle_noinit
+// MG:675-854, fmg MG:860-1122, fmg_noinit MG:1127-1189) and
+// MGPoisson2D_DD.f90 (vcycle DD:589-862, vcycle_noinit DD:867-1045) step for
+// step; the levels small enough for one CTA run their whole sub-cycle in
+// k_coarse_cycle.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mgp2d.h"
+#include "mgp_kernels.cuh"
+
+using namespace mgp;
+
+namespace {
+
+thread_local std::string g_err;
+int g_flags = 0;
+
+int set_err(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(x)                                                                                     \
+    do {                                                                                          \
+        cudaError_t e_ = (x);                                                                     \
+        if (e_ != cudaSuccess) return set_err(MGP_ECUDA, "%s: %s", #x, cudaGetErrorString(e_));   \
+    } while (0)
+#define RC(x)                   \
+    do {                        \
+        int r_ = (x);           \
+        if (r_) return r_;      \
+    } while (0)
+
+// Levels with at most this many cells run inside the single-CTA coarse cycle.
+constexpr long kCoarseCells = 4096;
+
+// ---------------------------------------------------------------------------
+// Device memory: every field of a solver comes out of one allocation.
+// ---------------------------------------------------------------------------
+struct Spec {
+    DF* dst;
+    int nxv, nyv, g;
+    size_t off;   // element offset of the field's block
+};
+
+struct Arena {
+    std::vector<Spec> specs;
+    size_t elems = 0;
+    double* base = nullptr;
+    void add(DF* dst, int nxv, int nyv, int g) {
+        const int ld = ((nxv + 2 * g + 31) / 32) * 32;
+        const size_t pad = g ? 32 : 0;
+        const size_t n = (size_t)(nyv + 2 * g) * ld + 2 * pad;
+        Spec s{dst, nxv, nyv, g, elems};
+        specs.push_back(s);
+        dst->ld = ld;
+        elems += (n + 31) / 32 * 32;
+    }
+    int commit(cudaStream_t st) {
+        if (elems == 0) return MGP_OK;
+        if (cudaMalloc(&base, elems * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            base = nullptr;
+            return set_err(MGP_ENOMEM, "cudaMalloc of %zu bytes failed", elems * sizeof(double));
+        }
+        for (auto& s : specs) {
+            const size_t pad = s.g ? 32 : 0;
+            s.dst->p = base + s.off + pad + (size_t)s.g * s.dst->ld;
+        }
+        CK(cudaMemsetAsync(base, 0, elems * sizeof(double), st));   // fresh arrays start at zero
+        return MGP_OK;
+    }
+    void release() {
+        if (base) cudaFree(base);
+        base = nullptr;
+        specs.clear();
+        elems = 0;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Argument checks and staging of caller arrays
+// ---------------------------------------------------------------------------
+int check_box(const mgp_box* v) {
+    if (!v) return set_err(MGP_EINVAL, "null box");
+    if (v->nx != v->ihi - v->ilo + 1 || v->ny != v->jhi - v->jlo + 1)
+        return set_err(MGP_EINVAL, "box extents are inconsistent (nx=%d ilo=%d ihi=%d)", v->nx, v->ilo, v->ihi);
+    if (v->nx < 3 || v->ny < 3) return set_err(MGP_EINVAL, "the operator needs at least 3 cells per direction");
+    if (!(v->dx > 0) || !(v->dy > 0)) return set_err(MGP_EINVAL, "dx and dy must be positive");
+    return MGP_OK;
+}
+
+int array_ld(const mgp_array* a, int nxv) { return a->ld ? a->ld : nxv + 2 * a->ngx; }
+
+int check_array(const mgp_array* a, int nxv, const char* what) {
+    if (!a || !a->data) return set_err(MGP_EINVAL, "%s: null array", what);
+    if (a->ngx < 0 || a->ngy < 0) return set_err(MGP_EINVAL, "%s: negative ghost count", what);
+    if (array_ld(a, nxv) < nxv + 2 * a->ngx) return set_err(MGP_EINVAL, "%s: leading dimension too small", what);
+    return MGP_OK;
+}
+
+// Copy the part of a caller array that the device field holds (valid cells
+// and up to `gmax` ghost layers).  cudaMemcpyDefault lets the driver tell host
+// from device memory.
+int stage_in(const mgp_array* u, int nxv, int nyv, const DF& d, int gmax, cudaStream_t st) {
+    const int gx = u->ngx < gmax ? u->ngx : gmax, gy = u->ngy < gmax ? u->ngy : gmax;
+    const long uld = array_ld(u, nxv);
+    const double* src = u->data + (u->ngx - gx) + (long)(u->ngy - gy) * uld;
+    double* dst = d.p - gx - (long)gy * d.ld;
+    CK(cudaMemcpy2DAsync(dst, (size_t)d.ld * 8, src, (size_t)uld * 8, (size_t)(nxv + 2 * gx) * 8, nyv + 2 * gy,
+                         cudaMemcpyDefault, st));
+    return MGP_OK;
+}
+
+int stage_out(const DF& d, const mgp_array* u, int nxv, int nyv, int gmax, cudaStream_t st) {
+    const int gx = u->ngx < gmax ? u->ngx : gmax, gy = u->ngy < gmax ? u->ngy : gmax;
+    const long uld = array_ld(u, nxv);
+    double* dst = u->data + (u->ngx - gx) + (long)(u->ngy - gy) * uld;
+    const double* src = d.p - gx - (long)gy * d.ld;
+    CK(cudaMemcpy2DAsync(dst, (size_t)uld * 8, src, (size_t)d.ld * 8, (size_t)(nxv + 2 * gx) * 8, nyv + 2 * gy,
+                         cudaMemcpyDefault, st));
+    return MGP_OK;
+}
+
+int read_scalar(const double* p, double* out) {
+    CK(cudaMemcpy(out, p, sizeof(double), cudaMemcpyDefault));
+    return MGP_OK;
+}
+
+// type(bdry_data) -> BCd.  NONUNIFORM values are copied to `dbuf` (device,
+// 2*(nx+ny) doubles).  homog selects which checks apply.
+int make_bc(const mgp_bdry* b, const mgp_box* v, int homog, double* dbuf, BCd* out, cudaStream_t st) {
+    if (!b) return set_err(MGP_EINVAL, "null bdry_data");
+    std::memset(out, 0, sizeof *out);
+    size_t off = 0;
+    for (int s = 0; s < 4; ++s) {
+        const int t = b->type[s], m = b->mode[s];
+        if (t == MGP_BCTYPE_CF) return set_err(MGP_ENOTSUP, "fill_ghosts: BCTYPE_CF is not supported");
+        if (t < MGP_BCTYPE_NONE || t > MGP_BCTYPE_EXTRAP2) return set_err(MGP_EINVAL, "fill_ghosts: invalid BCTYPE_");
+        if (m < MGP_BCMODE_UNIFORM || m > MGP_BCMODE_LAH) return set_err(MGP_EINVAL, "define_bdry_data: Bad BCMODE");
+        out->type[s] = t;
+        out->mode[s] = m;
+        const int n = (s < 2) ? v->ny : v->nx;
+        if (m == MGP_BCMODE_NONUNIFORM) {
+            if (!b->data[s]) return set_err(MGP_EINVAL, "null NONUNIFORM boundary data");
+            CK(cudaMemcpyAsync(dbuf + off, b->data[s], (size_t)n * 8, cudaMemcpyDefault, st));
+            out->d[s] = dbuf + off;
+            off += n;
+        } else {
+            double u = 0.0;
+            if (b->data[s]) RC(read_scalar(b->data[s], &u));
+            out->u[s] = u;
+        }
+    }
+    // The Fortran operator reads the north-face Neumann data at index jhi
+    // (poisson2d.f90:1208, 1248, 1298 `bc%data_yhi(j)`); keep that, and refuse
+    // the cases where that index is outside the array.
+    if (b->type[3] == MGP_BCTYPE_NEUM && !homog && b->mode[3] == MGP_BCMODE_NONUNIFORM) {
+        out->kyhi = v->jhi - v->ilo;
+        if (out->kyhi < 0 || out->kyhi >= v->nx)
+            return set_err(MGP_EINVAL, "north Neumann data is read at index jhi, outside its bounds");
+    }
+    // Y-side NONUNIFORM Dirichlet data is read as bcd(jlo:jhi) (arrayutils.f90:1224).
+    for (int s = 2; s < 4; ++s)
+        if (b->type[s] == MGP_BCTYPE_DIRI && !homog && b->mode[s] == MGP_BCMODE_NONUNIFORM) {
+            out->koffy = v->jlo - v->ilo;
+            if (out->koffy != 0)
+                return set_err(MGP_EINVAL, "y-side nonuniform Dirichlet data needs jlo == ilo");
+        }
+    return MGP_OK;
+}
+
+Geo make_geo(DF J, DF xx, DF xy, DF yx, DF yy, double dx, double dy) {
+    Geo g;
+    g.J = J; g.xx = xx; g.xy = xy; g.yx = yx; g.yy = yy;
+    g.dx = dx; g.dy = dy;
+    g.idx = 1.0 / dx;
+    g.idy = 1.0 / dy;
+    return g;
+}
+
+// ---------------------------------------------------------------------------
+// Schedule (MG:38-129)
+// ---------------------------------------------------------------------------
+void estimate_maxdepth(int* maxdepth, const mgp_box* v) {
+    int mgnx = v->nx, mgny = v->ny, d;
+    for (d = 0; d <= *maxdepth - 1; ++d) {
+        if (mgnx % 2 == 0) mgnx /= 2;
+        else if (mgny % 2 == 0) mgny /= 2;
+        else break;
+    }
+    if (d + 1 < *maxdepth) *maxdepth = d + 1;
+}
+
+void create_mgschedule(std::vector<int>& refx, std::vector<int>& refy, int* maxdepth, const mgp_box* v) {
+    const int min_nx = 4, min_ny = 4;
+    int mgnx = v->nx, mgny = v->ny, d;
+    double mgdx = v->dx, mgdy = v->dy;
+    refx.assign(*maxdepth + 1, 0);
+    refy.assign(*maxdepth + 1, 0);
+    for (d = 0; d <= *maxdepth - 1; ++d) {
+        if ((mgnx % 2 != 0) || (mgny % 2 != 0)) break;
+        const double max_dx = mgdx > mgdy ? mgdx : mgdy;
+        refx[d] = (mgdx <= max_dx / 2) ? 2 : 1;
+        refy[d] = (mgdy <= max_dx / 2) ? 2 : 1;
+        if (refx[d] * refy[d] == 1) refx[d] = refy[d] = 2;
+        mgnx /= refx[d];
+        mgny /= refy[d];
+        if ((mgnx < min_nx) || (mgny < min_ny)) break;
+        mgdx = mgdx * (double)refx[d];
+        mgdy = mgdy * (double)refy[d];
+    }
+    *maxdepth = d;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// The resident hierarchy
+// ---------------------------------------------------------------------------
+struct mgp_solver {
+    int kind = MGP_KIND_MG;
+    int flags = 0;
+    int maxdepth = 0;
+    int dc = 0;   // first level handled by the coarse CTA
+    mgp_box valid{};
+    int types[4] = {0, 0, 0, 0};
+    std::vector<int> refx, refy;
+    std::vector<Lv> lv;
+    Lv* d_lv = nullptr;
+    int* d_ref = nullptr;   // refx then refy
+    int* d_status = nullptr;
+    Arena fixed;            // geometry, inverse diagonals
+    Arena state;            // everything a solve writes; zeroed at the start of each solve
+    DF phi0{}, rhs0{};
+    double* d_bcbuf = nullptr;
+    double* d_red = nullptr;    // reduction partials + outputs
+    double* h_red = nullptr;    // pinned
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // MGP_FLAG_TIME_SMOOTHER: event pairs around the level-0 smoothing calls
+    std::vector<cudaEvent_t> tev;
+    size_t tev_used = 0;
+    long long t_sweeps = 0;
+};
+
+namespace {
+
+constexpr int kRedSlots = 2 * 296 + 8;
+
+void solver_free(mgp_solver* s) {
+    if (!s) return;
+    if (s->d_lv) cudaFree(s->d_lv);
+    if (s->d_ref) cudaFree(s->d_ref);
+    if (s->d_status) cudaFree(s->d_status);
+    if (s->d_bcbuf) cudaFree(s->d_bcbuf);
+    if (s->d_red) cudaFree(s->d_red);
+    if (s->h_red) cudaFreeHost(s->h_red);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    for (cudaEvent_t e : s->tev) cudaEventDestroy(e);
+    s->fixed.release();
+    s->state.release();
+    delete s;
+}
+
+double* red_partials(mgp_solver* s) { return s->d_red; }
+double* red_out(mgp_solver* s) { return s->d_red + 2 * 296; }
+
+// Schedule, allocation, geometry restriction and inverse diagonals:
+// MG:432-562 and DD:622-761.
+int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const mgp_bdry* bc, int maxdepth_user) {
+    cudaStream_t st = s->stream;
+    RC(check_box(valid));
+    if (valid->ilo < 0 || valid->jlo < 0 || (valid->ilo % 2) || (valid->jlo % 2))
+        return set_err(MGP_EINVAL, "solver: ilo and jlo must be even and non-negative");
+    if (!geo || !bc) return set_err(MGP_EINVAL, "null geometry or bdry_data");
+    RC(check_array(&geo->J, valid->nx, "J"));
+    RC(check_array(&geo->Jgup_xx, valid->nx + 1, "Jgup_xx"));
+    RC(check_array(&geo->Jgup_xy, valid->nx + 1, "Jgup_xy"));
+    RC(check_array(&geo->Jgup_yx, valid->nx, "Jgup_yx"));
+    RC(check_array(&geo->Jgup_yy, valid->nx, "Jgup_yy"));
+    for (int k = 0; k < 4; ++k) {
+        if (bc->type[k] == MGP_BCTYPE_CF) return set_err(MGP_ENOTSUP, "BCTYPE_CF is not supported");
+        if (bc->type[k] < MGP_BCTYPE_NONE || bc->type[k] > MGP_BCTYPE_EXTRAP2)
+            return set_err(MGP_EINVAL, "invalid BC type");
+        s->types[k] = bc->type[k];
+    }
+    s->valid = *valid;
+    int md = maxdepth_user < 0 ? 1000 : maxdepth_user;
+    estimate_maxdepth(&md, valid);
+    create_mgschedule(s->refx, s->refy, &md, valid);
+    s->maxdepth = md;
+    s->lv.assign(md + 1, Lv{});
+    // level boxes (coarsen_box, AU:154-170)
+    std::vector<mgp_box> boxes(md + 1);
+    boxes[0] = *valid;
+    for (int d = 1; d <= md; ++d) {
+        mgp_box b = boxes[d - 1];
+        b.ilo /= s->refx[d - 1]; b.ihi /= s->refx[d - 1]; b.nx = b.ihi - b.ilo + 1; b.dx = b.dx * s->refx[d - 1];
+        b.jlo /= s->refy[d - 1]; b.jhi /= s->refy[d - 1]; b.ny = b.jhi - b.jlo + 1; b.dy = b.dy * s->refy[d - 1];
+        boxes[d] = b;
+    }
+    s->dc = md;
+    for (int d = 0; d <= md; ++d)
+        if ((long)boxes[d].nx * boxes[d].ny <= kCoarseCells) { s->dc = d; break; }
+    for (int d = 0; d <= md; ++d) {
+        Lv& L = s->lv[d];
+        const int nx = boxes[d].nx, ny = boxes[d].ny;
+        L.nx = nx;
+        L.ny = ny;
+        s->fixed.add(&L.g.J, nx, ny, 0);
+        s->fixed.add(&L.g.xx, nx + 1, ny, 0);
+        s->fixed.add(&L.g.xy, nx + 1, ny, 0);
+        s->fixed.add(&L.g.yx, nx, ny + 1, 0);
+        s->fixed.add(&L.g.yy, nx, ny + 1, 0);
+        s->fixed.add(&L.invd, nx, ny, 0);
+        s->state.add(&L.e, nx, ny, 1);
+        s->state.add(&L.r, nx, ny, 0);
+        s->state.add(&L.w, nx, ny, 0);
+        if (d == md) {
+            s->state.add(&L.ea, nx, ny, 1);
+            s->state.add(&L.pt, nx, ny, 1);
+            s->state.add(&L.st, nx, ny, 1);
+            s->state.add(&L.rr, nx, ny, 0);
+            s->state.add(&L.rt, nx, ny, 0);
+            s->state.add(&L.pp, nx, ny, 0);
+            s->state.add(&L.tt, nx, ny, 0);
+            s->state.add(&L.vv, nx, ny, 0);
+        }
+        L.g.dx = boxes[d].dx;
+        L.g.dy = boxes[d].dy;
+        L.g.idx = 1.0 / boxes[d].dx;
+        L.g.idy = 1.0 / boxes[d].dy;
+        for (int k = 0; k < 4; ++k) {
+            L.bc.type[k] = bc->type[k];
+            L.bc.mode[k] = (s->kind == MGP_KIND_DD) ? MGP_BCMODE_LAH : MGP_BCMODE_UNIFORM;   // MG:516-522, DD:713-719
+            L.bc.u[k] = 0.0;
+            L.bc.d[k] = nullptr;
+        }
+    }
+    s->state.add(&s->phi0, valid->nx, valid->ny, 1);
+    s->state.add(&s->rhs0, valid->nx, valid->ny, 0);
+    RC(s->fixed.commit(st));
+    RC(s->state.commit(st));
+    if (cudaMalloc(&s->d_bcbuf, sizeof(double) * 2 * (valid->nx + valid->ny + 2)) != cudaSuccess ||
+        cudaMalloc(&s->d_red, sizeof(double) * kRedSlots) != cudaSuccess ||
+        cudaMalloc(&s->d_lv, sizeof(Lv) * (md + 1)) != cudaSuccess ||
+        cudaMalloc(&s->d_ref, sizeof(int) * 2 * (md + 1)) != cudaSuccess ||
+        cudaMalloc(&s->d_status, sizeof(int)) != cudaSuccess ||
+        cudaMallocHost(&s->h_red, sizeof(double) * 8) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(MGP_ENOMEM, "device allocation failed");
+    }
+    CK(cudaEventCreate(&s->ev0));
+    CK(cudaEventCreate(&s->ev1));
+    // level-0 geometry is copied (MG:538-545); coarser levels restrict it (MG:550-554)
+    Lv& L0 = s->lv[0];
+    RC(stage_in(&geo->J, valid->nx, valid->ny, L0.g.J, 0, st));
+    RC(stage_in(&geo->Jgup_xx, valid->nx + 1, valid->ny, L0.g.xx, 0, st));
+    RC(stage_in(&geo->Jgup_xy, valid->nx + 1, valid->ny, L0.g.xy, 0, st));
+    RC(stage_in(&geo->Jgup_yx, valid->nx, valid->ny + 1, L0.g.yx, 0, st));
+    RC(stage_in(&geo->Jgup_yy, valid->nx, valid->ny + 1, L0.g.yy, 0, st));
+    for (int d = 1; d <= md; ++d) {
+        Lv &U = s->lv[d - 1], &L = s->lv[d];
+        const int rx = s->refx[d - 1], ry = s->refy[d - 1];
+        CK(launch_restrict(U.g.J, L.g.J, L.nx, L.ny, rx, ry, 0, st));
+        CK(launch_restrict(U.g.xx, L.g.xx, L.nx, L.ny, rx, ry, 1, st));
+        CK(launch_restrict(U.g.xy, L.g.xy, L.nx, L.ny, rx, ry, 1, st));
+        CK(launch_restrict(U.g.yx, L.g.yx, L.nx, L.ny, rx, ry, 2, st));
+        CK(launch_restrict(U.g.yy, L.g.yy, L.nx, L.ny, rx, ry, 2, st));
+    }
+    for (int d = 0; d <= md; ++d) {
+        Lv& L = s->lv[d];
+        if (s->kind == MGP_KIND_DD) CK(launch_dd_invdiag(L.invd, L.g, L.nx, L.ny, st));   // DD:16-39
+        else CK(launch_invdiag(L.invd, L.g, L.bc, 1, L.nx, L.ny, (s->flags & MGP_FLAG_DIRICHLET_COUPLED_DIAG) ? 1 : 0,
+                               st));                                                      // P2:16-388
+    }
+    std::vector<int> ref(2 * (md + 1), 0);
+    for (int d = 0; d < md; ++d) { ref[d] = s->refx[d]; ref[md + 1 + d] = s->refy[d]; }
+    CK(cudaMemcpyAsync(s->d_lv, s->lv.data(), sizeof(Lv) * (md + 1), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->d_ref, ref.data(), sizeof(int) * 2 * (md + 1), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    return MGP_OK;
+}
+
+// ---- pieces of vcycle_noinit on the grid-wide kernels -------------------- //
+int smooth_body(mgp_solver* s, int d, int nu);
+
+// Level-0 smoothing, bracketed by an event pair when MGP_FLAG_TIME_SMOOTHER is set.
+int smooth(mgp_solver* s, int d, int nu) {
+    const bool timed = (d == 0) && (s->flags & MGP_FLAG_TIME_SMOOTHER) && nu > 0;
+    if (!timed) return smooth_body(s, d, nu);
+    if (s->tev_used + 2 > s->tev.size()) {
+        for (int k = 0; k < 2; ++k) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            s->tev.push_back(e);
+        }
+    }
+    CK(cudaEventRecord(s->tev[s->tev_used], s->stream));
+    RC(smooth_body(s, d, nu));
+    CK(cudaEventRecord(s->tev[s->tev_used + 1], s->stream));
+    s->tev_used += 2;
+    s->t_sweeps += nu;
+    return MGP_OK;
+}
+
+int smooth_body(mgp_solver* s, int d, int nu) {
+    Lv& L = s->lv[d];
+    cudaStream_t st = s->stream;
+    if (nu <= 0) return MGP_OK;
+    if (s->kind == MGP_KIND_DD) {
+        CK(launch_dd_modrhs(L.w, L.e, L.r, L.g, L.nx, L.ny, st));   // DD:226-250
+        for (int k = 0; k < nu; ++k) {
+            CK(launch_fill(L.e, L.g, L.bc, 1, 1, L.nx, L.ny, st));   // DD:259
+            CK(launch_dd_colour(L.e, L.w, L.invd, L.g, L.nx, L.ny, 4.0 / 5.0, 0, st));
+            CK(launch_dd_colour(L.e, L.w, L.invd, L.g, L.nx, L.ny, 4.0 / 5.0, 1, st));
+        }
+    } else {
+        for (int k = 0; k < nu; ++k) CK(launch_gs_sweep(L.e, L.r, L.invd, L.g, L.bc, 1, L.nx, L.ny, 1.0, st));
+    }
+    return MGP_OK;
+}
+
+int residual_level(mgp_solver* s, int d) {
+    Lv& L = s->lv[d];
+    cudaStream_t st = s->stream;
+    if (s->kind == MGP_KIND_DD) {
+        CK(launch_dd_apply(L.w, L.e, L.r, L.g, L.bc, L.nx, L.ny, 1, st));
+        CK(launch_fill(L.e, L.g, L.bc, 1, 1, L.nx, L.ny, st));
+    } else {
+        CK(launch_fill(L.e, L.g, L.bc, 1, 0, L.nx, L.ny, st));
+        CK(launch_apply(L.w, L.e, L.r, L.g, L.bc, 1, L.nx, L.ny, 1, 0, st));
+    }
+    return MGP_OK;
+}
+
+// prolong(e(d), e(d+1), ..., order), MG:262-394.
+int prolong_level(mgp_solver* s, int d, int order) {
+    Lv &F = s->lv[d], &Cl = s->lv[d + 1];
+    cudaStream_t st = s->stream;
+    const int rx = s->refx[d], ry = s->refy[d];
+    CK(launch_fill(Cl.e, Cl.g, Cl.bc, 1, 1, Cl.nx, Cl.ny, st));   // MG:318
+    CK(launch_prolong(F.e, Cl.e, Cl.nx, Cl.ny, rx, ry, order, st));
+    if (order >= 2 && rx == 2 && ry == 2) {
+        CK(launch_extrapolate(Cl.e, Cl.nx, Cl.ny, 1, 1, 3, st));   // MG:354
+        CK(launch_prolong_cross(F.e, Cl.e, Cl.nx, Cl.ny, st));
+    }
+    const bool rax = (Cl.bc.type[0] == T_PERIODIC && Cl.bc.type[1] == T_PERIODIC) ||
+                     (Cl.bc.type[0] == T_NEUM && Cl.bc.type[1] == T_NEUM);
+    const bool ray = (Cl.bc.type[2] == T_PERIODIC && Cl.bc.type[3] == T_PERIODIC) ||
+                     (Cl.bc.type[2] == T_NEUM && Cl.bc.type[3] == T_NEUM);
+    if (rax && ray) {
+        CK(launch_reduce(RED_JSUM, F.e, F.g.J, F.nx, F.ny, F.g.dx * F.g.dy, red_partials(s), red_out(s), st));
+        CK(launch_sub_mean(F.e, red_out(s), F.nx, F.ny, 1, 1, st));
+    }
+    return MGP_OK;
+}
+
+int coarse_cycle(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
+    CoarseArgs a;
+    a.lv = s->d_lv;
+    a.d0 = d;
+    a.maxdepth = s->maxdepth;
+    a.numcycles = numcycles;
+    a.nd = nd; a.nu = nu; a.nb = nb;
+    a.dd = (s->kind == MGP_KIND_DD);
+    a.refx = s->d_ref;
+    a.refy = s->d_ref + s->maxdepth + 1;
+    a.status = s->d_status;
+    CK(launch_coarse_cycle(a, s->stream));
+    return MGP_OK;
+}
+
+// vcycle_noinit(depth), MG:675-854 / DD:867-1045.
+int vcycle_noinit(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
+    if (d >= s->dc) return coarse_cycle(s, d, numcycles, nd, nu, nb);
+    Lv &L = s->lv[d], &Cl = s->lv[d + 1];
+    cudaStream_t st = s->stream;
+    const bool dd = (s->kind == MGP_KIND_DD);
+    if (dd) CK(launch_set_guess(L.e, L.r, L.invd, L.nx, L.ny, st));   // DD:971
+    RC(smooth(s, d, nd));
+    RC(residual_level(s, d));
+    CK(launch_restrict(L.w, Cl.r, Cl.nx, Cl.ny, s->refx[d], s->refy[d], 0, st));
+    if (!dd) CK(launch_set_guess(Cl.e, Cl.r, Cl.invd, Cl.nx, Cl.ny, st));   // MG:805-806
+    for (int c = 1; c <= numcycles; ++c) RC(vcycle_noinit(s, d + 1, numcycles, nd, nu, nb));
+    RC(prolong_level(s, d, 1));
+    RC(smooth(s, d, nu));
+    return MGP_OK;
+}
+
+// fmg_noinit(depth), MG:1127-1189.
+int fmg_noinit(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
+    Lv& L = s->lv[d];
+    cudaStream_t st = s->stream;
+    CK(launch_fillval(L.e, 0.0, L.nx, L.ny, 1, 1, st));
+    if (d < s->maxdepth) {
+        Lv& Cl = s->lv[d + 1];
+        CK(launch_restrict(L.r, Cl.r, Cl.nx, Cl.ny, s->refx[d], s->refy[d], 0, st));
+        RC(fmg_noinit(s, d + 1, numcycles, nd, nu, nb));
+        RC(prolong_level(s, d, 2));
+    }
+    for (int c = 1; c <= numcycles; ++c) RC(vcycle_noinit(s, d, numcycles, nd, nu, nb));
+    return MGP_OK;
+}
+
+// 0 = vcycle (MG:400-670), 1 = fmg (MG:860-1122), 2 = DD vcycle (DD:589-862)
+int solver_solve(mgp_solver* s, int which, mgp_array* phi, mgp_array* rhs, const mgp_bdry* bc, int homog, double tol,
+                 int maxiters, int numcycles, int nd, int nu, int nb, int zerophi, int verbosity, mgp_report* rep) {
+    const int nx = s->valid.nx, ny = s->valid.ny;
+    cudaStream_t st = s->stream;
+    if (which == 2 && s->kind != MGP_KIND_DD) return set_err(MGP_EINVAL, "solver was not created for the DD path");
+    if (which != 2 && s->kind == MGP_KIND_DD) return set_err(MGP_EINVAL, "solver was created for the DD path");
+    if (maxiters < 0 || numcycles < 0 || nd < 0 || nu < 0 || nb < 0) return set_err(MGP_EINVAL, "negative count");
+    RC(check_array(phi, nx, "phi"));
+    RC(check_array(rhs, nx, "rhs"));
+    if (!bc) return set_err(MGP_EINVAL, "null bdry_data");
+    for (int k = 0; k < 4; ++k)
+        if (bc->type[k] != s->types[k]) return set_err(MGP_EINVAL, "BC types differ from the ones the solver was built with");
+    BCd ubc;
+    RC(make_bc(bc, &s->valid, homog, s->d_bcbuf, &ubc, st));
+    Lv& L0 = s->lv[0];
+    const double vol = s->valid.dx * s->valid.dy;
+    std::vector<double> relres((size_t)maxiters + 1, 0.0);
+    int iters = 0, diverged = 0, status = MGP_OK;
+    double rscale = 0.0;
+
+    s->tev_used = 0;
+    s->t_sweeps = 0;
+    CK(cudaEventRecord(s->ev0, st));
+    // every solve starts from fresh (zeroed) work arrays, like the Fortran drivers' allocations
+    CK(cudaMemsetAsync(s->state.base, 0, s->state.elems * sizeof(double), st));
+    CK(cudaMemsetAsync(s->d_status, 0, sizeof(int), st));
+    RC(stage_in(phi, nx, ny, s->phi0, 1, st));
+    RC(stage_in(rhs, nx, ny, s->rhs0, 0, st));
+    if (zerophi) CK(launch_fillval(s->phi0, 0.0, nx, ny, 1, 1, st));
+    if (which == 2) CK(launch_muldiv(s->rhs0, L0.g.J, 1, nx, ny, st));   // DD:772-773
+    // r(0) = rhs - L[phi] with the caller's BCs (MG:579)
+    CK(launch_fill(s->phi0, L0.g, ubc, homog, 0, nx, ny, st));
+    CK(launch_apply(L0.r, s->phi0, s->rhs0, L0.g, ubc, homog, nx, ny, 1, 0, st));
+    CK(launch_reduce(RED_SUMSQ, L0.r, L0.r, nx, ny, vol, red_partials(s), red_out(s), st));
+    CK(cudaMemcpyAsync(s->h_red, red_out(s), sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    rscale = s->h_red[0];
+    if (rscale == 0.0) { relres[0] = rscale; rscale = 1.0; }
+    else relres[0] = 1.0;
+    if (verbosity >= 1) printf("max MG depth = %d\nV-Cycle iter 0: rel |res| = %.16e\n", s->maxdepth, relres[0]);
+    if (!std::isfinite(rscale)) status = MGP_EDIVERGED;
+    for (int iter = 1; iter <= maxiters && status == MGP_OK; ++iter) {
+        if (which == 0) CK(launch_set_guess(L0.e, L0.r, L0.invd, nx, ny, st));   // MG:600
+        if (which == 1) RC(fmg_noinit(s, 0, numcycles, nd, nu, nb));
+        else RC(vcycle_noinit(s, 0, numcycles, nd, nu, nb));
+        CK(launch_axpby(s->phi0, L0.e, 1.0, 1.0, nx, ny, 1, 1, st));   // MG:611 (whole array)
+        CK(launch_fill(s->phi0, L0.g, ubc, homog, 0, nx, ny, st));
+        CK(launch_apply(L0.r, s->phi0, s->rhs0, L0.g, ubc, homog, nx, ny, 1, 0, st));
+        CK(launch_reduce(RED_SUMSQ, L0.r, L0.r, nx, ny, vol, red_partials(s), red_out(s), st));
+        CK(cudaMemcpyAsync(s->h_red, red_out(s), sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        relres[iter] = s->h_red[0] / rscale;
+        iters = iter;
+        if (verbosity >= 1) printf("V-Cycle iter %d: rel |res| = %.16e\n", iter, relres[iter]);
+        if (!std::isfinite(relres[iter])) { status = MGP_EDIVERGED; break; }
+        if (relres[iter] <= tol) break;
+        if (relres[iter] > relres[iter - 1]) {   // MG:630-639
+            CK(launch_axpby(s->phi0, L0.e, 1.0, -1.0, nx, ny, 1, 1, st));
+            diverged = 1;
+            break;
+        }
+    }
+    int dstat = 0;
+    CK(cudaMemcpyAsync(&dstat, s->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    RC(stage_out(s->phi0, phi, nx, ny, 1, st));
+    if (which == 2) {   // DD:837-838
+        CK(launch_muldiv(s->rhs0, L0.g.J, 0, nx, ny, st));
+        RC(stage_out(s->rhs0, rhs, nx, ny, 0, st));
+    }
+    CK(cudaEventRecord(s->ev1, st));
+    CK(cudaStreamSynchronize(st));
+    if (status == MGP_OK && dstat) status = MGP_EDIVERGED;
+    if (rep) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+        rep->status = status;
+        rep->iterations = iters;
+        rep->maxdepth = s->maxdepth;
+        rep->diverged = diverged;
+        rep->rscale = rscale;
+        rep->final_relres = relres[iters];
+        rep->seconds = ms * 1e-3;
+        double sm = 0.0;
+        for (size_t k = 0; k + 1 < s->tev_used; k += 2) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, s->tev[k], s->tev[k + 1]);
+            sm += t * 1e-3;
+        }
+        rep->smooth0_seconds = sm;
+        rep->smooth0_sweeps = s->t_sweeps;
+        if (rep->relres)
+            for (int k = 0; k <= iters; ++k) rep->relres[k] = relres[k];
+    }
+    if (status) return set_err(status, "non-finite residual");
+    return MGP_OK;
+}
+
+int solver_new(const mgp_box* valid, const mgp_geo* geo, const mgp_bdry* bc, int kind, int flags, int maxdepth_user,
+               cudaStream_t stream, mgp_solver** out) {
+    if (!out) return set_err(MGP_EINVAL, "null output pointer");
+    *out = nullptr;
+    if (kind != MGP_KIND_MG && kind != MGP_KIND_DD) return set_err(MGP_EINVAL, "unknown solver kind");
+    mgp_solver* s = new mgp_solver();
+    s->kind = kind;
+    s->flags = flags;
+    s->stream = stream;
+    const int rc = solver_build(s, valid, geo, bc, maxdepth_user);
+    if (rc) {
+        solver_free(s);
+        return rc;
+    }
+    *out = s;
+    return MGP_OK;
+}
+
+int oneshot(int which, const mgp_box* valid, mgp_array* phi, mgp_array* rhs, const mgp_geo* geo, const mgp_bdry* bc,
+            int homog, double tol, int maxiters, int maxdepth_user, int numcycles, int nd, int nu, int nb, int zerophi,
+            int verbosity, mgp_report* rep) {
+    mgp_solver* s = nullptr;
+    RC(solver_new(valid, geo, bc, which == 2 ? MGP_KIND_DD : MGP_KIND_MG, g_flags, maxdepth_user, nullptr, &s));
+    const int rc = solver_solve(s, which, phi, rhs, bc, homog, tol, maxiters, numcycles, nd, nu, nb, zerophi, verbosity,
+                                rep);
+    solver_free(s);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Operator-level calls: a short-lived context that stages the arguments.
+// ---------------------------------------------------------------------------
+struct OpCtx {
+    std::vector<void*> bufs;
+    cudaStream_t st = nullptr;
+    ~OpCtx() {
+        for (void* p : bufs) cudaFree(p);
+    }
+    int field(DF* f, int nxv, int nyv, int g) {
+        const int ld = ((nxv + 2 * g + 31) / 32) * 32;
+        const size_t pad = g ? 32 : 0;
+        const size_t n = (size_t)(nyv + 2 * g) * ld + 2 * pad;
+        double* p = nullptr;
+        if (cudaMalloc(&p, n * 8) != cudaSuccess) {
+            cudaGetLastError();
+            return set_err(MGP_ENOMEM, "cudaMalloc failed");
+        }
+        bufs.push_back(p);
+        CK(cudaMemsetAsync(p, 0, n * 8, st));
+        f->ld = ld;
+        f->p = p + pad + (size_t)g * ld;
+        return MGP_OK;
+    }
+    int dbuf(double** p, size_t n) {
+        if (cudaMalloc(p, n * 8) != cudaSuccess) {
+            cudaGetLastError();
+            return set_err(MGP_ENOMEM, "cudaMalloc failed");
+        }
+        bufs.push_back(*p);
+        return MGP_OK;
+    }
+    int ibuf(int** p) {
+        if (cudaMalloc(p, sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            return set_err(MGP_ENOMEM, "cudaMalloc failed");
+        }
+        bufs.push_back(*p);
+        CK(cudaMemsetAsync(*p, 0, sizeof(int), st));
+        return MGP_OK;
+    }
+    // Geometry of a level: the five arrays.
+    int geo(const mgp_geo* g, const mgp_box* v, Geo* out) {
+        if (!g) return set_err(MGP_EINVAL, "null geometry");
+        DF J, xx, xy, yx, yy;
+        RC(check_array(&g->J, v->nx, "J"));
+        RC(check_array(&g->Jgup_xx, v->nx + 1, "Jgup_xx"));
+        RC(check_array(&g->Jgup_xy, v->nx + 1, "Jgup_xy"));
+        RC(check_array(&g->Jgup_yx, v->nx, "Jgup_yx"));
+        RC(check_array(&g->Jgup_yy, v->nx, "Jgup_yy"));
+        RC(field(&J, v->nx, v->ny, 0));
+        RC(field(&xx, v->nx + 1, v->ny, 0));
+        RC(field(&xy, v->nx + 1, v->ny, 0));
+        RC(field(&yx, v->nx, v->ny + 1, 0));
+        RC(field(&yy, v->nx, v->ny + 1, 0));
+        RC(stage_in(&g->J, v->nx, v->ny, J, 0, st));
+        RC(stage_in(&g->Jgup_xx, v->nx + 1, v->ny, xx, 0, st));
+        RC(stage_in(&g->Jgup_xy, v->nx + 1, v->ny, xy, 0, st));
+        RC(stage_in(&g->Jgup_yx, v->nx, v->ny + 1, yx, 0, st));
+        RC(stage_in(&g->Jgup_yy, v->nx, v->ny + 1, yy, 0, st));
+        *out = make_geo(J, xx, xy, yx, yy, g->dx, g->dy);
+        return MGP_OK;
+    }
+    int in(const mgp_array* a, int nxv, int nyv, int g, DF* f, const char* what) {
+        RC(check_array(a, nxv, what));
+        RC(field(f, nxv, nyv, g));
+        return stage_in(a, nxv, nyv, *f, g, st);
+    }
+    int bc(const mgp_bdry* b, const mgp_box* v, int homog, BCd* out) {
+        double* d = nullptr;
+        RC(dbuf(&d, 2 * (size_t)(v->nx + v->ny + 2)));
+        return make_bc(b, v, homog, d, out, st);
+    }
+    int finish() {
+        CK(cudaStreamSynchronize(st));
+        CK(cudaGetLastError());
+        return MGP_OK;
+    }
+};
+
+int no_lah(const mgp_bdry* bc) {
+    for (int k = 0; k < 4; ++k)
+        if (bc && bc->mode[k] == MGP_BCMODE_LAH) return set_err(MGP_EINVAL, "Poisson2d::compute_invdiags received BCMODE_LAH.");
+    return MGP_OK;
+}
+
+int ghost_cap(const mgp_array* a) {
+    if (a->ngx > 1 || a->ngy > 1) return set_err(MGP_EINVAL, "fill_ghosts: Can only handle 1 ghost layer max.");
+    return MGP_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* mgp_version(void) { return "mgp2d-b200 0.1 (sm_100a, FP64)"; }
+const char* mgp_last_error(void) { return g_err.c_str(); }
+long long mgp_kernel_launch_count(void) { return launch_count(); }
+
+int mgp_set_flags(int flags) {
+    const int old = g_flags;
+    g_flags = flags;
+    return old;
+}
+
+int mgp_estimate_maxdepth(int* maxdepth, const mgp_box* valid) {
+    if (!maxdepth || !valid) return set_err(MGP_EINVAL, "null argument");
+    estimate_maxdepth(maxdepth, valid);
+    return MGP_OK;
+}
+
+int mgp_create_mgschedule(int* refx, int* refy, int* maxdepth, const mgp_box* valid) {
+    if (!refx || !refy || !maxdepth || !valid) return set_err(MGP_EINVAL, "null argument");
+    std::vector<int> rx, ry;
+    const int in = *maxdepth;
+    create_mgschedule(rx, ry, maxdepth, valid);
+    for (int d = 0; d < in; ++d) {
+        refx[d] = rx[d];
+        refy[d] = ry[d];
+    }
+    return MGP_OK;
+}
+
+int mgp_fill_ghosts(const mgp_box* valid, mgp_array* phi, const mgp_bdry* bc, const mgp_geo* geo, int homog,
+                    int do_neum) {
+    RC(check_box(valid));
+    RC(check_array(phi, valid->nx, "phi"));
+    RC(ghost_cap(phi));
+    OpCtx c;
+    DF p;
+    Geo g;
+    BCd b;
+    RC(c.in(phi, valid->nx, valid->ny, 1, &p, "phi"));
+    RC(c.geo(geo, valid, &g));
+    RC(c.bc(bc, valid, homog, &b));
+    CK(launch_fill(p, g, b, homog, do_neum, valid->nx, valid->ny, c.st));
+    RC(stage_out(p, phi, valid->nx, valid->ny, 1, c.st));
+    return c.finish();
+}
+
+int mgp_extrapolate_ghosts(const mgp_box* valid, mgp_array* phi, int order) {
+    RC(check_box(valid));
+    RC(check_array(phi, valid->nx, "phi"));
+    RC(ghost_cap(phi));
+    if (order < 0 || order > 3) return set_err(MGP_EINVAL, "extrapolate_ghosts: order is not supported");
+    OpCtx c;
+    DF p;
+    RC(c.in(phi, valid->nx, valid->ny, 1, &p, "phi"));
+    CK(launch_extrapolate(p, valid->nx, valid->ny, phi->ngx, phi->ngy, order, c.st));
+    RC(stage_out(p, phi, valid->nx, valid->ny, 1, c.st));
+    return c.finish();
+}
+
+int mgp_compute_invdiags(const mgp_box* valid, mgp_array* invdiags, const mgp_geo* geo, const mgp_bdry* bc,
+                         int homog) {
+    RC(check_box(valid));
+    RC(no_lah(bc));
+    RC(check_array(invdiags, valid->nx, "invdiags"));
+    OpCtx c;
+    DF d;
+    Geo g;
+    BCd b;
+    RC(c.field(&d, valid->nx, valid->ny, 0));
+    RC(c.geo(geo, valid, &g));
+    RC(c.bc(bc, valid, homog, &b));
+    CK(launch_invdiag(d, g, b, homog, valid->nx, valid->ny, (g_flags & MGP_FLAG_DIRICHLET_COUPLED_DIAG) ? 1 : 0, c.st));
+    RC(stage_out(d, invdiags, valid->nx, valid->ny, 0, c.st));
+    return c.finish();
+}
+
+int mgp_compute_laplacian(const mgp_box* valid, mgp_array* lap, mgp_array* phi, const mgp_geo* geo,
+                          const mgp_bdry* bc, int homog, int jscale) {
+    RC(check_box(valid));
+    RC(no_lah(bc));
+    RC(check_array(lap, valid->nx, "lap"));
+    RC(check_array(phi, valid->nx, "phi"));
+    RC(ghost_cap(phi));
+    OpCtx c;
+    DF l, p;
+    Geo g;
+    BCd b;
+    RC(c.field(&l, valid->nx, valid->ny, 0));
+    RC(c.in(phi, valid->nx, valid->ny, 1, &p, "phi"));
+    RC(c.geo(geo, valid, &g));
+    RC(c.bc(bc, valid, homog, &b));
+    CK(launch_fill(p, g, b, homog, 0, valid->nx, valid->ny, c.st));
+    CK(launch_apply(l, p, l, g, b, homog, valid->nx, valid->ny, 0, jscale, c.st));
+    RC(stage_out(l, lap, valid->nx, valid->ny, 0, c.st));
+    RC(stage_out(p, phi, valid->nx, valid->ny, 1, c.st));
+    return c.finish();
+}
+
+int mgp_compute_residual(const mgp_box* valid, mgp_array* res, const mgp_array* rhs, mgp_array* phi,
+                         const mgp_geo* geo, const mgp_bdry* bc, int homog, int jscale) {
+    RC(check_box(valid));
+    RC(no_lah(bc));
+    RC(check_array(res, valid->nx, "res"));
+    RC(check_array(phi, valid->nx, "phi"));
+    RC(ghost_cap(phi));
+    OpCtx c;
+    DF r, f, p;
+    Geo g;
+    BCd b;
+    RC(c.field(&r, valid->nx, valid->ny, 0));
+    RC(c.in(rhs, valid->nx, valid->ny, 0, &f, "rhs"));
+    RC(c.in(phi, valid->nx, valid->ny, 1, &p, "phi"));
+    RC(c.geo(geo, valid, &g));
+    RC(c.bc(bc, valid, homog, &b));
+    CK(launch_fill(p, g, b, homog, 0, valid->nx, valid->ny, c.st));
+    CK(launch_apply(r, p, f, g, b, homog, valid->nx, valid->ny, 1, jscale, c.st));
+    RC(stage_out(r, res, valid->nx, valid->ny, 0, c.st));
+    RC(stage_out(p, phi, valid->nx, valid->ny, 1, c.st));
+    return c.finish();
+}
+
+int mgp_relax_gs(const mgp_box* valid, mgp_array* phi, const mgp_array* rhs, const mgp_geo* geo, const mgp_bdry* bc,
+                 int homog, const mgp_array* invdiags, double omega, double tol, int maxiters, int zerophi,
+                 int verbosity) {
+    RC(check_box(valid));
+    RC(no_lah(bc));
+    RC(check_array(phi, valid->nx, "phi"));
+    RC(ghost_cap(phi));
+    if (maxiters == 0) return MGP_OK;
+    const int nx = valid->nx, ny = valid->ny;
+    OpCtx c;
+    DF p, f, d, r;
+    Geo g;
+    BCd b;
+    double* red = nullptr;
+    RC(c.in(phi, nx, ny, 1, &p, "phi"));
+    RC(c.in(rhs, nx, ny, 0, &f, "rhs"));
+    RC(c.in(invdiags, nx, ny, 0, &d, "invdiags"));
+    RC(c.field(&r, nx, ny, 0));
+    RC(c.dbuf(&red, kRedSlots));
+    RC(c.geo(geo, valid, &g));
+    RC(c.bc(bc, valid, homog, &b));
+    if (zerophi) CK(launch_fillval(p, 0.0, nx, ny, 1, 1, c.st));
+    const double vol = valid->dx * valid->dy;
+    double rscale = 1.0, h = 0.0;
+    auto resnorm = [&](double* out) -> int {
+        CK(launch_fill(p, g, b, homog, 0, nx, ny, c.st));
+        CK(launch_apply(r, p, f, g, b, homog, nx, ny, 1, 0, c.st));
+        CK(launch_reduce(RED_SUMSQ, r, r, nx, ny, vol, red, red + 2 * 296, c.st));
+        CK(cudaMemcpyAsync(out, red + 2 * 296, 8, cudaMemcpyDeviceToHost, c.st));
+        CK(cudaStreamSynchronize(c.st));
+        return MGP_OK;
+    };
+    if (tol > 0.0) {
+        RC(resnorm(&rscale));
+        if (rscale == 0.0) rscale = 1.0;
+    }
+    for (int it = 1; it <= maxiters; ++it) {
+        CK(launch_gs_sweep(p, f, d, g, b, homog, nx, ny, omega, c.st));
+        if (tol > 0.0) {
+            RC(resnorm(&h));
+            if (verbosity >= 3) printf("iter %d: rel |res| = %.16e\n", it, h / rscale);
+            if (h / rscale <= tol) break;
+        }
+    }
+    RC(stage_out(p, phi, nx, ny, 1, c.st));
+    return c.finish();
+}
+
+int mgp_solve_bicgstab2(const mgp_box* valid, mgp_array* phi, const mgp_array* rhs, const mgp_geo* geo,
+                        const mgp_bdry* bc, int homog, const mgp_array* invdiags, double tol, int max_iters,
+                        int max_restarts, int zerophi, int verbosity) {
+    (void)verbosity;
+    RC(check_box(valid));
+    RC(no_lah(bc));
+    RC(check_array(phi, valid->nx, "phi"));
+    RC(ghost_cap(phi));
+    const int nx = valid->nx, ny = valid->ny;
+    OpCtx c;
+    BicgArgs a;
+    std::memset(&a, 0, sizeof a);
+    Lv& L = a.L;
+    L.nx = nx;
+    L.ny = ny;
+    RC(c.in(phi, nx, ny, 1, &a.phi, "phi"));
+    RC(c.in(rhs, nx, ny, 0, &a.rhs, "rhs"));
+    RC(c.in(invdiags, nx, ny, 0, &L.invd, "invdiags"));
+    RC(c.geo(geo, valid, &L.g));
+    RC(c.bc(bc, valid, homog, &L.bc));
+    RC(c.field(&L.w, nx, ny, 0));
+    RC(c.field(&L.ea, nx, ny, 1));
+    RC(c.field(&L.pt, nx, ny, 1));
+    RC(c.field(&L.st, nx, ny, 1));
+    RC(c.field(&L.rr, nx, ny, 0));
+    RC(c.field(&L.rt, nx, ny, 0));
+    RC(c.field(&L.pp, nx, ny, 0));
+    RC(c.field(&L.tt, nx, ny, 0));
+    RC(c.field(&L.vv, nx, ny, 0));
+    RC(c.ibuf(&a.status));
+    a.homog = homog;
+    a.tol = tol;
+    a.max_iters = max_iters;
+    a.max_restarts = max_restarts;
+    a.zerophi = zerophi;
+    a.dd = 0;
+    CK(launch_bicgstab(a, c.st));
+    RC(stage_out(a.phi, phi, nx, ny, 1, c.st));
+    return c.finish();
+}
+
+int mgp_restrict(const mgp_box* fine_valid, const mgp_array* fine, const mgp_box* crse_valid, mgp_array* crse,
+                 int offi, int offj) {
+    RC(check_box(fine_valid));
+    if (!crse_valid) return set_err(MGP_EINVAL, "null box");
+    if (crse_valid->nx < 1 || crse_valid->ny < 1) return set_err(MGP_EINVAL, "empty coarse box");
+    const int rx = fine_valid->nx / crse_valid->nx, ry = fine_valid->ny / crse_valid->ny;
+    if (rx < 1 || ry < 1 || rx * crse_valid->nx != fine_valid->nx || ry * crse_valid->ny != fine_valid->ny)
+        return set_err(MGP_EINVAL, "restrict: boxes are not refinements of each other");
+    const int kind = (offi == 1 && offj == 1) ? 0 : (offi == 0 && offj == 1) ? 1 : (offi == 1 && offj == 0) ? 2 : 3;
+    const int fx = fine_valid->nx + (offi == 0), fy = fine_valid->ny + (offj == 0);
+    const int cx = crse_valid->nx + (offi == 0), cy = crse_valid->ny + (offj == 0);
+    OpCtx c;
+    DF f, cr;
+    RC(c.in(fine, fx, fy, 0, &f, "fine"));
+    RC(check_array(crse, cx, "crse"));
+    const int cg = (crse->ngx > 0 || crse->ngy > 0) ? 1 : 0;
+    RC(c.field(&cr, cx, cy, cg));   // crse%data = zero (ghosts included)
+    CK(launch_restrict(f, cr, crse_valid->nx, crse_valid->ny, rx, ry, kind, c.st));
+    RC(stage_out(cr, crse, cx, cy, cg, c.st));
+    return c.finish();
+}
+
+int mgp_prolong(const mgp_box* fine_valid, mgp_array* fine, const mgp_box* crse_valid, mgp_array* crse,
+                const mgp_geo* fine_geo, const mgp_geo* crse_geo, const mgp_bdry* crse_bc, int order) {
+    RC(check_box(fine_valid));
+    RC(check_box(crse_valid));
+    if (!fine_geo || !crse_geo) return set_err(MGP_EINVAL, "null geometry");
+    if (fine_geo->dx * fine_geo->dy > crse_geo->dx * crse_geo->dy)
+        return set_err(MGP_EINVAL, "prolong: crse and fine geos passed in wrong order");
+    const int rx = fine_valid->nx / crse_valid->nx, ry = fine_valid->ny / crse_valid->ny;
+    if (!((rx == 1 || rx == 2) && (ry == 1 || ry == 2) && rx * ry > 1) || rx * crse_valid->nx != fine_valid->nx ||
+        ry * crse_valid->ny != fine_valid->ny)
+        return set_err(MGP_ENOTSUP, "prolong: Needs updatin'");
+    RC(ghost_cap(crse));
+    OpCtx c;
+    DF f, cr;
+    Geo fg, cg;
+    BCd b;
+    RC(c.in(fine, fine_valid->nx, fine_valid->ny, 1, &f, "fine"));
+    RC(c.in(crse, crse_valid->nx, crse_valid->ny, 1, &cr, "crse"));
+    RC(c.geo(fine_geo, fine_valid, &fg));
+    RC(c.geo(crse_geo, crse_valid, &cg));
+    RC(c.bc(crse_bc, crse_valid, 1, &b));
+    double* red = nullptr;
+    RC(c.dbuf(&red, kRedSlots));
+    if (order >= 1) CK(launch_fill(cr, cg, b, 1, 1, crse_valid->nx, crse_valid->ny, c.st));
+    CK(launch_prolong(f, cr, crse_valid->nx, crse_valid->ny, rx, ry, order, c.st));
+    if (order >= 2 && rx == 2 && ry == 2) {
+        CK(launch_extrapolate(cr, crse_valid->nx, crse_valid->ny, crse->ngx, crse->ngy, 3, c.st));
+        CK(launch_prolong_cross(f, cr, crse_valid->nx, crse_valid->ny, c.st));
+    }
+    const bool rax = (b.type[0] == T_PERIODIC && b.type[1] == T_PERIODIC) || (b.type[0] == T_NEUM && b.type[1] == T_NEUM);
+    const bool ray = (b.type[2] == T_PERIODIC && b.type[3] == T_PERIODIC) || (b.type[2] == T_NEUM && b.type[3] == T_NEUM);
+    if (rax && ray) {
+        const int gx = fine->ngx > 0 ? 1 : 0, gy = fine->ngy > 0 ? 1 : 0;
+        CK(launch_reduce(RED_JSUM, f, fg.J, fine_valid->nx, fine_valid->ny, fine_geo->dx * fine_geo->dy, red,
+                         red + 2 * 296, c.st));
+        CK(launch_sub_mean(f, red + 2 * 296, fine_valid->nx, fine_valid->ny, gx, gy, c.st));
+    }
+    RC(stage_out(f, fine, fine_valid->nx, fine_valid->ny, 1, c.st));
+    RC(stage_out(cr, crse, crse_valid->nx, crse_valid->ny, 1, c.st));
+    return c.finish();
+}
+
+int mgp_pnorm(const mgp_box* valid, const mgp_array* bd, int p, double* out) {
+    RC(check_box(valid));
+    if (!out) return set_err(MGP_EINVAL, "null output");
+    if (p != 0 && p != 1 && p != 2) return set_err(MGP_ENOTSUP, "pnorm: p must be 0, 1 or 2");
+    OpCtx c;
+    DF a;
+    double* red = nullptr;
+    RC(c.in(bd, valid->nx, valid->ny, 0, &a, "bd"));
+    RC(c.dbuf(&red, kRedSlots));
+    const int kind = p == 0 ? RED_MAXABS : p == 1 ? RED_ABSSUM : RED_SUMSQ;
+    CK(launch_reduce(kind, a, a, valid->nx, valid->ny, valid->dx * valid->dy, red, red + 2 * 296, c.st));
+    CK(cudaMemcpyAsync(out, red + 2 * 296, 8, cudaMemcpyDeviceToHost, c.st));
+    return c.finish();
+}
+
+int mgp_inner_prod(const mgp_box* valid, const mgp_array* a, const mgp_array* b, double* out) {
+    RC(check_box(valid));
+    if (!out) return set_err(MGP_EINVAL, "null output");
+    OpCtx c;
+    DF x, y;
+    double* red = nullptr;
+    RC(c.in(a, valid->nx, valid->ny, 0, &x, "a"));
+    RC(c.in(b, valid->nx, valid->ny, 0, &y, "b"));
+    RC(c.dbuf(&red, kRedSlots));
+    CK(launch_reduce(RED_DOT, x, y, valid->nx, valid->ny, valid->dx * valid->dy, red, red + 2 * 296, c.st));
+    CK(cudaMemcpyAsync(out, red + 2 * 296, 8, cudaMemcpyDeviceToHost, c.st));
+    return c.finish();
+}
+
+int mgp_vcycle(const mgp_box* valid, mgp_array* phi, mgp_array* rhs, const mgp_geo* geo, const mgp_bdry* bc, int homog,
+               int amrrefx, int amrrefy, double tol, int maxiters, int maxdepth_user, int numcycles, int smooth_down,
+               int smooth_up, int smooth_bottom, int zerophi, int verbosity, mgp_report* report) {
+    (void)amrrefx;
+    (void)amrrefy;   // unused by the Fortran driver too (MG:409)
+    return oneshot(0, valid, phi, rhs, geo, bc, homog, tol, maxiters, maxdepth_user, numcycles, smooth_down, smooth_up,
+                   smooth_bottom, zerophi, verbosity, report);
+}
+
+int mgp_fmg(const mgp_box* valid, mgp_array* phi, mgp_array* rhs, const mgp_geo* geo, const mgp_bdry* bc, int homog,
+            int amrrefx, int amrrefy, double tol, int maxiters, int maxdepth_user, int numcycles, int smooth_down,
+            int smooth_up, int smooth_bottom, int zerophi, int verbosity, mgp_report* report) {
+    (void)amrrefx;
+    (void)amrrefy;
+    return oneshot(1, valid, phi, rhs, geo, bc, homog, tol, maxiters, maxdepth_user, numcycles, smooth_down, smooth_up,
+                   smooth_bottom, zerophi, verbosity, report);
+}
+
+int mgp_dc_vcycle(const mgp_box* valid, mgp_array* phi, mgp_array* rhs, const mgp_geo* geo, const mgp_bdry* bc,
+                  int homog, int amrrefx, int amrrefy, double tol, int maxiters, int maxdepth_user, int numcycles,
+                  int smooth_down, int smooth_up, int smooth_bottom, int zerophi, int verbosity, mgp_report* report) {
+    (void)amrrefx;
+    (void)amrrefy;
+    return oneshot(2, valid, phi, rhs, geo, bc, homog, tol, maxiters, maxdepth_user, numcycles, smooth_down, smooth_up,
+                   smooth_bottom, zerophi, verbosity, report);
+}
+
+int mgp_solver_create(const mgp_box* valid, const mgp_geo* geo, const mgp_bdry* bc, int kind, int flags,
+                      int maxdepth_user, mgp_solver** out) {
+    return solver_new(valid, geo, bc, kind, flags, maxdepth_user, nullptr, out);
+}
+
+int mgp_solver_destroy(mgp_solver* s) {
+    solver_free(s);
+    return MGP_OK;
+}
+
+int mgp_solver_set_stream(mgp_solver* s, void* stream) {
+    if (!s) return set_err(MGP_EINVAL, "null solver");
+    s->stream = (cudaStream_t)stream;
+    return MGP_OK;
+}
+
+int mgp_solver_maxdepth(const mgp_solver* s, int* maxdepth) {
+    if (!s || !maxdepth) return set_err(MGP_EINVAL, "null argument");
+    *maxdepth = s->maxdepth;
+    return MGP_OK;
+}
+
+int mgp_solver_vcycle(mgp_solver* s, mgp_array* phi, mgp_array* rhs, const mgp_bdry* bc, int homog, double tol,
+                      int maxiters, int numcycles, int smooth_down, int smooth_up, int smooth_bottom, int zerophi,
+                      int verbosity, mgp_report* report) {
+    if (!s) return set_err(MGP_EINVAL, "null solver");
+    return solver_solve(s, 0, phi, rhs, bc, homog, tol, maxiters, numcycles, smooth_down, smooth_up, smooth_bottom,
+                        zerophi, verbosity, report);
+}
+
+int mgp_solver_fmg(mgp_solver* s, mgp_array* phi, mgp_array* rhs, const mgp_bdry* bc, int homog, double tol,
+                   int maxiters, int numcycles, int smooth_down, int smooth_up, int smooth_bottom, int zerophi,
+                   int verbosity, mgp_report* report) {
+    if (!s) return set_err(MGP_EINVAL, "null solver");
+    return solver_solve(s, 1, phi, rhs, bc, homog, tol, maxiters, numcycles, smooth_down, smooth_up, smooth_bottom,
+                        zerophi, verbosity, report);
+}
+
+int mgp_solver_dc_vcycle(mgp_solver* s, mgp_array* phi, mgp_array* rhs, const mgp_bdry* bc, int homog, double tol,
+                         int maxiters, int numcycles, int smooth_down, int smooth_up, int smooth_bottom, int zerophi,
+                         int verbosity, mgp_report* report) {
+    if (!s) return set_err(MGP_EINVAL, "null solver");
+    return solver_solve(s, 2, phi, rhs, bc, homog, tol, maxiters, numcycles, smooth_down, smooth_up, smooth_bottom,
+                        zerophi, verbosity, report);
+}
+
+}  // extern "C"

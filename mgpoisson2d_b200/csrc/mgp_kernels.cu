@@ -1,0 +1,861 @@
+// mgp_kernels.cu -- CUDA kernels of the B200 multigrid solver (sm_100a, FP64).
+//
+// Two execution shapes:
+//  * grid kernels, one thread per cell, for the large levels;
+//  * one 1024-thread CTA that runs a whole coarse sub-V-cycle, bottom
+//    BiCGStab included (vcycle_noinit from a given depth down, MG:675-854 and
+//    DD:867-1045), so the latency-bound small levels cost one launch.
+// Both call the same cell functions of mgp_core.cuh, so they produce the same
+// bits as each other and as the Fortran loop bodies.
+#include <atomic>
+
+#include "mgp_kernels.cuh"
+
+namespace mgp {
+
+static std::atomic<long long> g_launches{0};
+long long launch_count() { return g_launches.load(); }
+void count_launch(int n) { g_launches += n; }
+
+static inline dim3 cells_grid(int nx, int ny, dim3 blk) {
+    return dim3((unsigned)((nx + blk.x - 1) / blk.x), (unsigned)((ny + blk.y - 1) / blk.y));
+}
+static const dim3 kBlk2(32, 8);
+
+#define CELL_IJ                                              \
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;   \
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+
+// ---------------------------------------------------------------------------
+// Ghost fill (fill_ghosts, AU:1277-1492)
+// ---------------------------------------------------------------------------
+// phase 0: x sides, 1: y sides, 2: corners, 3: all four sides and corners at once
+// (used when no side's fill reads another side's ghosts).
+__global__ void k_fill(DF p, Geo g, BCd b, int homog, int do_neum, int nx, int ny, int phase) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int lo[4], cnt[4];
+    for (int s = 0; s < 4; ++s) side_range(b, s, nx, ny, do_neum, lo[s], cnt[s]);
+    int k = t;
+    const int s0 = (phase == 1) ? 2 : 0, s1 = (phase == 0) ? 2 : 4;
+    if (phase != 2) {
+        for (int s = s0; s < s1; ++s) {
+            if (k < cnt[s]) { fill_side_elem(p, g, b, homog, s, nx, ny, lo[s] + k); return; }
+            k -= cnt[s];
+        }
+    }
+    if (phase >= 2 && k < 4) fill_corner(p, b, nx, ny, k);
+}
+
+static bool fill_single_phase(const BCd& b, int do_neum) {
+    for (int s = 0; s < 4; ++s) {
+        const int t = b.type[s];
+        if (t == T_DIRI || t == T_NONE) continue;
+        if (t == T_NEUM && !do_neum) continue;
+        return false;
+    }
+    return true;
+}
+
+cudaError_t launch_fill(const DF& p, const Geo& g, const BCd& b, int homog, int do_neum, int nx, int ny,
+                        cudaStream_t st) {
+    const int n = 2 * (nx + ny) + 12;
+    const int blk = 256, grd = (n + blk - 1) / blk;
+    if (fill_single_phase(b, do_neum)) {
+        k_fill<<<grd, blk, 0, st>>>(p, g, b, homog, do_neum, nx, ny, 3);
+        count_launch();
+    } else {
+        for (int ph = 0; ph < 3; ++ph) k_fill<<<grd, blk, 0, st>>>(p, g, b, homog, do_neum, nx, ny, ph);
+        count_launch(3);
+    }
+    return cudaGetLastError();
+}
+
+// extrapolate_ghosts (AU:1497-1566): x columns over the whole j range of the
+// allocation, then y rows over the whole i range.
+__global__ void k_extrap(DF p, int nx, int ny, int ngx, int ngy, int order, int phase) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (phase == 0) {
+        const int a = t - ngy;
+        if (a > ny - 1 + ngy) return;
+        const double l3 = nx > 3 ? AT(p, 3, a) : 0.0, h3 = nx > 3 ? AT(p, nx - 4, a) : 0.0;
+        const double vl = extrap_val(order, AT(p, 0, a), AT(p, 1, a), AT(p, 2, a), l3);
+        const double vh = extrap_val(order, AT(p, nx - 1, a), AT(p, nx - 2, a), AT(p, nx - 3, a), h3);
+        AT(p, -1, a) = vl;
+        AT(p, nx, a) = vh;
+    } else {
+        const int a = t - ngx;
+        if (a > nx - 1 + ngx) return;
+        const double l3 = ny > 3 ? AT(p, a, 3) : 0.0, h3 = ny > 3 ? AT(p, a, ny - 4) : 0.0;
+        const double vl = extrap_val(order, AT(p, a, 0), AT(p, a, 1), AT(p, a, 2), l3);
+        const double vh = extrap_val(order, AT(p, a, ny - 1), AT(p, a, ny - 2), AT(p, a, ny - 3), h3);
+        AT(p, a, -1) = vl;
+        AT(p, a, ny) = vh;
+    }
+}
+
+cudaError_t launch_extrapolate(const DF& p, int nx, int ny, int ngx, int ngy, int order, cudaStream_t st) {
+    if (ngx > 0) {
+        const int n = ny + 2 * ngy;
+        k_extrap<<<(n + 255) / 256, 256, 0, st>>>(p, nx, ny, ngx, ngy, order, 0);
+        count_launch();
+    }
+    if (ngy > 0) {
+        const int n = nx + 2 * ngx;
+        k_extrap<<<(n + 255) / 256, 256, 0, st>>>(p, nx, ny, ngx, ngy, order, 1);
+        count_launch();
+    }
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Operator apply / residual (compute_laplacian P2:886-1319, compute_residual P2:1327-1353)
+// ---------------------------------------------------------------------------
+__global__ void k_apply(DF out, DF phi, DF rhs, Geo g, BCd b, int homog, int nx, int ny, int mode, int jscale) {
+    CELL_IJ
+    if (i >= nx || j >= ny) return;
+    double lap = apply9(phi, g, b, homog, nx, ny, i, j);
+    if (jscale) lap = lap / AT(g.J, i, j);
+    AT(out, i, j) = mode ? AT(rhs, i, j) - lap : lap;
+}
+
+cudaError_t launch_apply(const DF& out, const DF& phi, const DF& rhs, const Geo& g, const BCd& b, int homog,
+                         int nx, int ny, int mode, int jscale, cudaStream_t st) {
+    k_apply<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(out, phi, rhs, g, b, homog, nx, ny, mode, jscale);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Gauss-Seidel (relax_gs, P2:1460-1988), one colour per launch
+// ---------------------------------------------------------------------------
+__global__ void k_gs_colour(DF phi, DF rhs, DF invd, Geo g, BCd b, int homog, int nx, int ny, double omega,
+                            int ci, int cj) {
+    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ci;
+    const int j = 2 * (blockIdx.y * blockDim.y + threadIdx.y) + cj;
+    if (i >= nx || j >= ny) return;
+    gs9(phi, rhs, invd, g, b, homog, nx, ny, i, j, omega);
+}
+
+cudaError_t launch_gs_sweep(const DF& phi, const DF& rhs, const DF& invd, const Geo& g, const BCd& b, int homog,
+                            int nx, int ny, double omega, cudaStream_t st) {
+    cudaError_t err = launch_fill(phi, g, b, homog, 0, nx, ny, st);   // P2:1556
+    if (err != cudaSuccess) return err;
+    const dim3 grd = cells_grid((nx + 1) / 2, (ny + 1) / 2, kBlk2);
+    static const int ci[4] = {0, 1, 1, 0}, cj[4] = {0, 1, 0, 1};
+    for (int c = 0; c < 4; ++c)
+        k_gs_colour<<<grd, kBlk2, 0, st>>>(phi, rhs, invd, g, b, homog, nx, ny, omega, ci[c], cj[c]);
+    count_launch(4);
+    return cudaGetLastError();
+}
+
+// compute_invdiags (P2:16-388)
+__global__ void k_invdiag(DF invd, Geo g, BCd b, int homog, int nx, int ny, int coupled) {
+    CELL_IJ
+    if (i >= nx || j >= ny) return;
+    AT(invd, i, j) = 1.0 / diag9(g, b, homog, nx, ny, i, j, coupled != 0);
+}
+
+cudaError_t launch_invdiag(const DF& invd, const Geo& g, const BCd& b, int homog, int nx, int ny, int coupled,
+                           cudaStream_t st) {
+    k_invdiag<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(invd, g, b, homog, nx, ny, coupled);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Restriction (MG:135-257) and prolongation (MG:262-394)
+// ---------------------------------------------------------------------------
+__global__ void k_restrict(DF f, DF c, int ncx, int ncy, int refx, int refy, int kind) {
+    const int ci = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cj = blockIdx.y * blockDim.y + threadIdx.y;
+    if (kind == 0) {
+        if (ci >= ncx || cj >= ncy) return;
+        AT(c, ci, cj) = restrict_cc(f, ci, cj, refx, refy, 1.0 / (refx * refy));
+    } else if (kind == 1) {   // x-faces: inject in x, average in y (MG:192-199)
+        if (ci > ncx || cj >= ncy) return;
+        const double scale = 1.0 / refy;
+        double acc = 0.0;
+        for (int a = 0; a < refy; ++a) acc = acc + scale * AT(f, ci * refx, cj * refy + a);
+        AT(c, ci, cj) = acc;
+    } else if (kind == 2) {   // y-faces: average in x, inject in y (MG:234-241)
+        if (ci >= ncx || cj > ncy) return;
+        const double scale = 1.0 / refx;
+        double acc = 0.0;
+        for (int a = 0; a < refx; ++a) acc = acc + scale * AT(f, ci * refx + a, cj * refy);
+        AT(c, ci, cj) = acc;
+    } else {
+        if (ci > ncx || cj > ncy) return;
+        AT(c, ci, cj) = AT(f, ci * refx, cj * refy);
+    }
+}
+
+cudaError_t launch_restrict(const DF& f, const DF& c, int ncx, int ncy, int refx, int refy, int kind,
+                            cudaStream_t st) {
+    k_restrict<<<cells_grid(ncx + 1, ncy + 1, kBlk2), kBlk2, 0, st>>>(f, c, ncx, ncy, refx, refy, kind);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// Fine += constant + linear (+ second-difference) terms for one coarse cell.
+// The adds happen in the Fortran order: all constant adds (MG:304-314), then
+// the linear ones (MG:316-333), then the quadratic ones (MG:335-352).  Each
+// fine cell belongs to one coarse cell, so doing them per cell in sequence
+// gives the same bits.
+__device__ __forceinline__ void prolong_cell(const DF& fine, const DF& crse, int ci, int cj, int refx, int refy,
+                                             int order) {
+    const double c = AT(crse, ci, cj);
+    const int fi = refx * ci, fj = refy * cj;
+    double f00 = AT(fine, fi, fj);
+    double f10 = refx == 2 ? AT(fine, fi + 1, fj) : 0.0;
+    double f01 = refy == 2 ? AT(fine, fi, fj + 1) : 0.0;
+    double f11 = (refx == 2 && refy == 2) ? AT(fine, fi + 1, fj + 1) : 0.0;
+    f00 = f00 + c; f10 = f10 + c; f01 = f01 + c; f11 = f11 + c;
+    if (order >= 1) {
+        const double mx = 0.5 * (AT(crse, ci + 1, cj) - AT(crse, ci - 1, cj));
+        const double my = 0.5 * (AT(crse, ci, cj + 1) - AT(crse, ci, cj - 1));
+        if (refx == 2 && refy == 2) {
+            f00 = f00 + 0.25 * (-mx - my);
+            f10 = f10 + 0.25 * (mx - my);
+            f01 = f01 + 0.25 * (-mx + my);
+            f11 = f11 + 0.25 * (mx + my);
+        } else if (refx == 2) {
+            f00 = f00 + 0.25 * (-mx);
+            f10 = f10 + 0.25 * (mx);
+        } else {
+            f00 = f00 + 0.25 * (-my);
+            f01 = f01 + 0.25 * (my);
+        }
+    }
+    if (order >= 2) {
+        const double mx = 0.25 * (AT(crse, ci + 1, cj) - 2.0 * AT(crse, ci, cj) + AT(crse, ci - 1, cj));
+        const double my = 0.25 * (AT(crse, ci, cj + 1) - 2.0 * AT(crse, ci, cj) + AT(crse, ci, cj - 1));
+        const double q = (refx == 2 && refy == 2) ? 0.125 * (mx + my) : (refx == 2 ? 0.125 * mx : 0.125 * my);
+        f00 = f00 + q; f10 = f10 + q; f01 = f01 + q; f11 = f11 + q;
+    }
+    AT(fine, fi, fj) = f00;
+    if (refx == 2) AT(fine, fi + 1, fj) = f10;
+    if (refy == 2) AT(fine, fi, fj + 1) = f01;
+    if (refx == 2 && refy == 2) AT(fine, fi + 1, fj + 1) = f11;
+}
+
+// Cross term of the order-2 prolongation (MG:354-369); crse ghosts hold the
+// order-3 extrapolation.
+__device__ __forceinline__ void prolong_cross_cell(const DF& fine, const DF& crse, int ci, int cj) {
+    const int fi = 2 * ci, fj = 2 * cj;
+    const double mc = 0.0625 * (AT(crse, ci + 1, cj + 1) - AT(crse, ci + 1, cj - 1) - AT(crse, ci - 1, cj + 1) +
+                                AT(crse, ci - 1, cj - 1));
+    AT(fine, fi, fj) = AT(fine, fi, fj) + 0.25 * mc;
+    AT(fine, fi + 1, fj) = AT(fine, fi + 1, fj) - 0.25 * mc;
+    AT(fine, fi, fj + 1) = AT(fine, fi, fj + 1) - 0.25 * mc;
+    AT(fine, fi + 1, fj + 1) = AT(fine, fi + 1, fj + 1) + 0.25 * mc;
+}
+
+__global__ void k_prolong(DF fine, DF crse, int ncx, int ncy, int refx, int refy, int order) {
+    const int ci = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cj = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ci >= ncx || cj >= ncy) return;
+    prolong_cell(fine, crse, ci, cj, refx, refy, order);
+}
+
+__global__ void k_prolong_cross(DF fine, DF crse, int ncx, int ncy) {
+    const int ci = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cj = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ci >= ncx || cj >= ncy) return;
+    prolong_cross_cell(fine, crse, ci, cj);
+}
+
+cudaError_t launch_prolong(const DF& fine, const DF& crse, int ncx, int ncy, int refx, int refy, int order,
+                           cudaStream_t st) {
+    k_prolong<<<cells_grid(ncx, ncy, kBlk2), kBlk2, 0, st>>>(fine, crse, ncx, ncy, refx, refy, order);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prolong_cross(const DF& fine, const DF& crse, int ncx, int ncy, cudaStream_t st) {
+    k_prolong_cross<<<cells_grid(ncx, ncy, kBlk2), kBlk2, 0, st>>>(fine, crse, ncx, ncy);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Elementwise helpers
+// ---------------------------------------------------------------------------
+__global__ void k_set_guess(DF e, DF r, DF invd, int nx, int ny) {
+    CELL_IJ
+    if (i >= nx || j >= ny) return;
+    AT(e, i, j) = AT(r, i, j) * AT(invd, i, j);
+}
+
+cudaError_t launch_set_guess(const DF& e, const DF& r, const DF& invd, int nx, int ny, cudaStream_t st) {
+    k_set_guess<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(e, r, invd, nx, ny);
+    count_launch();
+    return cudaGetLastError();
+}
+
+__global__ void k_axpby(DF y, DF x, double a, double b, int nx, int ny, int gx, int gy) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x - gx;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y - gy;
+    if (i >= nx + gx || j >= ny + gy) return;
+    // a == 1: y + b*x (the Fortran `y = y + b*x`); b == 1 too: y + x.
+    const double yv = AT(y, i, j), xv = AT(x, i, j);
+    double v;
+    if (a == 1.0 && b == 1.0) v = yv + xv;
+    else if (a == 1.0 && b == -1.0) v = yv - xv;
+    else if (a == 1.0) v = yv + b * xv;
+    else if (a == 0.0) v = b * xv;
+    else v = a * yv + b * xv;
+    AT(y, i, j) = v;
+}
+
+cudaError_t launch_axpby(const DF& y, const DF& x, double a, double b, int nx, int ny, int gx, int gy,
+                         cudaStream_t st) {
+    k_axpby<<<cells_grid(nx + 2 * gx, ny + 2 * gy, kBlk2), kBlk2, 0, st>>>(y, x, a, b, nx, ny, gx, gy);
+    count_launch();
+    return cudaGetLastError();
+}
+
+__global__ void k_muldiv(DF y, DF x, int mul, int nx, int ny) {
+    CELL_IJ
+    if (i >= nx || j >= ny) return;
+    AT(y, i, j) = mul ? AT(y, i, j) * AT(x, i, j) : AT(y, i, j) / AT(x, i, j);
+}
+
+cudaError_t launch_muldiv(const DF& y, const DF& x, int mul, int nx, int ny, cudaStream_t st) {
+    k_muldiv<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(y, x, mul, nx, ny);
+    count_launch();
+    return cudaGetLastError();
+}
+
+__global__ void k_fillval(DF y, double v, int nx, int ny, int gx, int gy) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x - gx;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y - gy;
+    if (i >= nx + gx || j >= ny + gy) return;
+    AT(y, i, j) = v;
+}
+
+// y -= out[0] / out[1] over the whole allocation (prolong's mean removal, MG:371-383).
+__global__ void k_sub_mean(DF y, const double* out, int nx, int ny, int gx, int gy) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x - gx;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y - gy;
+    if (i >= nx + gx || j >= ny + gy) return;
+    AT(y, i, j) = AT(y, i, j) - out[0] / out[1];
+}
+
+cudaError_t launch_sub_mean(const DF& y, const double* out, int nx, int ny, int gx, int gy, cudaStream_t st) {
+    k_sub_mean<<<cells_grid(nx + 2 * gx, ny + 2 * gy, kBlk2), kBlk2, 0, st>>>(y, out, nx, ny, gx, gy);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fillval(const DF& y, double v, int nx, int ny, int gx, int gy, cudaStream_t st) {
+    k_fillval<<<cells_grid(nx + 2 * gx, ny + 2 * gy, kBlk2), kBlk2, 0, st>>>(y, v, nx, ny, gx, gy);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic reductions (pnorm AU:753-796, inner_prod AU:637-661,
+// the J-weighted mean of prolong MG:371-383).  Fixed assignment of cells to
+// threads and a fixed tree, so the result does not depend on scheduling.
+// ---------------------------------------------------------------------------
+constexpr int kRedThreads = 256;
+constexpr int kRedBlocks = 296;   // 2 x 148 SMs
+
+__device__ __forceinline__ double red_term(int kind, const DF& a, const DF& b, int i, int j, double& w) {
+    const double v = AT(a, i, j);
+    switch (kind) {
+        case RED_SUMSQ: return v * v;
+        case RED_MAXABS: return fabs(v);
+        case RED_DOT: return v * AT(b, i, j);
+        case RED_ABSSUM: return fabs(v);
+        default: { const double jj = AT(b, i, j); w = jj; return jj * v; }
+    }
+}
+
+__global__ void k_reduce_partial(int kind, DF a, DF b, int nx, int ny, double* partials) {
+    __shared__ double s0[kRedThreads], s1[kRedThreads];
+    const long n = (long)nx * ny;
+    double acc = 0.0, accw = 0.0;
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(k % nx), j = (int)(k / nx);
+        double w = 0.0;
+        const double t = red_term(kind, a, b, i, j, w);
+        if (kind == RED_MAXABS) acc = fmax(acc, t);
+        else acc = acc + t;
+        accw = accw + w;
+    }
+    s0[threadIdx.x] = acc;
+    s1[threadIdx.x] = accw;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            s0[threadIdx.x] = (kind == RED_MAXABS) ? fmax(s0[threadIdx.x], s0[threadIdx.x + s])
+                                                   : s0[threadIdx.x] + s0[threadIdx.x + s];
+            s1[threadIdx.x] = s1[threadIdx.x] + s1[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = s0[0];
+        partials[2 * blockIdx.x + 1] = s1[0];
+    }
+}
+
+__global__ void k_reduce_final(int kind, const double* partials, int nb, double vol, double* out) {
+    __shared__ double s0[512], s1[512];
+    double acc = 0.0, accw = 0.0;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+        acc = (kind == RED_MAXABS) ? fmax(acc, partials[2 * k]) : acc + partials[2 * k];
+        accw = accw + partials[2 * k + 1];
+    }
+    s0[threadIdx.x] = acc;
+    s1[threadIdx.x] = accw;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            s0[threadIdx.x] = (kind == RED_MAXABS) ? fmax(s0[threadIdx.x], s0[threadIdx.x + s])
+                                                   : s0[threadIdx.x] + s0[threadIdx.x + s];
+            s1[threadIdx.x] = s1[threadIdx.x] + s1[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        if (kind == RED_SUMSQ) out[0] = sqrt(vol * s0[0]);
+        else if (kind == RED_MAXABS) out[0] = s0[0];
+        else if (kind == RED_JSUM) { out[0] = vol * s0[0]; out[1] = vol * s1[0]; }
+        else out[0] = vol * s0[0];
+    }
+}
+
+cudaError_t launch_reduce(int kind, const DF& a, const DF& b, int nx, int ny, double vol, double* partials,
+                          double* out, cudaStream_t st) {
+    const long n = (long)nx * ny;
+    int nb = (int)((n + kRedThreads - 1) / kRedThreads);
+    if (nb > kRedBlocks) nb = kRedBlocks;
+    if (nb < 1) nb = 1;
+    k_reduce_partial<<<nb, kRedThreads, 0, st>>>(kind, a, b, nx, ny, partials);
+    k_reduce_final<<<1, 512, 0, st>>>(kind, partials, nb, vol, out);
+    count_launch(2);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Deferred-correction operators (DD:16-334)
+// ---------------------------------------------------------------------------
+__global__ void k_dd_invdiag(DF invd, Geo g, int nx, int ny) {
+    CELL_IJ
+    if (i >= nx || j >= ny) return;
+    const double idx2 = 1.0 / (g.dx * g.dx), idy2 = 1.0 / (g.dy * g.dy);
+    const double d = (AT(g.xx, i + 1, j) + AT(g.xx, i, j)) * idx2 + (AT(g.yy, i, j + 1) + AT(g.yy, i, j)) * idy2;
+    AT(invd, i, j) = -1.0 / d;
+}
+
+cudaError_t launch_dd_invdiag(const DF& invd, const Geo& g, int nx, int ny, cudaStream_t st) {
+    k_dd_invdiag<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(invd, g, nx, ny);
+    count_launch();
+    return cudaGetLastError();
+}
+
+__global__ void k_dd_apply(DF out, DF phi, DF rhs, Geo g, BCd b, int nx, int ny, int mode) {
+    CELL_IJ
+    if (i >= nx || j >= ny) return;
+    const double lap = dd_apply(phi, g, b, nx, ny, i, j);
+    AT(out, i, j) = mode ? AT(rhs, i, j) - lap : lap;
+}
+
+cudaError_t launch_dd_apply(const DF& out, const DF& phi, const DF& rhs, const Geo& g, const BCd& b, int nx, int ny,
+                            int mode, cudaStream_t st) {
+    k_dd_apply<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(out, phi, rhs, g, b, nx, ny, mode);
+    count_launch();
+    return cudaGetLastError();
+}
+
+__global__ void k_dd_modrhs(DF out, DF phi, DF rhs, Geo g, int nx, int ny) {
+    CELL_IJ
+    if (i >= nx || j >= ny) return;
+    AT(out, i, j) = dd_modrhs(phi, rhs, g, nx, ny, i, j);
+}
+
+cudaError_t launch_dd_modrhs(const DF& out, const DF& phi, const DF& rhs, const Geo& g, int nx, int ny,
+                             cudaStream_t st) {
+    k_dd_modrhs<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(out, phi, rhs, g, nx, ny);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// Red-black colour of DD:262-285 (parity of i+j relative to the valid corner).
+__global__ void k_dd_colour(DF phi, DF modrhs, DF invd, Geo g, int nx, int ny, double omega, int colour) {
+    const int jj = blockIdx.y * blockDim.y + threadIdx.y;
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    if (jj >= ny) return;
+    const int i = 2 * ii + ((colour + jj) & 1);
+    if (i >= nx) return;
+    dd_gs(phi, modrhs, invd, g, i, jj, omega);
+}
+
+cudaError_t launch_dd_colour(const DF& phi, const DF& modrhs, const DF& invd, const Geo& g, int nx, int ny,
+                             double omega, int colour, cudaStream_t st) {
+    k_dd_colour<<<cells_grid((nx + 1) / 2, ny, kBlk2), kBlk2, 0, st>>>(phi, modrhs, invd, g, nx, ny, omega, colour);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Single-CTA building blocks (every thread of the block calls them)
+// ---------------------------------------------------------------------------
+#define BLOOP(k, n) for (int k = threadIdx.x; k < (n); k += blockDim.x)
+
+__device__ void b_fill(const DF& p, const Geo& g, const BCd& b, int homog, int do_neum, int nx, int ny) {
+    int lo[4], cnt[4];
+    for (int s = 0; s < 4; ++s) side_range(b, s, nx, ny, do_neum, lo[s], cnt[s]);
+    BLOOP(k, cnt[0] + cnt[1]) {
+        if (k < cnt[0]) fill_side_elem(p, g, b, homog, 0, nx, ny, lo[0] + k);
+        else fill_side_elem(p, g, b, homog, 1, nx, ny, lo[1] + k - cnt[0]);
+    }
+    __syncthreads();
+    BLOOP(k, cnt[2] + cnt[3]) {
+        if (k < cnt[2]) fill_side_elem(p, g, b, homog, 2, nx, ny, lo[2] + k);
+        else fill_side_elem(p, g, b, homog, 3, nx, ny, lo[3] + k - cnt[2]);
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) fill_corner(p, b, nx, ny, threadIdx.x);
+    __syncthreads();
+}
+
+__device__ double b_sum(double v, double* sh) {
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] = sh[threadIdx.x] + sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+__device__ double b_max(double v, double* sh) {
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + s]);
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// pnorm (AU:753-796) with p = 2 or 0.
+__device__ double b_pnorm(const DF& a, int nx, int ny, int p, double vol, double* sh) {
+    double acc = 0.0;
+    BLOOP(k, nx * ny) {
+        const double v = AT(a, k % nx, k / nx);
+        acc = (p == 0) ? fmax(acc, fabs(v)) : acc + v * v;
+    }
+    if (p == 0) return b_max(acc, sh);
+    return sqrt(vol * b_sum(acc, sh));
+}
+
+__device__ double b_dot(const DF& a, const DF& c, int nx, int ny, double vol, double* sh) {
+    double acc = 0.0;
+    BLOOP(k, nx * ny) acc = acc + AT(a, k % nx, k / nx) * AT(c, k % nx, k / nx);
+    return vol * b_sum(acc, sh);
+}
+
+// y = a*y + b*x over [-g, n+g) in both directions (g = 1 for ghosted arrays).
+__device__ void b_axpby(const DF& y, const DF& x, double a, double bb, int nx, int ny, int g) {
+    const int w = nx + 2 * g, h = ny + 2 * g;
+    BLOOP(k, w * h) {
+        const int i = k % w - g, j = k / w - g;
+        const double yv = AT(y, i, j), xv = AT(x, i, j);
+        double v;
+        if (a == 1.0 && bb == 1.0) v = yv + xv;
+        else if (a == 1.0 && bb == -1.0) v = yv - xv;
+        else if (a == 1.0) v = yv + bb * xv;
+        else if (a == 0.0) v = bb * xv;
+        else v = a * yv + bb * xv;
+        AT(y, i, j) = v;
+    }
+    __syncthreads();
+}
+
+__device__ void b_setval(const DF& y, double v, int nx, int ny, int g) {
+    const int w = nx + 2 * g, h = ny + 2 * g;
+    BLOOP(k, w * h) AT(y, k % w - g, k / w - g) = v;
+    __syncthreads();
+}
+
+__device__ void b_mul(const DF& out, const DF& a, const DF& c, int nx, int ny) {
+    BLOOP(k, nx * ny) AT(out, k % nx, k / nx) = AT(a, k % nx, k / nx) * AT(c, k % nx, k / nx);
+    __syncthreads();
+}
+
+// 9-point sweeps (MG smoother), P2:1460-1988.
+__device__ void b_relax9(const Lv& L, const DF& phi, const DF& rhs, int homog, double omega, int sweeps) {
+    const int nx = L.nx, ny = L.ny;
+    const int hx = (nx + 1) / 2, hy = (ny + 1) / 2;
+    for (int it = 0; it < sweeps; ++it) {
+        b_fill(phi, L.g, L.bc, homog, 0, nx, ny);
+        for (int c = 0; c < 4; ++c) {
+            const int ci = colour_ci(c), cj = colour_cj(c);
+            BLOOP(k, hx * hy) {
+                const int i = 2 * (k % hx) + ci, j = 2 * (k / hx) + cj;
+                if (i < nx && j < ny) gs9(phi, rhs, L.invd, L.g, L.bc, homog, nx, ny, i, j, omega);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// 5-point red-black sweeps of the deferred-correction smoother (DD:153-334).
+// modrhs is computed once per call, into L.w.
+__device__ void b_relax_dd(const Lv& L, const DF& phi, const DF& rhs, int homog, double omega, int sweeps) {
+    const int nx = L.nx, ny = L.ny;
+    if (sweeps == 0) return;
+    BLOOP(k, nx * ny) AT(L.w, k % nx, k / nx) = dd_modrhs(phi, rhs, L.g, nx, ny, k % nx, k / nx);
+    __syncthreads();
+    const int hx = (nx + 1) / 2;
+    for (int it = 0; it < sweeps; ++it) {
+        b_fill(phi, L.g, L.bc, homog, 1, nx, ny);   // DD:259, neum_ghosts = .true.
+        for (int colour = 0; colour < 2; ++colour) {
+            BLOOP(k, hx * ny) {
+                const int j = k / hx, i = 2 * (k % hx) + ((colour + j) & 1);
+                if (i < nx) dd_gs(phi, L.w, L.invd, L.g, i, j, omega);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// out = rhs - L[phi] (mode 1) or L[phi] (mode 0); fills phi's ghosts first as the Fortran routines do.
+__device__ void b_apply(const Lv& L, const DF& out, const DF& phi, const DF& rhs, int homog, int mode, int dd) {
+    const int nx = L.nx, ny = L.ny;
+    if (dd) {
+        BLOOP(k, nx * ny) {
+            const int i = k % nx, j = k / nx;
+            const double lap = dd_apply(phi, L.g, L.bc, nx, ny, i, j);
+            AT(out, i, j) = mode ? AT(rhs, i, j) - lap : lap;
+        }
+        __syncthreads();
+        b_fill(phi, L.g, L.bc, homog, 1, nx, ny);   // ghost state the DD routine leaves (DD:99)
+    } else {
+        b_fill(phi, L.g, L.bc, homog, 0, nx, ny);   // P2:935
+        BLOOP(k, nx * ny) {
+            const int i = k % nx, j = k / nx;
+            const double lap = apply9(phi, L.g, L.bc, homog, nx, ny, i, j);
+            AT(out, i, j) = mode ? AT(rhs, i, j) - lap : lap;
+        }
+        __syncthreads();
+    }
+}
+
+__device__ void b_relax(const Lv& L, const DF& phi, const DF& rhs, int homog, double omega, int sweeps, int dd) {
+    if (dd) b_relax_dd(L, phi, rhs, homog, omega, sweeps);
+    else b_relax9(L, phi, rhs, homog, omega, sweeps);
+}
+
+// solve_bicgstab2 (P2:2253-2477; DD:339-566 with dd = 1).  Status: 0 or 3 (non-finite).
+__device__ int b_bicgstab(const Lv& L, const DF& phi, const DF& rhs, int homog, double tol, int max_iters,
+                          int max_restarts, int zerophi, int dd, double* sh) {
+    const double reps = 1.0e-12, hang = 1.0e-7, small = 1.0e-30;
+    const int norm_type = dd ? 0 : 2;
+    const double relax_omega = dd ? 4.0 / 5.0 : 1.0 - 1.0 / 3.0;
+    const int nx = L.nx, ny = L.ny;
+    const double vol = L.g.dx * L.g.dy;
+    const DF &e = L.ea, &pt = L.pt, &st = L.st, &r = L.rr, &rt = L.rt, &p = L.pp, &t = L.tt, &v = L.vv;
+    double rho[4] = {0, 0, 0, 0}, norm[2], alpha[2] = {0, 0}, beta[2] = {0, 0}, omg[2] = {0, 0};
+    int recount = 0, i = 0, restarts = 0, init = 1;
+    if (max_iters == 0) return 0;
+    if (zerophi) b_setval(phi, 0.0, nx, ny, 1);
+    b_apply(L, r, phi, rhs, homog, 1, dd);
+    b_axpby(rt, r, 0.0, 1.0, nx, ny, 0);
+    b_setval(e, 0.0, nx, ny, 1);
+    b_setval(pt, 0.0, nx, ny, 1);
+    b_setval(st, 0.0, nx, ny, 1);
+    norm[0] = b_pnorm(r, nx, ny, norm_type, vol, sh);
+    const double initial_norm = norm[0], initial_rnorm = norm[0];
+    norm[1] = norm[0];
+    while (((i < max_iters) && (norm[0] > tol * norm[1])) && (norm[1] > 0.0)) {
+        i = i + 1;
+        norm[1] = norm[0];
+        alpha[1] = alpha[0];
+        beta[1] = beta[0];
+        omg[1] = omg[0];
+        rho[3] = rho[2];
+        rho[2] = rho[1];
+        rho[1] = b_dot(rt, r, nx, ny, vol, sh);
+        if (rho[1] == 0.0) {
+            b_axpby(phi, e, 1.0, 1.0, nx, ny, 1);
+            return 0;
+        }
+        if (init) {
+            b_axpby(p, r, 0.0, 1.0, nx, ny, 0);
+            init = 0;
+        } else {
+            beta[1] = (rho[1] / rho[2]) * (alpha[1] / omg[1]);
+            BLOOP(k, nx * ny) {
+                const int a = k % nx, c = k / nx;
+                AT(p, a, c) = beta[1] * (AT(p, a, c) - omg[1] * AT(v, a, c)) + AT(r, a, c);
+            }
+            __syncthreads();
+        }
+        b_mul(pt, p, L.invd, nx, ny);
+        b_relax(L, pt, p, 1, relax_omega, 2, dd);
+        b_apply(L, v, pt, p, 1, 0, dd);
+        const double m = b_dot(rt, v, nx, ny, vol, sh);
+        alpha[0] = rho[1] / m;
+        if (fabs(m) > small * fabs(rho[1])) {
+            b_axpby(r, v, 1.0, -alpha[0], nx, ny, 0);
+            norm[0] = b_pnorm(r, nx, ny, norm_type, vol, sh);
+            b_axpby(e, pt, 1.0, alpha[0], nx, ny, 1);
+        } else {
+            b_setval(r, 0.0, nx, ny, 0);
+            norm[0] = 0.0;
+        }
+        if ((norm[0] > tol * initial_norm) && (norm[0] > reps * initial_rnorm)) {
+            b_mul(st, r, L.invd, nx, ny);
+            b_relax(L, st, r, 1, relax_omega, 2, dd);
+            b_apply(L, t, st, r, 1, 0, dd);
+            const double tr = b_dot(t, r, nx, ny, vol, sh);
+            const double tt = b_dot(t, t, nx, ny, vol, sh);
+            omg[0] = tr / tt;
+            b_axpby(e, st, 1.0, omg[0], nx, ny, 1);
+            b_axpby(r, t, 1.0, -omg[0], nx, ny, 0);
+            norm[0] = b_pnorm(r, nx, ny, norm_type, vol, sh);
+        }
+        if ((norm[0] <= tol * initial_norm) || (norm[0] <= reps * initial_rnorm)) break;
+        if ((omg[0] == 0.0) || (norm[0] > (1.0 - hang) * norm[1])) {
+            if (recount == 0) {
+                recount = 1;
+            } else {
+                recount = 0;
+                b_axpby(phi, e, 1.0, 1.0, nx, ny, 1);
+                if (restarts == max_restarts) break;   // then e is added again below (P2:2466)
+                b_apply(L, r, phi, rhs, homog, 1, dd);
+                norm[0] = b_pnorm(r, nx, ny, norm_type, vol, sh);
+                rho[1] = rho[2] = rho[3] = 0.0;
+                alpha[0] = beta[0] = omg[0] = 0.0;
+                b_axpby(rt, r, 0.0, 1.0, nx, ny, 0);
+                b_setval(e, 0.0, nx, ny, 1);
+                restarts = restarts + 1;
+                init = 1;
+            }
+        }
+    }
+    b_axpby(phi, e, 1.0, 1.0, nx, ny, 1);
+    return isfinite(norm[0]) ? 0 : 3;
+}
+
+// ---------------------------------------------------------------------------
+// The coarse sub-cycle: vcycle_noinit(d0) run to the bottom in one CTA.
+// ---------------------------------------------------------------------------
+__device__ void b_prolong(const Lv& F, const Lv& Cl, int refx, int refy, int order, double* sh) {
+    // fill_ghosts(crse, homog=.true., do_neum=.true.) (MG:318), then the fused add
+    b_fill(Cl.e, Cl.g, Cl.bc, 1, 1, Cl.nx, Cl.ny);
+    BLOOP(k, Cl.nx * Cl.ny) prolong_cell(F.e, Cl.e, k % Cl.nx, k / Cl.nx, refx, refy, order);
+    __syncthreads();
+    const bool rax = (Cl.bc.type[0] == T_PERIODIC && Cl.bc.type[1] == T_PERIODIC) ||
+                     (Cl.bc.type[0] == T_NEUM && Cl.bc.type[1] == T_NEUM);
+    const bool ray = (Cl.bc.type[2] == T_PERIODIC && Cl.bc.type[3] == T_PERIODIC) ||
+                     (Cl.bc.type[2] == T_NEUM && Cl.bc.type[3] == T_NEUM);
+    if (rax && ray) {   // MG:371-383
+        const double dxprod = F.g.dx * F.g.dy;
+        double s = 0.0, vv = 0.0;
+        BLOOP(k, F.nx * F.ny) {
+            const double jj = AT(F.g.J, k % F.nx, k / F.nx);
+            s = s + jj * AT(F.e, k % F.nx, k / F.nx);
+            vv = vv + jj;
+        }
+        const double sum = dxprod * b_sum(s, sh), vol = dxprod * b_sum(vv, sh);
+        const double avg = sum / vol;
+        const int w = F.nx + 2, h = F.ny + 2;
+        BLOOP(k, w * h) AT(F.e, k % w - 1, k / w - 1) = AT(F.e, k % w - 1, k / w - 1) - avg;
+        __syncthreads();
+    }
+}
+
+__device__ void b_set_guess(const Lv& L) {
+    BLOOP(k, L.nx * L.ny) AT(L.e, k % L.nx, k / L.nx) = AT(L.r, k % L.nx, k / L.nx) * AT(L.invd, k % L.nx, k / L.nx);
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kCoarseThreads) k_coarse_cycle(CoarseArgs a) {
+    __shared__ double sh[kCoarseThreads];
+    int cnt[32];
+    const double relax_omega = a.dd ? 4.0 / 5.0 : 1.0;
+    int d = a.d0;
+    int st = 0;
+visit:
+    {
+        const Lv& L = a.lv[d];
+        if (a.dd) b_set_guess(L);   // DD:931, DD:971
+        if (d == a.maxdepth) {
+            b_relax(L, L.e, L.r, 1, relax_omega, a.nb, a.dd);
+            const int s = b_bicgstab(L, L.e, L.r, 1, 1.0e-6, 80, 5, 0, a.dd, sh);
+            if (s) st = s;
+            goto up;
+        }
+        b_relax(L, L.e, L.r, 1, relax_omega, a.nd, a.dd);
+        b_apply(L, L.w, L.e, L.r, 1, 1, a.dd);
+        const Lv& Cl = a.lv[d + 1];
+        const int rx = a.refx[d], ry = a.refy[d];
+        BLOOP(k, Cl.nx * Cl.ny) AT(Cl.r, k % Cl.nx, k / Cl.nx) =
+            restrict_cc(L.w, k % Cl.nx, k / Cl.nx, rx, ry, 1.0 / (rx * ry));
+        __syncthreads();
+        if (!a.dd) b_set_guess(Cl);   // MG:805-806
+        cnt[d] = 0;
+        d = d + 1;
+        goto visit;
+    }
+up:
+    if (d == a.d0) {
+        if (threadIdx.x == 0 && st) *a.status = st;
+        return;
+    }
+    d = d - 1;
+    cnt[d] = cnt[d] + 1;
+    if (cnt[d] < a.numcycles) {
+        d = d + 1;
+        goto visit;
+    }
+    {
+        const Lv& L = a.lv[d];
+        b_prolong(L, a.lv[d + 1], a.refx[d], a.refy[d], 1, sh);
+        b_relax(L, L.e, L.r, 1, relax_omega, a.nu, a.dd);
+    }
+    goto up;
+}
+
+cudaError_t launch_coarse_cycle(const CoarseArgs& a, cudaStream_t st) {
+    k_coarse_cycle<<<1, kCoarseThreads, 0, st>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(kCoarseThreads) k_bicgstab(BicgArgs a) {
+    __shared__ double sh[kCoarseThreads];
+    const int s = b_bicgstab(a.L, a.phi, a.rhs, a.homog, a.tol, a.max_iters, a.max_restarts, a.zerophi, a.dd, sh);
+    if (threadIdx.x == 0 && s) *a.status = s;
+}
+
+cudaError_t launch_bicgstab(const BicgArgs& a, cudaStream_t st) {
+    k_bicgstab<<<1, kCoarseThreads, 0, st>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(kCoarseThreads) k_relax_block(Lv L, DF phi, DF rhs, int homog, double omega,
+                                                               int sweeps, int dd) {
+    b_relax(L, phi, rhs, homog, omega, sweeps, dd);
+}
+
+cudaError_t launch_relax_block(const Lv& L, const DF& phi, const DF& rhs, int homog, double omega, int sweeps,
+                               int dd, int* status, cudaStream_t st) {
+    (void)status;
+    k_relax_block<<<1, kCoarseThreads, 0, st>>>(L, phi, rhs, homog, omega, sweeps, dd);
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace mgp

@@ -1,0 +1,82 @@
+// mgp_kernels.cuh -- kernel launchers shared by the host drivers (mgp_host.cu)
+// and the kernels (mgp_kernels.cu).
+#pragma once
+#include "mgp_core.cuh"
+
+namespace mgp {
+
+// Reduction kinds of launch_reduce.
+enum RedKind { RED_SUMSQ = 0, RED_MAXABS = 1, RED_DOT = 2, RED_JSUM = 3, RED_ABSSUM = 4 };
+
+// Parameters of the single-CTA coarse cycle.
+struct CoarseArgs {
+    const Lv* lv;        // device array of levels
+    int d0;              // level the cycle starts at (vcycle_noinit(d0) semantics)
+    int maxdepth;
+    int numcycles;
+    int nd, nu, nb;      // smoothing counts
+    int dd;              // 1: DeferredPoisson2D operators
+    const int* refx;     // device arrays, maxdepth entries
+    const int* refy;
+    int* status;         // device int: 0 ok, nonzero = error code
+};
+
+// Parameters of the single-CTA BiCGStab (solve_bicgstab2).
+struct BicgArgs {
+    Lv L;
+    DF phi, rhs;
+    int homog;
+    double tol;
+    int max_iters, max_restarts, zerophi;
+    int dd;
+    int* status;
+};
+
+constexpr int kCoarseThreads = 1024;
+
+long long launch_count();
+void count_launch(int n = 1);
+
+cudaError_t launch_fill(const DF& p, const Geo& g, const BCd& b, int homog, int do_neum, int nx, int ny,
+                        cudaStream_t st);
+cudaError_t launch_extrapolate(const DF& p, int nx, int ny, int ngx, int ngy, int order, cudaStream_t st);
+// mode: 0 lap, 1 rhs - lap; jscale divides lap by J first.
+cudaError_t launch_apply(const DF& out, const DF& phi, const DF& rhs, const Geo& g, const BCd& b, int homog,
+                         int nx, int ny, int mode, int jscale, cudaStream_t st);
+cudaError_t launch_gs_sweep(const DF& phi, const DF& rhs, const DF& invd, const Geo& g, const BCd& b, int homog,
+                            int nx, int ny, double omega, cudaStream_t st);
+cudaError_t launch_invdiag(const DF& invd, const Geo& g, const BCd& b, int homog, int nx, int ny, int coupled,
+                           cudaStream_t st);
+// kind: 0 cell, 1 x-face, 2 y-face, 3 node.  ncx/ncy = coarse cell counts.
+cudaError_t launch_restrict(const DF& f, const DF& c, int ncx, int ncy, int refx, int refy, int kind,
+                            cudaStream_t st);
+// Constant, linear and (order 2) second-difference terms; crse ghosts must be filled.
+cudaError_t launch_prolong(const DF& fine, const DF& crse, int ncx, int ncy, int refx, int refy, int order,
+                           cudaStream_t st);
+cudaError_t launch_prolong_cross(const DF& fine, const DF& crse, int ncx, int ncy, cudaStream_t st);
+cudaError_t launch_set_guess(const DF& e, const DF& r, const DF& invd, int nx, int ny, cudaStream_t st);
+// y[i,j] = a*y + b*x over i in [-gx, nx+gx), j in [-gy, ny+gy).
+cudaError_t launch_axpby(const DF& y, const DF& x, double a, double b, int nx, int ny, int gx, int gy,
+                         cudaStream_t st);
+// y = y * x (mul=1) or y / x (mul=0) over the valid region.
+cudaError_t launch_muldiv(const DF& y, const DF& x, int mul, int nx, int ny, cudaStream_t st);
+cudaError_t launch_fillval(const DF& y, double v, int nx, int ny, int gx, int gy, cudaStream_t st);
+cudaError_t launch_sub_mean(const DF& y, const double* out, int nx, int ny, int gx, int gy, cudaStream_t st);
+// Reduction over the valid region into out[0] (and out[1] for RED_JSUM: volume).
+cudaError_t launch_reduce(int kind, const DF& a, const DF& b, int nx, int ny, double vol, double* partials,
+                          double* out, cudaStream_t st);
+// Deferred-correction operators.
+cudaError_t launch_dd_invdiag(const DF& invd, const Geo& g, int nx, int ny, cudaStream_t st);
+cudaError_t launch_dd_apply(const DF& out, const DF& phi, const DF& rhs, const Geo& g, const BCd& b, int nx, int ny,
+                            int mode, cudaStream_t st);
+cudaError_t launch_dd_modrhs(const DF& out, const DF& phi, const DF& rhs, const Geo& g, int nx, int ny,
+                             cudaStream_t st);
+cudaError_t launch_dd_colour(const DF& phi, const DF& modrhs, const DF& invd, const Geo& g, int nx, int ny,
+                             double omega, int colour, cudaStream_t st);
+// Single-CTA kernels.
+cudaError_t launch_coarse_cycle(const CoarseArgs& a, cudaStream_t st);
+cudaError_t launch_bicgstab(const BicgArgs& a, cudaStream_t st);
+cudaError_t launch_relax_block(const Lv& L, const DF& phi, const DF& rhs, int homog, double omega, int sweeps,
+                               int dd, int* status, cudaStream_t st);
+
+}  // namespace mgp

@@ -1,0 +1,108 @@
+"""Seeded synthetic inputs of the benchmark workloads and of the reference's
+own known-answer tests.  All functions return host containers
+(``Box``, ``GeoData``, ``BoxData`` rhs, ``BdryData``) plus whatever exact
+solution the workload has.
+
+* ``identity_dirichlet``  -- unit square, identity map, homogeneous Dirichlet,
+  rhs = Laplacian of sin(2 pi x) sin(3 pi y) plus seeded noise of amplitude 1e-3.
+* ``wavy_stretched``      -- x = xi + 0.1 sin(2 pi xi) sin(2 pi eta),
+  y = (e^{beta eta} - 1)/(e^beta - 1) with a 64:1 first-cell aspect ratio,
+  Dirichlet x sides, Neumann y sides, rhs = J f with f a seeded sum of 16
+  Fourier modes (J-weighted mean removed).
+* ``skew_stretched``      -- shear x = xi + tan(angle) y over a wall-layer
+  stretched y, nonuniform Dirichlet data from u = e^x cos(4 pi y).
+* ``terrain_neumann``     -- the reference's own solver test problem
+  (src/tests/test.f90:2336-2583): terrain map, 117-mode cosine solution, all
+  Neumann BCs from the operator's boundary fluxes.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import geometry as G
+from .types import (BCMODE_NONUNIFORM, BCMODE_UNIFORM, BCTYPE_DIRI, BCTYPE_NEUM, BD_CELL, BD_NODE, BdryData, Box,
+                    BoxData)
+
+
+def identity_dirichlet(n: int = 128, seed: int = 1):
+    v = Box.of_size(n, n)
+    fmap = G.map_identity()
+    geo = G.mapped_geometry(v, fmap)
+    X, Y = G.positions(v, fmap)
+    rng = np.random.default_rng(seed)
+    u = np.sin(2 * math.pi * X) * np.sin(3 * math.pi * Y)
+    f = -13.0 * math.pi ** 2 * u + rng.uniform(-1e-3, 1e-3, size=u.shape)
+    rhs = BoxData(v)
+    rhs.interior()[:] = f * geo.J.interior()
+    bc = BdryData.uniform(v, [BCTYPE_DIRI] * 4)
+    return v, geo, rhs, bc, u
+
+
+def fourier_rhs(v, geo, fmap, seed, modes=16, kmax=8):
+    X, Y = G.positions(v, fmap)
+    rng = np.random.default_rng(seed)
+    a = rng.uniform(-1, 1, modes)
+    m = rng.integers(1, kmax + 1, modes)
+    nn = rng.integers(1, kmax + 1, modes)
+    f = np.zeros_like(X)
+    for k in range(modes):
+        f += a[k] * np.cos(math.pi * m[k] * X) * np.cos(math.pi * nn[k] * Y)
+    J = geo.J.interior()
+    f -= (f * J).sum() / J.sum()
+    rhs = BoxData(v)
+    rhs.interior()[:] = J * f
+    return rhs
+
+
+def wavy_stretched(n: int = 1024, seed: int = 2, aspect: float = 64.0):
+    v = Box.of_size(n, n)
+    fmap = G.map_wavy_exp(0.1, aspect)
+    geo = G.mapped_geometry(v, fmap)
+    rhs = fourier_rhs(v, geo, fmap, seed)
+    bc = BdryData.uniform(v, [BCTYPE_DIRI, BCTYPE_DIRI, BCTYPE_NEUM, BCTYPE_NEUM])
+    return v, geo, rhs, bc, None
+
+
+def skew_stretched(n: int = 256, angle: float = 30.0, ratio: float = 1.05, layer: float = 96 / 4096,
+                   n_ref: int = 4096, nx: int = None):
+    nx = nx or n
+    v = Box.of_size(nx, n)
+    fmap = G.map_skew_stretch(angle, ratio, layer, n_ref)
+    geo = G.mapped_geometry(v, fmap)
+    X, Y = G.positions(v, fmap)
+    u = np.exp(X) * np.cos(4 * math.pi * Y)
+    rhs = BoxData(v)
+    rhs.interior()[:] = geo.J.interior() * (1.0 - 16 * math.pi ** 2) * u
+    # Dirichlet data at the boundary face centres
+    Xf, Yf = G.positions(v, fmap, BD_NODE, BD_CELL)
+    Xg, Yg = G.positions(v, fmap, BD_CELL, BD_NODE)
+    ue = lambda x, y: np.exp(x) * np.cos(4 * math.pi * y)
+    data = [ue(Xf[0], Yf[0]), ue(Xf[-1], Yf[-1]), ue(Xg[:, 0], Yg[:, 0]), ue(Xg[:, -1], Yg[:, -1])]
+    bc = BdryData(v, [BCTYPE_DIRI] * 4, [BCMODE_NONUNIFORM] * 4, data)
+    return v, geo, rhs, bc, u
+
+
+def terrain_solution(X, Y, L=1.0, H=1.0):
+    s = np.zeros_like(X)
+    for i in range(8, 241, 2):
+        s += np.cos(i * math.pi * X / L) * np.cos(i * math.pi * Y / H) / i
+    return s
+
+
+def terrain_neumann(n: int, boundary_fluxes, compute_laplacian):
+    """The problem of test_solver (test.f90:2336-2470).  ``boundary_fluxes`` and
+    ``compute_laplacian`` are the operator routines used to build the Neumann
+    data and the rhs (the reference uses its own compute_grad and
+    compute_laplacian there)."""
+    v = Box.of_size(n, n)
+    geo = G.terrain_geometry(v)
+    X, Y = G.terrain_positions(v, BD_CELL, BD_CELL, 1)
+    soln = BoxData(v, 1, 1)
+    soln.data[:] = terrain_solution(X, Y)
+    fl = boundary_fluxes(soln, geo)
+    bc = BdryData(v, [BCTYPE_NEUM] * 4, [BCMODE_NONUNIFORM] * 4, fl)
+    rhs = BoxData(v)
+    compute_laplacian(rhs, soln.copy(), geo, bc, False)
+    return v, geo, rhs, bc, soln

@@ -1,0 +1,294 @@
+"""CUDA library vs the CPU oracle on the same seeded inputs.
+
+Operator-level results must be bit-identical: both sides evaluate each cell
+with the same FP64 operations in the same order (no FMA contraction on either
+side).  Solves are compared against the oracle run in the device's colour
+order (tight tolerance: only reduction order differs) and against the oracle
+run in the reference's lexicographic order (converged-solution tolerance).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from helpers import BC_CASES, hierarchy_geo, rand_bc, rand_field, rand_geo, same
+from mgpoisson2d_b200.types import (BCMODE_LAH, BCMODE_UNIFORM, BCTYPE_DIRI, BCTYPE_EXTRAP0, BCTYPE_EXTRAP1,
+                                    BCTYPE_EXTRAP2, BCTYPE_NEUM, BCTYPE_NONE, BD_CELL, BD_NODE, KIND_DD, KIND_MG,
+                                    BdryData, Box, BoxData)
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def M():
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    import mgpoisson2d_b200.api as api
+    return api
+
+
+SIZES = [(16, 12), (9, 7), (24, 24)]
+
+
+def _problem(case, nx, ny, seed):
+    rng = np.random.default_rng(seed)
+    v = Box.of_size(nx, ny)
+    types, modes = BC_CASES[case]
+    if case in ("NNNN-NU",) and ny > nx:
+        pytest.skip("north Neumann data is read at index jhi, which needs ny <= nx")
+    return v, rand_geo(v, rng), rand_field(v, rng), rand_bc(v, types, modes, rng), rng
+
+
+@pytest.mark.parametrize("case", list(BC_CASES))
+@pytest.mark.parametrize("nx,ny", SIZES)
+@pytest.mark.parametrize("homog", [False, True])
+def test_laplacian_bitexact(M, case, nx, ny, homog):
+    v, geo, phi, bc, rng = _problem(case, nx, ny, 11)
+    lap_o, lap_d = BoxData(v), BoxData(v)
+    phi_o, phi_d = phi.copy(), phi.copy()
+    O.compute_laplacian(lap_o, phi_o, geo, bc, homog)
+    M.compute_laplacian(lap_d, phi_d, geo, bc, homog)
+    assert same(lap_o.data, lap_d.data)
+    assert same(phi_o.data, phi_d.data)   # ghost state after the call
+
+
+@pytest.mark.parametrize("case", ["DDDD-U", "NNNN-NU", "DNND-mixed"])
+@pytest.mark.parametrize("jscale", [False, True])
+def test_residual_bitexact(M, case, jscale):
+    v, geo, phi, bc, rng = _problem(case, 16, 12, 12)
+    rhs = rand_field(v, rng, 0)
+    r_o, r_d = BoxData(v), BoxData(v)
+    O.compute_residual(r_o, rhs, phi.copy(), geo, bc, False, jscale)
+    M.compute_residual(r_d, rhs, phi.copy(), geo, bc, False, jscale)
+    assert same(r_o.data, r_d.data)
+
+
+@pytest.mark.parametrize("case", list(BC_CASES))
+@pytest.mark.parametrize("coupled", [0, 1])
+def test_invdiags_bitexact(M, case, coupled):
+    import ctypes
+    v, geo, phi, bc, rng = _problem(case, 16, 12, 13)
+    O.lib().or_set_dirichlet_coupled_diagonal.argtypes = [ctypes.c_int]
+    O.lib().or_set_dirichlet_coupled_diagonal(coupled)
+    old = M.set_flags(coupled)
+    try:
+        d_o, d_d = BoxData(v), BoxData(v)
+        O.compute_invdiags(d_o, geo, bc, True)
+        M.compute_invdiags(d_d, geo, bc, True)
+        assert same(d_o.data, d_d.data)
+    finally:
+        M.set_flags(old)
+        O.lib().or_set_dirichlet_coupled_diagonal(0)
+
+
+FILL_TYPES = [
+    ([BCTYPE_DIRI] * 4, [BCMODE_UNIFORM] * 4),
+    ([BCTYPE_NEUM] * 4, [BCMODE_UNIFORM] * 4),
+    ([BCTYPE_NEUM] * 4, [1] * 4),
+    ([BCTYPE_NEUM, BCTYPE_DIRI, BCTYPE_NEUM, BCTYPE_DIRI], [1, 0, 0, 1]),
+    ([BCTYPE_DIRI, BCTYPE_NEUM, BCTYPE_DIRI, BCTYPE_NEUM], [BCMODE_LAH] * 4),
+    ([BCTYPE_EXTRAP0, BCTYPE_EXTRAP1, BCTYPE_EXTRAP2, BCTYPE_NONE], [0] * 4),
+    ([2, 2, BCTYPE_DIRI, BCTYPE_NEUM], [0, 0, 1, 0]),
+    ([BCTYPE_NEUM, BCTYPE_DIRI, 2, 2], [0, 1, 0, 0]),
+]
+
+
+@pytest.mark.parametrize("k", range(len(FILL_TYPES)))
+@pytest.mark.parametrize("homog", [False, True])
+@pytest.mark.parametrize("do_neum", [False, True])
+def test_fill_ghosts_bitexact(M, k, homog, do_neum):
+    types, modes = FILL_TYPES[k]
+    rng = np.random.default_rng(100 + k)
+    v = Box.of_size(12, 10)
+    geo = rand_geo(v, rng)
+    phi = rand_field(v, rng)
+    bc = rand_bc(v, types, modes, rng)
+    a, b = phi.copy(), phi.copy()
+    O.fill_ghosts(a, bc, geo, homog, do_neum)
+    M.fill_ghosts(b, bc, geo, homog, do_neum)
+    assert same(a.data, b.data)
+
+
+@pytest.mark.parametrize("order", range(4))
+def test_extrapolate_ghosts_bitexact(M, order):
+    rng = np.random.default_rng(5)
+    v = Box.of_size(10, 9)
+    phi = rand_field(v, rng)
+    a, b = phi.copy(), phi.copy()
+    O.extrapolate_ghosts(a, order)
+    M.extrapolate_ghosts(b, order)
+    assert same(a.data, b.data)
+
+
+@pytest.mark.parametrize("case", ["DDDD-U", "NNNN-NU", "DNND-mixed", "PPDD"])
+@pytest.mark.parametrize("omega", [1.0, 2.0 / 3.0])
+def test_relax_gs_colour_bitexact(M, case, omega):
+    v, geo, phi, bc, rng = _problem(case, 16, 12, 14)
+    rhs = rand_field(v, rng, 0)
+    inv = BoxData(v)
+    O.compute_invdiags(inv, geo, bc, True)
+    a, b = phi.copy(), phi.copy()
+    O.relax_gs(a, rhs, geo, bc, True, inv, omega, -1.0, 3, False, 0, gs_order=1)
+    M.relax_gs(b, rhs, geo, bc, True, inv, omega, -1.0, 3, False, 0)
+    assert same(a.data, b.data)
+
+
+@pytest.mark.parametrize("offi,offj", [(1, 1), (0, 1), (1, 0), (0, 0)])
+@pytest.mark.parametrize("ref", [(2, 2), (2, 1), (1, 2)])
+def test_restrict_bitexact(M, offi, offj, ref):
+    rng = np.random.default_rng(7)
+    v = Box.of_size(16, 12)
+    c = v.coarsened(*ref)
+    f = rand_field(v, rng, 0, offi, offj)
+    a, b = BoxData(c, 0, 0, offi, offj), BoxData(c, 0, 0, offi, offj)
+    O.restrict(f, a)
+    M.restrict(f, b)
+    assert same(a.data, b.data)
+
+
+@pytest.mark.parametrize("order", [0, 1, 2])
+@pytest.mark.parametrize("ref", [(2, 2), (2, 1), (1, 2)])
+@pytest.mark.parametrize("types", [[BCTYPE_DIRI] * 4, [BCTYPE_DIRI, BCTYPE_DIRI, BCTYPE_NEUM, BCTYPE_NEUM]])
+def test_prolong_bitexact(M, order, ref, types):
+    rng = np.random.default_rng(8)
+    v = Box.of_size(16, 12)
+    geo = rand_geo(v, rng)
+    c = v.coarsened(*ref)
+    cgeo = rand_geo(c, rng)
+    fine = rand_field(v, rng)
+    crse = rand_field(c, rng)
+    cbc = BdryData.uniform(c, types)
+    fa, fb, ca, cb = fine.copy(), fine.copy(), crse.copy(), crse.copy()
+    O.prolong(fa, ca, geo, cgeo, cbc, order)
+    M.prolong(fb, cb, geo, cgeo, cbc, order)
+    assert same(fa.data, fb.data)
+    assert same(ca.data, cb.data)
+
+
+def test_prolong_remove_mean(M):
+    """All-Neumann coarse BCs remove the J-weighted mean (MG:371-383); the
+    mean is a reduction, so equality is to rounding."""
+    rng = np.random.default_rng(9)
+    v = Box.of_size(16, 16)
+    geo = rand_geo(v, rng)
+    c, cgeo = hierarchy_geo(v, geo, O.restrict)
+    fine, crse = rand_field(v, rng), rand_field(c, rng)
+    cbc = BdryData.uniform(c, [BCTYPE_NEUM] * 4)
+    fa, fb = fine.copy(), fine.copy()
+    O.prolong(fa, crse.copy(), geo, cgeo, cbc, 1)
+    M.prolong(fb, crse.copy(), geo, cgeo, cbc, 1)
+    np.testing.assert_allclose(fb.interior(), fa.interior(), rtol=0, atol=1e-13)
+
+
+def test_norms(M):
+    rng = np.random.default_rng(10)
+    v = Box.of_size(33, 17)
+    a, b = rand_field(v, rng, 0), rand_field(v, rng, 0)
+    for p in (0, 1, 2):
+        np.testing.assert_allclose(M.pnorm(a, p), O.pnorm(a, p), rtol=1e-13)
+    np.testing.assert_allclose(M.inner_prod(a, b), O.inner_prod(a, b), rtol=1e-12)
+
+
+def test_bicgstab(M):
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, u = W.identity_dirichlet(8)
+    inv = BoxData(v)
+    O.compute_invdiags(inv, geo, bc, True)
+    a, b = BoxData(v, 1, 1), BoxData(v, 1, 1)
+    O.solve_bicgstab2(a, rhs, geo, bc, True, inv, 1e-10, 80, 5, False, 0, gs_order=1)
+    M.solve_bicgstab2(b, rhs, geo, bc, True, inv, 1e-10, 80, 5, False, 0)
+    np.testing.assert_allclose(b.interior(), a.interior(), rtol=1e-9, atol=1e-12)
+
+
+# ---------------------------------------------------------------------------
+# Solves
+# ---------------------------------------------------------------------------
+def _set_coupled(M, on):
+    import ctypes
+    O.lib().or_set_dirichlet_coupled_diagonal.argtypes = [ctypes.c_int]
+    O.lib().or_set_dirichlet_coupled_diagonal(int(on))
+    return M.set_flags(int(on))
+
+
+@pytest.mark.parametrize("n", [32, 64])
+def test_vcycle_matches_oracle(M, n):
+    from mgpoisson2d_b200 import workloads as W
+    old = _set_coupled(M, True)
+    try:
+        v, geo, rhs, bc, u = W.identity_dirichlet(n)
+        pa, pb, pc = BoxData(v, 1, 1), BoxData(v, 1, 1), BoxData(v, 1, 1)
+        ra = O.vcycle(pa, rhs, geo, bc, True, 1e-10, 30, gs_order=1)
+        rb = M.vcycle(pb, rhs, geo, bc, True, 1e-10, 30)
+        rc = O.vcycle(pc, rhs, geo, bc, True, 1e-10, 30, gs_order=0)
+    finally:
+        _set_coupled(M, old)
+    assert rb.iterations == ra.iterations
+    np.testing.assert_allclose(rb.relres, ra.relres, rtol=1e-7, atol=1e-14)
+    np.testing.assert_allclose(pb.interior(), pa.interior(), rtol=0, atol=1e-11 * np.abs(pa.interior()).max())
+    # against the reference's lexicographic order: same converged solution
+    assert rb.relres[-1] <= 1e-10 and rc.relres[-1] <= 1e-10
+    err = pb.interior() - pc.interior()
+    assert np.linalg.norm(err) / np.linalg.norm(pc.interior()) < 1e-8
+    assert np.abs(err).max() / np.abs(pc.interior()).max() < 1e-7
+
+
+def test_vcycle_reference_diverges_like_oracle(M):
+    """With the reference's own diagonal the V-cycle diverges on a Dirichlet
+    problem and stops after undoing the correction (MG:630-639); both sides
+    must take that same path."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, u = W.identity_dirichlet(32)
+    pa, pb = BoxData(v, 1, 1), BoxData(v, 1, 1)
+    ra = O.vcycle(pa, rhs, geo, bc, True, 1e-10, 20, gs_order=1)
+    rb = M.vcycle(pb, rhs, geo, bc, True, 1e-10, 20)
+    assert ra.diverged and rb.diverged and ra.iterations == rb.iterations == 1
+    np.testing.assert_allclose(rb.relres, ra.relres, rtol=1e-9)
+
+
+def test_fmg_terrain_neumann(M):
+    """The reference's solver test: FMG on the terrain map with all-Neumann data."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, soln = W.terrain_neumann(64, O.boundary_fluxes, O.compute_laplacian)
+    pa, pb = BoxData(v, 1, 1), BoxData(v, 1, 1)
+    ra = O.fmg(pa, rhs, geo, bc, False, 1e-30, 3, gs_order=1)
+    rb = M.fmg(pb, rhs, geo, bc, False, 1e-30, 3)
+    np.testing.assert_allclose(rb.relres, ra.relres, rtol=1e-6)
+    np.testing.assert_allclose(pb.interior(), pa.interior(), rtol=0, atol=1e-10 * np.abs(pa.interior()).max())
+
+
+def test_dc_vcycle(M):
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, u = W.identity_dirichlet(64)
+    f = rhs.copy()
+    f.interior()[:] /= geo.J.interior()
+    fa, fb = f.copy(), f.copy()
+    pa, pb = BoxData(v, 1, 1), BoxData(v, 1, 1)
+    ra = O.dc_vcycle(pa, fa, geo, bc, True, 1e-10, 60, smooth_down=8, smooth_up=8, smooth_bottom=8, gs_order=1)
+    rb = M.dc_vcycle(pb, fb, geo, bc, True, 1e-10, 60, smooth_down=8, smooth_up=8, smooth_bottom=8)
+    assert rb.iterations == ra.iterations
+    np.testing.assert_allclose(rb.relres, ra.relres, rtol=1e-6, atol=1e-14)
+    np.testing.assert_allclose(pb.interior(), pa.interior(), rtol=0, atol=1e-10 * np.abs(pa.interior()).max())
+    assert same(fa.data, fb.data)   # rhs*J/J written back exactly like the reference
+
+
+def test_resident_solver_equals_oneshot_and_device_arrays(M):
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, u = W.wavy_stretched(64)
+    old = M.set_flags(M.FLAG_DIRICHLET_COUPLED_DIAG)
+    try:
+        pa = BoxData(v, 1, 1)
+        ra = M.vcycle(pa, rhs, geo, bc, True, 1e-10, 15)
+    finally:
+        M.set_flags(old)
+    with M.Solver(v, geo, bc, KIND_MG, M.FLAG_DIRICHLET_COUPLED_DIAG) as s:
+        for _ in range(2):   # a second solve on the same hierarchy gives the same bits
+            pb = BoxData(v, 1, 1)
+            rb = s.vcycle(pb, rhs, bc, True, 1e-10, 15)
+            assert same(pa.data, pb.data) and np.array_equal(ra.relres, rb.relres)
+        pd, rd_ = BoxData(v, 1, 1).to_device(), rhs.to_device()
+        rd = s.vcycle(pd, rd_, bc, True, 1e-10, 15)
+        assert same(pa.data, pd.to_host().data) and np.array_equal(ra.relres, rd.relres)
