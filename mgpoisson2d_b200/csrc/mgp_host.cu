@@ -290,6 +290,7 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
     RC(check_box(valid));
     if (valid->ilo < 0 || valid->jlo < 0 || (valid->ilo % 2) || (valid->jlo % 2))
         return set_err(MGP_EINVAL, "solver: ilo and jlo must be even and non-negative");
+    if (valid->nx < 4 || valid->ny < 4) return set_err(MGP_EINVAL, "solver: at least 4 cells per direction");
     if (!geo || !bc) return set_err(MGP_EINVAL, "null geometry or bdry_data");
     RC(check_array(&geo->J, valid->nx, "J"));
     RC(check_array(&geo->Jgup_xx, valid->nx + 1, "Jgup_xx"));
@@ -306,6 +307,7 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
     int md = maxdepth_user < 0 ? 1000 : maxdepth_user;
     estimate_maxdepth(&md, valid);
     create_mgschedule(s->refx, s->refy, &md, valid);
+    if (md >= 32) return set_err(MGP_EINVAL, "multigrid depth %d exceeds 31", md);
     s->maxdepth = md;
     s->lv.assign(md + 1, Lv{});
     // level boxes (coarsen_box, AU:154-170)
@@ -874,6 +876,8 @@ int mgp_relax_gs(const mgp_box* valid, mgp_array* phi, const mgp_array* rhs, con
     RC(check_array(phi, valid->nx, "phi"));
     RC(ghost_cap(phi));
     if (maxiters == 0) return MGP_OK;
+    if (valid->nx < 4 || valid->ny < 4)
+        return set_err(MGP_EINVAL, "relax_gs: the device sweep needs at least 4 cells per direction");
     const int nx = valid->nx, ny = valid->ny;
     OpCtx c;
     DF p, f, d, r;
@@ -922,6 +926,8 @@ int mgp_solve_bicgstab2(const mgp_box* valid, mgp_array* phi, const mgp_array* r
     RC(no_lah(bc));
     RC(check_array(phi, valid->nx, "phi"));
     RC(ghost_cap(phi));
+    if (valid->nx < 4 || valid->ny < 4)
+        return set_err(MGP_EINVAL, "solve_bicgstab2: the device sweep needs at least 4 cells per direction");
     const int nx = valid->nx, ny = valid->ny;
     OpCtx c;
     BicgArgs a;

@@ -126,14 +126,63 @@ cudaError_t launch_apply(const DF& out, const DF& phi, const DF& rhs, const Geo&
 }
 
 // ---------------------------------------------------------------------------
-// Gauss-Seidel (relax_gs, P2:1460-1988), one colour per launch
+// Gauss-Seidel (relax_gs, P2:1460-1988) in the device order:
+//   1. ghosts once (P2:1556);
+//   2. colours (i mod 2, j mod 2) = (0,0),(1,1),(1,0),(0,1) over the interior
+//      cells -- their stencil reaches one cell, so each colour is an
+//      independent set (one launch per colour);
+//   3. the boundary cells, whose stencil reaches two cells inward (the
+//      quadratic extrapolation, P2:947-951): the edge cells colour by colour,
+//      then the four corners in turn (one CTA).
+// No cell of a sub-pass reads another cell of the same sub-pass.
 // ---------------------------------------------------------------------------
 __global__ void k_gs_colour(DF phi, DF rhs, DF invd, Geo g, BCd b, int homog, int nx, int ny, double omega,
                             int ci, int cj) {
     const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ci;
     const int j = 2 * (blockIdx.y * blockDim.y + threadIdx.y) + cj;
     if (i >= nx || j >= ny) return;
+    const Per pr = periodic_of(b);
+    if (region(i, nx, pr.xl, pr.xh) != RMID || region(j, ny, pr.yl, pr.yh) != RMID) return;
     gs9(phi, rhs, invd, g, b, homog, nx, ny, i, j, omega);
+}
+
+// Perimeter cell k (0 <= k < 2nx + 2(ny-2)): rows j = 0 and ny-1, then columns i = 0 and nx-1.
+__device__ __forceinline__ void perimeter_cell(int k, int nx, int ny, int& i, int& j) {
+    if (k < nx) { i = k; j = 0; }
+    else if (k < 2 * nx) { i = k - nx; j = ny - 1; }
+    else if (k < 2 * nx + ny - 2) { i = 0; j = 1 + k - 2 * nx; }
+    else { i = nx - 1; j = 1 + k - 2 * nx - (ny - 2); }
+}
+
+// Step 3 of the sweep; every thread of the block calls it.
+__device__ void b_gs_boundary(const DF& phi, const DF& rhs, const DF& invd, const Geo& g, const BCd& b, int homog,
+                              int nx, int ny, double omega) {
+    const Per pr = periodic_of(b);
+    const int np = 2 * nx + 2 * (ny - 2);
+    for (int c = 0; c < 4; ++c) {
+        const int ci = colour_ci(c), cj = colour_cj(c);
+        for (int k = threadIdx.x; k < np; k += blockDim.x) {
+            int i, j;
+            perimeter_cell(k, nx, ny, i, j);
+            if ((i & 1) != ci || (j & 1) != cj) continue;
+            const bool xm = region(i, nx, pr.xl, pr.xh) == RMID, ym = region(j, ny, pr.yl, pr.yh) == RMID;
+            if (xm != ym) gs9(phi, rhs, invd, g, b, homog, nx, ny, i, j, omega);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < 4; ++c) {
+            const int i = (c & 1) ? nx - 1 : 0, j = (c & 2) ? ny - 1 : 0;
+            if (region(i, nx, pr.xl, pr.xh) != RMID && region(j, ny, pr.yl, pr.yh) != RMID)
+                gs9(phi, rhs, invd, g, b, homog, nx, ny, i, j, omega);
+        }
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(1024) k_gs_boundary(DF phi, DF rhs, DF invd, Geo g, BCd b, int homog, int nx,
+                                                      int ny, double omega) {
+    b_gs_boundary(phi, rhs, invd, g, b, homog, nx, ny, omega);
 }
 
 cudaError_t launch_gs_sweep(const DF& phi, const DF& rhs, const DF& invd, const Geo& g, const BCd& b, int homog,
@@ -144,7 +193,14 @@ cudaError_t launch_gs_sweep(const DF& phi, const DF& rhs, const DF& invd, const 
     static const int ci[4] = {0, 1, 1, 0}, cj[4] = {0, 1, 0, 1};
     for (int c = 0; c < 4; ++c)
         k_gs_colour<<<grd, kBlk2, 0, st>>>(phi, rhs, invd, g, b, homog, nx, ny, omega, ci[c], cj[c]);
-    count_launch(4);
+    const Per pr = {b.type[S_XLO] == T_PERIODIC, b.type[S_XHI] == T_PERIODIC, b.type[S_YLO] == T_PERIODIC,
+                    b.type[S_YHI] == T_PERIODIC};
+    int n = 4;
+    if (!(pr.xl && pr.xh && pr.yl && pr.yh)) {
+        k_gs_boundary<<<1, 1024, 0, st>>>(phi, rhs, invd, g, b, homog, nx, ny, omega);
+        n = 5;
+    }
+    count_launch(n);
     return cudaGetLastError();
 }
 
@@ -595,16 +651,19 @@ __device__ void b_mul(const DF& out, const DF& a, const DF& c, int nx, int ny) {
 __device__ void b_relax9(const Lv& L, const DF& phi, const DF& rhs, int homog, double omega, int sweeps) {
     const int nx = L.nx, ny = L.ny;
     const int hx = (nx + 1) / 2, hy = (ny + 1) / 2;
+    const Per pr = periodic_of(L.bc);
     for (int it = 0; it < sweeps; ++it) {
         b_fill(phi, L.g, L.bc, homog, 0, nx, ny);
-        for (int c = 0; c < 4; ++c) {
+        for (int c = 0; c < 4; ++c) {   // interior cells, colour by colour
             const int ci = colour_ci(c), cj = colour_cj(c);
             BLOOP(k, hx * hy) {
                 const int i = 2 * (k % hx) + ci, j = 2 * (k / hx) + cj;
-                if (i < nx && j < ny) gs9(phi, rhs, L.invd, L.g, L.bc, homog, nx, ny, i, j, omega);
+                if (i < nx && j < ny && region(i, nx, pr.xl, pr.xh) == RMID && region(j, ny, pr.yl, pr.yh) == RMID)
+                    gs9(phi, rhs, L.invd, L.g, L.bc, homog, nx, ny, i, j, omega);
             }
             __syncthreads();
         }
+        b_gs_boundary(phi, rhs, L.invd, L.g, L.bc, homog, nx, ny, omega);
     }
 }
 
@@ -804,6 +863,7 @@ visit:
             restrict_cc(L.w, k % Cl.nx, k / Cl.nx, rx, ry, 1.0 / (rx * ry));
         __syncthreads();
         if (!a.dd) b_set_guess(Cl);   // MG:805-806
+        if (a.numcycles == 0) goto finish;   // `do curcycle = 1, numcycles` runs no coarse visit
         cnt[d] = 0;
         d = d + 1;
         goto visit;
@@ -819,6 +879,7 @@ up:
         d = d + 1;
         goto visit;
     }
+finish:
     {
         const Lv& L = a.lv[d];
         b_prolong(L, a.lv[d + 1], a.refx[d], a.refy[d], 1, sh);

@@ -724,15 +724,41 @@ static int gs_sweep(const mgp_box *valid, mgp_array *phi, const mgp_array *rhs, 
             gs_cell(P, F, D, &g, i, j, idx, idy, xregion(i, nx, px0, px1), yr, nb, omega);
         }
     } else {
-        /* device colour order: (0,0), (1,1), (1,0), (0,1) -- the cells with
-         * i+j even first, which is red-black order for 5-point couplings */
+        /* The device order.  Colours (i mod 2, j mod 2) = (0,0), (1,1), (1,0),
+         * (0,1) -- the cells with i+j even first, which is red-black order
+         * for 5-point couplings.  First the four colours over the interior
+         * cells (region MID in both directions: their stencil reaches one
+         * cell, so a colour is an independent set), then the boundary cells
+         * (whose stencil reaches two cells inward): edge cells colour by
+         * colour, then the four corners one after another. */
         static const int ci_of[4] = {0, 1, 1, 0}, cj_of[4] = {0, 1, 0, 1};
         for (c = 0; c < 4; ++c) {
             int ci = ci_of[c], cj = cj_of[c];
             for (j = cj; j < ny; j += 2) {
                 int yr = xregion(j, ny, py0, py1);
-                for (i = ci; i < nx; i += 2)
-                    gs_cell(P, F, D, &g, i, j, idx, idy, xregion(i, nx, px0, px1), yr, nb, omega);
+                if (yr != RMID) continue;
+                for (i = ci; i < nx; i += 2) {
+                    int xr = xregion(i, nx, px0, px1);
+                    if (xr == RMID) gs_cell(P, F, D, &g, i, j, idx, idy, xr, yr, nb, omega);
+                }
+            }
+        }
+        for (c = 0; c < 4; ++c) {
+            int ci = ci_of[c], cj = cj_of[c];
+            for (j = cj; j < ny; j += 2) {
+                int yr = xregion(j, ny, py0, py1);
+                for (i = ci; i < nx; i += 2) {
+                    int xr = xregion(i, nx, px0, px1);
+                    if ((xr == RMID) != (yr == RMID)) gs_cell(P, F, D, &g, i, j, idx, idy, xr, yr, nb, omega);
+                }
+            }
+        }
+        {
+            static const int cx[4] = {0, 1, 0, 1}, cy[4] = {0, 0, 1, 1};
+            for (c = 0; c < 4; ++c) {
+                int ii = cx[c] ? nx - 1 : 0, jj = cy[c] ? ny - 1 : 0;
+                int xr = xregion(ii, nx, px0, px1), yr = xregion(jj, ny, py0, py1);
+                if (xr != RMID && yr != RMID) gs_cell(P, F, D, &g, ii, jj, idx, idy, xr, yr, nb, omega);
             }
         }
     }

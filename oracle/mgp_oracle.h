@@ -20,9 +20,11 @@
  *
  * gs_order selects the Gauss-Seidel visiting order:
  *   0 = lexicographic, as the reference (P2:1560-1959, DD:288-306);
- *   1 = the device order: four colours (i mod 2, j mod 2) = (0,0),(1,1),
- *       (1,0),(0,1) for the 9-point sweep, and the reference's own red-black
- *       order (DD:262-285) for the deferred-correction 5-point sweep.
+ *   1 = the device order: for the 9-point sweep, four colours (i mod 2,
+ *       j mod 2) = (0,0),(1,1),(1,0),(0,1) over the interior cells, then the
+ *       boundary cells (edges colour by colour, then the corners); for the
+ *       deferred-correction 5-point sweep, the reference's own red-black
+ *       order (DD:262-285).
  */
 #ifndef MGP_ORACLE_H
 #define MGP_ORACLE_H
