@@ -1,0 +1,55 @@
+"""A short, fixed run of the benchmark workload for profilers:
+
+    python -m mgpoisson2d_b200.profile [--n 1024] [--vcycles 2] [--warmup 1]
+
+Builds the resident solver for the 1024x1024 stretched mapped grid (the bench
+workload), runs `warmup` solves capped at `vcycles` V-cycles, then one more,
+and prints the device time per V-cycle.  Under ncu, the kernels of the last
+solve follow those of the warm-up solves in launch order.
+"""
+from __future__ import annotations
+
+import argparse
+import time
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--n", type=int, default=1024)
+    p.add_argument("--vcycles", type=int, default=2)
+    p.add_argument("--warmup", type=int, default=1)
+    p.add_argument("--dd", action="store_true", help="deferred-correction driver")
+    a = p.parse_args()
+
+    import torch
+
+    import mgpoisson2d_b200.api as M
+    from mgpoisson2d_b200 import workloads as W
+    from mgpoisson2d_b200.types import BoxData
+
+    torch.cuda.set_device(0)
+    v, geo, rhs, bc, _ = W.wavy_stretched(a.n)
+    kind = M.KIND_DD if a.dd else M.KIND_MG
+    s = M.Solver(v, geo, bc, kind, M.FLAG_DIRICHLET_COUPLED_DIAG)
+    phi, f = BoxData(v, 1, 1).to_device(), rhs.to_device()
+    if a.dd:
+        f.data /= geo.J.to_device().data[1:-1, 1:-1]
+    run = (lambda: s.dc_vcycle(phi, f, bc, True, 1e-10, a.vcycles, 1, 8, 8, 8)) if a.dd else \
+        (lambda: s.vcycle(phi, f, bc, True, 1e-10, a.vcycles, 1, 8, 8, 8))
+    for _ in range(a.warmup):
+        phi.data.zero_()
+        run()
+    phi.data.zero_()
+    torch.cuda.synchronize()
+    l0 = M.kernel_launch_count()
+    t0 = time.perf_counter()
+    rep = run()
+    dt = time.perf_counter() - t0
+    print(f"n={a.n} vcycles={rep.iterations} device {rep.seconds * 1e3:.3f} ms "
+          f"({rep.seconds / max(rep.iterations, 1) * 1e3:.3f} ms/V-cycle), wall {dt * 1e3:.3f} ms, "
+          f"{M.kernel_launch_count() - l0} launches, relres {rep.relres[-1]:.3e}")
+    s.close()
+
+
+if __name__ == "__main__":
+    main()
