@@ -47,6 +47,7 @@ struct Lv {
     Geo g;
     BCd bc;
     DF e;      // correction, 1 ghost layer
+    DF e2;     // second buffer of e for the two-buffer sweep (grid-path levels)
     DF r;      // right-hand side of the residual equation
     DF w;      // work (residual before restriction)
     DF invd;   // inverse diagonal
@@ -54,6 +55,14 @@ struct Lv {
     DF pt, st;
     DF rr, rt, pp, tt, vv;   // bottom solver, no ghosts
 };
+
+// Asynchronous 8-byte global -> shared copy (cp.async, sm_80+): the thread does
+// not wait for the load, so a loop of them keeps many loads in flight.
+__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gsrc) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 __device__ __forceinline__ int region(int i, int n, bool per_lo, bool per_hi) {
     if (i == 0 && !per_lo) return RLO;
@@ -171,19 +180,38 @@ __device__ __forceinline__ double nbval(const BCd& b, int homog, int s, int k) {
     return b.d[s][k];
 }
 
+// The metric values the operator reads at one cell: its four faces.
+struct Faces {
+    double xxe, xxw, xye, xyw;   // Jgup_xx, Jgup_xy at x-faces i+1 (east) and i (west)
+    double yyn, yys, yxn, yxs;   // Jgup_yy, Jgup_yx at y-faces j+1 (north) and j (south)
+};
+
+__device__ __forceinline__ Faces faces_of(const Geo& g, int i, int j) {
+    Faces f;
+    f.xxe = AT(g.xx, i + 1, j); f.xxw = AT(g.xx, i, j);
+    f.xye = AT(g.xy, i + 1, j); f.xyw = AT(g.xy, i, j);
+    f.yyn = AT(g.yy, i, j + 1); f.yys = AT(g.yy, i, j);
+    f.yxn = AT(g.yx, i, j + 1); f.yxs = AT(g.yx, i, j);
+    return f;
+}
+
 // (xfe - xfw)/dx + (yfn - yfs)/dy with Neumann faces replaced by the BC flux.
-__device__ __forceinline__ double lap9(const St9& s, const Geo& g, int i, int j, int xr, int yr,
-                                       const BCd& b, int homog) {
-    const double idx = g.idx, idy = g.idy;
-    double xfe = AT(g.xx, i + 1, j) * (s.pe - s.p) * idx + AT(g.xy, i + 1, j) * 0.25 * (s.ene - s.ese + s.en - s.es) * idy;
-    double xfw = AT(g.xx, i, j) * (s.p - s.pw) * idx + AT(g.xy, i, j) * 0.25 * (s.en - s.es + s.enw - s.esw) * idy;
-    double yfn = AT(g.yy, i, j + 1) * (s.pn - s.p) * idy + AT(g.yx, i, j + 1) * 0.25 * (s.ene - s.enw + s.ee - s.ew) * idx;
-    double yfs = AT(g.yy, i, j) * (s.p - s.ps) * idy + AT(g.yx, i, j) * 0.25 * (s.ee - s.ew + s.ese - s.esw) * idx;
+__device__ __forceinline__ double lap9f(const St9& s, const Faces& f, double idx, double idy, int i, int j, int xr,
+                                        int yr, const BCd& b, int homog) {
+    double xfe = f.xxe * (s.pe - s.p) * idx + f.xye * 0.25 * (s.ene - s.ese + s.en - s.es) * idy;
+    double xfw = f.xxw * (s.p - s.pw) * idx + f.xyw * 0.25 * (s.en - s.es + s.enw - s.esw) * idy;
+    double yfn = f.yyn * (s.pn - s.p) * idy + f.yxn * 0.25 * (s.ene - s.enw + s.ee - s.ew) * idx;
+    double yfs = f.yys * (s.p - s.ps) * idy + f.yxs * 0.25 * (s.ee - s.ew + s.ese - s.esw) * idx;
     if (xr == RLO && b.type[S_XLO] == T_NEUM) xfw = nbval(b, homog, S_XLO, j);
     if (yr == RLO && b.type[S_YLO] == T_NEUM) yfs = nbval(b, homog, S_YLO, i);
     if (xr == RHI && b.type[S_XHI] == T_NEUM) xfe = nbval(b, homog, S_XHI, j);
     if (yr == RHI && b.type[S_YHI] == T_NEUM) yfn = nbval(b, homog, S_YHI, b.kyhi);
     return (xfe - xfw) * idx + (yfn - yfs) * idy;
+}
+
+__device__ __forceinline__ double lap9(const St9& s, const Geo& g, int i, int j, int xr, int yr,
+                                       const BCd& b, int homog) {
+    return lap9f(s, faces_of(g, i, j), g.idx, g.idy, i, j, xr, yr, b, homog);
 }
 
 struct Per {

@@ -48,7 +48,7 @@ int set_err(int code, const char* fmt, ...) {
     } while (0)
 
 // Levels with at most this many cells run inside the single-CTA coarse cycle.
-constexpr long kCoarseCells = 4096;
+constexpr long kCoarseCells = 1024;
 
 // ---------------------------------------------------------------------------
 // Device memory: every field of a solver comes out of one allocation.
@@ -244,6 +244,8 @@ struct mgp_solver {
     std::vector<int> refx, refy;
     std::vector<Lv> lv;
     Lv* d_lv = nullptr;
+    Lv* d_shadow = nullptr; // coarse levels' shared-memory layout (offsets), or nullptr
+    int shadow_bytes = 0;
     int* d_ref = nullptr;   // refx then refy
     int* d_status = nullptr;
     Arena fixed;            // geometry, inverse diagonals
@@ -267,6 +269,7 @@ constexpr int kRedSlots = 2 * 296 + 8;
 void solver_free(mgp_solver* s) {
     if (!s) return;
     if (s->d_lv) cudaFree(s->d_lv);
+    if (s->d_shadow) cudaFree(s->d_shadow);
     if (s->d_ref) cudaFree(s->d_ref);
     if (s->d_status) cudaFree(s->d_status);
     if (s->d_bcbuf) cudaFree(s->d_bcbuf);
@@ -334,6 +337,7 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
         s->fixed.add(&L.g.yy, nx, ny + 1, 0);
         s->fixed.add(&L.invd, nx, ny, 0);
         s->state.add(&L.e, nx, ny, 1);
+        if (d < s->dc) s->state.add(&L.e2, nx, ny, 1);
         s->state.add(&L.r, nx, ny, 0);
         s->state.add(&L.w, nx, ny, 0);
         if (d == md) {
@@ -394,6 +398,47 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
         else CK(launch_invdiag(L.invd, L.g, L.bc, 1, L.nx, L.ny, (s->flags & MGP_FLAG_DIRICHLET_COUPLED_DIAG) ? 1 : 0,
                                st));                                                      // P2:16-388
     }
+    // shared-memory layout of the coarse levels for k_coarse_cycle_smem
+    {
+        std::vector<Lv> sh(s->lv);
+        size_t off = 0;
+        auto place = [&](DF& f, int nxv, int nyv, int g) {
+            f.ld = nxv + 2 * g;
+            f.p = (double*)(uintptr_t)(off + (size_t)g * f.ld + g);
+            off += (size_t)f.ld * (nyv + 2 * g);
+        };
+        for (int d = s->dc; d <= md; ++d) {
+            Lv& L = sh[d];
+            place(L.e, L.nx, L.ny, 1);
+            place(L.r, L.nx, L.ny, 0);
+            place(L.w, L.nx, L.ny, 0);
+            place(L.invd, L.nx, L.ny, 0);
+            place(L.g.J, L.nx, L.ny, 0);
+            place(L.g.xx, L.nx + 1, L.ny, 0);
+            place(L.g.xy, L.nx + 1, L.ny, 0);
+            place(L.g.yx, L.nx, L.ny + 1, 0);
+            place(L.g.yy, L.nx, L.ny + 1, 0);
+            if (d == md) {
+                place(L.ea, L.nx, L.ny, 1);
+                place(L.pt, L.nx, L.ny, 1);
+                place(L.st, L.nx, L.ny, 1);
+                place(L.rr, L.nx, L.ny, 0);
+                place(L.rt, L.nx, L.ny, 0);
+                place(L.pp, L.nx, L.ny, 0);
+                place(L.tt, L.nx, L.ny, 0);
+                place(L.vv, L.nx, L.ny, 0);
+            }
+        }
+        const size_t bytes = off * sizeof(double);
+        if (md - s->dc + 1 <= kMaxCoarseLevels && bytes <= (size_t)kCoarseSmemMax) {
+            if (cudaMalloc(&s->d_shadow, sizeof(Lv) * (md + 1)) != cudaSuccess) {
+                cudaGetLastError();
+                return set_err(MGP_ENOMEM, "device allocation failed");
+            }
+            CK(cudaMemcpyAsync(s->d_shadow, sh.data(), sizeof(Lv) * (md + 1), cudaMemcpyHostToDevice, st));
+            s->shadow_bytes = (int)bytes;
+        }
+    }
     std::vector<int> ref(2 * (md + 1), 0);
     for (int d = 0; d < md; ++d) { ref[d] = s->refx[d]; ref[md + 1 + d] = s->refy[d]; }
     CK(cudaMemcpyAsync(s->d_lv, s->lv.data(), sizeof(Lv) * (md + 1), cudaMemcpyHostToDevice, st));
@@ -434,6 +479,13 @@ int smooth_body(mgp_solver* s, int d, int nu) {
             CK(launch_fill(L.e, L.g, L.bc, 1, 1, L.nx, L.ny, st));   // DD:259
             CK(launch_dd_colour(L.e, L.w, L.invd, L.g, L.nx, L.ny, 4.0 / 5.0, 0, st));
             CK(launch_dd_colour(L.e, L.w, L.invd, L.g, L.nx, L.ny, 4.0 / 5.0, 1, st));
+        }
+    } else if (L.e2.p && sweep_fusable(L.bc)) {
+        for (int k = 0; k < nu; ++k) {
+            CK(launch_sweep9(L.e, L.e2, L.r, L.invd, L.g, L.bc, 1, L.nx, L.ny, 1.0, st));
+            const DF t = L.e;
+            L.e = L.e2;
+            L.e2 = t;
         }
     } else {
         for (int k = 0; k < nu; ++k) CK(launch_gs_sweep(L.e, L.r, L.invd, L.g, L.bc, 1, L.nx, L.ny, 1.0, st));
@@ -487,6 +539,8 @@ int coarse_cycle(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
     a.refx = s->d_ref;
     a.refy = s->d_ref + s->maxdepth + 1;
     a.status = s->d_status;
+    a.shadow = s->d_shadow;
+    a.smem_bytes = s->shadow_bytes;
     CK(launch_coarse_cycle(a, s->stream));
     return MGP_OK;
 }
@@ -880,10 +934,11 @@ int mgp_relax_gs(const mgp_box* valid, mgp_array* phi, const mgp_array* rhs, con
         return set_err(MGP_EINVAL, "relax_gs: the device sweep needs at least 4 cells per direction");
     const int nx = valid->nx, ny = valid->ny;
     OpCtx c;
-    DF p, f, d, r;
+    DF p, p2, f, d, r;
     Geo g;
     BCd b;
     double* red = nullptr;
+    RC(c.field(&p2, nx, ny, 1));
     RC(c.in(phi, nx, ny, 1, &p, "phi"));
     RC(c.in(rhs, nx, ny, 0, &f, "rhs"));
     RC(c.in(invdiags, nx, ny, 0, &d, "invdiags"));
@@ -906,8 +961,16 @@ int mgp_relax_gs(const mgp_box* valid, mgp_array* phi, const mgp_array* rhs, con
         RC(resnorm(&rscale));
         if (rscale == 0.0) rscale = 1.0;
     }
+    const bool fused = sweep_fusable(b);
     for (int it = 1; it <= maxiters; ++it) {
-        CK(launch_gs_sweep(p, f, d, g, b, homog, nx, ny, omega, c.st));
+        if (fused) {
+            CK(launch_sweep9(p, p2, f, d, g, b, homog, nx, ny, omega, c.st));
+            const DF t = p;
+            p = p2;
+            p2 = t;
+        } else {
+            CK(launch_gs_sweep(p, f, d, g, b, homog, nx, ny, omega, c.st));
+        }
         if (tol > 0.0) {
             RC(resnorm(&h));
             if (verbosity >= 3) printf("iter %d: rel |res| = %.16e\n", it, h / rscale);

@@ -578,28 +578,34 @@ __device__ void b_fill(const DF& p, const Geo& g, const BCd& b, int homog, int d
     __syncthreads();
 }
 
+// Block-wide sum / max with a fixed combination order (warp shuffles, then the
+// warps' partials in one warp), so the result does not depend on scheduling.
 __device__ double b_sum(double v, double* sh) {
-    sh[threadIdx.x] = v;
+    for (int o = 16; o > 0; o >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if ((threadIdx.x & 31) == 0) sh[w] = v;
     __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) sh[threadIdx.x] = sh[threadIdx.x] + sh[threadIdx.x + s];
-        __syncthreads();
+    if (w == 0) {
+        double x = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, o);
+        if (threadIdx.x == 0) sh[32] = x;
     }
-    const double r = sh[0];
     __syncthreads();
-    return r;
+    return sh[32];
 }
 
 __device__ double b_max(double v, double* sh) {
-    sh[threadIdx.x] = v;
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if ((threadIdx.x & 31) == 0) sh[w] = v;
     __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + s]);
-        __syncthreads();
+    if (w == 0) {
+        double x = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_down_sync(0xffffffffu, x, o));
+        if (threadIdx.x == 0) sh[32] = x;
     }
-    const double r = sh[0];
     __syncthreads();
-    return r;
+    return sh[32];
 }
 
 // pnorm (AU:753-796) with p = 2 or 0.
@@ -839,15 +845,17 @@ __device__ void b_set_guess(const Lv& L) {
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kCoarseThreads) k_coarse_cycle(CoarseArgs a) {
-    __shared__ double sh[kCoarseThreads];
+// vcycle_noinit(d0) down to the bottom and back, on the levels lv[d0..maxdepth]
+// (every thread of the block runs it).  Returns a nonzero status on a
+// non-finite bottom residual.
+__device__ int coarse_body(const Lv* lv, const CoarseArgs& a, double* sh) {
     int cnt[32];
     const double relax_omega = a.dd ? 4.0 / 5.0 : 1.0;
     int d = a.d0;
     int st = 0;
 visit:
     {
-        const Lv& L = a.lv[d];
+        const Lv& L = lv[d];
         if (a.dd) b_set_guess(L);   // DD:931, DD:971
         if (d == a.maxdepth) {
             b_relax(L, L.e, L.r, 1, relax_omega, a.nb, a.dd);
@@ -857,7 +865,7 @@ visit:
         }
         b_relax(L, L.e, L.r, 1, relax_omega, a.nd, a.dd);
         b_apply(L, L.w, L.e, L.r, 1, 1, a.dd);
-        const Lv& Cl = a.lv[d + 1];
+        const Lv& Cl = lv[d + 1];
         const int rx = a.refx[d], ry = a.refy[d];
         BLOOP(k, Cl.nx * Cl.ny) AT(Cl.r, k % Cl.nx, k / Cl.nx) =
             restrict_cc(L.w, k % Cl.nx, k / Cl.nx, rx, ry, 1.0 / (rx * ry));
@@ -869,10 +877,7 @@ visit:
         goto visit;
     }
 up:
-    if (d == a.d0) {
-        if (threadIdx.x == 0 && st) *a.status = st;
-        return;
-    }
+    if (d == a.d0) return st;
     d = d - 1;
     cnt[d] = cnt[d] + 1;
     if (cnt[d] < a.numcycles) {
@@ -881,15 +886,86 @@ up:
     }
 finish:
     {
-        const Lv& L = a.lv[d];
-        b_prolong(L, a.lv[d + 1], a.refx[d], a.refy[d], 1, sh);
+        const Lv& L = lv[d];
+        b_prolong(L, lv[d + 1], a.refx[d], a.refy[d], 1, sh);
         b_relax(L, L.e, L.r, 1, relax_omega, a.nu, a.dd);
     }
     goto up;
 }
 
+__global__ void __launch_bounds__(kCoarseThreads) k_coarse_cycle(CoarseArgs a) {
+    __shared__ double sh[kCoarseThreads];
+    const int s = coarse_body(a.lv, a, sh);
+    if (threadIdx.x == 0 && s) *a.status = s;
+}
+
+__device__ void b_copy(const DF& dst, const DF& src, int i0, int i1, int j0, int j1) {
+    const int w = i1 - i0, n = w * (j1 - j0);
+    BLOOP(k, n) AT(dst, i0 + k % w, j0 + k / w) = AT(src, i0 + k % w, j0 + k / w);
+}
+
+// global -> shared with asynchronous copies; the caller waits (cp_async_wait_all).
+__device__ void b_copy_in(const DF& dst, const DF& src, int i0, int i1, int j0, int j1) {
+    const int w = i1 - i0, n = w * (j1 - j0);
+    BLOOP(k, n) cp_async8(&AT(dst, i0 + k % w, j0 + k / w), &AT(src, i0 + k % w, j0 + k / w));
+}
+
+__device__ __forceinline__ void rebase(DF& f, double* base) { f.p = base + (size_t)(uintptr_t)f.p; }
+
+// The same cycle with every coarse level held in shared memory: the levels'
+// arrays are copied in (the corrections with their ghosts, the operands, the
+// finest level's right-hand side), the cycle runs, the corrections go back.
+__global__ void __launch_bounds__(kCoarseThreads) k_coarse_cycle_smem(CoarseArgs a) {
+    extern __shared__ double smem[];
+    __shared__ double sh[kCoarseThreads];
+    __shared__ Lv sl[kMaxCoarseLevels];
+    const int nl = a.maxdepth - a.d0 + 1;
+    if (threadIdx.x < nl) {
+        Lv L = a.shadow[a.d0 + threadIdx.x];
+        rebase(L.e, smem); rebase(L.r, smem); rebase(L.w, smem); rebase(L.invd, smem);
+        rebase(L.g.J, smem); rebase(L.g.xx, smem); rebase(L.g.xy, smem); rebase(L.g.yx, smem); rebase(L.g.yy, smem);
+        if (a.d0 + (int)threadIdx.x == a.maxdepth) {
+            rebase(L.ea, smem); rebase(L.pt, smem); rebase(L.st, smem);
+            rebase(L.rr, smem); rebase(L.rt, smem); rebase(L.pp, smem); rebase(L.tt, smem); rebase(L.vv, smem);
+        }
+        sl[threadIdx.x] = L;
+    }
+    __syncthreads();
+    for (int k = 0; k < nl; ++k) {
+        const Lv &S = sl[k], &G = a.lv[a.d0 + k];
+        const int nx = S.nx, ny = S.ny;
+        b_copy_in(S.e, G.e, -1, nx + 1, -1, ny + 1);
+        b_copy_in(S.invd, G.invd, 0, nx, 0, ny);
+        b_copy_in(S.g.J, G.g.J, 0, nx, 0, ny);
+        b_copy_in(S.g.xx, G.g.xx, 0, nx + 1, 0, ny);
+        b_copy_in(S.g.xy, G.g.xy, 0, nx + 1, 0, ny);
+        b_copy_in(S.g.yx, G.g.yx, 0, nx, 0, ny + 1);
+        b_copy_in(S.g.yy, G.g.yy, 0, nx, 0, ny + 1);
+        if (k == 0) b_copy_in(S.r, G.r, 0, nx, 0, ny);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const int s = coarse_body(sl - a.d0, a, sh);
+    for (int k = 0; k < nl; ++k) {
+        const Lv &S = sl[k], &G = a.lv[a.d0 + k];
+        b_copy(G.e, S.e, -1, S.nx + 1, -1, S.ny + 1);
+    }
+    if (threadIdx.x == 0 && s) *a.status = s;
+}
+
 cudaError_t launch_coarse_cycle(const CoarseArgs& a, cudaStream_t st) {
-    k_coarse_cycle<<<1, kCoarseThreads, 0, st>>>(a);
+    if (a.shadow && a.smem_bytes > 0) {
+        static int attr_bytes = 0;
+        if (attr_bytes < a.smem_bytes) {
+            cudaError_t e = cudaFuncSetAttribute(k_coarse_cycle_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 a.smem_bytes);
+            if (e != cudaSuccess) return e;
+            attr_bytes = a.smem_bytes;
+        }
+        k_coarse_cycle_smem<<<1, kCoarseThreads, a.smem_bytes, st>>>(a);
+    } else {
+        k_coarse_cycle<<<1, kCoarseThreads, 0, st>>>(a);
+    }
     count_launch();
     return cudaGetLastError();
 }

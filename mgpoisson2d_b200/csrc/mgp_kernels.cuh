@@ -19,7 +19,13 @@ struct CoarseArgs {
     const int* refx;     // device arrays, maxdepth entries
     const int* refy;
     int* status;         // device int: 0 ok, nonzero = error code
+    const Lv* shadow;    // device array: the levels' layout in shared memory (offsets), or nullptr
+    int smem_bytes;      // dynamic shared memory the staged levels need
 };
+
+constexpr int kMaxCoarseLevels = 16;
+// Largest staged coarse hierarchy (bytes of dynamic shared memory).
+constexpr int kCoarseSmemMax = 200 * 1024;
 
 // Parameters of the single-CTA BiCGStab (solve_bicgstab2).
 struct BicgArgs {
@@ -32,7 +38,7 @@ struct BicgArgs {
     int* status;
 };
 
-constexpr int kCoarseThreads = 1024;
+constexpr int kCoarseThreads = 256;
 
 long long launch_count();
 void count_launch(int n = 1);
@@ -45,6 +51,11 @@ cudaError_t launch_apply(const DF& out, const DF& phi, const DF& rhs, const Geo&
                          int nx, int ny, int mode, int jscale, cudaStream_t st);
 cudaError_t launch_gs_sweep(const DF& phi, const DF& rhs, const DF& invd, const Geo& g, const BCd& b, int homog,
                             int nx, int ny, double omega, cudaStream_t st);
+// One sweep in a single launch, reading pin and writing pout (mgp_sweep.cu).
+// Sides must be DIRI, NEUM or PERIODIC (sweep_fusable).
+bool sweep_fusable(const BCd& b);
+cudaError_t launch_sweep9(const DF& pin, const DF& pout, const DF& rhs, const DF& invd, const Geo& g, const BCd& b,
+                          int homog, int nx, int ny, double omega, cudaStream_t st);
 cudaError_t launch_invdiag(const DF& invd, const Geo& g, const BCd& b, int homog, int nx, int ny, int coupled,
                            cudaStream_t st);
 // kind: 0 cell, 1 x-face, 2 y-face, 3 node.  ncx/ncy = coarse cell counts.
