@@ -184,6 +184,24 @@ int mgp_solve_bicgstab2(const mgp_box *valid, mgp_array *phi, const mgp_array *r
                         const mgp_geo *geo, const mgp_bdry *bc, int homog,
                         const mgp_array *invdiags, double tol, int max_iters,
                         int max_restarts, int zerophi, int verbosity);
+/* No counterpart in the reference.  solve_bicgstab2 for callers that cannot
+ * allocate device memory -- a service that reserves its whole device-memory
+ * budget at start-up and forbids allocation afterwards, or code running while
+ * another component owns the device allocator (cudaMalloc can fail there, and
+ * cudaMalloc/cudaFree synchronise the device).  Same arguments and results as
+ * mgp_solve_bicgstab2, but every array must be device memory (phi with exactly
+ * one ghost layer), the grid at most MGP_NOALLOC_MAX_SIDE cells per side
+ * (MGP_EINVAL otherwise), and the work arrays live in one file-scope
+ * __device__ array (about 1.2 MB) that every device loading the library keeps
+ * until the process exits.  The first call on a device looks up that array's
+ * address with the device current; make that first call before any stream
+ * capture.  All calls share the array: calls whose kernels overlap on the
+ * device race on it.  Runs on the default stream and returns when done. */
+#define MGP_NOALLOC_MAX_SIDE 128
+int mgp_solve_bicgstab2_noalloc(const mgp_box *valid, mgp_array *phi, const mgp_array *rhs,
+                                const mgp_geo *geo, const mgp_bdry *bc, int homog,
+                                const mgp_array *invdiags, double tol, int max_iters,
+                                int max_restarts, int zerophi, int verbosity);
 /* restrict, MGPoisson2D.f90:135-257.  offi/offj: 0 = node, 1 = cell
  * (BD_NODE/BD_CELL, arrayutils.f90:76-77); crse/fine give the cell-centred
  * valid boxes of the two levels. */

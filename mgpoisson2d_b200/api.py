@@ -48,6 +48,7 @@ _SIGS = {
     "mgp_compute_residual": [_B, _A, _A, _A, _G, _BC, _i, _i],
     "mgp_relax_gs": [_B, _A, _A, _G, _BC, _i, _A, _d, _d, _i, _i, _i],
     "mgp_solve_bicgstab2": [_B, _A, _A, _G, _BC, _i, _A, _d, _i, _i, _i, _i],
+    "mgp_solve_bicgstab2_noalloc": [_B, _A, _A, _G, _BC, _i, _A, _d, _i, _i, _i, _i],
     "mgp_restrict": [_B, _A, _B, _A, _i, _i],
     "mgp_prolong": [_B, _A, _B, _A, _G, _G, _BC, _i],
     "mgp_pnorm": [_B, _A, _i, _P(_d)],
@@ -167,6 +168,21 @@ def solve_bicgstab2(phi: BoxData, rhs: BoxData, geo: GeoData, bc: BdryData, homo
     p, f, b, g, d = phi.c(), rhs.c(), bc.c(), geo.c(), invdiags.c()
     _ck(_lib.mgp_solve_bicgstab2(_r(phi.valid.c()), _r(p), _r(f), _r(g), _r(b), int(homog), _r(d), tol, max_iters,
                                  max_restarts, int(zerophi), verbosity), "solve_bicgstab2")
+
+
+NOALLOC_MAX_SIDE = 128
+
+
+def solve_bicgstab2_noalloc(phi: BoxData, rhs: BoxData, geo: GeoData, bc: BdryData, homog: bool,
+                            invdiags: BoxData, tol: float, max_iters: int, max_restarts: int, zerophi: bool,
+                            verbosity: int = 0):
+    """mgp_solve_bicgstab2_noalloc: the bottom solver on device arrays without
+    allocating device memory (for callers that cannot allocate; grids of at
+    most NOALLOC_MAX_SIDE cells per side; concurrent calls share one scratch
+    array and must not overlap on the device)."""
+    p, f, b, g, d = phi.c(), rhs.c(), bc.c(), geo.c(), invdiags.c()
+    _ck(_lib.mgp_solve_bicgstab2_noalloc(_r(phi.valid.c()), _r(p), _r(f), _r(g), _r(b), int(homog), _r(d), tol,
+                                         max_iters, max_restarts, int(zerophi), verbosity), "solve_bicgstab2_noalloc")
 
 
 def restrict(fine: BoxData, crse: BoxData):
@@ -292,6 +308,6 @@ class Solver:
 
 
 __all__ = ["vcycle", "fmg", "dc_vcycle", "Solver", "fill_ghosts", "extrapolate_ghosts", "compute_invdiags",
-           "compute_laplacian", "compute_residual", "relax_gs", "solve_bicgstab2", "restrict", "prolong", "pnorm",
+           "compute_laplacian", "compute_residual", "relax_gs", "solve_bicgstab2", "solve_bicgstab2_noalloc", "NOALLOC_MAX_SIDE", "restrict", "prolong", "pnorm",
            "inner_prod", "estimate_maxdepth", "create_mgschedule", "MGPError", "library_path", "kernel_launch_count",
            "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "EXPORTS", "KIND_MG", "KIND_DD"]

@@ -797,6 +797,12 @@ int ghost_cap(const mgp_array* a) {
 
 }  // namespace
 
+// Lets other translation units of the library record the message that
+// mgp_last_error() returns.
+namespace mgp {
+int record_error(int code, const char* msg) { return set_err(code, "%s", msg); }
+}  // namespace mgp
+
 // ===========================================================================
 // C ABI
 // ===========================================================================
