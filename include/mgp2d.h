@@ -128,6 +128,15 @@ typedef struct mgp_report {
 /* Time the finest level's smoothing with CUDA events (reported in
  * mgp_report.smooth0_seconds); the events are read after the solve. */
 #define MGP_FLAG_TIME_SMOOTHER 2
+/* vcycle only: accelerate the V-cycle with BiCGStab.  The solve runs
+ * right-preconditioned BiCGStab on the correction equation L_h e = r0
+ * (homogeneous BCs), one unchanged V-cycle per preconditioner application,
+ * and stops on the same relative-residual test.  report.iterations and the
+ * relres history count V-cycles (two per BiCGStab step); final_relres is the
+ * true residual rhs - L[phi] recomputed at the end.  No reference counterpart:
+ * the Fortran vcycle is a stationary iteration only.  On strongly stretched
+ * grids it needs several times fewer V-cycles for the same tolerance. */
+#define MGP_FLAG_KRYLOV 4
 
 /* Solver kinds for the resident-hierarchy handle. */
 #define MGP_KIND_MG 0   /* module MGPoisson2D (vcycle, fmg)                  */

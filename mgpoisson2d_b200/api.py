@@ -23,6 +23,7 @@ from .types import (KIND_DD, KIND_MG, STATUS_NAMES, BdryData, Box, BoxData, GeoD
 
 FLAG_DIRICHLET_COUPLED_DIAG = 1
 FLAG_TIME_SMOOTHER = 2
+FLAG_KRYLOV = 4
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libmgp2d.so")
@@ -250,7 +251,7 @@ class Solver:
     """A hierarchy built once and kept in HBM (mgp_solver_create).
 
     ``kind`` is KIND_MG (vcycle / fmg) or KIND_DD (deferred-correction vcycle);
-    ``flags`` e.g. FLAG_DIRICHLET_COUPLED_DIAG.
+    ``flags`` e.g. FLAG_DIRICHLET_COUPLED_DIAG | FLAG_KRYLOV.
     """
 
     def __init__(self, valid: Box, geo: GeoData, bc: BdryData, kind: int = KIND_MG, flags: int = 0,
@@ -310,4 +311,4 @@ class Solver:
 __all__ = ["vcycle", "fmg", "dc_vcycle", "Solver", "fill_ghosts", "extrapolate_ghosts", "compute_invdiags",
            "compute_laplacian", "compute_residual", "relax_gs", "solve_bicgstab2", "solve_bicgstab2_noalloc", "NOALLOC_MAX_SIDE", "restrict", "prolong", "pnorm",
            "inner_prod", "estimate_maxdepth", "create_mgschedule", "MGPError", "library_path", "kernel_launch_count",
-           "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "EXPORTS", "KIND_MG", "KIND_DD"]
+           "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV", "EXPORTS", "KIND_MG", "KIND_DD"]

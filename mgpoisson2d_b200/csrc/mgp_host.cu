@@ -251,6 +251,9 @@ struct mgp_solver {
     Arena fixed;            // geometry, inverse diagonals
     Arena state;            // everything a solve writes; zeroed at the start of each solve
     DF phi0{}, rhs0{};
+    // MGP_FLAG_KRYLOV: BiCGStab vectors on level 0 (residual, shadow residual,
+    // search direction, A*y and A*z)
+    DF kr{}, krh{}, kp{}, kv{}, kt{};
     double* d_bcbuf = nullptr;
     double* d_red = nullptr;    // reduction partials + outputs
     double* h_red = nullptr;    // pinned
@@ -363,6 +366,8 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
     }
     s->state.add(&s->phi0, valid->nx, valid->ny, 1);
     s->state.add(&s->rhs0, valid->nx, valid->ny, 0);
+    if ((s->flags & MGP_FLAG_KRYLOV) && s->kind == MGP_KIND_MG)
+        for (DF* f : {&s->kr, &s->krh, &s->kp, &s->kv, &s->kt}) s->state.add(f, valid->nx, valid->ny, 0);
     RC(s->fixed.commit(st));
     RC(s->state.commit(st));
     if (cudaMalloc(&s->d_bcbuf, sizeof(double) * 2 * (valid->nx + valid->ny + 2)) != cudaSuccess ||
@@ -577,6 +582,111 @@ int fmg_noinit(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
     return MGP_OK;
 }
 
+// dst = src over the valid region of level 0.
+int copy_valid(const DF& dst, const DF& src, int nx, int ny, cudaStream_t st) {
+    CK(cudaMemcpy2DAsync(dst.p, dst.ld * sizeof(double), src.p, src.ld * sizeof(double), nx * sizeof(double), ny,
+                         cudaMemcpyDeviceToDevice, st));
+    return MGP_OK;
+}
+
+// Reads reduction slots 0..n-1 back to s->h_red (one copy, one synchronisation).
+int fetch_reductions(mgp_solver* s, int n) {
+    CK(cudaMemcpyAsync(s->h_red, red_out(s), n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return MGP_OK;
+}
+
+// MGP_FLAG_KRYLOV: right-preconditioned BiCGStab (van der Vorst, SIAM J. Sci.
+// Stat. Comput. 13, 1992) on L_h e = r0, where L_h is the level-0 operator
+// with homogeneous BCs and the preconditioner is one V-cycle started from
+// e = r * invdiags (the same call the stationary loop makes, MG:600-606).
+// Corrections go straight into phi0; kr carries the recursive residual.  When
+// it passes the tolerance, the true residual rhs - L[phi] is recomputed with
+// the caller's BCs; if that one has not passed, BiCGStab restarts from it.
+// On entry L0.r holds r0.  relres[k] is the residual after k V-cycles; the
+// last entry is the true residual.
+int krylov_loop(mgp_solver* s, const BCd& ubc, int homog, double tol, int maxiters, int numcycles, int nd, int nu,
+                int nb, double rscale, std::vector<double>& relres, int* iters_out, int verbosity) {
+    Lv& L0 = s->lv[0];   // L0.e moves between two buffers as the fused sweep swaps them
+    const int nx = s->valid.nx, ny = s->valid.ny;
+    const double vol = s->valid.dx * s->valid.dy;
+    cudaStream_t st = s->stream;
+    double* out = red_out(s);
+    int k = 0;
+    // y = M^-1 x in L0.e, then Ay = L_h y
+    auto precond_apply = [&](const DF& x, const DF& Ay) -> int {
+        RC(copy_valid(L0.r, x, nx, ny, st));
+        CK(launch_set_guess(L0.e, L0.r, L0.invd, nx, ny, st));
+        RC(vcycle_noinit(s, 0, numcycles, nd, nu, nb));
+        CK(launch_fill(L0.e, L0.g, L0.bc, 1, 0, nx, ny, st));
+        CK(launch_apply(Ay, L0.e, L0.r, L0.g, L0.bc, 1, nx, ny, 0, 0, st));
+        return MGP_OK;
+    };
+    auto record = [&](double res) -> int {
+        relres[k] = res / rscale;
+        *iters_out = k;
+        if (verbosity >= 1) printf("BiCGStab V-Cycle %d: rel |res| = %.16e\n", k, relres[k]);
+        return std::isfinite(relres[k]) ? MGP_OK : MGP_EDIVERGED;
+    };
+    *iters_out = 0;
+    if (relres[0] <= tol) return MGP_OK;
+    RC(copy_valid(s->kr, L0.r, nx, ny, st));
+    for (;;) {   // one pass per (re)start
+        RC(copy_valid(s->krh, s->kr, nx, ny, st));
+        RC(copy_valid(s->kp, s->kr, nx, ny, st));
+        CK(launch_reduce(RED_DOT, s->krh, s->kr, nx, ny, vol, red_partials(s), out, st));
+        RC(fetch_reductions(s, 1));
+        double rho = s->h_red[0];
+        bool passed = false;
+        while (k < maxiters) {
+            // first half: alpha, s = r - alpha v
+            RC(precond_apply(s->kp, s->kv));
+            ++k;
+            CK(launch_reduce(RED_DOT, s->krh, s->kv, nx, ny, vol, red_partials(s), out, st));
+            RC(fetch_reductions(s, 1));
+            const double alpha = rho / s->h_red[0];
+            if (!std::isfinite(alpha)) { relres[k] = relres[k - 1]; break; }   // breakdown: restart
+            CK(launch_axpby(s->phi0, L0.e, 1.0, alpha, nx, ny, 0, 0, st));
+            CK(launch_axpby(s->kr, s->kv, 1.0, -alpha, nx, ny, 0, 0, st));
+            CK(launch_reduce(RED_SUMSQ, s->kr, s->kr, nx, ny, vol, red_partials(s), out, st));
+            RC(fetch_reductions(s, 1));
+            RC(record(s->h_red[0]));
+            if (relres[k] <= tol) { passed = true; break; }
+            if (k >= maxiters) break;
+            // second half: omega, r = s - omega t
+            RC(precond_apply(s->kr, s->kt));
+            ++k;
+            CK(launch_reduce(RED_DOT, s->kt, s->kr, nx, ny, vol, red_partials(s), out, st));
+            CK(launch_reduce(RED_DOT, s->kt, s->kt, nx, ny, vol, red_partials(s), out + 1, st));
+            RC(fetch_reductions(s, 2));
+            const double omega = s->h_red[0] / s->h_red[1];
+            if (!std::isfinite(omega) || omega == 0.0) { relres[k] = relres[k - 1]; break; }
+            CK(launch_axpby(s->phi0, L0.e, 1.0, omega, nx, ny, 0, 0, st));
+            CK(launch_axpby(s->kr, s->kt, 1.0, -omega, nx, ny, 0, 0, st));
+            CK(launch_reduce(RED_SUMSQ, s->kr, s->kr, nx, ny, vol, red_partials(s), out, st));
+            CK(launch_reduce(RED_DOT, s->krh, s->kr, nx, ny, vol, red_partials(s), out + 1, st));
+            RC(fetch_reductions(s, 2));
+            RC(record(s->h_red[0]));
+            if (relres[k] <= tol) { passed = true; break; }
+            const double rho_new = s->h_red[1];
+            const double beta = (rho_new / rho) * (alpha / omega);
+            if (!std::isfinite(beta) || rho_new == 0.0) break;   // breakdown: restart
+            rho = rho_new;
+            CK(launch_axpby(s->kp, s->kv, 1.0, -omega, nx, ny, 0, 0, st));   // p = r + beta (p - omega v)
+            CK(launch_axpby(s->kp, s->kr, beta, 1.0, nx, ny, 0, 0, st));
+        }
+        // true residual with the caller's BCs (MG:579)
+        CK(launch_fill(s->phi0, L0.g, ubc, homog, 0, nx, ny, st));
+        CK(launch_apply(L0.r, s->phi0, s->rhs0, L0.g, ubc, homog, nx, ny, 1, 0, st));
+        CK(launch_reduce(RED_SUMSQ, L0.r, L0.r, nx, ny, vol, red_partials(s), out, st));
+        RC(fetch_reductions(s, 1));
+        RC(record(s->h_red[0]));
+        *iters_out = k;
+        if ((passed && relres[k] <= tol) || k >= maxiters) return MGP_OK;
+        RC(copy_valid(s->kr, L0.r, nx, ny, st));
+    }
+}
+
 // 0 = vcycle (MG:400-670), 1 = fmg (MG:860-1122), 2 = DD vcycle (DD:589-862)
 int solver_solve(mgp_solver* s, int which, mgp_array* phi, mgp_array* rhs, const mgp_bdry* bc, int homog, double tol,
                  int maxiters, int numcycles, int nd, int nu, int nb, int zerophi, int verbosity, mgp_report* rep) {
@@ -619,7 +729,14 @@ int solver_solve(mgp_solver* s, int which, mgp_array* phi, mgp_array* rhs, const
     else relres[0] = 1.0;
     if (verbosity >= 1) printf("max MG depth = %d\nV-Cycle iter 0: rel |res| = %.16e\n", s->maxdepth, relres[0]);
     if (!std::isfinite(rscale)) status = MGP_EDIVERGED;
-    for (int iter = 1; iter <= maxiters && status == MGP_OK; ++iter) {
+    const bool krylov = which == 0 && (s->flags & MGP_FLAG_KRYLOV) && s->kr.p;
+    if (krylov && status == MGP_OK) {
+        const int rc = krylov_loop(s, ubc, homog, tol, maxiters, numcycles, nd, nu, nb, rscale, relres, &iters,
+                                   verbosity);
+        if (rc == MGP_EDIVERGED) status = rc;
+        else if (rc) return rc;
+    }
+    for (int iter = 1; !krylov && iter <= maxiters && status == MGP_OK; ++iter) {
         if (which == 0) CK(launch_set_guess(L0.e, L0.r, L0.invd, nx, ny, st));   // MG:600
         if (which == 1) RC(fmg_noinit(s, 0, numcycles, nd, nu, nb));
         else RC(vcycle_noinit(s, 0, numcycles, nd, nu, nb));

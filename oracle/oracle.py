@@ -248,3 +248,96 @@ def dc_vcycle(phi, rhs, geo, bc, homog, tol, maxiters, maxdepth_user=-1, numcycl
               smooth_bottom=1, zerophi=False, verbosity=0, gs_order=0):
     return _driver(lib().or_dc_vcycle, "dc_vcycle", phi, rhs, geo, bc, homog, tol, maxiters, maxdepth_user,
                    numcycles, smooth_down, smooth_up, smooth_bottom, zerophi, verbosity, gs_order)
+
+
+def krylov_vcycle(phi: BoxData, rhs: BoxData, geo: GeoData, bc: BdryData, homog: bool, tol: float,
+                  maxiters: int, numcycles: int = 1, smooth_down: int = 8, smooth_up: int = 8,
+                  smooth_bottom: int = 8, gs_order: int = 1):
+    """Oracle for the solver's MGP_FLAG_KRYLOV mode (no Fortran counterpart).
+
+    Right-preconditioned BiCGStab (van der Vorst 1992) on L_h e = r0, where
+    L_h is compute_laplacian with homogeneous BCs and the preconditioner is one
+    V-cycle of ``vcycle`` (MG:400-670) started from phi = 0 with the input as
+    its rhs -- exactly the set_guess + vcycle_noinit step of MG:600-606.
+    Returns the relative-residual history (one entry per V-cycle, the last one
+    recomputed as rhs - L[phi]).  Norms and inner products are numpy sums, so
+    the history agrees with the device's to rounding, not bitwise.
+    """
+    v = rhs.valid
+    vol = v.dx * v.dy
+
+    def nrm(a):
+        return float(np.sqrt(vol * np.sum(a * a)))
+
+    def dot(a, b):
+        return float(vol * np.sum(a * b))
+
+    def true_residual():
+        rb = BoxData(v)
+        compute_residual(rb, rhs, phi, geo, bc, homog)
+        return rb.interior().copy()
+
+    def precond(x):
+        e, f = BoxData(v, 1, 1), BoxData(v)
+        f.interior()[:] = x
+        rep = vcycle(e, f, geo, bc, True, 0.0, 1, numcycles=numcycles, smooth_down=smooth_down,
+                     smooth_up=smooth_up, smooth_bottom=smooth_bottom, zerophi=True, gs_order=gs_order)
+        if rep.diverged:
+            raise RuntimeError("preconditioning V-cycle raised the residual")
+        lap = BoxData(v)
+        compute_laplacian(lap, e, geo, bc, True)
+        return e.interior().copy(), lap.interior().copy()
+
+    r = true_residual()
+    rscale = nrm(r)
+    relres = [1.0]
+    if rscale == 0.0:
+        relres, rscale = [0.0], 1.0
+    if relres[0] <= tol:
+        return relres
+    x = phi.interior()
+    k = 0
+    while True:
+        rh, p = r.copy(), r.copy()
+        rho = dot(rh, r)
+        passed = False
+        while k < maxiters:
+            y, vv = precond(p)
+            k += 1
+            alpha = rho / dot(rh, vv)
+            if not np.isfinite(alpha):
+                relres.append(relres[-1])
+                break
+            x[:] = x + alpha * y
+            r = r - alpha * vv
+            relres.append(nrm(r) / rscale)
+            if relres[-1] <= tol:
+                passed = True
+                break
+            if k >= maxiters:
+                break
+            z, t = precond(r)
+            k += 1
+            omega = dot(t, r) / dot(t, t)
+            if not np.isfinite(omega) or omega == 0.0:
+                relres.append(relres[-1])
+                break
+            x[:] = x + omega * z
+            r = r - omega * t
+            relres.append(nrm(r) / rscale)
+            if relres[-1] <= tol:
+                passed = True
+                break
+            rho_new = dot(rh, r)
+            beta = (rho_new / rho) * (alpha / omega)
+            if not np.isfinite(beta) or rho_new == 0.0:
+                break
+            rho = rho_new
+            p = p - omega * vv
+            p = beta * p + r
+        r = true_residual()
+        relres[k] = nrm(r) / rscale
+        del relres[k + 1:]
+        if (passed and relres[k] <= tol) or k >= maxiters:
+            fill_ghosts(phi, bc, geo, homog, False)
+            return relres

@@ -309,3 +309,65 @@ def test_resident_solver_equals_oneshot_and_device_arrays(M):
         pd, rd_ = BoxData(v, 1, 1).to_device(), rhs.to_device()
         rd = s.vcycle(pd, rd_, bc, True, 1e-10, 15)
         assert same(pa.data, pd.to_host().data) and np.array_equal(ra.relres, rd.relres)
+
+
+# ---------------------------------------------------------------------------
+# BiCGStab-accelerated V-cycle (MGP_FLAG_KRYLOV; no reference counterpart)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("n", [64, 128])
+def test_krylov_vcycle_matches_oracle(M, n):
+    """Same V-cycles as the oracle (bit-exact in the device order); the inner
+    products are summed in a different order, so the histories agree to
+    rounding.  The converged solution must match the plain V-cycle's."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, _ = W.wavy_stretched(n)
+    old = _set_coupled(M, True)
+    try:
+        pa, pc = BoxData(v, 1, 1), BoxData(v, 1, 1)
+        ra = O.krylov_vcycle(pa, rhs, geo, bc, True, 1e-10, 400)
+        O.vcycle(pc, rhs, geo, bc, True, 1e-10, 2000, gs_order=1)
+    finally:
+        _set_coupled(M, old)
+    with M.Solver(v, geo, bc, KIND_MG, M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV) as s:
+        pb = BoxData(v, 1, 1)
+        rb = s.vcycle(pb, rhs, bc, True, 1e-10, 400)
+        pd = BoxData(v, 1, 1)
+        rd = s.vcycle(pd, rhs, bc, True, 1e-10, 400)
+    assert rb.status == 0 and rb.final_relres <= 1e-10 and rb.relres[-1] == rb.final_relres
+    assert abs(rb.iterations - (len(ra) - 1)) <= 2
+    k = min(12, len(ra), len(rb.relres))
+    np.testing.assert_allclose(rb.relres[:k], ra[:k], rtol=1e-6)
+    assert same(pb.data, pd.data) and np.array_equal(rb.relres, rd.relres)   # deterministic
+    for ref in (pa, pc):
+        err = pb.interior() - ref.interior()
+        assert np.linalg.norm(err) / np.linalg.norm(ref.interior()) < 1e-8
+    np.testing.assert_allclose(pb.data, pa.data, rtol=0, atol=1e-9 * np.abs(pa.data).max())   # ghosts too
+
+
+def test_krylov_oneshot_device_arrays_and_maxiters(M):
+    """The flag through mgp_set_flags and the one-shot driver, device arrays,
+    and the V-cycle budget: an odd maxiters stops after the first half step
+    with the true residual as the last entry."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, u = W.identity_dirichlet(64)
+    old = M.set_flags(M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV)
+    try:
+        pa = BoxData(v, 1, 1)
+        ra = M.vcycle(pa, rhs, geo, bc, True, 1e-11, 50)
+        pd, rd_ = BoxData(v, 1, 1).to_device(), rhs.to_device()
+        rd = M.vcycle(pd, rd_, geo, bc, True, 1e-11, 50)
+        pe = BoxData(v, 1, 1)
+        re = M.vcycle(pe, rhs, geo, bc, True, 1e-30, 3)
+    finally:
+        M.set_flags(old)
+    assert ra.final_relres <= 1e-11 and ra.iterations < 20
+    assert same(pa.data, pd.to_host().data) and np.array_equal(ra.relres, rd.relres)
+    assert re.iterations == 3 and len(re.relres) == 4 and re.final_relres == re.relres[-1] > 0
+    oa = BoxData(v, 1, 1)
+    O.lib().or_set_dirichlet_coupled_diagonal(1)
+    try:
+        ro = O.krylov_vcycle(oa, rhs, geo, bc, True, 1e-30, 3)
+    finally:
+        O.lib().or_set_dirichlet_coupled_diagonal(0)
+    np.testing.assert_allclose(re.relres, ro, rtol=1e-7)
+    np.testing.assert_allclose(pe.data, oa.data, rtol=0, atol=1e-10 * np.abs(oa.data).max())

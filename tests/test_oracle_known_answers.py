@@ -295,3 +295,21 @@ def test_dc_vcycle_dirichlet_converges():
     rep = O.dc_vcycle(phi, f, geo, bc, True, 1e-10, 60, smooth_down=8, smooth_up=8, smooth_bottom=8)
     assert rep.relres[-1] <= 1e-10
     assert np.abs(phi.interior() - u).max() < 2e-3
+
+
+def test_krylov_oracle_same_solution_fewer_vcycles():
+    """The BiCGStab restatement behind MGP_FLAG_KRYLOV reaches the plain
+    V-cycle's converged solution on the stretched wavy grid with several
+    times fewer V-cycles."""
+    v, geo, rhs, bc, _ = W.wavy_stretched(64)
+    _coupled(True)
+    try:
+        pa, pb = BoxData(v, 1, 1), BoxData(v, 1, 1)
+        ra = O.vcycle(pa, rhs, geo, bc, True, 1e-10, 2000, gs_order=1)
+        rk = O.krylov_vcycle(pb, rhs, geo, bc, True, 1e-10, 2000)
+    finally:
+        _coupled(False)
+    assert ra.relres[-1] <= 1e-10 and rk[-1] <= 1e-10
+    assert 3 * (len(rk) - 1) < ra.iterations
+    err = pb.interior() - pa.interior()
+    assert np.linalg.norm(err) / np.linalg.norm(pa.interior()) < 1e-8
