@@ -63,6 +63,14 @@ __device__ __forceinline__ void cp_async8(double* smem_dst, const double* gsrc) 
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// The same by shared-space address, without a memory clobber: the copies of
+// a staging loop are ordered against later reads by cp_async_wait_all.
+__device__ __forceinline__ void cp_async8s(unsigned sdst, const double* gsrc) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sdst), "l"(gsrc));
+}
+__device__ __forceinline__ void cp_async16s(unsigned sdst, const double* gsrc) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sdst), "l"(gsrc));
+}
 
 __device__ __forceinline__ int region(int i, int n, bool per_lo, bool per_hi) {
     if (i == 0 && !per_lo) return RLO;

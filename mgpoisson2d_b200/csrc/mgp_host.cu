@@ -64,7 +64,9 @@ struct Arena {
     size_t elems = 0;
     double* base = nullptr;
     void add(DF* dst, int nxv, int nyv, int g) {
-        const int ld = ((nxv + 2 * g + 31) / 32) * 32;
+        // arrays with ghosts keep one spare column, so the sweep's TMA window
+        // (from column -2) still covers the ghost column nx
+        const int ld = ((nxv + 3 * g + 31) / 32) * 32;
         const size_t pad = g ? 32 : 0;
         const size_t n = (size_t)(nyv + 2 * g) * ld + 2 * pad;
         Spec s{dst, nxv, nyv, g, elems};
@@ -254,6 +256,7 @@ struct mgp_solver {
     // MGP_FLAG_KRYLOV: BiCGStab vectors on level 0 (residual, shadow residual,
     // search direction, A*y and A*z)
     DF kr{}, krh{}, kp{}, kv{}, kt{};
+    std::vector<SweepTma> tma;   // per level, for the fused sweep
     double* d_bcbuf = nullptr;
     double* d_red = nullptr;    // reduction partials + outputs
     double* h_red = nullptr;    // pinned
@@ -444,6 +447,11 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
             s->shadow_bytes = (int)bytes;
         }
     }
+    s->tma.assign(md + 1, SweepTma{});
+    for (int d = 0; d < s->dc; ++d) {
+        Lv& L = s->lv[d];
+        if (L.e2.p) sweep_tma_prepare(&s->tma[d], L.e, L.e2, L.r, L.invd, L.g, L.nx, L.ny);
+    }
     std::vector<int> ref(2 * (md + 1), 0);
     for (int d = 0; d < md; ++d) { ref[d] = s->refx[d]; ref[md + 1 + d] = s->refy[d]; }
     CK(cudaMemcpyAsync(s->d_lv, s->lv.data(), sizeof(Lv) * (md + 1), cudaMemcpyHostToDevice, st));
@@ -487,7 +495,7 @@ int smooth_body(mgp_solver* s, int d, int nu) {
         }
     } else if (L.e2.p && sweep_fusable(L.bc)) {
         for (int k = 0; k < nu; ++k) {
-            CK(launch_sweep9(L.e, L.e2, L.r, L.invd, L.g, L.bc, 1, L.nx, L.ny, 1.0, st));
+            CK(launch_sweep9(L.e, L.e2, L.r, L.invd, L.g, L.bc, 1, L.nx, L.ny, 1.0, &s->tma[d], s->d_status, st));
             const DF t = L.e;
             L.e = L.e2;
             L.e2 = t;
@@ -766,7 +774,7 @@ int solver_solve(mgp_solver* s, int which, mgp_array* phi, mgp_array* rhs, const
     }
     CK(cudaEventRecord(s->ev1, st));
     CK(cudaStreamSynchronize(st));
-    if (status == MGP_OK && dstat) status = MGP_EDIVERGED;
+    if (status == MGP_OK && dstat) status = (dstat == 2) ? MGP_ETIMEOUT : (dstat == 3) ? MGP_ECUDA : MGP_EDIVERGED;
     if (rep) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, s->ev0, s->ev1);
@@ -788,6 +796,8 @@ int solver_solve(mgp_solver* s, int which, mgp_array* phi, mgp_array* rhs, const
         if (rep->relres)
             for (int k = 0; k <= iters; ++k) rep->relres[k] = relres[k];
     }
+    if (status == MGP_ETIMEOUT) return set_err(status, "a device wait ran out of its iteration limit");
+    if (status == MGP_ECUDA) return set_err(status, "misaligned shared-memory window in the sweep");
     if (status) return set_err(status, "non-finite residual");
     return MGP_OK;
 }
@@ -1087,7 +1097,7 @@ int mgp_relax_gs(const mgp_box* valid, mgp_array* phi, const mgp_array* rhs, con
     const bool fused = sweep_fusable(b);
     for (int it = 1; it <= maxiters; ++it) {
         if (fused) {
-            CK(launch_sweep9(p, p2, f, d, g, b, homog, nx, ny, omega, c.st));
+            CK(launch_sweep9(p, p2, f, d, g, b, homog, nx, ny, omega, nullptr, nullptr, c.st));
             const DF t = p;
             p = p2;
             p2 = t;

@@ -1,6 +1,8 @@
 // mgp_kernels.cuh -- kernel launchers shared by the host drivers (mgp_host.cu)
 // and the kernels (mgp_kernels.cu).
 #pragma once
+#include <cuda.h>
+
 #include "mgp_core.cuh"
 
 namespace mgp {
@@ -54,8 +56,28 @@ cudaError_t launch_gs_sweep(const DF& phi, const DF& rhs, const DF& invd, const 
 // One sweep in a single launch, reading pin and writing pout (mgp_sweep.cu).
 // Sides must be DIRI, NEUM or PERIODIC (sweep_fusable).
 bool sweep_fusable(const BCd& b);
+// TMA descriptors of the seven fields one sweep stages; phi element (i,j) is
+// map coordinate (i - pcb, j - prb), the operands' (i,j) is (i,j).
+struct SweepMaps {
+    CUtensorMap pin, rhs, invd, xx, xy, yx, yy;
+    int pcb, prb;
+};
+// Descriptors for sweeping one level with phi in either of its two buffers.
+struct SweepTma {
+    SweepMaps ma, mb;
+    const double *pa = nullptr, *pb = nullptr, *rhs = nullptr, *invd = nullptr, *xx = nullptr;
+    bool ok = false;
+};
+// Builds the descriptors when the arrays allow it (16-byte aligned bases and
+// pitches, phi with a ghost layer and pitch >= nx + 3); else t->ok = false
+// and the sweep stages with cp.async.
+void sweep_tma_prepare(SweepTma* t, const DF& ea, const DF& eb, const DF& rhs, const DF& invd, const Geo& g, int nx,
+                       int ny);
+// status (nullable) receives 2 if a CTA's staging never completed, 3 if the
+// shared-memory window was not 128-byte aligned (neither is expected).
 cudaError_t launch_sweep9(const DF& pin, const DF& pout, const DF& rhs, const DF& invd, const Geo& g, const BCd& b,
-                          int homog, int nx, int ny, double omega, cudaStream_t st);
+                          int homog, int nx, int ny, double omega, const SweepTma* tma, int* status,
+                          cudaStream_t st);
 cudaError_t launch_invdiag(const DF& invd, const Geo& g, const BCd& b, int homog, int nx, int ny, int coupled,
                            cudaStream_t st);
 // kind: 0 cell, 1 x-face, 2 y-face, 3 node.  ncx/ncy = coarse cell counts.

@@ -22,6 +22,16 @@
 // The halo cells are recomputed by every CTA that needs them, with the same
 // operations in the same order, so the result is bit-identical to running the
 // sub-passes over the whole grid one after another.
+//
+// Staging: on the solver's own arrays (aligned, with a spare column) one
+// thread issues seven TMA tile loads (cp.async.bulk.tensor.2d) of the CTA's
+// 46 x 44 window of each field, completing on one mbarrier; elsewhere (caller
+// arrays of any pitch and alignment) the threads stage with cp.async.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
 #include "mgp_kernels.cuh"
 
 namespace mgp {
@@ -30,14 +40,21 @@ namespace {
 
 constexpr int kTX = 32, kTY = 32;
 constexpr int kH = 6;   // phi halo: 4 for the colour passes + E = 2 for the boundary pass
-constexpr int kG = 5;   // operand halo: the largest pass region, tile + 3 + E
-constexpr int kSweepThreads = 256;
+constexpr int kSweepThreads = 512;
 
-constexpr int PW = kTX + 2 * kH, PH = kTY + 2 * kH;         // phi
-constexpr int CW = kTX + 2 * kG, CH = kTY + 2 * kG;         // rhs, invdiag (cells)
-constexpr int XW = CW + 1, YH = CH + 1;                      // x-faces (XW x CH), y-faces (CW x YH)
-constexpr int kSmemDoubles = PW * PH + 2 * CW * CH + 2 * XW * CH + 2 * CW * YH;
-constexpr size_t kSmemBytes = kSmemDoubles * sizeof(double);
+// All seven staged arrays share one window -- origin (pox, poy) with pox the
+// even column at or below tile corner - kH, pitch PW -- so one offset
+// addresses a cell in every array: phi and the cell operands at o, the
+// west/east x-faces at o and o + 1, the south/north y-faces at o and o + PW.
+// The operands are needed on tile + (3 + E) <= tile + 5 cells (faces one
+// further), inside the phi footprint tile + kH.
+constexpr int PW = kTX + 2 * kH + 2, PH = kTY + 2 * kH;   // 46 x 44: one spare column for the even origin
+constexpr int kA = (PW * PH + 15) / 16 * 16;              // array stride: 128-byte aligned
+constexpr int oF = kA, oD = 2 * kA, oXX = 3 * kA, oXY = 4 * kA, oYX = 5 * kA, oYY = 6 * kA;
+constexpr int oBar = 7 * kA;                              // the TMA mbarrier (8 bytes)
+constexpr size_t kSmemBytes = (7 * kA + 2) * sizeof(double);
+constexpr unsigned kBoxBytes = PW * PH * sizeof(double);
+constexpr long kWaitLimit = 1L << 22;   // mbarrier polls before a CTA gives up (far above any real wait)
 
 struct SLoad {
     const double* c;
@@ -45,75 +62,141 @@ struct SLoad {
     __device__ __forceinline__ double operator()(int di, int dj) const { return c[di + dj * ld]; }
 };
 
-// The value fill_ghosts (do_neum = .false.) gives ghost (i,j) at the start of
-// the sweep, for sides of type DIRI, NEUM (left as stored) and PERIODIC.
-__device__ double sweep_ghost(const DF& pin, const BCd& b, int homog, int nx, int ny, int i, int j) {
+// phi at the start of the sweep: the staged copy where it holds (i,j), else
+// global memory (the far side of a periodic domain).
+struct PinLoad {
+    const double* s;
+    int pox, poy, pi0, pi1, pj0, pj1;
+    DF pin;
+    __device__ __forceinline__ double operator()(int i, int j) const {
+        if (i >= pi0 && i < pi1 && j >= pj0 && j < pj1) return s[(j - poy) * PW + (i - pox)];
+        return AT(pin, i, j);
+    }
+};
+
+// The value fill_ghosts (do_neum = .false.) gives the y-side ghost (i,j),
+// 0 <= i < nx, for sides of type DIRI, NEUM (left as stored) and PERIODIC.
+__device__ __forceinline__ double ghost_yside(const PinLoad& P, const BCd& b, int homog, int ny, int i, int j) {
+    const int s = (j < 0) ? S_YLO : S_YHI;
+    const int t = b.type[s];
+    if (t == T_DIRI) {
+        const int jj = (j < 0) ? 0 : ny - 1, e = (j < 0) ? -1 : 1;
+        return ghost_diri(b, homog, s, i, P(i, jj), P(i, jj - e), P(i, jj - 2 * e));
+    }
+    if (t == T_PERIODIC) return P(i, (j < 0) ? ny - 1 : 0);
+    return P(i, j);
+}
+
+// The same for the x-side ghost (i,j), 0 <= j < ny.
+__device__ __forceinline__ double ghost_xside(const PinLoad& P, const BCd& b, int homog, int nx, int i, int j) {
+    const int s = (i < 0) ? S_XLO : S_XHI;
+    const int t = b.type[s];
+    if (t == T_DIRI) {
+        const int ii = (i < 0) ? 0 : nx - 1, e = (i < 0) ? -1 : 1;
+        return ghost_diri(b, homog, s, j, P(ii, j), P(ii - e, j), P(ii - 2 * e, j));
+    }
+    if (t == T_PERIODIC) return P((i < 0) ? nx - 1 : 0, j);
+    return P(i, j);
+}
+
+// Any ghost cell; corners as AU:1460-1490.
+__device__ double sweep_ghost(const PinLoad& P, const BCd& b, int homog, int nx, int ny, int i, int j) {
     const bool xin = (i >= 0 && i < nx), yin = (j >= 0 && j < ny);
-    if (xin && !yin) {
-        const int s = (j < 0) ? S_YLO : S_YHI;
-        const int t = b.type[s];
-        if (t == T_DIRI) {
-            const int jj = (j < 0) ? 0 : ny - 1, e = (j < 0) ? -1 : 1;
-            return ghost_diri(b, homog, s, i, AT(pin, i, jj), AT(pin, i, jj - e), AT(pin, i, jj - 2 * e));
-        }
-        if (t == T_PERIODIC) return AT(pin, i, (j < 0) ? ny - 1 : 0);
-        return AT(pin, i, j);
-    }
-    if (yin && !xin) {
-        const int s = (i < 0) ? S_XLO : S_XHI;
-        const int t = b.type[s];
-        if (t == T_DIRI) {
-            const int ii = (i < 0) ? 0 : nx - 1, e = (i < 0) ? -1 : 1;
-            return ghost_diri(b, homog, s, j, AT(pin, ii, j), AT(pin, ii - e, j), AT(pin, ii - 2 * e, j));
-        }
-        if (t == T_PERIODIC) return AT(pin, (i < 0) ? nx - 1 : 0, j);
-        return AT(pin, i, j);
-    }
-    // corners (AU:1460-1490)
+    if (xin && !yin) return ghost_yside(P, b, homog, ny, i, j);
+    if (yin && !xin) return ghost_xside(P, b, homog, nx, i, j);
     const bool px = b.type[S_XLO] == T_PERIODIC, py = b.type[S_YLO] == T_PERIODIC;
     if (!px && !py) return kBogus;
     const int wi = (i < 0) ? nx - 1 : 0, wj = (j < 0) ? ny - 1 : 0;
-    if (px && py) return AT(pin, wi, wj);
-    if (px) return sweep_ghost(pin, b, homog, nx, ny, wi, j);   // a y-side ghost
-    return sweep_ghost(pin, b, homog, nx, ny, i, wj);           // an x-side ghost
+    if (px && py) return P(wi, wj);
+    if (px) return ghost_yside(P, b, homog, ny, wi, j);
+    return ghost_xside(P, b, homog, nx, i, wj);
 }
 
 // Copy rows [j0,j1) x columns [i0,i1) of a global field into a shared array
-// whose (0,0) is cell (ox, oy) and whose row pitch is w.
+// whose (0,0) is cell (ox, oy) and whose row pitch is w.  Warp w8 takes rows
+// j0 + w8, j0 + w8 + 8, ...; where a row's global and shared addresses have
+// the same 16-byte phase its lanes copy pairs of doubles, else single ones.
 __device__ __forceinline__ void stage(double* s, int w, int ox, int oy, const DF& f, int i0, int i1, int j0, int j1) {
-    const int cw = i1 - i0, n = cw * (j1 - j0);
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        const int i = i0 + k % cw, j = j0 + k / cw;
-        cp_async8(&s[(j - oy) * w + (i - ox)], &AT(f, i, j));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const unsigned sbase = (unsigned)__cvta_generic_to_shared(s);
+    for (int j = j0 + warp; j < j1; j += nw) {
+        const double* g = f.p + (long)j * f.ld + i0;
+        unsigned sa = sbase + (unsigned)(((j - oy) * w + (i0 - ox)) * 8);
+        const int n = i1 - i0;
+        if (n <= 0) continue;
+        if (((unsigned)(uintptr_t)g ^ sa) & 8) {
+            for (int k = lane; k < n; k += 32) cp_async8s(sa + 8 * k, g + k);
+            continue;
+        }
+        int k0 = 0;
+        if (sa & 8) {   // leading single
+            if (lane == 0) cp_async8s(sa, g);
+            k0 = 1;
+        }
+        const int np = (n - k0) >> 1;
+        for (int k = lane; k < np; k += 32) cp_async16s(sa + 8 * (k0 + 2 * k), g + k0 + 2 * k);
+        if (((n - k0) & 1) && lane == 31) cp_async8s(sa + 8 * (n - 1), g + n - 1);   // trailing single
     }
 }
 
+// ---- TMA staging ---------------------------------------------------------- //
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for phase 0 of the barrier; false if it did not complete.
+__device__ __forceinline__ bool mbar_wait0(unsigned bar) {
+    for (long k = 0; k < kWaitLimit; ++k)
+        if (mbar_try_wait(bar, 0)) return true;
+    return false;
+}
+// One 2-D tile (box PW x PH) of `map` at element coordinates (x, y), x even.
+__device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map, int x, int y, unsigned bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+        ::"r"(dst), "l"((unsigned long long)map), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
 struct Tile {
-    double *ph, *f, *d, *xx, *xy, *yx, *yy;
-    int pox, poy, cox, coy;
+    double* s;   // seven arrays of PW x PH, origin (pox, poy)
+    int pox, poy;
 };
 
 // One Gauss-Seidel update of (i,j) from shared memory (same operations as gs9).
 __device__ __forceinline__ void gs9_tile(const Tile& t, double idx, double idy, const BCd& b, int homog, int i, int j,
                                          int xr, int yr, double omega) {
-    double* c = t.ph + (j - t.poy) * PW + (i - t.pox);
+    double* c = t.s + (j - t.poy) * PW + (i - t.pox);
     St9 s;
     gather9(SLoad{c, PW}, xr, yr, s);
-    const int ci = i - t.cox, cj = j - t.coy;
     Faces fc;
-    fc.xxe = t.xx[cj * XW + ci + 1]; fc.xxw = t.xx[cj * XW + ci];
-    fc.xye = t.xy[cj * XW + ci + 1]; fc.xyw = t.xy[cj * XW + ci];
-    fc.yyn = t.yy[(cj + 1) * CW + ci]; fc.yys = t.yy[cj * CW + ci];
-    fc.yxn = t.yx[(cj + 1) * CW + ci]; fc.yxs = t.yx[cj * CW + ci];
+    fc.xxw = c[oXX]; fc.xxe = c[oXX + 1];
+    fc.xyw = c[oXY]; fc.xye = c[oXY + 1];
+    fc.yys = c[oYY]; fc.yyn = c[oYY + PW];
+    fc.yxs = c[oYX]; fc.yxn = c[oYX + PW];
     const double lphi = lap9f(s, fc, idx, idy, i, j, xr, yr, b, homog);
     const double p = c[0];
-    const double newphi = p + (t.f[cj * CW + ci] - lphi) * t.d[cj * CW + ci];
+    const double newphi = p + (c[oF] - lphi) * c[oD];
     c[0] = omega * newphi + (1.0 - omega) * p;
 }
 
-__global__ void __launch_bounds__(kSweepThreads) k_sweep9(DF pin, DF pout, DF rhs, DF invd, Geo g, BCd b, int homog,
-                                                          int nx, int ny, double omega) {
-    extern __shared__ double smem[];
+template <bool kTma>
+__global__ void __launch_bounds__(kSweepThreads, 2)
+    k_sweep9(const __grid_constant__ SweepMaps m, DF pin, DF pout, DF rhs, DF invd, Geo g, BCd b, int homog, int nx,
+             int ny, double omega, int* status) {
+    extern __shared__ __align__(1024) double smem[];
     const int X0 = (int)((long)blockIdx.x * nx / gridDim.x), X1 = (int)((long)(blockIdx.x + 1) * nx / gridDim.x);
     const int Y0 = (int)((long)blockIdx.y * ny / gridDim.y), Y1 = (int)((long)(blockIdx.y + 1) * ny / gridDim.y);
     const Per pr = periodic_of(b);
@@ -121,73 +204,108 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep9(DF pin, DF pout, DF rh
     const int E = edge_tile ? 2 : 0;
 
     Tile t;
-    t.ph = smem;
-    t.f = t.ph + PW * PH;
-    t.d = t.f + CW * CH;
-    t.xx = t.d + CW * CH;
-    t.xy = t.xx + XW * CH;
-    t.yx = t.xy + XW * CH;
-    t.yy = t.yx + CW * YH;
-    t.pox = X0 - kH; t.poy = Y0 - kH;
-    t.cox = X0 - kG; t.coy = Y0 - kG;
+    t.s = smem;
+    t.pox = (X0 - kH) & ~1; t.poy = Y0 - kH;
 
     // 1. stage phi on tile + (4 + E) and the operands on tile + (3 + E)
     const int hp = 4 + E, hc = 3 + E;
     const int pi0 = max(X0 - hp, -1), pi1 = min(X1 + hp, nx + 1), pj0 = max(Y0 - hp, -1), pj1 = min(Y1 + hp, ny + 1);
     const int ci0 = max(X0 - hc, 0), ci1 = min(X1 + hc, nx), cj0 = max(Y0 - hc, 0), cj1 = min(Y1 + hc, ny);
-    stage(t.ph, PW, t.pox, t.poy, pin, pi0, pi1, pj0, pj1);
-    stage(t.f, CW, t.cox, t.coy, rhs, ci0, ci1, cj0, cj1);
-    stage(t.d, CW, t.cox, t.coy, invd, ci0, ci1, cj0, cj1);
-    stage(t.xx, XW, t.cox, t.coy, g.xx, ci0, ci1 + 1, cj0, cj1);
-    stage(t.xy, XW, t.cox, t.coy, g.xy, ci0, ci1 + 1, cj0, cj1);
-    stage(t.yx, CW, t.cox, t.coy, g.yx, ci0, ci1, cj0, cj1 + 1);
-    stage(t.yy, CW, t.cox, t.coy, g.yy, ci0, ci1, cj0, cj1 + 1);
-    cp_async_wait_all();
-    __syncthreads();
-    // 2. sweep-start ghost fill on the staged ghost cells
-    {
-        const int lw = pi1 - pi0, n = lw * (pj1 - pj0);
-        for (int k = threadIdx.x; k < n; k += blockDim.x) {
-            const int i = pi0 + k % lw, j = pj0 + k / lw;
+    if (kTma) {
+        // the whole window of every array; what lies outside a field reads as 0 and is never used
+        const unsigned sb = (unsigned)__cvta_generic_to_shared(smem), bar = sb + oBar * 8;
+        if (sb & 127) {   // TMA destinations must be 128-byte aligned
+            if (threadIdx.x == 0 && status) atomicExch(status, 3);
+            return;
+        }
+        if (threadIdx.x == 0) mbar_init(bar, 1);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            mbar_expect_tx(bar, 7 * kBoxBytes);
+            tma_load_2d(sb, &m.pin, t.pox - m.pcb, t.poy - m.prb, bar);
+            tma_load_2d(sb + oF * 8, &m.rhs, t.pox, t.poy, bar);
+            tma_load_2d(sb + oD * 8, &m.invd, t.pox, t.poy, bar);
+            tma_load_2d(sb + oXX * 8, &m.xx, t.pox, t.poy, bar);
+            tma_load_2d(sb + oXY * 8, &m.xy, t.pox, t.poy, bar);
+            tma_load_2d(sb + oYX * 8, &m.yx, t.pox, t.poy, bar);
+            tma_load_2d(sb + oYY * 8, &m.yy, t.pox, t.poy, bar);
+        }
+        if (!mbar_wait0(bar)) {   // never seen; leave the tile unwritten and report
+            if (status) atomicExch(status, 2);
+            mbar_wait0(bar);      // let copies still in flight land before the CTA exits
+            return;
+        }
+    } else {
+        stage(smem, PW, t.pox, t.poy, pin, pi0, pi1, pj0, pj1);
+        stage(smem + oF, PW, t.pox, t.poy, rhs, ci0, ci1, cj0, cj1);
+        stage(smem + oD, PW, t.pox, t.poy, invd, ci0, ci1, cj0, cj1);
+        stage(smem + oXX, PW, t.pox, t.poy, g.xx, ci0, ci1 + 1, cj0, cj1);
+        stage(smem + oXY, PW, t.pox, t.poy, g.xy, ci0, ci1 + 1, cj0, cj1);
+        stage(smem + oYX, PW, t.pox, t.poy, g.yx, ci0, ci1, cj0, cj1 + 1);
+        stage(smem + oYY, PW, t.pox, t.poy, g.yy, ci0, ci1, cj0, cj1 + 1);
+        cp_async_wait_all();
+        __syncthreads();
+    }
+    // 2. sweep-start ghost fill on the staged ghost cells (the ghost rows and
+    //    columns of tiles on the domain boundary only)
+    if (pi0 < 0 || pi1 > nx || pj0 < 0 || pj1 > ny) {
+        const PinLoad P{smem, t.pox, t.poy, pi0, pi1, pj0, pj1, pin};
+        const int lw = pi1 - pi0, lh = pj1 - pj0;
+        for (int k = threadIdx.x; k < 2 * (lw + lh); k += blockDim.x) {
+            int i, j;
+            if (k < lw) { i = pi0 + k; j = pj0; }
+            else if (k < 2 * lw) { i = pi0 + k - lw; j = pj1 - 1; }
+            else if (k < 2 * lw + lh) { i = pi0; j = pj0 + k - 2 * lw; }
+            else { i = pi1 - 1; j = pj0 + k - 2 * lw - lh; }
             if (i >= 0 && i < nx && j >= 0 && j < ny) continue;
-            t.ph[(j - t.poy) * PW + (i - t.pox)] = sweep_ghost(pin, b, homog, nx, ny, i, j);
+            smem[(j - t.poy) * PW + (i - t.pox)] = sweep_ghost(P, b, homog, nx, ny, i, j);
         }
     }
     __syncthreads();
 
-    // 3. interior colour passes on shrinking regions
+    // 3. interior colour passes on shrinking regions.  Interior cells are
+    //    i in [mi0, mi1), j in [mj0, mj1); one thread per cell of the colour
+    //    (a pass has at most 21 x 21 of them).
+    const int mi0 = pr.xl ? 0 : 1, mi1 = pr.xh ? nx : nx - 1;
+    const int mj0 = pr.yl ? 0 : 1, mj1 = pr.yh ? ny : ny - 1;
 #pragma unroll 1
     for (int c = 0; c < 4; ++c) {
         const int ci = colour_ci(c), cj = colour_cj(c);
         const int grow = 3 - c + E;
-        int i0 = max(X0 - grow, 0), i1 = min(X1 + grow, nx);
-        int j0 = max(Y0 - grow, 0), j1 = min(Y1 + grow, ny);
+        int i0 = max(X0 - grow, mi0), i1 = min(X1 + grow, mi1);
+        int j0 = max(Y0 - grow, mj0), j1 = min(Y1 + grow, mj1);
         i0 += (i0 & 1) != ci;
         j0 += (j0 & 1) != cj;
         const int cw = (i1 - i0 + 1) / 2, chh = (j1 - j0 + 1) / 2;
         for (int k = threadIdx.x; k < cw * chh; k += blockDim.x) {
-            const int i = i0 + 2 * (k % cw), j = j0 + 2 * (k / cw);
-            if (i >= i1 || j >= j1) continue;
-            const int xr = region(i, nx, pr.xl, pr.xh), yr = region(j, ny, pr.yl, pr.yh);
-            if (xr != RMID || yr != RMID) continue;
-            gs9_tile(t, g.idx, g.idy, b, homog, i, j, xr, yr, omega);
+            const int kj = k / cw;
+            const int i = i0 + 2 * (k - kj * cw), j = j0 + 2 * kj;
+            gs9_tile(t, g.idx, g.idy, b, homog, i, j, RMID, RMID, omega);
         }
         __syncthreads();
     }
 
-    // 4. boundary pass (edge tiles only; uniform per CTA)
+    // 4. boundary pass (edge tiles only; uniform per CTA): per colour, the
+    //    edge cells of that colour along each non-periodic side within the
+    //    tile grown by one, then the corners in turn
     if (edge_tile) {
-        const int i0 = max(X0 - 1, 0), i1 = min(X1 + 1, nx);
-        const int j0 = max(Y0 - 1, 0), j1 = min(Y1 + 1, ny);
-        const int w = i1 - i0, h = j1 - j0;
+        const int ei0 = max(X0 - 1, mi0), ei1 = min(X1 + 1, mi1);
+        const int ej0 = max(Y0 - 1, mj0), ej1 = min(Y1 + 1, mj1);
+        const bool sxl = !pr.xl && X0 == 0, sxh = !pr.xh && X1 >= nx;
+        const bool syl = !pr.yl && Y0 == 0, syh = !pr.yh && Y1 >= ny;
         for (int c = 0; c < 4; ++c) {
             const int ci = colour_ci(c), cj = colour_cj(c);
-            for (int k = threadIdx.x; k < w * h; k += blockDim.x) {
-                const int i = i0 + k % w, j = j0 + k / w;
-                if ((i & 1) != ci || (j & 1) != cj) continue;
-                const int xr = region(i, nx, pr.xl, pr.xh), yr = region(j, ny, pr.yl, pr.yh);
-                if ((xr == RMID) == (yr == RMID)) continue;   // edges only
-                gs9_tile(t, g.idx, g.idy, b, homog, i, j, xr, yr, omega);
+            const int ia = ei0 + ((ei0 & 1) != ci), ja = ej0 + ((ej0 & 1) != cj);
+            const int ni = (ei1 > ia) ? (ei1 - ia + 1) / 2 : 0, nj = (ej1 > ja) ? (ej1 - ja + 1) / 2 : 0;
+            const int n0 = (syl && cj == 0) ? ni : 0;
+            const int n1 = n0 + ((syh && ((ny - 1) & 1) == cj) ? ni : 0);
+            const int n2 = n1 + ((sxl && ci == 0) ? nj : 0);
+            const int n3 = n2 + ((sxh && ((nx - 1) & 1) == ci) ? nj : 0);
+            for (int k = threadIdx.x; k < n3; k += blockDim.x) {
+                if (k < n0) gs9_tile(t, g.idx, g.idy, b, homog, ia + 2 * k, 0, RMID, RLO, omega);
+                else if (k < n1) gs9_tile(t, g.idx, g.idy, b, homog, ia + 2 * (k - n0), ny - 1, RMID, RHI, omega);
+                else if (k < n2) gs9_tile(t, g.idx, g.idy, b, homog, 0, ja + 2 * (k - n1), RLO, RMID, omega);
+                else gs9_tile(t, g.idx, g.idy, b, homog, nx - 1, ja + 2 * (k - n2), RHI, RMID, omega);
             }
             __syncthreads();
         }
@@ -206,10 +324,11 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep9(DF pin, DF pout, DF rh
     //    leaves: filled at the start of the sweep)
     const int wi0 = (X0 == 0) ? -1 : X0, wi1 = (X1 >= nx) ? nx + 1 : X1;
     const int wj0 = (Y0 == 0) ? -1 : Y0, wj1 = (Y1 >= ny) ? ny + 1 : Y1;
-    const int ww = wi1 - wi0, wh = wj1 - wj0;
-    for (int k = threadIdx.x; k < ww * wh; k += blockDim.x) {
-        const int i = wi0 + k % ww, j = wj0 + k / ww;
-        AT(pout, i, j) = t.ph[(j - t.poy) * PW + (i - t.pox)];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int j = wj0 + warp; j < wj1; j += (blockDim.x >> 5)) {
+        const double* srow = smem + (j - t.poy) * PW - t.pox;
+        double* grow = &AT(pout, 0, j);
+        for (int i = wi0 + lane; i < wi1; i += 32) grow[i] = srow[i];
     }
 }
 
@@ -223,16 +342,92 @@ bool sweep_fusable(const BCd& b) {
     return true;
 }
 
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// A FP64 2-D map of `width` x `height` elements at `base`, row pitch ld, box PW x PH.
+bool encode(CUtensorMap* m, const double* base, long width, long height, int ld) {
+    const PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+    if (!fn || ((uintptr_t)base & 15) || (((long)ld * 8) & 15) || width > ld || width <= 0 || height <= 0) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)width, (cuuint64_t)height};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 8};
+    const cuuint32_t box[2] = {PW, PH};
+    const cuuint32_t es[2] = {1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool prepare_maps(SweepMaps* m, const DF& e, const DF& rhs, const DF& invd, const Geo& g, int nx, int ny) {
+    // phi from column -2 (an even offset keeps x even) and row -1; the ghost column nx must lie inside
+    m->pcb = -2;
+    m->prb = -1;
+    if (e.ld < nx + 3) return false;
+    return encode(&m->pin, &AT(e, -2, -1), e.ld, ny + 2, e.ld) && encode(&m->rhs, rhs.p, nx, ny, rhs.ld) &&
+           encode(&m->invd, invd.p, nx, ny, invd.ld) && encode(&m->xx, g.xx.p, nx + 1, ny, g.xx.ld) &&
+           encode(&m->xy, g.xy.p, nx + 1, ny, g.xy.ld) && encode(&m->yx, g.yx.p, nx, ny + 1, g.yx.ld) &&
+           encode(&m->yy, g.yy.p, nx, ny + 1, g.yy.ld);
+}
+
+// Per-device: dynamic shared memory above 48 KB must be opted into.
+cudaError_t set_smem_attr() {
+    static std::mutex mu;
+    static unsigned long long done = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 64 && (done >> dev) & 1ull) return cudaSuccess;
+    e = cudaFuncSetAttribute(k_sweep9<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sweep9<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+    if (e == cudaSuccess && dev < 64) done |= 1ull << dev;
+    return e;
+}
+
+}  // namespace
+
+void sweep_tma_prepare(SweepTma* t, const DF& ea, const DF& eb, const DF& rhs, const DF& invd, const Geo& g, int nx,
+                       int ny) {
+    t->ok = prepare_maps(&t->ma, ea, rhs, invd, g, nx, ny) && prepare_maps(&t->mb, eb, rhs, invd, g, nx, ny);
+    t->pa = ea.p;
+    t->pb = eb.p;
+    t->rhs = rhs.p;
+    t->invd = invd.p;
+    t->xx = g.xx.p;
+}
+
 cudaError_t launch_sweep9(const DF& pin, const DF& pout, const DF& rhs, const DF& invd, const Geo& g, const BCd& b,
-                          int homog, int nx, int ny, double omega, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_sweep9, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+                          int homog, int nx, int ny, double omega, const SweepTma* tma, int* status,
+                          cudaStream_t st) {
+    cudaError_t e = set_smem_attr();
+    if (e != cudaSuccess) return e;
+    const SweepMaps* m = nullptr;
+    if (tma && tma->ok && rhs.p == tma->rhs && invd.p == tma->invd && g.xx.p == tma->xx)
+        m = (pin.p == tma->pa) ? &tma->ma : (pin.p == tma->pb) ? &tma->mb : nullptr;
     dim3 grd((nx + kTX - 1) / kTX, (ny + kTY - 1) / kTY);
-    k_sweep9<<<grd, kSweepThreads, kSmemBytes, st>>>(pin, pout, rhs, invd, g, b, homog, nx, ny, omega);
+    if (m) {
+        k_sweep9<true><<<grd, kSweepThreads, kSmemBytes, st>>>(*m, pin, pout, rhs, invd, g, b, homog, nx, ny, omega,
+                                                               status);
+    } else {
+        static const SweepMaps none{};
+        k_sweep9<false><<<grd, kSweepThreads, kSmemBytes, st>>>(none, pin, pout, rhs, invd, g, b, homog, nx, ny,
+                                                                omega, status);
+    }
     count_launch();
     return cudaGetLastError();
 }
