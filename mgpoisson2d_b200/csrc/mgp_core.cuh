@@ -232,14 +232,19 @@ __device__ __forceinline__ Per periodic_of(const BCd& b) {
     return p;
 }
 
+// L[phi] at (i,j) in regions (xr, yr); phi's ghosts must be set.
+__device__ __forceinline__ double apply9r(const DF& phi, const Geo& g, const BCd& b, int homog, int i, int j, int xr,
+                                          int yr) {
+    St9 s;
+    gather9(GLoad{&AT(phi, i, j), phi.ld}, xr, yr, s);
+    return lap9(s, g, i, j, xr, yr, b, homog);
+}
+
 // L[phi] at (i,j); phi's ghosts must be set.
 __device__ __forceinline__ double apply9(const DF& phi, const Geo& g, const BCd& b, int homog, int nx, int ny,
                                          int i, int j) {
     const Per pr = periodic_of(b);
-    const int xr = region(i, nx, pr.xl, pr.xh), yr = region(j, ny, pr.yl, pr.yh);
-    St9 s;
-    gather9(GLoad{&AT(phi, i, j), phi.ld}, xr, yr, s);
-    return lap9(s, g, i, j, xr, yr, b, homog);
+    return apply9r(phi, g, b, homog, i, j, region(i, nx, pr.xl, pr.xh), region(j, ny, pr.yl, pr.yh));
 }
 
 // Diagonal of the operator at (i,j) (compute_invdiags, P2:16-388), before inversion.
@@ -259,14 +264,75 @@ __device__ __forceinline__ double diag9(const Geo& g, const BCd& b, int homog, i
     return lap9(s, g, i, j, xr, yr, b, homog);
 }
 
-// One Gauss-Seidel update of (i,j) (P2:1768-1771).
-__device__ __forceinline__ void gs9(const DF& phi, const DF& rhs, const DF& invd, const Geo& g, const BCd& b,
-                                    int homog, int nx, int ny, int i, int j, double omega) {
-    const double lphi = apply9(phi, g, b, homog, nx, ny, i, j);
+// One Gauss-Seidel update of (i,j) in regions (xr, yr) (P2:1768-1771).
+__device__ __forceinline__ void gs9r(const DF& phi, const DF& rhs, const DF& invd, const Geo& g, const BCd& b,
+                                     int homog, int i, int j, int xr, int yr, double omega) {
+    const double lphi = apply9r(phi, g, b, homog, i, j, xr, yr);
     const double p = AT(phi, i, j);
     const double newphi = p + (AT(rhs, i, j) - lphi) * AT(invd, i, j);
     AT(phi, i, j) = omega * newphi + (1.0 - omega) * p;
 }
+
+// The same, regions from the position.
+__device__ __forceinline__ void gs9(const DF& phi, const DF& rhs, const DF& invd, const Geo& g, const BCd& b,
+                                    int homog, int nx, int ny, int i, int j, double omega) {
+    const Per pr = periodic_of(b);
+    gs9r(phi, rhs, invd, g, b, homog, i, j, region(i, nx, pr.xl, pr.xh), region(j, ny, pr.yl, pr.yh), omega);
+}
+
+// ---------------------------------------------------------------------------
+// The ghost values a Gauss-Seidel sweep starts from: fill_ghosts with
+// do_neum = .false. (P2:1556) for sides of type DIRI, NEUM (left as stored)
+// and PERIODIC, computed from interior values only, so all ghost cells can
+// be filled at once.  P(i,j) reads phi as it stands at the sweep start.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double ghost_diri(const BCd& b, int homog, int s, int k, double p0, double p1, double p2);
+
+// y-side ghost (i,j), 0 <= i < nx.
+template <class P>
+__device__ __forceinline__ double sweep_ghost_y(const P& p, const BCd& b, int homog, int ny, int i, int j) {
+    const int s = (j < 0) ? S_YLO : S_YHI;
+    const int t = b.type[s];
+    if (t == T_DIRI) {
+        const int jj = (j < 0) ? 0 : ny - 1, e = (j < 0) ? -1 : 1;
+        return ghost_diri(b, homog, s, i, p(i, jj), p(i, jj - e), p(i, jj - 2 * e));
+    }
+    if (t == T_PERIODIC) return p(i, (j < 0) ? ny - 1 : 0);
+    return p(i, j);
+}
+
+// x-side ghost (i,j), 0 <= j < ny.
+template <class P>
+__device__ __forceinline__ double sweep_ghost_x(const P& p, const BCd& b, int homog, int nx, int i, int j) {
+    const int s = (i < 0) ? S_XLO : S_XHI;
+    const int t = b.type[s];
+    if (t == T_DIRI) {
+        const int ii = (i < 0) ? 0 : nx - 1, e = (i < 0) ? -1 : 1;
+        return ghost_diri(b, homog, s, j, p(ii, j), p(ii - e, j), p(ii - 2 * e, j));
+    }
+    if (t == T_PERIODIC) return p((i < 0) ? nx - 1 : 0, j);
+    return p(i, j);
+}
+
+// Any ghost cell; corners as AU:1460-1490.
+template <class P>
+__device__ __forceinline__ double sweep_ghost(const P& p, const BCd& b, int homog, int nx, int ny, int i, int j) {
+    const bool xin = (i >= 0 && i < nx), yin = (j >= 0 && j < ny);
+    if (xin && !yin) return sweep_ghost_y(p, b, homog, ny, i, j);
+    if (yin && !xin) return sweep_ghost_x(p, b, homog, nx, i, j);
+    const bool px = b.type[S_XLO] == T_PERIODIC, py = b.type[S_YLO] == T_PERIODIC;
+    if (!px && !py) return kBogus;
+    const int wi = (i < 0) ? nx - 1 : 0, wj = (j < 0) ? ny - 1 : 0;
+    if (px && py) return p(wi, wj);
+    if (px) return sweep_ghost_y(p, b, homog, ny, wi, j);
+    return sweep_ghost_x(p, b, homog, nx, i, wj);
+}
+
+// Reads a field directly.
+struct DFLoad {
+    DF f;
+    __device__ __forceinline__ double operator()(int i, int j) const { return AT(f, i, j); }
+};
 
 // Colour c of the 4-colour sweep: (i mod 2, j mod 2) = (0,0), (1,1), (1,0), (0,1).
 __device__ __forceinline__ int colour_ci(int c) { return (c == 1 || c == 2) ? 1 : 0; }

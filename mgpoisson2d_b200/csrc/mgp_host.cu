@@ -257,6 +257,16 @@ struct mgp_solver {
     // search direction, A*y and A*z)
     DF kr{}, krh{}, kp{}, kv{}, kt{};
     std::vector<SweepTma> tma;   // per level, for the fused sweep
+    // V-cycles captured as CUDA graphs, keyed by their arguments and by which
+    // buffer holds e on each grid-path level when the cycle starts
+    struct VGraph {
+        int d, numcycles, nd, nu, nb;
+        std::vector<double*> e_in, e_out;
+        cudaGraphExec_t exec;
+        long long launches;
+    };
+    std::vector<VGraph> graphs;
+    cudaStream_t cap = nullptr;   // capture-only stream
     double* d_bcbuf = nullptr;
     double* d_red = nullptr;    // reduction partials + outputs
     double* h_red = nullptr;    // pinned
@@ -284,6 +294,8 @@ void solver_free(mgp_solver* s) {
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     for (cudaEvent_t e : s->tev) cudaEventDestroy(e);
+    for (auto& g : s->graphs) cudaGraphExecDestroy(g.exec);
+    if (s->cap) cudaStreamDestroy(s->cap);
     s->fixed.release();
     s->state.release();
     delete s;
@@ -590,6 +602,67 @@ int fmg_noinit(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
     return MGP_OK;
 }
 
+// vcycle_noinit(d) replayed from a CUDA graph: the first call with a given
+// key captures the cycle's launches (on a capture-only stream, so nothing
+// runs), later calls launch the graph on the solver's stream.  The host-side
+// e/e2 buffer swaps the capture made are applied again after every replay.
+// Off when the level-0 smoothing is timed with events.
+int vcycle_run(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
+    if ((s->flags & MGP_FLAG_TIME_SMOOTHER) || d >= s->dc) return vcycle_noinit(s, d, numcycles, nd, nu, nb);
+    std::vector<double*> cur;
+    for (int k = d; k < s->dc; ++k) cur.push_back(s->lv[k].e.p);
+    auto apply_out = [&](const mgp_solver::VGraph& g) {
+        for (int k = d; k < s->dc; ++k) {
+            Lv& L = s->lv[k];
+            if (L.e.p != g.e_out[k - d]) std::swap(L.e, L.e2);
+        }
+    };
+    for (const auto& g : s->graphs) {
+        if (g.d == d && g.numcycles == numcycles && g.nd == nd && g.nu == nu && g.nb == nb && g.e_in == cur) {
+            CK(cudaGraphLaunch(g.exec, s->stream));
+            count_launch((int)g.launches);
+            apply_out(g);
+            return MGP_OK;
+        }
+    }
+    CK(sweep_kernels_init());
+    CK(coarse_kernels_init());
+    if (!s->cap) CK(cudaStreamCreateWithFlags(&s->cap, cudaStreamNonBlocking));
+    const cudaStream_t saved = s->stream;
+    const long long l0 = launch_count();
+    s->stream = s->cap;
+    CK(cudaStreamBeginCapture(s->cap, cudaStreamCaptureModeThreadLocal));
+    const int rc = vcycle_noinit(s, d, numcycles, nd, nu, nb);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(s->cap, &graph);
+    s->stream = saved;
+    mgp_solver::VGraph g{d, numcycles, nd, nu, nb, cur, {}, nullptr, launch_count() - l0};
+    for (int k = d; k < s->dc; ++k) g.e_out.push_back(s->lv[k].e.p);
+    // the capture ran nothing: put the buffers back as they were
+    for (int k = d; k < s->dc; ++k) {
+        Lv& L = s->lv[k];
+        if (L.e.p != cur[k - d]) std::swap(L.e, L.e2);
+    }
+    count_launch((int)-g.launches);
+    if (rc || ce != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        if (rc) return rc;
+        return set_err(MGP_ECUDA, "V-cycle graph capture failed: %s", cudaGetErrorString(ce));
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(MGP_ECUDA, "V-cycle graph instantiation failed: %s", cudaGetErrorString(ie));
+    }
+    s->graphs.push_back(g);
+    CK(cudaGraphLaunch(g.exec, s->stream));
+    count_launch((int)g.launches);
+    apply_out(g);
+    return MGP_OK;
+}
+
 // dst = src over the valid region of level 0.
 int copy_valid(const DF& dst, const DF& src, int nx, int ny, cudaStream_t st) {
     CK(cudaMemcpy2DAsync(dst.p, dst.ld * sizeof(double), src.p, src.ld * sizeof(double), nx * sizeof(double), ny,
@@ -625,7 +698,7 @@ int krylov_loop(mgp_solver* s, const BCd& ubc, int homog, double tol, int maxite
     auto precond_apply = [&](const DF& x, const DF& Ay) -> int {
         RC(copy_valid(L0.r, x, nx, ny, st));
         CK(launch_set_guess(L0.e, L0.r, L0.invd, nx, ny, st));
-        RC(vcycle_noinit(s, 0, numcycles, nd, nu, nb));
+        RC(vcycle_run(s, 0, numcycles, nd, nu, nb));
         CK(launch_fill(L0.e, L0.g, L0.bc, 1, 0, nx, ny, st));
         CK(launch_apply(Ay, L0.e, L0.r, L0.g, L0.bc, 1, nx, ny, 0, 0, st));
         return MGP_OK;
@@ -747,7 +820,7 @@ int solver_solve(mgp_solver* s, int which, mgp_array* phi, mgp_array* rhs, const
     for (int iter = 1; !krylov && iter <= maxiters && status == MGP_OK; ++iter) {
         if (which == 0) CK(launch_set_guess(L0.e, L0.r, L0.invd, nx, ny, st));   // MG:600
         if (which == 1) RC(fmg_noinit(s, 0, numcycles, nd, nu, nb));
-        else RC(vcycle_noinit(s, 0, numcycles, nd, nu, nb));
+        else RC(vcycle_run(s, 0, numcycles, nd, nu, nb));
         CK(launch_axpby(s->phi0, L0.e, 1.0, 1.0, nx, ny, 1, 1, st));   // MG:611 (whole array)
         CK(launch_fill(s->phi0, L0.g, ubc, homog, 0, nx, ny, st));
         CK(launch_apply(L0.r, s->phi0, s->rhs0, L0.g, ubc, homog, nx, ny, 1, 0, st));

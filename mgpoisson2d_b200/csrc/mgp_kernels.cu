@@ -9,6 +9,8 @@
 // bits as each other and as the Fortran loop bodies.
 #include <atomic>
 
+#include <mutex>
+
 #include "mgp_kernels.cuh"
 
 namespace mgp {
@@ -654,8 +656,77 @@ __device__ void b_mul(const DF& out, const DF& a, const DF& c, int nx, int ny) {
 }
 
 // 9-point sweeps (MG smoother), P2:1460-1988.
+// One sweep in the device order by the whole block, for sides of type DIRI,
+// NEUM and PERIODIC: the sweep-start ghost fill in one pass (every ghost
+// depends on interior values only), the interior colours over precomputed
+// ranges, the edge cells colour by colour along each non-periodic side, then
+// the corners -- at once when the grid is at least 4 x 4 (their stencils,
+// two cells deep, then neither read nor write each other), else in turn.
+__device__ void b_sweep9(const DF& phi, const DF& rhs, const DF& invd, const Geo& g, const BCd& b, int homog, int nx,
+                         int ny, double omega) {
+    const Per pr = periodic_of(b);
+    const int ng = 2 * (nx + 2) + 2 * ny;
+    BLOOP(k, ng) {
+        int i, j;
+        if (k < nx + 2) { i = k - 1; j = -1; }
+        else if (k < 2 * (nx + 2)) { i = k - (nx + 2) - 1; j = ny; }
+        else if (k < 2 * (nx + 2) + ny) { i = -1; j = k - 2 * (nx + 2); }
+        else { i = nx; j = k - 2 * (nx + 2) - ny; }
+        AT(phi, i, j) = sweep_ghost(DFLoad{phi}, b, homog, nx, ny, i, j);
+    }
+    __syncthreads();
+    const int mi0 = pr.xl ? 0 : 1, mi1 = pr.xh ? nx : nx - 1;
+    const int mj0 = pr.yl ? 0 : 1, mj1 = pr.yh ? ny : ny - 1;
+    for (int c = 0; c < 4; ++c) {
+        const int ci = colour_ci(c), cj = colour_cj(c);
+        const int i0 = mi0 + ((mi0 & 1) != ci), j0 = mj0 + ((mj0 & 1) != cj);
+        const int cw = (mi1 > i0) ? (mi1 - i0 + 1) / 2 : 0, ch = (mj1 > j0) ? (mj1 - j0 + 1) / 2 : 0;
+        BLOOP(k, cw * ch) {
+            const int kj = k / cw;
+            gs9r(phi, rhs, invd, g, b, homog, i0 + 2 * (k - kj * cw), j0 + 2 * kj, RMID, RMID, omega);
+        }
+        __syncthreads();
+    }
+    const bool sxl = !pr.xl, sxh = !pr.xh, syl = !pr.yl, syh = !pr.yh;
+    for (int c = 0; c < 4; ++c) {
+        const int ci = colour_ci(c), cj = colour_cj(c);
+        const int ia = mi0 + ((mi0 & 1) != ci), ja = mj0 + ((mj0 & 1) != cj);
+        const int ni = (mi1 > ia) ? (mi1 - ia + 1) / 2 : 0, nj = (mj1 > ja) ? (mj1 - ja + 1) / 2 : 0;
+        const int n0 = (syl && cj == 0) ? ni : 0;
+        const int n1 = n0 + ((syh && ((ny - 1) & 1) == cj) ? ni : 0);
+        const int n2 = n1 + ((sxl && ci == 0) ? nj : 0);
+        const int n3 = n2 + ((sxh && ((nx - 1) & 1) == ci) ? nj : 0);
+        BLOOP(k, n3) {
+            if (k < n0) gs9r(phi, rhs, invd, g, b, homog, ia + 2 * k, 0, RMID, RLO, omega);
+            else if (k < n1) gs9r(phi, rhs, invd, g, b, homog, ia + 2 * (k - n0), ny - 1, RMID, RHI, omega);
+            else if (k < n2) gs9r(phi, rhs, invd, g, b, homog, 0, ja + 2 * (k - n1), RLO, RMID, omega);
+            else gs9r(phi, rhs, invd, g, b, homog, nx - 1, ja + 2 * (k - n2), RHI, RMID, omega);
+        }
+        __syncthreads();
+    }
+    const bool apart = nx >= 4 && ny >= 4;
+    if (apart ? threadIdx.x < 4 : threadIdx.x == 0) {
+        for (int c = apart ? threadIdx.x : 0; c < (apart ? (int)threadIdx.x + 1 : 4); ++c) {
+            const int i = (c & 1) ? nx - 1 : 0, j = (c & 2) ? ny - 1 : 0;
+            const int xr = region(i, nx, pr.xl, pr.xh), yr = region(j, ny, pr.yl, pr.yh);
+            if (xr != RMID && yr != RMID) gs9r(phi, rhs, invd, g, b, homog, i, j, xr, yr, omega);
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ bool fusable_sides(const BCd& b) {
+    for (int s = 0; s < 4; ++s)
+        if (b.type[s] != T_DIRI && b.type[s] != T_NEUM && b.type[s] != T_PERIODIC) return false;
+    return true;
+}
+
 __device__ void b_relax9(const Lv& L, const DF& phi, const DF& rhs, int homog, double omega, int sweeps) {
     const int nx = L.nx, ny = L.ny;
+    if (fusable_sides(L.bc)) {
+        for (int it = 0; it < sweeps; ++it) b_sweep9(phi, rhs, L.invd, L.g, L.bc, homog, nx, ny, omega);
+        return;
+    }
     const int hx = (nx + 1) / 2, hy = (ny + 1) / 2;
     const Per pr = periodic_of(L.bc);
     for (int it = 0; it < sweeps; ++it) {
@@ -953,15 +1024,24 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse_cycle_smem(CoarseArgs
     if (threadIdx.x == 0 && s) *a.status = s;
 }
 
+// Per device: opt the shared-memory coarse kernel into its largest window.
+cudaError_t coarse_kernels_init() {
+    static std::mutex mu;
+    static unsigned long long done = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 64 && ((done >> dev) & 1ull)) return cudaSuccess;
+    e = cudaFuncSetAttribute(k_coarse_cycle_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, kCoarseSmemMax);
+    if (e == cudaSuccess && dev < 64) done |= 1ull << dev;
+    return e;
+}
+
 cudaError_t launch_coarse_cycle(const CoarseArgs& a, cudaStream_t st) {
     if (a.shadow && a.smem_bytes > 0) {
-        static int attr_bytes = 0;
-        if (attr_bytes < a.smem_bytes) {
-            cudaError_t e = cudaFuncSetAttribute(k_coarse_cycle_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 a.smem_bytes);
-            if (e != cudaSuccess) return e;
-            attr_bytes = a.smem_bytes;
-        }
+        const cudaError_t e = coarse_kernels_init();
+        if (e != cudaSuccess) return e;
         k_coarse_cycle_smem<<<1, kCoarseThreads, a.smem_bytes, st>>>(a);
     } else {
         k_coarse_cycle<<<1, kCoarseThreads, 0, st>>>(a);

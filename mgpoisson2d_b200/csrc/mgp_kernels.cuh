@@ -106,6 +106,9 @@ cudaError_t launch_dd_modrhs(const DF& out, const DF& phi, const DF& rhs, const 
                              cudaStream_t st);
 cudaError_t launch_dd_colour(const DF& phi, const DF& modrhs, const DF& invd, const Geo& g, int nx, int ny,
                              double omega, int colour, cudaStream_t st);
+// Per-device kernel attributes (idempotent; call before any stream capture).
+cudaError_t sweep_kernels_init();
+cudaError_t coarse_kernels_init();
 // Single-CTA kernels.
 cudaError_t launch_coarse_cycle(const CoarseArgs& a, cudaStream_t st);
 cudaError_t launch_bicgstab(const BicgArgs& a, cudaStream_t st);

@@ -74,44 +74,6 @@ struct PinLoad {
     }
 };
 
-// The value fill_ghosts (do_neum = .false.) gives the y-side ghost (i,j),
-// 0 <= i < nx, for sides of type DIRI, NEUM (left as stored) and PERIODIC.
-__device__ __forceinline__ double ghost_yside(const PinLoad& P, const BCd& b, int homog, int ny, int i, int j) {
-    const int s = (j < 0) ? S_YLO : S_YHI;
-    const int t = b.type[s];
-    if (t == T_DIRI) {
-        const int jj = (j < 0) ? 0 : ny - 1, e = (j < 0) ? -1 : 1;
-        return ghost_diri(b, homog, s, i, P(i, jj), P(i, jj - e), P(i, jj - 2 * e));
-    }
-    if (t == T_PERIODIC) return P(i, (j < 0) ? ny - 1 : 0);
-    return P(i, j);
-}
-
-// The same for the x-side ghost (i,j), 0 <= j < ny.
-__device__ __forceinline__ double ghost_xside(const PinLoad& P, const BCd& b, int homog, int nx, int i, int j) {
-    const int s = (i < 0) ? S_XLO : S_XHI;
-    const int t = b.type[s];
-    if (t == T_DIRI) {
-        const int ii = (i < 0) ? 0 : nx - 1, e = (i < 0) ? -1 : 1;
-        return ghost_diri(b, homog, s, j, P(ii, j), P(ii - e, j), P(ii - 2 * e, j));
-    }
-    if (t == T_PERIODIC) return P((i < 0) ? nx - 1 : 0, j);
-    return P(i, j);
-}
-
-// Any ghost cell; corners as AU:1460-1490.
-__device__ double sweep_ghost(const PinLoad& P, const BCd& b, int homog, int nx, int ny, int i, int j) {
-    const bool xin = (i >= 0 && i < nx), yin = (j >= 0 && j < ny);
-    if (xin && !yin) return ghost_yside(P, b, homog, ny, i, j);
-    if (yin && !xin) return ghost_xside(P, b, homog, nx, i, j);
-    const bool px = b.type[S_XLO] == T_PERIODIC, py = b.type[S_YLO] == T_PERIODIC;
-    if (!px && !py) return kBogus;
-    const int wi = (i < 0) ? nx - 1 : 0, wj = (j < 0) ? ny - 1 : 0;
-    if (px && py) return P(wi, wj);
-    if (px) return ghost_yside(P, b, homog, ny, wi, j);
-    return ghost_xside(P, b, homog, nx, i, wj);
-}
-
 // Copy rows [j0,j1) x columns [i0,i1) of a global field into a shared array
 // whose (0,0) is cell (ox, oy) and whose row pitch is w.  Warp w8 takes rows
 // j0 + w8, j0 + w8 + 8, ...; where a row's global and shared addresses have
@@ -383,8 +345,10 @@ bool prepare_maps(SweepMaps* m, const DF& e, const DF& rhs, const DF& invd, cons
            encode(&m->yy, g.yy.p, nx, ny + 1, g.yy.ld);
 }
 
-// Per-device: dynamic shared memory above 48 KB must be opted into.
-cudaError_t set_smem_attr() {
+}  // namespace
+
+// Per device: dynamic shared memory above 48 KB must be opted into.
+cudaError_t sweep_kernels_init() {
     static std::mutex mu;
     static unsigned long long done = 0;
     int dev = 0;
@@ -399,8 +363,6 @@ cudaError_t set_smem_attr() {
     return e;
 }
 
-}  // namespace
-
 void sweep_tma_prepare(SweepTma* t, const DF& ea, const DF& eb, const DF& rhs, const DF& invd, const Geo& g, int nx,
                        int ny) {
     t->ok = prepare_maps(&t->ma, ea, rhs, invd, g, nx, ny) && prepare_maps(&t->mb, eb, rhs, invd, g, nx, ny);
@@ -414,7 +376,7 @@ void sweep_tma_prepare(SweepTma* t, const DF& ea, const DF& eb, const DF& rhs, c
 cudaError_t launch_sweep9(const DF& pin, const DF& pout, const DF& rhs, const DF& invd, const Geo& g, const BCd& b,
                           int homog, int nx, int ny, double omega, const SweepTma* tma, int* status,
                           cudaStream_t st) {
-    cudaError_t e = set_smem_attr();
+    cudaError_t e = sweep_kernels_init();
     if (e != cudaSuccess) return e;
     const SweepMaps* m = nullptr;
     if (tma && tma->ok && rhs.p == tma->rhs && invd.p == tma->invd && g.xx.p == tma->xx)
