@@ -331,16 +331,23 @@ def main():
     if rank == 0 and not args.no_e2e:
         # end to end through the reference-facing call: host arrays, hierarchy
         # built inside the call (mgp_vcycle has the Fortran argument list)
-        phi_h = BoxData(v, 1, 1)
+        # one untimed call, then the median of up to three timed calls
         M.set_flags(flags)
-        t0 = time.perf_counter()
-        erep = M.vcycle(phi_h, rhs, geo, bc, True, TOL, MAXITERS, -1, 1, *NU)
-        e2e_s = time.perf_counter() - t0
+        times = []
+        for k in range(1 + min(args.steps, 3)):
+            phi_h = BoxData(v, 1, 1)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            erep = M.vcycle(phi_h, rhs, geo, bc, True, TOL, MAXITERS, -1, 1, *NU)
+            if k:
+                times.append(time.perf_counter() - t0)
         M.set_flags(0)
+        e2e_s = sorted(times)[len(times) // 2]
         h2d = 8 * (phi_h.data.size + rhs.data.size + v.nx * v.ny + 4 * (v.nx + 1) * v.ny)
         line["e2e"] = {"value": 1.0 / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d,
-                       "d2h_bytes_per_step": 8 * phi_h.data.size, "api": "mgp_vcycle (host arrays)",
-                       "vcycles": erep.iterations}
+                       "d2h_bytes_per_step": 8 * phi_h.data.size,
+                       "api": "mgp_vcycle (host arrays; hierarchy built inside the call)",
+                       "vcycles": erep.iterations, "timed_calls": len(times), "stat": "median"}
     if rank == 0 and world == 1 and not args.no_cpu:
         tvc, nvc = cpu_sample(args.n, args.cpu_vcycles)
         iters = solve_vcycles_estimate(args.n)
