@@ -334,6 +334,16 @@ struct DFLoad {
     __device__ __forceinline__ double operator()(int i, int j) const { return AT(f, i, j); }
 };
 
+// k / d by a multiply: exact for 0 <= k < 65536 and 1 <= d <= 1024 (every
+// pair checked on the host).  The magic number costs one divide; compute it
+// off the critical path.
+__device__ __forceinline__ unsigned long long fastdiv_magic(int d) {
+    return ((1ull << 32) + (unsigned)d - 1) / (unsigned)d;
+}
+__device__ __forceinline__ int fastdiv(int k, unsigned long long m) {
+    return (int)(((unsigned long long)(unsigned)k * m) >> 32);
+}
+
 // Colour c of the 4-colour sweep: (i mod 2, j mod 2) = (0,0), (1,1), (1,0), (0,1).
 __device__ __forceinline__ int colour_ci(int c) { return (c == 1 || c == 2) ? 1 : 0; }
 __device__ __forceinline__ int colour_cj(int c) { return (c == 1 || c == 3) ? 1 : 0; }

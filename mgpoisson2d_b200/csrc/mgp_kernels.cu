@@ -665,6 +665,19 @@ __device__ void b_mul(const DF& out, const DF& a, const DF& c, int nx, int ny) {
 __device__ void b_sweep9(const DF& phi, const DF& rhs, const DF& invd, const Geo& g, const BCd& b, int homog, int nx,
                          int ny, double omega) {
     const Per pr = periodic_of(b);
+    const int mi0 = pr.xl ? 0 : 1, mi1 = pr.xh ? nx : nx - 1;
+    const int mj0 = pr.yl ? 0 : 1, mj1 = pr.yh ? ny : ny - 1;
+    // interior colour ranges and their divide-free index maps, set up before the fill
+    int ci0[4], cj0[4], ccw[4], cnt[4];
+    unsigned long long cm[4];
+    for (int c = 0; c < 4; ++c) {
+        ci0[c] = mi0 + ((mi0 & 1) != colour_ci(c));
+        cj0[c] = mj0 + ((mj0 & 1) != colour_cj(c));
+        ccw[c] = (mi1 > ci0[c]) ? (mi1 - ci0[c] + 1) / 2 : 0;
+        const int ch = (mj1 > cj0[c]) ? (mj1 - cj0[c] + 1) / 2 : 0;
+        cnt[c] = ccw[c] * ch;
+        cm[c] = fastdiv_magic(ccw[c] > 0 ? ccw[c] : 1);
+    }
     const int ng = 2 * (nx + 2) + 2 * ny;
     BLOOP(k, ng) {
         int i, j;
@@ -675,15 +688,11 @@ __device__ void b_sweep9(const DF& phi, const DF& rhs, const DF& invd, const Geo
         AT(phi, i, j) = sweep_ghost(DFLoad{phi}, b, homog, nx, ny, i, j);
     }
     __syncthreads();
-    const int mi0 = pr.xl ? 0 : 1, mi1 = pr.xh ? nx : nx - 1;
-    const int mj0 = pr.yl ? 0 : 1, mj1 = pr.yh ? ny : ny - 1;
+#pragma unroll
     for (int c = 0; c < 4; ++c) {
-        const int ci = colour_ci(c), cj = colour_cj(c);
-        const int i0 = mi0 + ((mi0 & 1) != ci), j0 = mj0 + ((mj0 & 1) != cj);
-        const int cw = (mi1 > i0) ? (mi1 - i0 + 1) / 2 : 0, ch = (mj1 > j0) ? (mj1 - j0 + 1) / 2 : 0;
-        BLOOP(k, cw * ch) {
-            const int kj = k / cw;
-            gs9r(phi, rhs, invd, g, b, homog, i0 + 2 * (k - kj * cw), j0 + 2 * kj, RMID, RMID, omega);
+        BLOOP(k, cnt[c]) {
+            const int kj = fastdiv(k, cm[c]);
+            gs9r(phi, rhs, invd, g, b, homog, ci0[c] + 2 * (k - kj * ccw[c]), cj0[c] + 2 * kj, RMID, RMID, omega);
         }
         __syncthreads();
     }
@@ -964,7 +973,7 @@ finish:
     goto up;
 }
 
-__global__ void __launch_bounds__(kCoarseThreads) k_coarse_cycle(CoarseArgs a) {
+__global__ void __launch_bounds__(kCoarseThreads, 1) k_coarse_cycle(CoarseArgs a) {
     __shared__ double sh[kCoarseThreads];
     const int s = coarse_body(a.lv, a, sh);
     if (threadIdx.x == 0 && s) *a.status = s;
@@ -986,7 +995,7 @@ __device__ __forceinline__ void rebase(DF& f, double* base) { f.p = base + (size
 // The same cycle with every coarse level held in shared memory: the levels'
 // arrays are copied in (the corrections with their ghosts, the operands, the
 // finest level's right-hand side), the cycle runs, the corrections go back.
-__global__ void __launch_bounds__(kCoarseThreads) k_coarse_cycle_smem(CoarseArgs a) {
+__global__ void __launch_bounds__(kCoarseThreads, 1) k_coarse_cycle_smem(CoarseArgs a) {
     extern __shared__ double smem[];
     __shared__ double sh[kCoarseThreads];
     __shared__ Lv sl[kMaxCoarseLevels];
@@ -1050,7 +1059,7 @@ cudaError_t launch_coarse_cycle(const CoarseArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-__global__ void __launch_bounds__(kCoarseThreads) k_bicgstab(BicgArgs a) {
+__global__ void __launch_bounds__(kCoarseThreads, 1) k_bicgstab(BicgArgs a) {
     __shared__ double sh[kCoarseThreads];
     const int s = b_bicgstab(a.L, a.phi, a.rhs, a.homog, a.tol, a.max_iters, a.max_restarts, a.zerophi, a.dd, sh);
     if (threadIdx.x == 0 && s) *a.status = s;

@@ -132,6 +132,27 @@ __device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map
         : "memory");
 }
 
+// Interior colour c on the tile grown by (3 - c + E): first cell (ci0, cj0),
+// cw cells per row, n cells, and the magic number for k / cw.
+__device__ __forceinline__ void colour_ranges(int X0, int X1, int Y0, int Y1, int E, int mi0, int mi1, int mj0,
+                                              int mj1, int* ci0, int* cj0, int* ccw, int* cn,
+                                              unsigned long long* cm) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int grow = 3 - c + E;
+        int i0 = max(X0 - grow, mi0), i1 = min(X1 + grow, mi1);
+        int j0 = max(Y0 - grow, mj0), j1 = min(Y1 + grow, mj1);
+        i0 += (i0 & 1) != colour_ci(c);
+        j0 += (j0 & 1) != colour_cj(c);
+        const int cw = (i1 - i0 + 1) / 2, ch = (j1 - j0 + 1) / 2;
+        ci0[c] = i0;
+        cj0[c] = j0;
+        ccw[c] = cw;
+        cn[c] = (cw > 0 && ch > 0) ? cw * ch : 0;
+        cm[c] = fastdiv_magic(cw > 0 ? cw : 1);
+    }
+}
+
 struct Tile {
     double* s;   // seven arrays of PW x PH, origin (pox, poy)
     int pox, poy;
@@ -169,10 +190,17 @@ __global__ void __launch_bounds__(kSweepThreads, 2)
     t.s = smem;
     t.pox = (X0 - kH) & ~1; t.poy = Y0 - kH;
 
+    // interior colour ranges (i in [mi0, mi1), j in [mj0, mj1)) on shrinking
+    // regions, and their divide-free index maps, set up while the loads fly
+    const int mi0 = pr.xl ? 0 : 1, mi1 = pr.xh ? nx : nx - 1;
+    const int mj0 = pr.yl ? 0 : 1, mj1 = pr.yh ? ny : ny - 1;
+    int ci0[4], cj0[4], ccw[4], cn[4];
+    unsigned long long cm[4];
+
     // 1. stage phi on tile + (4 + E) and the operands on tile + (3 + E)
     const int hp = 4 + E, hc = 3 + E;
     const int pi0 = max(X0 - hp, -1), pi1 = min(X1 + hp, nx + 1), pj0 = max(Y0 - hp, -1), pj1 = min(Y1 + hp, ny + 1);
-    const int ci0 = max(X0 - hc, 0), ci1 = min(X1 + hc, nx), cj0 = max(Y0 - hc, 0), cj1 = min(Y1 + hc, ny);
+    const int ci0s = max(X0 - hc, 0), ci1s = min(X1 + hc, nx), cj0s = max(Y0 - hc, 0), cj1s = min(Y1 + hc, ny);
     if (kTma) {
         // the whole window of every array; what lies outside a field reads as 0 and is never used
         const unsigned sb = (unsigned)__cvta_generic_to_shared(smem), bar = sb + oBar * 8;
@@ -192,6 +220,7 @@ __global__ void __launch_bounds__(kSweepThreads, 2)
             tma_load_2d(sb + oYX * 8, &m.yx, t.pox, t.poy, bar);
             tma_load_2d(sb + oYY * 8, &m.yy, t.pox, t.poy, bar);
         }
+        colour_ranges(X0, X1, Y0, Y1, E, mi0, mi1, mj0, mj1, ci0, cj0, ccw, cn, cm);
         if (!mbar_wait0(bar)) {   // never seen; leave the tile unwritten and report
             if (status) atomicExch(status, 2);
             mbar_wait0(bar);      // let copies still in flight land before the CTA exits
@@ -199,12 +228,13 @@ __global__ void __launch_bounds__(kSweepThreads, 2)
         }
     } else {
         stage(smem, PW, t.pox, t.poy, pin, pi0, pi1, pj0, pj1);
-        stage(smem + oF, PW, t.pox, t.poy, rhs, ci0, ci1, cj0, cj1);
-        stage(smem + oD, PW, t.pox, t.poy, invd, ci0, ci1, cj0, cj1);
-        stage(smem + oXX, PW, t.pox, t.poy, g.xx, ci0, ci1 + 1, cj0, cj1);
-        stage(smem + oXY, PW, t.pox, t.poy, g.xy, ci0, ci1 + 1, cj0, cj1);
-        stage(smem + oYX, PW, t.pox, t.poy, g.yx, ci0, ci1, cj0, cj1 + 1);
-        stage(smem + oYY, PW, t.pox, t.poy, g.yy, ci0, ci1, cj0, cj1 + 1);
+        stage(smem + oF, PW, t.pox, t.poy, rhs, ci0s, ci1s, cj0s, cj1s);
+        stage(smem + oD, PW, t.pox, t.poy, invd, ci0s, ci1s, cj0s, cj1s);
+        stage(smem + oXX, PW, t.pox, t.poy, g.xx, ci0s, ci1s + 1, cj0s, cj1s);
+        stage(smem + oXY, PW, t.pox, t.poy, g.xy, ci0s, ci1s + 1, cj0s, cj1s);
+        stage(smem + oYX, PW, t.pox, t.poy, g.yx, ci0s, ci1s, cj0s, cj1s + 1);
+        stage(smem + oYY, PW, t.pox, t.poy, g.yy, ci0s, ci1s, cj0s, cj1s + 1);
+        colour_ranges(X0, X1, Y0, Y1, E, mi0, mi1, mj0, mj1, ci0, cj0, ccw, cn, cm);
         cp_async_wait_all();
         __syncthreads();
     }
@@ -228,20 +258,11 @@ __global__ void __launch_bounds__(kSweepThreads, 2)
     // 3. interior colour passes on shrinking regions.  Interior cells are
     //    i in [mi0, mi1), j in [mj0, mj1); one thread per cell of the colour
     //    (a pass has at most 21 x 21 of them).
-    const int mi0 = pr.xl ? 0 : 1, mi1 = pr.xh ? nx : nx - 1;
-    const int mj0 = pr.yl ? 0 : 1, mj1 = pr.yh ? ny : ny - 1;
-#pragma unroll 1
+#pragma unroll
     for (int c = 0; c < 4; ++c) {
-        const int ci = colour_ci(c), cj = colour_cj(c);
-        const int grow = 3 - c + E;
-        int i0 = max(X0 - grow, mi0), i1 = min(X1 + grow, mi1);
-        int j0 = max(Y0 - grow, mj0), j1 = min(Y1 + grow, mj1);
-        i0 += (i0 & 1) != ci;
-        j0 += (j0 & 1) != cj;
-        const int cw = (i1 - i0 + 1) / 2, chh = (j1 - j0 + 1) / 2;
-        for (int k = threadIdx.x; k < cw * chh; k += blockDim.x) {
-            const int kj = k / cw;
-            const int i = i0 + 2 * (k - kj * cw), j = j0 + 2 * kj;
+        for (int k = threadIdx.x; k < cn[c]; k += blockDim.x) {
+            const int kj = fastdiv(k, cm[c]);
+            const int i = ci0[c] + 2 * (k - kj * ccw[c]), j = cj0[c] + 2 * kj;
             gs9_tile(t, g.idx, g.idy, b, homog, i, j, RMID, RMID, omega);
         }
         __syncthreads();
