@@ -18,7 +18,8 @@
  *    which one each pointer is (cudaPointerGetAttributes).  Host arrays are
  *    staged through device buffers inside the call.
  *  - All arithmetic is IEEE FP64 without fused multiply-add, in the same
- *    operation order as the Fortran routines.
+ *    operation order as the Fortran routines (MGP_FLAG_MIXED, an opt-in
+ *    extension, runs the V-cycle's grid levels in FP32).
  *  - Every function returns an mgp_status (0 = MGP_OK).  Nothing calls exit();
  *    where the Fortran library prints and stops, this library returns an
  *    error code and records a message readable through mgp_last_error().
@@ -137,6 +138,13 @@ typedef struct mgp_report {
  * the Fortran vcycle is a stationary iteration only.  On strongly stretched
  * grids it needs several times fewer V-cycles for the same tolerance. */
 #define MGP_FLAG_KRYLOV 4
+/* vcycle only: run the V-cycle's grid levels (every level above the
+ * single-CTA coarse cycle) in FP32 inside the FP64 outer iteration.  The
+ * residual, the solution update, the convergence test and the coarse levels
+ * with the bottom solve stay FP64; geometry and inverse diagonals are the
+ * FP64 hierarchy's values rounded to FP32.  Combine with MGP_FLAG_KRYLOV (the
+ * FP32 cycle is then the preconditioner).  No reference counterpart. */
+#define MGP_FLAG_MIXED 8
 
 /* Solver kinds for the resident-hierarchy handle. */
 #define MGP_KIND_MG 0   /* module MGPoisson2D (vcycle, fmg)                  */

@@ -12,7 +12,7 @@ _API_NAMES = {
     "vcycle", "fmg", "dc_vcycle", "Solver", "fill_ghosts", "extrapolate_ghosts", "compute_invdiags",
     "compute_laplacian", "compute_residual", "relax_gs", "solve_bicgstab2", "solve_bicgstab2_noalloc", "restrict", "prolong",
     "pnorm", "inner_prod", "estimate_maxdepth", "create_mgschedule", "MGPError", "library_path",
-    "kernel_launch_count", "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV",
+    "kernel_launch_count", "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV", "FLAG_MIXED",
     "NOALLOC_MAX_SIDE", "EXPORTS",
 }
 

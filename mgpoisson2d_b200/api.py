@@ -24,6 +24,7 @@ from .types import (KIND_DD, KIND_MG, STATUS_NAMES, BdryData, Box, BoxData, GeoD
 FLAG_DIRICHLET_COUPLED_DIAG = 1
 FLAG_TIME_SMOOTHER = 2
 FLAG_KRYLOV = 4
+FLAG_MIXED = 8
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libmgp2d.so")
@@ -311,4 +312,4 @@ class Solver:
 __all__ = ["vcycle", "fmg", "dc_vcycle", "Solver", "fill_ghosts", "extrapolate_ghosts", "compute_invdiags",
            "compute_laplacian", "compute_residual", "relax_gs", "solve_bicgstab2", "solve_bicgstab2_noalloc", "NOALLOC_MAX_SIDE", "restrict", "prolong", "pnorm",
            "inner_prod", "estimate_maxdepth", "create_mgschedule", "MGPError", "library_path", "kernel_launch_count",
-           "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV", "EXPORTS", "KIND_MG", "KIND_DD"]
+           "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV", "FLAG_MIXED", "EXPORTS", "KIND_MG", "KIND_DD"]

@@ -19,17 +19,34 @@ enum { T_NONE = -1, T_NEUM = 0, T_DIRI = 1, T_PERIODIC = 2, T_CF = 3, T_EX0 = 4,
 enum { M_UNIFORM = 0, M_NONUNIFORM = 1, M_LAH = 2 };
 enum { S_XLO = 0, S_XHI = 1, S_YLO = 2, S_YHI = 3 };
 
-// A 2-D FP64 field; p points at valid element (0,0), ld is the row pitch.
-struct DF {
-    double* p;
+// A 2-D field; p points at valid element (0,0), ld is the row pitch.  The
+// solver's own arithmetic is FP64 (DF); the mixed-precision V-cycle keeps
+// its grid levels in FP32 (DF32).
+template <class T>
+struct DFT {
+    T* p;
     int ld;
 };
+using DF = DFT<double>;
+using DF32 = DFT<float>;
 #define AT(f, i, j) ((f).p[(long)(i) + (long)(j) * (long)(f).ld])
 
-struct Geo {
-    DF J, xx, xy, yx, yy;   // J cell-centred; xx, xy on x-faces; yx, yy on y-faces
+template <class T>
+struct GeoT {
+    DFT<T> J, xx, xy, yx, yy;   // J cell-centred; xx, xy on x-faces; yx, yy on y-faces
     double dx, dy, idx, idy;
 };
+using Geo = GeoT<double>;
+using Geo32 = GeoT<float>;
+
+// The value fill_ghosts puts in non-periodic corner ghosts (precision.f90:53);
+// FP32 fields hold a large finite stand-in.
+template <class T>
+__device__ __forceinline__ T bogus();
+template <>
+__device__ __forceinline__ double bogus<double>() { return kBogus; }
+template <>
+__device__ __forceinline__ float bogus<float>() { return 1.2345e30f; }
 
 // Boundary conditions of one level (type(bdry_data), AU:55-70).
 struct BCd {
@@ -81,16 +98,20 @@ __device__ __forceinline__ int region(int i, int n, bool per_lo, bool per_hi) {
 // ---------------------------------------------------------------------------
 // The mapped 9-point operator, P2:886-1319
 // ---------------------------------------------------------------------------
-struct St9 {
-    double p, pe, pw, pn, ps, ee, ew, en, es, ene, enw, ese, esw;
+template <class T>
+struct St9T {
+    T p, pe, pw, pn, ps, ee, ew, en, es, ene, enw, ese, esw;
 };
+using St9 = St9T<double>;
 
 // Reads phi around the cell from global memory.
-struct GLoad {
-    const double* c;
+template <class T>
+struct GLoadT {
+    const T* c;
     long ld;
-    __device__ __forceinline__ double operator()(int di, int dj) const { return c[di + (long)dj * ld]; }
+    __device__ __forceinline__ T operator()(int di, int dj) const { return c[di + (long)dj * ld]; }
 };
+using GLoad = GLoadT<double>;
 
 // A unit impulse at the cell, zero elsewhere; the four own-row/column ghosts
 // may carry the Dirichlet coupling (-3) for the coupled diagonal.
@@ -107,75 +128,76 @@ struct DeltaLoad {
 };
 
 // The transverse values of the nine region blocks of compute_laplacian.
-template <class L>
-__device__ __forceinline__ void gather9(const L& P, int xr, int yr, St9& s) {
-    const double p = P(0, 0), pe = P(1, 0), pw = P(-1, 0), pn = P(0, 1), ps = P(0, -1);
-    double ee, ew, en, es, ene, enw, ese, esw;
+template <class L, class T>
+__device__ __forceinline__ void gather9(const L& P, int xr, int yr, St9T<T>& s) {
+    const T p = P(0, 0), pe = P(1, 0), pw = P(-1, 0), pn = P(0, 1), ps = P(0, -1);
+    const T three = T(3.0), half = T(0.5);
+    T ee, ew, en, es, ene, enw, ese, esw;
     s.p = p; s.pe = pe; s.pw = pw; s.pn = pn; s.ps = ps;
     if (yr == RLO) {
         if (xr == RLO) {              // P2:937-958
             ee = P(1, 0); en = P(0, 1);
-            ew = 3.0 * (p - ee) + P(2, 0);
-            es = 3.0 * (p - en) + P(0, 2);
+            ew = three * (p - ee) + P(2, 0);
+            es = three * (p - en) + P(0, 2);
             ene = P(1, 1);
-            enw = 3.0 * (en - ene) + P(2, 1);
-            ese = 3.0 * (ee - ene) + P(1, 2);
-            esw = 0.5 * ((3.0 * (es - ese) + P(2, -1)) + (3.0 * (ew - enw) + P(-1, 2)));
+            enw = three * (en - ene) + P(2, 1);
+            ese = three * (ee - ene) + P(1, 2);
+            esw = half * ((three * (es - ese) + P(2, -1)) + (three * (ew - enw) + P(-1, 2)));
         } else if (xr == RMID) {      // P2:986-1002
             ee = P(1, 0); ew = P(-1, 0); en = P(0, 1);
-            es = 3.0 * (p - en) + P(0, 2);
+            es = three * (p - en) + P(0, 2);
             ene = P(1, 1); enw = P(-1, 1);
-            ese = 3.0 * (ee - ene) + P(1, 2);
-            esw = 3.0 * (ew - enw) + P(-1, 2);
+            ese = three * (ee - ene) + P(1, 2);
+            esw = three * (ew - enw) + P(-1, 2);
         } else {                      // P2:1021-1039
             ew = P(-1, 0); en = P(0, 1);
-            ee = 3.0 * (p - ew) + P(-2, 0);
-            es = 3.0 * (p - en) + P(0, 2);
+            ee = three * (p - ew) + P(-2, 0);
+            es = three * (p - en) + P(0, 2);
             enw = P(-1, 1);
-            ene = 3.0 * (pn - enw) + P(-2, 1);
-            esw = 3.0 * (pw - enw) + P(-1, 2);
-            ese = 0.5 * ((3.0 * (es - esw) + P(-2, -1)) + (3.0 * (ee - ene) + P(1, 2)));
+            ene = three * (pn - enw) + P(-2, 1);
+            esw = three * (pw - enw) + P(-1, 2);
+            ese = half * ((three * (es - esw) + P(-2, -1)) + (three * (ee - ene) + P(1, 2)));
         }
     } else if (yr == RMID) {
         if (xr == RLO) {              // P2:1068-1085
             ee = P(1, 0); en = P(0, 1); es = P(0, -1);
-            ew = 3.0 * (p - ee) + P(2, 0);
+            ew = three * (p - ee) + P(2, 0);
             ene = P(1, 1); ese = P(1, -1);
-            enw = 3.0 * (en - ene) + P(2, 1);
-            esw = 3.0 * (es - ese) + P(2, -1);
+            enw = three * (en - ene) + P(2, 1);
+            esw = three * (es - ese) + P(2, -1);
         } else if (xr == RMID) {      // P2:1103-1125
             ee = P(1, 0); ew = P(-1, 0); en = P(0, 1); es = P(0, -1);
             ene = P(1, 1); enw = P(-1, 1); ese = P(1, -1); esw = P(-1, -1);
         } else {                      // P2:1128-1147
             ew = P(-1, 0); en = P(0, 1); es = P(0, -1);
-            ee = 3.0 * (p - ew) + P(-2, 0);
+            ee = three * (p - ew) + P(-2, 0);
             enw = P(-1, 1); esw = P(-1, -1);
-            ene = 3.0 * (en - enw) + P(-2, 1);
-            ese = 3.0 * (es - esw) + P(-2, -1);
+            ene = three * (en - enw) + P(-2, 1);
+            ese = three * (es - esw) + P(-2, -1);
         }
     } else {
         if (xr == RLO) {              // P2:1176-1194
             ee = P(1, 0); es = P(0, -1);
-            ew = 3.0 * (p - ee) + P(2, 0);
-            en = 3.0 * (p - es) + P(0, -2);
+            ew = three * (p - ee) + P(2, 0);
+            en = three * (p - es) + P(0, -2);
             ese = P(1, -1);
-            ene = 3.0 * (ee - ese) + P(1, -2);
-            esw = 3.0 * (es - ese) + P(2, -1);
-            enw = 0.5 * ((3.0 * (ew - esw) + P(-1, -2)) + (3.0 * (en - ene) + P(2, 1)));
+            ene = three * (ee - ese) + P(1, -2);
+            esw = three * (es - ese) + P(2, -1);
+            enw = half * ((three * (ew - esw) + P(-1, -2)) + (three * (en - ene) + P(2, 1)));
         } else if (xr == RMID) {      // P2:1223-1239
             ee = P(1, 0); ew = P(-1, 0); es = P(0, -1);
-            en = 3.0 * (p - es) + P(0, -2);
+            en = three * (p - es) + P(0, -2);
             ese = P(1, -1); esw = P(-1, -1);
-            ene = 3.0 * (ee - ese) + P(1, -2);
-            enw = 3.0 * (ew - esw) + P(-1, -2);
+            ene = three * (ee - ese) + P(1, -2);
+            enw = three * (ew - esw) + P(-1, -2);
         } else {                      // P2:1258-1276
             ew = P(-1, 0); es = P(0, -1);
-            ee = 3.0 * (p - ew) + P(-2, 0);
-            en = 3.0 * (p - es) + P(0, -2);
+            ee = three * (p - ew) + P(-2, 0);
+            en = three * (p - es) + P(0, -2);
             esw = P(-1, -1);
-            enw = 3.0 * (ew - esw) + P(-1, -2);
-            ese = 3.0 * (es - esw) + P(-2, -1);
-            ene = 0.5 * ((3.0 * (en - enw) + P(-2, 1)) + (3.0 * (ee - ese) + P(1, -2)));
+            enw = three * (ew - esw) + P(-1, -2);
+            ese = three * (es - esw) + P(-2, -1);
+            ene = half * ((three * (en - enw) + P(-2, 1)) + (three * (ee - ese) + P(1, -2)));
         }
     }
     s.ee = ee; s.ew = ew; s.en = en; s.es = es;
@@ -189,13 +211,16 @@ __device__ __forceinline__ double nbval(const BCd& b, int homog, int s, int k) {
 }
 
 // The metric values the operator reads at one cell: its four faces.
-struct Faces {
-    double xxe, xxw, xye, xyw;   // Jgup_xx, Jgup_xy at x-faces i+1 (east) and i (west)
-    double yyn, yys, yxn, yxs;   // Jgup_yy, Jgup_yx at y-faces j+1 (north) and j (south)
+template <class T>
+struct FacesT {
+    T xxe, xxw, xye, xyw;   // Jgup_xx, Jgup_xy at x-faces i+1 (east) and i (west)
+    T yyn, yys, yxn, yxs;   // Jgup_yy, Jgup_yx at y-faces j+1 (north) and j (south)
 };
+using Faces = FacesT<double>;
 
-__device__ __forceinline__ Faces faces_of(const Geo& g, int i, int j) {
-    Faces f;
+template <class T>
+__device__ __forceinline__ FacesT<T> faces_of(const GeoT<T>& g, int i, int j) {
+    FacesT<T> f;
     f.xxe = AT(g.xx, i + 1, j); f.xxw = AT(g.xx, i, j);
     f.xye = AT(g.xy, i + 1, j); f.xyw = AT(g.xy, i, j);
     f.yyn = AT(g.yy, i, j + 1); f.yys = AT(g.yy, i, j);
@@ -204,22 +229,25 @@ __device__ __forceinline__ Faces faces_of(const Geo& g, int i, int j) {
 }
 
 // (xfe - xfw)/dx + (yfn - yfs)/dy with Neumann faces replaced by the BC flux.
-__device__ __forceinline__ double lap9f(const St9& s, const Faces& f, double idx, double idy, int i, int j, int xr,
-                                        int yr, const BCd& b, int homog) {
-    double xfe = f.xxe * (s.pe - s.p) * idx + f.xye * 0.25 * (s.ene - s.ese + s.en - s.es) * idy;
-    double xfw = f.xxw * (s.p - s.pw) * idx + f.xyw * 0.25 * (s.en - s.es + s.enw - s.esw) * idy;
-    double yfn = f.yyn * (s.pn - s.p) * idy + f.yxn * 0.25 * (s.ene - s.enw + s.ee - s.ew) * idx;
-    double yfs = f.yys * (s.p - s.ps) * idy + f.yxs * 0.25 * (s.ee - s.ew + s.ese - s.esw) * idx;
-    if (xr == RLO && b.type[S_XLO] == T_NEUM) xfw = nbval(b, homog, S_XLO, j);
-    if (yr == RLO && b.type[S_YLO] == T_NEUM) yfs = nbval(b, homog, S_YLO, i);
-    if (xr == RHI && b.type[S_XHI] == T_NEUM) xfe = nbval(b, homog, S_XHI, j);
-    if (yr == RHI && b.type[S_YHI] == T_NEUM) yfn = nbval(b, homog, S_YHI, b.kyhi);
+template <class T>
+__device__ __forceinline__ T lap9f(const St9T<T>& s, const FacesT<T>& f, T idx, T idy, int i, int j, int xr, int yr,
+                                   const BCd& b, int homog) {
+    const T q = T(0.25);
+    T xfe = f.xxe * (s.pe - s.p) * idx + f.xye * q * (s.ene - s.ese + s.en - s.es) * idy;
+    T xfw = f.xxw * (s.p - s.pw) * idx + f.xyw * q * (s.en - s.es + s.enw - s.esw) * idy;
+    T yfn = f.yyn * (s.pn - s.p) * idy + f.yxn * q * (s.ene - s.enw + s.ee - s.ew) * idx;
+    T yfs = f.yys * (s.p - s.ps) * idy + f.yxs * q * (s.ee - s.ew + s.ese - s.esw) * idx;
+    if (xr == RLO && b.type[S_XLO] == T_NEUM) xfw = T(nbval(b, homog, S_XLO, j));
+    if (yr == RLO && b.type[S_YLO] == T_NEUM) yfs = T(nbval(b, homog, S_YLO, i));
+    if (xr == RHI && b.type[S_XHI] == T_NEUM) xfe = T(nbval(b, homog, S_XHI, j));
+    if (yr == RHI && b.type[S_YHI] == T_NEUM) yfn = T(nbval(b, homog, S_YHI, b.kyhi));
     return (xfe - xfw) * idx + (yfn - yfs) * idy;
 }
 
-__device__ __forceinline__ double lap9(const St9& s, const Geo& g, int i, int j, int xr, int yr,
-                                       const BCd& b, int homog) {
-    return lap9f(s, faces_of(g, i, j), g.idx, g.idy, i, j, xr, yr, b, homog);
+template <class T>
+__device__ __forceinline__ T lap9(const St9T<T>& s, const GeoT<T>& g, int i, int j, int xr, int yr, const BCd& b,
+                                  int homog) {
+    return lap9f(s, faces_of(g, i, j), T(g.idx), T(g.idy), i, j, xr, yr, b, homog);
 }
 
 struct Per {
@@ -233,16 +261,18 @@ __device__ __forceinline__ Per periodic_of(const BCd& b) {
 }
 
 // L[phi] at (i,j) in regions (xr, yr); phi's ghosts must be set.
-__device__ __forceinline__ double apply9r(const DF& phi, const Geo& g, const BCd& b, int homog, int i, int j, int xr,
-                                          int yr) {
-    St9 s;
-    gather9(GLoad{&AT(phi, i, j), phi.ld}, xr, yr, s);
+template <class T>
+__device__ __forceinline__ T apply9r(const DFT<T>& phi, const GeoT<T>& g, const BCd& b, int homog, int i, int j,
+                                     int xr, int yr) {
+    St9T<T> s;
+    gather9(GLoadT<T>{&AT(phi, i, j), phi.ld}, xr, yr, s);
     return lap9(s, g, i, j, xr, yr, b, homog);
 }
 
 // L[phi] at (i,j); phi's ghosts must be set.
-__device__ __forceinline__ double apply9(const DF& phi, const Geo& g, const BCd& b, int homog, int nx, int ny,
-                                         int i, int j) {
+template <class T>
+__device__ __forceinline__ T apply9(const DFT<T>& phi, const GeoT<T>& g, const BCd& b, int homog, int nx, int ny,
+                                    int i, int j) {
     const Per pr = periodic_of(b);
     return apply9r(phi, g, b, homog, i, j, region(i, nx, pr.xl, pr.xh), region(j, ny, pr.yl, pr.yh));
 }
@@ -265,17 +295,19 @@ __device__ __forceinline__ double diag9(const Geo& g, const BCd& b, int homog, i
 }
 
 // One Gauss-Seidel update of (i,j) in regions (xr, yr) (P2:1768-1771).
-__device__ __forceinline__ void gs9r(const DF& phi, const DF& rhs, const DF& invd, const Geo& g, const BCd& b,
-                                     int homog, int i, int j, int xr, int yr, double omega) {
-    const double lphi = apply9r(phi, g, b, homog, i, j, xr, yr);
-    const double p = AT(phi, i, j);
-    const double newphi = p + (AT(rhs, i, j) - lphi) * AT(invd, i, j);
-    AT(phi, i, j) = omega * newphi + (1.0 - omega) * p;
+template <class T>
+__device__ __forceinline__ void gs9r(const DFT<T>& phi, const DFT<T>& rhs, const DFT<T>& invd, const GeoT<T>& g,
+                                     const BCd& b, int homog, int i, int j, int xr, int yr, double omega) {
+    const T lphi = apply9r(phi, g, b, homog, i, j, xr, yr);
+    const T p = AT(phi, i, j);
+    const T newphi = p + (AT(rhs, i, j) - lphi) * AT(invd, i, j);
+    AT(phi, i, j) = T(omega) * newphi + T(1.0 - omega) * p;
 }
 
 // The same, regions from the position.
-__device__ __forceinline__ void gs9(const DF& phi, const DF& rhs, const DF& invd, const Geo& g, const BCd& b,
-                                    int homog, int nx, int ny, int i, int j, double omega) {
+template <class T>
+__device__ __forceinline__ void gs9(const DFT<T>& phi, const DFT<T>& rhs, const DFT<T>& invd, const GeoT<T>& g,
+                                    const BCd& b, int homog, int nx, int ny, int i, int j, double omega) {
     const Per pr = periodic_of(b);
     gs9r(phi, rhs, invd, g, b, homog, i, j, region(i, nx, pr.xl, pr.xh), region(j, ny, pr.yl, pr.yh), omega);
 }
@@ -286,11 +318,12 @@ __device__ __forceinline__ void gs9(const DF& phi, const DF& rhs, const DF& invd
 // and PERIODIC, computed from interior values only, so all ghost cells can
 // be filled at once.  P(i,j) reads phi as it stands at the sweep start.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double ghost_diri(const BCd& b, int homog, int s, int k, double p0, double p1, double p2);
+template <class T>
+__device__ __forceinline__ T ghost_diri(const BCd& b, int homog, int s, int k, T p0, T p1, T p2);
 
 // y-side ghost (i,j), 0 <= i < nx.
 template <class P>
-__device__ __forceinline__ double sweep_ghost_y(const P& p, const BCd& b, int homog, int ny, int i, int j) {
+__device__ __forceinline__ auto sweep_ghost_y(const P& p, const BCd& b, int homog, int ny, int i, int j) {
     const int s = (j < 0) ? S_YLO : S_YHI;
     const int t = b.type[s];
     if (t == T_DIRI) {
@@ -303,7 +336,7 @@ __device__ __forceinline__ double sweep_ghost_y(const P& p, const BCd& b, int ho
 
 // x-side ghost (i,j), 0 <= j < ny.
 template <class P>
-__device__ __forceinline__ double sweep_ghost_x(const P& p, const BCd& b, int homog, int nx, int i, int j) {
+__device__ __forceinline__ auto sweep_ghost_x(const P& p, const BCd& b, int homog, int nx, int i, int j) {
     const int s = (i < 0) ? S_XLO : S_XHI;
     const int t = b.type[s];
     if (t == T_DIRI) {
@@ -316,12 +349,12 @@ __device__ __forceinline__ double sweep_ghost_x(const P& p, const BCd& b, int ho
 
 // Any ghost cell; corners as AU:1460-1490.
 template <class P>
-__device__ __forceinline__ double sweep_ghost(const P& p, const BCd& b, int homog, int nx, int ny, int i, int j) {
+__device__ __forceinline__ auto sweep_ghost(const P& p, const BCd& b, int homog, int nx, int ny, int i, int j) {
     const bool xin = (i >= 0 && i < nx), yin = (j >= 0 && j < ny);
     if (xin && !yin) return sweep_ghost_y(p, b, homog, ny, i, j);
     if (yin && !xin) return sweep_ghost_x(p, b, homog, nx, i, j);
     const bool px = b.type[S_XLO] == T_PERIODIC, py = b.type[S_YLO] == T_PERIODIC;
-    if (!px && !py) return kBogus;
+    if (!px && !py) return bogus<decltype(p(0, 0))>();
     const int wi = (i < 0) ? nx - 1 : 0, wj = (j < 0) ? ny - 1 : 0;
     if (px && py) return p(wi, wj);
     if (px) return sweep_ghost_y(p, b, homog, ny, wi, j);
@@ -329,10 +362,12 @@ __device__ __forceinline__ double sweep_ghost(const P& p, const BCd& b, int homo
 }
 
 // Reads a field directly.
-struct DFLoad {
-    DF f;
-    __device__ __forceinline__ double operator()(int i, int j) const { return AT(f, i, j); }
+template <class T>
+struct DFLoadT {
+    DFT<T> f;
+    __device__ __forceinline__ T operator()(int i, int j) const { return AT(f, i, j); }
 };
+using DFLoad = DFLoadT<double>;
 
 // k / d by a multiply: exact for 0 <= k < 65536 and 1 <= d <= 1024 (every
 // pair checked on the host).  The magic number costs one divide; compute it
@@ -354,66 +389,71 @@ __device__ __forceinline__ int colour_cj(int c) { return (c == 1 || c == 3) ? 1 
 // ---------------------------------------------------------------------------
 
 // Dirichlet, order 3 (AU:1161-1177, AU:1215-1231).  k = index along the side.
-__device__ __forceinline__ double ghost_diri(const BCd& b, int homog, int s, int k, double p0, double p1, double p2) {
-    const double sixteenfifth = 16.0 / 5.0, fifth = 1.0 / 5.0;
+template <class T>
+__device__ __forceinline__ T ghost_diri(const BCd& b, int homog, int s, int k, T p0, T p1, T p2) {
+    const T sixteenfifth = T(16.0 / 5.0), fifth = T(1.0 / 5.0), three = T(3.0);
     if (b.mode[s] == M_LAH) return -p0;
-    if (homog) return -(3.0 * p0) + p1 - fifth * p2;
-    if (b.mode[s] == M_UNIFORM) return sixteenfifth * b.u[s] - 3.0 * p0 + p1 - fifth * p2;
-    const double g = (s < 2) ? b.d[s][k] : b.d[s][b.koffy + k];
-    return sixteenfifth * g - 3.0 * p0 + p1 - fifth * p2;
+    if (homog) return -(three * p0) + p1 - fifth * p2;
+    if (b.mode[s] == M_UNIFORM) return sixteenfifth * T(b.u[s]) - three * p0 + p1 - fifth * p2;
+    const T g = T((s < 2) ? b.d[s][k] : b.d[s][b.koffy + k]);
+    return sixteenfifth * g - three * p0 + p1 - fifth * p2;
 }
 
 // Neumann on an x side (AU:926-985), ghost of row j.  Which formula last wrote
 // row j depends on homog: homogeneous fills are one-sided at both ends;
 // inhomogeneous fills rewrite jlo with the centred formula (which reads the y
 // ghosts at jlo-1).
-__device__ __forceinline__ double ghost_neum_x(const DF& p, const Geo& g, const BCd& b, int homog, int s, int nx,
+template <class T>
+__device__ __forceinline__ T ghost_neum_x(const DFT<T>& p, const GeoT<T>& g, const BCd& b, int homog, int s, int nx,
                                                int ny, int j) {
     const bool lo = (s == S_XLO);
     const int e = lo ? -1 : 1, i = lo ? 0 : nx - 1;
-    const double dx = lo ? -g.dx : g.dx, dy = g.dy;
+    const T dx = T(lo ? -g.dx : g.dx), dy = T(g.dy);
     if (b.mode[s] == M_LAH) return AT(p, i, j);
-    double dpn, dpf, cross;
+    T dpn, dpf, cross;
+    const T c3 = T(3.0), c4 = T(4.0), half = T(0.5), c15 = T(1.5);
     const bool onesided_lo = (j == 0) && homog;
     const bool onesided_hi = (j == ny - 1);
     if (onesided_lo) {
-        dpn = -((3.0 * AT(p, i, j) - 4.0 * AT(p, i, j + 1) + AT(p, i, j + 2)) * 0.5 / dy);
-        dpf = -((3.0 * AT(p, i - e, j) - 4.0 * AT(p, i - e, j + 1) + AT(p, i - e, j + 2)) * 0.5 / dy);
-        cross = 0.5 * (3.0 * dpn - dpf) * AT(g.xy, i, j);
+        dpn = -((c3 * AT(p, i, j) - c4 * AT(p, i, j + 1) + AT(p, i, j + 2)) * half / dy);
+        dpf = -((c3 * AT(p, i - e, j) - c4 * AT(p, i - e, j + 1) + AT(p, i - e, j + 2)) * half / dy);
+        cross = half * (c3 * dpn - dpf) * AT(g.xy, i, j);
     } else if (onesided_hi) {
-        dpn = (3.0 * AT(p, i, j) - 4.0 * AT(p, i, j - 1) + AT(p, i, j - 2)) * 0.5 / dy;
-        dpf = (3.0 * AT(p, i - e, j) - 4.0 * AT(p, i - e, j - 1) + AT(p, i - e, j - 2)) * 0.5 / dy;
-        cross = 0.5 * (3.0 * dpn - dpf) * AT(g.xy, i, j);
+        dpn = (c3 * AT(p, i, j) - c4 * AT(p, i, j - 1) + AT(p, i, j - 2)) * half / dy;
+        dpf = (c3 * AT(p, i - e, j) - c4 * AT(p, i - e, j - 1) + AT(p, i - e, j - 2)) * half / dy;
+        cross = half * (c3 * dpn - dpf) * AT(g.xy, i, j);
     } else {
-        dpn = (AT(p, i, j + 1) - AT(p, i, j - 1)) * 0.5 / dy;
-        dpf = (AT(p, i - e, j + 1) - AT(p, i - e, j - 1)) * 0.5 / dy;
-        cross = (1.5 * dpn - 0.5 * dpf) * AT(g.xy, i, j);
+        dpn = (AT(p, i, j + 1) - AT(p, i, j - 1)) * half / dy;
+        dpf = (AT(p, i - e, j + 1) - AT(p, i - e, j - 1)) * half / dy;
+        cross = (c15 * dpn - half * dpf) * AT(g.xy, i, j);
     }
     if (homog) return AT(p, i, j) - (-cross) * dx / AT(g.xx, i, j);
-    const double bv = (b.mode[s] == M_UNIFORM) ? b.u[s] : b.d[s][j];
+    const T bv = T((b.mode[s] == M_UNIFORM) ? b.u[s] : b.d[s][j]);
     return AT(p, i, j) - (bv - cross) * dx / AT(g.xx, i, j);
 }
 
 // Neumann on a y side (AU:990-1062), ghost of column i.  Column ilo always
 // ends with the centred formula (it reads the x ghosts), ihi one-sided.
-__device__ __forceinline__ double ghost_neum_y(const DF& p, const Geo& g, const BCd& b, int homog, int s, int nx,
+template <class T>
+__device__ __forceinline__ T ghost_neum_y(const DFT<T>& p, const GeoT<T>& g, const BCd& b, int homog, int s, int nx,
                                                int ny, int i) {
     const bool lo = (s == S_YLO);
     const int e = lo ? -1 : 1, j = lo ? 0 : ny - 1;
-    const double dy = lo ? -g.dy : g.dy, dx = g.dx;
+    const T dy = T(lo ? -g.dy : g.dy), dx = T(g.dx);
     if (b.mode[s] == M_LAH) return AT(p, i, j);
-    double dpn, dpf, cross;
+    T dpn, dpf, cross;
+    const T c3 = T(3.0), c4 = T(4.0), half = T(0.5), c15 = T(1.5);
     if (i == nx - 1) {
-        dpn = (3.0 * AT(p, i, j) - 4.0 * AT(p, i - 1, j) + AT(p, i - 2, j)) * 0.5 / dx;
-        dpf = (3.0 * AT(p, i, j - e) - 4.0 * AT(p, i - 1, j - e) + AT(p, i - 2, j - e)) * 0.5 / dx;
-        cross = 0.5 * (3.0 * dpn - dpf) * AT(g.yx, i, j);
+        dpn = (c3 * AT(p, i, j) - c4 * AT(p, i - 1, j) + AT(p, i - 2, j)) * half / dx;
+        dpf = (c3 * AT(p, i, j - e) - c4 * AT(p, i - 1, j - e) + AT(p, i - 2, j - e)) * half / dx;
+        cross = half * (c3 * dpn - dpf) * AT(g.yx, i, j);
     } else {
-        dpn = (AT(p, i + 1, j) - AT(p, i - 1, j)) * 0.5 / dx;
-        dpf = (AT(p, i + 1, j - e) - AT(p, i - 1, j - e)) * 0.5 / dx;
-        cross = (1.5 * dpn - 0.5 * dpf) * AT(g.yx, i, j);
+        dpn = (AT(p, i + 1, j) - AT(p, i - 1, j)) * half / dx;
+        dpf = (AT(p, i + 1, j - e) - AT(p, i - 1, j - e)) * half / dx;
+        cross = (c15 * dpn - half * dpf) * AT(g.yx, i, j);
     }
     if (homog) return AT(p, i, j) - (-cross) * dy / AT(g.yy, i, j);
-    const double bv = (b.mode[s] == M_UNIFORM) ? b.u[s] : b.d[s][i];
+    const T bv = T((b.mode[s] == M_UNIFORM) ? b.u[s] : b.d[s][i]);
     return AT(p, i, j) - (bv - cross) * dy / AT(g.yy, i, j);
 }
 
@@ -430,42 +470,44 @@ __device__ __forceinline__ void side_range(const BCd& b, int s, int nx, int ny, 
 
 // Ghost k of side s (k counted from `lo` of side_range).  Returns false if the
 // side writes nothing there.  Writes the value.
-__device__ __forceinline__ void fill_side_elem(const DF& p, const Geo& g, const BCd& b, int homog, int s, int nx,
+template <class T>
+__device__ __forceinline__ void fill_side_elem(const DFT<T>& p, const GeoT<T>& g, const BCd& b, int homog, int s, int nx,
                                                int ny, int k) {
     const int t = b.type[s];
     if (s < 2) {
         const bool lo = (s == S_XLO);
         const int i = lo ? 0 : nx - 1, e = lo ? -1 : 1;
-        double v;
+        T v;
         if (t == T_NEUM) v = ghost_neum_x(p, g, b, homog, s, nx, ny, k);
         else if (t == T_DIRI) v = ghost_diri(b, homog, s, k, AT(p, i, k), AT(p, i - e, k), AT(p, i - 2 * e, k));
         else if (t == T_PERIODIC) v = lo ? AT(p, nx - 1, k) : AT(p, 0, k);
         else {
-            const double v0 = AT(p, i, k), v1 = AT(p, i - e, k), v2 = AT(p, i - 2 * e, k);
-            v = (t == T_EX0) ? v0 : (t == T_EX1) ? 2.0 * v0 - v1 : 3.0 * (v0 - v1) + v2;
+            const T v0 = AT(p, i, k), v1 = AT(p, i - e, k), v2 = AT(p, i - 2 * e, k);
+            v = (t == T_EX0) ? v0 : (t == T_EX1) ? T(2.0) * v0 - v1 : T(3.0) * (v0 - v1) + v2;
         }
         AT(p, i + e, k) = v;
     } else {
         const bool lo = (s == S_YLO);
         const int j = lo ? 0 : ny - 1, e = lo ? -1 : 1;
-        double v;
+        T v;
         if (t == T_NEUM) v = ghost_neum_y(p, g, b, homog, s, nx, ny, k);
         else if (t == T_DIRI) v = ghost_diri(b, homog, s, k, AT(p, k, j), AT(p, k, j - e), AT(p, k, j - 2 * e));
         else if (t == T_PERIODIC) v = lo ? AT(p, k, ny - 1) : AT(p, k, 0);
         else {
-            const double v0 = AT(p, k, j), v1 = AT(p, k, j - e), v2 = AT(p, k, j - 2 * e);
-            v = (t == T_EX0) ? v0 : (t == T_EX1) ? 2.0 * v0 - v1 : 3.0 * (v0 - v1) + v2;
+            const T v0 = AT(p, k, j), v1 = AT(p, k, j - e), v2 = AT(p, k, j - 2 * e);
+            v = (t == T_EX0) ? v0 : (t == T_EX1) ? T(2.0) * v0 - v1 : T(3.0) * (v0 - v1) + v2;
         }
         AT(p, k, j + e) = v;
     }
 }
 
 // Corner ghosts, AU:1460-1490.  Corner c = 0..3: (-1,-1), (-1,ny), (nx,-1), (nx,ny).
-__device__ __forceinline__ void fill_corner(const DF& p, const BCd& b, int nx, int ny, int c) {
+template <class T>
+__device__ __forceinline__ void fill_corner(const DFT<T>& p, const BCd& b, int nx, int ny, int c) {
     const bool px = b.type[S_XLO] == T_PERIODIC, py = b.type[S_YLO] == T_PERIODIC;
     const int ci = (c >= 2) ? nx : -1, cj = (c & 1) ? ny : -1;
-    double v;
-    if (!px && !py) v = kBogus;
+    T v;
+    if (!px && !py) v = bogus<T>();
     else if (px && py) v = AT(p, ci < 0 ? nx - 1 : 0, cj < 0 ? ny - 1 : 0);
     else if (px) v = AT(p, ci < 0 ? nx - 1 : 0, cj);
     else v = AT(p, ci, cj < 0 ? ny - 1 : 0);
@@ -473,12 +515,13 @@ __device__ __forceinline__ void fill_corner(const DF& p, const BCd& b, int nx, i
 }
 
 // extrapolate_ghosts value for an x-ghost column (lo/hi) at row a, AU:1497-1566.
-__device__ __forceinline__ double extrap_val(int order, double v0, double v1, double v2, double v3) {
+template <class T>
+__device__ __forceinline__ T extrap_val(int order, T v0, T v1, T v2, T v3) {
     switch (order) {
         case 0: return v0;
-        case 1: return 2.0 * v0 - v1;
-        case 2: return 3.0 * (v0 - v1) + v2;
-        default: return 4.0 * (v0 + v2) - 6.0 * v1 - v3;
+        case 1: return T(2.0) * v0 - v1;
+        case 2: return T(3.0) * (v0 - v1) + v2;
+        default: return T(4.0) * (v0 + v2) - T(6.0) * v1 - v3;
     }
 }
 
@@ -486,10 +529,12 @@ __device__ __forceinline__ double extrap_val(int order, double v0, double v1, do
 // Transfers, MG:135-394
 // ---------------------------------------------------------------------------
 // Cell-centred restriction (MG:145-158): sum in the Fortran loop order.
-__device__ __forceinline__ double restrict_cc(const DF& f, int ci, int cj, int refx, int refy, double scale) {
-    double acc = 0.0;
+template <class T>
+__device__ __forceinline__ T restrict_cc(const DFT<T>& f, int ci, int cj, int refx, int refy, double scale) {
+    T acc = T(0.0);
+    const T sc = T(scale);
     for (int a = 0; a < refy; ++a)
-        for (int c = 0; c < refx; ++c) acc = acc + scale * AT(f, ci * refx + c, cj * refy + a);
+        for (int c = 0; c < refx; ++c) acc = acc + sc * AT(f, ci * refx + c, cj * refy + a);
     return acc;
 }
 

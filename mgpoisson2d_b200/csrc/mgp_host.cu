@@ -53,39 +53,43 @@ constexpr long kCoarseCells = 1024;
 // ---------------------------------------------------------------------------
 // Device memory: every field of a solver comes out of one allocation.
 // ---------------------------------------------------------------------------
+template <class T>
 struct Spec {
-    DF* dst;
+    DFT<T>* dst;
     int nxv, nyv, g;
     size_t off;   // element offset of the field's block
 };
 
-struct Arena {
-    std::vector<Spec> specs;
+template <class T>
+struct ArenaT {
+    std::vector<Spec<T>> specs;
     size_t elems = 0;
-    double* base = nullptr;
-    void add(DF* dst, int nxv, int nyv, int g) {
-        // arrays with ghosts keep one spare column, so the sweep's TMA window
-        // (from column -2) still covers the ghost column nx
-        const int ld = ((nxv + 3 * g + 31) / 32) * 32;
+    T* base = nullptr;
+    void add(DFT<T>* dst, int nxv, int nyv, int g) {
+        // arrays with ghosts keep spare columns, so the sweep's TMA window (from
+        // the 16-byte-aligned column left of the ghost column -1) still covers
+        // the ghost column nx
+        const int spare = g ? 16 / (int)sizeof(T) - 1 : 0;
+        const int ld = ((nxv + 2 * g + spare + 31) / 32) * 32;
         const size_t pad = g ? 32 : 0;
         const size_t n = (size_t)(nyv + 2 * g) * ld + 2 * pad;
-        Spec s{dst, nxv, nyv, g, elems};
+        Spec<T> s{dst, nxv, nyv, g, elems};
         specs.push_back(s);
         dst->ld = ld;
         elems += (n + 31) / 32 * 32;
     }
     int commit(cudaStream_t st) {
         if (elems == 0) return MGP_OK;
-        if (cudaMalloc(&base, elems * sizeof(double)) != cudaSuccess) {
+        if (cudaMalloc(&base, elems * sizeof(T)) != cudaSuccess) {
             cudaGetLastError();
             base = nullptr;
-            return set_err(MGP_ENOMEM, "cudaMalloc of %zu bytes failed", elems * sizeof(double));
+            return set_err(MGP_ENOMEM, "cudaMalloc of %zu bytes failed", elems * sizeof(T));
         }
         for (auto& s : specs) {
             const size_t pad = s.g ? 32 : 0;
             s.dst->p = base + s.off + pad + (size_t)s.g * s.dst->ld;
         }
-        CK(cudaMemsetAsync(base, 0, elems * sizeof(double), st));   // fresh arrays start at zero
+        CK(cudaMemsetAsync(base, 0, elems * sizeof(T), st));   // fresh arrays start at zero
         return MGP_OK;
     }
     void release() {
@@ -95,6 +99,8 @@ struct Arena {
         elems = 0;
     }
 };
+using Arena = ArenaT<double>;
+using Arena32 = ArenaT<float>;
 
 // ---------------------------------------------------------------------------
 // Argument checks and staging of caller arrays
@@ -257,11 +263,22 @@ struct mgp_solver {
     // search direction, A*y and A*z)
     DF kr{}, krh{}, kp{}, kv{}, kt{};
     std::vector<SweepTma> tma;   // per level, for the fused sweep
+    // MGP_FLAG_MIXED: FP32 copies of the grid-path levels 0 .. dc-1
+    struct Lv32 {
+        int nx = 0, ny = 0;
+        Geo32 g{};
+        DF32 e{}, e2{}, r{}, w{}, invd{};
+    };
+    std::vector<Lv32> lv32;
+    std::vector<SweepTma> tma32;
+    Arena32 fixed32, state32;
     // V-cycles captured as CUDA graphs, keyed by their arguments and by which
     // buffer holds e on each grid-path level when the cycle starts
     struct VGraph {
-        int d, numcycles, nd, nu, nb;
-        std::vector<double*> e_in, e_out;
+        int d;
+        bool mix;
+        int numcycles, nd, nu, nb;
+        std::vector<const void*> e_in, e_out;
         cudaGraphExec_t exec;
         long long launches;
     };
@@ -298,11 +315,60 @@ void solver_free(mgp_solver* s) {
     if (s->cap) cudaStreamDestroy(s->cap);
     s->fixed.release();
     s->state.release();
+    s->fixed32.release();
+    s->state32.release();
     delete s;
 }
 
 double* red_partials(mgp_solver* s) { return s->d_red; }
 double* red_out(mgp_solver* s) { return s->d_red + 2 * 296; }
+
+// The mixed-precision V-cycle: MGP_FLAG_MIXED on a vcycle/fmg solver whose
+// grid path has at least one level.
+bool mixed(const mgp_solver* s) { return (s->flags & MGP_FLAG_MIXED) && s->kind == MGP_KIND_MG && s->dc > 0; }
+
+// FP32 copies of the grid-path levels: geometry and inverse diagonals rounded
+// from the FP64 hierarchy (built first, so the coarse operators are the FP64
+// restrictions), corrections, right-hand sides and work arrays in FP32.
+int build_fp32_levels(mgp_solver* s) {
+    cudaStream_t st = s->stream;
+    s->lv32.assign(s->dc, mgp_solver::Lv32{});
+    for (int d = 0; d < s->dc; ++d) {
+        const Lv& L = s->lv[d];
+        auto& M = s->lv32[d];
+        M.nx = L.nx;
+        M.ny = L.ny;
+        s->fixed32.add(&M.g.J, L.nx, L.ny, 0);
+        s->fixed32.add(&M.g.xx, L.nx + 1, L.ny, 0);
+        s->fixed32.add(&M.g.xy, L.nx + 1, L.ny, 0);
+        s->fixed32.add(&M.g.yx, L.nx, L.ny + 1, 0);
+        s->fixed32.add(&M.g.yy, L.nx, L.ny + 1, 0);
+        s->fixed32.add(&M.invd, L.nx, L.ny, 0);
+        s->state32.add(&M.e, L.nx, L.ny, 1);
+        s->state32.add(&M.e2, L.nx, L.ny, 1);
+        s->state32.add(&M.r, L.nx, L.ny, 0);
+        s->state32.add(&M.w, L.nx, L.ny, 0);
+        M.g.dx = L.g.dx;
+        M.g.dy = L.g.dy;
+        M.g.idx = L.g.idx;
+        M.g.idy = L.g.idy;
+    }
+    RC(s->fixed32.commit(st));
+    RC(s->state32.commit(st));
+    s->tma32.assign(s->dc, SweepTma{});
+    for (int d = 0; d < s->dc; ++d) {
+        const Lv& L = s->lv[d];
+        auto& M = s->lv32[d];
+        CK(launch_convert(M.g.J, L.g.J, L.nx, L.ny, 0, 0, st));
+        CK(launch_convert(M.g.xx, L.g.xx, L.nx + 1, L.ny, 0, 0, st));
+        CK(launch_convert(M.g.xy, L.g.xy, L.nx + 1, L.ny, 0, 0, st));
+        CK(launch_convert(M.g.yx, L.g.yx, L.nx, L.ny + 1, 0, 0, st));
+        CK(launch_convert(M.g.yy, L.g.yy, L.nx, L.ny + 1, 0, 0, st));
+        CK(launch_convert(M.invd, L.invd, L.nx, L.ny, 0, 0, st));
+        sweep_tma_prepare(&s->tma32[d], M.e, M.e2, M.r, M.invd, M.g, M.nx, M.ny);
+    }
+    return MGP_OK;
+}
 
 // Schedule, allocation, geometry restriction and inverse diagonals:
 // MG:432-562 and DD:622-761.
@@ -464,6 +530,7 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
         Lv& L = s->lv[d];
         if (L.e2.p) sweep_tma_prepare(&s->tma[d], L.e, L.e2, L.r, L.invd, L.g, L.nx, L.ny);
     }
+    if (mixed(s)) RC(build_fp32_levels(s));
     std::vector<int> ref(2 * (md + 1), 0);
     for (int d = 0; d < md; ++d) { ref[d] = s->refx[d]; ref[md + 1 + d] = s->refy[d]; }
     CK(cudaMemcpyAsync(s->d_lv, s->lv.data(), sizeof(Lv) * (md + 1), cudaMemcpyHostToDevice, st));
@@ -587,6 +654,54 @@ int vcycle_noinit(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
     return MGP_OK;
 }
 
+// The mixed-precision V-cycle from grid level d < dc: the same schedule and
+// kernels as vcycle_noinit on the FP32 copies of the grid-path levels; the
+// restriction into level dc writes the FP64 right-hand side of the coarse
+// CTA's levels (which, with the bottom solve, stay FP64) and the prolongation
+// from level dc reads its FP64 correction.
+int vcycle32(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
+    auto& L = s->lv32[d];
+    const Lv& F = s->lv[d];   // BCs of the level
+    cudaStream_t st = s->stream;
+    auto smooth32 = [&](int nu_) -> int {
+        for (int k = 0; k < nu_; ++k) {
+            CK(launch_sweep9(L.e, L.e2, L.r, L.invd, L.g, F.bc, 1, L.nx, L.ny, 1.0, &s->tma32[d], s->d_status, st));
+            std::swap(L.e, L.e2);
+        }
+        return MGP_OK;
+    };
+    RC(smooth32(nd));
+    CK(launch_fill(L.e, L.g, F.bc, 1, 0, L.nx, L.ny, st));
+    CK(launch_apply(L.w, L.e, L.r, L.g, F.bc, 1, L.nx, L.ny, 1, 0, st));
+    const int rx = s->refx[d], ry = s->refy[d];
+    const bool fine_next = d + 1 < s->dc;
+    Lv& C = s->lv[d + 1];
+    if (fine_next) {
+        auto& N = s->lv32[d + 1];
+        CK(launch_restrict(L.w, N.r, N.nx, N.ny, rx, ry, st));
+        CK(launch_set_guess(N.e, N.r, N.invd, N.nx, N.ny, st));   // MG:805-806
+        for (int c = 1; c <= numcycles; ++c) RC(vcycle32(s, d + 1, numcycles, nd, nu, nb));
+        CK(launch_fill(N.e, N.g, C.bc, 1, 1, N.nx, N.ny, st));    // MG:318
+        CK(launch_prolong(L.e, N.e, N.nx, N.ny, rx, ry, 1, st));
+    } else {
+        CK(launch_restrict(L.w, C.r, C.nx, C.ny, rx, ry, st));
+        CK(launch_set_guess(C.e, C.r, C.invd, C.nx, C.ny, st));
+        for (int c = 1; c <= numcycles; ++c) RC(vcycle_noinit(s, d + 1, numcycles, nd, nu, nb));
+        CK(launch_fill(C.e, C.g, C.bc, 1, 1, C.nx, C.ny, st));
+        CK(launch_prolong(L.e, C.e, C.nx, C.ny, rx, ry, 1, st));
+    }
+    const bool rax = (C.bc.type[0] == T_PERIODIC && C.bc.type[1] == T_PERIODIC) ||
+                     (C.bc.type[0] == T_NEUM && C.bc.type[1] == T_NEUM);
+    const bool ray = (C.bc.type[2] == T_PERIODIC && C.bc.type[3] == T_PERIODIC) ||
+                     (C.bc.type[2] == T_NEUM && C.bc.type[3] == T_NEUM);
+    if (rax && ray) {   // MG:371-383
+        CK(launch_reduce(RED_JSUM, L.e, L.g.J, L.nx, L.ny, L.g.dx * L.g.dy, red_partials(s), red_out(s), st));
+        CK(launch_sub_mean(L.e, red_out(s), L.nx, L.ny, 1, 1, st));
+    }
+    RC(smooth32(nu));
+    return MGP_OK;
+}
+
 // fmg_noinit(depth), MG:1127-1189.
 int fmg_noinit(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
     Lv& L = s->lv[d];
@@ -607,21 +722,33 @@ int fmg_noinit(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
 // runs), later calls launch the graph on the solver's stream.  The host-side
 // e/e2 buffer swaps the capture made are applied again after every replay.
 // Off when the level-0 smoothing is timed with events.
-int vcycle_run(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
-    if ((s->flags & MGP_FLAG_TIME_SMOOTHER) || d >= s->dc) return vcycle_noinit(s, d, numcycles, nd, nu, nb);
-    std::vector<double*> cur;
-    for (int k = d; k < s->dc; ++k) cur.push_back(s->lv[k].e.p);
-    auto apply_out = [&](const mgp_solver::VGraph& g) {
+int vcycle_run(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb, bool mix) {
+    auto run = [&]() { return mix ? vcycle32(s, d, numcycles, nd, nu, nb) : vcycle_noinit(s, d, numcycles, nd, nu, nb); };
+    if ((s->flags & MGP_FLAG_TIME_SMOOTHER) || d >= s->dc) return run();
+    // which buffer holds e on each grid-path level
+    auto state = [&]() {
+        std::vector<const void*> v;
+        for (int k = d; k < s->dc; ++k) v.push_back(mix ? (const void*)s->lv32[k].e.p : (const void*)s->lv[k].e.p);
+        return v;
+    };
+    auto set_state = [&](const std::vector<const void*>& v) {
         for (int k = d; k < s->dc; ++k) {
-            Lv& L = s->lv[k];
-            if (L.e.p != g.e_out[k - d]) std::swap(L.e, L.e2);
+            if (mix) {
+                auto& L = s->lv32[k];
+                if ((const void*)L.e.p != v[k - d]) std::swap(L.e, L.e2);
+            } else {
+                Lv& L = s->lv[k];
+                if ((const void*)L.e.p != v[k - d]) std::swap(L.e, L.e2);
+            }
         }
     };
+    const std::vector<const void*> cur = state();
     for (const auto& g : s->graphs) {
-        if (g.d == d && g.numcycles == numcycles && g.nd == nd && g.nu == nu && g.nb == nb && g.e_in == cur) {
+        if (g.d == d && g.mix == mix && g.numcycles == numcycles && g.nd == nd && g.nu == nu && g.nb == nb &&
+            g.e_in == cur) {
             CK(cudaGraphLaunch(g.exec, s->stream));
             count_launch((int)g.launches);
-            apply_out(g);
+            set_state(g.e_out);
             return MGP_OK;
         }
     }
@@ -632,17 +759,12 @@ int vcycle_run(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
     const long long l0 = launch_count();
     s->stream = s->cap;
     CK(cudaStreamBeginCapture(s->cap, cudaStreamCaptureModeThreadLocal));
-    const int rc = vcycle_noinit(s, d, numcycles, nd, nu, nb);
+    const int rc = run();
     cudaGraph_t graph = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(s->cap, &graph);
     s->stream = saved;
-    mgp_solver::VGraph g{d, numcycles, nd, nu, nb, cur, {}, nullptr, launch_count() - l0};
-    for (int k = d; k < s->dc; ++k) g.e_out.push_back(s->lv[k].e.p);
-    // the capture ran nothing: put the buffers back as they were
-    for (int k = d; k < s->dc; ++k) {
-        Lv& L = s->lv[k];
-        if (L.e.p != cur[k - d]) std::swap(L.e, L.e2);
-    }
+    mgp_solver::VGraph g{d, mix, numcycles, nd, nu, nb, cur, state(), nullptr, launch_count() - l0};
+    set_state(cur);   // the capture ran nothing: put the buffers back as they were
     count_launch((int)-g.launches);
     if (rc || ce != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
@@ -659,7 +781,31 @@ int vcycle_run(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
     s->graphs.push_back(g);
     CK(cudaGraphLaunch(g.exec, s->stream));
     count_launch((int)g.launches);
-    apply_out(g);
+    set_state(g.e_out);
+    return MGP_OK;
+}
+
+// dst = src over the valid region of level 0.
+int copy_valid(const DF& dst, const DF& src, int nx, int ny, cudaStream_t st);
+
+// One V-cycle on level 0 for the right-hand side x (MG:600-606): e = x * invd,
+// vcycle_noinit(0); the correction ends in L0.e.  With MGP_FLAG_MIXED the
+// cycle runs on the FP32 copies: x is rounded into the FP32 right-hand side
+// and the FP32 correction (with its ghosts) is widened into L0.e.
+int vcycle_top(mgp_solver* s, const DF& x, int numcycles, int nd, int nu, int nb) {
+    Lv& L0 = s->lv[0];
+    const int nx = L0.nx, ny = L0.ny;
+    cudaStream_t st = s->stream;
+    if (!mixed(s)) {
+        if (x.p != L0.r.p) RC(copy_valid(L0.r, x, nx, ny, st));
+        CK(launch_set_guess(L0.e, L0.r, L0.invd, nx, ny, st));
+        return vcycle_run(s, 0, numcycles, nd, nu, nb, false);
+    }
+    auto& M = s->lv32[0];
+    CK(launch_convert(M.r, x, nx, ny, 0, 0, st));
+    CK(launch_set_guess(M.e, M.r, M.invd, nx, ny, st));
+    RC(vcycle_run(s, 0, numcycles, nd, nu, nb, true));
+    CK(launch_convert(L0.e, M.e, nx, ny, 1, 1, st));
     return MGP_OK;
 }
 
@@ -696,9 +842,7 @@ int krylov_loop(mgp_solver* s, const BCd& ubc, int homog, double tol, int maxite
     int k = 0;
     // y = M^-1 x in L0.e, then Ay = L_h y
     auto precond_apply = [&](const DF& x, const DF& Ay) -> int {
-        RC(copy_valid(L0.r, x, nx, ny, st));
-        CK(launch_set_guess(L0.e, L0.r, L0.invd, nx, ny, st));
-        RC(vcycle_run(s, 0, numcycles, nd, nu, nb));
+        RC(vcycle_top(s, x, numcycles, nd, nu, nb));
         CK(launch_fill(L0.e, L0.g, L0.bc, 1, 0, nx, ny, st));
         CK(launch_apply(Ay, L0.e, L0.r, L0.g, L0.bc, 1, nx, ny, 0, 0, st));
         return MGP_OK;
@@ -794,6 +938,7 @@ int solver_solve(mgp_solver* s, int which, mgp_array* phi, mgp_array* rhs, const
     CK(cudaEventRecord(s->ev0, st));
     // every solve starts from fresh (zeroed) work arrays, like the Fortran drivers' allocations
     CK(cudaMemsetAsync(s->state.base, 0, s->state.elems * sizeof(double), st));
+    if (s->state32.base) CK(cudaMemsetAsync(s->state32.base, 0, s->state32.elems * sizeof(float), st));
     CK(cudaMemsetAsync(s->d_status, 0, sizeof(int), st));
     RC(stage_in(phi, nx, ny, s->phi0, 1, st));
     RC(stage_in(rhs, nx, ny, s->rhs0, 0, st));
@@ -818,9 +963,9 @@ int solver_solve(mgp_solver* s, int which, mgp_array* phi, mgp_array* rhs, const
         else if (rc) return rc;
     }
     for (int iter = 1; !krylov && iter <= maxiters && status == MGP_OK; ++iter) {
-        if (which == 0) CK(launch_set_guess(L0.e, L0.r, L0.invd, nx, ny, st));   // MG:600
-        if (which == 1) RC(fmg_noinit(s, 0, numcycles, nd, nu, nb));
-        else RC(vcycle_run(s, 0, numcycles, nd, nu, nb));
+        if (which == 0) RC(vcycle_top(s, L0.r, numcycles, nd, nu, nb));   // MG:600-606
+        else if (which == 1) RC(fmg_noinit(s, 0, numcycles, nd, nu, nb));
+        else RC(vcycle_run(s, 0, numcycles, nd, nu, nb, false));
         CK(launch_axpby(s->phi0, L0.e, 1.0, 1.0, nx, ny, 1, 1, st));   // MG:611 (whole array)
         CK(launch_fill(s->phi0, L0.g, ubc, homog, 0, nx, ny, st));
         CK(launch_apply(L0.r, s->phi0, s->rhs0, L0.g, ubc, homog, nx, ny, 1, 0, st));

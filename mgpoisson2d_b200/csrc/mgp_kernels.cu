@@ -33,7 +33,8 @@ static const dim3 kBlk2(32, 8);
 // ---------------------------------------------------------------------------
 // phase 0: x sides, 1: y sides, 2: corners, 3: all four sides and corners at once
 // (used when no side's fill reads another side's ghosts).
-__global__ void k_fill(DF p, Geo g, BCd b, int homog, int do_neum, int nx, int ny, int phase) {
+template <class T>
+__global__ void k_fill(DFT<T> p, GeoT<T> g, BCd b, int homog, int do_neum, int nx, int ny, int phase) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     int lo[4], cnt[4];
     for (int s = 0; s < 4; ++s) side_range(b, s, nx, ny, do_neum, lo[s], cnt[s]);
@@ -58,8 +59,9 @@ static bool fill_single_phase(const BCd& b, int do_neum) {
     return true;
 }
 
-cudaError_t launch_fill(const DF& p, const Geo& g, const BCd& b, int homog, int do_neum, int nx, int ny,
-                        cudaStream_t st) {
+template <class T>
+cudaError_t fill_impl(const DFT<T>& p, const GeoT<T>& g, const BCd& b, int homog, int do_neum, int nx, int ny,
+                      cudaStream_t st) {
     const int n = 2 * (nx + ny) + 12;
     const int blk = 256, grd = (n + blk - 1) / blk;
     if (fill_single_phase(b, do_neum)) {
@@ -70,6 +72,14 @@ cudaError_t launch_fill(const DF& p, const Geo& g, const BCd& b, int homog, int 
         count_launch(3);
     }
     return cudaGetLastError();
+}
+cudaError_t launch_fill(const DF& p, const Geo& g, const BCd& b, int homog, int do_neum, int nx, int ny,
+                        cudaStream_t st) {
+    return fill_impl(p, g, b, homog, do_neum, nx, ny, st);
+}
+cudaError_t launch_fill(const DF32& p, const Geo32& g, const BCd& b, int homog, int do_neum, int nx, int ny,
+                        cudaStream_t st) {
+    return fill_impl(p, g, b, homog, do_neum, nx, ny, st);
 }
 
 // extrapolate_ghosts (AU:1497-1566): x columns over the whole j range of the
@@ -112,15 +122,23 @@ cudaError_t launch_extrapolate(const DF& p, int nx, int ny, int ngx, int ngy, in
 // ---------------------------------------------------------------------------
 // Operator apply / residual (compute_laplacian P2:886-1319, compute_residual P2:1327-1353)
 // ---------------------------------------------------------------------------
-__global__ void k_apply(DF out, DF phi, DF rhs, Geo g, BCd b, int homog, int nx, int ny, int mode, int jscale) {
+template <class T>
+__global__ void k_apply(DFT<T> out, DFT<T> phi, DFT<T> rhs, GeoT<T> g, BCd b, int homog, int nx, int ny, int mode,
+                        int jscale) {
     CELL_IJ
     if (i >= nx || j >= ny) return;
-    double lap = apply9(phi, g, b, homog, nx, ny, i, j);
+    T lap = apply9(phi, g, b, homog, nx, ny, i, j);
     if (jscale) lap = lap / AT(g.J, i, j);
     AT(out, i, j) = mode ? AT(rhs, i, j) - lap : lap;
 }
 
 cudaError_t launch_apply(const DF& out, const DF& phi, const DF& rhs, const Geo& g, const BCd& b, int homog,
+                         int nx, int ny, int mode, int jscale, cudaStream_t st) {
+    k_apply<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(out, phi, rhs, g, b, homog, nx, ny, mode, jscale);
+    count_launch();
+    return cudaGetLastError();
+}
+cudaError_t launch_apply(const DF32& out, const DF32& phi, const DF32& rhs, const Geo32& g, const BCd& b, int homog,
                          int nx, int ny, int mode, int jscale, cudaStream_t st) {
     k_apply<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(out, phi, rhs, g, b, homog, nx, ny, mode, jscale);
     count_launch();
@@ -254,46 +272,69 @@ cudaError_t launch_restrict(const DF& f, const DF& c, int ncx, int ncy, int refx
     return cudaGetLastError();
 }
 
+// Cell-centred restriction of an FP32 field, into FP32 or (for the FP64
+// coarse levels) FP64; the sum runs in the fine field's type.
+template <class TF, class TC>
+__global__ void k_restrict_cc(DFT<TF> f, DFT<TC> c, int ncx, int ncy, int refx, int refy) {
+    const int ci = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cj = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ci >= ncx || cj >= ncy) return;
+    AT(c, ci, cj) = TC(restrict_cc(f, ci, cj, refx, refy, 1.0 / (refx * refy)));
+}
+cudaError_t launch_restrict(const DF32& f, const DF32& c, int ncx, int ncy, int refx, int refy, cudaStream_t st) {
+    k_restrict_cc<<<cells_grid(ncx, ncy, kBlk2), kBlk2, 0, st>>>(f, c, ncx, ncy, refx, refy);
+    count_launch();
+    return cudaGetLastError();
+}
+cudaError_t launch_restrict(const DF32& f, const DF& c, int ncx, int ncy, int refx, int refy, cudaStream_t st) {
+    k_restrict_cc<<<cells_grid(ncx, ncy, kBlk2), kBlk2, 0, st>>>(f, c, ncx, ncy, refx, refy);
+    count_launch();
+    return cudaGetLastError();
+}
+
 // Fine += constant + linear (+ second-difference) terms for one coarse cell.
 // The adds happen in the Fortran order: all constant adds (MG:304-314), then
 // the linear ones (MG:316-333), then the quadratic ones (MG:335-352).  Each
 // fine cell belongs to one coarse cell, so doing them per cell in sequence
 // gives the same bits.
-__device__ __forceinline__ void prolong_cell(const DF& fine, const DF& crse, int ci, int cj, int refx, int refy,
+template <class TF, class TC>
+__device__ __forceinline__ void prolong_cell(const DFT<TF>& fine, const DFT<TC>& crse, int ci, int cj, int refx, int refy,
                                              int order) {
-    const double c = AT(crse, ci, cj);
+    using R = TC;   // arithmetic in the coarse field's type
+    const R half = R(0.5), quarter = R(0.25), two = R(2.0), eighth = R(0.125);
+    const R c = AT(crse, ci, cj);
     const int fi = refx * ci, fj = refy * cj;
-    double f00 = AT(fine, fi, fj);
-    double f10 = refx == 2 ? AT(fine, fi + 1, fj) : 0.0;
-    double f01 = refy == 2 ? AT(fine, fi, fj + 1) : 0.0;
-    double f11 = (refx == 2 && refy == 2) ? AT(fine, fi + 1, fj + 1) : 0.0;
+    R f00 = R(AT(fine, fi, fj));
+    R f10 = refx == 2 ? R(AT(fine, fi + 1, fj)) : R(0.0);
+    R f01 = refy == 2 ? R(AT(fine, fi, fj + 1)) : R(0.0);
+    R f11 = (refx == 2 && refy == 2) ? R(AT(fine, fi + 1, fj + 1)) : R(0.0);
     f00 = f00 + c; f10 = f10 + c; f01 = f01 + c; f11 = f11 + c;
     if (order >= 1) {
-        const double mx = 0.5 * (AT(crse, ci + 1, cj) - AT(crse, ci - 1, cj));
-        const double my = 0.5 * (AT(crse, ci, cj + 1) - AT(crse, ci, cj - 1));
+        const R mx = half * (AT(crse, ci + 1, cj) - AT(crse, ci - 1, cj));
+        const R my = half * (AT(crse, ci, cj + 1) - AT(crse, ci, cj - 1));
         if (refx == 2 && refy == 2) {
-            f00 = f00 + 0.25 * (-mx - my);
-            f10 = f10 + 0.25 * (mx - my);
-            f01 = f01 + 0.25 * (-mx + my);
-            f11 = f11 + 0.25 * (mx + my);
+            f00 = f00 + quarter * (-mx - my);
+            f10 = f10 + quarter * (mx - my);
+            f01 = f01 + quarter * (-mx + my);
+            f11 = f11 + quarter * (mx + my);
         } else if (refx == 2) {
-            f00 = f00 + 0.25 * (-mx);
-            f10 = f10 + 0.25 * (mx);
+            f00 = f00 + quarter * (-mx);
+            f10 = f10 + quarter * (mx);
         } else {
-            f00 = f00 + 0.25 * (-my);
-            f01 = f01 + 0.25 * (my);
+            f00 = f00 + quarter * (-my);
+            f01 = f01 + quarter * (my);
         }
     }
     if (order >= 2) {
-        const double mx = 0.25 * (AT(crse, ci + 1, cj) - 2.0 * AT(crse, ci, cj) + AT(crse, ci - 1, cj));
-        const double my = 0.25 * (AT(crse, ci, cj + 1) - 2.0 * AT(crse, ci, cj) + AT(crse, ci, cj - 1));
-        const double q = (refx == 2 && refy == 2) ? 0.125 * (mx + my) : (refx == 2 ? 0.125 * mx : 0.125 * my);
+        const R mx = quarter * (AT(crse, ci + 1, cj) - two * AT(crse, ci, cj) + AT(crse, ci - 1, cj));
+        const R my = quarter * (AT(crse, ci, cj + 1) - two * AT(crse, ci, cj) + AT(crse, ci, cj - 1));
+        const R q = (refx == 2 && refy == 2) ? eighth * (mx + my) : (refx == 2 ? eighth * mx : eighth * my);
         f00 = f00 + q; f10 = f10 + q; f01 = f01 + q; f11 = f11 + q;
     }
-    AT(fine, fi, fj) = f00;
-    if (refx == 2) AT(fine, fi + 1, fj) = f10;
-    if (refy == 2) AT(fine, fi, fj + 1) = f01;
-    if (refx == 2 && refy == 2) AT(fine, fi + 1, fj + 1) = f11;
+    AT(fine, fi, fj) = TF(f00);
+    if (refx == 2) AT(fine, fi + 1, fj) = TF(f10);
+    if (refy == 2) AT(fine, fi, fj + 1) = TF(f01);
+    if (refx == 2 && refy == 2) AT(fine, fi + 1, fj + 1) = TF(f11);
 }
 
 // Cross term of the order-2 prolongation (MG:354-369); crse ghosts hold the
@@ -308,7 +349,8 @@ __device__ __forceinline__ void prolong_cross_cell(const DF& fine, const DF& crs
     AT(fine, fi + 1, fj + 1) = AT(fine, fi + 1, fj + 1) + 0.25 * mc;
 }
 
-__global__ void k_prolong(DF fine, DF crse, int ncx, int ncy, int refx, int refy, int order) {
+template <class TF, class TC>
+__global__ void k_prolong(DFT<TF> fine, DFT<TC> crse, int ncx, int ncy, int refx, int refy, int order) {
     const int ci = blockIdx.x * blockDim.x + threadIdx.x;
     const int cj = blockIdx.y * blockDim.y + threadIdx.y;
     if (ci >= ncx || cj >= ncy) return;
@@ -329,6 +371,19 @@ cudaError_t launch_prolong(const DF& fine, const DF& crse, int ncx, int ncy, int
     return cudaGetLastError();
 }
 
+cudaError_t launch_prolong(const DF32& fine, const DF32& crse, int ncx, int ncy, int refx, int refy, int order,
+                           cudaStream_t st) {
+    k_prolong<<<cells_grid(ncx, ncy, kBlk2), kBlk2, 0, st>>>(fine, crse, ncx, ncy, refx, refy, order);
+    count_launch();
+    return cudaGetLastError();
+}
+cudaError_t launch_prolong(const DF32& fine, const DF& crse, int ncx, int ncy, int refx, int refy, int order,
+                           cudaStream_t st) {
+    k_prolong<<<cells_grid(ncx, ncy, kBlk2), kBlk2, 0, st>>>(fine, crse, ncx, ncy, refx, refy, order);
+    count_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t launch_prolong_cross(const DF& fine, const DF& crse, int ncx, int ncy, cudaStream_t st) {
     k_prolong_cross<<<cells_grid(ncx, ncy, kBlk2), kBlk2, 0, st>>>(fine, crse, ncx, ncy);
     count_launch();
@@ -338,7 +393,8 @@ cudaError_t launch_prolong_cross(const DF& fine, const DF& crse, int ncx, int nc
 // ---------------------------------------------------------------------------
 // Elementwise helpers
 // ---------------------------------------------------------------------------
-__global__ void k_set_guess(DF e, DF r, DF invd, int nx, int ny) {
+template <class T>
+__global__ void k_set_guess(DFT<T> e, DFT<T> r, DFT<T> invd, int nx, int ny) {
     CELL_IJ
     if (i >= nx || j >= ny) return;
     AT(e, i, j) = AT(r, i, j) * AT(invd, i, j);
@@ -346,6 +402,30 @@ __global__ void k_set_guess(DF e, DF r, DF invd, int nx, int ny) {
 
 cudaError_t launch_set_guess(const DF& e, const DF& r, const DF& invd, int nx, int ny, cudaStream_t st) {
     k_set_guess<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(e, r, invd, nx, ny);
+    count_launch();
+    return cudaGetLastError();
+}
+cudaError_t launch_set_guess(const DF32& e, const DF32& r, const DF32& invd, int nx, int ny, cudaStream_t st) {
+    k_set_guess<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(e, r, invd, nx, ny);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// dst = src (rounded to dst's type) over i in [-gx, nx+gx), j in [-gy, ny+gy).
+template <class TD, class TS>
+__global__ void k_convert(DFT<TD> dst, DFT<TS> src, int nx, int ny, int gx, int gy) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x - gx;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y - gy;
+    if (i >= nx + gx || j >= ny + gy) return;
+    AT(dst, i, j) = TD(AT(src, i, j));
+}
+cudaError_t launch_convert(const DF32& dst, const DF& src, int nx, int ny, int gx, int gy, cudaStream_t st) {
+    k_convert<<<cells_grid(nx + 2 * gx, ny + 2 * gy, kBlk2), kBlk2, 0, st>>>(dst, src, nx, ny, gx, gy);
+    count_launch();
+    return cudaGetLastError();
+}
+cudaError_t launch_convert(const DF& dst, const DF32& src, int nx, int ny, int gx, int gy, cudaStream_t st) {
+    k_convert<<<cells_grid(nx + 2 * gx, ny + 2 * gy, kBlk2), kBlk2, 0, st>>>(dst, src, nx, ny, gx, gy);
     count_launch();
     return cudaGetLastError();
 }
@@ -392,14 +472,20 @@ __global__ void k_fillval(DF y, double v, int nx, int ny, int gx, int gy) {
 }
 
 // y -= out[0] / out[1] over the whole allocation (prolong's mean removal, MG:371-383).
-__global__ void k_sub_mean(DF y, const double* out, int nx, int ny, int gx, int gy) {
+template <class T>
+__global__ void k_sub_mean(DFT<T> y, const double* out, int nx, int ny, int gx, int gy) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x - gx;
     const int j = blockIdx.y * blockDim.y + threadIdx.y - gy;
     if (i >= nx + gx || j >= ny + gy) return;
-    AT(y, i, j) = AT(y, i, j) - out[0] / out[1];
+    AT(y, i, j) = AT(y, i, j) - T(out[0] / out[1]);
 }
 
 cudaError_t launch_sub_mean(const DF& y, const double* out, int nx, int ny, int gx, int gy, cudaStream_t st) {
+    k_sub_mean<<<cells_grid(nx + 2 * gx, ny + 2 * gy, kBlk2), kBlk2, 0, st>>>(y, out, nx, ny, gx, gy);
+    count_launch();
+    return cudaGetLastError();
+}
+cudaError_t launch_sub_mean(const DF32& y, const double* out, int nx, int ny, int gx, int gy, cudaStream_t st) {
     k_sub_mean<<<cells_grid(nx + 2 * gx, ny + 2 * gy, kBlk2), kBlk2, 0, st>>>(y, out, nx, ny, gx, gy);
     count_launch();
     return cudaGetLastError();
@@ -419,7 +505,8 @@ cudaError_t launch_fillval(const DF& y, double v, int nx, int ny, int gx, int gy
 constexpr int kRedThreads = 256;
 constexpr int kRedBlocks = 296;   // 2 x 148 SMs
 
-__device__ __forceinline__ double red_term(int kind, const DF& a, const DF& b, int i, int j, double& w) {
+template <class T>
+__device__ __forceinline__ double red_term(int kind, const DFT<T>& a, const DFT<T>& b, int i, int j, double& w) {
     const double v = AT(a, i, j);
     switch (kind) {
         case RED_SUMSQ: return v * v;
@@ -430,7 +517,8 @@ __device__ __forceinline__ double red_term(int kind, const DF& a, const DF& b, i
     }
 }
 
-__global__ void k_reduce_partial(int kind, DF a, DF b, int nx, int ny, double* partials) {
+template <class T>
+__global__ void k_reduce_partial(int kind, DFT<T> a, DFT<T> b, int nx, int ny, double* partials) {
     __shared__ double s0[kRedThreads], s1[kRedThreads];
     const long n = (long)nx * ny;
     double acc = 0.0, accw = 0.0;
@@ -486,6 +574,17 @@ __global__ void k_reduce_final(int kind, const double* partials, int nb, double 
 }
 
 cudaError_t launch_reduce(int kind, const DF& a, const DF& b, int nx, int ny, double vol, double* partials,
+                          double* out, cudaStream_t st) {
+    const long n = (long)nx * ny;
+    int nb = (int)((n + kRedThreads - 1) / kRedThreads);
+    if (nb > kRedBlocks) nb = kRedBlocks;
+    if (nb < 1) nb = 1;
+    k_reduce_partial<<<nb, kRedThreads, 0, st>>>(kind, a, b, nx, ny, partials);
+    k_reduce_final<<<1, 512, 0, st>>>(kind, partials, nb, vol, out);
+    count_launch(2);
+    return cudaGetLastError();
+}
+cudaError_t launch_reduce(int kind, const DF32& a, const DF32& b, int nx, int ny, double vol, double* partials,
                           double* out, cudaStream_t st) {
     const long n = (long)nx * ny;
     int nb = (int)((n + kRedThreads - 1) / kRedThreads);

@@ -48,6 +48,27 @@ void count_launch(int n = 1);
 cudaError_t launch_fill(const DF& p, const Geo& g, const BCd& b, int homog, int do_neum, int nx, int ny,
                         cudaStream_t st);
 cudaError_t launch_extrapolate(const DF& p, int nx, int ny, int ngx, int ngy, int order, cudaStream_t st);
+
+// ---- FP32 grid levels of the mixed-precision V-cycle --------------------- //
+cudaError_t launch_fill(const DF32& p, const Geo32& g, const BCd& b, int homog, int do_neum, int nx, int ny,
+                        cudaStream_t st);
+cudaError_t launch_apply(const DF32& out, const DF32& phi, const DF32& rhs, const Geo32& g, const BCd& b, int homog,
+                         int nx, int ny, int mode, int jscale, cudaStream_t st);
+// Cell-centred restriction into an FP32 or an FP64 coarse field.
+cudaError_t launch_restrict(const DF32& f, const DF32& c, int ncx, int ncy, int refx, int refy, cudaStream_t st);
+cudaError_t launch_restrict(const DF32& f, const DF& c, int ncx, int ncy, int refx, int refy, cudaStream_t st);
+// Prolongation from an FP32 or an FP64 coarse field (arithmetic in the coarse type).
+cudaError_t launch_prolong(const DF32& fine, const DF32& crse, int ncx, int ncy, int refx, int refy, int order,
+                           cudaStream_t st);
+cudaError_t launch_prolong(const DF32& fine, const DF& crse, int ncx, int ncy, int refx, int refy, int order,
+                           cudaStream_t st);
+cudaError_t launch_set_guess(const DF32& e, const DF32& r, const DF32& invd, int nx, int ny, cudaStream_t st);
+cudaError_t launch_sub_mean(const DF32& y, const double* out, int nx, int ny, int gx, int gy, cudaStream_t st);
+cudaError_t launch_reduce(int kind, const DF32& a, const DF32& b, int nx, int ny, double vol, double* partials,
+                          double* out, cudaStream_t st);
+// dst = src rounded to dst's type, over i in [-gx, nx+gx), j in [-gy, ny+gy).
+cudaError_t launch_convert(const DF32& dst, const DF& src, int nx, int ny, int gx, int gy, cudaStream_t st);
+cudaError_t launch_convert(const DF& dst, const DF32& src, int nx, int ny, int gx, int gy, cudaStream_t st);
 // mode: 0 lap, 1 rhs - lap; jscale divides lap by J first.
 cudaError_t launch_apply(const DF& out, const DF& phi, const DF& rhs, const Geo& g, const BCd& b, int homog,
                          int nx, int ny, int mode, int jscale, cudaStream_t st);
@@ -65,7 +86,7 @@ struct SweepMaps {
 // Descriptors for sweeping one level with phi in either of its two buffers.
 struct SweepTma {
     SweepMaps ma, mb;
-    const double *pa = nullptr, *pb = nullptr, *rhs = nullptr, *invd = nullptr, *xx = nullptr;
+    const void *pa = nullptr, *pb = nullptr, *rhs = nullptr, *invd = nullptr, *xx = nullptr;
     bool ok = false;
 };
 // Builds the descriptors when the arrays allow it (16-byte aligned bases and
@@ -73,10 +94,15 @@ struct SweepTma {
 // and the sweep stages with cp.async.
 void sweep_tma_prepare(SweepTma* t, const DF& ea, const DF& eb, const DF& rhs, const DF& invd, const Geo& g, int nx,
                        int ny);
+void sweep_tma_prepare(SweepTma* t, const DF32& ea, const DF32& eb, const DF32& rhs, const DF32& invd,
+                       const Geo32& g, int nx, int ny);
 // status (nullable) receives 2 if a CTA's staging never completed, 3 if the
 // shared-memory window was not 128-byte aligned (neither is expected).
 cudaError_t launch_sweep9(const DF& pin, const DF& pout, const DF& rhs, const DF& invd, const Geo& g, const BCd& b,
                           int homog, int nx, int ny, double omega, const SweepTma* tma, int* status,
+                          cudaStream_t st);
+cudaError_t launch_sweep9(const DF32& pin, const DF32& pout, const DF32& rhs, const DF32& invd, const Geo32& g,
+                          const BCd& b, int homog, int nx, int ny, double omega, const SweepTma* tma, int* status,
                           cudaStream_t st);
 cudaError_t launch_invdiag(const DF& invd, const Geo& g, const BCd& b, int homog, int nx, int ny, int coupled,
                            cudaStream_t st);

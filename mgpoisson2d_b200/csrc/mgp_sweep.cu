@@ -23,10 +23,13 @@
 // operations in the same order, so the result is bit-identical to running the
 // sub-passes over the whole grid one after another.
 //
-// Staging: on the solver's own arrays (aligned, with a spare column) one
+// Staging: on the solver's own arrays (aligned, with spare columns) one
 // thread issues seven TMA tile loads (cp.async.bulk.tensor.2d) of the CTA's
-// 46 x 44 window of each field, completing on one mbarrier; elsewhere (caller
-// arrays of any pitch and alignment) the threads stage with cp.async.
+// window of each field, completing on one mbarrier; elsewhere (caller arrays
+// of any pitch and alignment) the threads stage with cp.async.
+//
+// The kernel is compiled for FP64 fields (the solver's arithmetic) and for
+// FP32 fields (the grid levels of the mixed-precision V-cycle).
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -41,35 +44,46 @@ namespace {
 constexpr int kTX = 32, kTY = 32;
 constexpr int kH = 6;   // phi halo: 4 for the colour passes + E = 2 for the boundary pass
 constexpr int kSweepThreads = 512;
-
-// All seven staged arrays share one window -- origin (pox, poy) with pox the
-// even column at or below tile corner - kH, pitch PW -- so one offset
-// addresses a cell in every array: phi and the cell operands at o, the
-// west/east x-faces at o and o + 1, the south/north y-faces at o and o + PW.
-// The operands are needed on tile + (3 + E) <= tile + 5 cells (faces one
-// further), inside the phi footprint tile + kH.
-constexpr int PW = kTX + 2 * kH + 2, PH = kTY + 2 * kH;   // 46 x 44: one spare column for the even origin
-constexpr int kA = (PW * PH + 15) / 16 * 16;              // array stride: 128-byte aligned
-constexpr int oF = kA, oD = 2 * kA, oXX = 3 * kA, oXY = 4 * kA, oYX = 5 * kA, oYY = 6 * kA;
-constexpr int oBar = 7 * kA;                              // the TMA mbarrier (8 bytes)
-constexpr size_t kSmemBytes = (7 * kA + 2) * sizeof(double);
-constexpr unsigned kBoxBytes = PW * PH * sizeof(double);
 constexpr long kWaitLimit = 1L << 22;   // mbarrier polls before a CTA gives up (far above any real wait)
 
-struct SLoad {
-    const double* c;
+// Shared-memory window of one field type.  All seven staged arrays share one
+// window -- origin (pox, poy) with pox the column at or below tile corner - kH
+// that is a multiple of kAlign (a 16-byte boundary, as TMA needs), pitch PW --
+// so one offset addresses a cell in every array: phi and the cell operands
+// at o, the west/east x-faces at o and o + 1, the south/north y-faces at o
+// and o + PW.  The operands are needed on tile + (3 + E) <= tile + 5 cells
+// (faces one further), inside the phi footprint tile + kH.
+template <class T>
+struct Win {
+    static constexpr int kAlign = 16 / (int)sizeof(T);   // 2 doubles, 4 floats
+    static constexpr int PW = (kTX + 2 * kH + (kAlign - 1) + kAlign - 1) / kAlign * kAlign;   // 46 / 48
+    static constexpr int PH = kTY + 2 * kH;                                                        // 44
+    static constexpr int kA = (PW * PH * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);     // 128-B aligned
+    static constexpr int oF = kA, oD = 2 * kA, oXX = 3 * kA, oXY = 4 * kA, oYX = 5 * kA, oYY = 6 * kA;
+    static constexpr int oBarBytes = 7 * kA * (int)sizeof(T);   // the TMA mbarrier (8 bytes)
+    static constexpr size_t kSmemBytes = (size_t)oBarBytes + 16;
+    static constexpr unsigned kBoxBytes = PW * PH * sizeof(T);
+    static constexpr int kMinBlocks = sizeof(T) == 8 ? 2 : 3;   // CTAs per SM the window allows
+};
+
+static_assert(Win<double>::PW == 46 && Win<float>::PW == 48, "window pitch");
+
+template <class T>
+struct SLoadT {
+    const T* c;
     int ld;
-    __device__ __forceinline__ double operator()(int di, int dj) const { return c[di + dj * ld]; }
+    __device__ __forceinline__ T operator()(int di, int dj) const { return c[di + dj * ld]; }
 };
 
 // phi at the start of the sweep: the staged copy where it holds (i,j), else
 // global memory (the far side of a periodic domain).
+template <class T>
 struct PinLoad {
-    const double* s;
+    const T* s;
     int pox, poy, pi0, pi1, pj0, pj1;
-    DF pin;
-    __device__ __forceinline__ double operator()(int i, int j) const {
-        if (i >= pi0 && i < pi1 && j >= pj0 && j < pj1) return s[(j - poy) * PW + (i - pox)];
+    DFT<T> pin;
+    __device__ __forceinline__ T operator()(int i, int j) const {
+        if (i >= pi0 && i < pi1 && j >= pj0 && j < pj1) return s[(j - poy) * Win<T>::PW + (i - pox)];
         return AT(pin, i, j);
     }
 };
@@ -101,6 +115,18 @@ __device__ __forceinline__ void stage(double* s, int w, int ox, int oy, const DF
     }
 }
 
+// The same for FP32 fields, one element per copy.
+__device__ __forceinline__ void stage(float* s, int w, int ox, int oy, const DF32& f, int i0, int i1, int j0, int j1) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const unsigned sbase = (unsigned)__cvta_generic_to_shared(s);
+    for (int j = j0 + warp; j < j1; j += nw) {
+        const float* g = f.p + (long)j * f.ld + i0;
+        const unsigned sa = sbase + (unsigned)(((j - oy) * w + (i0 - ox)) * 4);
+        for (int k = lane; k < i1 - i0; k += 32)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa + 4 * k), "l"(g + k));
+    }
+}
+
 // ---- TMA staging ---------------------------------------------------------- //
 __device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
@@ -124,7 +150,8 @@ __device__ __forceinline__ bool mbar_wait0(unsigned bar) {
         if (mbar_try_wait(bar, 0)) return true;
     return false;
 }
-// One 2-D tile (box PW x PH) of `map` at element coordinates (x, y), x even.
+// One 2-D tile (the map's box) of `map` at element coordinates (x, y); x is a
+// multiple of 16 bytes.
 __device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map, int x, int y, unsigned bar) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
@@ -153,42 +180,49 @@ __device__ __forceinline__ void colour_ranges(int X0, int X1, int Y0, int Y1, in
     }
 }
 
+template <class T>
 struct Tile {
-    double* s;   // seven arrays of PW x PH, origin (pox, poy)
+    T* s;   // seven arrays of PW x PH, origin (pox, poy)
     int pox, poy;
 };
 
 // One Gauss-Seidel update of (i,j) from shared memory (same operations as gs9).
-__device__ __forceinline__ void gs9_tile(const Tile& t, double idx, double idy, const BCd& b, int homog, int i, int j,
-                                         int xr, int yr, double omega) {
-    double* c = t.s + (j - t.poy) * PW + (i - t.pox);
-    St9 s;
-    gather9(SLoad{c, PW}, xr, yr, s);
-    Faces fc;
-    fc.xxw = c[oXX]; fc.xxe = c[oXX + 1];
-    fc.xyw = c[oXY]; fc.xye = c[oXY + 1];
-    fc.yys = c[oYY]; fc.yyn = c[oYY + PW];
-    fc.yxs = c[oYX]; fc.yxn = c[oYX + PW];
-    const double lphi = lap9f(s, fc, idx, idy, i, j, xr, yr, b, homog);
-    const double p = c[0];
-    const double newphi = p + (c[oF] - lphi) * c[oD];
-    c[0] = omega * newphi + (1.0 - omega) * p;
+template <class T>
+__device__ __forceinline__ void gs9_tile(const Tile<T>& t, T idx, T idy, const BCd& b, int homog, int i, int j, int xr,
+                                         int yr, double omega) {
+    using W = Win<T>;
+    T* c = t.s + (j - t.poy) * W::PW + (i - t.pox);
+    St9T<T> s;
+    gather9(SLoadT<T>{c, W::PW}, xr, yr, s);
+    FacesT<T> fc;
+    fc.xxw = c[W::oXX]; fc.xxe = c[W::oXX + 1];
+    fc.xyw = c[W::oXY]; fc.xye = c[W::oXY + 1];
+    fc.yys = c[W::oYY]; fc.yyn = c[W::oYY + W::PW];
+    fc.yxs = c[W::oYX]; fc.yxn = c[W::oYX + W::PW];
+    const T lphi = lap9f(s, fc, idx, idy, i, j, xr, yr, b, homog);
+    const T p = c[0];
+    const T newphi = p + (c[W::oF] - lphi) * c[W::oD];
+    c[0] = T(omega) * newphi + T(1.0 - omega) * p;
 }
 
-template <bool kTma>
-__global__ void __launch_bounds__(kSweepThreads, 2)
-    k_sweep9(const __grid_constant__ SweepMaps m, DF pin, DF pout, DF rhs, DF invd, Geo g, BCd b, int homog, int nx,
-             int ny, double omega, int* status) {
-    extern __shared__ __align__(1024) double smem[];
+template <bool kTma, class T>
+__global__ void __launch_bounds__(kSweepThreads, Win<T>::kMinBlocks)
+    k_sweep9(const __grid_constant__ SweepMaps m, DFT<T> pin, DFT<T> pout, DFT<T> rhs, DFT<T> invd, GeoT<T> g, BCd b,
+             int homog, int nx, int ny, double omega, int* status) {
+    using W = Win<T>;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    T* smem = reinterpret_cast<T*>(smem_raw);
     const int X0 = (int)((long)blockIdx.x * nx / gridDim.x), X1 = (int)((long)(blockIdx.x + 1) * nx / gridDim.x);
     const int Y0 = (int)((long)blockIdx.y * ny / gridDim.y), Y1 = (int)((long)(blockIdx.y + 1) * ny / gridDim.y);
     const Per pr = periodic_of(b);
     const bool edge_tile = (!pr.xl && X0 == 0) || (!pr.xh && X1 >= nx) || (!pr.yl && Y0 == 0) || (!pr.yh && Y1 >= ny);
     const int E = edge_tile ? 2 : 0;
+    const T idx = T(g.idx), idy = T(g.idy);
 
-    Tile t;
+    Tile<T> t;
     t.s = smem;
-    t.pox = (X0 - kH) & ~1; t.poy = Y0 - kH;
+    t.pox = (X0 - kH) & ~(W::kAlign - 1);
+    t.poy = Y0 - kH;
 
     // interior colour ranges (i in [mi0, mi1), j in [mj0, mj1)) on shrinking
     // regions, and their divide-free index maps, set up while the loads fly
@@ -203,7 +237,8 @@ __global__ void __launch_bounds__(kSweepThreads, 2)
     const int ci0s = max(X0 - hc, 0), ci1s = min(X1 + hc, nx), cj0s = max(Y0 - hc, 0), cj1s = min(Y1 + hc, ny);
     if (kTma) {
         // the whole window of every array; what lies outside a field reads as 0 and is never used
-        const unsigned sb = (unsigned)__cvta_generic_to_shared(smem), bar = sb + oBar * 8;
+        const unsigned sb = (unsigned)__cvta_generic_to_shared(smem), bar = sb + W::oBarBytes;
+        constexpr unsigned kS = sizeof(T);
         if (sb & 127) {   // TMA destinations must be 128-byte aligned
             if (threadIdx.x == 0 && status) atomicExch(status, 3);
             return;
@@ -211,14 +246,14 @@ __global__ void __launch_bounds__(kSweepThreads, 2)
         if (threadIdx.x == 0) mbar_init(bar, 1);
         __syncthreads();
         if (threadIdx.x == 0) {
-            mbar_expect_tx(bar, 7 * kBoxBytes);
+            mbar_expect_tx(bar, 7 * W::kBoxBytes);
             tma_load_2d(sb, &m.pin, t.pox - m.pcb, t.poy - m.prb, bar);
-            tma_load_2d(sb + oF * 8, &m.rhs, t.pox, t.poy, bar);
-            tma_load_2d(sb + oD * 8, &m.invd, t.pox, t.poy, bar);
-            tma_load_2d(sb + oXX * 8, &m.xx, t.pox, t.poy, bar);
-            tma_load_2d(sb + oXY * 8, &m.xy, t.pox, t.poy, bar);
-            tma_load_2d(sb + oYX * 8, &m.yx, t.pox, t.poy, bar);
-            tma_load_2d(sb + oYY * 8, &m.yy, t.pox, t.poy, bar);
+            tma_load_2d(sb + W::oF * kS, &m.rhs, t.pox, t.poy, bar);
+            tma_load_2d(sb + W::oD * kS, &m.invd, t.pox, t.poy, bar);
+            tma_load_2d(sb + W::oXX * kS, &m.xx, t.pox, t.poy, bar);
+            tma_load_2d(sb + W::oXY * kS, &m.xy, t.pox, t.poy, bar);
+            tma_load_2d(sb + W::oYX * kS, &m.yx, t.pox, t.poy, bar);
+            tma_load_2d(sb + W::oYY * kS, &m.yy, t.pox, t.poy, bar);
         }
         colour_ranges(X0, X1, Y0, Y1, E, mi0, mi1, mj0, mj1, ci0, cj0, ccw, cn, cm);
         if (!mbar_wait0(bar)) {   // never seen; leave the tile unwritten and report
@@ -227,13 +262,13 @@ __global__ void __launch_bounds__(kSweepThreads, 2)
             return;
         }
     } else {
-        stage(smem, PW, t.pox, t.poy, pin, pi0, pi1, pj0, pj1);
-        stage(smem + oF, PW, t.pox, t.poy, rhs, ci0s, ci1s, cj0s, cj1s);
-        stage(smem + oD, PW, t.pox, t.poy, invd, ci0s, ci1s, cj0s, cj1s);
-        stage(smem + oXX, PW, t.pox, t.poy, g.xx, ci0s, ci1s + 1, cj0s, cj1s);
-        stage(smem + oXY, PW, t.pox, t.poy, g.xy, ci0s, ci1s + 1, cj0s, cj1s);
-        stage(smem + oYX, PW, t.pox, t.poy, g.yx, ci0s, ci1s, cj0s, cj1s + 1);
-        stage(smem + oYY, PW, t.pox, t.poy, g.yy, ci0s, ci1s, cj0s, cj1s + 1);
+        stage(smem, W::PW, t.pox, t.poy, pin, pi0, pi1, pj0, pj1);
+        stage(smem + W::oF, W::PW, t.pox, t.poy, rhs, ci0s, ci1s, cj0s, cj1s);
+        stage(smem + W::oD, W::PW, t.pox, t.poy, invd, ci0s, ci1s, cj0s, cj1s);
+        stage(smem + W::oXX, W::PW, t.pox, t.poy, g.xx, ci0s, ci1s + 1, cj0s, cj1s);
+        stage(smem + W::oXY, W::PW, t.pox, t.poy, g.xy, ci0s, ci1s + 1, cj0s, cj1s);
+        stage(smem + W::oYX, W::PW, t.pox, t.poy, g.yx, ci0s, ci1s, cj0s, cj1s + 1);
+        stage(smem + W::oYY, W::PW, t.pox, t.poy, g.yy, ci0s, ci1s, cj0s, cj1s + 1);
         colour_ranges(X0, X1, Y0, Y1, E, mi0, mi1, mj0, mj1, ci0, cj0, ccw, cn, cm);
         cp_async_wait_all();
         __syncthreads();
@@ -241,7 +276,7 @@ __global__ void __launch_bounds__(kSweepThreads, 2)
     // 2. sweep-start ghost fill on the staged ghost cells (the ghost rows and
     //    columns of tiles on the domain boundary only)
     if (pi0 < 0 || pi1 > nx || pj0 < 0 || pj1 > ny) {
-        const PinLoad P{smem, t.pox, t.poy, pi0, pi1, pj0, pj1, pin};
+        const PinLoad<T> P{smem, t.pox, t.poy, pi0, pi1, pj0, pj1, pin};
         const int lw = pi1 - pi0, lh = pj1 - pj0;
         for (int k = threadIdx.x; k < 2 * (lw + lh); k += blockDim.x) {
             int i, j;
@@ -250,7 +285,7 @@ __global__ void __launch_bounds__(kSweepThreads, 2)
             else if (k < 2 * lw + lh) { i = pi0; j = pj0 + k - 2 * lw; }
             else { i = pi1 - 1; j = pj0 + k - 2 * lw - lh; }
             if (i >= 0 && i < nx && j >= 0 && j < ny) continue;
-            smem[(j - t.poy) * PW + (i - t.pox)] = sweep_ghost(P, b, homog, nx, ny, i, j);
+            smem[(j - t.poy) * W::PW + (i - t.pox)] = sweep_ghost(P, b, homog, nx, ny, i, j);
         }
     }
     __syncthreads();
@@ -263,7 +298,7 @@ __global__ void __launch_bounds__(kSweepThreads, 2)
         for (int k = threadIdx.x; k < cn[c]; k += blockDim.x) {
             const int kj = fastdiv(k, cm[c]);
             const int i = ci0[c] + 2 * (k - kj * ccw[c]), j = cj0[c] + 2 * kj;
-            gs9_tile(t, g.idx, g.idy, b, homog, i, j, RMID, RMID, omega);
+            gs9_tile(t, idx, idy, b, homog, i, j, RMID, RMID, omega);
         }
         __syncthreads();
     }
@@ -285,10 +320,10 @@ __global__ void __launch_bounds__(kSweepThreads, 2)
             const int n2 = n1 + ((sxl && ci == 0) ? nj : 0);
             const int n3 = n2 + ((sxh && ((nx - 1) & 1) == ci) ? nj : 0);
             for (int k = threadIdx.x; k < n3; k += blockDim.x) {
-                if (k < n0) gs9_tile(t, g.idx, g.idy, b, homog, ia + 2 * k, 0, RMID, RLO, omega);
-                else if (k < n1) gs9_tile(t, g.idx, g.idy, b, homog, ia + 2 * (k - n0), ny - 1, RMID, RHI, omega);
-                else if (k < n2) gs9_tile(t, g.idx, g.idy, b, homog, 0, ja + 2 * (k - n1), RLO, RMID, omega);
-                else gs9_tile(t, g.idx, g.idy, b, homog, nx - 1, ja + 2 * (k - n2), RHI, RMID, omega);
+                if (k < n0) gs9_tile(t, idx, idy, b, homog, ia + 2 * k, 0, RMID, RLO, omega);
+                else if (k < n1) gs9_tile(t, idx, idy, b, homog, ia + 2 * (k - n0), ny - 1, RMID, RHI, omega);
+                else if (k < n2) gs9_tile(t, idx, idy, b, homog, 0, ja + 2 * (k - n1), RLO, RMID, omega);
+                else gs9_tile(t, idx, idy, b, homog, nx - 1, ja + 2 * (k - n2), RHI, RMID, omega);
             }
             __syncthreads();
         }
@@ -297,7 +332,7 @@ __global__ void __launch_bounds__(kSweepThreads, 2)
                 const int i = (c & 1) ? nx - 1 : 0, j = (c & 2) ? ny - 1 : 0;
                 if (i < X0 || i >= X1 || j < Y0 || j >= Y1) continue;
                 const int xr = region(i, nx, pr.xl, pr.xh), yr = region(j, ny, pr.yl, pr.yh);
-                if (xr != RMID && yr != RMID) gs9_tile(t, g.idx, g.idy, b, homog, i, j, xr, yr, omega);
+                if (xr != RMID && yr != RMID) gs9_tile(t, idx, idy, b, homog, i, j, xr, yr, omega);
             }
         }
         __syncthreads();
@@ -309,8 +344,8 @@ __global__ void __launch_bounds__(kSweepThreads, 2)
     const int wj0 = (Y0 == 0) ? -1 : Y0, wj1 = (Y1 >= ny) ? ny + 1 : Y1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int j = wj0 + warp; j < wj1; j += (blockDim.x >> 5)) {
-        const double* srow = smem + (j - t.poy) * PW - t.pox;
-        double* grow = &AT(pout, 0, j);
+        const T* srow = smem + (j - t.poy) * W::PW - t.pox;
+        T* grow = &AT(pout, 0, j);
         for (int i = wi0 + lane; i < wi1; i += 32) grow[i] = srow[i];
     }
 }
@@ -342,28 +377,85 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-// A FP64 2-D map of `width` x `height` elements at `base`, row pitch ld, box PW x PH.
-bool encode(CUtensorMap* m, const double* base, long width, long height, int ld) {
+template <class T>
+constexpr CUtensorMapDataType map_type() {
+    return sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+}
+
+// A 2-D map of `width` x `height` elements at `base`, row pitch ld, box PW x PH.
+template <class T>
+bool encode(CUtensorMap* m, const T* base, long width, long height, int ld) {
     const PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
-    if (!fn || ((uintptr_t)base & 15) || (((long)ld * 8) & 15) || width > ld || width <= 0 || height <= 0) return false;
+    if (!fn || ((uintptr_t)base & 15) || (((long)ld * (long)sizeof(T)) & 15) || width > ld || width <= 0 ||
+        height <= 0)
+        return false;
     const cuuint64_t dims[2] = {(cuuint64_t)width, (cuuint64_t)height};
-    const cuuint64_t strides[1] = {(cuuint64_t)ld * 8};
-    const cuuint32_t box[2] = {PW, PH};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(T)};
+    const cuuint32_t box[2] = {(cuuint32_t)Win<T>::PW, (cuuint32_t)Win<T>::PH};
     const cuuint32_t es[2] = {1, 1};
-    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims, strides, box, es,
-              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+    return fn(m, map_type<T>(), 2, const_cast<T*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-bool prepare_maps(SweepMaps* m, const DF& e, const DF& rhs, const DF& invd, const Geo& g, int nx, int ny) {
-    // phi from column -2 (an even offset keeps x even) and row -1; the ghost column nx must lie inside
-    m->pcb = -2;
+template <class T>
+bool prepare_maps(SweepMaps* m, const DFT<T>& e, const DFT<T>& rhs, const DFT<T>& invd, const GeoT<T>& g, int nx,
+                  int ny) {
+    // phi from the 16-byte-aligned column kAlign left of column 0 (so the
+    // ghost column -1 is inside), and row -1; the ghost column nx must lie
+    // inside the pitch
+    m->pcb = -Win<T>::kAlign;
     m->prb = -1;
-    if (e.ld < nx + 3) return false;
-    return encode(&m->pin, &AT(e, -2, -1), e.ld, ny + 2, e.ld) && encode(&m->rhs, rhs.p, nx, ny, rhs.ld) &&
+    if (e.ld < nx + 1 + Win<T>::kAlign) return false;
+    return encode(&m->pin, &AT(e, m->pcb, -1), e.ld, ny + 2, e.ld) && encode(&m->rhs, rhs.p, nx, ny, rhs.ld) &&
            encode(&m->invd, invd.p, nx, ny, invd.ld) && encode(&m->xx, g.xx.p, nx + 1, ny, g.xx.ld) &&
            encode(&m->xy, g.xy.p, nx + 1, ny, g.xy.ld) && encode(&m->yx, g.yx.p, nx, ny + 1, g.yx.ld) &&
            encode(&m->yy, g.yy.p, nx, ny + 1, g.yy.ld);
+}
+
+template <class T>
+cudaError_t set_attr() {
+    cudaError_t e = cudaFuncSetAttribute(k_sweep9<true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)Win<T>::kSmemBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sweep9<false, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)Win<T>::kSmemBytes);
+    return e;
+}
+
+template <class T>
+void tma_prepare(SweepTma* t, const DFT<T>& ea, const DFT<T>& eb, const DFT<T>& rhs, const DFT<T>& invd,
+                 const GeoT<T>& g, int nx, int ny) {
+    t->ok = prepare_maps(&t->ma, ea, rhs, invd, g, nx, ny) && prepare_maps(&t->mb, eb, rhs, invd, g, nx, ny);
+    t->pa = ea.p;
+    t->pb = eb.p;
+    t->rhs = rhs.p;
+    t->invd = invd.p;
+    t->xx = g.xx.p;
+}
+
+template <class T>
+cudaError_t sweep_impl(const DFT<T>& pin, const DFT<T>& pout, const DFT<T>& rhs, const DFT<T>& invd,
+                       const GeoT<T>& g, const BCd& b, int homog, int nx, int ny, double omega, const SweepTma* tma,
+                       int* status, cudaStream_t st) {
+    cudaError_t e = sweep_kernels_init();
+    if (e != cudaSuccess) return e;
+    const SweepMaps* m = nullptr;
+    if (tma && tma->ok && (const void*)rhs.p == tma->rhs && (const void*)invd.p == tma->invd &&
+        (const void*)g.xx.p == tma->xx)
+        m = ((const void*)pin.p == tma->pa) ? &tma->ma : ((const void*)pin.p == tma->pb) ? &tma->mb : nullptr;
+    dim3 grd((nx + kTX - 1) / kTX, (ny + kTY - 1) / kTY);
+    const size_t smem = Win<T>::kSmemBytes;
+    if (m) {
+        k_sweep9<true, T><<<grd, kSweepThreads, smem, st>>>(*m, pin, pout, rhs, invd, g, b, homog, nx, ny, omega,
+                                                            status);
+    } else {
+        static const SweepMaps none{};
+        k_sweep9<false, T><<<grd, kSweepThreads, smem, st>>>(none, pin, pout, rhs, invd, g, b, homog, nx, ny, omega,
+                                                             status);
+    }
+    count_launch();
+    return cudaGetLastError();
 }
 
 }  // namespace
@@ -377,42 +469,30 @@ cudaError_t sweep_kernels_init() {
     if (e != cudaSuccess) return e;
     std::lock_guard<std::mutex> lock(mu);
     if (dev < 64 && (done >> dev) & 1ull) return cudaSuccess;
-    e = cudaFuncSetAttribute(k_sweep9<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_sweep9<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+    e = set_attr<double>();
+    if (e == cudaSuccess) e = set_attr<float>();
     if (e == cudaSuccess && dev < 64) done |= 1ull << dev;
     return e;
 }
 
 void sweep_tma_prepare(SweepTma* t, const DF& ea, const DF& eb, const DF& rhs, const DF& invd, const Geo& g, int nx,
                        int ny) {
-    t->ok = prepare_maps(&t->ma, ea, rhs, invd, g, nx, ny) && prepare_maps(&t->mb, eb, rhs, invd, g, nx, ny);
-    t->pa = ea.p;
-    t->pb = eb.p;
-    t->rhs = rhs.p;
-    t->invd = invd.p;
-    t->xx = g.xx.p;
+    tma_prepare(t, ea, eb, rhs, invd, g, nx, ny);
+}
+void sweep_tma_prepare(SweepTma* t, const DF32& ea, const DF32& eb, const DF32& rhs, const DF32& invd,
+                       const Geo32& g, int nx, int ny) {
+    tma_prepare(t, ea, eb, rhs, invd, g, nx, ny);
 }
 
 cudaError_t launch_sweep9(const DF& pin, const DF& pout, const DF& rhs, const DF& invd, const Geo& g, const BCd& b,
                           int homog, int nx, int ny, double omega, const SweepTma* tma, int* status,
                           cudaStream_t st) {
-    cudaError_t e = sweep_kernels_init();
-    if (e != cudaSuccess) return e;
-    const SweepMaps* m = nullptr;
-    if (tma && tma->ok && rhs.p == tma->rhs && invd.p == tma->invd && g.xx.p == tma->xx)
-        m = (pin.p == tma->pa) ? &tma->ma : (pin.p == tma->pb) ? &tma->mb : nullptr;
-    dim3 grd((nx + kTX - 1) / kTX, (ny + kTY - 1) / kTY);
-    if (m) {
-        k_sweep9<true><<<grd, kSweepThreads, kSmemBytes, st>>>(*m, pin, pout, rhs, invd, g, b, homog, nx, ny, omega,
-                                                               status);
-    } else {
-        static const SweepMaps none{};
-        k_sweep9<false><<<grd, kSweepThreads, kSmemBytes, st>>>(none, pin, pout, rhs, invd, g, b, homog, nx, ny,
-                                                                omega, status);
-    }
-    count_launch();
-    return cudaGetLastError();
+    return sweep_impl(pin, pout, rhs, invd, g, b, homog, nx, ny, omega, tma, status, st);
+}
+cudaError_t launch_sweep9(const DF32& pin, const DF32& pout, const DF32& rhs, const DF32& invd, const Geo32& g,
+                          const BCd& b, int homog, int nx, int ny, double omega, const SweepTma* tma, int* status,
+                          cudaStream_t st) {
+    return sweep_impl(pin, pout, rhs, invd, g, b, homog, nx, ny, omega, tma, status, st);
 }
 
 }  // namespace mgp

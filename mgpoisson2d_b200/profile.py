@@ -1,6 +1,6 @@
 """A short, fixed run of the benchmark workload for profilers:
 
-    python -m mgpoisson2d_b200.profile [--n 1024] [--vcycles 2] [--warmup 1]
+    python -m mgpoisson2d_b200.profile [--n 1024] [--vcycles 2] [--warmup 1] [--mixed] [--krylov]
 
 Builds the resident solver for the 1024x1024 stretched mapped grid (the bench
 workload), runs `warmup` solves capped at `vcycles` V-cycles, then one more,
@@ -19,6 +19,8 @@ def main():
     p.add_argument("--vcycles", type=int, default=2)
     p.add_argument("--warmup", type=int, default=1)
     p.add_argument("--dd", action="store_true", help="deferred-correction driver")
+    p.add_argument("--mixed", action="store_true", help="FP32 grid levels (MGP_FLAG_MIXED)")
+    p.add_argument("--krylov", action="store_true", help="BiCGStab acceleration (MGP_FLAG_KRYLOV)")
     a = p.parse_args()
 
     import torch
@@ -30,7 +32,8 @@ def main():
     torch.cuda.set_device(0)
     v, geo, rhs, bc, _ = W.wavy_stretched(a.n)
     kind = M.KIND_DD if a.dd else M.KIND_MG
-    s = M.Solver(v, geo, bc, kind, M.FLAG_DIRICHLET_COUPLED_DIAG)
+    flags = M.FLAG_DIRICHLET_COUPLED_DIAG | (M.FLAG_MIXED if a.mixed else 0) | (M.FLAG_KRYLOV if a.krylov else 0)
+    s = M.Solver(v, geo, bc, kind, flags)
     phi, f = BoxData(v, 1, 1).to_device(), rhs.to_device()
     if a.dd:
         f.data /= geo.J.to_device().data[1:-1, 1:-1]

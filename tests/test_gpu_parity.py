@@ -371,3 +371,63 @@ def test_krylov_oneshot_device_arrays_and_maxiters(M):
         O.lib().or_set_dirichlet_coupled_diagonal(0)
     np.testing.assert_allclose(re.relres, ro, rtol=1e-7)
     np.testing.assert_allclose(pe.data, oa.data, rtol=0, atol=1e-10 * np.abs(oa.data).max())
+
+
+# ---------------------------------------------------------------------------
+# Mixed precision (MGP_FLAG_MIXED; no reference counterpart): FP32 grid levels
+# inside the FP64 outer iteration
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("krylov", [False, True])
+def test_mixed_vcycle_converges_to_fp64_solution(M, krylov):
+    """The outer iteration and its residual stay FP64, so the mixed solve must
+    reach the same 1e-10 relative residual and the same solution as the FP64
+    oracle, in about as many V-cycles as the FP64 device solve."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, _ = W.wavy_stretched(128)
+    base = M.FLAG_DIRICHLET_COUPLED_DIAG | (M.FLAG_KRYLOV if krylov else 0)
+    old = _set_coupled(M, True)
+    try:
+        po = BoxData(v, 1, 1)
+        O.vcycle(po, rhs, geo, bc, True, 1e-11, 3000, gs_order=1)
+    finally:
+        _set_coupled(M, old)
+    with M.Solver(v, geo, bc, KIND_MG, base) as s:
+        p64 = BoxData(v, 1, 1)
+        r64 = s.vcycle(p64, rhs, bc, True, 1e-10, 3000)
+    with M.Solver(v, geo, bc, KIND_MG, base | M.FLAG_MIXED) as s:
+        p32 = BoxData(v, 1, 1)
+        r32 = s.vcycle(p32, rhs, bc, True, 1e-10, 3000)
+        p32b = BoxData(v, 1, 1)
+        r32b = s.vcycle(p32b, rhs, bc, True, 1e-10, 3000)
+    assert r32.status == 0 and not r32.diverged and r32.final_relres <= 1e-10
+    # the plain iteration contracts at the same rate in FP32; BiCGStab's count
+    # moves with the preconditioner's rounding, within a fifth either way
+    assert abs(r32.iterations - r64.iterations) <= max(3, r64.iterations // (5 if krylov else 10))
+    assert same(p32.data, p32b.data) and np.array_equal(r32.relres, r32b.relres)   # deterministic
+    err = p32.interior() - po.interior()
+    assert np.linalg.norm(err) / np.linalg.norm(po.interior()) < 1e-8
+    assert np.abs(err).max() / np.abs(po.interior()).max() < 1e-7
+
+
+def test_mixed_all_neumann_and_identity(M):
+    """Mixed precision with the mean removal of an all-Neumann hierarchy (the
+    terrain solver test) and on the identity map with Dirichlet sides."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, soln = W.terrain_neumann(64, O.boundary_fluxes, O.compute_laplacian)
+    pa, pb = BoxData(v, 1, 1), BoxData(v, 1, 1)
+    with M.Solver(v, geo, bc, KIND_MG, 0) as s:
+        ra = s.vcycle(pa, rhs, bc, False, 1e-9, 200)
+    with M.Solver(v, geo, bc, KIND_MG, M.FLAG_MIXED) as s:
+        rb = s.vcycle(pb, rhs, bc, False, 1e-9, 200)
+    assert ra.final_relres <= 1e-9 and rb.final_relres <= 1e-9
+    d = (pb.interior() - pb.interior().mean()) - (pa.interior() - pa.interior().mean())
+    assert np.abs(d).max() < 1e-7 * np.abs(pa.interior()).max()
+    v, geo, rhs, bc, u = W.identity_dirichlet(96)
+    with M.Solver(v, geo, bc, KIND_MG, M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_MIXED | M.FLAG_KRYLOV) as s:
+        pc = BoxData(v, 1, 1)
+        rc = s.vcycle(pc, rhs, bc, True, 1e-11, 100)
+    with M.Solver(v, geo, bc, KIND_MG, M.FLAG_DIRICHLET_COUPLED_DIAG) as s:
+        pd = BoxData(v, 1, 1)
+        s.vcycle(pd, rhs, bc, True, 1e-11, 100)
+    assert rc.final_relres <= 1e-11
+    assert np.abs(pc.interior() - pd.interior()).max() < 1e-8 * np.abs(pd.interior()).max()
