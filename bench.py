@@ -7,9 +7,12 @@ x sides, Neumann y sides; seeded 16-mode Fourier rhs, J-weighted mean removed).
 
 One step = one full solve (until |r|/|r0| <= 1e-10) of that problem.  The
 default solver is the V-cycle accelerated by BiCGStab (MGP_FLAG_KRYLOV: one
-unchanged V-cycle per preconditioner application); --solver vcycle times the
-reference's stationary V-cycle iteration instead.  The line always carries the
-plain V-cycle solve's numbers too ("plain_vcycle", one timed solve).  Under
+unchanged V-cycle per preconditioner application) with the V-cycle's grid
+levels in FP32 inside the FP64 outer iteration (MGP_FLAG_MIXED);
+--solver vcycle and --precision fp64 select the reference's stationary
+iteration and plain FP64.  The line also carries one timed solve of the same
+solver in FP64 ("fp64_same_solver") and of the plain FP64 V-cycle iteration
+("plain_vcycle"), and the headline solution's error against both.  Under
 torchrun every rank solves its own copy (replicas; the solve does not shard)
 and rank 0 prints one JSON line.
 
@@ -36,7 +39,7 @@ N_GRID = 1024
 TOL = 1e-10
 MAXITERS = 4000
 NU = (8, 8, 8)            # smooth_down, smooth_up, smooth_bottom (the reference test setting, test.f90:2546-2548)
-METRIC = "solves/s @1e-10 rel resid (FP64 GPU)"
+METRIC = "solves/s @1e-10 rel resid"
 WORKLOAD = "wavy_stretched_1024"
 # words moved per cell by one smoothing sweep: read phi, rhs, invdiag, 4 Jgup; write phi
 SWEEP_WORDS = 8
@@ -54,6 +57,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--solver", default="krylov", choices=["krylov", "vcycle"])
+    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                   help="mixed: FP32 grid levels inside the FP64 outer iteration (MGP_FLAG_MIXED)")
     p.add_argument("--no-plain", action="store_true", help="skip the extra plain V-cycle solve")
     return p.parse_args()
 
@@ -228,7 +233,8 @@ def main():
 
     v, geo, rhs, bc, _ = workload(args.n)
     base_flags = M.FLAG_DIRICHLET_COUPLED_DIAG
-    flags = base_flags | (M.FLAG_KRYLOV if args.solver == "krylov" else 0)
+    fp64_flags = base_flags | (M.FLAG_KRYLOV if args.solver == "krylov" else 0)
+    flags = fp64_flags | (M.FLAG_MIXED if args.precision == "mixed" else 0)
     solver = M.Solver(v, geo, bc, M.KIND_MG, flags)
     phi_d = BoxData(v, 1, 1).to_device()
     rhs_d = rhs.to_device()
@@ -277,23 +283,41 @@ def main():
     latency = {"p50": srt[len(srt) // 2], "p99": srt[min(len(srt) - 1, math.ceil(0.99 * len(srt)) - 1)],
                "unit": "ms", "samples": len(srt)}
 
-    # the reference's stationary iteration on the same solver, for comparison
-    plain = None
-    if args.solver == "vcycle":
-        plain = {"solves_per_s": value, "ms_per_solve": total_ms / args.steps, "vcycles": last.iterations}
-    elif not args.no_plain:
-        ps = M.Solver(v, geo, bc, M.KIND_MG, base_flags)
+    sol = phi_d.to_host().interior().copy()
+
+    def one_solve(fl):
+        """One timed solve with other flags; returns (summary, solution)."""
+        ps = M.Solver(v, geo, bc, M.KIND_MG, fl)
         phi_d.data.zero_()
         flush.fill_(1.0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        prep_ = ps.vcycle(phi_d, rhs_d, bc, True, TOL, MAXITERS, 1, *NU)
+        r = ps.vcycle(phi_d, rhs_d, bc, True, TOL, MAXITERS, 1, *NU)
         e1.record(stream)
         e1.synchronize()
         ps.close()
-        pms = e0.elapsed_time(e1)
-        plain = {"solves_per_s": 1e3 / pms, "ms_per_solve": pms, "vcycles": prep_.iterations,
-                 "final_relres": prep_.final_relres, "timed_solves": 1}
+        ms = e0.elapsed_time(e1)
+        return ({"solves_per_s": 1e3 / ms, "ms_per_solve": ms, "vcycles": r.iterations,
+                 "final_relres": r.final_relres, "timed_solves": 1}, phi_d.to_host().interior().copy())
+
+    def err(a, ref):
+        return {"rel_l2": float(np.linalg.norm(a - ref) / np.linalg.norm(ref)),
+                "rel_max": float(np.abs(a - ref).max() / np.abs(ref).max())}
+
+    # the same solver in plain FP64, and the reference's stationary iteration
+    # (FP64 V-cycles), for comparison; the error of the headline solution is
+    # stated against both FP64 solutions
+    fp64 = plain = None
+    accuracy = {}
+    if not args.no_plain:
+        if args.precision == "mixed":
+            fp64, sol64 = one_solve(fp64_flags)
+            accuracy["vs_fp64_same_solver"] = err(sol, sol64)
+        if args.solver == "vcycle" and args.precision == "fp64":
+            plain = {"solves_per_s": value, "ms_per_solve": total_ms / args.steps, "vcycles": last.iterations}
+        else:
+            plain, solp = one_solve(base_flags)
+            accuracy["vs_fp64_vcycle"] = err(sol, solp)
 
     # live roofline of the dominant kernel: one more solve with the finest
     # level's smoothing bracketed by events
@@ -303,11 +327,12 @@ def main():
     prep = prof.vcycle(phi_d, rhs_d, bc, True, TOL, MAXITERS, 1, *NU)
     prof.close()
     sweep_s = prep.smooth0_seconds / max(prep.smooth0_sweeps, 1)
-    alg_bytes = SWEEP_WORDS * 8 * v.nx * v.ny
+    word = 4 if args.precision == "mixed" else 8
+    alg_bytes = SWEEP_WORDS * word * v.nx * v.ny
     peak, peak_kind = measured_peak()
     achieved = alg_bytes / sweep_s / 1e9
     tr = committed_traffic()
-    roofline = {"bound": "hbm", "kernel": "gs_sweep level 0 (ghost fill + 4 colour passes)",
+    roofline = {"bound": "hbm", "kernel": f"k_sweep9 level 0 ({'FP32' if word == 4 else 'FP64'} fields, TMA staging)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "traffic": (tr or {}).get("bytes_per_sweep"),
                 "alg_bytes_per_sweep": alg_bytes, "sweep_us": sweep_s * 1e6}
@@ -315,14 +340,17 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64+f32" if args.precision == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n": args.n, "tol": TOL, "nu": list(NU),
                    "solver": "bicgstab(vcycle)" if args.solver == "krylov" else "vcycle",
-                   "flags": "dirichlet_coupled_diag" + ("|krylov" if args.solver == "krylov" else ""),
+                   "precision": ("FP32 grid levels, FP64 outer iteration / residual / update / coarse levels"
+                                 if args.precision == "mixed" else "FP64"),
+                   "flags": "dirichlet_coupled_diag" + ("|krylov" if args.solver == "krylov" else "") +
+                            ("|mixed" if args.precision == "mixed" else ""),
                    "vcycles_per_solve": last.iterations, "final_relres": last.final_relres,
                    "maxdepth": last.maxdepth, "l2": "flushed between steps (256 MiB write, outside step events)",
                    "parallelism": f"replicas{world}"},
-        "latency_ms": latency, "plain_vcycle": plain,
+        "latency_ms": latency, "fp64_same_solver": fp64, "plain_vcycle": plain, "accuracy": accuracy,
         "roofline": roofline, "clocks": clocks, "gpu_launches": launches,
         "unknowns_vcycles_per_s": value * last.iterations * v.nx * v.ny,
         "wall_s": wall,

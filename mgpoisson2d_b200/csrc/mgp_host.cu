@@ -543,9 +543,10 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
 int smooth_body(mgp_solver* s, int d, int nu);
 
 // Level-0 smoothing, bracketed by an event pair when MGP_FLAG_TIME_SMOOTHER is set.
-int smooth(mgp_solver* s, int d, int nu) {
+template <class Body>
+int timed_smooth(mgp_solver* s, int d, int nu, Body body) {
     const bool timed = (d == 0) && (s->flags & MGP_FLAG_TIME_SMOOTHER) && nu > 0;
-    if (!timed) return smooth_body(s, d, nu);
+    if (!timed) return body();
     if (s->tev_used + 2 > s->tev.size()) {
         for (int k = 0; k < 2; ++k) {
             cudaEvent_t e;
@@ -554,11 +555,15 @@ int smooth(mgp_solver* s, int d, int nu) {
         }
     }
     CK(cudaEventRecord(s->tev[s->tev_used], s->stream));
-    RC(smooth_body(s, d, nu));
+    RC(body());
     CK(cudaEventRecord(s->tev[s->tev_used + 1], s->stream));
     s->tev_used += 2;
     s->t_sweeps += nu;
     return MGP_OK;
+}
+
+int smooth(mgp_solver* s, int d, int nu) {
+    return timed_smooth(s, d, nu, [&]() { return smooth_body(s, d, nu); });
 }
 
 int smooth_body(mgp_solver* s, int d, int nu) {
@@ -664,11 +669,14 @@ int vcycle32(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
     const Lv& F = s->lv[d];   // BCs of the level
     cudaStream_t st = s->stream;
     auto smooth32 = [&](int nu_) -> int {
-        for (int k = 0; k < nu_; ++k) {
-            CK(launch_sweep9(L.e, L.e2, L.r, L.invd, L.g, F.bc, 1, L.nx, L.ny, 1.0, &s->tma32[d], s->d_status, st));
-            std::swap(L.e, L.e2);
-        }
-        return MGP_OK;
+        return timed_smooth(s, d, nu_, [&]() -> int {
+            for (int k = 0; k < nu_; ++k) {
+                CK(launch_sweep9(L.e, L.e2, L.r, L.invd, L.g, F.bc, 1, L.nx, L.ny, 1.0, &s->tma32[d], s->d_status,
+                                 st));
+                std::swap(L.e, L.e2);
+            }
+            return MGP_OK;
+        });
     };
     RC(smooth32(nd));
     CK(launch_fill(L.e, L.g, F.bc, 1, 0, L.nx, L.ny, st));
