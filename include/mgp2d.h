@@ -27,6 +27,8 @@
 #ifndef MGP2D_H
 #define MGP2D_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -285,6 +287,45 @@ int mgp_solver_dc_vcycle(mgp_solver *s, mgp_array *phi, mgp_array *rhs, const mg
                          int homog, double tol, int maxiters, int numcycles, int smooth_down,
                          int smooth_up, int smooth_bottom, int zerophi, int verbosity,
                          mgp_report *report);
+
+/* ------------------------------------------------------------------------ */
+/* Many solves at once.  No reference counterpart: the Fortran library solves */
+/* one problem per call.  Both front ends run the single-problem solver       */
+/* unchanged on several host workers, each with its own CUDA stream, so the   */
+/* latency-bound kernels of different problems overlap on the device; every  */
+/* result is identical to solving its problem alone.                          */
+/* ------------------------------------------------------------------------ */
+typedef struct mgp_batch mgp_batch;
+/* nprob independent problems (arrays of nprob boxes, geometries and BC types),
+ * each with its own resident hierarchy; nstreams workers. */
+int mgp_batch_create(int nprob, const mgp_box *valid, const mgp_geo *geo, const mgp_bdry *bc, int kind,
+                     int flags, int maxdepth_user, int nstreams, mgp_batch **out);
+int mgp_batch_destroy(mgp_batch *b);
+int mgp_batch_size(const mgp_batch *b, int *nprob);
+/* vcycle on every problem: phi, rhs, bc and reports (nullable) are arrays of
+ * nprob.  Returns the first nonzero status; each report holds its own. */
+int mgp_batch_vcycle(mgp_batch *b, mgp_array *phi, mgp_array *rhs, const mgp_bdry *bc, int homog,
+                     double tol, int maxiters, int numcycles, int smooth_down, int smooth_up,
+                     int smooth_bottom, int zerophi, mgp_report *reports);
+
+typedef struct mgp_server mgp_server;
+/* A solve server with nworkers slots.  Requests start in arrival order as a
+ * slot frees up and the device memory their hierarchy needs fits within
+ * mem_budget bytes (0: 90% of the memory free at creation), evicting idle
+ * cached hierarchies first.  The hierarchy of a request with a nonzero key
+ * stays resident and serves later requests with the same key and box. */
+int mgp_server_create(int nworkers, size_t mem_budget, int flags, mgp_server **out);
+/* Queue one vcycle solve (the mgp_solver_vcycle arguments).  Every array the
+ * request names must stay alive until mgp_server_wait returns for it. */
+int mgp_server_submit(mgp_server *s, unsigned long long key, const mgp_box *valid,
+                      const mgp_geo *geo, const mgp_bdry *bc, mgp_array *phi, mgp_array *rhs,
+                      int homog, double tol, int maxiters, int numcycles, int smooth_down,
+                      int smooth_up, int smooth_bottom, int zerophi, long long *ticket);
+/* Block until the ticket's solve is done; report, latency (submit to done) and
+ * queue time (submit to start), in seconds, are each nullable. */
+int mgp_server_wait(mgp_server *s, long long ticket, mgp_report *report, double *latency_s,
+                    double *queue_s);
+int mgp_server_destroy(mgp_server *s);
 
 #ifdef __cplusplus
 }

@@ -9,7 +9,7 @@ use; they raise ImportError when the CUDA library has not been built.
 from .types import *  # noqa: F401,F403
 
 _API_NAMES = {
-    "vcycle", "fmg", "dc_vcycle", "Solver", "fill_ghosts", "extrapolate_ghosts", "compute_invdiags",
+    "vcycle", "fmg", "dc_vcycle", "Solver", "Batch", "Server", "fill_ghosts", "extrapolate_ghosts", "compute_invdiags",
     "compute_laplacian", "compute_residual", "relax_gs", "solve_bicgstab2", "solve_bicgstab2_noalloc", "restrict", "prolong",
     "pnorm", "inner_prod", "estimate_maxdepth", "create_mgschedule", "MGPError", "library_path",
     "kernel_launch_count", "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV", "FLAG_MIXED",

@@ -65,6 +65,15 @@ _SIGS = {
     "mgp_solver_vcycle": [_vp, _A, _A, _BC, _i, _d, _i, _i, _i, _i, _i, _i, _i, _R],
     "mgp_solver_fmg": [_vp, _A, _A, _BC, _i, _d, _i, _i, _i, _i, _i, _i, _i, _R],
     "mgp_solver_dc_vcycle": [_vp, _A, _A, _BC, _i, _d, _i, _i, _i, _i, _i, _i, _i, _R],
+    "mgp_batch_create": [_i, _B, _G, _BC, _i, _i, _i, _i, _P(_vp)],
+    "mgp_batch_destroy": [_vp],
+    "mgp_batch_size": [_vp, _P(_i)],
+    "mgp_batch_vcycle": [_vp, _A, _A, _BC, _i, _d, _i, _i, _i, _i, _i, _i, _R],
+    "mgp_server_create": [_i, C.c_size_t, _i, _P(_vp)],
+    "mgp_server_submit": [_vp, C.c_ulonglong, _B, _G, _BC, _A, _A, _i, _d, _i, _i, _i, _i, _i, _i,
+                          _P(C.c_longlong)],
+    "mgp_server_wait": [_vp, C.c_longlong, _R, _P(_d), _P(_d)],
+    "mgp_server_destroy": [_vp],
 }
 for _name, _args in _SIGS.items():
     _f = getattr(_lib, _name)
@@ -309,7 +318,103 @@ class Solver:
                            numcycles, smooth_down, smooth_up, smooth_bottom, zerophi, verbosity)
 
 
+class Batch:
+    """Independent problems solved concurrently (mgp_batch_*): one resident
+    hierarchy per problem, ``nstreams`` host workers with their own streams.
+    ``problems`` is a list of (valid, geo, bc)."""
+
+    def __init__(self, problems, kind: int = KIND_MG, flags: int = 0, maxdepth_user: int = -1, nstreams: int = 8):
+        n = len(problems)
+        self._boxes = (MgpBox * n)(*[p[0].c() for p in problems])
+        self._geos = (MgpGeo * n)(*[p[1].c() for p in problems])
+        self._bcs = (MgpBdry * n)(*[p[2].c() for p in problems])
+        self._keep = problems   # the geometry arrays must outlive the batch's set-up
+        self._h = C.c_void_p()
+        _ck(_lib.mgp_batch_create(n, self._boxes, self._geos, self._bcs, kind, flags, maxdepth_user, nstreams,
+                                  _r(self._h)), "batch_create")
+        self.n = n
+
+    def close(self):
+        if self._h:
+            _lib.mgp_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def vcycle(self, phis, rhss, bcs, homog, tol, maxiters, numcycles=1, smooth_down=8, smooth_up=8,
+               smooth_bottom=8, zerophi=False):
+        n = self.n
+        reps, bufs = zip(*[make_report(maxiters) for _ in range(n)])
+        rarr = (MgpReport * n)(*reps)
+        parr = (MgpArray * n)(*[p.c() for p in phis])
+        farr = (MgpArray * n)(*[f.c() for f in rhss])
+        barr = (MgpBdry * n)(*[b.c() for b in bcs])
+        _ck(_lib.mgp_batch_vcycle(self._h, parr, farr, barr, int(homog), tol, maxiters, numcycles, smooth_down,
+                                  smooth_up, smooth_bottom, int(zerophi), rarr), "batch_vcycle")
+        return [read_report(rarr[k], bufs[k]) for k in range(n)]
+
+
+class Server:
+    """A solve server (mgp_server_*): ``nworkers`` slots, admission by device
+    memory (``mem_budget`` bytes, 0 = 90 % of the free memory), resident
+    hierarchies reused per nonzero ``key``.  ``submit`` returns a ticket;
+    ``wait`` returns (Report, latency_s, queue_s)."""
+
+    def __init__(self, nworkers: int = 8, mem_budget: int = 0, flags: int = 0):
+        self._h = C.c_void_p()
+        _ck(_lib.mgp_server_create(nworkers, mem_budget, flags, _r(self._h)), "server_create")
+        self._live = {}
+
+    def submit(self, valid: Box, geo: GeoData, bc: BdryData, phi: BoxData, rhs: BoxData, homog, tol, maxiters,
+               key: int = 0, numcycles=1, smooth_down=8, smooth_up=8, smooth_bottom=8, zerophi=False) -> int:
+        t = C.c_longlong()
+        b, g, c, p, f = valid.c(), geo.c(), bc.c(), phi.c(), rhs.c()
+        _ck(_lib.mgp_server_submit(self._h, key, _r(b), _r(g), _r(c), _r(p), _r(f), int(homog), tol, maxiters,
+                                   numcycles, smooth_down, smooth_up, smooth_bottom, int(zerophi), _r(t)),
+            "server_submit")
+        # the arrays (and the structs describing them) must outlive the request
+        self._live[t.value] = (b, g, c, p, f, valid, geo, bc, phi, rhs, maxiters)
+        return t.value
+
+    def wait(self, ticket: int):
+        maxiters = self._live[ticket][-1]
+        rep, buf = make_report(maxiters)
+        lat, qt = C.c_double(), C.c_double()
+        rc = _lib.mgp_server_wait(self._h, ticket, _r(rep), _r(lat), _r(qt))
+        self._live.pop(ticket, None)
+        _ck(rc, "server_wait")
+        return read_report(rep, buf), lat.value, qt.value
+
+    def close(self):
+        if self._h:
+            _lib.mgp_server_destroy(self._h)
+            self._h = C.c_void_p()
+            self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
 __all__ = ["vcycle", "fmg", "dc_vcycle", "Solver", "fill_ghosts", "extrapolate_ghosts", "compute_invdiags",
            "compute_laplacian", "compute_residual", "relax_gs", "solve_bicgstab2", "solve_bicgstab2_noalloc", "NOALLOC_MAX_SIDE", "restrict", "prolong", "pnorm",
            "inner_prod", "estimate_maxdepth", "create_mgschedule", "MGPError", "library_path", "kernel_launch_count",
-           "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV", "FLAG_MIXED", "EXPORTS", "KIND_MG", "KIND_DD"]
+           "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV", "FLAG_MIXED", "Batch", "Server", "EXPORTS", "KIND_MG", "KIND_DD"]

@@ -1,0 +1,413 @@
+// mgp_batch.cu -- many independent solves at once: a batch of resident
+// hierarchies solved concurrently, and a request server that admits solves
+// as slots and device memory free up (continuous batching).
+//
+// Neither has a counterpart in the Fortran library, which solves one problem
+// per call.  Both run the single-problem solver unchanged: concurrency comes
+// from host workers that each own a CUDA stream, so the latency-bound kernels
+// of different problems (the small levels, the single-CTA coarse cycle)
+// overlap on the device.  A problem's kernels, their order and its
+// reductions do not depend on what else runs, so every result is identical
+// alone and in the mix.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <list>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/mgp2d.h"
+#include "mgp_kernels.cuh"
+
+namespace mgp {
+int record_error(int code, const char* msg);
+int solver_create_on(const mgp_box* valid, const mgp_geo* geo, const mgp_bdry* bc, int kind, int flags,
+                     int maxdepth_user, cudaStream_t st, mgp_solver** out);
+size_t solver_device_bytes(const mgp_solver* s);
+}  // namespace mgp
+
+using namespace mgp;
+
+namespace {
+
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Device bytes a hierarchy of nx x ny cells takes, before it exists: FP64
+// fields ~21 per cell over all levels (geometry, inverse diagonal,
+// corrections, residuals, the BiCGStab vectors), FP32 copies ~14, plus
+// padding and the small buffers.
+size_t estimate_bytes(const mgp_box* v, int flags) {
+    const double n = (double)v->nx * (double)v->ny;
+    const double per = 8.0 * 21.0 + ((flags & MGP_FLAG_MIXED) ? 4.0 * 14.0 : 0.0);
+    return (size_t)(n * per) + ((size_t)8 << 20);
+}
+
+}  // namespace
+
+// ===========================================================================
+// Batch
+// ===========================================================================
+struct mgp_batch {
+    int dev = 0;
+    int nstreams = 1;
+    std::vector<mgp_solver*> solvers;
+    std::vector<cudaStream_t> streams;
+};
+
+extern "C" {
+
+int mgp_batch_create(int nprob, const mgp_box* valid, const mgp_geo* geo, const mgp_bdry* bc, int kind, int flags,
+                     int maxdepth_user, int nstreams, mgp_batch** out) {
+    if (!out || nprob <= 0 || !valid || !geo || !bc) return record_error(MGP_EINVAL, "batch_create: bad argument");
+    *out = nullptr;
+    mgp_batch* b = new mgp_batch();
+    if (cudaGetDevice(&b->dev) != cudaSuccess) {
+        cudaGetLastError();
+        delete b;
+        return record_error(MGP_ECUDA, "batch_create: no CUDA device");
+    }
+    b->nstreams = std::max(1, std::min(nstreams, nprob));
+    for (int k = 0; k < b->nstreams; ++k) {
+        cudaStream_t st;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            mgp_batch_destroy(b);
+            return record_error(MGP_ECUDA, "batch_create: stream creation failed");
+        }
+        b->streams.push_back(st);
+    }
+    for (int i = 0; i < nprob; ++i) {
+        mgp_solver* s = nullptr;
+        const int rc = mgp_solver_create(&valid[i], &geo[i], &bc[i], kind, flags, maxdepth_user, &s);
+        if (rc) {
+            mgp_batch_destroy(b);
+            return rc;
+        }
+        b->solvers.push_back(s);
+    }
+    *out = b;
+    return MGP_OK;
+}
+
+int mgp_batch_destroy(mgp_batch* b) {
+    if (!b) return MGP_OK;
+    for (mgp_solver* s : b->solvers) mgp_solver_destroy(s);
+    for (cudaStream_t st : b->streams) cudaStreamDestroy(st);
+    delete b;
+    return MGP_OK;
+}
+
+int mgp_batch_size(const mgp_batch* b, int* nprob) {
+    if (!b || !nprob) return record_error(MGP_EINVAL, "batch_size: null argument");
+    *nprob = (int)b->solvers.size();
+    return MGP_OK;
+}
+
+int mgp_batch_vcycle(mgp_batch* b, mgp_array* phi, mgp_array* rhs, const mgp_bdry* bc, int homog, double tol,
+                     int maxiters, int numcycles, int smooth_down, int smooth_up, int smooth_bottom, int zerophi,
+                     mgp_report* reports) {
+    if (!b || !phi || !rhs || !bc) return record_error(MGP_EINVAL, "batch_vcycle: null argument");
+    const int n = (int)b->solvers.size();
+    std::atomic<int> next{0};
+    std::vector<int> status(n, MGP_OK);
+    std::vector<std::string> msg(n);
+    auto work = [&](int w) {
+        cudaSetDevice(b->dev);
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= n) break;
+            mgp_solver_set_stream(b->solvers[i], b->streams[w]);
+            status[i] = mgp_solver_vcycle(b->solvers[i], &phi[i], &rhs[i], &bc[i], homog, tol, maxiters, numcycles,
+                                          smooth_down, smooth_up, smooth_bottom, zerophi, 0,
+                                          reports ? &reports[i] : nullptr);
+            if (status[i]) msg[i] = mgp_last_error();
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < b->nstreams; ++w) pool.emplace_back(work, w);
+    work(0);
+    for (auto& t : pool) t.join();
+    for (int i = 0; i < n; ++i)
+        if (status[i]) {
+            record_error(status[i], msg[i].c_str());
+            return status[i];
+        }
+    return MGP_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Server
+// ===========================================================================
+namespace {
+
+struct Request {
+    long long ticket = 0;
+    unsigned long long key = 0;
+    mgp_box valid{};
+    mgp_geo geo{};
+    mgp_bdry bc{};
+    mgp_array phi{}, rhs{};
+    int homog = 0, maxiters = 0, numcycles = 1, nd = 8, nu = 8, nb = 8, zerophi = 0;
+    double tol = 0.0;
+    std::vector<double> relres;
+    mgp_report rep{};
+    int status = MGP_OK;
+    std::string err;
+    bool done = false;
+    double t_submit = 0.0, t_start = 0.0, t_end = 0.0;
+};
+
+struct Entry {   // a resident hierarchy kept for its key
+    unsigned long long key;
+    mgp_box valid;
+    mgp_solver* s;
+    size_t bytes;
+    bool busy;
+    double last_use;
+};
+
+}  // namespace
+
+struct mgp_server {
+    int dev = 0;
+    int flags = 0;
+    size_t budget = 0;
+    size_t used = 0;   // bytes of hierarchies alive (running or cached)
+    int running = 0;
+    bool stop = false;
+    long long next_ticket = 1;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done, cv_mem;
+    std::deque<Request*> queue;
+    std::map<long long, Request*> reqs;
+    std::list<Entry> cache;
+    std::vector<std::thread> workers;
+};
+
+namespace {
+
+bool same_box(const mgp_box& a, const mgp_box& b) {
+    return a.ilo == b.ilo && a.ihi == b.ihi && a.jlo == b.jlo && a.jhi == b.jhi && a.dx == b.dx && a.dy == b.dy;
+}
+
+// Frees the least recently used idle cached hierarchy; false if there is none.
+// Called with the lock held.
+bool evict_one(mgp_server* S, std::vector<mgp_solver*>& doomed) {
+    auto victim = S->cache.end();
+    for (auto it = S->cache.begin(); it != S->cache.end(); ++it)
+        if (!it->busy && (victim == S->cache.end() || it->last_use < victim->last_use)) victim = it;
+    if (victim == S->cache.end()) return false;
+    S->used -= victim->bytes;
+    doomed.push_back(victim->s);
+    S->cache.erase(victim);
+    return true;
+}
+
+void serve(mgp_server* S) {
+    cudaSetDevice(S->dev);
+    cudaStream_t st = nullptr;
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    for (;;) {
+        Request* r = nullptr;
+        {
+            std::unique_lock<std::mutex> lock(S->mu);
+            S->cv_work.wait(lock, [&] { return S->stop || !S->queue.empty(); });
+            if (S->queue.empty()) break;   // stopping
+            r = S->queue.front();
+            S->queue.pop_front();
+            ++S->running;
+        }
+        r->t_start = now_s();
+        mgp_solver* sv = nullptr;
+        size_t bytes = 0;
+        bool cached = false;
+        int rc = MGP_OK;
+        std::vector<mgp_solver*> doomed;
+        {
+            std::unique_lock<std::mutex> lock(S->mu);
+            if (r->key) {
+                for (auto& e : S->cache)
+                    if (e.key == r->key && !e.busy && same_box(e.valid, r->valid)) {
+                        e.busy = true;
+                        sv = e.s;
+                        bytes = e.bytes;
+                        cached = true;
+                        break;
+                    }
+            }
+            if (!sv) {   // admission by device memory
+                bytes = estimate_bytes(&r->valid, S->flags);
+                while (S->used + bytes > S->budget) {
+                    if (evict_one(S, doomed)) continue;
+                    if (S->running <= 1) break;   // nothing else will free memory: try anyway
+                    S->cv_mem.wait(lock);
+                }
+                S->used += bytes;
+            }
+        }
+        for (mgp_solver* d : doomed) mgp_solver_destroy(d);
+        if (!sv) {
+            rc = solver_create_on(&r->valid, &r->geo, &r->bc, MGP_KIND_MG, S->flags, -1, st, &sv);
+            const size_t actual = rc ? 0 : solver_device_bytes(sv);
+            std::lock_guard<std::mutex> lock(S->mu);
+            S->used = S->used - bytes + actual;
+            bytes = actual;
+        }
+        if (!rc) {
+            mgp_solver_set_stream(sv, st);
+            rc = mgp_solver_vcycle(sv, &r->phi, &r->rhs, &r->bc, r->homog, r->tol, r->maxiters, r->numcycles, r->nd,
+                                   r->nu, r->nb, r->zerophi, 0, &r->rep);
+        }
+        if (rc) r->err = mgp_last_error();
+        r->t_end = now_s();
+        mgp_solver* drop = nullptr;
+        {
+            std::lock_guard<std::mutex> lock(S->mu);
+            if (sv && r->key && !rc) {
+                if (cached) {
+                    for (auto& e : S->cache)
+                        if (e.s == sv) {
+                            e.busy = false;
+                            e.last_use = r->t_end;
+                        }
+                } else {
+                    S->cache.push_back(Entry{r->key, r->valid, sv, bytes, false, r->t_end});
+                }
+            } else if (sv) {
+                if (cached) S->cache.remove_if([&](const Entry& e) { return e.s == sv; });
+                S->used -= bytes;
+                drop = sv;
+            }
+            r->status = rc;
+            r->done = true;
+            --S->running;
+        }
+        if (drop) mgp_solver_destroy(drop);
+        S->cv_done.notify_all();
+        S->cv_mem.notify_all();
+    }
+    if (st) cudaStreamDestroy(st);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mgp_server_create(int nworkers, size_t mem_budget, int flags, mgp_server** out) {
+    if (!out || nworkers <= 0) return record_error(MGP_EINVAL, "server_create: bad argument");
+    *out = nullptr;
+    mgp_server* S = new mgp_server();
+    if (cudaGetDevice(&S->dev) != cudaSuccess) {
+        cudaGetLastError();
+        delete S;
+        return record_error(MGP_ECUDA, "server_create: no CUDA device");
+    }
+    S->flags = flags;
+    if (mem_budget == 0) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+            cudaGetLastError();
+            delete S;
+            return record_error(MGP_ECUDA, "server_create: cudaMemGetInfo failed");
+        }
+        mem_budget = fr / 10 * 9;
+    }
+    S->budget = mem_budget;
+    for (int w = 0; w < nworkers; ++w) S->workers.emplace_back(serve, S);
+    *out = S;
+    return MGP_OK;
+}
+
+int mgp_server_submit(mgp_server* S, unsigned long long key, const mgp_box* valid, const mgp_geo* geo,
+                      const mgp_bdry* bc, mgp_array* phi, mgp_array* rhs, int homog, double tol, int maxiters,
+                      int numcycles, int smooth_down, int smooth_up, int smooth_bottom, int zerophi,
+                      long long* ticket) {
+    if (!S || !valid || !geo || !bc || !phi || !rhs || !ticket || maxiters < 0)
+        return record_error(MGP_EINVAL, "server_submit: bad argument");
+    Request* r = new Request();
+    r->key = key;
+    r->valid = *valid;
+    r->geo = *geo;
+    r->bc = *bc;
+    r->phi = *phi;
+    r->rhs = *rhs;
+    r->homog = homog;
+    r->tol = tol;
+    r->maxiters = maxiters;
+    r->numcycles = numcycles;
+    r->nd = smooth_down;
+    r->nu = smooth_up;
+    r->nb = smooth_bottom;
+    r->zerophi = zerophi;
+    r->relres.assign((size_t)maxiters + 1, 0.0);
+    r->rep.relres = r->relres.data();
+    r->t_submit = now_s();
+    {
+        std::lock_guard<std::mutex> lock(S->mu);
+        if (S->stop) {
+            delete r;
+            return record_error(MGP_EINVAL, "server_submit: server is stopping");
+        }
+        r->ticket = S->next_ticket++;
+        S->reqs[r->ticket] = r;
+        S->queue.push_back(r);
+    }
+    *ticket = r->ticket;
+    S->cv_work.notify_one();
+    return MGP_OK;
+}
+
+int mgp_server_wait(mgp_server* S, long long ticket, mgp_report* report, double* latency_s, double* queue_s) {
+    if (!S) return record_error(MGP_EINVAL, "server_wait: null server");
+    Request* r = nullptr;
+    {
+        std::unique_lock<std::mutex> lock(S->mu);
+        auto it = S->reqs.find(ticket);
+        if (it == S->reqs.end()) return record_error(MGP_EINVAL, "server_wait: unknown ticket");
+        r = it->second;
+        S->cv_done.wait(lock, [&] { return r->done; });
+        S->reqs.erase(it);
+    }
+    if (report) {
+        double* dst = report->relres;
+        *report = r->rep;
+        report->relres = dst;
+        if (dst)
+            for (int k = 0; k <= r->rep.iterations && k <= r->maxiters; ++k) dst[k] = r->relres[k];
+    }
+    if (latency_s) *latency_s = r->t_end - r->t_submit;
+    if (queue_s) *queue_s = r->t_start - r->t_submit;
+    const int rc = r->status;
+    if (rc) record_error(rc, r->err.c_str());
+    delete r;
+    return rc;
+}
+
+int mgp_server_destroy(mgp_server* S) {
+    if (!S) return MGP_OK;
+    {
+        std::lock_guard<std::mutex> lock(S->mu);
+        S->stop = true;
+    }
+    S->cv_work.notify_all();
+    S->cv_mem.notify_all();
+    for (auto& t : S->workers) t.join();
+    for (auto& e : S->cache) mgp_solver_destroy(e.s);
+    for (auto& kv : S->reqs) delete kv.second;
+    delete S;
+    return MGP_OK;
+}
+
+}  // extern "C"

@@ -1154,6 +1154,18 @@ int ghost_cap(const mgp_array* a) {
 // mgp_last_error() returns.
 namespace mgp {
 int record_error(int code, const char* msg) { return set_err(code, "%s", msg); }
+
+// For the batch and server front ends (mgp_batch.cu): a solver whose set-up
+// runs on the given stream, and the device bytes it holds.
+int solver_create_on(const mgp_box* valid, const mgp_geo* geo, const mgp_bdry* bc, int kind, int flags,
+                     int maxdepth_user, cudaStream_t st, mgp_solver** out) {
+    return solver_new(valid, geo, bc, kind, flags, maxdepth_user, st, out);
+}
+size_t solver_device_bytes(const mgp_solver* s) {
+    if (!s) return 0;
+    return (s->fixed.elems + s->state.elems) * sizeof(double) +
+           (s->fixed32.elems + s->state32.elems) * sizeof(float) + (size_t)s->shadow_bytes;
+}
 }  // namespace mgp
 
 // ===========================================================================

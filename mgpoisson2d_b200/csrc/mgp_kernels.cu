@@ -761,8 +761,12 @@ __device__ void b_mul(const DF& out, const DF& a, const DF& c, int nx, int ny) {
 // ranges, the edge cells colour by colour along each non-periodic side, then
 // the corners -- at once when the grid is at least 4 x 4 (their stencils,
 // two cells deep, then neither read nor write each other), else in turn.
-__device__ void b_sweep9(const DF& phi, const DF& rhs, const DF& invd, const Geo& g, const BCd& b, int homog, int nx,
-                         int ny, double omega) {
+__device__ void b_sweep9(const DF& phi_, const DF& rhs_, const DF& invd_, const Geo& g_, const BCd& b, int homog,
+                         int nx, int ny, double omega) {
+    // field descriptors in registers: the level structs live in shared memory,
+    // and every barrier would otherwise make the compiler reload them
+    const DF phi = phi_, rhs = rhs_, invd = invd_;
+    const Geo g = g_;
     const Per pr = periodic_of(b);
     const int mi0 = pr.xl ? 0 : 1, mi1 = pr.xh ? nx : nx - 1;
     const int mj0 = pr.yl ? 0 : 1, mj1 = pr.yh ? ny : ny - 1;

@@ -106,3 +106,29 @@ def terrain_neumann(n: int, boundary_fluxes, compute_laplacian):
     rhs = BoxData(v)
     compute_laplacian(rhs, soln.copy(), geo, bc, False)
     return v, geo, rhs, bc, soln
+
+
+def batch_problem(i: int, seed: int = 4, nmin: int = 64, nmax: int = 1024):
+    """Problem i of the batched workload (seed*10^6 + i): each side
+    log-uniform in [nmin, nmax], rounded to a multiple of 16 (the reference
+    schedule stops at depth 0 on odd sizes); y stretched by a ratio U[1, 1.08]
+    per cell in a wall layer of min(64, ny/4) cells, then sheared by U[0, 25]
+    degrees; the 16-mode Fourier rhs of wavy_stretched; homogeneous Dirichlet
+    on all sides."""
+    pseed = seed * 1_000_000 + i
+    rng = np.random.default_rng(pseed)
+
+    def side():
+        n = math.exp(rng.uniform(math.log(nmin), math.log(nmax)))
+        return int(max(nmin, min(nmax, 16 * round(n / 16))))
+
+    nx, ny = side(), side()
+    ratio = float(rng.uniform(1.0, 1.08))
+    angle = float(rng.uniform(0.0, 25.0))
+    layer_cells = min(64, ny // 4)
+    v = Box.of_size(nx, ny)
+    fmap = G.map_skew_stretch(angle, ratio, layer_cells / ny, ny)
+    geo = G.mapped_geometry(v, fmap)
+    rhs = fourier_rhs(v, geo, fmap, pseed)
+    bc = BdryData.uniform(v, [BCTYPE_DIRI] * 4)
+    return v, geo, rhs, bc

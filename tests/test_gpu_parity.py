@@ -431,3 +431,49 @@ def test_mixed_all_neumann_and_identity(M):
         s.vcycle(pd, rhs, bc, True, 1e-11, 100)
     assert rc.final_relres <= 1e-11
     assert np.abs(pc.interior() - pd.interior()).max() < 1e-8 * np.abs(pd.interior()).max()
+
+
+# ---------------------------------------------------------------------------
+# Batches and the solve server: every result identical to solving alone
+# ---------------------------------------------------------------------------
+def _alone(M, prob, flags, tol=1e-10, maxiters=400):
+    v, geo, rhs, bc = prob
+    with M.Solver(v, geo, bc, KIND_MG, flags) as s:
+        p = BoxData(v, 1, 1)
+        r = s.vcycle(p, rhs, bc, True, tol, maxiters)
+    return p, r
+
+
+def test_batch_matches_individual_solves(M):
+    from mgpoisson2d_b200 import workloads as W
+    probs = [W.batch_problem(i, nmax=192) for i in range(5)]
+    flags = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV | M.FLAG_MIXED
+    with M.Batch([(v, g, bc) for v, g, _, bc in probs], KIND_MG, flags, nstreams=3) as b:
+        phis = [BoxData(p[0], 1, 1) for p in probs]
+        reps = b.vcycle(phis, [p[2] for p in probs], [p[3] for p in probs], True, 1e-10, 400)
+    for k, prob in enumerate(probs):
+        pa, ra = _alone(M, prob, flags)
+        assert reps[k].status == 0 and reps[k].final_relres <= 1e-10
+        assert same(phis[k].data, pa.data) and np.array_equal(reps[k].relres, ra.relres)
+
+
+def test_server_results_same_alone_and_in_the_mix(M):
+    """Requests overlap on the device (3 slots, 7 requests, two keys reused);
+    each result must equal the same solve run alone."""
+    from mgpoisson2d_b200 import workloads as W
+    probs = [W.batch_problem(i, nmax=160) for i in range(4)]
+    flags = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV
+    order = [0, 1, 2, 3, 0, 1, 0]
+    with M.Server(nworkers=3, flags=flags) as srv:
+        outs, tickets = [], []
+        for n, k in enumerate(order):
+            v, geo, rhs, bc = probs[k]
+            p = BoxData(v, 1, 1)
+            outs.append(p)
+            tickets.append(srv.submit(v, geo, bc, p, rhs, True, 1e-10, 400, key=(k + 1 if k < 2 else 0)))
+        results = [srv.wait(t) for t in tickets]
+    for n, k in enumerate(order):
+        pa, ra = _alone(M, probs[k], flags)
+        rep, lat, qt = results[n]
+        assert rep.status == 0 and lat >= qt >= 0.0
+        assert same(outs[n].data, pa.data) and np.array_equal(rep.relres, ra.relres)

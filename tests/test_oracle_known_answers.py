@@ -313,3 +313,17 @@ def test_krylov_oracle_same_solution_fewer_vcycles():
     assert 3 * (len(rk) - 1) < ra.iterations
     err = pb.interior() - pa.interior()
     assert np.linalg.norm(err) / np.linalg.norm(pa.interior()) < 1e-8
+
+
+def test_batch_problem_generator():
+    """The batched workload: seeded, sides multiples of 16 within [64, 1024],
+    Dirichlet all round, the rhs with zero J-weighted mean."""
+    a, b = W.batch_problem(7), W.batch_problem(7)
+    assert a[0].nx == b[0].nx and a[0].ny == b[0].ny
+    assert np.array_equal(a[2].interior(), b[2].interior())
+    for i in range(12):
+        v, geo, rhs, bc = W.batch_problem(i, nmax=256)
+        assert v.nx % 16 == 0 and v.ny % 16 == 0 and 64 <= v.nx <= 256 and 64 <= v.ny <= 256
+        assert bc.types == [BCTYPE_DIRI] * 4
+        assert np.all(geo.J.interior() > 0)
+        assert abs(rhs.interior().sum()) < 1e-9 * np.abs(rhs.interior()).sum()
