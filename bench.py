@@ -16,6 +16,11 @@ solver in FP64 ("fp64_same_solver") and of the plain FP64 V-cycle iteration
 torchrun every rank solves its own copy (replicas; the solve does not shard)
 and rank 0 prints one JSON line.
 
+At N=1 the line also carries two legs on many independent problems (the
+batched workload: sides log-uniform in [64,1024]): "batched" (all problems as
+one mgp_batch on 16 streams vs one after another) and "served" (Poisson
+arrivals into an mgp_server with resident hierarchies; p50/p99 latency).
+
 --impl reference times the CPU restatement of the reference algorithm (the
 reference is Fortran and no Fortran compiler exists on these hosts) on all
 host cores, on a bounded sample of V-cycles of the same solve.
@@ -60,6 +65,9 @@ def parse():
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                    help="mixed: FP32 grid levels inside the FP64 outer iteration (MGP_FLAG_MIXED)")
     p.add_argument("--no-plain", action="store_true", help="skip the extra plain V-cycle solve")
+    p.add_argument("--no-batch", action="store_true", help="skip the batched and served legs")
+    p.add_argument("--batch", type=int, default=48, help="problems in the batched leg")
+    p.add_argument("--streams", type=int, default=16, help="concurrent solves in the batched and served legs")
     return p.parse_args()
 
 
@@ -206,6 +214,103 @@ def solve_vcycles_estimate(n):
         return int(json.load(open(path))[str(n)])
     except Exception:
         return _VCYCLES.get(n, 1000)
+
+
+# --------------------------------------------------------------------------- #
+# Batched and served legs (many independent problems)
+# --------------------------------------------------------------------------- #
+def batched_leg(M, args, flags_list):
+    """`args.batch` problems of the batched workload (sides log-uniform in
+    [64, 1024], rounded to 16; random stretch and skew; Dirichlet), solved to
+    1e-10 one after another on one stream and as one batch on `args.streams`
+    streams, for each flag set.  Inputs and hierarchies resident."""
+    import numpy as np
+    import torch
+    from mgpoisson2d_b200 import workloads as W
+    from mgpoisson2d_b200.types import BoxData
+    probs = [W.batch_problem(i) for i in range(args.batch)]
+    rhs_d = [p[2].to_device() for p in probs]
+    cells = sum(p[0].nx * p[0].ny for p in probs)
+    out = {"problems": args.batch, "cells": cells, "streams": args.streams,
+           "workload": "sides log-uniform [64,1024] rounded to 16, stretch U[1,1.08] in a min(64,ny/4)-cell layer, "
+                       "skew U[0,25] deg, 16-mode rhs, Dirichlet; seeds 4e6+i"}
+    for name, fl in flags_list:
+        with M.Batch([(v, g, bc) for v, g, _, bc in probs], M.KIND_MG, fl, nstreams=args.streams) as b:
+            phis = [BoxData(p[0], 1, 1).to_device() for p in probs]
+            bcs = [p[3] for p in probs]
+            b.vcycle(phis, rhs_d, bcs, True, TOL, MAXITERS)   # warm-up (graph capture)
+            for p in phis:
+                p.data.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            reps = b.vcycle(phis, rhs_d, bcs, True, TOL, MAXITERS)
+            torch.cuda.synchronize()
+            tb = time.perf_counter() - t0
+        assert all(r.final_relres <= TOL for r in reps), "batched solve did not converge"
+        # the same problems one at a time on one stream
+        solvers = [M.Solver(v, g, bc, M.KIND_MG, fl) for v, g, _, bc in probs]
+        for s, p, f, (v, g, _, bc) in zip(solvers, phis, rhs_d, probs):
+            p.data.zero_()
+            s.vcycle(p, f, bc, True, TOL, MAXITERS)   # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for s, p, f, (v, g, _, bc) in zip(solvers, phis, rhs_d, probs):
+            p.data.zero_()
+            s.vcycle(p, f, bc, True, TOL, MAXITERS)
+        torch.cuda.synchronize()
+        ts = time.perf_counter() - t0
+        for s in solvers:
+            s.close()
+        out[name] = {"batched_solves_per_s": args.batch / tb, "sequential_solves_per_s": args.batch / ts,
+                     "speedup": ts / tb, "vcycles_mean": float(np.mean([r.iterations for r in reps]))}
+    return out, probs, rhs_d
+
+
+def served_leg(M, args, probs, rhs_d, flags_list, nreq=240, seed=5):
+    """Poisson arrivals of solves drawn from the batched workload's problems
+    (hierarchies resident per problem), tolerance 1e-8 or 1e-10 with
+    probability 1/2 each; `args.streams` slots.  Offered load: 0.5x and 2x the
+    batched throughput.  Reports p50/p99 latency (submit to done) and the
+    achieved solves/s."""
+    import numpy as np
+    from mgpoisson2d_b200.types import BoxData
+    out = {"requests": nreq, "slots": args.streams, "tolerances": [1e-8, 1e-10]}
+    for name, fl, cap in flags_list:
+        res = {}
+        for load in (0.5, 2.0):
+            rng = np.random.default_rng(seed)
+            rate = load * cap
+            gaps = rng.exponential(1.0 / rate, nreq)
+            which = rng.integers(0, len(probs), nreq)
+            tols = np.where(rng.random(nreq) < 0.5, 1e-8, 1e-10)
+            with M.Server(nworkers=args.streams, flags=fl) as srv:
+                # warm the resident hierarchies (one request per problem)
+                warm = [srv.submit(v, g, bc, BoxData(v, 1, 1).to_device(), rhs_d[k], True, 1e-10, MAXITERS,
+                                   key=k + 1) for k, (v, g, _, bc) in enumerate(probs)]
+                for t in warm:
+                    srv.wait(t)
+                outs = [BoxData(probs[k][0], 1, 1).to_device() for k in which]
+                tickets = []
+                t0 = time.perf_counter()
+                t_next = t0
+                for n in range(nreq):
+                    t_next += gaps[n]
+                    while time.perf_counter() < t_next:
+                        time.sleep(max(0.0, min(0.001, t_next - time.perf_counter())))
+                    v, g, _, bc = probs[which[n]]
+                    tickets.append(srv.submit(v, g, bc, outs[n], rhs_d[which[n]], True, float(tols[n]), MAXITERS,
+                                              key=int(which[n]) + 1))
+                lats = []
+                for t in tickets:
+                    rep, lat, qt = srv.wait(t)
+                    lats.append(lat)
+                span = time.perf_counter() - t0
+            lats = np.sort(np.array(lats)) * 1e3
+            res[f"offered_{load}x"] = {"offered_per_s": rate, "solves_per_s": nreq / span,
+                                       "p50_ms": float(lats[len(lats) // 2]),
+                                       "p99_ms": float(lats[min(len(lats) - 1, int(math.ceil(0.99 * len(lats))) - 1)])}
+        out[name] = res
+    return out
 
 
 # --------------------------------------------------------------------------- #
@@ -376,6 +481,13 @@ def main():
                        "d2h_bytes_per_step": 8 * phi_h.data.size,
                        "api": "mgp_vcycle (host arrays; hierarchy built inside the call)",
                        "vcycles": erep.iterations, "timed_calls": len(times), "stat": "median"}
+    if rank == 0 and world == 1 and not args.no_batch:
+        kry = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV
+        fls = [("mixed", kry | M.FLAG_MIXED), ("fp64", kry)]
+        batched, probs, rhs_b = batched_leg(M, args, fls)
+        line["batched"] = batched
+        line["served"] = served_leg(M, args, probs, rhs_b,
+                                    [(n, f, batched[n]["batched_solves_per_s"]) for n, f in fls])
     if rank == 0 and world == 1 and not args.no_cpu:
         tvc, nvc = cpu_sample(args.n, args.cpu_vcycles)
         iters = solve_vcycles_estimate(args.n)
