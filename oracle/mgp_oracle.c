@@ -628,6 +628,141 @@ int or_boundary_fluxes(const mgp_box *valid, const mgp_array *phi, const mgp_geo
     return MGP_OK;
 }
 
+static mgp_array alloc_like(int nx, int ny, int ngx, int ngy);
+
+/* ---- gradient and divergence: P2:404-879, AU:1571-1622 ------------------ */
+/* compute_pd (P2:404-795): d(phi)/d(dir) onto the faces nodal in `nodedir`
+ * (1: x-faces, (nx+1) x ny; 2: y-faces, nx x (ny+1)).  The nodal derivative
+ * reads the ghosts; the transverse one uses interior differences, one-sided
+ * ones at the sides across it (P2:455-478, P2:618-641) and the
+ * compute_laplacian region values on the faces along the sides
+ * (simple_bdry_stencil = .false., P2:488-611, P2:651-793). */
+int or_compute_pd(const mgp_box *valid, mgp_array *pd, const mgp_array *phi, int dir, int nodedir)
+{
+    const int nx = valid->nx, ny = valid->ny;
+    V D = view(pd), P = view(phi);
+    st9 s;
+    int i, j;
+    if ((dir != 1 && dir != 2) || (nodedir != 1 && nodedir != 2)) return fail(MGP_EINVAL, "compute_pd: bad direction");
+    if (nx < 3 || ny < 3) return fail(MGP_EINVAL, "compute_pd needs at least 3 cells per direction");
+    if (dir == 1 && nodedir == 1) {   /* P2:446-449 */
+        const double scale = one / valid->dx;
+        for (j = 0; j < ny; ++j)
+            for (i = 0; i <= nx; ++i) AT(D, i, j) = scale * (AT(P, i, j) - AT(P, i - 1, j));
+    } else if (dir == 2 && nodedir == 2) {   /* P2:614-617 */
+        const double scale = one / valid->dy;
+        for (j = 0; j <= ny; ++j)
+            for (i = 0; i < nx; ++i) AT(D, i, j) = scale * (AT(P, i, j) - AT(P, i, j - 1));
+    } else if (dir == 1) {   /* d/dx onto y-faces, P2:450-612 */
+        const double scale = fourth / valid->dx;
+        for (j = 1; j < ny; ++j)
+            for (i = 1; i < nx - 1; ++i)
+                AT(D, i, j) = scale * (AT(P, i + 1, j) - AT(P, i - 1, j) + AT(P, i + 1, j - 1) - AT(P, i - 1, j - 1));
+        for (j = 1; j < ny; ++j) {
+            AT(D, 0, j) = -scale * (three * AT(P, 0, j) - four * AT(P, 1, j) + AT(P, 2, j) + three * AT(P, 0, j - 1) -
+                                    four * AT(P, 1, j - 1) + AT(P, 2, j - 1));
+            AT(D, nx - 1, j) = scale * (three * AT(P, nx - 1, j) - four * AT(P, nx - 2, j) + AT(P, nx - 3, j) +
+                                        three * AT(P, nx - 1, j - 1) - four * AT(P, nx - 2, j - 1) +
+                                        AT(P, nx - 3, j - 1));
+        }
+        for (i = 0; i < nx; ++i) {
+            const int xr = xregion(i, nx, 0, 0);
+            gather(&AT(P, i, 0), P.ld, xr, RLO, &s);
+            AT(D, i, 0) = scale * (s.ee - s.ew + s.ese - s.esw);
+            gather(&AT(P, i, ny - 1), P.ld, xr, RHI, &s);
+            AT(D, i, ny) = scale * (s.ene - s.enw + s.ee - s.ew);
+        }
+    } else {   /* d/dy onto x-faces, P2:613-794 */
+        const double scale = fourth / valid->dy;
+        for (j = 1; j < ny - 1; ++j)
+            for (i = 1; i < nx; ++i)
+                AT(D, i, j) = scale * (AT(P, i, j + 1) - AT(P, i, j - 1) + AT(P, i - 1, j + 1) - AT(P, i - 1, j - 1));
+        for (i = 1; i < nx; ++i) {
+            AT(D, i, 0) = -scale * (three * AT(P, i, 0) - four * AT(P, i, 1) + AT(P, i, 2) + three * AT(P, i - 1, 0) -
+                                    four * AT(P, i - 1, 1) + AT(P, i - 1, 2));
+            AT(D, i, ny - 1) = scale * (three * AT(P, i, ny - 1) - four * AT(P, i, ny - 2) + AT(P, i, ny - 3) +
+                                        three * AT(P, i - 1, ny - 1) - four * AT(P, i - 1, ny - 2) +
+                                        AT(P, i - 1, ny - 3));
+        }
+        for (j = 0; j < ny; ++j) {
+            const int yr = xregion(j, ny, 0, 0);
+            gather(&AT(P, 0, j), P.ld, RLO, yr, &s);
+            AT(D, 0, j) = scale * (s.en - s.es + s.enw - s.esw);
+            gather(&AT(P, nx - 1, j), P.ld, RHI, yr, &s);
+            AT(D, nx, j) = scale * (s.ene - s.ese + s.en - s.es);
+        }
+    }
+    return MGP_OK;
+}
+
+/* fill_boundary_fluxes (AU:1574-1622): the faces on Neumann sides take the
+ * BC flux (0 when homogeneous).  UNIFORM values (and zeros) go to the whole
+ * face column or row, ghost rows included (the `(ilo,:)` sections);
+ * NONUNIFORM values to the valid faces. */
+int or_fill_boundary_fluxes(const mgp_box *valid, mgp_array *xflux, mgp_array *yflux, const mgp_bdry *bc, int homog)
+{
+    const int nx = valid->nx, ny = valid->ny;
+    V X = view(xflux), Y = view(yflux);
+    int s, k;
+    for (s = 0; s < 4; ++s) {
+        const int isx = s < 2, n = isx ? ny : nx;
+        const int ng = isx ? xflux->ngy : yflux->ngx;
+        const int edge = (s == MGP_XLO || s == MGP_YLO) ? 0 : (isx ? nx : ny);
+        if (bc->type[s] != MGP_BCTYPE_NEUM) continue;
+        for (k = -ng; k < n + ng; ++k) {
+            double v;
+            if (homog || bc->mode[s] == MGP_BCMODE_LAH) v = zero;
+            else if (bc->mode[s] == MGP_BCMODE_UNIFORM) v = bc->data[s][0];
+            else if (k >= 0 && k < n) v = bc->data[s][k];
+            else continue;
+            if (isx) AT(X, edge, k) = v;
+            else AT(Y, k, edge) = v;
+        }
+    }
+    return MGP_OK;
+}
+
+/* compute_grad (P2:809-850): J Grad[phi] on the faces; phi's ghosts are
+ * filled first (do_neum = .false.). */
+int or_compute_grad(const mgp_box *valid, mgp_array *xflux, mgp_array *yflux, mgp_array *phi, const mgp_geo *geo,
+                    const mgp_bdry *bc, int homog)
+{
+    const int nx = valid->nx, ny = valid->ny;
+    mgp_array xwk = alloc_like(nx + 1, ny, 0, 0), ywk = alloc_like(nx, ny + 1, 0, 0);
+    V X = view(xflux), Y = view(yflux), XW, YW;
+    G g = gview(geo);
+    int rc = MGP_OK, i, j;
+    if (!xwk.data || !ywk.data) { rc = fail(MGP_ENOMEM, "compute_grad: out of memory"); goto done; }
+    XW = view(&xwk);
+    YW = view(&ywk);
+    if ((rc = or_fill_ghosts(valid, phi, bc, geo, homog, 0))) goto done;
+    if ((rc = or_compute_pd(valid, xflux, phi, 1, 1))) goto done;
+    if ((rc = or_compute_pd(valid, &xwk, phi, 2, 1))) goto done;
+    for (j = 0; j < ny; ++j)
+        for (i = 0; i <= nx; ++i) AT(X, i, j) = AT(g.xx, i, j) * AT(X, i, j) + AT(g.xy, i, j) * AT(XW, i, j);
+    if ((rc = or_compute_pd(valid, &ywk, phi, 1, 2))) goto done;
+    if ((rc = or_compute_pd(valid, yflux, phi, 2, 2))) goto done;
+    for (j = 0; j <= ny; ++j)
+        for (i = 0; i < nx; ++i) AT(Y, i, j) = AT(g.yx, i, j) * AT(YW, i, j) + AT(g.yy, i, j) * AT(Y, i, j);
+    rc = or_fill_boundary_fluxes(valid, xflux, yflux, bc, homog);
+done:
+    free(xwk.data);
+    free(ywk.data);
+    return rc;
+}
+
+/* compute_div (P2:860-879): J Div[flux] = (xflux(i+1)-xflux(i))/dx + (yflux(j+1)-yflux(j))/dy. */
+int or_compute_div(const mgp_box *valid, mgp_array *div, const mgp_array *xflux, const mgp_array *yflux)
+{
+    const double invdx = one / valid->dx, invdy = one / valid->dy;
+    V D = view(div), X = view(xflux), Y = view(yflux);
+    int i, j;
+    for (j = 0; j < valid->ny; ++j)
+        for (i = 0; i < valid->nx; ++i)
+            AT(D, i, j) = invdx * (AT(X, i + 1, j) - AT(X, i, j)) + invdy * (AT(Y, i, j + 1) - AT(Y, i, j));
+    return MGP_OK;
+}
+
 /* ---- reductions: AU:637-661, AU:670-710, AU:753-796 --------------------- */
 double or_pnorm(const mgp_box *valid, const mgp_array *bd, int p)
 {

@@ -66,6 +66,13 @@ int or_prolong(const mgp_box *fine_valid, mgp_array *fine, const mgp_box *crse_v
                mgp_array *crse, const mgp_geo *fine_geo, const mgp_geo *crse_geo,
                const mgp_bdry *crse_bc, int order);
 
+/* compute_pd P2:404-795, fill_boundary_fluxes AU:1574-1622, compute_grad
+ * P2:809-850, compute_div P2:860-879. */
+int or_compute_pd(const mgp_box *valid, mgp_array *pd, const mgp_array *phi, int dir, int nodedir);
+int or_fill_boundary_fluxes(const mgp_box *valid, mgp_array *xflux, mgp_array *yflux, const mgp_bdry *bc, int homog);
+int or_compute_grad(const mgp_box *valid, mgp_array *xflux, mgp_array *yflux, mgp_array *phi, const mgp_geo *geo,
+                    const mgp_bdry *bc, int homog);
+int or_compute_div(const mgp_box *valid, mgp_array *div, const mgp_array *xflux, const mgp_array *yflux);
 double or_pnorm(const mgp_box *valid, const mgp_array *bd, int p);
 double or_inner_prod(const mgp_box *valid, const mgp_array *a, const mgp_array *b);
 double or_integrate2d(const mgp_box *valid, const mgp_array *bd, const mgp_geo *geo, int jscale);

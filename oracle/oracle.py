@@ -196,6 +196,29 @@ def boundary_fluxes(phi: BoxData, geo: GeoData):
     return out
 
 
+def compute_pd(pd: BoxData, phi: BoxData, dir: int, nodedir: int):
+    """compute_pd (P2:404-795); pd nodal in x (nodedir 1) or y (2)."""
+    a, p = _host(pd), _host(phi)
+    _ck(lib().or_compute_pd(_r(phi.valid.c()), _r(a), _r(p), dir, nodedir), "compute_pd")
+
+
+def fill_boundary_fluxes(xflux: BoxData, yflux: BoxData, bc: BdryData, homog: bool):
+    x, y, b = _host(xflux), _host(yflux), bc.c()
+    _ck(lib().or_fill_boundary_fluxes(_r(xflux.valid.c()), _r(x), _r(y), _r(b), int(homog)), "fill_boundary_fluxes")
+
+
+def compute_grad(xflux: BoxData, yflux: BoxData, phi: BoxData, geo: GeoData, bc: BdryData, homog: bool):
+    """compute_grad (P2:809-850): J Grad[phi] on x- and y-faces."""
+    x, y, p, g, b = _host(xflux), _host(yflux), _host(phi), geo.c(), bc.c()
+    _ck(lib().or_compute_grad(_r(phi.valid.c()), _r(x), _r(y), _r(p), _r(g), _r(b), int(homog)), "compute_grad")
+
+
+def compute_div(div: BoxData, xflux: BoxData, yflux: BoxData):
+    """compute_div (P2:860-879)."""
+    d, x, y = _host(div), _host(xflux), _host(yflux)
+    _ck(lib().or_compute_div(_r(div.valid.c()), _r(d), _r(x), _r(y)), "compute_div")
+
+
 # ---- deferred correction -------------------------------------------------- #
 def dd_compute_invdiags(invdiags: BoxData, geo: GeoData):
     a, g = _host(invdiags), geo.c()

@@ -327,3 +327,54 @@ def test_batch_problem_generator():
         assert bc.types == [BCTYPE_DIRI] * 4
         assert np.all(geo.J.interior() > 0)
         assert abs(rhs.interior().sum()) < 1e-9 * np.abs(rhs.interior()).sum()
+
+
+@pytest.mark.parametrize("case", ["DDDD-U", "NNNN-NU", "DDNN-U", "NNDD-NU"])
+def test_div_grad_is_the_laplacian(case):
+    """compute_pd uses compute_laplacian's stencils (P2:396-398), so
+    compute_div(compute_grad(phi)) is compute_laplacian(phi) up to rounding,
+    Neumann faces replaced by the BC data in both."""
+    from helpers import BC_CASES, rand_bc, rand_field, rand_geo
+    rng = np.random.default_rng(11)
+    v = Box.of_size(24, 18)
+    types, modes = BC_CASES[case]
+    geo, phi, bc = rand_geo(v, rng), rand_field(v, rng), rand_bc(v, types, modes, rng)
+    xf, yf = BoxData(v, 0, 0, BD_NODE, BD_CELL), BoxData(v, 0, 0, BD_CELL, BD_NODE)
+    O.compute_grad(xf, yf, phi, geo, bc, False)
+    div, lap = BoxData(v), BoxData(v)
+    O.compute_div(div, xf, yf)
+    O.compute_laplacian(lap, phi, geo, bc, False)
+    scale = np.abs(lap.interior()).max()
+    d, l = div.interior(), lap.interior()
+    if types[3] == BCTYPE_NEUM and modes[3] == BCMODE_NONUNIFORM:
+        # compute_laplacian reads the north Neumann data at index jhi for every
+        # column (P2:1220, P2:1256, P2:1303); fill_boundary_fluxes uses the
+        # column's own value
+        d, l = d[:, :-1], l[:, :-1]
+    np.testing.assert_allclose(d, l, rtol=0, atol=1e-12 * scale)
+
+
+def test_compute_pd_exact_for_quadratics():
+    """Every compute_pd stencil -- the centred and one-sided differences and
+    the quadratic extrapolation of the region values -- is exact for a
+    quadratic in (xi, eta): the derivatives on both face families must match
+    the analytic ones to rounding."""
+    v = Box.of_size(20, 14)
+    c = (0.3, 1.7, -0.8, 0.9, -1.3, 0.6)
+
+    def q(xi, eta):
+        return c[0] + c[1] * xi + c[2] * eta + c[3] * xi * xi + c[4] * xi * eta + c[5] * eta * eta
+
+    i = np.arange(-1, v.nx + 1)[:, None]
+    j = np.arange(-1, v.ny + 1)[None, :]
+    phi = BoxData(v, 1, 1)
+    phi.data[:] = q((i + 0.5) * v.dx, (j + 0.5) * v.dy)
+    for nodedir, offs in ((1, (BD_NODE, BD_CELL)), (2, (BD_CELL, BD_NODE))):
+        fi = np.arange(v.nx + (nodedir == 1))[:, None] + (0.0 if nodedir == 1 else 0.5)
+        fj = np.arange(v.ny + (nodedir == 2))[None, :] + (0.0 if nodedir == 2 else 0.5)
+        XI, ETA = fi * v.dx, fj * v.dy
+        exact = {1: c[1] + 2 * c[3] * XI + c[4] * ETA, 2: c[2] + c[4] * XI + 2 * c[5] * ETA}
+        for d in (1, 2):
+            pd = BoxData(v, 0, 0, *offs)
+            O.compute_pd(pd, phi, d, nodedir)
+            np.testing.assert_allclose(pd.interior(), exact[d], rtol=0, atol=1e-10)
