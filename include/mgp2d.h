@@ -173,6 +173,26 @@ int mgp_estimate_maxdepth(int *maxdepth, const mgp_box *valid);
 /* create_mgschedule, MGPoisson2D.f90:67-129.  refx/refy hold maxdepth ints. */
 int mgp_create_mgschedule(int *refx, int *refy, int *maxdepth, const mgp_box *valid);
 
+/* compute_pd, poisson2d.f90:404-795: d(phi)/d(dir) (1 = x, 2 = y) onto the
+ * faces nodal in `nodedir` (1: x-faces, (nx+1) x ny; 2: y-faces,
+ * nx x (ny+1)); the transverse derivative uses the operator's boundary
+ * stencils (simple_bdry_stencil = .false.).  The nodal derivative reads
+ * phi's ghosts as given. */
+int mgp_compute_pd(const mgp_box *valid, mgp_array *pd, const mgp_array *phi, int dir, int nodedir);
+/* compute_grad, poisson2d.f90:809-850: J Grad[phi] on x- and y-faces (fills
+ * phi's ghosts first, do_neum = .false.; Neumann faces take the BC data).
+ * The workspaces of the Fortran signature are internal.  Only valid faces
+ * are written; ghost rows of the flux arrays are left as they are. */
+int mgp_compute_grad(const mgp_box *valid, mgp_array *xflux, mgp_array *yflux, mgp_array *phi,
+                     const mgp_geo *geo, const mgp_bdry *bc, int homog);
+/* fill_boundary_fluxes, arrayutils.f90:1574-1622 (valid faces only, as above). */
+int mgp_fill_boundary_fluxes(const mgp_box *valid, mgp_array *xflux, mgp_array *yflux,
+                             const mgp_bdry *bc, int homog);
+/* compute_div, poisson2d.f90:860-879: J Div[flux] = (xflux(i+1)-xflux(i))/dx
+ * + (yflux(j+1)-yflux(j))/dy on cells. */
+int mgp_compute_div(const mgp_box *valid, mgp_array *div, const mgp_array *xflux, const mgp_array *yflux);
+
+
 /* ------------------------------------------------------------------------ */
 /* Operator-level calls (module Poisson2D and arrayutils)                     */
 /* ------------------------------------------------------------------------ */

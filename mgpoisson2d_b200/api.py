@@ -52,6 +52,10 @@ _SIGS = {
     "mgp_solve_bicgstab2": [_B, _A, _A, _G, _BC, _i, _A, _d, _i, _i, _i, _i],
     "mgp_solve_bicgstab2_noalloc": [_B, _A, _A, _G, _BC, _i, _A, _d, _i, _i, _i, _i],
     "mgp_restrict": [_B, _A, _B, _A, _i, _i],
+    "mgp_compute_pd": [_B, _A, _A, _i, _i],
+    "mgp_compute_grad": [_B, _A, _A, _A, _G, _BC, _i],
+    "mgp_fill_boundary_fluxes": [_B, _A, _A, _BC, _i],
+    "mgp_compute_div": [_B, _A, _A, _A],
     "mgp_prolong": [_B, _A, _B, _A, _G, _G, _BC, _i],
     "mgp_pnorm": [_B, _A, _i, _P(_d)],
     "mgp_inner_prod": [_B, _A, _A, _P(_d)],
@@ -155,6 +159,31 @@ def compute_laplacian(lap: BoxData, phi: BoxData, geo: GeoData, bc: BdryData, ho
     l, p, b, g = lap.c(), phi.c(), bc.c(), geo.c()
     _ck(_lib.mgp_compute_laplacian(_r(lap.valid.c()), _r(l), _r(p), _r(g), _r(b), int(homog), int(jscale)),
         "compute_laplacian")
+
+
+def compute_pd(pd: BoxData, phi: BoxData, dir: int, nodedir: int):
+    """compute_pd, poisson2d.f90:404-795 (pd nodal in x for nodedir 1, y for 2)."""
+    d, p = pd.c(), phi.c()
+    _ck(_lib.mgp_compute_pd(_r(phi.valid.c()), _r(d), _r(p), dir, nodedir), "compute_pd")
+
+
+def compute_grad(xflux: BoxData, yflux: BoxData, phi: BoxData, geo: GeoData, bc: BdryData, homog: bool):
+    """compute_grad, poisson2d.f90:809-850: J Grad[phi] on x- and y-faces."""
+    x, y, p, g, b = xflux.c(), yflux.c(), phi.c(), geo.c(), bc.c()
+    _ck(_lib.mgp_compute_grad(_r(phi.valid.c()), _r(x), _r(y), _r(p), _r(g), _r(b), int(homog)), "compute_grad")
+
+
+def fill_boundary_fluxes(xflux: BoxData, yflux: BoxData, bc: BdryData, homog: bool):
+    """fill_boundary_fluxes, arrayutils.f90:1574-1622."""
+    x, y, b = xflux.c(), yflux.c(), bc.c()
+    _ck(_lib.mgp_fill_boundary_fluxes(_r(xflux.valid.c()), _r(x), _r(y), _r(b), int(homog)),
+        "fill_boundary_fluxes")
+
+
+def compute_div(div: BoxData, xflux: BoxData, yflux: BoxData):
+    """compute_div, poisson2d.f90:860-879."""
+    d, x, y = div.c(), xflux.c(), yflux.c()
+    _ck(_lib.mgp_compute_div(_r(div.valid.c()), _r(d), _r(x), _r(y)), "compute_div")
 
 
 def compute_residual(res: BoxData, rhs: BoxData, phi: BoxData, geo: GeoData, bc: BdryData, homog: bool,
@@ -415,6 +444,6 @@ class Server:
 
 
 __all__ = ["vcycle", "fmg", "dc_vcycle", "Solver", "fill_ghosts", "extrapolate_ghosts", "compute_invdiags",
-           "compute_laplacian", "compute_residual", "relax_gs", "solve_bicgstab2", "solve_bicgstab2_noalloc", "NOALLOC_MAX_SIDE", "restrict", "prolong", "pnorm",
+           "compute_laplacian", "compute_residual", "compute_pd", "compute_grad", "fill_boundary_fluxes", "compute_div", "relax_gs", "solve_bicgstab2", "solve_bicgstab2_noalloc", "NOALLOC_MAX_SIDE", "restrict", "prolong", "pnorm",
            "inner_prod", "estimate_maxdepth", "create_mgschedule", "MGPError", "library_path", "kernel_launch_count",
            "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV", "FLAG_MIXED", "Batch", "Server", "EXPORTS", "KIND_MG", "KIND_DD"]

@@ -1270,6 +1270,81 @@ int mgp_compute_laplacian(const mgp_box* valid, mgp_array* lap, mgp_array* phi, 
     return c.finish();
 }
 
+int mgp_compute_pd(const mgp_box* valid, mgp_array* pd, const mgp_array* phi, int dir, int nodedir) {
+    RC(check_box(valid));
+    if ((dir != 1 && dir != 2) || (nodedir != 1 && nodedir != 2))
+        return set_err(MGP_EINVAL, "compute_pd: direction and nodal direction must be 1 or 2");
+    const int nx = valid->nx, ny = valid->ny, fx = nx + (nodedir == 1), fy = ny + (nodedir == 2);
+    RC(check_array(pd, fx, "pd"));
+    RC(check_array(phi, nx, "phi"));
+    RC(ghost_cap(phi));
+    if (dir == nodedir && ((dir == 1 && phi->ngx < 1) || (dir == 2 && phi->ngy < 1)))
+        return set_err(MGP_EINVAL, "compute_pd: the nodal derivative needs a ghost layer");
+    OpCtx c;
+    DF d, p;
+    RC(c.field(&d, fx, fy, 0));
+    RC(c.in(phi, nx, ny, 1, &p, "phi"));
+    CK(launch_pd(d, p, nx, ny, valid->dx, valid->dy, dir, nodedir, c.st));
+    RC(stage_out(d, pd, fx, fy, 0, c.st));
+    return c.finish();
+}
+
+int mgp_compute_grad(const mgp_box* valid, mgp_array* xflux, mgp_array* yflux, mgp_array* phi, const mgp_geo* geo,
+                     const mgp_bdry* bc, int homog) {
+    RC(check_box(valid));
+    const int nx = valid->nx, ny = valid->ny;
+    RC(check_array(xflux, nx + 1, "xflux"));
+    RC(check_array(yflux, nx, "yflux"));
+    RC(check_array(phi, nx, "phi"));
+    RC(ghost_cap(phi));
+    if (phi->ngx < 1 || phi->ngy < 1) return set_err(MGP_EINVAL, "compute_grad: phi needs a ghost layer");
+    OpCtx c;
+    DF x, y, p;
+    Geo g;
+    BCd b;
+    RC(c.field(&x, nx + 1, ny, 0));
+    RC(c.field(&y, nx, ny + 1, 0));
+    RC(c.in(phi, nx, ny, 1, &p, "phi"));
+    RC(c.geo(geo, valid, &g));
+    RC(c.bc(bc, valid, homog, &b));
+    CK(launch_fill(p, g, b, homog, 0, nx, ny, c.st));   // P2:828
+    CK(launch_grad(x, y, p, g, b, homog, nx, ny, c.st));
+    RC(stage_out(x, xflux, nx + 1, ny, 0, c.st));
+    RC(stage_out(y, yflux, nx, ny + 1, 0, c.st));
+    RC(stage_out(p, phi, nx, ny, 1, c.st));
+    return c.finish();
+}
+
+int mgp_fill_boundary_fluxes(const mgp_box* valid, mgp_array* xflux, mgp_array* yflux, const mgp_bdry* bc,
+                             int homog) {
+    RC(check_box(valid));
+    const int nx = valid->nx, ny = valid->ny;
+    OpCtx c;
+    DF x, y;
+    BCd b;
+    RC(c.in(xflux, nx + 1, ny, 0, &x, "xflux"));
+    RC(c.in(yflux, nx, ny + 1, 0, &y, "yflux"));
+    RC(c.bc(bc, valid, homog, &b));
+    CK(launch_boundary_fluxes(x, y, b, homog, nx, ny, c.st));
+    RC(stage_out(x, xflux, nx + 1, ny, 0, c.st));
+    RC(stage_out(y, yflux, nx, ny + 1, 0, c.st));
+    return c.finish();
+}
+
+int mgp_compute_div(const mgp_box* valid, mgp_array* div, const mgp_array* xflux, const mgp_array* yflux) {
+    RC(check_box(valid));
+    const int nx = valid->nx, ny = valid->ny;
+    RC(check_array(div, nx, "div"));
+    OpCtx c;
+    DF d, x, y;
+    RC(c.field(&d, nx, ny, 0));
+    RC(c.in(xflux, nx + 1, ny, 0, &x, "xflux"));
+    RC(c.in(yflux, nx, ny + 1, 0, &y, "yflux"));
+    CK(launch_div(d, x, y, nx, ny, valid->dx, valid->dy, c.st));
+    RC(stage_out(d, div, nx, ny, 0, c.st));
+    return c.finish();
+}
+
 int mgp_compute_residual(const mgp_box* valid, mgp_array* res, const mgp_array* rhs, mgp_array* phi,
                          const mgp_geo* geo, const mgp_bdry* bc, int homog, int jscale) {
     RC(check_box(valid));

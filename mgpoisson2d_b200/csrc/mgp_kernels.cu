@@ -146,6 +146,142 @@ cudaError_t launch_apply(const DF32& out, const DF32& phi, const DF32& rhs, cons
 }
 
 // ---------------------------------------------------------------------------
+// Gradient and divergence (compute_pd P2:404-795, compute_grad P2:809-850,
+// compute_div P2:860-879, fill_boundary_fluxes AU:1574-1622)
+// ---------------------------------------------------------------------------
+// d(phi)/d(dir) on face (i,j) of the faces nodal in `nodedir` (1: x-faces,
+// i in [0,nx], j in [0,ny); 2: y-faces).  Same operations, in the same order,
+// as compute_pd; the nodal derivative reads the ghosts.
+__device__ double pd_face(const DF& P, int nx, int ny, double dx, double dy, int dir, int nodedir, int i, int j) {
+    St9 s;
+    if (dir == 1 && nodedir == 1) {   // P2:446-449
+        const double scale = 1.0 / dx;
+        return scale * (AT(P, i, j) - AT(P, i - 1, j));
+    }
+    if (dir == 2 && nodedir == 2) {   // P2:614-617
+        const double scale = 1.0 / dy;
+        return scale * (AT(P, i, j) - AT(P, i, j - 1));
+    }
+    if (dir == 1) {   // d/dx on y-faces, P2:450-612
+        const double scale = 0.25 / dx;
+        if (j == 0) {
+            gather9(GLoad{&AT(P, i, 0), P.ld}, region(i, nx, false, false), RLO, s);
+            return scale * (s.ee - s.ew + s.ese - s.esw);
+        }
+        if (j == ny) {
+            gather9(GLoad{&AT(P, i, ny - 1), P.ld}, region(i, nx, false, false), RHI, s);
+            return scale * (s.ene - s.enw + s.ee - s.ew);
+        }
+        if (i == 0)
+            return -scale * (3.0 * AT(P, 0, j) - 4.0 * AT(P, 1, j) + AT(P, 2, j) + 3.0 * AT(P, 0, j - 1) -
+                             4.0 * AT(P, 1, j - 1) + AT(P, 2, j - 1));
+        if (i == nx - 1)
+            return scale * (3.0 * AT(P, nx - 1, j) - 4.0 * AT(P, nx - 2, j) + AT(P, nx - 3, j) +
+                            3.0 * AT(P, nx - 1, j - 1) - 4.0 * AT(P, nx - 2, j - 1) + AT(P, nx - 3, j - 1));
+        return scale * (AT(P, i + 1, j) - AT(P, i - 1, j) + AT(P, i + 1, j - 1) - AT(P, i - 1, j - 1));
+    }
+    // d/dy on x-faces, P2:613-794
+    const double scale = 0.25 / dy;
+    if (i == 0) {
+        gather9(GLoad{&AT(P, 0, j), P.ld}, RLO, region(j, ny, false, false), s);
+        return scale * (s.en - s.es + s.enw - s.esw);
+    }
+    if (i == nx) {
+        gather9(GLoad{&AT(P, nx - 1, j), P.ld}, RHI, region(j, ny, false, false), s);
+        return scale * (s.ene - s.ese + s.en - s.es);
+    }
+    if (j == 0)
+        return -scale * (3.0 * AT(P, i, 0) - 4.0 * AT(P, i, 1) + AT(P, i, 2) + 3.0 * AT(P, i - 1, 0) -
+                         4.0 * AT(P, i - 1, 1) + AT(P, i - 1, 2));
+    if (j == ny - 1)
+        return scale * (3.0 * AT(P, i, ny - 1) - 4.0 * AT(P, i, ny - 2) + AT(P, i, ny - 3) +
+                        3.0 * AT(P, i - 1, ny - 1) - 4.0 * AT(P, i - 1, ny - 2) + AT(P, i - 1, ny - 3));
+    return scale * (AT(P, i, j + 1) - AT(P, i, j - 1) + AT(P, i - 1, j + 1) - AT(P, i - 1, j - 1));
+}
+
+// The value fill_boundary_fluxes writes on face k of Neumann side s.
+__device__ __forceinline__ double bflux(const BCd& b, int homog, int s, int k) {
+    if (homog || b.mode[s] == M_LAH) return 0.0;
+    if (b.mode[s] == M_UNIFORM) return b.u[s];
+    return b.d[s][k];
+}
+
+__global__ void k_pd(DF pd, DF phi, int nx, int ny, double dx, double dy, int dir, int nodedir) {
+    CELL_IJ
+    if (i >= nx + (nodedir == 1) || j >= ny + (nodedir == 2)) return;
+    AT(pd, i, j) = pd_face(phi, nx, ny, dx, dy, dir, nodedir, i, j);
+}
+
+cudaError_t launch_pd(const DF& pd, const DF& phi, int nx, int ny, double dx, double dy, int dir, int nodedir,
+                      cudaStream_t st) {
+    k_pd<<<cells_grid(nx + 1, ny + 1, kBlk2), kBlk2, 0, st>>>(pd, phi, nx, ny, dx, dy, dir, nodedir);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// J Grad[phi] on one face family (ghosts of phi filled), Neumann faces
+// replaced by the BC flux (fill_boundary_fluxes).
+__global__ void k_grad(DF flux, DF phi, Geo g, BCd b, int homog, int nx, int ny, int nodedir) {
+    CELL_IJ
+    if (nodedir == 1) {
+        if (i > nx || j >= ny) return;
+        const double pdn = pd_face(phi, nx, ny, g.dx, g.dy, 1, 1, i, j);
+        const double pdt = pd_face(phi, nx, ny, g.dx, g.dy, 2, 1, i, j);
+        double v = AT(g.xx, i, j) * pdn + AT(g.xy, i, j) * pdt;   // P2:833-834
+        if (i == 0 && b.type[S_XLO] == T_NEUM) v = bflux(b, homog, S_XLO, j);
+        if (i == nx && b.type[S_XHI] == T_NEUM) v = bflux(b, homog, S_XHI, j);
+        AT(flux, i, j) = v;
+    } else {
+        if (i >= nx || j > ny) return;
+        const double pdt = pd_face(phi, nx, ny, g.dx, g.dy, 1, 2, i, j);
+        const double pdn = pd_face(phi, nx, ny, g.dx, g.dy, 2, 2, i, j);
+        double v = AT(g.yx, i, j) * pdt + AT(g.yy, i, j) * pdn;   // P2:843-844
+        if (j == 0 && b.type[S_YLO] == T_NEUM) v = bflux(b, homog, S_YLO, i);
+        if (j == ny && b.type[S_YHI] == T_NEUM) v = bflux(b, homog, S_YHI, i);
+        AT(flux, i, j) = v;
+    }
+}
+
+cudaError_t launch_grad(const DF& xflux, const DF& yflux, const DF& phi, const Geo& g, const BCd& b, int homog,
+                        int nx, int ny, cudaStream_t st) {
+    k_grad<<<cells_grid(nx + 1, ny, kBlk2), kBlk2, 0, st>>>(xflux, phi, g, b, homog, nx, ny, 1);
+    k_grad<<<cells_grid(nx, ny + 1, kBlk2), kBlk2, 0, st>>>(yflux, phi, g, b, homog, nx, ny, 2);
+    count_launch(2);
+    return cudaGetLastError();
+}
+
+__global__ void k_boundary_fluxes(DF xflux, DF yflux, BCd b, int homog, int nx, int ny) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int s = 0; s < 4; ++s) {
+        if (b.type[s] != T_NEUM) continue;
+        if (s < 2 && k < ny) AT(xflux, s == S_XLO ? 0 : nx, k) = bflux(b, homog, s, k);
+        if (s >= 2 && k < nx) AT(yflux, k, s == S_YLO ? 0 : ny) = bflux(b, homog, s, k);
+    }
+}
+
+cudaError_t launch_boundary_fluxes(const DF& xflux, const DF& yflux, const BCd& b, int homog, int nx, int ny,
+                                   cudaStream_t st) {
+    const int n = nx > ny ? nx : ny;
+    k_boundary_fluxes<<<(n + 255) / 256, 256, 0, st>>>(xflux, yflux, b, homog, nx, ny);
+    count_launch();
+    return cudaGetLastError();
+}
+
+__global__ void k_div(DF div, DF xflux, DF yflux, int nx, int ny, double dx, double dy) {
+    CELL_IJ
+    if (i >= nx || j >= ny) return;
+    const double invdx = 1.0 / dx, invdy = 1.0 / dy;
+    AT(div, i, j) = invdx * (AT(xflux, i + 1, j) - AT(xflux, i, j)) + invdy * (AT(yflux, i, j + 1) - AT(yflux, i, j));
+}
+
+cudaError_t launch_div(const DF& div, const DF& xflux, const DF& yflux, int nx, int ny, double dx, double dy,
+                       cudaStream_t st) {
+    k_div<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(div, xflux, yflux, nx, ny, dx, dy);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Gauss-Seidel (relax_gs, P2:1460-1988) in the device order:
 //   1. ghosts once (P2:1556);
 //   2. colours (i mod 2, j mod 2) = (0,0),(1,1),(1,0),(0,1) over the interior

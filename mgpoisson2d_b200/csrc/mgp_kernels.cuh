@@ -124,6 +124,16 @@ cudaError_t launch_sub_mean(const DF& y, const double* out, int nx, int ny, int 
 // Reduction over the valid region into out[0] (and out[1] for RED_JSUM: volume).
 cudaError_t launch_reduce(int kind, const DF& a, const DF& b, int nx, int ny, double vol, double* partials,
                           double* out, cudaStream_t st);
+// Gradient and divergence (compute_pd, compute_grad, compute_div,
+// fill_boundary_fluxes); phi's ghosts filled by the caller.
+cudaError_t launch_pd(const DF& pd, const DF& phi, int nx, int ny, double dx, double dy, int dir, int nodedir,
+                      cudaStream_t st);
+cudaError_t launch_grad(const DF& xflux, const DF& yflux, const DF& phi, const Geo& g, const BCd& b, int homog,
+                        int nx, int ny, cudaStream_t st);
+cudaError_t launch_boundary_fluxes(const DF& xflux, const DF& yflux, const BCd& b, int homog, int nx, int ny,
+                                   cudaStream_t st);
+cudaError_t launch_div(const DF& div, const DF& xflux, const DF& yflux, int nx, int ny, double dx, double dy,
+                       cudaStream_t st);
 // Deferred-correction operators.
 cudaError_t launch_dd_invdiag(const DF& invd, const Geo& g, int nx, int ny, cudaStream_t st);
 cudaError_t launch_dd_apply(const DF& out, const DF& phi, const DF& rhs, const Geo& g, const BCd& b, int nx, int ny,

@@ -477,3 +477,48 @@ def test_server_results_same_alone_and_in_the_mix(M):
         rep, lat, qt = results[n]
         assert rep.status == 0 and lat >= qt >= 0.0
         assert same(outs[n].data, pa.data) and np.array_equal(rep.relres, ra.relres)
+
+
+# ---------------------------------------------------------------------------
+# Gradient and divergence (compute_pd, compute_grad, compute_div,
+# fill_boundary_fluxes): bit-exact
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("dir,nodedir", [(1, 1), (2, 1), (1, 2), (2, 2)])
+@pytest.mark.parametrize("nx,ny", [(16, 12), (9, 7), (40, 33)])
+def test_compute_pd_bitexact(M, dir, nodedir, nx, ny):
+    rng = np.random.default_rng(nx * 100 + ny + 7 * dir + nodedir)
+    v = Box.of_size(nx, ny)
+    phi = rand_field(v, rng)
+    offs = (BD_NODE, BD_CELL) if nodedir == 1 else (BD_CELL, BD_NODE)
+    a, b = BoxData(v, 0, 0, *offs), BoxData(v, 0, 0, *offs)
+    O.compute_pd(a, phi, dir, nodedir)
+    M.compute_pd(b, phi, dir, nodedir)
+    assert same(a.data, b.data)
+
+
+@pytest.mark.parametrize("case", list(BC_CASES))
+@pytest.mark.parametrize("homog", [False, True])
+def test_compute_grad_div_bitexact(M, case, homog):
+    v, geo, phi, bc, rng = _problem(case, 20, 14, 77)
+    xa, ya = BoxData(v, 0, 0, BD_NODE, BD_CELL), BoxData(v, 0, 0, BD_CELL, BD_NODE)
+    xb, yb = BoxData(v, 0, 0, BD_NODE, BD_CELL), BoxData(v, 0, 0, BD_CELL, BD_NODE)
+    pa, pb = phi.copy(), phi.copy()
+    O.compute_grad(xa, ya, pa, geo, bc, homog)
+    M.compute_grad(xb, yb, pb, geo, bc, homog)
+    assert same(xa.data, xb.data) and same(ya.data, yb.data)
+    assert same(pa.data, pb.data)   # the ghosts compute_grad fills
+    da, db = BoxData(v), BoxData(v)
+    O.compute_div(da, xa, ya)
+    M.compute_div(db, xa, ya)
+    assert same(da.data, db.data)
+
+
+@pytest.mark.parametrize("case", ["NNNN-U", "NNNN-NU", "DNND-mixed"])
+@pytest.mark.parametrize("homog", [False, True])
+def test_fill_boundary_fluxes_bitexact(M, case, homog):
+    v, geo, phi, bc, rng = _problem(case, 12, 10, 5)
+    xa, ya = rand_field(v, rng, 0, BD_NODE, BD_CELL), rand_field(v, rng, 0, BD_CELL, BD_NODE)
+    xb, yb = xa.copy(), ya.copy()
+    O.fill_boundary_fluxes(xa, ya, bc, homog)
+    M.fill_boundary_fluxes(xb, yb, bc, homog)
+    assert same(xa.data, xb.data) and same(ya.data, yb.data)
