@@ -211,6 +211,12 @@ int mgp_compute_laplacian(const mgp_box *valid, mgp_array *lap, mgp_array *phi,
 int mgp_compute_residual(const mgp_box *valid, mgp_array *res, const mgp_array *rhs,
                          mgp_array *phi, const mgp_geo *geo, const mgp_bdry *bc,
                          int homog, int jscale);
+/* relax_jacobi, poisson2d.f90:1358-1451: weighted Jacobi iterations
+ * (phi <- omega (phi + r invdiag) + (1 - omega) phi over every cell, then the
+ * residual again); tol > 0 stops on |r|/|r0| <= tol. */
+int mgp_relax_jacobi(const mgp_box *valid, mgp_array *phi, const mgp_array *rhs, const mgp_geo *geo,
+                     const mgp_bdry *bc, int homog, const mgp_array *invdiags, double omega, double tol,
+                     int maxiters, int zerophi, int verbosity);
 /* relax_gs, poisson2d.f90:1460-1988.  The device sweep visits the four
  * colours (i mod 2, j mod 2) = (0,0),(1,1),(1,0),(0,1) in turn instead of the
  * lexicographic order; ghosts are refreshed once per sweep as in P2:1556. */

@@ -11,7 +11,7 @@ from .types import *  # noqa: F401,F403
 _API_NAMES = {
     "vcycle", "fmg", "dc_vcycle", "Solver", "Batch", "Server", "fill_ghosts", "extrapolate_ghosts", "compute_invdiags",
     "compute_laplacian", "compute_residual", "compute_pd", "compute_grad", "fill_boundary_fluxes",
-    "compute_div", "relax_gs", "solve_bicgstab2", "solve_bicgstab2_noalloc", "restrict", "prolong",
+    "compute_div", "relax_gs", "relax_jacobi", "solve_bicgstab2", "solve_bicgstab2_noalloc", "restrict", "prolong",
     "pnorm", "inner_prod", "estimate_maxdepth", "create_mgschedule", "MGPError", "library_path",
     "kernel_launch_count", "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV", "FLAG_MIXED",
     "NOALLOC_MAX_SIDE", "EXPORTS",

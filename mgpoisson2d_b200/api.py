@@ -49,6 +49,7 @@ _SIGS = {
     "mgp_compute_laplacian": [_B, _A, _A, _G, _BC, _i, _i],
     "mgp_compute_residual": [_B, _A, _A, _A, _G, _BC, _i, _i],
     "mgp_relax_gs": [_B, _A, _A, _G, _BC, _i, _A, _d, _d, _i, _i, _i],
+    "mgp_relax_jacobi": [_B, _A, _A, _G, _BC, _i, _A, _d, _d, _i, _i, _i],
     "mgp_solve_bicgstab2": [_B, _A, _A, _G, _BC, _i, _A, _d, _i, _i, _i, _i],
     "mgp_solve_bicgstab2_noalloc": [_B, _A, _A, _G, _BC, _i, _A, _d, _i, _i, _i, _i],
     "mgp_restrict": [_B, _A, _B, _A, _i, _i],
@@ -192,6 +193,14 @@ def compute_residual(res: BoxData, rhs: BoxData, phi: BoxData, geo: GeoData, bc:
     r, f, p, b, g = res.c(), rhs.c(), phi.c(), bc.c(), geo.c()
     _ck(_lib.mgp_compute_residual(_r(res.valid.c()), _r(r), _r(f), _r(p), _r(g), _r(b), int(homog), int(jscale)),
         "compute_residual")
+
+
+def relax_jacobi(phi: BoxData, rhs: BoxData, geo: GeoData, bc: BdryData, homog: bool, invdiags: BoxData,
+                 omega: float, tol: float, maxiters: int, zerophi: bool = False, verbosity: int = 0):
+    """relax_jacobi, poisson2d.f90:1358-1451."""
+    p, f, b, g, d = phi.c(), rhs.c(), bc.c(), geo.c(), invdiags.c()
+    _ck(_lib.mgp_relax_jacobi(_r(phi.valid.c()), _r(p), _r(f), _r(g), _r(b), int(homog), _r(d), omega, tol,
+                              maxiters, int(zerophi), verbosity), "relax_jacobi")
 
 
 def relax_gs(phi: BoxData, rhs: BoxData, geo: GeoData, bc: BdryData, homog: bool, invdiags: BoxData, omega: float,
@@ -444,6 +453,6 @@ class Server:
 
 
 __all__ = ["vcycle", "fmg", "dc_vcycle", "Solver", "fill_ghosts", "extrapolate_ghosts", "compute_invdiags",
-           "compute_laplacian", "compute_residual", "compute_pd", "compute_grad", "fill_boundary_fluxes", "compute_div", "relax_gs", "solve_bicgstab2", "solve_bicgstab2_noalloc", "NOALLOC_MAX_SIDE", "restrict", "prolong", "pnorm",
+           "compute_laplacian", "compute_residual", "compute_pd", "compute_grad", "fill_boundary_fluxes", "compute_div", "relax_gs", "relax_jacobi", "solve_bicgstab2", "solve_bicgstab2_noalloc", "NOALLOC_MAX_SIDE", "restrict", "prolong", "pnorm",
            "inner_prod", "estimate_maxdepth", "create_mgschedule", "MGPError", "library_path", "kernel_launch_count",
            "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV", "FLAG_MIXED", "Batch", "Server", "EXPORTS", "KIND_MG", "KIND_DD"]

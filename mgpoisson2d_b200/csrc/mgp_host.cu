@@ -1368,6 +1368,59 @@ int mgp_compute_residual(const mgp_box* valid, mgp_array* res, const mgp_array* 
     return c.finish();
 }
 
+int mgp_relax_jacobi(const mgp_box* valid, mgp_array* phi, const mgp_array* rhs, const mgp_geo* geo,
+                     const mgp_bdry* bc, int homog, const mgp_array* invdiags, double omega, double tol, int maxiters,
+                     int zerophi, int verbosity) {
+    RC(check_box(valid));
+    RC(no_lah(bc));
+    RC(check_array(phi, valid->nx, "phi"));
+    RC(ghost_cap(phi));
+    if (maxiters == 0) return MGP_OK;
+    const int nx = valid->nx, ny = valid->ny;
+    OpCtx c;
+    DF p, f, d, r;
+    Geo g;
+    BCd b;
+    double* red = nullptr;
+    RC(c.in(phi, nx, ny, 1, &p, "phi"));
+    RC(c.in(rhs, nx, ny, 0, &f, "rhs"));
+    RC(c.in(invdiags, nx, ny, 0, &d, "invdiags"));
+    RC(c.field(&r, nx, ny, 0));
+    RC(c.dbuf(&red, kRedSlots));
+    RC(c.geo(geo, valid, &g));
+    RC(c.bc(bc, valid, homog, &b));
+    if (zerophi) CK(launch_fillval(p, 0.0, nx, ny, 1, 1, c.st));
+    const double vol = valid->dx * valid->dy;
+    double rscale = 1.0, h = 0.0;
+    auto residual = [&]() -> int {   // compute_residual (P2:1327-1353)
+        CK(launch_fill(p, g, b, homog, 0, nx, ny, c.st));
+        CK(launch_apply(r, p, f, g, b, homog, nx, ny, 1, 0, c.st));
+        return MGP_OK;
+    };
+    auto norm = [&](double* out) -> int {
+        CK(launch_reduce(RED_SUMSQ, r, r, nx, ny, vol, red, red + 2 * 296, c.st));
+        CK(cudaMemcpyAsync(out, red + 2 * 296, 8, cudaMemcpyDeviceToHost, c.st));
+        CK(cudaStreamSynchronize(c.st));
+        return MGP_OK;
+    };
+    RC(residual());
+    if (tol > 0.0) {
+        RC(norm(&rscale));
+        if (rscale == 0.0) rscale = 1.0;
+    }
+    for (int it = 1; it <= maxiters; ++it) {
+        CK(launch_jacobi(p, r, d, omega, nx, ny, c.st));   // P2:1419-1424
+        RC(residual());
+        if (tol > 0.0) {
+            RC(norm(&h));
+            if (verbosity >= 3) printf("iter %d: rel |res| = %.16e\n", it, h / rscale);
+            if (h / rscale <= tol) break;
+        }
+    }
+    RC(stage_out(p, phi, nx, ny, 1, c.st));
+    return c.finish();
+}
+
 int mgp_relax_gs(const mgp_box* valid, mgp_array* phi, const mgp_array* rhs, const mgp_geo* geo, const mgp_bdry* bc,
                  int homog, const mgp_array* invdiags, double omega, double tol, int maxiters, int zerophi,
                  int verbosity) {

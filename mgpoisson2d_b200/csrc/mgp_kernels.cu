@@ -566,6 +566,21 @@ cudaError_t launch_convert(const DF& dst, const DF32& src, int nx, int ny, int g
     return cudaGetLastError();
 }
 
+// One weighted Jacobi update (relax_jacobi, P2:1419-1424).
+__global__ void k_jacobi(DF phi, DF r, DF invd, double omega, int nx, int ny) {
+    CELL_IJ
+    if (i >= nx || j >= ny) return;
+    const double p = AT(phi, i, j);
+    const double newphi = p + AT(r, i, j) * AT(invd, i, j);
+    AT(phi, i, j) = omega * newphi + (1.0 - omega) * p;
+}
+
+cudaError_t launch_jacobi(const DF& phi, const DF& r, const DF& invd, double omega, int nx, int ny, cudaStream_t st) {
+    k_jacobi<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(phi, r, invd, omega, nx, ny);
+    count_launch();
+    return cudaGetLastError();
+}
+
 __global__ void k_axpby(DF y, DF x, double a, double b, int nx, int ny, int gx, int gy) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x - gx;
     const int j = blockIdx.y * blockDim.y + threadIdx.y - gy;

@@ -114,6 +114,7 @@ cudaError_t launch_prolong(const DF& fine, const DF& crse, int ncx, int ncy, int
                            cudaStream_t st);
 cudaError_t launch_prolong_cross(const DF& fine, const DF& crse, int ncx, int ncy, cudaStream_t st);
 cudaError_t launch_set_guess(const DF& e, const DF& r, const DF& invd, int nx, int ny, cudaStream_t st);
+cudaError_t launch_jacobi(const DF& phi, const DF& r, const DF& invd, double omega, int nx, int ny, cudaStream_t st);
 // y[i,j] = a*y + b*x over i in [-gx, nx+gx), j in [-gy, ny+gy).
 cudaError_t launch_axpby(const DF& y, const DF& x, double a, double b, int nx, int ny, int gx, int gy,
                          cudaStream_t st);

@@ -943,6 +943,47 @@ int or_relax_gs(const mgp_box *valid, mgp_array *phi, const mgp_array *rhs,
     return rc;
 }
 
+/* relax_jacobi (P2:1358-1451): phi += r*invdiag for every cell, weighted by
+ * omega, then the residual again; tol > 0 stops on the relative residual. */
+int or_relax_jacobi(const mgp_box *valid, mgp_array *phi, const mgp_array *rhs, const mgp_geo *geo,
+                    const mgp_bdry *bc, int homog, const mgp_array *invd, double omega, double tol, int maxiters,
+                    int zerophi, int verbosity)
+{
+    const int nx = valid->nx, ny = valid->ny;
+    mgp_array r;
+    V R, PH, D;
+    double rscale = one, relres;
+    int rc, iter, i, j;
+    if (maxiters == 0) return MGP_OK;
+    if ((rc = check_op(valid, bc))) return rc;
+    r = alloc_like(nx, ny, 0, 0);
+    if (!r.data) return fail(MGP_ENOMEM, "relax_jacobi: out of memory");
+    R = view(&r); PH = view(phi); D = view(invd);
+    if (zerophi) zero_all(phi, nx, ny);
+    if ((rc = or_compute_residual(valid, &r, rhs, phi, geo, bc, homog, 0))) goto done;
+    if (tol > zero) {
+        rscale = or_pnorm(valid, &r, 2);
+        if (rscale == zero) rscale = one;
+        if (verbosity >= 3) printf("scale |res| = %.16e\n", rscale);
+    }
+    for (iter = 1; iter <= maxiters; ++iter) {
+        for (j = 0; j < ny; ++j)
+            for (i = 0; i < nx; ++i) {
+                const double newphi = AT(PH, i, j) + AT(R, i, j) * AT(D, i, j);
+                AT(PH, i, j) = omega * newphi + (one - omega) * AT(PH, i, j);
+            }
+        if ((rc = or_compute_residual(valid, &r, rhs, phi, geo, bc, homog, 0))) break;
+        if (tol > zero) {
+            relres = or_pnorm(valid, &r, 2) / rscale;
+            if (verbosity >= 3) printf("iter %d: rel |res| = %.16e\n", iter, relres);
+            if (relres <= tol) break;
+        }
+    }
+done:
+    free(r.data);
+    return rc;
+}
+
 /* ---- solve_bicgstab2: P2:2253-2477 and DD:339-566 ------------------------ */
 
 typedef struct {

@@ -55,6 +55,10 @@ int or_relax_gs(const mgp_box *valid, mgp_array *phi, const mgp_array *rhs,
                 const mgp_geo *geo, const mgp_bdry *bc, int homog, const mgp_array *invd,
                 double omega, double tol, int maxiters, int zerophi, int verbosity,
                 int gs_order);
+/* relax_jacobi, P2:1358-1451. */
+int or_relax_jacobi(const mgp_box *valid, mgp_array *phi, const mgp_array *rhs, const mgp_geo *geo,
+                    const mgp_bdry *bc, int homog, const mgp_array *invd, double omega, double tol, int maxiters,
+                    int zerophi, int verbosity);
 int or_solve_bicgstab2(const mgp_box *valid, mgp_array *phi, const mgp_array *rhs,
                        const mgp_geo *geo, const mgp_bdry *bc, int homog,
                        const mgp_array *invd, double tol, int max_iters, int max_restarts,

@@ -48,6 +48,11 @@ def _load():
         "or_compute_laplacian": [B, A, A, G, BC, i, i],
         "or_compute_residual": [B, A, A, A, G, BC, i, i],
         "or_relax_gs": [B, A, A, G, BC, i, A, d, d, i, i, i, i],
+        "or_relax_jacobi": [B, A, A, G, BC, i, A, d, d, i, i, i],
+        "or_compute_pd": [B, A, A, i, i],
+        "or_fill_boundary_fluxes": [B, A, A, BC, i],
+        "or_compute_grad": [B, A, A, A, G, BC, i],
+        "or_compute_div": [B, A, A, A],
         "or_solve_bicgstab2": [B, A, A, G, BC, i, A, d, i, i, i, i, i],
         "or_restrict": [B, A, B, A, i, i],
         "or_prolong": [B, A, B, A, G, G, BC, i],
@@ -149,6 +154,14 @@ def relax_gs(phi: BoxData, rhs: BoxData, geo: GeoData, bc: BdryData, homog: bool
     p, f, b, g, d = _host(phi), _host(rhs), bc.c(), geo.c(), _host(invdiags)
     _ck(lib().or_relax_gs(_r(phi.valid.c()), _r(p), _r(f), _r(g), _r(b), int(homog), _r(d), omega, tol,
                           maxiters, int(zerophi), verbosity, gs_order), "relax_gs")
+
+
+def relax_jacobi(phi: BoxData, rhs: BoxData, geo: GeoData, bc: BdryData, homog: bool, invdiags: BoxData,
+                 omega: float, tol: float, maxiters: int, zerophi: bool, verbosity: int = 0):
+    """relax_jacobi (P2:1358-1451)."""
+    p, f, b, g, d = _host(phi), _host(rhs), bc.c(), geo.c(), _host(invdiags)
+    _ck(lib().or_relax_jacobi(_r(phi.valid.c()), _r(p), _r(f), _r(g), _r(b), int(homog), _r(d), omega, tol,
+                              maxiters, int(zerophi), verbosity), "relax_jacobi")
 
 
 def solve_bicgstab2(phi: BoxData, rhs: BoxData, geo: GeoData, bc: BdryData, homog: bool, invdiags: BoxData,

@@ -522,3 +522,15 @@ def test_fill_boundary_fluxes_bitexact(M, case, homog):
     O.fill_boundary_fluxes(xa, ya, bc, homog)
     M.fill_boundary_fluxes(xb, yb, bc, homog)
     assert same(xa.data, xb.data) and same(ya.data, yb.data)
+
+
+@pytest.mark.parametrize("case", ["DDDD-U", "NNNN-NU", "DNND-mixed", "PPDD"])
+@pytest.mark.parametrize("omega", [1.0, 0.8])
+def test_relax_jacobi_bitexact(M, case, omega):
+    v, geo, phi, bc, rng = _problem(case, 18, 14, 31)
+    rhs, d = rand_field(v, rng, 0), BoxData(v)
+    d.data[:] = rng.uniform(-0.5, -0.1, d.data.shape)
+    pa, pb = phi.copy(), phi.copy()
+    O.relax_jacobi(pa, rhs, geo, bc, False, d, omega, -1.0, 5, False)
+    M.relax_jacobi(pb, rhs, geo, bc, False, d, omega, -1.0, 5)
+    assert same(pa.data, pb.data)
