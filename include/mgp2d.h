@@ -315,6 +315,30 @@ int mgp_solver_dc_vcycle(mgp_solver *s, mgp_array *phi, mgp_array *rhs, const mg
                          mgp_report *report);
 
 /* ------------------------------------------------------------------------ */
+/* Metric terms and right-hand sides generated on the device from an analytic */
+/* map (the Fortran test program builds them on the host, test.f90:566-716).  */
+/* Arrays may be device or host memory; device arrays are written in place.   */
+/* ------------------------------------------------------------------------ */
+#define MGP_MAP_IDENTITY   0   /* x = xi, y = eta                                  */
+#define MGP_MAP_WAVY_EXP   1   /* params {a, beta}: x = xi + a sin(2 pi xi) sin(2 pi eta),
+                                  y = (e^{beta eta} - 1)/(e^beta - 1)             */
+#define MGP_MAP_SKEW_LAYER 2   /* params {tan(angle), ratio, t*, n_ref}: y grows by
+                                  `ratio` per cell (of n_ref cells) up to t* cells
+                                  from y = 0, uniformly beyond, normalised to
+                                  [0,1]; x = xi + tan(angle) y                     */
+/* J, Jgup_xx, Jgup_xy, Jgup_yx, Jgup_yy over the whole allocation of each array
+ * (valid points and ghosts), by one-cell differences of the map half a cell
+ * either side: J = x_xi y_eta - x_eta y_xi, Jgup_xx = (x_eta^2 + y_eta^2)/J,
+ * Jgup_xy = Jgup_yx = -(x_xi x_eta + y_xi y_eta)/J, Jgup_yy = (x_xi^2 + y_xi^2)/J.
+ * Sets geo->dx, geo->dy from the box. */
+int mgp_map_geometry(const mgp_box *valid, int map, const double *params, mgp_geo *geo);
+/* rhs = J (f - <f>_J), f = sum_k amp[k] cos(pi m_x[k] x) cos(pi m_y[k] y) at the
+ * mapped cell centres, <f>_J its J-weighted mean. */
+int mgp_map_fourier_rhs(const mgp_box *valid, int map, const double *params, int nmodes,
+                        const double *amp, const int *m_x, const int *m_y, const mgp_array *J,
+                        mgp_array *rhs);
+
+/* ------------------------------------------------------------------------ */
 /* Many solves at once.  No reference counterpart: the Fortran library solves */
 /* one problem per call.  Both front ends run the single-problem solver       */
 /* unchanged on several host workers, each with its own CUDA stream, so the   */

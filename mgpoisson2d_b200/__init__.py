@@ -9,7 +9,8 @@ use; they raise ImportError when the CUDA library has not been built.
 from .types import *  # noqa: F401,F403
 
 _API_NAMES = {
-    "vcycle", "fmg", "dc_vcycle", "Solver", "Batch", "Server", "fill_ghosts", "extrapolate_ghosts", "compute_invdiags",
+    "vcycle", "fmg", "dc_vcycle", "Solver", "Batch", "Server", "map_geometry", "map_fourier_rhs", "MAP_IDENTITY", "MAP_WAVY_EXP",
+    "MAP_SKEW_LAYER", "fill_ghosts", "extrapolate_ghosts", "compute_invdiags",
     "compute_laplacian", "compute_residual", "compute_pd", "compute_grad", "fill_boundary_fluxes",
     "compute_div", "relax_gs", "relax_jacobi", "solve_bicgstab2", "solve_bicgstab2_noalloc", "restrict", "prolong",
     "pnorm", "inner_prod", "estimate_maxdepth", "create_mgschedule", "MGPError", "library_path",

@@ -18,8 +18,8 @@ from typing import Optional
 
 import numpy as np
 
-from .types import (KIND_DD, KIND_MG, STATUS_NAMES, BdryData, Box, BoxData, GeoData, MgpArray, MgpBdry, MgpBox,
-                    MgpGeo, MgpReport, Report, make_report, read_report)
+from .types import (BD_CELL, BD_NODE, KIND_DD, KIND_MG, STATUS_NAMES, BdryData, Box, BoxData, GeoData, MgpArray,
+                    MgpBdry, MgpBox, MgpGeo, MgpReport, Report, make_report, read_report)
 
 FLAG_DIRICHLET_COUPLED_DIAG = 1
 FLAG_TIME_SMOOTHER = 2
@@ -70,6 +70,8 @@ _SIGS = {
     "mgp_solver_vcycle": [_vp, _A, _A, _BC, _i, _d, _i, _i, _i, _i, _i, _i, _i, _R],
     "mgp_solver_fmg": [_vp, _A, _A, _BC, _i, _d, _i, _i, _i, _i, _i, _i, _i, _R],
     "mgp_solver_dc_vcycle": [_vp, _A, _A, _BC, _i, _d, _i, _i, _i, _i, _i, _i, _i, _R],
+    "mgp_map_geometry": [_B, _i, _P(_d), _G],
+    "mgp_map_fourier_rhs": [_B, _i, _P(_d), _i, _P(_d), _P(_i), _P(_i), _A, _A],
     "mgp_batch_create": [_i, _B, _G, _BC, _i, _i, _i, _i, _P(_vp)],
     "mgp_batch_destroy": [_vp],
     "mgp_batch_size": [_vp, _P(_i)],
@@ -356,6 +358,40 @@ class Solver:
                            numcycles, smooth_down, smooth_up, smooth_bottom, zerophi, verbosity)
 
 
+MAP_IDENTITY, MAP_WAVY_EXP, MAP_SKEW_LAYER = 0, 1, 2
+
+
+def _params(params):
+    arr = (C.c_double * max(1, len(params)))(*params)
+    return arr
+
+
+def map_geometry(valid: Box, kind: int, params=(), device: bool = True, ng: int = 1) -> GeoData:
+    """Metric terms of an analytic map, generated on the device
+    (mgp_map_geometry); the arrays stay on the device unless device=False."""
+    mk = (lambda oi, oj: BoxData.device_zeros(valid, ng, ng, oi, oj)) if device else \
+        (lambda oi, oj: BoxData(valid, ng, ng, oi, oj))
+    geo = GeoData(mk(BD_CELL, BD_CELL), mk(BD_NODE, BD_CELL), mk(BD_NODE, BD_CELL), mk(BD_CELL, BD_NODE),
+                  mk(BD_CELL, BD_NODE), valid.dx, valid.dy)
+    g = geo.c()
+    _ck(_lib.mgp_map_geometry(_r(valid.c()), kind, _params(params), _r(g)), "map_geometry")
+    return geo
+
+
+def map_fourier_rhs(valid: Box, kind: int, params, amp, mx, my, J: BoxData, device: bool = True) -> BoxData:
+    """rhs = J (f - <f>_J), f = sum amp cos(pi mx x) cos(pi my y) at the mapped
+    cell centres (mgp_map_fourier_rhs)."""
+    rhs = BoxData.device_zeros(valid) if device else BoxData(valid)
+    n = len(amp)
+    a = (C.c_double * max(1, n))(*amp)
+    m1 = (C.c_int * max(1, n))(*[int(v) for v in mx])
+    m2 = (C.c_int * max(1, n))(*[int(v) for v in my])
+    j, r = J.c(), rhs.c()
+    _ck(_lib.mgp_map_fourier_rhs(_r(valid.c()), kind, _params(params), n, a, m1, m2, _r(j), _r(r)),
+        "map_fourier_rhs")
+    return rhs
+
+
 class Batch:
     """Independent problems solved concurrently (mgp_batch_*): one resident
     hierarchy per problem, ``nstreams`` host workers with their own streams.
@@ -455,4 +491,5 @@ class Server:
 __all__ = ["vcycle", "fmg", "dc_vcycle", "Solver", "fill_ghosts", "extrapolate_ghosts", "compute_invdiags",
            "compute_laplacian", "compute_residual", "compute_pd", "compute_grad", "fill_boundary_fluxes", "compute_div", "relax_gs", "relax_jacobi", "solve_bicgstab2", "solve_bicgstab2_noalloc", "NOALLOC_MAX_SIDE", "restrict", "prolong", "pnorm",
            "inner_prod", "estimate_maxdepth", "create_mgschedule", "MGPError", "library_path", "kernel_launch_count",
-           "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV", "FLAG_MIXED", "Batch", "Server", "EXPORTS", "KIND_MG", "KIND_DD"]
+           "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV", "FLAG_MIXED", "Batch", "Server", "map_geometry", "map_fourier_rhs",
+           "MAP_IDENTITY", "MAP_WAVY_EXP", "MAP_SKEW_LAYER", "EXPORTS", "KIND_MG", "KIND_DD"]

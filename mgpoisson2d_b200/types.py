@@ -163,6 +163,16 @@ class BoxData:
             d = np.full(self.data.shape, fill, dtype=np.float64, order="F")
         return BoxData(self.valid, self.ngx, self.ngy, self.offi, self.offj, data=d)
 
+    @staticmethod
+    def device_zeros(valid: Box, ngx: int = 0, ngy: int = 0, offi: int = BD_CELL, offj: int = BD_CELL,
+                     device="cuda") -> "BoxData":
+        """Zero-filled storage allocated on the device (no host copy)."""
+        import torch
+        nvx = valid.nx + (1 if offi == BD_NODE else 0)
+        nvy = valid.ny + (1 if offj == BD_NODE else 0)
+        t = torch.zeros((nvy + 2 * ngy, nvx + 2 * ngx), dtype=torch.float64, device=device)
+        return BoxData(valid, ngx, ngy, offi, offj, data=t)
+
     def to_device(self, device="cuda") -> "BoxData":
         import torch
         t = torch.from_numpy(np.ascontiguousarray(self.host().T)).to(device)

@@ -40,12 +40,18 @@ def identity_dirichlet(n: int = 128, seed: int = 1):
     return v, geo, rhs, bc, u
 
 
-def fourier_rhs(v, geo, fmap, seed, modes=16, kmax=8):
-    X, Y = G.positions(v, fmap)
+def fourier_modes(seed, modes=16, kmax=8):
+    """Amplitudes U(-1,1) and wave numbers U{1..kmax} of the seeded rhs."""
     rng = np.random.default_rng(seed)
     a = rng.uniform(-1, 1, modes)
     m = rng.integers(1, kmax + 1, modes)
     nn = rng.integers(1, kmax + 1, modes)
+    return a, m, nn
+
+
+def fourier_rhs(v, geo, fmap, seed, modes=16, kmax=8):
+    X, Y = G.positions(v, fmap)
+    a, m, nn = fourier_modes(seed, modes, kmax)
     f = np.zeros_like(X)
     for k in range(modes):
         f += a[k] * np.cos(math.pi * m[k] * X) * np.cos(math.pi * nn[k] * Y)
@@ -115,8 +121,18 @@ def batch_problem(i: int, seed: int = 4, nmin: int = 64, nmax: int = 1024):
     per cell in a wall layer of min(64, ny/4) cells, then sheared by U[0, 25]
     degrees; the 16-mode Fourier rhs of wavy_stretched; homogeneous Dirichlet
     on all sides."""
-    pseed = seed * 1_000_000 + i
-    rng = np.random.default_rng(pseed)
+    nx, ny, angle, ratio, layer_cells = batch_problem_params(i, seed, nmin, nmax)
+    v = Box.of_size(nx, ny)
+    fmap = G.map_skew_stretch(angle, ratio, layer_cells / ny, ny)
+    geo = G.mapped_geometry(v, fmap)
+    rhs = fourier_rhs(v, geo, fmap, seed * 1_000_000 + i)
+    bc = BdryData.uniform(v, [BCTYPE_DIRI] * 4)
+    return v, geo, rhs, bc
+
+
+def batch_problem_params(i: int, seed: int = 4, nmin: int = 64, nmax: int = 1024):
+    """The parameters batch_problem(i) draws: (nx, ny, angle, ratio, layer cells)."""
+    rng = np.random.default_rng(seed * 1_000_000 + i)
 
     def side():
         n = math.exp(rng.uniform(math.log(nmin), math.log(nmax)))
@@ -125,10 +141,19 @@ def batch_problem(i: int, seed: int = 4, nmin: int = 64, nmax: int = 1024):
     nx, ny = side(), side()
     ratio = float(rng.uniform(1.0, 1.08))
     angle = float(rng.uniform(0.0, 25.0))
-    layer_cells = min(64, ny // 4)
+    return nx, ny, angle, ratio, min(64, ny // 4)
+
+
+def batch_problem_device(i: int, seed: int = 4, nmin: int = 64, nmax: int = 1024):
+    """batch_problem(i) with the geometry and the rhs generated on the device
+    (mgp_map_geometry, mgp_map_fourier_rhs): equal to the host version to the
+    rounding of the map's transcendentals."""
+    from . import api as M
+    nx, ny, angle, ratio, layer_cells = batch_problem_params(i, seed, nmin, nmax)
     v = Box.of_size(nx, ny)
-    fmap = G.map_skew_stretch(angle, ratio, layer_cells / ny, ny)
-    geo = G.mapped_geometry(v, fmap)
-    rhs = fourier_rhs(v, geo, fmap, pseed)
+    params = (math.tan(math.radians(angle)), ratio, float(layer_cells), float(ny))
+    geo = M.map_geometry(v, M.MAP_SKEW_LAYER, params)
+    a, m, nn = fourier_modes(seed * 1_000_000 + i)
+    rhs = M.map_fourier_rhs(v, M.MAP_SKEW_LAYER, params, a, m, nn, geo.J)
     bc = BdryData.uniform(v, [BCTYPE_DIRI] * 4)
     return v, geo, rhs, bc

@@ -534,3 +534,50 @@ def test_relax_jacobi_bitexact(M, case, omega):
     O.relax_jacobi(pa, rhs, geo, bc, False, d, omega, -1.0, 5, False)
     M.relax_jacobi(pb, rhs, geo, bc, False, d, omega, -1.0, 5)
     assert same(pa.data, pb.data)
+
+
+# ---------------------------------------------------------------------------
+# Metric terms and rhs generated on the device from analytic maps
+# ---------------------------------------------------------------------------
+def _close(a, b, rel):
+    a, b = a.host(), b.host()
+    assert np.abs(a - b).max() <= rel * np.abs(b).max(), np.abs(a - b).max() / np.abs(b).max()
+
+
+@pytest.mark.parametrize("which", ["identity", "wavy", "skew"])
+def test_map_geometry_matches_host_generator(M, which):
+    """Same formulas as the host generator; only the rounding of the map's
+    transcendentals differs, amplified by the one-cell differences."""
+    import math
+    from mgpoisson2d_b200 import geometry as G
+    v = Box.of_size(96, 80)
+    if which == "identity":
+        kind, params, fmap = M.MAP_IDENTITY, (), G.map_identity()
+    elif which == "wavy":
+        beta = G.exp_stretch_beta(64.0)
+        kind, params, fmap = M.MAP_WAVY_EXP, (0.1, beta), G.map_wavy_exp(0.1, 64.0)
+    else:
+        kind, params = M.MAP_SKEW_LAYER, (math.tan(math.radians(20.0)), 1.05, 24.0, 80.0)
+        fmap = G.map_skew_stretch(20.0, 1.05, 24.0 / 80.0, 80)
+    gd = M.map_geometry(v, kind, params)
+    gh = G.mapped_geometry(v, fmap)
+    for a, b in zip((gd.J, gd.Jgup_xx, gd.Jgup_xy, gd.Jgup_yx, gd.Jgup_yy),
+                    (gh.J, gh.Jgup_xx, gh.Jgup_xy, gh.Jgup_yx, gh.Jgup_yy)):
+        if np.abs(b.host()).max() == 0:
+            assert np.abs(a.host()).max() < 1e-12
+        else:
+            _close(a, b, 1e-9)
+    gc = M.map_geometry(v, kind, params, device=False)   # host arrays: the same bits
+    for a, b in zip((gd.J, gd.Jgup_xx, gd.Jgup_yy), (gc.J, gc.Jgup_xx, gc.Jgup_yy)):
+        assert same(a.host(), b.host())
+
+
+def test_batch_problem_device_matches_host(M):
+    from mgpoisson2d_b200 import workloads as W
+    for i in (0, 3):
+        vh, gh, rh, bh = W.batch_problem(i, nmax=256)
+        vd, gd, rd, bd = W.batch_problem_device(i, nmax=256)
+        assert (vh.nx, vh.ny) == (vd.nx, vd.ny)
+        _close(gd.J, gh.J, 1e-9)
+        _close(gd.Jgup_xy, gh.Jgup_xy, 1e-8)
+        _close(rd, rh, 1e-9)
