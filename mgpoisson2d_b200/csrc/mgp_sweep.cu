@@ -256,9 +256,14 @@ __global__ void __launch_bounds__(kSweepThreads, Win<T>::kMinBlocks)
             tma_load_2d(sb + W::oYY * kS, &m.yy, t.pox, t.poy, bar);
         }
         colour_ranges(X0, X1, Y0, Y1, E, mi0, mi1, mj0, mj1, ci0, cj0, ccw, cn, cm);
-        if (!mbar_wait0(bar)) {   // never seen; leave the tile unwritten and report
-            if (status) atomicExch(status, 2);
-            mbar_wait0(bar);      // let copies still in flight land before the CTA exits
+        // one warp polls the barrier; the others sleep in the block barrier
+        // instead of taking issue slots from the CTAs that are computing
+        const bool landed = threadIdx.x >= 32 || mbar_wait0(bar);
+        if (!__syncthreads_and(landed)) {   // never seen; leave the tile unwritten and report
+            if (threadIdx.x == 0) {
+                if (status) atomicExch(status, 2);
+                mbar_wait0(bar);   // let copies still in flight land before the CTA exits
+            }
             return;
         }
     } else {
