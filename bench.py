@@ -436,7 +436,7 @@ def main():
     alg_bytes = SWEEP_WORDS * word * v.nx * v.ny
     peak, peak_kind = measured_peak()
     achieved = alg_bytes / sweep_s / 1e9
-    tr = committed_traffic()
+    tr = (committed_traffic() or {}).get("fp32" if word == 4 else "fp64")
     roofline = {"bound": "hbm", "kernel": f"k_sweep9 level 0 ({'FP32' if word == 4 else 'FP64'} fields, TMA staging)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "traffic": (tr or {}).get("bytes_per_sweep"),
