@@ -19,7 +19,10 @@ and rank 0 prints one JSON line.
 At N=1 the line also carries two legs on many independent problems (the
 batched workload: sides log-uniform in [64,1024]): "batched" (all problems as
 one mgp_batch on 16 streams vs one after another) and "served" (Poisson
-arrivals into an mgp_server with resident hierarchies; p50/p99 latency).
+arrivals into an mgp_server with resident hierarchies; p50/p99 latency), and
+"precision_study": mixed precision against FP64 and against the exact solution
+of a manufactured problem on the skewed, stretched grid at 512..4096, with the
+observed order of the discretisation error.
 
 --impl reference times the CPU restatement of the reference algorithm (the
 reference is Fortran and no Fortran compiler exists on these hosts) on all
@@ -68,6 +71,9 @@ def parse():
     p.add_argument("--no-batch", action="store_true", help="skip the batched and served legs")
     p.add_argument("--batch", type=int, default=512, help="problems in the batched leg")
     p.add_argument("--streams", type=int, default=16, help="concurrent solves in the batched and served legs")
+    p.add_argument("--no-study", action="store_true", help="skip the precision/convergence study leg")
+    p.add_argument("--study-sizes", default="512,1024,2048,4096",
+                   help="grid sides of the precision/convergence study")
     return p.parse_args()
 
 
@@ -356,6 +362,49 @@ def served_leg(M, args, probs, rhs_d, flags_list, nreq=240, seed=5):
 # --------------------------------------------------------------------------- #
 # GPU arm
 # --------------------------------------------------------------------------- #
+def precision_study(M, sizes):
+    """Mixed precision against FP64 and against the exact solution on the
+    skewed, boundary-layer-stretched manufactured problem (u = e^x cos 4 pi y,
+    Dirichlet data at the face centres, metric generated on the device):
+    V-cycles, solve time, relative max / L2 error against u, the mixed
+    solution's distance from the FP64 one, and the observed order
+    log2(e_n / e_2n) of the discretisation error."""
+    import torch
+    from mgpoisson2d_b200 import workloads as W
+    from mgpoisson2d_b200.types import BoxData
+    kry = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV
+    stream = torch.cuda.current_stream()
+    rows = []
+    for n in sizes:
+        v, geo, rhs, bc, u = W.skew_stretched_device(n)
+        row = {"n": n}
+        sol = {}
+        for name, fl in (("mixed", kry | M.FLAG_MIXED), ("fp64", kry)):
+            with M.Solver(v, geo, bc, M.KIND_MG, fl) as s:
+                phi = BoxData.device_zeros(v, 1, 1)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                r = s.vcycle(phi, rhs, bc, False, TOL, MAXITERS)
+                e1.record(stream)
+                e1.synchronize()
+            p = phi.data[1:-1, 1:-1]
+            sol[name] = p
+            row[name] = {"vcycles": r.iterations, "final_relres": r.final_relres, "ms": e0.elapsed_time(e1),
+                         "err_max": float((p - u).abs().max() / u.abs().max()),
+                         "err_l2": float(torch.linalg.norm(p - u) / torch.linalg.norm(u))}
+        d = sol["mixed"] - sol["fp64"]
+        row["mixed_vs_fp64"] = {"rel_l2": float(torch.linalg.norm(d) / torch.linalg.norm(sol["fp64"])),
+                                "rel_max": float(d.abs().max() / sol["fp64"].abs().max())}
+        rows.append(row)
+        del v, geo, rhs, bc, u, sol, d
+    for a, b in zip(rows, rows[1:]):
+        for name in ("mixed", "fp64"):
+            b[name]["order_l2"] = math.log2(a[name]["err_l2"] / b[name]["err_l2"]) / math.log2(b["n"] / a["n"])
+    torch.cuda.empty_cache()
+    return {"workload": "skew_stretched (30 deg skew, 1.05 boundary-layer stretch, u = e^x cos 4 pi y)",
+            "tol": TOL, "solver": "bicgstab(vcycle)", "rows": rows}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -532,6 +581,8 @@ def main():
         line["batched"] = batched
         line["served"] = served_leg(M, args, probs, rhs_b,
                                     [(n, f, batched[n]["batched_solves_per_s"]) for n, f in fls])
+    if rank == 0 and world == 1 and not args.no_study:
+        line["precision_study"] = precision_study(M, [int(x) for x in args.study_sizes.split(",") if x])
     if rank == 0 and world == 1 and not args.no_cpu:
         tvc, nvc = cpu_sample(args.n, args.cpu_vcycles)
         iters = solve_vcycles_estimate(args.n)

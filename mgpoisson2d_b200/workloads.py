@@ -157,3 +157,33 @@ def batch_problem_device(i: int, seed: int = 4, nmin: int = 64, nmax: int = 1024
     rhs = M.map_fourier_rhs(v, M.MAP_SKEW_LAYER, params, a, m, nn, geo.J)
     bc = BdryData.uniform(v, [BCTYPE_DIRI] * 4)
     return v, geo, rhs, bc
+
+
+def skew_stretched_device(n: int, angle: float = 30.0, ratio: float = 1.05, layer_cells: float = 96.0,
+                          n_ref: int = 4096):
+    """skew_stretched(n) with the metric terms generated on the device
+    (mgp_map_geometry) and the manufactured rhs and exact solution assembled
+    on the device from 1-D factors: x = xi + tan(angle) y(eta), so
+    u = e^x cos(4 pi y) = e^xi * (e^{tan(angle) y} cos(4 pi y)).  Returns
+    (valid, geo, rhs, bc, u_exact) with rhs and u_exact on the device."""
+    import torch
+    from . import api as M
+    v = Box.of_size(n, n)
+    t = math.tan(math.radians(angle))
+    params = (t, ratio, float(layer_cells), float(n_ref))
+    geo = M.map_geometry(v, M.MAP_SKEW_LAYER, params)
+    ys = G.layer_stretch(ratio, layer_cells / n_ref, n_ref)
+    xi = (np.arange(n) + 0.5) * v.dx
+    yc = ys((np.arange(n) + 0.5) * v.dy)
+    fx = np.exp(xi)
+    fy = np.exp(t * yc) * np.cos(4 * math.pi * yc)
+    dev = geo.J.data.device
+    # device arrays are (ny, nx) row-major views of the column-major fields
+    u = torch.outer(torch.from_numpy(fy).to(dev), torch.from_numpy(fx).to(dev))
+    rhs = BoxData.device_zeros(v)
+    rhs.data[:] = geo.J.data[1:-1, 1:-1] * ((1.0 - 16 * math.pi ** 2) * u)
+    ue = lambda x, y: np.exp(x) * np.cos(4 * math.pi * y)
+    y_side = yc
+    data = [ue(t * y_side, y_side), ue(1.0 + t * y_side, y_side), ue(xi, np.zeros(n)), ue(xi + t * 1.0, np.ones(n))]
+    bc = BdryData(v, [BCTYPE_DIRI] * 4, [BCMODE_NONUNIFORM] * 4, data)
+    return v, geo, rhs, bc, u
