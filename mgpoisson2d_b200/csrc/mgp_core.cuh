@@ -379,6 +379,17 @@ __device__ __forceinline__ int fastdiv(int k, unsigned long long m) {
     return (int)(((unsigned long long)(unsigned)k * m) >> 32);
 }
 
+// The same with a 24-bit magic number, which one 32-bit divide makes:
+// m = ceil(2^24 / d), and floor(k * m / 2^24) = floor(k / d) whenever
+// k * (d - 1) < 2^24 (so for k < 16384 with d <= 1024, and k < 65536 with
+// d <= 256; both ranges checked exhaustively on the host).
+__device__ __forceinline__ unsigned fastdiv24_magic(int d) {
+    return ((1u << 24) + (unsigned)d - 1u) / (unsigned)d;
+}
+__device__ __forceinline__ int fastdiv24(int k, unsigned m) {
+    return (int)(((unsigned long long)(unsigned)k * m) >> 24);
+}
+
 // Colour c of the 4-colour sweep: (i mod 2, j mod 2) = (0,0), (1,1), (1,0), (0,1).
 __device__ __forceinline__ int colour_ci(int c) { return (c == 1 || c == 2) ? 1 : 0; }
 __device__ __forceinline__ int colour_cj(int c) { return (c == 1 || c == 3) ? 1 : 0; }

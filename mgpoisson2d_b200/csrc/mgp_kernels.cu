@@ -922,15 +922,20 @@ __device__ void b_sweep9(const DF& phi_, const DF& rhs_, const DF& invd_, const 
     const int mi0 = pr.xl ? 0 : 1, mi1 = pr.xh ? nx : nx - 1;
     const int mj0 = pr.yl ? 0 : 1, mj1 = pr.yh ? ny : ny - 1;
     // interior colour ranges and their divide-free index maps, set up before the fill
+    // (the multiply is exact while cnt * (cw - 1) < 2^24, which every level
+    // of up to 1024 cells meets; a larger level -- a depth capped by the
+    // caller -- divides)
     int ci0[4], cj0[4], ccw[4], cnt[4];
-    unsigned long long cm[4];
+    unsigned cm[4];
+    bool fast[4];
     for (int c = 0; c < 4; ++c) {
         ci0[c] = mi0 + ((mi0 & 1) != colour_ci(c));
         cj0[c] = mj0 + ((mj0 & 1) != colour_cj(c));
         ccw[c] = (mi1 > ci0[c]) ? (mi1 - ci0[c] + 1) / 2 : 0;
         const int ch = (mj1 > cj0[c]) ? (mj1 - cj0[c] + 1) / 2 : 0;
         cnt[c] = ccw[c] * ch;
-        cm[c] = fastdiv_magic(ccw[c] > 0 ? ccw[c] : 1);
+        cm[c] = fastdiv24_magic(ccw[c] > 0 ? ccw[c] : 1);
+        fast[c] = (long)cnt[c] * (ccw[c] > 0 ? ccw[c] - 1 : 0) < (1L << 24);
     }
     const int ng = 2 * (nx + 2) + 2 * ny;
     BLOOP(k, ng) {
@@ -945,7 +950,7 @@ __device__ void b_sweep9(const DF& phi_, const DF& rhs_, const DF& invd_, const 
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
         BLOOP(k, cnt[c]) {
-            const int kj = fastdiv(k, cm[c]);
+            const int kj = fast[c] ? fastdiv24(k, cm[c]) : k / ccw[c];
             gs9r(phi, rhs, invd, g, b, homog, ci0[c] + 2 * (k - kj * ccw[c]), cj0[c] + 2 * kj, RMID, RMID, omega);
         }
         __syncthreads();

@@ -87,6 +87,7 @@ struct SweepMaps {
 struct SweepTma {
     SweepMaps ma, mb;
     const void *pa = nullptr, *pb = nullptr, *rhs = nullptr, *invd = nullptr, *xx = nullptr;
+    int tx = 32;   // tile width the descriptors' boxes are cut for
     bool ok = false;
 };
 // Builds the descriptors when the arrays allow it (16-byte aligned bases and

@@ -5,7 +5,9 @@
 // buffers), so no CTA ever reads a value another CTA has already replaced.
 // Each CTA owns one tile of a balanced partition of the grid (tiles at most
 // TX x TY and, when there is more than one, at least TX/2 x TY/2, so every
-// corner's neighbourhood lies inside the tile that owns the corner).
+// corner's neighbourhood lies inside the tile that owns the corner: with
+// g = ceil(n / TX) tiles along a side, n / g lies in [TX/2, TX] for n > TX
+// and equals TX only when g divides n).
 //
 // A CTA first stages everything its tile's update reads -- phi with its
 // halo, rhs, the inverse diagonal and the four metric face arrays, each on
@@ -28,8 +30,12 @@
 // window of each field, completing on one mbarrier; elsewhere (caller arrays
 // of any pitch and alignment) the threads stage with cp.async.
 //
-// The kernel is compiled for FP64 fields (the solver's arithmetic) and for
-// FP32 fields (the grid levels of the mixed-precision V-cycle).
+// The kernel is compiled for FP64 fields (the solver's arithmetic; the
+// update is gs9's, bit for bit) and for FP32 fields (the grid levels of the
+// mixed-precision V-cycle), where each thread updates two interior cells at
+// once in packed FP32x2 arithmetic with fused multiply-adds (gs9_pair).  The
+// result depends on neither the tiling nor the launch: the same inputs give
+// the same bits.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -41,32 +47,43 @@ namespace mgp {
 
 namespace {
 
-constexpr int kTX = 32, kTY = 32;
+constexpr int kTY = 32;
 constexpr int kH = 6;   // phi halo: 4 for the colour passes + E = 2 for the boundary pass
 constexpr int kSweepThreads = 512;
-constexpr long kWaitLimit = 1L << 22;   // mbarrier polls before a CTA gives up (far above any real wait)
+// A CTA gives up on its tile loads after kWaitLimit polls or kWaitNs, far
+// above any real wait (microseconds); each poll sleeps up to kSuspendNs.
+constexpr long kWaitLimit = 1L << 22;
+constexpr unsigned long long kWaitNs = 200000000ull;
+constexpr unsigned kSuspendNs = 20000;
 
-// Shared-memory window of one field type.  All seven staged arrays share one
+// Tile and shared-memory window of one field type and tile width: 32 x 32
+// tiles (FP64: two CTAs of 114 KB per SM; FP32: three of 59 KB) and, for
+// FP32 levels large enough to fill the GPU, 64 x 32 tiles (two CTAs of
+// 99 KB), which spread each thread's fixed work over more cells and
+// recompute a smaller share of halo.  All seven staged arrays share one
 // window -- origin (pox, poy) with pox the column at or below tile corner - kH
 // that is a multiple of kAlign (a 16-byte boundary, as TMA needs), pitch PW --
 // so one offset addresses a cell in every array: phi and the cell operands
 // at o, the west/east x-faces at o and o + 1, the south/north y-faces at o
 // and o + PW.  The operands are needed on tile + (3 + E) <= tile + 5 cells
 // (faces one further), inside the phi footprint tile + kH.
-template <class T>
+template <class T, int TX_>
 struct Win {
+    static constexpr int TX = TX_;
     static constexpr int kAlign = 16 / (int)sizeof(T);   // 2 doubles, 4 floats
-    static constexpr int PW = (kTX + 2 * kH + (kAlign - 1) + kAlign - 1) / kAlign * kAlign;   // 46 / 48
+    static constexpr int PW = (TX + 2 * kH + (kAlign - 1) + kAlign - 1) / kAlign * kAlign;   // 46 / 48 / 80
     static constexpr int PH = kTY + 2 * kH;                                                        // 44
     static constexpr int kA = (PW * PH * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);     // 128-B aligned
     static constexpr int oF = kA, oD = 2 * kA, oXX = 3 * kA, oXY = 4 * kA, oYX = 5 * kA, oYY = 6 * kA;
     static constexpr int oBarBytes = 7 * kA * (int)sizeof(T);   // the TMA mbarrier (8 bytes)
     static constexpr size_t kSmemBytes = (size_t)oBarBytes + 16;
     static constexpr unsigned kBoxBytes = PW * PH * sizeof(T);
-    static constexpr int kMinBlocks = sizeof(T) == 8 ? 2 : 3;   // CTAs per SM the window allows
+    static constexpr int kMinBlocks = (int)((228 * 1024) / (kSmemBytes + 1024));   // CTAs per SM the window allows
 };
 
-static_assert(Win<double>::PW == 46 && Win<float>::PW == 48, "window pitch");
+static_assert(Win<double, 32>::PW == 46 && Win<float, 32>::PW == 48 && Win<float, 64>::PW == 80, "window pitch");
+static_assert(Win<double, 32>::kMinBlocks == 2 && Win<float, 32>::kMinBlocks == 3 && Win<float, 64>::kMinBlocks == 2,
+              "CTAs per SM");
 
 template <class T>
 struct SLoadT {
@@ -77,13 +94,13 @@ struct SLoadT {
 
 // phi at the start of the sweep: the staged copy where it holds (i,j), else
 // global memory (the far side of a periodic domain).
-template <class T>
+template <class T, int PW>
 struct PinLoad {
     const T* s;
     int pox, poy, pi0, pi1, pj0, pj1;
     DFT<T> pin;
     __device__ __forceinline__ T operator()(int i, int j) const {
-        if (i >= pi0 && i < pi1 && j >= pj0 && j < pj1) return s[(j - poy) * Win<T>::PW + (i - pox)];
+        if (i >= pi0 && i < pi1 && j >= pj0 && j < pj1) return s[(j - poy) * PW + (i - pox)];
         return AT(pin, i, j);
     }
 };
@@ -135,19 +152,35 @@ __device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
 __device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
 }
+// Test phase `parity`; a thread whose phase is not complete sleeps in the
+// instruction until it completes or kSuspendNs pass.
 __device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
     unsigned ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
-        : "r"(bar), "r"(parity)
+        : "r"(bar), "r"(parity), "r"(kSuspendNs)
         : "memory");
     return ok != 0;
 }
-// Bounded wait for phase 0 of the barrier; false if it did not complete.
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait for phase 0 of the barrier (kWaitLimit polls and kWaitNs at
+// most); false if it did not complete.  Between polls the warp sleeps, 32 ns
+// at first and at most 256 ns, so a CTA waiting for its tile takes few issue
+// slots from the CTAs computing beside it.
 __device__ __forceinline__ bool mbar_wait0(unsigned bar) {
-    for (long k = 0; k < kWaitLimit; ++k)
+    const unsigned long long t0 = global_ns();
+    unsigned nap = 32;
+    for (long k = 0; k < kWaitLimit; ++k) {
         if (mbar_try_wait(bar, 0)) return true;
+        if (global_ns() - t0 > kWaitNs) break;
+        __nanosleep(nap);
+        nap = nap < 256 ? 2 * nap : nap;
+    }
     return false;
 }
 // One 2-D tile (the map's box) of `map` at element coordinates (x, y); x is a
@@ -160,23 +193,28 @@ __device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map
 }
 
 // Interior colour c on the tile grown by (3 - c + E): first cell (ci0, cj0),
-// cw cells per row, n cells, and the magic number for k / cw.
+// cw cells per row, n cells, and the magic number for k / cw (n <= 37 x 21
+// and cw <= 37, well inside the exact range of the 24-bit multiply).  Lane
+// c of each group of four computes colour c; every lane then reads all four
+// by shuffle, so a warp spends one divide, not four per thread.
 __device__ __forceinline__ void colour_ranges(int X0, int X1, int Y0, int Y1, int E, int mi0, int mi1, int mj0,
-                                              int mj1, int* ci0, int* cj0, int* ccw, int* cn,
-                                              unsigned long long* cm) {
+                                              int mj1, int* ci0, int* cj0, int* ccw, int* cn, unsigned* cm) {
+    const int c = threadIdx.x & 3;
+    const int grow = 3 - c + E;
+    int i0 = max(X0 - grow, mi0), i1 = min(X1 + grow, mi1);
+    int j0 = max(Y0 - grow, mj0), j1 = min(Y1 + grow, mj1);
+    i0 += (i0 & 1) != colour_ci(c);
+    j0 += (j0 & 1) != colour_cj(c);
+    const int cw = (i1 - i0 + 1) / 2, ch = (j1 - j0 + 1) / 2;
+    const int n = (cw > 0 && ch > 0) ? cw * ch : 0;
+    const unsigned m = fastdiv24_magic(cw > 0 ? cw : 1);
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        const int grow = 3 - c + E;
-        int i0 = max(X0 - grow, mi0), i1 = min(X1 + grow, mi1);
-        int j0 = max(Y0 - grow, mj0), j1 = min(Y1 + grow, mj1);
-        i0 += (i0 & 1) != colour_ci(c);
-        j0 += (j0 & 1) != colour_cj(c);
-        const int cw = (i1 - i0 + 1) / 2, ch = (j1 - j0 + 1) / 2;
-        ci0[c] = i0;
-        cj0[c] = j0;
-        ccw[c] = cw;
-        cn[c] = (cw > 0 && ch > 0) ? cw * ch : 0;
-        cm[c] = fastdiv_magic(cw > 0 ? cw : 1);
+    for (int k = 0; k < 4; ++k) {
+        ci0[k] = __shfl_sync(0xffffffffu, i0, k);
+        cj0[k] = __shfl_sync(0xffffffffu, j0, k);
+        ccw[k] = __shfl_sync(0xffffffffu, cw, k);
+        cn[k] = __shfl_sync(0xffffffffu, n, k);
+        cm[k] = __shfl_sync(0xffffffffu, m, k);
     }
 }
 
@@ -187,10 +225,9 @@ struct Tile {
 };
 
 // One Gauss-Seidel update of (i,j) from shared memory (same operations as gs9).
-template <class T>
+template <class W, class T>
 __device__ __forceinline__ void gs9_tile(const Tile<T>& t, T idx, T idy, const BCd& b, int homog, int i, int j, int xr,
-                                         int yr, double omega) {
-    using W = Win<T>;
+                                         int yr, T om, T om1) {
     T* c = t.s + (j - t.poy) * W::PW + (i - t.pox);
     St9T<T> s;
     gather9(SLoadT<T>{c, W::PW}, xr, yr, s);
@@ -202,22 +239,66 @@ __device__ __forceinline__ void gs9_tile(const Tile<T>& t, T idx, T idy, const B
     const T lphi = lap9f(s, fc, idx, idy, i, j, xr, yr, b, homog);
     const T p = c[0];
     const T newphi = p + (c[W::oF] - lphi) * c[W::oD];
-    c[0] = T(omega) * newphi + T(1.0 - omega) * p;
+    c[0] = om * newphi + om1 * p;
 }
 
-template <bool kTma, class T>
-__global__ void __launch_bounds__(kSweepThreads, Win<T>::kMinBlocks)
-    k_sweep9(const __grid_constant__ SweepMaps m, DFT<T> pin, DFT<T> pout, DFT<T> rhs, DFT<T> invd, GeoT<T> g, BCd b,
-             int homog, int nx, int ny, double omega, int* status) {
-    using W = Win<T>;
+// Two interior updates at once in packed FP32 arithmetic (add / mul / fma on
+// a pair of floats, one instruction for both lanes): cells a and b of the
+// same colour, each lane the operations of gs9_tile on an interior cell in
+// the same order, except that the seven places where a product is added to
+// another term -- each flux's two terms, the operator's x and y parts, the
+// update p + (f - Lp) d and the relaxation om new + om1 p -- are fused
+// multiply-adds, rounded once.  (The code generator fuses packed multiplies
+// into adds on its own; writing the fused form makes the arithmetic defined
+// by the source.)  Differences are a + b * (-1): an exact product and one
+// rounding, the same as a - b.  Where the colour has an odd number of cells
+// the last thread's b is a itself and only a is written back.
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+
+template <class W>
+__device__ __forceinline__ void gs9_pair(float* a, float* b, bool write_b, float2 idx, float2 idy, float2 om,
+                                         float2 om1) {
+    constexpr int P = W::PW;
+    const auto L = [a, b](int o) { return make_float2(a[o], b[o]); };
+    const float2 p = L(0), pe = L(1), pw = L(-1), pn = L(P), ps = L(-P);
+    const float2 ene = L(1 + P), enw = L(-1 + P), ese = L(1 - P), esw = L(-1 - P);
+    const float2 q = make_float2(0.25f, 0.25f);
+    // interior cell: ee = pe, ew = pw, en = pn, es = ps (lap9f's four fluxes)
+    const float2 xfe = f2fma(f2mul(L(W::oXX + 1), f2sub(pe, p)), idx,
+                             f2mul(f2mul(f2mul(L(W::oXY + 1), q), f2sub(f2add(f2sub(ene, ese), pn), ps)), idy));
+    const float2 xfw = f2fma(f2mul(L(W::oXX), f2sub(p, pw)), idx,
+                             f2mul(f2mul(f2mul(L(W::oXY), q), f2sub(f2add(f2sub(pn, ps), enw), esw)), idy));
+    const float2 yfn = f2fma(f2mul(L(W::oYY + P), f2sub(pn, p)), idy,
+                             f2mul(f2mul(f2mul(L(W::oYX + P), q), f2sub(f2add(f2sub(ene, enw), pe), pw)), idx));
+    const float2 yfs = f2fma(f2mul(L(W::oYY), f2sub(p, ps)), idy,
+                             f2mul(f2mul(f2mul(L(W::oYX), q), f2sub(f2add(f2sub(pe, pw), ese), esw)), idx));
+    const float2 lphi = f2fma(f2sub(xfe, xfw), idx, f2mul(f2sub(yfn, yfs), idy));
+    const float2 newphi = f2fma(f2sub(L(W::oF), lphi), L(W::oD), p);
+    const float2 r = f2fma(om, newphi, f2mul(om1, p));
+    a[0] = r.x;
+    if (write_b) b[0] = r.y;
+}
+
+template <bool kTma, class T, int TX>
+__global__ void __launch_bounds__(kSweepThreads, (Win<T, TX>::kMinBlocks))
+    k_sweep9(const __grid_constant__ SweepMaps m, DFT<T> pin, DFT<T> pout, DFT<T> rhs, DFT<T> invd, GeoT<T> g,
+             const __grid_constant__ BCd b, int homog, int nx, int ny, int4 part, double omega, int* status) {
+    using W = Win<T, TX>;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     T* smem = reinterpret_cast<T*>(smem_raw);
-    const int X0 = (int)((long)blockIdx.x * nx / gridDim.x), X1 = (int)((long)(blockIdx.x + 1) * nx / gridDim.x);
-    const int Y0 = (int)((long)blockIdx.y * ny / gridDim.y), Y1 = (int)((long)(blockIdx.y + 1) * ny / gridDim.y);
+    // tile bounds: part = (nx / gx, nx % gx, ny / gy, ny % gy); the first
+    // nx % gx columns of tiles are one cell wider
+    const int bx = blockIdx.x, by = blockIdx.y;
+    const int X0 = bx * part.x + min(bx, part.y), X1 = X0 + part.x + (bx < part.y ? 1 : 0);
+    const int Y0 = by * part.z + min(by, part.w), Y1 = Y0 + part.z + (by < part.w ? 1 : 0);
     const Per pr = periodic_of(b);
     const bool edge_tile = (!pr.xl && X0 == 0) || (!pr.xh && X1 >= nx) || (!pr.yl && Y0 == 0) || (!pr.yh && Y1 >= ny);
     const int E = edge_tile ? 2 : 0;
     const T idx = T(g.idx), idy = T(g.idy);
+    const T om = T(omega), om1 = T(1.0 - omega);
 
     Tile<T> t;
     t.s = smem;
@@ -229,7 +310,7 @@ __global__ void __launch_bounds__(kSweepThreads, Win<T>::kMinBlocks)
     const int mi0 = pr.xl ? 0 : 1, mi1 = pr.xh ? nx : nx - 1;
     const int mj0 = pr.yl ? 0 : 1, mj1 = pr.yh ? ny : ny - 1;
     int ci0[4], cj0[4], ccw[4], cn[4];
-    unsigned long long cm[4];
+    unsigned cm[4];
 
     // 1. stage phi on tile + (4 + E) and the operands on tile + (3 + E)
     const int hp = 4 + E, hc = 3 + E;
@@ -281,7 +362,7 @@ __global__ void __launch_bounds__(kSweepThreads, Win<T>::kMinBlocks)
     // 2. sweep-start ghost fill on the staged ghost cells (the ghost rows and
     //    columns of tiles on the domain boundary only)
     if (pi0 < 0 || pi1 > nx || pj0 < 0 || pj1 > ny) {
-        const PinLoad<T> P{smem, t.pox, t.poy, pi0, pi1, pj0, pj1, pin};
+        const PinLoad<T, W::PW> P{smem, t.pox, t.poy, pi0, pi1, pj0, pj1, pin};
         const int lw = pi1 - pi0, lh = pj1 - pj0;
         for (int k = threadIdx.x; k < 2 * (lw + lh); k += blockDim.x) {
             int i, j;
@@ -296,16 +377,37 @@ __global__ void __launch_bounds__(kSweepThreads, Win<T>::kMinBlocks)
     __syncthreads();
 
     // 3. interior colour passes on shrinking regions.  Interior cells are
-    //    i in [mi0, mi1), j in [mj0, mj1); one thread per cell of the colour
-    //    (a pass has at most 21 x 21 of them).
+    //    i in [mi0, mi1), j in [mj0, mj1) (a pass has at most 21 x 21 of them
+    //    on a 32 x 32 tile, 37 x 21 on a 64 x 32 one).  FP64: a thread per
+    //    cell.  FP32: a thread per two cells, k and k + ceil(n/2) of the
+    //    colour's list, so a warp's lanes still read consecutive cells of the
+    //    colour (two-way bank conflicts, as one cell per thread).
+    if constexpr (sizeof(T) == 4) {
+        const float2 idx2 = make_float2(idx, idx), idy2 = make_float2(idy, idy);
+        const float2 om2 = make_float2(om, om), om12 = make_float2(om1, om1);
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        for (int k = threadIdx.x; k < cn[c]; k += blockDim.x) {
-            const int kj = fastdiv(k, cm[c]);
-            const int i = ci0[c] + 2 * (k - kj * ccw[c]), j = cj0[c] + 2 * kj;
-            gs9_tile(t, idx, idy, b, homog, i, j, RMID, RMID, omega);
+        for (int c = 0; c < 4; ++c) {
+            const int nh = (cn[c] + 1) >> 1;
+            for (int k = threadIdx.x; k < nh; k += blockDim.x) {
+                const int kb = (k + nh < cn[c]) ? k + nh : k;
+                const int ja = fastdiv24(k, cm[c]), jb = fastdiv24(kb, cm[c]);
+                const int ia = ci0[c] + 2 * (k - ja * ccw[c]), ib = ci0[c] + 2 * (kb - jb * ccw[c]);
+                T* ca = t.s + (cj0[c] + 2 * ja - t.poy) * W::PW + (ia - t.pox);
+                T* cb = t.s + (cj0[c] + 2 * jb - t.poy) * W::PW + (ib - t.pox);
+                gs9_pair<W>(ca, cb, kb != k, idx2, idy2, om2, om12);
+            }
+            __syncthreads();
         }
-        __syncthreads();
+    } else {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            for (int k = threadIdx.x; k < cn[c]; k += blockDim.x) {
+                const int kj = fastdiv24(k, cm[c]);
+                const int i = ci0[c] + 2 * (k - kj * ccw[c]), j = cj0[c] + 2 * kj;
+                gs9_tile<W>(t, idx, idy, b, homog, i, j, RMID, RMID, om, om1);
+            }
+            __syncthreads();
+        }
     }
 
     // 4. boundary pass (edge tiles only; uniform per CTA): per colour, the
@@ -325,10 +427,10 @@ __global__ void __launch_bounds__(kSweepThreads, Win<T>::kMinBlocks)
             const int n2 = n1 + ((sxl && ci == 0) ? nj : 0);
             const int n3 = n2 + ((sxh && ((nx - 1) & 1) == ci) ? nj : 0);
             for (int k = threadIdx.x; k < n3; k += blockDim.x) {
-                if (k < n0) gs9_tile(t, idx, idy, b, homog, ia + 2 * k, 0, RMID, RLO, omega);
-                else if (k < n1) gs9_tile(t, idx, idy, b, homog, ia + 2 * (k - n0), ny - 1, RMID, RHI, omega);
-                else if (k < n2) gs9_tile(t, idx, idy, b, homog, 0, ja + 2 * (k - n1), RLO, RMID, omega);
-                else gs9_tile(t, idx, idy, b, homog, nx - 1, ja + 2 * (k - n2), RHI, RMID, omega);
+                if (k < n0) gs9_tile<W>(t, idx, idy, b, homog, ia + 2 * k, 0, RMID, RLO, om, om1);
+                else if (k < n1) gs9_tile<W>(t, idx, idy, b, homog, ia + 2 * (k - n0), ny - 1, RMID, RHI, om, om1);
+                else if (k < n2) gs9_tile<W>(t, idx, idy, b, homog, 0, ja + 2 * (k - n1), RLO, RMID, om, om1);
+                else gs9_tile<W>(t, idx, idy, b, homog, nx - 1, ja + 2 * (k - n2), RHI, RMID, om, om1);
             }
             __syncthreads();
         }
@@ -337,7 +439,7 @@ __global__ void __launch_bounds__(kSweepThreads, Win<T>::kMinBlocks)
                 const int i = (c & 1) ? nx - 1 : 0, j = (c & 2) ? ny - 1 : 0;
                 if (i < X0 || i >= X1 || j < Y0 || j >= Y1) continue;
                 const int xr = region(i, nx, pr.xl, pr.xh), yr = region(j, ny, pr.yl, pr.yh);
-                if (xr != RMID && yr != RMID) gs9_tile(t, idx, idy, b, homog, i, j, xr, yr, omega);
+                if (xr != RMID && yr != RMID) gs9_tile<W>(t, idx, idy, b, homog, i, j, xr, yr, om, om1);
             }
         }
         __syncthreads();
@@ -388,7 +490,7 @@ constexpr CUtensorMapDataType map_type() {
 }
 
 // A 2-D map of `width` x `height` elements at `base`, row pitch ld, box PW x PH.
-template <class T>
+template <class W, class T>
 bool encode(CUtensorMap* m, const T* base, long width, long height, int ld) {
     const PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
     if (!fn || ((uintptr_t)base & 15) || (((long)ld * (long)sizeof(T)) & 15) || width > ld || width <= 0 ||
@@ -396,47 +498,93 @@ bool encode(CUtensorMap* m, const T* base, long width, long height, int ld) {
         return false;
     const cuuint64_t dims[2] = {(cuuint64_t)width, (cuuint64_t)height};
     const cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(T)};
-    const cuuint32_t box[2] = {(cuuint32_t)Win<T>::PW, (cuuint32_t)Win<T>::PH};
+    const cuuint32_t box[2] = {(cuuint32_t)W::PW, (cuuint32_t)W::PH};
     const cuuint32_t es[2] = {1, 1};
     return fn(m, map_type<T>(), 2, const_cast<T*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <class T>
+template <class W, class T>
 bool prepare_maps(SweepMaps* m, const DFT<T>& e, const DFT<T>& rhs, const DFT<T>& invd, const GeoT<T>& g, int nx,
                   int ny) {
     // phi from the 16-byte-aligned column kAlign left of column 0 (so the
     // ghost column -1 is inside), and row -1; the ghost column nx must lie
     // inside the pitch
-    m->pcb = -Win<T>::kAlign;
+    m->pcb = -W::kAlign;
     m->prb = -1;
-    if (e.ld < nx + 1 + Win<T>::kAlign) return false;
-    return encode(&m->pin, &AT(e, m->pcb, -1), e.ld, ny + 2, e.ld) && encode(&m->rhs, rhs.p, nx, ny, rhs.ld) &&
-           encode(&m->invd, invd.p, nx, ny, invd.ld) && encode(&m->xx, g.xx.p, nx + 1, ny, g.xx.ld) &&
-           encode(&m->xy, g.xy.p, nx + 1, ny, g.xy.ld) && encode(&m->yx, g.yx.p, nx, ny + 1, g.yx.ld) &&
-           encode(&m->yy, g.yy.p, nx, ny + 1, g.yy.ld);
+    if (e.ld < nx + 1 + W::kAlign) return false;
+    return encode<W>(&m->pin, &AT(e, m->pcb, -1), e.ld, ny + 2, e.ld) && encode<W>(&m->rhs, rhs.p, nx, ny, rhs.ld) &&
+           encode<W>(&m->invd, invd.p, nx, ny, invd.ld) && encode<W>(&m->xx, g.xx.p, nx + 1, ny, g.xx.ld) &&
+           encode<W>(&m->xy, g.xy.p, nx + 1, ny, g.xy.ld) && encode<W>(&m->yx, g.yx.p, nx, ny + 1, g.yx.ld) &&
+           encode<W>(&m->yy, g.yy.p, nx, ny + 1, g.yy.ld);
 }
 
-template <class T>
+template <class T, int TX>
 cudaError_t set_attr() {
-    cudaError_t e = cudaFuncSetAttribute(k_sweep9<true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)Win<T>::kSmemBytes);
+    cudaError_t e = cudaFuncSetAttribute(k_sweep9<true, T, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)Win<T, TX>::kSmemBytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_sweep9<false, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)Win<T>::kSmemBytes);
+        e = cudaFuncSetAttribute(k_sweep9<false, T, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)Win<T, TX>::kSmemBytes);
     return e;
+}
+
+int sm_count() {
+    static std::mutex mu;
+    static int n[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!n[dev] && cudaDeviceGetAttribute(&n[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        n[dev] = 148;
+    }
+    return n[dev];
+}
+
+// Tile width for a level: FP32 levels take 64-wide tiles when those alone
+// fill every SM with as many CTAs as fit; smaller levels, whose sweep lasts
+// about one CTA's latency, keep the narrower tiles and their larger grid.
+template <class T>
+int tile_width(int nx, int ny) {
+    if (sizeof(T) == 8) return 32;
+    const long wide = (long)((nx + 63) / 64) * ((ny + kTY - 1) / kTY);
+    return wide >= (long)Win<float, 64>::kMinBlocks * sm_count() ? 64 : 32;
 }
 
 template <class T>
 void tma_prepare(SweepTma* t, const DFT<T>& ea, const DFT<T>& eb, const DFT<T>& rhs, const DFT<T>& invd,
                  const GeoT<T>& g, int nx, int ny) {
-    t->ok = prepare_maps(&t->ma, ea, rhs, invd, g, nx, ny) && prepare_maps(&t->mb, eb, rhs, invd, g, nx, ny);
+    t->tx = tile_width<T>(nx, ny);
+    if (t->tx == 64)
+        t->ok = prepare_maps<Win<T, 64>>(&t->ma, ea, rhs, invd, g, nx, ny) &&
+                prepare_maps<Win<T, 64>>(&t->mb, eb, rhs, invd, g, nx, ny);
+    else
+        t->ok = prepare_maps<Win<T, 32>>(&t->ma, ea, rhs, invd, g, nx, ny) &&
+                prepare_maps<Win<T, 32>>(&t->mb, eb, rhs, invd, g, nx, ny);
     t->pa = ea.p;
     t->pb = eb.p;
     t->rhs = rhs.p;
     t->invd = invd.p;
     t->xx = g.xx.p;
+}
+
+template <class T, int TX>
+void launch_tiles(const SweepMaps* m, const DFT<T>& pin, const DFT<T>& pout, const DFT<T>& rhs, const DFT<T>& invd,
+                  const GeoT<T>& g, const BCd& b, int homog, int nx, int ny, double omega, int* status,
+                  cudaStream_t st) {
+    using W = Win<T, TX>;
+    dim3 grd((nx + TX - 1) / TX, (ny + kTY - 1) / kTY);
+    const int4 part = make_int4(nx / (int)grd.x, nx % (int)grd.x, ny / (int)grd.y, ny % (int)grd.y);
+    if (m) {
+        k_sweep9<true, T, TX><<<grd, kSweepThreads, W::kSmemBytes, st>>>(*m, pin, pout, rhs, invd, g, b, homog, nx,
+                                                                         ny, part, omega, status);
+    } else {
+        static const SweepMaps none{};
+        k_sweep9<false, T, TX><<<grd, kSweepThreads, W::kSmemBytes, st>>>(none, pin, pout, rhs, invd, g, b, homog,
+                                                                          nx, ny, part, omega, status);
+    }
 }
 
 template <class T>
@@ -449,16 +597,13 @@ cudaError_t sweep_impl(const DFT<T>& pin, const DFT<T>& pout, const DFT<T>& rhs,
     if (tma && tma->ok && (const void*)rhs.p == tma->rhs && (const void*)invd.p == tma->invd &&
         (const void*)g.xx.p == tma->xx)
         m = ((const void*)pin.p == tma->pa) ? &tma->ma : ((const void*)pin.p == tma->pb) ? &tma->mb : nullptr;
-    dim3 grd((nx + kTX - 1) / kTX, (ny + kTY - 1) / kTY);
-    const size_t smem = Win<T>::kSmemBytes;
-    if (m) {
-        k_sweep9<true, T><<<grd, kSweepThreads, smem, st>>>(*m, pin, pout, rhs, invd, g, b, homog, nx, ny, omega,
-                                                            status);
-    } else {
-        static const SweepMaps none{};
-        k_sweep9<false, T><<<grd, kSweepThreads, smem, st>>>(none, pin, pout, rhs, invd, g, b, homog, nx, ny, omega,
-                                                             status);
+    const int tx = m ? tma->tx : tile_width<T>(nx, ny);
+    bool wide = false;
+    if constexpr (sizeof(T) == 4) {
+        wide = tx == 64;
+        if (wide) launch_tiles<T, 64>(m, pin, pout, rhs, invd, g, b, homog, nx, ny, omega, status, st);
     }
+    if (!wide) launch_tiles<T, 32>(m, pin, pout, rhs, invd, g, b, homog, nx, ny, omega, status, st);
     count_launch();
     return cudaGetLastError();
 }
@@ -474,8 +619,9 @@ cudaError_t sweep_kernels_init() {
     if (e != cudaSuccess) return e;
     std::lock_guard<std::mutex> lock(mu);
     if (dev < 64 && (done >> dev) & 1ull) return cudaSuccess;
-    e = set_attr<double>();
-    if (e == cudaSuccess) e = set_attr<float>();
+    e = set_attr<double, 32>();
+    if (e == cudaSuccess) e = set_attr<float, 32>();
+    if (e == cudaSuccess) e = set_attr<float, 64>();
     if (e == cudaSuccess && dev < 64) done |= 1ull << dev;
     return e;
 }

@@ -1,9 +1,10 @@
 """A short, fixed run of the benchmark workload for profilers:
 
     python -m mgpoisson2d_b200.profile [--n 1024] [--vcycles 2] [--warmup 1] [--mixed] [--krylov]
+                                       [--workload wavy|skew]
 
-Builds the resident solver for the 1024x1024 stretched mapped grid (the bench
-workload), runs `warmup` solves capped at `vcycles` V-cycles, then one more,
+Builds the resident solver for the stretched mapped grid (wavy: the bench
+workload; skew: the skewed boundary-layer manufactured problem), runs `warmup` solves capped at `vcycles` V-cycles, then one more,
 and prints the device time per V-cycle.  Under ncu, the kernels of the last
 solve follow those of the warm-up solves in launch order.
 """
@@ -21,6 +22,8 @@ def main():
     p.add_argument("--dd", action="store_true", help="deferred-correction driver")
     p.add_argument("--mixed", action="store_true", help="FP32 grid levels (MGP_FLAG_MIXED)")
     p.add_argument("--krylov", action="store_true", help="BiCGStab acceleration (MGP_FLAG_KRYLOV)")
+    p.add_argument("--workload", default="wavy", choices=["wavy", "skew"])
+    p.add_argument("--time-smoother", action="store_true", help="also report the finest level's time per sweep")
     a = p.parse_args()
 
     import torch
@@ -30,15 +33,21 @@ def main():
     from mgpoisson2d_b200.types import BoxData
 
     torch.cuda.set_device(0)
-    v, geo, rhs, bc, _ = W.wavy_stretched(a.n)
+    if a.workload == "wavy":
+        v, geo, rhs, bc, _ = W.wavy_stretched(a.n)
+        homog = True
+    else:
+        v, geo, rhs, bc, _ = W.skew_stretched_device(a.n)
+        homog = False
     kind = M.KIND_DD if a.dd else M.KIND_MG
     flags = M.FLAG_DIRICHLET_COUPLED_DIAG | (M.FLAG_MIXED if a.mixed else 0) | (M.FLAG_KRYLOV if a.krylov else 0)
+    flags |= M.FLAG_TIME_SMOOTHER if a.time_smoother else 0
     s = M.Solver(v, geo, bc, kind, flags)
-    phi, f = BoxData(v, 1, 1).to_device(), rhs.to_device()
+    phi, f = BoxData.device_zeros(v, 1, 1), (rhs.to_device() if a.workload == "wavy" else rhs)
     if a.dd:
         f.data /= geo.J.to_device().data[1:-1, 1:-1]
-    run = (lambda: s.dc_vcycle(phi, f, bc, True, 1e-10, a.vcycles, 1, 8, 8, 8)) if a.dd else \
-        (lambda: s.vcycle(phi, f, bc, True, 1e-10, a.vcycles, 1, 8, 8, 8))
+    run = (lambda: s.dc_vcycle(phi, f, bc, homog, 1e-10, a.vcycles, 1, 8, 8, 8)) if a.dd else \
+        (lambda: s.vcycle(phi, f, bc, homog, 1e-10, a.vcycles, 1, 8, 8, 8))
     for _ in range(a.warmup):
         phi.data.zero_()
         run()
@@ -51,6 +60,9 @@ def main():
     print(f"n={a.n} vcycles={rep.iterations} device {rep.seconds * 1e3:.3f} ms "
           f"({rep.seconds / max(rep.iterations, 1) * 1e3:.3f} ms/V-cycle), wall {dt * 1e3:.3f} ms, "
           f"{M.kernel_launch_count() - l0} launches, relres {rep.relres[-1]:.3e}")
+    if a.time_smoother:
+        print(f"finest-level sweep {rep.smooth0_seconds / max(rep.smooth0_sweeps, 1) * 1e6:.2f} us "
+              f"({rep.smooth0_sweeps} sweeps)")
     s.close()
 
 
