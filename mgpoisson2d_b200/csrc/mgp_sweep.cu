@@ -26,7 +26,8 @@
 // sub-passes over the whole grid one after another.
 //
 // Staging: on the solver's own arrays (aligned, with spare columns) one
-// thread issues seven TMA tile loads (cp.async.bulk.tensor.2d) of the CTA's
+// thread issues seven TMA tile loads (five on the wide FP32 tiles;
+// cp.async.bulk.tensor.2d) of the CTA's
 // window of each field, completing on one mbarrier; elsewhere (caller arrays
 // of any pitch and alignment) the threads stage with cp.async.
 //
@@ -49,7 +50,6 @@ namespace {
 
 constexpr int kTY = 32;
 constexpr int kH = 6;   // phi halo: 4 for the colour passes + E = 2 for the boundary pass
-constexpr int kSweepThreads = 512;
 // A CTA gives up on its tile loads after kWaitLimit polls or kWaitNs, far
 // above any real wait (microseconds); each poll sleeps up to kSuspendNs.
 constexpr long kWaitLimit = 1L << 22;
@@ -58,9 +58,13 @@ constexpr unsigned kSuspendNs = 20000;
 
 // Tile and shared-memory window of one field type and tile width: 32 x 32
 // tiles (FP64: two CTAs of 114 KB per SM; FP32: three of 59 KB) and, for
-// FP32 levels large enough to fill the GPU, 64 x 32 tiles (two CTAs of
-// 99 KB), which spread each thread's fixed work over more cells and
-// recompute a smaller share of halo.  All seven staged arrays share one
+// FP32 levels large enough to fill the GPU, 64 x 32 tiles, which spread each
+// thread's fixed work over more cells and recompute a smaller share of halo.
+// The wide tiles stage five arrays, not seven: rhs and the inverse diagonal,
+// read once per update and only at the updated cell, come from global memory
+// there, so the window (70 KB) leaves room for three CTAs per SM -- a tile's
+// colour passes are latency-bound, and more CTAs in flight hide it.  All
+// staged arrays share one
 // window -- origin (pox, poy) with pox the column at or below tile corner - kH
 // that is a multiple of kAlign (a 16-byte boundary, as TMA needs), pitch PW --
 // so one offset addresses a cell in every array: phi and the cell operands
@@ -74,15 +78,26 @@ struct Win {
     static constexpr int PW = (TX + 2 * kH + (kAlign - 1) + kAlign - 1) / kAlign * kAlign;   // 46 / 48 / 80
     static constexpr int PH = kTY + 2 * kH;                                                        // 44
     static constexpr int kA = (PW * PH * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);     // 128-B aligned
-    static constexpr int oF = kA, oD = 2 * kA, oXX = 3 * kA, oXY = 4 * kA, oYX = 5 * kA, oYY = 6 * kA;
-    static constexpr int oBarBytes = 7 * kA * (int)sizeof(T);   // the TMA mbarrier (8 bytes)
+    static constexpr bool kRI = !(sizeof(T) == 4 && TX_ == 64);   // rhs and inverse diagonal staged
+    static constexpr int NA = kRI ? 7 : 5;                          // staged arrays
+    static constexpr int oF = kA, oD = 2 * kA;                      // (when kRI)
+    static_assert(oD == oF + kA, "rhs and inverse diagonal adjacent");
+    static constexpr int oXX = (kRI ? 3 : 1) * kA, oXY = oXX + kA, oYX = oXX + 2 * kA, oYY = oXX + 3 * kA;
+    static constexpr int oBarBytes = NA * kA * (int)sizeof(T);   // the TMA mbarrier (8 bytes)
     static constexpr size_t kSmemBytes = (size_t)oBarBytes + 16;
     static constexpr unsigned kBoxBytes = PW * PH * sizeof(T);
-    static constexpr int kMinBlocks = (int)((228 * 1024) / (kSmemBytes + 1024));   // CTAs per SM the window allows
+    // threads: the wide tiles' colour passes hold 256 to 333 cell pairs (up to
+    // 389 on tiles at the domain edge), so 12 warps cover them, and three
+    // CTAs of 384 threads leave 56 registers a thread
+    static constexpr int kThreads = kRI ? 512 : 384;
+    // CTAs per SM the window and the thread count allow
+    static constexpr int kMinBlocks = (int)((228 * 1024) / (kSmemBytes + 1024)) < 2048 / kThreads
+                                          ? (int)((228 * 1024) / (kSmemBytes + 1024))
+                                          : 2048 / kThreads;
 };
 
 static_assert(Win<double, 32>::PW == 46 && Win<float, 32>::PW == 48 && Win<float, 64>::PW == 80, "window pitch");
-static_assert(Win<double, 32>::kMinBlocks == 2 && Win<float, 32>::kMinBlocks == 3 && Win<float, 64>::kMinBlocks == 2,
+static_assert(Win<double, 32>::kMinBlocks == 2 && Win<float, 32>::kMinBlocks == 3 && Win<float, 64>::kMinBlocks == 3,
               "CTAs per SM");
 
 template <class T>
@@ -225,9 +240,10 @@ struct Tile {
 };
 
 // One Gauss-Seidel update of (i,j) from shared memory (same operations as gs9).
+// f and d are rhs and the inverse diagonal at (i,j).
 template <class W, class T>
 __device__ __forceinline__ void gs9_tile(const Tile<T>& t, T idx, T idy, const BCd& b, int homog, int i, int j, int xr,
-                                         int yr, T om, T om1) {
+                                         int yr, T om, T om1, T f, T d) {
     T* c = t.s + (j - t.poy) * W::PW + (i - t.pox);
     St9T<T> s;
     gather9(SLoadT<T>{c, W::PW}, xr, yr, s);
@@ -238,7 +254,7 @@ __device__ __forceinline__ void gs9_tile(const Tile<T>& t, T idx, T idy, const B
     fc.yxs = c[W::oYX]; fc.yxn = c[W::oYX + W::PW];
     const T lphi = lap9f(s, fc, idx, idy, i, j, xr, yr, b, homog);
     const T p = c[0];
-    const T newphi = p + (c[W::oF] - lphi) * c[W::oD];
+    const T newphi = p + (f - lphi) * d;
     c[0] = om * newphi + om1 * p;
 }
 
@@ -258,9 +274,10 @@ __device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return __fmul2_rn(
 __device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 f2sub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
 
+// f and d hold rhs and the inverse diagonal at the two cells.
 template <class W>
-__device__ __forceinline__ void gs9_pair(float* a, float* b, bool write_b, float2 idx, float2 idy, float2 om,
-                                         float2 om1) {
+__device__ __forceinline__ void gs9_pair(float* a, float* b, bool write_b, float2 f, float2 d, float2 idx, float2 idy,
+                                         float2 om, float2 om1) {
     constexpr int P = W::PW;
     const auto L = [a, b](int o) { return make_float2(a[o], b[o]); };
     const float2 p = L(0), pe = L(1), pw = L(-1), pn = L(P), ps = L(-P);
@@ -276,14 +293,14 @@ __device__ __forceinline__ void gs9_pair(float* a, float* b, bool write_b, float
     const float2 yfs = f2fma(f2mul(L(W::oYY), f2sub(p, ps)), idy,
                              f2mul(f2mul(f2mul(L(W::oYX), q), f2sub(f2add(f2sub(pe, pw), ese), esw)), idx));
     const float2 lphi = f2fma(f2sub(xfe, xfw), idx, f2mul(f2sub(yfn, yfs), idy));
-    const float2 newphi = f2fma(f2sub(L(W::oF), lphi), L(W::oD), p);
+    const float2 newphi = f2fma(f2sub(f, lphi), d, p);
     const float2 r = f2fma(om, newphi, f2mul(om1, p));
     a[0] = r.x;
     if (write_b) b[0] = r.y;
 }
 
 template <bool kTma, class T, int TX>
-__global__ void __launch_bounds__(kSweepThreads, (Win<T, TX>::kMinBlocks))
+__global__ void __launch_bounds__((Win<T, TX>::kThreads), (Win<T, TX>::kMinBlocks))
     k_sweep9(const __grid_constant__ SweepMaps m, DFT<T> pin, DFT<T> pout, DFT<T> rhs, DFT<T> invd, GeoT<T> g,
              const __grid_constant__ BCd b, int homog, int nx, int ny, int4 part, double omega, int* status) {
     using W = Win<T, TX>;
@@ -299,11 +316,23 @@ __global__ void __launch_bounds__(kSweepThreads, (Win<T, TX>::kMinBlocks))
     const int E = edge_tile ? 2 : 0;
     const T idx = T(g.idx), idy = T(g.idy);
     const T om = T(omega), om1 = T(1.0 - omega);
-
     Tile<T> t;
     t.s = smem;
     t.pox = (X0 - kH) & ~(W::kAlign - 1);
     t.poy = Y0 - kH;
+    // one scalar update, rhs and the inverse diagonal from the window or global memory
+    const auto gs = [&](int i, int j, int xr, int yr) {
+        T f, d;
+        if constexpr (W::kRI) {
+            const int o = (j - t.poy) * W::PW + (i - t.pox);
+            f = t.s[o + W::oF];
+            d = t.s[o + W::oD];
+        } else {
+            f = AT(rhs, i, j);
+            d = AT(invd, i, j);
+        }
+        gs9_tile<W>(t, idx, idy, b, homog, i, j, xr, yr, om, om1, f, d);
+    };
 
     // interior colour ranges (i in [mi0, mi1), j in [mj0, mj1)) on shrinking
     // regions, and their divide-free index maps, set up while the loads fly
@@ -327,10 +356,12 @@ __global__ void __launch_bounds__(kSweepThreads, (Win<T, TX>::kMinBlocks))
         if (threadIdx.x == 0) mbar_init(bar, 1);
         __syncthreads();
         if (threadIdx.x == 0) {
-            mbar_expect_tx(bar, 7 * W::kBoxBytes);
+            mbar_expect_tx(bar, W::NA * W::kBoxBytes);
             tma_load_2d(sb, &m.pin, t.pox - m.pcb, t.poy - m.prb, bar);
-            tma_load_2d(sb + W::oF * kS, &m.rhs, t.pox, t.poy, bar);
-            tma_load_2d(sb + W::oD * kS, &m.invd, t.pox, t.poy, bar);
+            if constexpr (W::kRI) {
+                tma_load_2d(sb + W::oF * kS, &m.rhs, t.pox, t.poy, bar);
+                tma_load_2d(sb + W::oD * kS, &m.invd, t.pox, t.poy, bar);
+            }
             tma_load_2d(sb + W::oXX * kS, &m.xx, t.pox, t.poy, bar);
             tma_load_2d(sb + W::oXY * kS, &m.xy, t.pox, t.poy, bar);
             tma_load_2d(sb + W::oYX * kS, &m.yx, t.pox, t.poy, bar);
@@ -349,8 +380,10 @@ __global__ void __launch_bounds__(kSweepThreads, (Win<T, TX>::kMinBlocks))
         }
     } else {
         stage(smem, W::PW, t.pox, t.poy, pin, pi0, pi1, pj0, pj1);
-        stage(smem + W::oF, W::PW, t.pox, t.poy, rhs, ci0s, ci1s, cj0s, cj1s);
-        stage(smem + W::oD, W::PW, t.pox, t.poy, invd, ci0s, ci1s, cj0s, cj1s);
+        if constexpr (W::kRI) {
+            stage(smem + W::oF, W::PW, t.pox, t.poy, rhs, ci0s, ci1s, cj0s, cj1s);
+            stage(smem + W::oD, W::PW, t.pox, t.poy, invd, ci0s, ci1s, cj0s, cj1s);
+        }
         stage(smem + W::oXX, W::PW, t.pox, t.poy, g.xx, ci0s, ci1s + 1, cj0s, cj1s);
         stage(smem + W::oXY, W::PW, t.pox, t.poy, g.xy, ci0s, ci1s + 1, cj0s, cj1s);
         stage(smem + W::oYX, W::PW, t.pox, t.poy, g.yx, ci0s, ci1s, cj0s, cj1s + 1);
@@ -394,7 +427,17 @@ __global__ void __launch_bounds__(kSweepThreads, (Win<T, TX>::kMinBlocks))
                 const int ia = ci0[c] + 2 * (k - ja * ccw[c]), ib = ci0[c] + 2 * (kb - jb * ccw[c]);
                 T* ca = t.s + (cj0[c] + 2 * ja - t.poy) * W::PW + (ia - t.pox);
                 T* cb = t.s + (cj0[c] + 2 * jb - t.poy) * W::PW + (ib - t.pox);
-                gs9_pair<W>(ca, cb, kb != k, idx2, idy2, om2, om12);
+                float2 f2, d2;
+                if constexpr (W::kRI) {
+                    f2 = make_float2(ca[W::oF], cb[W::oF]);
+                    d2 = make_float2(ca[W::oD], cb[W::oD]);
+                } else {
+                    const long ga = (long)(cj0[c] + 2 * ja) * rhs.ld + ia, gb = (long)(cj0[c] + 2 * jb) * rhs.ld + ib;
+                    const long ha = (long)(cj0[c] + 2 * ja) * invd.ld + ia, hb = (long)(cj0[c] + 2 * jb) * invd.ld + ib;
+                    f2 = make_float2(__ldg(rhs.p + ga), __ldg(rhs.p + gb));
+                    d2 = make_float2(__ldg(invd.p + ha), __ldg(invd.p + hb));
+                }
+                gs9_pair<W>(ca, cb, kb != k, f2, d2, idx2, idy2, om2, om12);
             }
             __syncthreads();
         }
@@ -404,7 +447,7 @@ __global__ void __launch_bounds__(kSweepThreads, (Win<T, TX>::kMinBlocks))
             for (int k = threadIdx.x; k < cn[c]; k += blockDim.x) {
                 const int kj = fastdiv24(k, cm[c]);
                 const int i = ci0[c] + 2 * (k - kj * ccw[c]), j = cj0[c] + 2 * kj;
-                gs9_tile<W>(t, idx, idy, b, homog, i, j, RMID, RMID, om, om1);
+                gs(i, j, RMID, RMID);
             }
             __syncthreads();
         }
@@ -427,10 +470,10 @@ __global__ void __launch_bounds__(kSweepThreads, (Win<T, TX>::kMinBlocks))
             const int n2 = n1 + ((sxl && ci == 0) ? nj : 0);
             const int n3 = n2 + ((sxh && ((nx - 1) & 1) == ci) ? nj : 0);
             for (int k = threadIdx.x; k < n3; k += blockDim.x) {
-                if (k < n0) gs9_tile<W>(t, idx, idy, b, homog, ia + 2 * k, 0, RMID, RLO, om, om1);
-                else if (k < n1) gs9_tile<W>(t, idx, idy, b, homog, ia + 2 * (k - n0), ny - 1, RMID, RHI, om, om1);
-                else if (k < n2) gs9_tile<W>(t, idx, idy, b, homog, 0, ja + 2 * (k - n1), RLO, RMID, om, om1);
-                else gs9_tile<W>(t, idx, idy, b, homog, nx - 1, ja + 2 * (k - n2), RHI, RMID, om, om1);
+                if (k < n0) gs(ia + 2 * k, 0, RMID, RLO);
+                else if (k < n1) gs(ia + 2 * (k - n0), ny - 1, RMID, RHI);
+                else if (k < n2) gs(0, ja + 2 * (k - n1), RLO, RMID);
+                else gs(nx - 1, ja + 2 * (k - n2), RHI, RMID);
             }
             __syncthreads();
         }
@@ -439,7 +482,7 @@ __global__ void __launch_bounds__(kSweepThreads, (Win<T, TX>::kMinBlocks))
                 const int i = (c & 1) ? nx - 1 : 0, j = (c & 2) ? ny - 1 : 0;
                 if (i < X0 || i >= X1 || j < Y0 || j >= Y1) continue;
                 const int xr = region(i, nx, pr.xl, pr.xh), yr = region(j, ny, pr.yl, pr.yh);
-                if (xr != RMID && yr != RMID) gs9_tile<W>(t, idx, idy, b, homog, i, j, xr, yr, om, om1);
+                if (xr != RMID && yr != RMID) gs(i, j, xr, yr);
             }
         }
         __syncthreads();
@@ -557,10 +600,14 @@ template <class T>
 void tma_prepare(SweepTma* t, const DFT<T>& ea, const DFT<T>& eb, const DFT<T>& rhs, const DFT<T>& invd,
                  const GeoT<T>& g, int nx, int ny) {
     t->tx = tile_width<T>(nx, ny);
-    if (t->tx == 64)
-        t->ok = prepare_maps<Win<T, 64>>(&t->ma, ea, rhs, invd, g, nx, ny) &&
-                prepare_maps<Win<T, 64>>(&t->mb, eb, rhs, invd, g, nx, ny);
-    else
+    bool wide = false;
+    if constexpr (sizeof(T) == 4) {
+        wide = t->tx == 64;
+        if (wide)
+            t->ok = prepare_maps<Win<T, 64>>(&t->ma, ea, rhs, invd, g, nx, ny) &&
+                    prepare_maps<Win<T, 64>>(&t->mb, eb, rhs, invd, g, nx, ny);
+    }
+    if (!wide)
         t->ok = prepare_maps<Win<T, 32>>(&t->ma, ea, rhs, invd, g, nx, ny) &&
                 prepare_maps<Win<T, 32>>(&t->mb, eb, rhs, invd, g, nx, ny);
     t->pa = ea.p;
@@ -578,11 +625,11 @@ void launch_tiles(const SweepMaps* m, const DFT<T>& pin, const DFT<T>& pout, con
     dim3 grd((nx + TX - 1) / TX, (ny + kTY - 1) / kTY);
     const int4 part = make_int4(nx / (int)grd.x, nx % (int)grd.x, ny / (int)grd.y, ny % (int)grd.y);
     if (m) {
-        k_sweep9<true, T, TX><<<grd, kSweepThreads, W::kSmemBytes, st>>>(*m, pin, pout, rhs, invd, g, b, homog, nx,
+        k_sweep9<true, T, TX><<<grd, W::kThreads, W::kSmemBytes, st>>>(*m, pin, pout, rhs, invd, g, b, homog, nx,
                                                                          ny, part, omega, status);
     } else {
         static const SweepMaps none{};
-        k_sweep9<false, T, TX><<<grd, kSweepThreads, W::kSmemBytes, st>>>(none, pin, pout, rhs, invd, g, b, homog,
+        k_sweep9<false, T, TX><<<grd, W::kThreads, W::kSmemBytes, st>>>(none, pin, pout, rhs, invd, g, b, homog,
                                                                           nx, ny, part, omega, status);
     }
 }
