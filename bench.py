@@ -1,4 +1,4 @@
-"""Benchmark: multigrid solves/s to 1e-10 relative residual, plain FP64, on the
+"""Benchmark: multigrid solves/s to 1e-10 relative residual on the
 1024x1024 stretched mapped grid (x = xi + 0.1 sin(2 pi xi) sin(2 pi eta),
 y = (e^{beta eta} - 1)/(e^beta - 1) with a 64:1 first-cell aspect ratio; Dirichlet
 x sides, Neumann y sides; seeded 16-mode Fourier rhs, J-weighted mean removed).
@@ -7,10 +7,11 @@ x sides, Neumann y sides; seeded 16-mode Fourier rhs, J-weighted mean removed).
 
 One step = one full solve (until |r|/|r0| <= 1e-10) of that problem.  The
 default solver is the V-cycle accelerated by BiCGStab (MGP_FLAG_KRYLOV: one
-unchanged V-cycle per preconditioner application) with the V-cycle's grid
-levels in FP32 inside the FP64 outer iteration (MGP_FLAG_MIXED);
---solver vcycle and --precision fp64 select the reference's stationary
-iteration and plain FP64.  The line also carries one timed solve of the same
+V-cycle per preconditioner application) with the V-cycle's grid levels in
+FP32 inside the FP64 outer iteration (MGP_FLAG_MIXED) and its bottom solved
+exactly on the 8 x 8 level (MGP_FLAG_DIRECT_COARSE); --solver vcycle,
+--precision fp64 and --coarse reference select the reference's stationary
+iteration, plain FP64 and the reference's bottom solver.  The line also carries one timed solve of the same
 solver in FP64 ("fp64_same_solver") and of the plain FP64 V-cycle iteration
 ("plain_vcycle"), and the headline solution's error against both.  Under
 torchrun every rank solves its own copy (replicas; the solve does not shard)
@@ -67,6 +68,8 @@ def parse():
     p.add_argument("--solver", default="krylov", choices=["krylov", "vcycle"])
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                    help="mixed: FP32 grid levels inside the FP64 outer iteration (MGP_FLAG_MIXED)")
+    p.add_argument("--coarse", default="direct", choices=["direct", "reference"],
+                   help="bottom of the BiCGStab solver's V-cycle: exact (MGP_FLAG_DIRECT_COARSE) or the reference's")
     p.add_argument("--no-plain", action="store_true", help="skip the extra plain V-cycle solve")
     p.add_argument("--no-batch", action="store_true", help="skip the batched and served legs")
     p.add_argument("--batch", type=int, default=512, help="problems in the batched leg")
@@ -372,7 +375,7 @@ def precision_study(M, sizes):
     import torch
     from mgpoisson2d_b200 import workloads as W
     from mgpoisson2d_b200.types import BoxData
-    kry = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV
+    kry = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV | M.FLAG_DIRECT_COARSE
     stream = torch.cuda.current_stream()
     rows = []
     for n in sizes:
@@ -402,7 +405,7 @@ def precision_study(M, sizes):
             b[name]["order_l2"] = math.log2(a[name]["err_l2"] / b[name]["err_l2"]) / math.log2(b["n"] / a["n"])
     torch.cuda.empty_cache()
     return {"workload": "skew_stretched (30 deg skew, 1.05 boundary-layer stretch, u = e^x cos 4 pi y)",
-            "tol": TOL, "solver": "bicgstab(vcycle)", "rows": rows}
+            "tol": TOL, "solver": "bicgstab(vcycle), exact bottom", "rows": rows}
 
 
 def main():
@@ -428,6 +431,8 @@ def main():
     v, geo, rhs, bc, _ = workload(args.n)
     base_flags = M.FLAG_DIRICHLET_COUPLED_DIAG
     fp64_flags = base_flags | (M.FLAG_KRYLOV if args.solver == "krylov" else 0)
+    if args.solver == "krylov" and args.coarse == "direct":
+        fp64_flags |= M.FLAG_DIRECT_COARSE
     flags = fp64_flags | (M.FLAG_MIXED if args.precision == "mixed" else 0)
     solver = M.Solver(v, geo, bc, M.KIND_MG, flags)
     phi_d = BoxData(v, 1, 1).to_device()
@@ -540,7 +545,10 @@ def main():
                    "precision": ("FP32 grid levels, FP64 outer iteration / residual / update / coarse levels"
                                  if args.precision == "mixed" else "FP64"),
                    "flags": "dirichlet_coupled_diag" + ("|krylov" if args.solver == "krylov" else "") +
-                            ("|mixed" if args.precision == "mixed" else ""),
+                            ("|mixed" if args.precision == "mixed" else "") +
+                            ("|direct_coarse" if fp64_flags & M.FLAG_DIRECT_COARSE else ""),
+                   "bottom": ("exact solve of the first level <= 64 cells" if fp64_flags & M.FLAG_DIRECT_COARSE
+                              else "relax + BiCGStab to 1e-6 (reference)"),
                    "vcycles_per_solve": last.iterations, "final_relres": last.final_relres,
                    "maxdepth": last.maxdepth, "l2": "flushed between steps (256 MiB write, outside step events)",
                    "parallelism": f"replicas{world}"},
@@ -571,11 +579,12 @@ def main():
                        "api": "mgp_vcycle (host arrays; hierarchy built inside the call)",
                        "vcycles": erep.iterations, "timed_calls": len(times), "stat": "median"}
     if world > 1 and not args.no_batch:   # every rank: its share of the batch
-        batched_n = batched_multi(M, args, M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV | M.FLAG_MIXED, rank, world)
+        batched_n = batched_multi(M, args, M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV | M.FLAG_MIXED |
+                                  M.FLAG_DIRECT_COARSE, rank, world)
         if rank == 0:
             line["batched"] = batched_n
     if rank == 0 and world == 1 and not args.no_batch:
-        kry = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV
+        kry = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV | M.FLAG_DIRECT_COARSE
         fls = [("mixed", kry | M.FLAG_MIXED), ("fp64", kry)]
         batched, probs, rhs_b = batched_leg(M, args, fls)
         line["batched"] = batched

@@ -147,6 +147,15 @@ typedef struct mgp_report {
  * FP64 hierarchy's values rounded to FP32.  Combine with MGP_FLAG_KRYLOV (the
  * FP32 cycle is then the preconditioner).  No reference counterpart. */
 #define MGP_FLAG_MIXED 8
+/* MG kind only: end the V-cycle at the first level of at most 64 cells and
+ * solve that level exactly, with the inverse of its operator (homogeneous
+ * BCs) built and factored when the solver is created, in place of the bottom
+ * relaxation and solve_bicgstab2 to 1e-6 (MGPoisson2D.f90:733-761).  Needs a
+ * Dirichlet side (a nonsingular bottom operator); without one, or when no
+ * level is that small, or for cycles that start below that level (fmg), the
+ * reference bottom runs.  No reference counterpart: the V-cycle is then a
+ * different (stronger) preconditioner, for use with MGP_FLAG_KRYLOV. */
+#define MGP_FLAG_DIRECT_COARSE 16
 
 /* Solver kinds for the resident-hierarchy handle. */
 #define MGP_KIND_MG 0   /* module MGPoisson2D (vcycle, fmg)                  */

@@ -9,11 +9,13 @@
 // k_coarse_cycle.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/mgp2d.h"
@@ -254,6 +256,10 @@ struct mgp_solver {
     Lv* d_lv = nullptr;
     Lv* d_shadow = nullptr; // coarse levels' shared-memory layout (offsets), or nullptr
     int shadow_bytes = 0;
+    // MGP_FLAG_DIRECT_COARSE: level db (>= dc) is the V-cycle's bottom, solved
+    // with d_ainv, its operator's inverse (transposed); db = -1 without
+    int db = -1;
+    double* d_ainv = nullptr;
     int* d_ref = nullptr;   // refx then refy
     int* d_status = nullptr;
     Arena fixed;            // geometry, inverse diagonals
@@ -303,6 +309,7 @@ void solver_free(mgp_solver* s) {
     if (!s) return;
     if (s->d_lv) cudaFree(s->d_lv);
     if (s->d_shadow) cudaFree(s->d_shadow);
+    if (s->d_ainv) cudaFree(s->d_ainv);
     if (s->d_ref) cudaFree(s->d_ref);
     if (s->d_status) cudaFree(s->d_status);
     if (s->d_bcbuf) cudaFree(s->d_bcbuf);
@@ -330,6 +337,97 @@ bool mixed(const mgp_solver* s) { return (s->flags & MGP_FLAG_MIXED) && s->kind 
 // FP32 copies of the grid-path levels: geometry and inverse diagonals rounded
 // from the FP64 hierarchy (built first, so the coarse operators are the FP64
 // restrictions), corrections, right-hand sides and work arrays in FP32.
+// Inverse of an n x n matrix (row-major) by Gauss-Jordan elimination with
+// partial pivoting; false if a pivot falls below 1e-13 of the largest entry
+// (the matrix is singular to working precision).
+bool invert_dense(std::vector<double> a, int n, std::vector<double>* inv) {
+    std::vector<double>& b = *inv;
+    b.assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) b[(size_t)i * n + i] = 1.0;
+    double amax = 0.0;
+    for (double v : a) amax = std::max(amax, std::fabs(v));
+    if (!(amax > 0.0)) return false;
+    for (int c = 0; c < n; ++c) {
+        int p = c;
+        for (int r = c + 1; r < n; ++r)
+            if (std::fabs(a[(size_t)r * n + c]) > std::fabs(a[(size_t)p * n + c])) p = r;
+        const double piv = a[(size_t)p * n + c];
+        if (!(std::fabs(piv) > 1e-13 * amax)) return false;
+        if (p != c)
+            for (int k = 0; k < n; ++k) {
+                std::swap(a[(size_t)p * n + k], a[(size_t)c * n + k]);
+                std::swap(b[(size_t)p * n + k], b[(size_t)c * n + k]);
+            }
+        const double ip = 1.0 / piv;
+        for (int k = 0; k < n; ++k) {
+            a[(size_t)c * n + k] *= ip;
+            b[(size_t)c * n + k] *= ip;
+        }
+        for (int r = 0; r < n; ++r) {
+            if (r == c) continue;
+            const double f = a[(size_t)r * n + c];
+            if (f == 0.0) continue;
+            for (int k = 0; k < n; ++k) {
+                a[(size_t)r * n + k] -= f * a[(size_t)c * n + k];
+                b[(size_t)r * n + k] -= f * b[(size_t)c * n + k];
+            }
+        }
+    }
+    return true;
+}
+
+// MGP_FLAG_DIRECT_COARSE: the first level from dc down with at most
+// kDirectCells cells becomes the bottom, solved with its operator's inverse.
+// The operator (homogeneous BCs) is assembled on the device column by column,
+// so the inverse is that of the very operator the V-cycle's residuals use.
+// Kept only with a Dirichlet side: otherwise the operator is singular.
+int build_direct_coarse(mgp_solver* s, cudaStream_t st) {
+    bool diri = false;
+    for (int k = 0; k < 4; ++k) diri = diri || s->types[k] == MGP_BCTYPE_DIRI;
+    if (!diri) return MGP_OK;
+    int db = -1;
+    for (int d = s->dc; d <= s->maxdepth; ++d)
+        if ((long)s->lv[d].nx * s->lv[d].ny <= kDirectCells) {
+            db = d;
+            break;
+        }
+    if (db < 0) return MGP_OK;
+    const Lv& L = s->lv[db];
+    const int n = L.nx * L.ny;
+    const size_t sz = (size_t)(L.nx + 2) * (L.ny + 2);
+    double *scratch = nullptr, *A = nullptr;
+    if (cudaMalloc(&scratch, sizeof(double) * 2 * sz * n) != cudaSuccess ||
+        cudaMalloc(&A, sizeof(double) * n * n) != cudaSuccess) {
+        cudaGetLastError();
+        if (scratch) cudaFree(scratch);
+        return set_err(MGP_ENOMEM, "device allocation failed");
+    }
+    std::vector<double> h((size_t)n * n), inv;
+    cudaError_t e = launch_direct_columns(L, scratch, A, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), A, sizeof(double) * n * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(scratch);
+    if (e != cudaSuccess) {
+        cudaFree(A);
+        return set_err(MGP_ECUDA, "direct coarse operator: %s", cudaGetErrorString(e));
+    }
+    if (!invert_dense(h, n, &inv)) {   // singular to working precision: keep the reference bottom
+        cudaFree(A);
+        return MGP_OK;
+    }
+    for (int k = 0; k < n; ++k)
+        for (int m = 0; m < n; ++m) h[(size_t)m * n + k] = inv[(size_t)k * n + m];
+    e = cudaMemcpyAsync(A, h.data(), sizeof(double) * n * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cudaFree(A);
+        return set_err(MGP_ECUDA, "direct coarse operator: %s", cudaGetErrorString(e));
+    }
+    s->d_ainv = A;
+    s->db = db;
+    return MGP_OK;
+}
+
 int build_fp32_levels(mgp_solver* s) {
     cudaStream_t st = s->stream;
     s->lv32.assign(s->dc, mgp_solver::Lv32{});
@@ -484,6 +582,7 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
         else CK(launch_invdiag(L.invd, L.g, L.bc, 1, L.nx, L.ny, (s->flags & MGP_FLAG_DIRICHLET_COUPLED_DIAG) ? 1 : 0,
                                st));                                                      // P2:16-388
     }
+    if ((s->flags & MGP_FLAG_DIRECT_COARSE) && s->kind == MGP_KIND_MG) RC(build_direct_coarse(s, st));
     // shared-memory layout of the coarse levels for k_coarse_cycle_smem
     {
         std::vector<Lv> sh(s->lv);
@@ -629,7 +728,11 @@ int coarse_cycle(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
     CoarseArgs a;
     a.lv = s->d_lv;
     a.d0 = d;
-    a.maxdepth = s->maxdepth;
+    // the exact bottom serves cycles that reach it from above (fmg's cycles
+    // that start below it keep the reference bottom)
+    const bool direct = s->d_ainv && d <= s->db;
+    a.maxdepth = direct ? s->db : s->maxdepth;
+    a.ainv = direct ? s->d_ainv : nullptr;
     a.numcycles = numcycles;
     a.nd = nd; a.nu = nu; a.nb = nb;
     a.dd = (s->kind == MGP_KIND_DD);

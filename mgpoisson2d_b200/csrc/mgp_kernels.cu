@@ -1184,6 +1184,31 @@ __device__ void b_set_guess(const Lv& L) {
     __syncthreads();
 }
 
+// e = A^{-1} r on the bottom level (MGP_FLAG_DIRECT_COARSE).  ainv holds the
+// inverse transposed, ainv[m * n + k] = (A^{-1})_{k m}; row k takes four
+// threads, each summing a quarter of the row, combined by two shuffles.
+static_assert(4 * kDirectCells <= kCoarseThreads, "four threads per row of the bottom inverse");
+__device__ void b_direct(const Lv& L, const double* ainv) {
+    const int nx = L.nx, n = L.nx * L.ny;
+    const int k = threadIdx.x >> 2, q = threadIdx.x & 3;
+    double s = 0.0;
+    if (k < n) {
+        const int m0 = q * n / 4, m1 = (q + 1) * n / 4;
+        int i = m0 % nx, j = m0 / nx;
+        for (int m = m0; m < m1; ++m) {
+            s = s + ainv[(size_t)m * n + k] * AT(L.r, i, j);
+            if (++i == nx) {
+                i = 0;
+                ++j;
+            }
+        }
+    }
+    s = s + __shfl_xor_sync(0xffffffffu, s, 1);
+    s = s + __shfl_xor_sync(0xffffffffu, s, 2);
+    if (k < n && q == 0) AT(L.e, k % nx, k / nx) = s;
+    __syncthreads();
+}
+
 // vcycle_noinit(d0) down to the bottom and back, on the levels lv[d0..maxdepth]
 // (every thread of the block runs it).  Returns a nonzero status on a
 // non-finite bottom residual.
@@ -1197,6 +1222,10 @@ visit:
         const Lv& L = lv[d];
         if (a.dd) b_set_guess(L);   // DD:931, DD:971
         if (d == a.maxdepth) {
+            if (a.ainv) {   // exact bottom solve
+                b_direct(L, a.ainv);
+                goto up;
+            }
             b_relax(L, L.e, L.r, 1, relax_omega, a.nb, a.dd);
             const int s = b_bicgstab(L, L.e, L.r, 1, 1.0e-6, 80, 5, 0, a.dd, sh);
             if (s) st = s;
@@ -1263,7 +1292,7 @@ __global__ void __launch_bounds__(kCoarseThreads, 1) k_coarse_cycle_smem(CoarseA
         Lv L = a.shadow[a.d0 + threadIdx.x];
         rebase(L.e, smem); rebase(L.r, smem); rebase(L.w, smem); rebase(L.invd, smem);
         rebase(L.g.J, smem); rebase(L.g.xx, smem); rebase(L.g.xy, smem); rebase(L.g.yx, smem); rebase(L.g.yy, smem);
-        if (a.d0 + (int)threadIdx.x == a.maxdepth) {
+        if (a.d0 + (int)threadIdx.x == a.maxdepth && !a.ainv) {
             rebase(L.ea, smem); rebase(L.pt, smem); rebase(L.st, smem);
             rebase(L.rr, smem); rebase(L.rt, smem); rebase(L.pp, smem); rebase(L.tt, smem); rebase(L.vv, smem);
         }
@@ -1290,6 +1319,24 @@ __global__ void __launch_bounds__(kCoarseThreads, 1) k_coarse_cycle_smem(CoarseA
         b_copy(G.e, S.e, -1, S.nx + 1, -1, S.ny + 1);
     }
     if (threadIdx.x == 0 && s) *a.status = s;
+}
+
+__global__ void __launch_bounds__(kCoarseThreads) k_direct_columns(Lv L, double* scratch, double* A) {
+    const int nx = L.nx, ny = L.ny, n = nx * ny, k = blockIdx.x;
+    const int ld = nx + 2;
+    const size_t sz = (size_t)ld * (ny + 2);
+    const DF phi{scratch + 2 * sz * k + ld + 1, ld}, out{scratch + (2 * k + 1) * sz + ld + 1, ld};
+    b_setval(phi, 0.0, nx, ny, 1);
+    if (threadIdx.x == 0) AT(phi, k % nx, k / nx) = 1.0;
+    __syncthreads();
+    b_apply(L, out, phi, out, 1, 0, 0);
+    BLOOP(m, n) A[(size_t)m * n + k] = AT(out, m % nx, m / nx);
+}
+
+cudaError_t launch_direct_columns(const Lv& L, double* scratch, double* A, cudaStream_t st) {
+    k_direct_columns<<<L.nx * L.ny, kCoarseThreads, 0, st>>>(L, scratch, A);
+    count_launch();
+    return cudaGetLastError();
 }
 
 // Per device: opt the shared-memory coarse kernel into its largest window.

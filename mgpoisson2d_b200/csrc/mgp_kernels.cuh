@@ -23,7 +23,12 @@ struct CoarseArgs {
     int* status;         // device int: 0 ok, nonzero = error code
     const Lv* shadow;    // device array: the levels' layout in shared memory (offsets), or nullptr
     int smem_bytes;      // dynamic shared memory the staged levels need
+    const double* ainv;  // MGP_FLAG_DIRECT_COARSE: inverse of level maxdepth's operator, transposed, or nullptr
 };
+
+// Largest bottom level solved by its precomputed inverse (cells); b_direct
+// gives each row four threads of the coarse CTA.
+constexpr int kDirectCells = 64;
 
 constexpr int kMaxCoarseLevels = 16;
 // Largest staged coarse hierarchy (bytes of dynamic shared memory).
@@ -149,6 +154,10 @@ cudaError_t sweep_kernels_init();
 cudaError_t coarse_kernels_init();
 // Single-CTA kernels.
 cudaError_t launch_coarse_cycle(const CoarseArgs& a, cudaStream_t st);
+// A[m * n + k] = (L e_k)_m for the level's operator with homogeneous BCs
+// (n = nx * ny columns, one CTA each; scratch holds 2 n fields of
+// (nx + 2) x (ny + 2)).
+cudaError_t launch_direct_columns(const Lv& L, double* scratch, double* A, cudaStream_t st);
 cudaError_t launch_bicgstab(const BicgArgs& a, cudaStream_t st);
 cudaError_t launch_relax_block(const Lv& L, const DF& phi, const DF& rhs, int homog, double omega, int sweeps,
                                int dd, int* status, cudaStream_t st);

@@ -434,6 +434,102 @@ def test_mixed_all_neumann_and_identity(M):
 
 
 # ---------------------------------------------------------------------------
+# Exact coarse solve (MGP_FLAG_DIRECT_COARSE; no reference counterpart): the
+# V-cycle's bottom is the first level of at most 64 cells, solved with the
+# inverse of its operator
+# ---------------------------------------------------------------------------
+def _oracle_operator(v, geo, bc):
+    """Dense matrix of the oracle's operator with homogeneous BCs: column k is
+    compute_laplacian of the k-th unit vector (cells numbered i fastest)."""
+    n = v.nx * v.ny
+    A = np.zeros((n, n))
+    for k in range(n):
+        e = BoxData(v, 1, 1)
+        e.interior()[k % v.nx, k // v.nx] = 1.0
+        lap = BoxData(v)
+        O.compute_laplacian(lap, e, geo, bc, True)
+        A[:, k] = lap.interior().reshape(-1, order="F")
+    return A
+
+
+@pytest.mark.parametrize("case", ["DDDD-U", "DNND-mixed", "PPDD", "DDNN-U"])
+@pytest.mark.parametrize("nx,ny", [(8, 8), (16, 4)])
+def test_direct_coarse_solves_a_bottom_sized_grid_in_one_cycle(M, case, nx, ny):
+    """A grid of 64 cells is its own bottom level: one V-cycle is the exact
+    solve, phi = A^-1 (rhs - L[0]), against numpy's dense solve of the
+    oracle's operator."""
+    v, geo, rhs, bc, _ = _problem(case, nx, ny, 5)
+    res = BoxData(v)
+    O.compute_residual(res, rhs, BoxData(v, 1, 1), geo, bc, False)
+    A = _oracle_operator(v, geo, bc)
+    want = np.linalg.solve(A, res.interior().reshape(-1, order="F")).reshape((nx, ny), order="F")
+    with M.Solver(v, geo, bc, KIND_MG, M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_DIRECT_COARSE) as s:
+        phi = BoxData(v, 1, 1)
+        r = s.vcycle(phi, rhs, bc, False, 1e-12, 5)
+    assert r.status == 0 and r.iterations == 1 and r.final_relres <= 1e-12, (r.iterations, r.final_relres)
+    assert np.abs(phi.interior() - want).max() <= 1e-11 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_direct_coarse_vcycle_converges_to_oracle_solution(M, mixed):
+    """On the stretched grid (bottom 8 x 8 instead of 4 x 4 with BiCGStab) the
+    BiCGStab(V-cycle) solve reaches 1e-10 in no more V-cycles than with the
+    reference bottom, and the oracle's FP64 solution."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, _ = W.wavy_stretched(128)
+    base = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV | (M.FLAG_MIXED if mixed else 0)
+    old = _set_coupled(M, True)
+    try:
+        po = BoxData(v, 1, 1)
+        O.vcycle(po, rhs, geo, bc, True, 1e-11, 3000, gs_order=1)
+    finally:
+        _set_coupled(M, old)
+    with M.Solver(v, geo, bc, KIND_MG, base) as s:
+        pr = BoxData(v, 1, 1)
+        rr = s.vcycle(pr, rhs, bc, True, 1e-10, 3000)
+    with M.Solver(v, geo, bc, KIND_MG, base | M.FLAG_DIRECT_COARSE) as s:
+        pd = BoxData(v, 1, 1)
+        rd = s.vcycle(pd, rhs, bc, True, 1e-10, 3000)
+        pd2 = BoxData(v, 1, 1)
+        rd2 = s.vcycle(pd2, rhs, bc, True, 1e-10, 3000)
+    assert rd.status == 0 and not rd.diverged and rd.final_relres <= 1e-10
+    assert rd.iterations <= rr.iterations + 2, (rd.iterations, rr.iterations)
+    assert same(pd.data, pd2.data)   # deterministic
+    err = pd.interior() - po.interior()
+    assert np.linalg.norm(err) / np.linalg.norm(po.interior()) < 1e-8
+    assert np.abs(err).max() / np.abs(po.interior()).max() < 1e-7
+
+
+def test_direct_coarse_keeps_the_reference_bottom_when_singular(M):
+    """All-Neumann: the bottom operator is singular, the flag changes nothing
+    (same bits as without it)."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, _ = W.terrain_neumann(64, O.boundary_fluxes, O.compute_laplacian)
+    out = []
+    for fl in (0, M.FLAG_DIRECT_COARSE):
+        with M.Solver(v, geo, bc, KIND_MG, fl) as s:
+            p = BoxData(v, 1, 1)
+            r = s.vcycle(p, rhs, bc, False, 1e-9, 200)
+        out.append((p, r))
+    assert same(out[0][0].data, out[1][0].data) and np.array_equal(out[0][1].relres, out[1][1].relres)
+
+
+def test_direct_coarse_with_fmg(M):
+    """fmg's cycles that start below the direct level keep the reference
+    bottom; the solve still reaches the same solution."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, _ = W.wavy_stretched(128)
+    sols = []
+    for fl in (M.FLAG_DIRICHLET_COUPLED_DIAG, M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_DIRECT_COARSE):
+        with M.Solver(v, geo, bc, KIND_MG, fl) as s:
+            p = BoxData(v, 1, 1)
+            r = s.fmg(p, rhs, bc, True, 1e-10, 2000)
+        assert r.status == 0 and r.final_relres <= 1e-10
+        sols.append(p.interior())
+    assert np.abs(sols[1] - sols[0]).max() <= 1e-7 * np.abs(sols[0]).max()
+
+
+# ---------------------------------------------------------------------------
 # Batches and the solve server: every result identical to solving alone
 # ---------------------------------------------------------------------------
 def _alone(M, prob, flags, tol=1e-10, maxiters=400):
