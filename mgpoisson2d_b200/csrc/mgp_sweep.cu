@@ -198,6 +198,14 @@ __device__ __forceinline__ bool mbar_wait0(unsigned bar) {
     }
     return false;
 }
+// Programmatic dependent launch: a grid launched with the programmatic
+// serialization attribute may start before the grid ahead of it in the stream
+// has finished; griddepcontrol.wait returns once that grid has completed and
+// its writes are visible (at once when there is none), and launch_dependents
+// lets the next such grid start as SM resources free up.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void allow_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // One 2-D tile (the map's box) of `map` at element coordinates (x, y); x is a
 // multiple of 16 bytes.
 __device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map, int x, int y, unsigned bar) {
@@ -304,6 +312,7 @@ __global__ void __launch_bounds__((Win<T, TX>::kThreads), (Win<T, TX>::kMinBlock
     k_sweep9(const __grid_constant__ SweepMaps m, DFT<T> pin, DFT<T> pout, DFT<T> rhs, DFT<T> invd, GeoT<T> g,
              const __grid_constant__ BCd b, int homog, int nx, int ny, int4 part, double omega, int* status) {
     using W = Win<T, TX>;
+    allow_dependents();
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     T* smem = reinterpret_cast<T*>(smem_raw);
     // tile bounds: part = (nx / gx, nx % gx, ny / gy, ny % gy); the first
@@ -355,17 +364,23 @@ __global__ void __launch_bounds__((Win<T, TX>::kThreads), (Win<T, TX>::kMinBlock
         }
         if (threadIdx.x == 0) mbar_init(bar, 1);
         __syncthreads();
+        // The descriptors exist only for a solver's own arrays, whose faces
+        // and inverse diagonal do not change during a solve: their tiles are
+        // requested before the wait for the previous grid (the solver
+        // launches these sweeps as programmatic dependents of the kernel
+        // before them), phi and rhs after it.
         if (threadIdx.x == 0) {
             mbar_expect_tx(bar, W::NA * W::kBoxBytes);
-            tma_load_2d(sb, &m.pin, t.pox - m.pcb, t.poy - m.prb, bar);
-            if constexpr (W::kRI) {
-                tma_load_2d(sb + W::oF * kS, &m.rhs, t.pox, t.poy, bar);
-                tma_load_2d(sb + W::oD * kS, &m.invd, t.pox, t.poy, bar);
-            }
+            if constexpr (W::kRI) tma_load_2d(sb + W::oD * kS, &m.invd, t.pox, t.poy, bar);
             tma_load_2d(sb + W::oXX * kS, &m.xx, t.pox, t.poy, bar);
             tma_load_2d(sb + W::oXY * kS, &m.xy, t.pox, t.poy, bar);
             tma_load_2d(sb + W::oYX * kS, &m.yx, t.pox, t.poy, bar);
             tma_load_2d(sb + W::oYY * kS, &m.yy, t.pox, t.poy, bar);
+        }
+        grid_dependency_wait();
+        if (threadIdx.x == 0) {
+            tma_load_2d(sb, &m.pin, t.pox - m.pcb, t.poy - m.prb, bar);
+            if constexpr (W::kRI) tma_load_2d(sb + W::oF * kS, &m.rhs, t.pox, t.poy, bar);
         }
         colour_ranges(X0, X1, Y0, Y1, E, mi0, mi1, mj0, mj1, ci0, cj0, ccw, cn, cm);
         // one warp polls the barrier; the others sleep in the block barrier
@@ -379,6 +394,7 @@ __global__ void __launch_bounds__((Win<T, TX>::kThreads), (Win<T, TX>::kMinBlock
             return;
         }
     } else {
+        grid_dependency_wait();
         stage(smem, W::PW, t.pox, t.poy, pin, pi0, pi1, pj0, pj1);
         if constexpr (W::kRI) {
             stage(smem + W::oF, W::PW, t.pox, t.poy, rhs, ci0s, ci1s, cj0s, cj1s);
@@ -618,20 +634,31 @@ void tma_prepare(SweepTma* t, const DFT<T>& ea, const DFT<T>& eb, const DFT<T>& 
 }
 
 template <class T, int TX>
-void launch_tiles(const SweepMaps* m, const DFT<T>& pin, const DFT<T>& pout, const DFT<T>& rhs, const DFT<T>& invd,
-                  const GeoT<T>& g, const BCd& b, int homog, int nx, int ny, double omega, int* status,
-                  cudaStream_t st) {
+cudaError_t launch_tiles(const SweepMaps* m, const DFT<T>& pin, const DFT<T>& pout, const DFT<T>& rhs,
+                         const DFT<T>& invd, const GeoT<T>& g, const BCd& b, int homog, int nx, int ny, double omega,
+                         int* status, cudaStream_t st) {
     using W = Win<T, TX>;
     dim3 grd((nx + TX - 1) / TX, (ny + kTY - 1) / kTY);
     const int4 part = make_int4(nx / (int)grd.x, nx % (int)grd.x, ny / (int)grd.y, ny % (int)grd.y);
     if (m) {
-        k_sweep9<true, T, TX><<<grd, W::kThreads, W::kSmemBytes, st>>>(*m, pin, pout, rhs, invd, g, b, homog, nx,
-                                                                         ny, part, omega, status);
-    } else {
-        static const SweepMaps none{};
-        k_sweep9<false, T, TX><<<grd, W::kThreads, W::kSmemBytes, st>>>(none, pin, pout, rhs, invd, g, b, homog,
-                                                                          nx, ny, part, omega, status);
+        // a solver's sweep: a programmatic dependent of the kernel before it
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grd;
+        cfg.blockDim = dim3(W::kThreads);
+        cfg.dynamicSmemBytes = W::kSmemBytes;
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, k_sweep9<true, T, TX>, *m, pin, pout, rhs, invd, g, b, homog, nx, ny, part,
+                                  omega, status);
     }
+    static const SweepMaps none{};
+    k_sweep9<false, T, TX><<<grd, W::kThreads, W::kSmemBytes, st>>>(none, pin, pout, rhs, invd, g, b, homog, nx, ny,
+                                                                    part, omega, status);
+    return cudaGetLastError();
 }
 
 template <class T>
@@ -648,11 +675,11 @@ cudaError_t sweep_impl(const DFT<T>& pin, const DFT<T>& pout, const DFT<T>& rhs,
     bool wide = false;
     if constexpr (sizeof(T) == 4) {
         wide = tx == 64;
-        if (wide) launch_tiles<T, 64>(m, pin, pout, rhs, invd, g, b, homog, nx, ny, omega, status, st);
+        if (wide) e = launch_tiles<T, 64>(m, pin, pout, rhs, invd, g, b, homog, nx, ny, omega, status, st);
     }
-    if (!wide) launch_tiles<T, 32>(m, pin, pout, rhs, invd, g, b, homog, nx, ny, omega, status, st);
+    if (!wide) e = launch_tiles<T, 32>(m, pin, pout, rhs, invd, g, b, homog, nx, ny, omega, status, st);
     count_launch();
-    return cudaGetLastError();
+    return e;
 }
 
 }  // namespace
