@@ -75,6 +75,8 @@ def parse():
     p.add_argument("--batch", type=int, default=512, help="problems in the batched leg")
     p.add_argument("--streams", type=int, default=16, help="concurrent solves in the batched and served legs")
     p.add_argument("--no-study", action="store_true", help="skip the precision/convergence study leg")
+    p.add_argument("--serve-sweep", action="store_true",
+                   help="add the served workload swept over arrival rates (several minutes)")
     p.add_argument("--study-sizes", default="512,1024,2048,4096",
                    help="grid sides of the precision/convergence study")
     return p.parse_args()
@@ -362,9 +364,90 @@ def served_leg(M, args, probs, rhs_d, flags_list, nreq=240, seed=5):
     return out
 
 
+def served_sweep(M, args, flags_list, pool=64, seed=5, rates=(10, 30, 100, 300, 1000, 3000)):
+    """The served workload swept over arrival rates: a pool of `pool` problems
+    (sides log-uniform in [32, 2048] rounded to a multiple of 8, maps as the
+    batched workload, seed 5), requests drawn from the pool with Poisson
+    arrivals at each rate, tolerance 1e-8 or 1e-10 with probability 1/2,
+    min(2000, 8 x rate) requests per rate (at least 100), hierarchies resident
+    per problem; stops after the first rate whose p99 has diverged (above 10x
+    the lowest rate's p99, or fewer than 0.7 of the offered solves/s)."""
+    import numpy as np
+    import torch
+    from mgpoisson2d_b200 import workloads as W
+    from mgpoisson2d_b200.types import BoxData
+    probs = [W.batch_problem_device(i, seed=seed, nmin=32, nmax=2048, round_to=8) for i in range(pool)]
+    torch.cuda.synchronize()
+    out = {"pool": pool, "sides": [32, 2048], "slots": args.streams, "tolerances": [1e-8, 1e-10],
+           "cells_mean": float(np.mean([p[0].nx * p[0].ny for p in probs]))}
+    for name, fl in flags_list:
+        rows = []
+        with M.Server(nworkers=args.streams, flags=fl) as srv:
+            warm = [srv.submit(v, g, bc, BoxData.device_zeros(v, 1, 1), rhs, True, 1e-10, MAXITERS, key=k + 1)
+                    for k, (v, g, rhs, bc) in enumerate(probs)]
+            for t in warm:
+                srv.wait(t)
+            base_p99 = None
+            for lam in rates:
+                nreq = int(min(2000, max(100, 8 * lam)))
+                rng = np.random.default_rng(seed * 1000 + lam)
+                gaps = rng.exponential(1.0 / lam, nreq)
+                which = rng.integers(0, pool, nreq)
+                tols = np.where(rng.random(nreq) < 0.5, 1e-8, 1e-10)
+                outs = [BoxData.device_zeros(probs[k][0], 1, 1) for k in which]
+                tickets = []
+                t0 = time.perf_counter()
+                t_next = t0
+                for n in range(nreq):
+                    t_next += gaps[n]
+                    while time.perf_counter() < t_next:
+                        time.sleep(max(0.0, min(0.001, t_next - time.perf_counter())))
+                    v, g, rhs, bc = probs[which[n]]
+                    tickets.append(srv.submit(v, g, bc, outs[n], rhs, True, float(tols[n]), MAXITERS,
+                                              key=int(which[n]) + 1))
+                lats = np.sort(np.array([srv.wait(t)[1] for t in tickets])) * 1e3
+                span = time.perf_counter() - t0
+                p99 = float(lats[min(len(lats) - 1, int(math.ceil(0.99 * len(lats))) - 1)])
+                row = {"offered_per_s": lam, "requests": nreq, "solves_per_s": nreq / span,
+                       "p50_ms": float(lats[len(lats) // 2]), "p99_ms": p99}
+                rows.append(row)
+                base_p99 = base_p99 or p99
+                if p99 > 10 * base_p99 or row["solves_per_s"] < 0.7 * lam:
+                    break
+        out[name] = rows
+    return out
+
+
 # --------------------------------------------------------------------------- #
 # GPU arm
 # --------------------------------------------------------------------------- #
+def vcycle_bytes(M, v, mixed, direct, nu=NU):
+    """Algorithmic bytes of one V-cycle: per level with N cells and word size
+    w, N w [8 (nu1 + nu2) + 6 + rho + 2 + rho + 3] (sweeps; residual fused
+    with restriction; prolongation; the coarse guess r invdiag; rho = coarse
+    cells per fine cell), plus 11 FP64 words per finest cell for the outer
+    residual, norm and update.  Levels of at most 1024 cells (the coarse CTA)
+    are FP64; with FP32 grid levels the others take 4 B.  The bottom solve
+    is counted as time, not bytes."""
+    md = M.estimate_maxdepth(1000, v)
+    rx, ry, md = M.create_mgschedule(md, v)
+    nx, ny, levels = v.nx, v.ny, []
+    for d in range(md + 1):
+        levels.append((nx, ny))
+        if d < md:
+            nx, ny = nx // rx[d], ny // ry[d]
+    bottom = len(levels) - 1
+    if direct:
+        bottom = next((d for d, (a, b) in enumerate(levels) if a * b <= 64), bottom)
+    total = 11 * 8 * v.nx * v.ny
+    for d in range(bottom):
+        n = levels[d][0] * levels[d][1]
+        w = 4 if (mixed and n > 1024) else 8
+        rho = 1.0 / (rx[d] * ry[d])
+        total += n * w * (8 * (nu[0] + nu[1]) + 6 + rho + 2 + rho + 3)
+    return total
+
+
 def precision_study(M, sizes):
     """Mixed precision against FP64 and against the exact solution on the
     skewed, boundary-layer-stretched manufactured problem (u = e^x cos 4 pi y,
@@ -536,6 +619,13 @@ def main():
                 "peak_kind": peak_kind, "traffic": (tr or {}).get("bytes_per_sweep"),
                 "alg_bytes_per_sweep": alg_bytes, "sweep_us": sweep_s * 1e6}
 
+    vb = vcycle_bytes(M, v, args.precision == "mixed", bool(fp64_flags & M.FLAG_DIRECT_COARSE))
+    vc_s = (total_ms / args.steps) * 1e-3 / max(last.iterations, 1)
+    vcycle_roofline = {"bytes_per_vcycle": vb, "s_per_vcycle": vc_s, "achieved": vb / vc_s / 1e9, "peak": peak,
+                       "unit": "GB/s", "frac": vb / vc_s / 1e9 / peak,
+                       "note": "whole V-cycle, algorithmic bytes of every level (bottom solve as time); the time is "
+                               "the solve's divided by its V-cycles, Krylov vector work included"}
+
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -553,7 +643,7 @@ def main():
                    "maxdepth": last.maxdepth, "l2": "flushed between steps (256 MiB write, outside step events)",
                    "parallelism": f"replicas{world}"},
         "latency_ms": latency, "fp64_same_solver": fp64, "plain_vcycle": plain, "accuracy": accuracy,
-        "roofline": roofline, "clocks": clocks, "gpu_launches": launches,
+        "roofline": roofline, "vcycle_roofline": vcycle_roofline, "clocks": clocks, "gpu_launches": launches,
         "unknowns_vcycles_per_s": value * last.iterations * v.nx * v.ny,
         "wall_s": wall,
     }
@@ -590,6 +680,9 @@ def main():
         line["batched"] = batched
         line["served"] = served_leg(M, args, probs, rhs_b,
                                     [(n, f, batched[n]["batched_solves_per_s"]) for n, f in fls])
+    if rank == 0 and world == 1 and args.serve_sweep:
+        kry = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV | M.FLAG_DIRECT_COARSE
+        line["served_sweep"] = served_sweep(M, args, [("mixed", kry | M.FLAG_MIXED), ("fp64", kry)])
     if rank == 0 and world == 1 and not args.no_study:
         line["precision_study"] = precision_study(M, [int(x) for x in args.study_sizes.split(",") if x])
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -51,6 +51,10 @@ int set_err(int code, const char* fmt, ...) {
 
 // Levels with at most this many cells run inside the single-CTA coarse cycle.
 constexpr long kCoarseCells = 1024;
+// When the schedule stops above that (an odd side), the coarse cycle runs on
+// the coarsest level alone; beyond this many cells it runs as a cooperative
+// grid of one CTA per 256 cells (at most one per SM) instead of one CTA.
+constexpr long kGridCoarseCells = 8192;
 
 // ---------------------------------------------------------------------------
 // Device memory: every field of a solver comes out of one allocation.
@@ -260,6 +264,9 @@ struct mgp_solver {
     // with d_ainv, its operator's inverse (transposed); db = -1 without
     int db = -1;
     double* d_ainv = nullptr;
+    // coarse cycle as a cooperative grid of grid_ctas CTAs (0: one CTA)
+    int grid_ctas = 0;
+    GridCtl gctl{};
     int* d_ref = nullptr;   // refx then refy
     int* d_status = nullptr;
     Arena fixed;            // geometry, inverse diagonals
@@ -310,6 +317,8 @@ void solver_free(mgp_solver* s) {
     if (s->d_lv) cudaFree(s->d_lv);
     if (s->d_shadow) cudaFree(s->d_shadow);
     if (s->d_ainv) cudaFree(s->d_ainv);
+    if (s->gctl.bar) cudaFree(s->gctl.bar);
+    if (s->gctl.part) cudaFree(s->gctl.part);
     if (s->d_ref) cudaFree(s->d_ref);
     if (s->d_status) cudaFree(s->d_status);
     if (s->d_bcbuf) cudaFree(s->d_bcbuf);
@@ -583,6 +592,18 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
                                st));                                                      // P2:16-388
     }
     if ((s->flags & MGP_FLAG_DIRECT_COARSE) && s->kind == MGP_KIND_MG) RC(build_direct_coarse(s, st));
+    if (const long cells = (long)s->lv[s->dc].nx * s->lv[s->dc].ny; cells > kGridCoarseCells) {
+        int dev = 0, nsm = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        s->grid_ctas = (int)std::min<long>(std::max(nsm, 1), std::max<long>(2, cells / 256));
+        if (cudaMalloc(&s->gctl.bar, 2 * sizeof(unsigned)) != cudaSuccess ||
+            cudaMalloc(&s->gctl.part, 2 * sizeof(double) * s->grid_ctas) != cudaSuccess) {
+            cudaGetLastError();
+            return set_err(MGP_ENOMEM, "device allocation failed");
+        }
+        s->gctl.status = s->d_status;
+    }
     // shared-memory layout of the coarse levels for k_coarse_cycle_smem
     {
         std::vector<Lv> sh(s->lv);
@@ -741,6 +762,9 @@ int coarse_cycle(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
     a.status = s->d_status;
     a.shadow = s->d_shadow;
     a.smem_bytes = s->shadow_bytes;
+    a.grid_ctas = s->grid_ctas;
+    a.gctl = s->gctl;
+    if (a.grid_ctas > 1) CK(cudaMemsetAsync(s->gctl.bar, 0, 2 * sizeof(unsigned), s->stream));
     CK(launch_coarse_cycle(a, s->stream));
     return MGP_OK;
 }

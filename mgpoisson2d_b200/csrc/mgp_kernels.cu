@@ -310,35 +310,91 @@ __device__ __forceinline__ void perimeter_cell(int k, int nx, int ny, int& i, in
     else { i = nx - 1; j = 1 + k - 2 * nx - (ny - 2); }
 }
 
-// Step 3 of the sweep; every thread of the block calls it.
+// ---------------------------------------------------------------------------
+// Scopes of the cooperative building blocks (b_*): every thread of one CTA
+// (BlockScope), or of a cooperative grid whose CTAs are all resident
+// (GridScope: grid-stride loops, a grid barrier in place of __syncthreads,
+// reductions combined across CTAs in CTA order).  With one CTA both run the
+// same loops; BlockScope is what the single-CTA kernels use.
+// ---------------------------------------------------------------------------
+__shared__ GridCtl s_gctl;   // the grid kernel's barrier and partials (set on entry)
+__shared__ int s_gred;       // grid reductions so far (parity of the partials buffer)
+
+// A CTA gives up on a grid barrier after kGridWaitLimit polls (each sleeps up
+// to 256 ns: seconds, far above any real wait) and reports status 2.
+constexpr long kGridWaitLimit = 1L << 24;
+
+__device__ void grid_barrier() {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned* bar = s_gctl.bar;
+        volatile unsigned* gen = bar + 1;
+        const unsigned g0 = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {   // the last to arrive opens the next generation
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            unsigned nap = 32;
+            for (long k = 0; *gen == g0; ++k) {
+                if (k > kGridWaitLimit) {
+                    atomicExch(s_gctl.status, 2);
+                    break;
+                }
+                __nanosleep(nap);
+                nap = nap < 256 ? 2 * nap : nap;
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+struct BlockScope {
+    static constexpr bool kGrid = false;
+    __device__ static int rank() { return threadIdx.x; }
+    __device__ static int size() { return blockDim.x; }
+    __device__ static void sync() { __syncthreads(); }
+};
+struct GridScope {
+    static constexpr bool kGrid = true;
+    __device__ static int rank() { return blockIdx.x * blockDim.x + threadIdx.x; }
+    __device__ static int size() { return gridDim.x * blockDim.x; }
+    __device__ static void sync() { grid_barrier(); }
+};
+#define SLOOP(k, n) for (int k = S::rank(); k < (n); k += S::size())
+
+// Step 3 of the sweep; every thread of the scope calls it.
+template <class S>
 __device__ void b_gs_boundary(const DF& phi, const DF& rhs, const DF& invd, const Geo& g, const BCd& b, int homog,
                               int nx, int ny, double omega) {
     const Per pr = periodic_of(b);
     const int np = 2 * nx + 2 * (ny - 2);
     for (int c = 0; c < 4; ++c) {
         const int ci = colour_ci(c), cj = colour_cj(c);
-        for (int k = threadIdx.x; k < np; k += blockDim.x) {
+        SLOOP(k, np) {
             int i, j;
             perimeter_cell(k, nx, ny, i, j);
             if ((i & 1) != ci || (j & 1) != cj) continue;
             const bool xm = region(i, nx, pr.xl, pr.xh) == RMID, ym = region(j, ny, pr.yl, pr.yh) == RMID;
             if (xm != ym) gs9(phi, rhs, invd, g, b, homog, nx, ny, i, j, omega);
         }
-        __syncthreads();
+        S::sync();
     }
-    if (threadIdx.x == 0) {
+    if (S::rank() == 0) {
         for (int c = 0; c < 4; ++c) {
             const int i = (c & 1) ? nx - 1 : 0, j = (c & 2) ? ny - 1 : 0;
             if (region(i, nx, pr.xl, pr.xh) != RMID && region(j, ny, pr.yl, pr.yh) != RMID)
                 gs9(phi, rhs, invd, g, b, homog, nx, ny, i, j, omega);
         }
     }
-    __syncthreads();
+    S::sync();
 }
 
 __global__ void __launch_bounds__(1024) k_gs_boundary(DF phi, DF rhs, DF invd, Geo g, BCd b, int homog, int nx,
                                                       int ny, double omega) {
-    b_gs_boundary(phi, rhs, invd, g, b, homog, nx, ny, omega);
+    b_gs_boundary<BlockScope>(phi, rhs, invd, g, b, homog, nx, ny, omega);
 }
 
 cudaError_t launch_gs_sweep(const DF& phi, const DF& rhs, const DF& invd, const Geo& g, const BCd& b, int homog,
@@ -813,74 +869,92 @@ cudaError_t launch_dd_colour(const DF& phi, const DF& modrhs, const DF& invd, co
 // ---------------------------------------------------------------------------
 #define BLOOP(k, n) for (int k = threadIdx.x; k < (n); k += blockDim.x)
 
+template <class S>
 __device__ void b_fill(const DF& p, const Geo& g, const BCd& b, int homog, int do_neum, int nx, int ny) {
     int lo[4], cnt[4];
     for (int s = 0; s < 4; ++s) side_range(b, s, nx, ny, do_neum, lo[s], cnt[s]);
-    BLOOP(k, cnt[0] + cnt[1]) {
+    SLOOP(k, cnt[0] + cnt[1]) {
         if (k < cnt[0]) fill_side_elem(p, g, b, homog, 0, nx, ny, lo[0] + k);
         else fill_side_elem(p, g, b, homog, 1, nx, ny, lo[1] + k - cnt[0]);
     }
-    __syncthreads();
-    BLOOP(k, cnt[2] + cnt[3]) {
+    S::sync();
+    SLOOP(k, cnt[2] + cnt[3]) {
         if (k < cnt[2]) fill_side_elem(p, g, b, homog, 2, nx, ny, lo[2] + k);
         else fill_side_elem(p, g, b, homog, 3, nx, ny, lo[3] + k - cnt[2]);
     }
-    __syncthreads();
-    if (threadIdx.x < 4) fill_corner(p, b, nx, ny, threadIdx.x);
-    __syncthreads();
+    S::sync();
+    if (S::rank() < 4) fill_corner(p, b, nx, ny, S::rank());
+    S::sync();
 }
 
 // Block-wide sum / max with a fixed combination order (warp shuffles, then the
-// warps' partials in one warp), so the result does not depend on scheduling.
-__device__ double b_sum(double v, double* sh) {
-    for (int o = 16; o > 0; o >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, o);
+// warps' partials in one warp), so the result does not depend on scheduling;
+// in GridScope the CTAs' results are then combined in CTA order by every CTA
+// (partials double-buffered: the barrier inside the next reduction keeps a
+// fast CTA from overwriting partials a slow one still reads).
+template <class S, bool kMax>
+__device__ double b_reduce(double v, double* sh) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const double u = __shfl_down_sync(0xffffffffu, v, o);
+        v = kMax ? fmax(v, u) : v + u;
+    }
     const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if ((threadIdx.x & 31) == 0) sh[w] = v;
     __syncthreads();
     if (w == 0) {
         double x = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, o);
+        for (int o = 16; o > 0; o >>= 1) {
+            const double u = __shfl_down_sync(0xffffffffu, x, o);
+            x = kMax ? fmax(x, u) : x + u;
+        }
         if (threadIdx.x == 0) sh[32] = x;
     }
     __syncthreads();
-    return sh[32];
-}
-
-__device__ double b_max(double v, double* sh) {
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if ((threadIdx.x & 31) == 0) sh[w] = v;
-    __syncthreads();
-    if (w == 0) {
-        double x = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_down_sync(0xffffffffu, x, o));
-        if (threadIdx.x == 0) sh[32] = x;
+    if constexpr (!S::kGrid) {
+        return sh[32];
+    } else {
+        volatile double* part = s_gctl.part + (s_gred & 1) * gridDim.x;
+        if (threadIdx.x == 0) part[blockIdx.x] = sh[32];
+        grid_barrier();
+        if (threadIdx.x == 0) {
+            double t = part[0];
+            for (int c = 1; c < (int)gridDim.x; ++c) t = kMax ? fmax(t, part[c]) : t + part[c];
+            sh[33] = t;
+            s_gred = s_gred + 1;
+        }
+        __syncthreads();
+        return sh[33];
     }
-    __syncthreads();
-    return sh[32];
 }
+template <class S>
+__device__ double b_sum(double v, double* sh) { return b_reduce<S, false>(v, sh); }
+template <class S>
+__device__ double b_max(double v, double* sh) { return b_reduce<S, true>(v, sh); }
 
 // pnorm (AU:753-796) with p = 2 or 0.
+template <class S>
 __device__ double b_pnorm(const DF& a, int nx, int ny, int p, double vol, double* sh) {
     double acc = 0.0;
-    BLOOP(k, nx * ny) {
+    SLOOP(k, nx * ny) {
         const double v = AT(a, k % nx, k / nx);
         acc = (p == 0) ? fmax(acc, fabs(v)) : acc + v * v;
     }
-    if (p == 0) return b_max(acc, sh);
-    return sqrt(vol * b_sum(acc, sh));
+    if (p == 0) return b_max<S>(acc, sh);
+    return sqrt(vol * b_sum<S>(acc, sh));
 }
 
+template <class S>
 __device__ double b_dot(const DF& a, const DF& c, int nx, int ny, double vol, double* sh) {
     double acc = 0.0;
-    BLOOP(k, nx * ny) acc = acc + AT(a, k % nx, k / nx) * AT(c, k % nx, k / nx);
-    return vol * b_sum(acc, sh);
+    SLOOP(k, nx * ny) acc = acc + AT(a, k % nx, k / nx) * AT(c, k % nx, k / nx);
+    return vol * b_sum<S>(acc, sh);
 }
 
 // y = a*y + b*x over [-g, n+g) in both directions (g = 1 for ghosted arrays).
+template <class S>
 __device__ void b_axpby(const DF& y, const DF& x, double a, double bb, int nx, int ny, int g) {
     const int w = nx + 2 * g, h = ny + 2 * g;
-    BLOOP(k, w * h) {
+    SLOOP(k, w * h) {
         const int i = k % w - g, j = k / w - g;
         const double yv = AT(y, i, j), xv = AT(x, i, j);
         double v;
@@ -891,18 +965,20 @@ __device__ void b_axpby(const DF& y, const DF& x, double a, double bb, int nx, i
         else v = a * yv + bb * xv;
         AT(y, i, j) = v;
     }
-    __syncthreads();
+    S::sync();
 }
 
+template <class S>
 __device__ void b_setval(const DF& y, double v, int nx, int ny, int g) {
     const int w = nx + 2 * g, h = ny + 2 * g;
-    BLOOP(k, w * h) AT(y, k % w - g, k / w - g) = v;
-    __syncthreads();
+    SLOOP(k, w * h) AT(y, k % w - g, k / w - g) = v;
+    S::sync();
 }
 
+template <class S>
 __device__ void b_mul(const DF& out, const DF& a, const DF& c, int nx, int ny) {
-    BLOOP(k, nx * ny) AT(out, k % nx, k / nx) = AT(a, k % nx, k / nx) * AT(c, k % nx, k / nx);
-    __syncthreads();
+    SLOOP(k, nx * ny) AT(out, k % nx, k / nx) = AT(a, k % nx, k / nx) * AT(c, k % nx, k / nx);
+    S::sync();
 }
 
 // 9-point sweeps (MG smoother), P2:1460-1988.
@@ -912,6 +988,7 @@ __device__ void b_mul(const DF& out, const DF& a, const DF& c, int nx, int ny) {
 // ranges, the edge cells colour by colour along each non-periodic side, then
 // the corners -- at once when the grid is at least 4 x 4 (their stencils,
 // two cells deep, then neither read nor write each other), else in turn.
+template <class S>
 __device__ void b_sweep9(const DF& phi_, const DF& rhs_, const DF& invd_, const Geo& g_, const BCd& b, int homog,
                          int nx, int ny, double omega) {
     // field descriptors in registers: the level structs live in shared memory,
@@ -938,7 +1015,7 @@ __device__ void b_sweep9(const DF& phi_, const DF& rhs_, const DF& invd_, const 
         fast[c] = (long)cnt[c] * (ccw[c] > 0 ? ccw[c] - 1 : 0) < (1L << 24);
     }
     const int ng = 2 * (nx + 2) + 2 * ny;
-    BLOOP(k, ng) {
+    SLOOP(k, ng) {
         int i, j;
         if (k < nx + 2) { i = k - 1; j = -1; }
         else if (k < 2 * (nx + 2)) { i = k - (nx + 2) - 1; j = ny; }
@@ -946,14 +1023,14 @@ __device__ void b_sweep9(const DF& phi_, const DF& rhs_, const DF& invd_, const 
         else { i = nx; j = k - 2 * (nx + 2) - ny; }
         AT(phi, i, j) = sweep_ghost(DFLoad{phi}, b, homog, nx, ny, i, j);
     }
-    __syncthreads();
+    S::sync();
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-        BLOOP(k, cnt[c]) {
+        SLOOP(k, cnt[c]) {
             const int kj = fast[c] ? fastdiv24(k, cm[c]) : k / ccw[c];
             gs9r(phi, rhs, invd, g, b, homog, ci0[c] + 2 * (k - kj * ccw[c]), cj0[c] + 2 * kj, RMID, RMID, omega);
         }
-        __syncthreads();
+        S::sync();
     }
     const bool sxl = !pr.xl, sxh = !pr.xh, syl = !pr.yl, syh = !pr.yh;
     for (int c = 0; c < 4; ++c) {
@@ -964,23 +1041,23 @@ __device__ void b_sweep9(const DF& phi_, const DF& rhs_, const DF& invd_, const 
         const int n1 = n0 + ((syh && ((ny - 1) & 1) == cj) ? ni : 0);
         const int n2 = n1 + ((sxl && ci == 0) ? nj : 0);
         const int n3 = n2 + ((sxh && ((nx - 1) & 1) == ci) ? nj : 0);
-        BLOOP(k, n3) {
+        SLOOP(k, n3) {
             if (k < n0) gs9r(phi, rhs, invd, g, b, homog, ia + 2 * k, 0, RMID, RLO, omega);
             else if (k < n1) gs9r(phi, rhs, invd, g, b, homog, ia + 2 * (k - n0), ny - 1, RMID, RHI, omega);
             else if (k < n2) gs9r(phi, rhs, invd, g, b, homog, 0, ja + 2 * (k - n1), RLO, RMID, omega);
             else gs9r(phi, rhs, invd, g, b, homog, nx - 1, ja + 2 * (k - n2), RHI, RMID, omega);
         }
-        __syncthreads();
+        S::sync();
     }
     const bool apart = nx >= 4 && ny >= 4;
-    if (apart ? threadIdx.x < 4 : threadIdx.x == 0) {
-        for (int c = apart ? threadIdx.x : 0; c < (apart ? (int)threadIdx.x + 1 : 4); ++c) {
+    if (apart ? S::rank() < 4 : S::rank() == 0) {
+        for (int c = apart ? S::rank() : 0; c < (apart ? S::rank() + 1 : 4); ++c) {
             const int i = (c & 1) ? nx - 1 : 0, j = (c & 2) ? ny - 1 : 0;
             const int xr = region(i, nx, pr.xl, pr.xh), yr = region(j, ny, pr.yl, pr.yh);
             if (xr != RMID && yr != RMID) gs9r(phi, rhs, invd, g, b, homog, i, j, xr, yr, omega);
         }
     }
-    __syncthreads();
+    S::sync();
 }
 
 __device__ __forceinline__ bool fusable_sides(const BCd& b) {
@@ -989,77 +1066,82 @@ __device__ __forceinline__ bool fusable_sides(const BCd& b) {
     return true;
 }
 
+template <class S>
 __device__ void b_relax9(const Lv& L, const DF& phi, const DF& rhs, int homog, double omega, int sweeps) {
     const int nx = L.nx, ny = L.ny;
     if (fusable_sides(L.bc)) {
-        for (int it = 0; it < sweeps; ++it) b_sweep9(phi, rhs, L.invd, L.g, L.bc, homog, nx, ny, omega);
+        for (int it = 0; it < sweeps; ++it) b_sweep9<S>(phi, rhs, L.invd, L.g, L.bc, homog, nx, ny, omega);
         return;
     }
     const int hx = (nx + 1) / 2, hy = (ny + 1) / 2;
     const Per pr = periodic_of(L.bc);
     for (int it = 0; it < sweeps; ++it) {
-        b_fill(phi, L.g, L.bc, homog, 0, nx, ny);
+        b_fill<S>(phi, L.g, L.bc, homog, 0, nx, ny);
         for (int c = 0; c < 4; ++c) {   // interior cells, colour by colour
             const int ci = colour_ci(c), cj = colour_cj(c);
-            BLOOP(k, hx * hy) {
+            SLOOP(k, hx * hy) {
                 const int i = 2 * (k % hx) + ci, j = 2 * (k / hx) + cj;
                 if (i < nx && j < ny && region(i, nx, pr.xl, pr.xh) == RMID && region(j, ny, pr.yl, pr.yh) == RMID)
                     gs9(phi, rhs, L.invd, L.g, L.bc, homog, nx, ny, i, j, omega);
             }
-            __syncthreads();
+            S::sync();
         }
-        b_gs_boundary(phi, rhs, L.invd, L.g, L.bc, homog, nx, ny, omega);
+        b_gs_boundary<S>(phi, rhs, L.invd, L.g, L.bc, homog, nx, ny, omega);
     }
 }
 
 // 5-point red-black sweeps of the deferred-correction smoother (DD:153-334).
 // modrhs is computed once per call, into L.w.
+template <class S>
 __device__ void b_relax_dd(const Lv& L, const DF& phi, const DF& rhs, int homog, double omega, int sweeps) {
     const int nx = L.nx, ny = L.ny;
     if (sweeps == 0) return;
-    BLOOP(k, nx * ny) AT(L.w, k % nx, k / nx) = dd_modrhs(phi, rhs, L.g, nx, ny, k % nx, k / nx);
-    __syncthreads();
+    SLOOP(k, nx * ny) AT(L.w, k % nx, k / nx) = dd_modrhs(phi, rhs, L.g, nx, ny, k % nx, k / nx);
+    S::sync();
     const int hx = (nx + 1) / 2;
     for (int it = 0; it < sweeps; ++it) {
-        b_fill(phi, L.g, L.bc, homog, 1, nx, ny);   // DD:259, neum_ghosts = .true.
+        b_fill<S>(phi, L.g, L.bc, homog, 1, nx, ny);   // DD:259, neum_ghosts = .true.
         for (int colour = 0; colour < 2; ++colour) {
-            BLOOP(k, hx * ny) {
+            SLOOP(k, hx * ny) {
                 const int j = k / hx, i = 2 * (k % hx) + ((colour + j) & 1);
                 if (i < nx) dd_gs(phi, L.w, L.invd, L.g, i, j, omega);
             }
-            __syncthreads();
+            S::sync();
         }
     }
 }
 
 // out = rhs - L[phi] (mode 1) or L[phi] (mode 0); fills phi's ghosts first as the Fortran routines do.
+template <class S>
 __device__ void b_apply(const Lv& L, const DF& out, const DF& phi, const DF& rhs, int homog, int mode, int dd) {
     const int nx = L.nx, ny = L.ny;
     if (dd) {
-        BLOOP(k, nx * ny) {
+        SLOOP(k, nx * ny) {
             const int i = k % nx, j = k / nx;
             const double lap = dd_apply(phi, L.g, L.bc, nx, ny, i, j);
             AT(out, i, j) = mode ? AT(rhs, i, j) - lap : lap;
         }
-        __syncthreads();
-        b_fill(phi, L.g, L.bc, homog, 1, nx, ny);   // ghost state the DD routine leaves (DD:99)
+        S::sync();
+        b_fill<S>(phi, L.g, L.bc, homog, 1, nx, ny);   // ghost state the DD routine leaves (DD:99)
     } else {
-        b_fill(phi, L.g, L.bc, homog, 0, nx, ny);   // P2:935
-        BLOOP(k, nx * ny) {
+        b_fill<S>(phi, L.g, L.bc, homog, 0, nx, ny);   // P2:935
+        SLOOP(k, nx * ny) {
             const int i = k % nx, j = k / nx;
             const double lap = apply9(phi, L.g, L.bc, homog, nx, ny, i, j);
             AT(out, i, j) = mode ? AT(rhs, i, j) - lap : lap;
         }
-        __syncthreads();
+        S::sync();
     }
 }
 
+template <class S>
 __device__ void b_relax(const Lv& L, const DF& phi, const DF& rhs, int homog, double omega, int sweeps, int dd) {
-    if (dd) b_relax_dd(L, phi, rhs, homog, omega, sweeps);
-    else b_relax9(L, phi, rhs, homog, omega, sweeps);
+    if (dd) b_relax_dd<S>(L, phi, rhs, homog, omega, sweeps);
+    else b_relax9<S>(L, phi, rhs, homog, omega, sweeps);
 }
 
 // solve_bicgstab2 (P2:2253-2477; DD:339-566 with dd = 1).  Status: 0 or 3 (non-finite).
+template <class S>
 __device__ int b_bicgstab(const Lv& L, const DF& phi, const DF& rhs, int homog, double tol, int max_iters,
                           int max_restarts, int zerophi, int dd, double* sh) {
     const double reps = 1.0e-12, hang = 1.0e-7, small = 1.0e-30;
@@ -1071,13 +1153,13 @@ __device__ int b_bicgstab(const Lv& L, const DF& phi, const DF& rhs, int homog, 
     double rho[4] = {0, 0, 0, 0}, norm[2], alpha[2] = {0, 0}, beta[2] = {0, 0}, omg[2] = {0, 0};
     int recount = 0, i = 0, restarts = 0, init = 1;
     if (max_iters == 0) return 0;
-    if (zerophi) b_setval(phi, 0.0, nx, ny, 1);
-    b_apply(L, r, phi, rhs, homog, 1, dd);
-    b_axpby(rt, r, 0.0, 1.0, nx, ny, 0);
-    b_setval(e, 0.0, nx, ny, 1);
-    b_setval(pt, 0.0, nx, ny, 1);
-    b_setval(st, 0.0, nx, ny, 1);
-    norm[0] = b_pnorm(r, nx, ny, norm_type, vol, sh);
+    if (zerophi) b_setval<S>(phi, 0.0, nx, ny, 1);
+    b_apply<S>(L, r, phi, rhs, homog, 1, dd);
+    b_axpby<S>(rt, r, 0.0, 1.0, nx, ny, 0);
+    b_setval<S>(e, 0.0, nx, ny, 1);
+    b_setval<S>(pt, 0.0, nx, ny, 1);
+    b_setval<S>(st, 0.0, nx, ny, 1);
+    norm[0] = b_pnorm<S>(r, nx, ny, norm_type, vol, sh);
     const double initial_norm = norm[0], initial_rnorm = norm[0];
     norm[1] = norm[0];
     while (((i < max_iters) && (norm[0] > tol * norm[1])) && (norm[1] > 0.0)) {
@@ -1088,45 +1170,45 @@ __device__ int b_bicgstab(const Lv& L, const DF& phi, const DF& rhs, int homog, 
         omg[1] = omg[0];
         rho[3] = rho[2];
         rho[2] = rho[1];
-        rho[1] = b_dot(rt, r, nx, ny, vol, sh);
+        rho[1] = b_dot<S>(rt, r, nx, ny, vol, sh);
         if (rho[1] == 0.0) {
-            b_axpby(phi, e, 1.0, 1.0, nx, ny, 1);
+            b_axpby<S>(phi, e, 1.0, 1.0, nx, ny, 1);
             return 0;
         }
         if (init) {
-            b_axpby(p, r, 0.0, 1.0, nx, ny, 0);
+            b_axpby<S>(p, r, 0.0, 1.0, nx, ny, 0);
             init = 0;
         } else {
             beta[1] = (rho[1] / rho[2]) * (alpha[1] / omg[1]);
-            BLOOP(k, nx * ny) {
+            SLOOP(k, nx * ny) {
                 const int a = k % nx, c = k / nx;
                 AT(p, a, c) = beta[1] * (AT(p, a, c) - omg[1] * AT(v, a, c)) + AT(r, a, c);
             }
-            __syncthreads();
+            S::sync();
         }
-        b_mul(pt, p, L.invd, nx, ny);
-        b_relax(L, pt, p, 1, relax_omega, 2, dd);
-        b_apply(L, v, pt, p, 1, 0, dd);
-        const double m = b_dot(rt, v, nx, ny, vol, sh);
+        b_mul<S>(pt, p, L.invd, nx, ny);
+        b_relax<S>(L, pt, p, 1, relax_omega, 2, dd);
+        b_apply<S>(L, v, pt, p, 1, 0, dd);
+        const double m = b_dot<S>(rt, v, nx, ny, vol, sh);
         alpha[0] = rho[1] / m;
         if (fabs(m) > small * fabs(rho[1])) {
-            b_axpby(r, v, 1.0, -alpha[0], nx, ny, 0);
-            norm[0] = b_pnorm(r, nx, ny, norm_type, vol, sh);
-            b_axpby(e, pt, 1.0, alpha[0], nx, ny, 1);
+            b_axpby<S>(r, v, 1.0, -alpha[0], nx, ny, 0);
+            norm[0] = b_pnorm<S>(r, nx, ny, norm_type, vol, sh);
+            b_axpby<S>(e, pt, 1.0, alpha[0], nx, ny, 1);
         } else {
-            b_setval(r, 0.0, nx, ny, 0);
+            b_setval<S>(r, 0.0, nx, ny, 0);
             norm[0] = 0.0;
         }
         if ((norm[0] > tol * initial_norm) && (norm[0] > reps * initial_rnorm)) {
-            b_mul(st, r, L.invd, nx, ny);
-            b_relax(L, st, r, 1, relax_omega, 2, dd);
-            b_apply(L, t, st, r, 1, 0, dd);
-            const double tr = b_dot(t, r, nx, ny, vol, sh);
-            const double tt = b_dot(t, t, nx, ny, vol, sh);
+            b_mul<S>(st, r, L.invd, nx, ny);
+            b_relax<S>(L, st, r, 1, relax_omega, 2, dd);
+            b_apply<S>(L, t, st, r, 1, 0, dd);
+            const double tr = b_dot<S>(t, r, nx, ny, vol, sh);
+            const double tt = b_dot<S>(t, t, nx, ny, vol, sh);
             omg[0] = tr / tt;
-            b_axpby(e, st, 1.0, omg[0], nx, ny, 1);
-            b_axpby(r, t, 1.0, -omg[0], nx, ny, 0);
-            norm[0] = b_pnorm(r, nx, ny, norm_type, vol, sh);
+            b_axpby<S>(e, st, 1.0, omg[0], nx, ny, 1);
+            b_axpby<S>(r, t, 1.0, -omg[0], nx, ny, 0);
+            norm[0] = b_pnorm<S>(r, nx, ny, norm_type, vol, sh);
         }
         if ((norm[0] <= tol * initial_norm) || (norm[0] <= reps * initial_rnorm)) break;
         if ((omg[0] == 0.0) || (norm[0] > (1.0 - hang) * norm[1])) {
@@ -1134,31 +1216,32 @@ __device__ int b_bicgstab(const Lv& L, const DF& phi, const DF& rhs, int homog, 
                 recount = 1;
             } else {
                 recount = 0;
-                b_axpby(phi, e, 1.0, 1.0, nx, ny, 1);
+                b_axpby<S>(phi, e, 1.0, 1.0, nx, ny, 1);
                 if (restarts == max_restarts) break;   // then e is added again below (P2:2466)
-                b_apply(L, r, phi, rhs, homog, 1, dd);
-                norm[0] = b_pnorm(r, nx, ny, norm_type, vol, sh);
+                b_apply<S>(L, r, phi, rhs, homog, 1, dd);
+                norm[0] = b_pnorm<S>(r, nx, ny, norm_type, vol, sh);
                 rho[1] = rho[2] = rho[3] = 0.0;
                 alpha[0] = beta[0] = omg[0] = 0.0;
-                b_axpby(rt, r, 0.0, 1.0, nx, ny, 0);
-                b_setval(e, 0.0, nx, ny, 1);
+                b_axpby<S>(rt, r, 0.0, 1.0, nx, ny, 0);
+                b_setval<S>(e, 0.0, nx, ny, 1);
                 restarts = restarts + 1;
                 init = 1;
             }
         }
     }
-    b_axpby(phi, e, 1.0, 1.0, nx, ny, 1);
+    b_axpby<S>(phi, e, 1.0, 1.0, nx, ny, 1);
     return isfinite(norm[0]) ? 0 : 3;
 }
 
 // ---------------------------------------------------------------------------
 // The coarse sub-cycle: vcycle_noinit(d0) run to the bottom in one CTA.
 // ---------------------------------------------------------------------------
+template <class S>
 __device__ void b_prolong(const Lv& F, const Lv& Cl, int refx, int refy, int order, double* sh) {
     // fill_ghosts(crse, homog=.true., do_neum=.true.) (MG:318), then the fused add
-    b_fill(Cl.e, Cl.g, Cl.bc, 1, 1, Cl.nx, Cl.ny);
-    BLOOP(k, Cl.nx * Cl.ny) prolong_cell(F.e, Cl.e, k % Cl.nx, k / Cl.nx, refx, refy, order);
-    __syncthreads();
+    b_fill<S>(Cl.e, Cl.g, Cl.bc, 1, 1, Cl.nx, Cl.ny);
+    SLOOP(k, Cl.nx * Cl.ny) prolong_cell(F.e, Cl.e, k % Cl.nx, k / Cl.nx, refx, refy, order);
+    S::sync();
     const bool rax = (Cl.bc.type[0] == T_PERIODIC && Cl.bc.type[1] == T_PERIODIC) ||
                      (Cl.bc.type[0] == T_NEUM && Cl.bc.type[1] == T_NEUM);
     const bool ray = (Cl.bc.type[2] == T_PERIODIC && Cl.bc.type[3] == T_PERIODIC) ||
@@ -1166,31 +1249,33 @@ __device__ void b_prolong(const Lv& F, const Lv& Cl, int refx, int refy, int ord
     if (rax && ray) {   // MG:371-383
         const double dxprod = F.g.dx * F.g.dy;
         double s = 0.0, vv = 0.0;
-        BLOOP(k, F.nx * F.ny) {
+        SLOOP(k, F.nx * F.ny) {
             const double jj = AT(F.g.J, k % F.nx, k / F.nx);
             s = s + jj * AT(F.e, k % F.nx, k / F.nx);
             vv = vv + jj;
         }
-        const double sum = dxprod * b_sum(s, sh), vol = dxprod * b_sum(vv, sh);
+        const double sum = dxprod * b_sum<S>(s, sh), vol = dxprod * b_sum<S>(vv, sh);
         const double avg = sum / vol;
         const int w = F.nx + 2, h = F.ny + 2;
-        BLOOP(k, w * h) AT(F.e, k % w - 1, k / w - 1) = AT(F.e, k % w - 1, k / w - 1) - avg;
-        __syncthreads();
+        SLOOP(k, w * h) AT(F.e, k % w - 1, k / w - 1) = AT(F.e, k % w - 1, k / w - 1) - avg;
+        S::sync();
     }
 }
 
+template <class S>
 __device__ void b_set_guess(const Lv& L) {
-    BLOOP(k, L.nx * L.ny) AT(L.e, k % L.nx, k / L.nx) = AT(L.r, k % L.nx, k / L.nx) * AT(L.invd, k % L.nx, k / L.nx);
-    __syncthreads();
+    SLOOP(k, L.nx * L.ny) AT(L.e, k % L.nx, k / L.nx) = AT(L.r, k % L.nx, k / L.nx) * AT(L.invd, k % L.nx, k / L.nx);
+    S::sync();
 }
 
 // e = A^{-1} r on the bottom level (MGP_FLAG_DIRECT_COARSE).  ainv holds the
 // inverse transposed, ainv[m * n + k] = (A^{-1})_{k m}; row k takes four
 // threads, each summing a quarter of the row, combined by two shuffles.
 static_assert(4 * kDirectCells <= kCoarseThreads, "four threads per row of the bottom inverse");
+template <class S>
 __device__ void b_direct(const Lv& L, const double* ainv) {
     const int nx = L.nx, n = L.nx * L.ny;
-    const int k = threadIdx.x >> 2, q = threadIdx.x & 3;
+    const int k = S::rank() >> 2, q = S::rank() & 3;
     double s = 0.0;
     if (k < n) {
         const int m0 = q * n / 4, m1 = (q + 1) * n / 4;
@@ -1206,12 +1291,13 @@ __device__ void b_direct(const Lv& L, const double* ainv) {
     s = s + __shfl_xor_sync(0xffffffffu, s, 1);
     s = s + __shfl_xor_sync(0xffffffffu, s, 2);
     if (k < n && q == 0) AT(L.e, k % nx, k / nx) = s;
-    __syncthreads();
+    S::sync();
 }
 
 // vcycle_noinit(d0) down to the bottom and back, on the levels lv[d0..maxdepth]
 // (every thread of the block runs it).  Returns a nonzero status on a
 // non-finite bottom residual.
+template <class S>
 __device__ int coarse_body(const Lv* lv, const CoarseArgs& a, double* sh) {
     int cnt[32];
     const double relax_omega = a.dd ? 4.0 / 5.0 : 1.0;
@@ -1220,25 +1306,25 @@ __device__ int coarse_body(const Lv* lv, const CoarseArgs& a, double* sh) {
 visit:
     {
         const Lv& L = lv[d];
-        if (a.dd) b_set_guess(L);   // DD:931, DD:971
+        if (a.dd) b_set_guess<S>(L);   // DD:931, DD:971
         if (d == a.maxdepth) {
             if (a.ainv) {   // exact bottom solve
-                b_direct(L, a.ainv);
+                b_direct<S>(L, a.ainv);
                 goto up;
             }
-            b_relax(L, L.e, L.r, 1, relax_omega, a.nb, a.dd);
-            const int s = b_bicgstab(L, L.e, L.r, 1, 1.0e-6, 80, 5, 0, a.dd, sh);
+            b_relax<S>(L, L.e, L.r, 1, relax_omega, a.nb, a.dd);
+            const int s = b_bicgstab<S>(L, L.e, L.r, 1, 1.0e-6, 80, 5, 0, a.dd, sh);
             if (s) st = s;
             goto up;
         }
-        b_relax(L, L.e, L.r, 1, relax_omega, a.nd, a.dd);
-        b_apply(L, L.w, L.e, L.r, 1, 1, a.dd);
+        b_relax<S>(L, L.e, L.r, 1, relax_omega, a.nd, a.dd);
+        b_apply<S>(L, L.w, L.e, L.r, 1, 1, a.dd);
         const Lv& Cl = lv[d + 1];
         const int rx = a.refx[d], ry = a.refy[d];
-        BLOOP(k, Cl.nx * Cl.ny) AT(Cl.r, k % Cl.nx, k / Cl.nx) =
+        SLOOP(k, Cl.nx * Cl.ny) AT(Cl.r, k % Cl.nx, k / Cl.nx) =
             restrict_cc(L.w, k % Cl.nx, k / Cl.nx, rx, ry, 1.0 / (rx * ry));
-        __syncthreads();
-        if (!a.dd) b_set_guess(Cl);   // MG:805-806
+        S::sync();
+        if (!a.dd) b_set_guess<S>(Cl);   // MG:805-806
         if (a.numcycles == 0) goto finish;   // `do curcycle = 1, numcycles` runs no coarse visit
         cnt[d] = 0;
         d = d + 1;
@@ -1255,15 +1341,15 @@ up:
 finish:
     {
         const Lv& L = lv[d];
-        b_prolong(L, lv[d + 1], a.refx[d], a.refy[d], 1, sh);
-        b_relax(L, L.e, L.r, 1, relax_omega, a.nu, a.dd);
+        b_prolong<S>(L, lv[d + 1], a.refx[d], a.refy[d], 1, sh);
+        b_relax<S>(L, L.e, L.r, 1, relax_omega, a.nu, a.dd);
     }
     goto up;
 }
 
 __global__ void __launch_bounds__(kCoarseThreads, 1) k_coarse_cycle(CoarseArgs a) {
     __shared__ double sh[kCoarseThreads];
-    const int s = coarse_body(a.lv, a, sh);
+    const int s = coarse_body<BlockScope>(a.lv, a, sh);
     if (threadIdx.x == 0 && s) *a.status = s;
 }
 
@@ -1313,7 +1399,7 @@ __global__ void __launch_bounds__(kCoarseThreads, 1) k_coarse_cycle_smem(CoarseA
     }
     cp_async_wait_all();
     __syncthreads();
-    const int s = coarse_body(sl - a.d0, a, sh);
+    const int s = coarse_body<BlockScope>(sl - a.d0, a, sh);
     for (int k = 0; k < nl; ++k) {
         const Lv &S = sl[k], &G = a.lv[a.d0 + k];
         b_copy(G.e, S.e, -1, S.nx + 1, -1, S.ny + 1);
@@ -1326,10 +1412,10 @@ __global__ void __launch_bounds__(kCoarseThreads) k_direct_columns(Lv L, double*
     const int ld = nx + 2;
     const size_t sz = (size_t)ld * (ny + 2);
     const DF phi{scratch + 2 * sz * k + ld + 1, ld}, out{scratch + (2 * k + 1) * sz + ld + 1, ld};
-    b_setval(phi, 0.0, nx, ny, 1);
+    b_setval<BlockScope>(phi, 0.0, nx, ny, 1);
     if (threadIdx.x == 0) AT(phi, k % nx, k / nx) = 1.0;
     __syncthreads();
-    b_apply(L, out, phi, out, 1, 0, 0);
+    b_apply<BlockScope>(L, out, phi, out, 1, 0, 0);
     BLOOP(m, n) A[(size_t)m * n + k] = AT(out, m % nx, m / nx);
 }
 
@@ -1353,7 +1439,35 @@ cudaError_t coarse_kernels_init() {
     return e;
 }
 
+// The coarse sub-cycle over a cooperative grid of a.grid_ctas CTAs (all
+// resident: one per SM at most), for hierarchies whose coarsest level is too
+// large for one CTA (the schedule stops coarsening at an odd side).
+__global__ void __launch_bounds__(kCoarseThreads, 1) k_coarse_cycle_grid(CoarseArgs a) {
+    __shared__ double sh[kCoarseThreads];
+    if (threadIdx.x == 0) {
+        s_gctl = a.gctl;
+        s_gred = 0;
+    }
+    __syncthreads();
+    const int s = coarse_body<GridScope>(a.lv, a, sh);
+    if (GridScope::rank() == 0 && s) *a.status = s;
+}
+
 cudaError_t launch_coarse_cycle(const CoarseArgs& a, cudaStream_t st) {
+    if (a.grid_ctas > 1) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(a.grid_ctas);
+        cfg.blockDim = dim3(kCoarseThreads);
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        const cudaError_t e = cudaLaunchKernelEx(&cfg, k_coarse_cycle_grid, a);
+        count_launch();
+        return e;
+    }
     if (a.shadow && a.smem_bytes > 0) {
         const cudaError_t e = coarse_kernels_init();
         if (e != cudaSuccess) return e;
@@ -1367,7 +1481,8 @@ cudaError_t launch_coarse_cycle(const CoarseArgs& a, cudaStream_t st) {
 
 __global__ void __launch_bounds__(kCoarseThreads, 1) k_bicgstab(BicgArgs a) {
     __shared__ double sh[kCoarseThreads];
-    const int s = b_bicgstab(a.L, a.phi, a.rhs, a.homog, a.tol, a.max_iters, a.max_restarts, a.zerophi, a.dd, sh);
+    const int s = b_bicgstab<BlockScope>(a.L, a.phi, a.rhs, a.homog, a.tol, a.max_iters, a.max_restarts, a.zerophi,
+                                         a.dd, sh);
     if (threadIdx.x == 0 && s) *a.status = s;
 }
 
@@ -1379,7 +1494,7 @@ cudaError_t launch_bicgstab(const BicgArgs& a, cudaStream_t st) {
 
 __global__ void __launch_bounds__(kCoarseThreads) k_relax_block(Lv L, DF phi, DF rhs, int homog, double omega,
                                                                int sweeps, int dd) {
-    b_relax(L, phi, rhs, homog, omega, sweeps, dd);
+    b_relax<BlockScope>(L, phi, rhs, homog, omega, sweeps, dd);
 }
 
 cudaError_t launch_relax_block(const Lv& L, const DF& phi, const DF& rhs, int homog, double omega, int sweeps,

@@ -11,6 +11,14 @@ namespace mgp {
 enum RedKind { RED_SUMSQ = 0, RED_MAXABS = 1, RED_DOT = 2, RED_JSUM = 3, RED_ABSSUM = 4 };
 
 // Parameters of the single-CTA coarse cycle.
+// Barrier and reduction partials of a cooperative grid running the
+// coarse cycle (k_coarse_cycle_grid).
+struct GridCtl {
+    unsigned* bar;   // [0] arrivals, [1] generation; arrivals 0 at launch
+    double* part;    // 2 x (CTAs) partial sums
+    int* status;     // set to 2 if a barrier wait gives up
+};
+
 struct CoarseArgs {
     const Lv* lv;        // device array of levels
     int d0;              // level the cycle starts at (vcycle_noinit(d0) semantics)
@@ -24,6 +32,8 @@ struct CoarseArgs {
     const Lv* shadow;    // device array: the levels' layout in shared memory (offsets), or nullptr
     int smem_bytes;      // dynamic shared memory the staged levels need
     const double* ainv;  // MGP_FLAG_DIRECT_COARSE: inverse of level maxdepth's operator, transposed, or nullptr
+    int grid_ctas;       // > 1: run as a cooperative grid of this many CTAs (gctl set)
+    GridCtl gctl;
 };
 
 // Largest bottom level solved by its precomputed inverse (cells); b_direct

@@ -114,14 +114,14 @@ def terrain_neumann(n: int, boundary_fluxes, compute_laplacian):
     return v, geo, rhs, bc, soln
 
 
-def batch_problem(i: int, seed: int = 4, nmin: int = 64, nmax: int = 1024):
+def batch_problem(i: int, seed: int = 4, nmin: int = 64, nmax: int = 1024, round_to: int = 16):
     """Problem i of the batched workload (seed*10^6 + i): each side
-    log-uniform in [nmin, nmax], rounded to a multiple of 16 (the reference
+    log-uniform in [nmin, nmax], rounded to a multiple of round_to (the reference
     schedule stops at depth 0 on odd sizes); y stretched by a ratio U[1, 1.08]
     per cell in a wall layer of min(64, ny/4) cells, then sheared by U[0, 25]
     degrees; the 16-mode Fourier rhs of wavy_stretched; homogeneous Dirichlet
     on all sides."""
-    nx, ny, angle, ratio, layer_cells = batch_problem_params(i, seed, nmin, nmax)
+    nx, ny, angle, ratio, layer_cells = batch_problem_params(i, seed, nmin, nmax, round_to)
     v = Box.of_size(nx, ny)
     fmap = G.map_skew_stretch(angle, ratio, layer_cells / ny, ny)
     geo = G.mapped_geometry(v, fmap)
@@ -130,13 +130,13 @@ def batch_problem(i: int, seed: int = 4, nmin: int = 64, nmax: int = 1024):
     return v, geo, rhs, bc
 
 
-def batch_problem_params(i: int, seed: int = 4, nmin: int = 64, nmax: int = 1024):
+def batch_problem_params(i: int, seed: int = 4, nmin: int = 64, nmax: int = 1024, round_to: int = 16):
     """The parameters batch_problem(i) draws: (nx, ny, angle, ratio, layer cells)."""
     rng = np.random.default_rng(seed * 1_000_000 + i)
 
     def side():
         n = math.exp(rng.uniform(math.log(nmin), math.log(nmax)))
-        return int(max(nmin, min(nmax, 16 * round(n / 16))))
+        return int(max(nmin, min(nmax, round_to * round(n / round_to))))
 
     nx, ny = side(), side()
     ratio = float(rng.uniform(1.0, 1.08))
@@ -144,12 +144,12 @@ def batch_problem_params(i: int, seed: int = 4, nmin: int = 64, nmax: int = 1024
     return nx, ny, angle, ratio, min(64, ny // 4)
 
 
-def batch_problem_device(i: int, seed: int = 4, nmin: int = 64, nmax: int = 1024):
+def batch_problem_device(i: int, seed: int = 4, nmin: int = 64, nmax: int = 1024, round_to: int = 16):
     """batch_problem(i) with the geometry and the rhs generated on the device
     (mgp_map_geometry, mgp_map_fourier_rhs): equal to the host version to the
     rounding of the map's transcendentals."""
     from . import api as M
-    nx, ny, angle, ratio, layer_cells = batch_problem_params(i, seed, nmin, nmax)
+    nx, ny, angle, ratio, layer_cells = batch_problem_params(i, seed, nmin, nmax, round_to)
     v = Box.of_size(nx, ny)
     params = (math.tan(math.radians(angle)), ratio, float(layer_cells), float(ny))
     geo = M.map_geometry(v, M.MAP_SKEW_LAYER, params)

@@ -292,6 +292,56 @@ def test_dc_vcycle(M):
     assert same(fa.data, fb.data)   # rhs*J/J written back exactly like the reference
 
 
+@pytest.mark.parametrize("kind", ["mg", "dd"])
+def test_grid_coarse_cycle_matches_oracle(M, kind):
+    """Depth capped at 1 on 256^2 leaves a 128 x 128 bottom (16384 cells, as an
+    odd side leaves on many grids): the coarse cycle -- the bottom's 8 sweeps
+    and BiCGStab -- then runs as a cooperative grid of CTAs.  Its reductions
+    combine in another order than the oracle's, and BiCGStab's iterates
+    amplify that rounding: the bottom solve (to 1e-6) differs at that level,
+    so the histories agree to 1e-3 relative, not to rounding.  Same V-cycle
+    count, and the converged solutions agree to 1e-9 of the maximum."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, u = W.identity_dirichlet(256)
+    pa, pb = BoxData(v, 1, 1), BoxData(v, 1, 1)
+    if kind == "mg":
+        old = _set_coupled(M, True)
+        try:
+            ra = O.vcycle(pa, rhs, geo, bc, True, 1e-10, 30, maxdepth_user=1, gs_order=1)
+            rb = M.vcycle(pb, rhs, geo, bc, True, 1e-10, 30, maxdepth_user=1)
+        finally:
+            _set_coupled(M, old)
+    else:
+        f = rhs.copy()
+        f.interior()[:] /= geo.J.interior()
+        fa, fb = f.copy(), f.copy()
+        ra = O.dc_vcycle(pa, fa, geo, bc, True, 1e-10, 60, maxdepth_user=1, smooth_down=8, smooth_up=8,
+                         smooth_bottom=8, gs_order=1)
+        rb = M.dc_vcycle(pb, fb, geo, bc, True, 1e-10, 60, maxdepth_user=1, smooth_down=8, smooth_up=8,
+                         smooth_bottom=8)
+    assert rb.status == 0 and rb.maxdepth == 1
+    assert rb.iterations == ra.iterations
+    np.testing.assert_allclose(rb.relres, ra.relres, rtol=1e-3, atol=1e-14)
+    np.testing.assert_allclose(pb.interior(), pa.interior(), rtol=0, atol=1e-9 * np.abs(pa.interior()).max())
+
+
+def test_grid_coarse_cycle_in_resident_solver(M):
+    """The resident solver with the grid coarse cycle inside its replayed
+    V-cycle graphs (BiCGStab-accelerated): converges, and a second solve on
+    the same hierarchy gives the same bits."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, u = W.identity_dirichlet(256)
+    fl = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV
+    outs = []
+    with M.Solver(v, geo, bc, KIND_MG, fl, maxdepth_user=1) as s:
+        for _ in range(2):
+            p = BoxData(v, 1, 1)
+            r = s.vcycle(p, rhs, bc, True, 1e-10, 100)
+            assert r.status == 0 and r.final_relres <= 1e-10
+            outs.append(p)
+    assert same(outs[0].data, outs[1].data)
+
+
 def test_resident_solver_equals_oneshot_and_device_arrays(M):
     from mgpoisson2d_b200 import workloads as W
     v, geo, rhs, bc, u = W.wavy_stretched(64)
