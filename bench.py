@@ -22,8 +22,10 @@ batched workload: sides log-uniform in [64,1024]): "batched" (all problems as
 one mgp_batch on 16 streams vs one after another) and "served" (Poisson
 arrivals into an mgp_server with resident hierarchies; p50/p99 latency), and
 "precision_study": mixed precision against FP64 and against the exact solution
-of a manufactured problem on the skewed, stretched grid at 512..4096, with the
-observed order of the discretisation error.
+of a manufactured problem on the skewed, stretched grid at 512..4096, for the
+BiCGStab(V-cycle) solve and the deferred-correction solve, with the observed
+order of the discretisation error.  --serve-sweep adds "served_sweep" (the
+served workload over arrival rates 10..3000/s, sides 32..2048; minutes).
 
 --impl reference times the CPU restatement of the reference algorithm (the
 reference is Fortran and no Fortran compiler exists on these hosts) on all
@@ -451,26 +453,39 @@ def vcycle_bytes(M, v, mixed, direct, nu=NU):
 def precision_study(M, sizes):
     """Mixed precision against FP64 and against the exact solution on the
     skewed, boundary-layer-stretched manufactured problem (u = e^x cos 4 pi y,
-    Dirichlet data at the face centres, metric generated on the device):
-    V-cycles, solve time, relative max / L2 error against u, the mixed
-    solution's distance from the FP64 one, and the observed order
-    log2(e_n / e_2n) of the discretisation error."""
+    Dirichlet data at the face centres, metric generated on the device), for
+    two solvers: BiCGStab(V-cycle) with the exact bottom ("mixed", "fp64") and
+    the deferred-correction solve, DD V-cycles inside the FP64 9-point
+    residual loop, nu = 8/8/8 ("dc_mixed", "dc_fp64").  Per solve: V-cycles
+    (DC iterations), time, relative max / L2 error against u; per pair the
+    mixed solution's distance from the FP64 one; per size step the observed
+    order log2(e_n / e_2n) of the discretisation error."""
     import torch
     from mgpoisson2d_b200 import workloads as W
     from mgpoisson2d_b200.types import BoxData
     kry = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV | M.FLAG_DIRECT_COARSE
+    solvers = (("mixed", M.KIND_MG, kry | M.FLAG_MIXED), ("fp64", M.KIND_MG, kry),
+               ("dc_mixed", M.KIND_DD, M.FLAG_MIXED), ("dc_fp64", M.KIND_DD, 0))
     stream = torch.cuda.current_stream()
     rows = []
     for n in sizes:
         v, geo, rhs, bc, u = W.skew_stretched_device(n)
+        f = BoxData.device_zeros(v)   # the DC solve takes f; rhs = J f
+        f.data[:] = rhs.data / geo.J.data[1:-1, 1:-1]
         row = {"n": n}
         sol = {}
-        for name, fl in (("mixed", kry | M.FLAG_MIXED), ("fp64", kry)):
-            with M.Solver(v, geo, bc, M.KIND_MG, fl) as s:
+        for name, kind, fl in solvers:
+            with M.Solver(v, geo, bc, kind, fl) as s:
                 phi = BoxData.device_zeros(v, 1, 1)
+                if kind == M.KIND_DD:
+                    ff = BoxData.device_zeros(v)
+                    ff.data[:] = f.data
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-                r = s.vcycle(phi, rhs, bc, False, TOL, MAXITERS)
+                if kind == M.KIND_DD:
+                    r = s.dc_vcycle(phi, ff, bc, False, TOL, MAXITERS, 1, 8, 8, 8)
+                else:
+                    r = s.vcycle(phi, rhs, bc, False, TOL, MAXITERS)
                 e1.record(stream)
                 e1.synchronize()
             p = phi.data[1:-1, 1:-1]
@@ -478,17 +493,20 @@ def precision_study(M, sizes):
             row[name] = {"vcycles": r.iterations, "final_relres": r.final_relres, "ms": e0.elapsed_time(e1),
                          "err_max": float((p - u).abs().max() / u.abs().max()),
                          "err_l2": float(torch.linalg.norm(p - u) / torch.linalg.norm(u))}
-        d = sol["mixed"] - sol["fp64"]
-        row["mixed_vs_fp64"] = {"rel_l2": float(torch.linalg.norm(d) / torch.linalg.norm(sol["fp64"])),
-                                "rel_max": float(d.abs().max() / sol["fp64"].abs().max())}
+        for a, b, key in (("mixed", "fp64", "mixed_vs_fp64"), ("dc_mixed", "dc_fp64", "dc_mixed_vs_fp64")):
+            d = sol[a] - sol[b]
+            row[key] = {"rel_l2": float(torch.linalg.norm(d) / torch.linalg.norm(sol[b])),
+                        "rel_max": float(d.abs().max() / sol[b].abs().max())}
         rows.append(row)
-        del v, geo, rhs, bc, u, sol, d
+        del v, geo, rhs, bc, u, f, sol
     for a, b in zip(rows, rows[1:]):
-        for name in ("mixed", "fp64"):
+        for name, _, _ in solvers:
             b[name]["order_l2"] = math.log2(a[name]["err_l2"] / b[name]["err_l2"]) / math.log2(b["n"] / a["n"])
     torch.cuda.empty_cache()
     return {"workload": "skew_stretched (30 deg skew, 1.05 boundary-layer stretch, u = e^x cos 4 pi y)",
-            "tol": TOL, "solver": "bicgstab(vcycle), exact bottom", "rows": rows}
+            "tol": TOL, "solvers": {"mixed / fp64": "bicgstab(vcycle), exact bottom",
+                                    "dc_mixed / dc_fp64": "deferred correction (dc_vcycle), nu 8/8/8"},
+            "rows": rows}
 
 
 def main():

@@ -140,7 +140,7 @@ typedef struct mgp_report {
  * the Fortran vcycle is a stationary iteration only.  On strongly stretched
  * grids it needs several times fewer V-cycles for the same tolerance. */
 #define MGP_FLAG_KRYLOV 4
-/* vcycle only: run the V-cycle's grid levels (every level above the
+/* vcycle and dc_vcycle: run the V-cycle's grid levels (every level above the
  * single-CTA coarse cycle) in FP32 inside the FP64 outer iteration.  The
  * residual, the solution update, the convergence test and the coarse levels
  * with the bottom solve stay FP64; geometry and inverse diagonals are the

@@ -553,7 +553,8 @@ __device__ __forceinline__ T restrict_cc(const DFT<T>& f, int ci, int cj, int re
 // Deferred-correction operators, DD:45-334
 // ---------------------------------------------------------------------------
 // Value of phi at (i,j) after extrapolate_ghosts(phi, 0): indices clamped to the valid region.
-__device__ __forceinline__ double clampv(const DF& p, int nx, int ny, int i, int j) {
+template <class T>
+__device__ __forceinline__ T clampv(const DFT<T>& p, int nx, int ny, int i, int j) {
     i = i < 0 ? 0 : (i > nx - 1 ? nx - 1 : i);
     j = j < 0 ? 0 : (j > ny - 1 ? ny - 1 : j);
     return AT(p, i, j);
@@ -562,7 +563,8 @@ __device__ __forceinline__ double clampv(const DF& p, int nx, int ny, int i, int
 // Value of phi at a neighbour after fill_ghosts with LAH BCs (AU:935-936, AU:1135-1136):
 // Dirichlet ghost = -cell, Neumann ghost = cell, periodic = wrapped.  (i,j) is a
 // valid cell and (di,dj) a unit step.
-__device__ __forceinline__ double lahv(const DF& p, const BCd& b, int nx, int ny, int i, int j, int di, int dj) {
+template <class T>
+__device__ __forceinline__ T lahv(const DFT<T>& p, const BCd& b, int nx, int ny, int i, int j, int di, int dj) {
     const int ii = i + di, jj = j + dj;
     int s = -1;
     if (ii < 0) s = S_XLO;
@@ -580,54 +582,63 @@ __device__ __forceinline__ double lahv(const DF& p, const BCd& b, int nx, int ny
     return AT(p, ii, jj);   // other types leave the ghost as stored
 }
 
+// The three DD routines below are written for both field types; for FP64 the
+// operations are those of the Fortran routines in their order (T(x) of a
+// double is x), for FP32 the same operations in single precision.
+
 // Lagged corner cross terms of the DD smoother's modified rhs (DD:226-250).
-__device__ __forceinline__ double dd_modrhs(const DF& phi, const DF& rhs, const Geo& g, int nx, int ny, int i, int j) {
-    const double xyscale = 0.5 * g.idx * g.idy;
-    const double pne = clampv(phi, nx, ny, i + 1, j + 1), pnw = clampv(phi, nx, ny, i - 1, j + 1);
-    const double psw = clampv(phi, nx, ny, i - 1, j - 1), pse = clampv(phi, nx, ny, i + 1, j - 1);
-    const double gxye = AT(g.xy, i + 1, j) * (pne - pse);
-    const double gxyw = AT(g.xy, i, j) * (pnw - psw);
-    const double gyxn = AT(g.yx, i, j + 1) * (pne - pnw);
-    const double gyxs = AT(g.yx, i, j) * (pse - psw);
+template <class T>
+__device__ __forceinline__ T dd_modrhs(const DFT<T>& phi, const DFT<T>& rhs, const GeoT<T>& g, int nx, int ny, int i,
+                                       int j) {
+    const T xyscale = T(0.5 * g.idx * g.idy);
+    const T pne = clampv(phi, nx, ny, i + 1, j + 1), pnw = clampv(phi, nx, ny, i - 1, j + 1);
+    const T psw = clampv(phi, nx, ny, i - 1, j - 1), pse = clampv(phi, nx, ny, i + 1, j - 1);
+    const T gxye = AT(g.xy, i + 1, j) * (pne - pse);
+    const T gxyw = AT(g.xy, i, j) * (pnw - psw);
+    const T gyxn = AT(g.yx, i, j + 1) * (pne - pnw);
+    const T gyxs = AT(g.yx, i, j) * (pse - psw);
     return AT(rhs, i, j) - (gxye - gxyw + gyxn - gyxs) * xyscale;
 }
 
 // DD compute_laplacian (DD:45-119) at (i,j), reading phi's valid cells only.
-__device__ __forceinline__ double dd_apply(const DF& phi, const Geo& g, const BCd& b, int nx, int ny, int i, int j) {
-    const double xyscale = 0.25 * g.idx * g.idy;
-    double pe = clampv(phi, nx, ny, i + 1, j), pw = clampv(phi, nx, ny, i - 1, j);
-    double pn = clampv(phi, nx, ny, i, j + 1), ps = clampv(phi, nx, ny, i, j - 1);
-    const double pne = clampv(phi, nx, ny, i + 1, j + 1), pnw = clampv(phi, nx, ny, i - 1, j + 1);
-    const double psw = clampv(phi, nx, ny, i - 1, j - 1), pse = clampv(phi, nx, ny, i + 1, j - 1);
-    const double gxye = AT(g.xy, i + 1, j) * (pne - pse + pn - ps);
-    const double gxyw = AT(g.xy, i, j) * (pn - ps + pnw - psw);
-    const double gyxn = AT(g.yx, i, j + 1) * (pne - pnw + pe - pw);
-    const double gyxs = AT(g.yx, i, j) * (pe - pw + pse - psw);
-    const double cross = (gxye - gxyw + gyxn - gyxs) * xyscale;
-    const double p = AT(phi, i, j);
+template <class T>
+__device__ __forceinline__ T dd_apply(const DFT<T>& phi, const GeoT<T>& g, const BCd& b, int nx, int ny, int i, int j) {
+    const T xyscale = T(0.25 * g.idx * g.idy), idx = T(g.idx), idy = T(g.idy);
+    T pe = clampv(phi, nx, ny, i + 1, j), pw = clampv(phi, nx, ny, i - 1, j);
+    T pn = clampv(phi, nx, ny, i, j + 1), ps = clampv(phi, nx, ny, i, j - 1);
+    const T pne = clampv(phi, nx, ny, i + 1, j + 1), pnw = clampv(phi, nx, ny, i - 1, j + 1);
+    const T psw = clampv(phi, nx, ny, i - 1, j - 1), pse = clampv(phi, nx, ny, i + 1, j - 1);
+    const T gxye = AT(g.xy, i + 1, j) * (pne - pse + pn - ps);
+    const T gxyw = AT(g.xy, i, j) * (pn - ps + pnw - psw);
+    const T gyxn = AT(g.yx, i, j + 1) * (pne - pnw + pe - pw);
+    const T gyxs = AT(g.yx, i, j) * (pe - pw + pse - psw);
+    const T cross = (gxye - gxyw + gyxn - gyxs) * xyscale;
+    const T p = AT(phi, i, j);
     pe = lahv(phi, b, nx, ny, i, j, 1, 0);
     pw = lahv(phi, b, nx, ny, i, j, -1, 0);
     pn = lahv(phi, b, nx, ny, i, j, 0, 1);
     ps = lahv(phi, b, nx, ny, i, j, 0, -1);
-    const double xfe = AT(g.xx, i + 1, j) * (pe - p) * g.idx;
-    const double xfw = AT(g.xx, i, j) * (p - pw) * g.idx;
-    const double yfn = AT(g.yy, i, j + 1) * (pn - p) * g.idy;
-    const double yfs = AT(g.yy, i, j) * (p - ps) * g.idy;
-    return cross + (xfe - xfw) * g.idx + (yfn - yfs) * g.idy;
+    const T xfe = AT(g.xx, i + 1, j) * (pe - p) * idx;
+    const T xfw = AT(g.xx, i, j) * (p - pw) * idx;
+    const T yfn = AT(g.yy, i, j + 1) * (pn - p) * idy;
+    const T yfs = AT(g.yy, i, j) * (p - ps) * idy;
+    return cross + (xfe - xfw) * idx + (yfn - yfs) * idy;
 }
 
 // One DD Gauss-Seidel update (DD:288-306); phi's ghosts hold the LAH fill.
-__device__ __forceinline__ void dd_gs(const DF& phi, const DF& modrhs, const DF& invd, const Geo& g, int i, int j,
-                                      double omega) {
-    const double p = AT(phi, i, j), pe = AT(phi, i + 1, j), pw = AT(phi, i - 1, j);
-    const double pn = AT(phi, i, j + 1), ps = AT(phi, i, j - 1);
-    const double xfe = AT(g.xx, i + 1, j) * (pe - p) * g.idx;
-    const double xfw = AT(g.xx, i, j) * (p - pw) * g.idx;
-    const double yfn = AT(g.yy, i, j + 1) * (pn - p) * g.idy;
-    const double yfs = AT(g.yy, i, j) * (p - ps) * g.idy;
-    const double lphi = (xfe - xfw) * g.idx + (yfn - yfs) * g.idy;
-    const double newphi = p + (AT(modrhs, i, j) - lphi) * AT(invd, i, j);
-    AT(phi, i, j) = omega * newphi + (1.0 - omega) * p;
+template <class T>
+__device__ __forceinline__ void dd_gs(const DFT<T>& phi, const DFT<T>& modrhs, const DFT<T>& invd, const GeoT<T>& g,
+                                      int i, int j, double omega) {
+    const T idx = T(g.idx), idy = T(g.idy);
+    const T p = AT(phi, i, j), pe = AT(phi, i + 1, j), pw = AT(phi, i - 1, j);
+    const T pn = AT(phi, i, j + 1), ps = AT(phi, i, j - 1);
+    const T xfe = AT(g.xx, i + 1, j) * (pe - p) * idx;
+    const T xfw = AT(g.xx, i, j) * (p - pw) * idx;
+    const T yfn = AT(g.yy, i, j + 1) * (pn - p) * idy;
+    const T yfs = AT(g.yy, i, j) * (p - ps) * idy;
+    const T lphi = (xfe - xfw) * idx + (yfn - yfs) * idy;
+    const T newphi = p + (AT(modrhs, i, j) - lphi) * AT(invd, i, j);
+    AT(phi, i, j) = T(omega) * newphi + T(1.0 - omega) * p;
 }
 
 }  // namespace mgp

@@ -341,11 +341,10 @@ double* red_out(mgp_solver* s) { return s->d_red + 2 * 296; }
 
 // The mixed-precision V-cycle: MGP_FLAG_MIXED on a vcycle/fmg solver whose
 // grid path has at least one level.
-bool mixed(const mgp_solver* s) { return (s->flags & MGP_FLAG_MIXED) && s->kind == MGP_KIND_MG && s->dc > 0; }
+bool mixed(const mgp_solver* s) {
+    return (s->flags & MGP_FLAG_MIXED) && (s->kind == MGP_KIND_MG || s->kind == MGP_KIND_DD) && s->dc > 0;
+}
 
-// FP32 copies of the grid-path levels: geometry and inverse diagonals rounded
-// from the FP64 hierarchy (built first, so the coarse operators are the FP64
-// restrictions), corrections, right-hand sides and work arrays in FP32.
 // Inverse of an n x n matrix (row-major) by Gauss-Jordan elimination with
 // partial pivoting; false if a pivot falls below 1e-13 of the largest entry
 // (the matrix is singular to working precision).
@@ -437,6 +436,9 @@ int build_direct_coarse(mgp_solver* s, cudaStream_t st) {
     return MGP_OK;
 }
 
+// FP32 copies of the grid-path levels: geometry and inverse diagonals rounded
+// from the FP64 hierarchy (built first, so the coarse operators are the FP64
+// restrictions), corrections, right-hand sides and work arrays in FP32.
 int build_fp32_levels(mgp_solver* s) {
     cudaStream_t st = s->stream;
     s->lv32.assign(s->dc, mgp_solver::Lv32{});
@@ -787,7 +789,8 @@ int vcycle_noinit(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
 }
 
 // The mixed-precision V-cycle from grid level d < dc: the same schedule and
-// kernels as vcycle_noinit on the FP32 copies of the grid-path levels; the
+// kernels as vcycle_noinit on the FP32 copies of the grid-path levels (the 9-
+// point sweeps and residual for MG, the DD smoother and residual for DD); the
 // restriction into level dc writes the FP64 right-hand side of the coarse
 // CTA's levels (which, with the bottom solve, stay FP64) and the prolongation
 // from level dc reads its FP64 correction.
@@ -795,8 +798,20 @@ int vcycle32(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
     auto& L = s->lv32[d];
     const Lv& F = s->lv[d];   // BCs of the level
     cudaStream_t st = s->stream;
+    const bool dd = (s->kind == MGP_KIND_DD);
+    if (dd) CK(launch_set_guess(L.e, L.r, L.invd, L.nx, L.ny, st));   // DD:971
     auto smooth32 = [&](int nu_) -> int {
         return timed_smooth(s, d, nu_, [&]() -> int {
+            if (dd) {
+                if (nu_ <= 0) return MGP_OK;
+                CK(launch_dd_modrhs(L.w, L.e, L.r, L.g, L.nx, L.ny, st));   // DD:226-250
+                for (int k = 0; k < nu_; ++k) {
+                    CK(launch_fill(L.e, L.g, F.bc, 1, 1, L.nx, L.ny, st));   // DD:259
+                    CK(launch_dd_colour(L.e, L.w, L.invd, L.g, L.nx, L.ny, 4.0 / 5.0, 0, st));
+                    CK(launch_dd_colour(L.e, L.w, L.invd, L.g, L.nx, L.ny, 4.0 / 5.0, 1, st));
+                }
+                return MGP_OK;
+            }
             for (int k = 0; k < nu_; ++k) {
                 CK(launch_sweep9(L.e, L.e2, L.r, L.invd, L.g, F.bc, 1, L.nx, L.ny, 1.0, &s->tma32[d], s->d_status,
                                  st));
@@ -806,21 +821,26 @@ int vcycle32(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
         });
     };
     RC(smooth32(nd));
-    CK(launch_fill(L.e, L.g, F.bc, 1, 0, L.nx, L.ny, st));
-    CK(launch_apply(L.w, L.e, L.r, L.g, F.bc, 1, L.nx, L.ny, 1, 0, st));
+    if (dd) {
+        CK(launch_dd_apply(L.w, L.e, L.r, L.g, F.bc, L.nx, L.ny, 1, st));
+        CK(launch_fill(L.e, L.g, F.bc, 1, 1, L.nx, L.ny, st));
+    } else {
+        CK(launch_fill(L.e, L.g, F.bc, 1, 0, L.nx, L.ny, st));
+        CK(launch_apply(L.w, L.e, L.r, L.g, F.bc, 1, L.nx, L.ny, 1, 0, st));
+    }
     const int rx = s->refx[d], ry = s->refy[d];
     const bool fine_next = d + 1 < s->dc;
     Lv& C = s->lv[d + 1];
     if (fine_next) {
         auto& N = s->lv32[d + 1];
         CK(launch_restrict(L.w, N.r, N.nx, N.ny, rx, ry, st));
-        CK(launch_set_guess(N.e, N.r, N.invd, N.nx, N.ny, st));   // MG:805-806
+        if (!dd) CK(launch_set_guess(N.e, N.r, N.invd, N.nx, N.ny, st));   // MG:805-806
         for (int c = 1; c <= numcycles; ++c) RC(vcycle32(s, d + 1, numcycles, nd, nu, nb));
         CK(launch_fill(N.e, N.g, C.bc, 1, 1, N.nx, N.ny, st));    // MG:318
         CK(launch_prolong(L.e, N.e, N.nx, N.ny, rx, ry, 1, st));
     } else {
         CK(launch_restrict(L.w, C.r, C.nx, C.ny, rx, ry, st));
-        CK(launch_set_guess(C.e, C.r, C.invd, C.nx, C.ny, st));
+        if (!dd) CK(launch_set_guess(C.e, C.r, C.invd, C.nx, C.ny, st));
         for (int c = 1; c <= numcycles; ++c) RC(vcycle_noinit(s, d + 1, numcycles, nd, nu, nb));
         CK(launch_fill(C.e, C.g, C.bc, 1, 1, C.nx, C.ny, st));
         CK(launch_prolong(L.e, C.e, C.nx, C.ny, rx, ry, 1, st));
@@ -1100,7 +1120,13 @@ int solver_solve(mgp_solver* s, int which, mgp_array* phi, mgp_array* rhs, const
     for (int iter = 1; !krylov && iter <= maxiters && status == MGP_OK; ++iter) {
         if (which == 0) RC(vcycle_top(s, L0.r, numcycles, nd, nu, nb));   // MG:600-606
         else if (which == 1) RC(fmg_noinit(s, 0, numcycles, nd, nu, nb));
-        else RC(vcycle_run(s, 0, numcycles, nd, nu, nb, false));
+        else if (!mixed(s)) RC(vcycle_run(s, 0, numcycles, nd, nu, nb, false));
+        else {   // DD with FP32 grid levels: the residual rounded in, the correction widened out
+            auto& M = s->lv32[0];
+            CK(launch_convert(M.r, L0.r, nx, ny, 0, 0, st));
+            RC(vcycle_run(s, 0, numcycles, nd, nu, nb, true));
+            CK(launch_convert(L0.e, M.e, nx, ny, 1, 1, st));
+        }
         CK(launch_axpby(s->phi0, L0.e, 1.0, 1.0, nx, ny, 1, 1, st));   // MG:611 (whole array)
         CK(launch_fill(s->phi0, L0.g, ubc, homog, 0, nx, ny, st));
         CK(launch_apply(L0.r, s->phi0, s->rhs0, L0.g, ubc, homog, nx, ny, 1, 0, st));

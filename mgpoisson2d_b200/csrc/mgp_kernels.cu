@@ -820,35 +820,57 @@ cudaError_t launch_dd_invdiag(const DF& invd, const Geo& g, int nx, int ny, cuda
     return cudaGetLastError();
 }
 
-__global__ void k_dd_apply(DF out, DF phi, DF rhs, Geo g, BCd b, int nx, int ny, int mode) {
+template <class T>
+__global__ void k_dd_apply(DFT<T> out, DFT<T> phi, DFT<T> rhs, GeoT<T> g, BCd b, int nx, int ny, int mode) {
     CELL_IJ
     if (i >= nx || j >= ny) return;
-    const double lap = dd_apply(phi, g, b, nx, ny, i, j);
+    const T lap = dd_apply(phi, g, b, nx, ny, i, j);
     AT(out, i, j) = mode ? AT(rhs, i, j) - lap : lap;
 }
 
-cudaError_t launch_dd_apply(const DF& out, const DF& phi, const DF& rhs, const Geo& g, const BCd& b, int nx, int ny,
-                            int mode, cudaStream_t st) {
-    k_dd_apply<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(out, phi, rhs, g, b, nx, ny, mode);
+template <class T>
+cudaError_t dd_apply_impl(const DFT<T>& out, const DFT<T>& phi, const DFT<T>& rhs, const GeoT<T>& g, const BCd& b,
+                          int nx, int ny, int mode, cudaStream_t st) {
+    k_dd_apply<T><<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(out, phi, rhs, g, b, nx, ny, mode);
     count_launch();
     return cudaGetLastError();
 }
+cudaError_t launch_dd_apply(const DF& out, const DF& phi, const DF& rhs, const Geo& g, const BCd& b, int nx, int ny,
+                            int mode, cudaStream_t st) {
+    return dd_apply_impl(out, phi, rhs, g, b, nx, ny, mode, st);
+}
+cudaError_t launch_dd_apply(const DF32& out, const DF32& phi, const DF32& rhs, const Geo32& g, const BCd& b, int nx,
+                            int ny, int mode, cudaStream_t st) {
+    return dd_apply_impl(out, phi, rhs, g, b, nx, ny, mode, st);
+}
 
-__global__ void k_dd_modrhs(DF out, DF phi, DF rhs, Geo g, int nx, int ny) {
+template <class T>
+__global__ void k_dd_modrhs(DFT<T> out, DFT<T> phi, DFT<T> rhs, GeoT<T> g, int nx, int ny) {
     CELL_IJ
     if (i >= nx || j >= ny) return;
     AT(out, i, j) = dd_modrhs(phi, rhs, g, nx, ny, i, j);
 }
 
-cudaError_t launch_dd_modrhs(const DF& out, const DF& phi, const DF& rhs, const Geo& g, int nx, int ny,
-                             cudaStream_t st) {
-    k_dd_modrhs<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(out, phi, rhs, g, nx, ny);
+template <class T>
+cudaError_t dd_modrhs_impl(const DFT<T>& out, const DFT<T>& phi, const DFT<T>& rhs, const GeoT<T>& g, int nx, int ny,
+                           cudaStream_t st) {
+    k_dd_modrhs<T><<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(out, phi, rhs, g, nx, ny);
     count_launch();
     return cudaGetLastError();
 }
+cudaError_t launch_dd_modrhs(const DF& out, const DF& phi, const DF& rhs, const Geo& g, int nx, int ny,
+                             cudaStream_t st) {
+    return dd_modrhs_impl(out, phi, rhs, g, nx, ny, st);
+}
+cudaError_t launch_dd_modrhs(const DF32& out, const DF32& phi, const DF32& rhs, const Geo32& g, int nx, int ny,
+                             cudaStream_t st) {
+    return dd_modrhs_impl(out, phi, rhs, g, nx, ny, st);
+}
 
 // Red-black colour of DD:262-285 (parity of i+j relative to the valid corner).
-__global__ void k_dd_colour(DF phi, DF modrhs, DF invd, Geo g, int nx, int ny, double omega, int colour) {
+template <class T>
+__global__ void k_dd_colour(DFT<T> phi, DFT<T> modrhs, DFT<T> invd, GeoT<T> g, int nx, int ny, double omega,
+                            int colour) {
     const int jj = blockIdx.y * blockDim.y + threadIdx.y;
     const int ii = blockIdx.x * blockDim.x + threadIdx.x;
     if (jj >= ny) return;
@@ -857,11 +879,21 @@ __global__ void k_dd_colour(DF phi, DF modrhs, DF invd, Geo g, int nx, int ny, d
     dd_gs(phi, modrhs, invd, g, i, jj, omega);
 }
 
-cudaError_t launch_dd_colour(const DF& phi, const DF& modrhs, const DF& invd, const Geo& g, int nx, int ny,
-                             double omega, int colour, cudaStream_t st) {
-    k_dd_colour<<<cells_grid((nx + 1) / 2, ny, kBlk2), kBlk2, 0, st>>>(phi, modrhs, invd, g, nx, ny, omega, colour);
+template <class T>
+cudaError_t dd_colour_impl(const DFT<T>& phi, const DFT<T>& modrhs, const DFT<T>& invd, const GeoT<T>& g, int nx,
+                           int ny, double omega, int colour, cudaStream_t st) {
+    k_dd_colour<T><<<cells_grid((nx + 1) / 2, ny, kBlk2), kBlk2, 0, st>>>(phi, modrhs, invd, g, nx, ny, omega,
+                                                                         colour);
     count_launch();
     return cudaGetLastError();
+}
+cudaError_t launch_dd_colour(const DF& phi, const DF& modrhs, const DF& invd, const Geo& g, int nx, int ny,
+                             double omega, int colour, cudaStream_t st) {
+    return dd_colour_impl(phi, modrhs, invd, g, nx, ny, omega, colour, st);
+}
+cudaError_t launch_dd_colour(const DF32& phi, const DF32& modrhs, const DF32& invd, const Geo32& g, int nx, int ny,
+                             double omega, int colour, cudaStream_t st) {
+    return dd_colour_impl(phi, modrhs, invd, g, nx, ny, omega, colour, st);
 }
 
 // ---------------------------------------------------------------------------

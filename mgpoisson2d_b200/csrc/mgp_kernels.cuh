@@ -159,6 +159,13 @@ cudaError_t launch_dd_modrhs(const DF& out, const DF& phi, const DF& rhs, const 
                              cudaStream_t st);
 cudaError_t launch_dd_colour(const DF& phi, const DF& modrhs, const DF& invd, const Geo& g, int nx, int ny,
                              double omega, int colour, cudaStream_t st);
+// The same three on FP32 fields (the grid levels of a mixed-precision DD V-cycle).
+cudaError_t launch_dd_apply(const DF32& out, const DF32& phi, const DF32& rhs, const Geo32& g, const BCd& b, int nx,
+                            int ny, int mode, cudaStream_t st);
+cudaError_t launch_dd_modrhs(const DF32& out, const DF32& phi, const DF32& rhs, const Geo32& g, int nx, int ny,
+                             cudaStream_t st);
+cudaError_t launch_dd_colour(const DF32& phi, const DF32& modrhs, const DF32& invd, const Geo32& g, int nx, int ny,
+                             double omega, int colour, cudaStream_t st);
 // Per-device kernel attributes (idempotent; call before any stream capture).
 cudaError_t sweep_kernels_init();
 cudaError_t coarse_kernels_init();

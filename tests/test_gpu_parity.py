@@ -459,6 +459,36 @@ def test_mixed_vcycle_converges_to_fp64_solution(M, krylov):
     assert np.abs(err).max() / np.abs(po.interior()).max() < 1e-7
 
 
+@pytest.mark.parametrize("which", ["skew", "identity"])
+def test_mixed_dc_vcycle_converges_to_fp64_solution(M, which):
+    """The deferred-correction solve (DD kind) with FP32 grid levels: the
+    outer residual is the FP64 9-point one, so it reaches the FP64 DC solve's
+    tolerance and solution, in about as many iterations.  (On the wavy 64:1
+    grid the reference DC iteration itself diverges, FP64 or not.)"""
+    from mgpoisson2d_b200 import workloads as W
+    if which == "skew":
+        v, geo, rhs, bc, _ = W.skew_stretched(128)
+        homog = False
+    else:
+        v, geo, rhs, bc, _ = W.identity_dirichlet(128)
+        homog = True
+    f = rhs.copy()
+    f.interior()[:] /= geo.J.interior()
+    sols, reps = [], []
+    for fl in (0, M.FLAG_MIXED, M.FLAG_MIXED):
+        with M.Solver(v, geo, bc, KIND_DD, fl) as s:
+            p = BoxData(v, 1, 1)
+            r = s.dc_vcycle(p, f.copy(), bc, homog, 1e-10, 400, 1, 8, 8, 8)
+        assert r.status == 0 and not r.diverged and r.final_relres <= 1e-10, (fl, r.iterations, r.final_relres)
+        sols.append(p)
+        reps.append(r)
+    assert abs(reps[1].iterations - reps[0].iterations) <= max(3, reps[0].iterations // 10)
+    assert same(sols[1].data, sols[2].data)   # deterministic
+    err = sols[1].interior() - sols[0].interior()
+    assert np.linalg.norm(err) / np.linalg.norm(sols[0].interior()) < 1e-8
+    assert np.abs(err).max() / np.abs(sols[0].interior()).max() < 1e-7
+
+
 def test_mixed_all_neumann_and_identity(M):
     """Mixed precision with the mean removal of an all-Neumann hierarchy (the
     terrain solver test) and on the identity map with Dirichlet sides."""
