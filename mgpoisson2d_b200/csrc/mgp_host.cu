@@ -594,11 +594,14 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
                                st));                                                      // P2:16-388
     }
     if ((s->flags & MGP_FLAG_DIRECT_COARSE) && s->kind == MGP_KIND_MG) RC(build_direct_coarse(s, st));
-    if (const long cells = (long)s->lv[s->dc].nx * s->lv[s->dc].ny; cells > kGridCoarseCells) {
+    // (one CTA per 256 cells, at most one per SM and at most what the device
+    // keeps resident; a device without cooperative launch keeps one CTA)
+    const int grid_max = coarse_grid_ctas_max();
+    if (const long cells = (long)s->lv[s->dc].nx * s->lv[s->dc].ny; cells > kGridCoarseCells && grid_max > 1) {
         int dev = 0, nsm = 0;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        s->grid_ctas = (int)std::min<long>(std::max(nsm, 1), std::max<long>(2, cells / 256));
+        s->grid_ctas = (int)std::min<long>(std::min(std::max(nsm, 1), grid_max), std::max<long>(2, cells / 256));
         if (cudaMalloc(&s->gctl.bar, 2 * sizeof(unsigned)) != cudaSuccess ||
             cudaMalloc(&s->gctl.part, 2 * sizeof(double) * s->grid_ctas) != cudaSuccess) {
             cudaGetLastError();
@@ -812,9 +815,19 @@ int vcycle32(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
                 }
                 return MGP_OK;
             }
-            for (int k = 0; k < nu_; ++k) {
-                CK(launch_sweep9(L.e, L.e2, L.r, L.invd, L.g, F.bc, 1, L.nx, L.ny, 1.0, &s->tma32[d], s->d_status,
-                                 st));
+            // on small levels two sweeps per launch where the level allows it
+            // (the same bits as two launches; half the launches and loads)
+            const bool pairs = sweep_pair_ok(&s->tma32[d], F.bc);
+            for (int k = 0; k < nu_;) {
+                if (pairs && nu_ - k >= 2) {
+                    CK(launch_sweep9_pair(L.e, L.e2, L.r, L.invd, L.g, F.bc, 1, L.nx, L.ny, 1.0, &s->tma32[d],
+                                          s->d_status, st));
+                    k += 2;
+                } else {
+                    CK(launch_sweep9(L.e, L.e2, L.r, L.invd, L.g, F.bc, 1, L.nx, L.ny, 1.0, &s->tma32[d],
+                                     s->d_status, st));
+                    k += 1;
+                }
                 std::swap(L.e, L.e2);
             }
             return MGP_OK;

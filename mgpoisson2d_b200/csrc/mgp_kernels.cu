@@ -1485,6 +1485,21 @@ __global__ void __launch_bounds__(kCoarseThreads, 1) k_coarse_cycle_grid(CoarseA
     if (GridScope::rank() == 0 && s) *a.status = s;
 }
 
+// How many CTAs of k_coarse_cycle_grid the current device can keep resident
+// at once (0 if it cannot launch cooperative grids).
+int coarse_grid_ctas_max() {
+    int dev = 0, coop = 0, nsm = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_coarse_cycle_grid, kCoarseThreads, 0) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return coop ? nsm * per_sm : 0;
+}
+
 cudaError_t launch_coarse_cycle(const CoarseArgs& a, cudaStream_t st) {
     if (a.grid_ctas > 1) {
         cudaLaunchConfig_t cfg = {};

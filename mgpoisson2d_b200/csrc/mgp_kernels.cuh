@@ -104,6 +104,8 @@ struct SweepTma {
     const void *pa = nullptr, *pb = nullptr, *rhs = nullptr, *invd = nullptr, *xx = nullptr;
     int tx = 32;   // tile width the descriptors' boxes are cut for
     bool ok = false;
+    SweepMaps ma2, mb2;   // boxes for two sweeps per launch (small FP32 levels)
+    bool ok2 = false;
 };
 // Builds the descriptors when the arrays allow it (16-byte aligned bases and
 // pitches, phi with a ghost layer and pitch >= nx + 3); else t->ok = false
@@ -120,6 +122,13 @@ cudaError_t launch_sweep9(const DF& pin, const DF& pout, const DF& rhs, const DF
 cudaError_t launch_sweep9(const DF32& pin, const DF32& pout, const DF32& rhs, const DF32& invd, const Geo32& g,
                           const BCd& b, int homog, int nx, int ny, double omega, const SweepTma* tma, int* status,
                           cudaStream_t st);
+// Two sweeps in one launch on an FP32 level whose descriptors allow it
+// (sweep_pair_ok: small levels of 32-wide tiles, no periodic side): the
+// result of two launch_sweep9 calls, bit for bit, written to pout.
+bool sweep_pair_ok(const SweepTma* tma, const BCd& b);
+cudaError_t launch_sweep9_pair(const DF32& pin, const DF32& pout, const DF32& rhs, const DF32& invd, const Geo32& g,
+                               const BCd& b, int homog, int nx, int ny, double omega, const SweepTma* tma,
+                               int* status, cudaStream_t st);
 cudaError_t launch_invdiag(const DF& invd, const Geo& g, const BCd& b, int homog, int nx, int ny, int coupled,
                            cudaStream_t st);
 // kind: 0 cell, 1 x-face, 2 y-face, 3 node.  ncx/ncy = coarse cell counts.
@@ -171,6 +180,8 @@ cudaError_t sweep_kernels_init();
 cudaError_t coarse_kernels_init();
 // Single-CTA kernels.
 cudaError_t launch_coarse_cycle(const CoarseArgs& a, cudaStream_t st);
+// Largest cooperative grid of the coarse cycle the current device keeps resident (0: none).
+int coarse_grid_ctas_max();
 // A[m * n + k] = (L e_k)_m for the level's operator with homogeneous BCs
 // (n = nx * ny columns, one CTA each; scratch holds 2 n fields of
 // (nx + 2) x (ny + 2)).

@@ -49,7 +49,7 @@ namespace mgp {
 namespace {
 
 constexpr int kTY = 32;
-constexpr int kH = 6;   // phi halo: 4 for the colour passes + E = 2 for the boundary pass
+constexpr int kH1 = 6;   // phi halo of one sweep: 4 for the colour passes + E = 2 for the boundary pass
 // A CTA gives up on its tile loads after kWaitLimit polls or kWaitNs, far
 // above any real wait (microseconds); each poll sleeps up to kSuspendNs.
 constexpr long kWaitLimit = 1L << 22;
@@ -71,9 +71,10 @@ constexpr unsigned kSuspendNs = 20000;
 // at o, the west/east x-faces at o and o + 1, the south/north y-faces at o
 // and o + PW.  The operands are needed on tile + (3 + E) <= tile + 5 cells
 // (faces one further), inside the phi footprint tile + kH.
-template <class T, int TX_>
+template <class T, int TX_, int K_ = 1>
 struct Win {
     static constexpr int TX = TX_;
+    static constexpr int kH = K_ * kH1;   // phi halo of K_ sweeps per launch
     static constexpr int kAlign = 16 / (int)sizeof(T);   // 2 doubles, 4 floats
     static constexpr int PW = (TX + 2 * kH + (kAlign - 1) + kAlign - 1) / kAlign * kAlign;   // 46 / 48 / 80
     static constexpr int PH = kTY + 2 * kH;                                                        // 44
@@ -90,6 +91,7 @@ struct Win {
     // 389 on tiles at the domain edge), so 12 warps cover them, and three
     // CTAs of 384 threads leave 56 registers a thread
     static constexpr int kThreads = kRI ? 512 : 384;
+    static_assert(K_ == 1 || (sizeof(T) == 4 && TX_ == 32), "two sweeps per launch: 32-wide FP32 tiles only");
     // CTAs per SM the window and the thread count allow
     static constexpr int kMinBlocks = (int)((228 * 1024) / (kSmemBytes + 1024)) < 2048 / kThreads
                                           ? (int)((228 * 1024) / (kSmemBytes + 1024))
@@ -99,6 +101,8 @@ struct Win {
 static_assert(Win<double, 32>::PW == 46 && Win<float, 32>::PW == 48 && Win<float, 64>::PW == 80, "window pitch");
 static_assert(Win<double, 32>::kMinBlocks == 2 && Win<float, 32>::kMinBlocks == 3 && Win<float, 64>::kMinBlocks == 3,
               "CTAs per SM");
+static_assert(Win<float, 32, 2>::PW == 60 && Win<float, 32, 2>::PH == 56 && Win<float, 32, 2>::kMinBlocks == 2,
+              "two-sweep window");
 
 template <class T>
 struct SLoadT {
@@ -215,15 +219,16 @@ __device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map
         : "memory");
 }
 
-// Interior colour c on the tile grown by (3 - c + E): first cell (ci0, cj0),
-// cw cells per row, n cells, and the magic number for k / cw (n <= 37 x 21
-// and cw <= 37, well inside the exact range of the 24-bit multiply).  Lane
+// Interior colour c on the tile grown by (3 - c + E + G), G the extra grow of
+// an early sweep of a multi-sweep launch: first cell (ci0, cj0), cw cells
+// per row, n cells, and the magic number for k / cw (n <= 37 x 25 and cw <=
+// 37, well inside the exact range of the 24-bit multiply).  Lane
 // c of each group of four computes colour c; every lane then reads all four
 // by shuffle, so a warp spends one divide, not four per thread.
-__device__ __forceinline__ void colour_ranges(int X0, int X1, int Y0, int Y1, int E, int mi0, int mi1, int mj0,
-                                              int mj1, int* ci0, int* cj0, int* ccw, int* cn, unsigned* cm) {
+__device__ __forceinline__ void colour_ranges(int X0, int X1, int Y0, int Y1, int E, int G, int mi0, int mi1,
+                                              int mj0, int mj1, int* ci0, int* cj0, int* ccw, int* cn, unsigned* cm) {
     const int c = threadIdx.x & 3;
-    const int grow = 3 - c + E;
+    const int grow = 3 - c + E + G;
     int i0 = max(X0 - grow, mi0), i1 = min(X1 + grow, mi1);
     int j0 = max(Y0 - grow, mj0), j1 = min(Y1 + grow, mj1);
     i0 += (i0 & 1) != colour_ci(c);
@@ -307,11 +312,11 @@ __device__ __forceinline__ void gs9_pair(float* a, float* b, bool write_b, float
     if (write_b) b[0] = r.y;
 }
 
-template <bool kTma, class T, int TX>
-__global__ void __launch_bounds__((Win<T, TX>::kThreads), (Win<T, TX>::kMinBlocks))
+template <bool kTma, class T, int TX, int K = 1>
+__global__ void __launch_bounds__((Win<T, TX, K>::kThreads), (Win<T, TX, K>::kMinBlocks))
     k_sweep9(const __grid_constant__ SweepMaps m, DFT<T> pin, DFT<T> pout, DFT<T> rhs, DFT<T> invd, GeoT<T> g,
              const __grid_constant__ BCd b, int homog, int nx, int ny, int4 part, double omega, int* status) {
-    using W = Win<T, TX>;
+    using W = Win<T, TX, K>;
     allow_dependents();
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     T* smem = reinterpret_cast<T*>(smem_raw);
@@ -327,8 +332,8 @@ __global__ void __launch_bounds__((Win<T, TX>::kThreads), (Win<T, TX>::kMinBlock
     const T om = T(omega), om1 = T(1.0 - omega);
     Tile<T> t;
     t.s = smem;
-    t.pox = (X0 - kH) & ~(W::kAlign - 1);
-    t.poy = Y0 - kH;
+    t.pox = (X0 - W::kH) & ~(W::kAlign - 1);
+    t.poy = Y0 - W::kH;
     // one scalar update, rhs and the inverse diagonal from the window or global memory
     const auto gs = [&](int i, int j, int xr, int yr) {
         T f, d;
@@ -351,7 +356,9 @@ __global__ void __launch_bounds__((Win<T, TX>::kThreads), (Win<T, TX>::kMinBlock
     unsigned cm[4];
 
     // 1. stage phi on tile + (4 + E) and the operands on tile + (3 + E)
-    const int hp = 4 + E, hc = 3 + E;
+    // (the first of K sweeps works on the tile grown by G0 = (K - 1)(4 + E))
+    const int G0 = (K - 1) * (4 + E);
+    const int hp = G0 + 4 + E, hc = G0 + 3 + E;
     const int pi0 = max(X0 - hp, -1), pi1 = min(X1 + hp, nx + 1), pj0 = max(Y0 - hp, -1), pj1 = min(Y1 + hp, ny + 1);
     const int ci0s = max(X0 - hc, 0), ci1s = min(X1 + hc, nx), cj0s = max(Y0 - hc, 0), cj1s = min(Y1 + hc, ny);
     if (kTma) {
@@ -382,7 +389,7 @@ __global__ void __launch_bounds__((Win<T, TX>::kThreads), (Win<T, TX>::kMinBlock
             tma_load_2d(sb, &m.pin, t.pox - m.pcb, t.poy - m.prb, bar);
             if constexpr (W::kRI) tma_load_2d(sb + W::oF * kS, &m.rhs, t.pox, t.poy, bar);
         }
-        colour_ranges(X0, X1, Y0, Y1, E, mi0, mi1, mj0, mj1, ci0, cj0, ccw, cn, cm);
+        colour_ranges(X0, X1, Y0, Y1, E, G0, mi0, mi1, mj0, mj1, ci0, cj0, ccw, cn, cm);
         // one warp polls the barrier; the others sleep in the block barrier
         // instead of taking issue slots from the CTAs that are computing
         const bool landed = threadIdx.x >= 32 || mbar_wait0(bar);
@@ -404,105 +411,115 @@ __global__ void __launch_bounds__((Win<T, TX>::kThreads), (Win<T, TX>::kMinBlock
         stage(smem + W::oXY, W::PW, t.pox, t.poy, g.xy, ci0s, ci1s + 1, cj0s, cj1s);
         stage(smem + W::oYX, W::PW, t.pox, t.poy, g.yx, ci0s, ci1s, cj0s, cj1s + 1);
         stage(smem + W::oYY, W::PW, t.pox, t.poy, g.yy, ci0s, ci1s, cj0s, cj1s + 1);
-        colour_ranges(X0, X1, Y0, Y1, E, mi0, mi1, mj0, mj1, ci0, cj0, ccw, cn, cm);
+        colour_ranges(X0, X1, Y0, Y1, E, G0, mi0, mi1, mj0, mj1, ci0, cj0, ccw, cn, cm);
         cp_async_wait_all();
         __syncthreads();
     }
-    // 2. sweep-start ghost fill on the staged ghost cells (the ghost rows and
-    //    columns of tiles on the domain boundary only)
-    if (pi0 < 0 || pi1 > nx || pj0 < 0 || pj1 > ny) {
-        const PinLoad<T, W::PW> P{smem, t.pox, t.poy, pi0, pi1, pj0, pj1, pin};
-        const int lw = pi1 - pi0, lh = pj1 - pj0;
-        for (int k = threadIdx.x; k < 2 * (lw + lh); k += blockDim.x) {
-            int i, j;
-            if (k < lw) { i = pi0 + k; j = pj0; }
-            else if (k < 2 * lw) { i = pi0 + k - lw; j = pj1 - 1; }
-            else if (k < 2 * lw + lh) { i = pi0; j = pj0 + k - 2 * lw; }
-            else { i = pi1 - 1; j = pj0 + k - 2 * lw - lh; }
-            if (i >= 0 && i < nx && j >= 0 && j < ny) continue;
-            smem[(j - t.poy) * W::PW + (i - t.pox)] = sweep_ghost(P, b, homog, nx, ny, i, j);
-        }
-    }
-    __syncthreads();
-
-    // 3. interior colour passes on shrinking regions.  Interior cells are
-    //    i in [mi0, mi1), j in [mj0, mj1) (a pass has at most 21 x 21 of them
-    //    on a 32 x 32 tile, 37 x 21 on a 64 x 32 one).  FP64: a thread per
-    //    cell.  FP32: a thread per two cells, k and k + ceil(n/2) of the
-    //    colour's list, so a warp's lanes still read consecutive cells of the
-    //    colour (two-way bank conflicts, as one cell per thread).
-    if constexpr (sizeof(T) == 4) {
-        const float2 idx2 = make_float2(idx, idx), idy2 = make_float2(idy, idy);
-        const float2 om2 = make_float2(om, om), om12 = make_float2(om1, om1);
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int nh = (cn[c] + 1) >> 1;
-            for (int k = threadIdx.x; k < nh; k += blockDim.x) {
-                const int kb = (k + nh < cn[c]) ? k + nh : k;
-                const int ja = fastdiv24(k, cm[c]), jb = fastdiv24(kb, cm[c]);
-                const int ia = ci0[c] + 2 * (k - ja * ccw[c]), ib = ci0[c] + 2 * (kb - jb * ccw[c]);
-                T* ca = t.s + (cj0[c] + 2 * ja - t.poy) * W::PW + (ia - t.pox);
-                T* cb = t.s + (cj0[c] + 2 * jb - t.poy) * W::PW + (ib - t.pox);
-                float2 f2, d2;
-                if constexpr (W::kRI) {
-                    f2 = make_float2(ca[W::oF], cb[W::oF]);
-                    d2 = make_float2(ca[W::oD], cb[W::oD]);
-                } else {
-                    const long ga = (long)(cj0[c] + 2 * ja) * rhs.ld + ia, gb = (long)(cj0[c] + 2 * jb) * rhs.ld + ib;
-                    const long ha = (long)(cj0[c] + 2 * ja) * invd.ld + ia, hb = (long)(cj0[c] + 2 * jb) * invd.ld + ib;
-                    f2 = make_float2(__ldg(rhs.p + ga), __ldg(rhs.p + gb));
-                    d2 = make_float2(__ldg(invd.p + ha), __ldg(invd.p + hb));
-                }
-                gs9_pair<W>(ca, cb, kb != k, f2, d2, idx2, idy2, om2, om12);
-            }
-            __syncthreads();
-        }
-    } else {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            for (int k = threadIdx.x; k < cn[c]; k += blockDim.x) {
-                const int kj = fastdiv24(k, cm[c]);
-                const int i = ci0[c] + 2 * (k - kj * ccw[c]), j = cj0[c] + 2 * kj;
-                gs(i, j, RMID, RMID);
-            }
-            __syncthreads();
-        }
-    }
-
-    // 4. boundary pass (edge tiles only; uniform per CTA): per colour, the
-    //    edge cells of that colour along each non-periodic side within the
-    //    tile grown by one, then the corners in turn
-    if (edge_tile) {
-        const int ei0 = max(X0 - 1, mi0), ei1 = min(X1 + 1, mi1);
-        const int ej0 = max(Y0 - 1, mj0), ej1 = min(Y1 + 1, mj1);
-        const bool sxl = !pr.xl && X0 == 0, sxh = !pr.xh && X1 >= nx;
-        const bool syl = !pr.yl && Y0 == 0, syh = !pr.yh && Y1 >= ny;
-        for (int c = 0; c < 4; ++c) {
-            const int ci = colour_ci(c), cj = colour_cj(c);
-            const int ia = ei0 + ((ei0 & 1) != ci), ja = ej0 + ((ej0 & 1) != cj);
-            const int ni = (ei1 > ia) ? (ei1 - ia + 1) / 2 : 0, nj = (ej1 > ja) ? (ej1 - ja + 1) / 2 : 0;
-            const int n0 = (syl && cj == 0) ? ni : 0;
-            const int n1 = n0 + ((syh && ((ny - 1) & 1) == cj) ? ni : 0);
-            const int n2 = n1 + ((sxl && ci == 0) ? nj : 0);
-            const int n3 = n2 + ((sxh && ((nx - 1) & 1) == ci) ? nj : 0);
-            for (int k = threadIdx.x; k < n3; k += blockDim.x) {
-                if (k < n0) gs(ia + 2 * k, 0, RMID, RLO);
-                else if (k < n1) gs(ia + 2 * (k - n0), ny - 1, RMID, RHI);
-                else if (k < n2) gs(0, ja + 2 * (k - n1), RLO, RMID);
-                else gs(nx - 1, ja + 2 * (k - n2), RHI, RMID);
-            }
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) {
-            for (int c = 0; c < 4; ++c) {
-                const int i = (c & 1) ? nx - 1 : 0, j = (c & 2) ? ny - 1 : 0;
-                if (i < X0 || i >= X1 || j < Y0 || j >= Y1) continue;
-                const int xr = region(i, nx, pr.xl, pr.xh), yr = region(j, ny, pr.yl, pr.yh);
-                if (xr != RMID && yr != RMID) gs(i, j, xr, yr);
+    // 2.-4. once per sweep.  Sweep s of K works on the tile grown by
+    //    G = (K - 1 - s)(4 + E): what the next sweep reads of it (tile +
+    //    G) comes out exact, as the halo argument above gives for one sweep.
+    for (int sw = 0; sw < K; ++sw) {
+        const int G = (K - 1 - sw) * (4 + E);
+        if (sw > 0) colour_ranges(X0, X1, Y0, Y1, E, G, mi0, mi1, mj0, mj1, ci0, cj0, ccw, cn, cm);
+        // 2. sweep-start ghost fill on the staged ghost cells (the ghost rows and
+        //    columns of tiles on the domain boundary only), on the sweep's footprint
+        const int qi0 = max(X0 - (G + 4 + E), -1), qi1 = min(X1 + G + 4 + E, nx + 1);
+        const int qj0 = max(Y0 - (G + 4 + E), -1), qj1 = min(Y1 + G + 4 + E, ny + 1);
+        if (qi0 < 0 || qi1 > nx || qj0 < 0 || qj1 > ny) {
+            const PinLoad<T, W::PW> P{smem, t.pox, t.poy, pi0, pi1, pj0, pj1, pin};
+            const int lw = qi1 - qi0, lh = qj1 - qj0;
+            for (int k = threadIdx.x; k < 2 * (lw + lh); k += blockDim.x) {
+                int i, j;
+                if (k < lw) { i = qi0 + k; j = qj0; }
+                else if (k < 2 * lw) { i = qi0 + k - lw; j = qj1 - 1; }
+                else if (k < 2 * lw + lh) { i = qi0; j = qj0 + k - 2 * lw; }
+                else { i = qi1 - 1; j = qj0 + k - 2 * lw - lh; }
+                if (i >= 0 && i < nx && j >= 0 && j < ny) continue;
+                smem[(j - t.poy) * W::PW + (i - t.pox)] = sweep_ghost(P, b, homog, nx, ny, i, j);
             }
         }
         __syncthreads();
-    }
+
+        // 3. interior colour passes on shrinking regions.  Interior cells are
+        //    i in [mi0, mi1), j in [mj0, mj1) (a pass has at most 21 x 21 of them
+        //    on a 32 x 32 tile, 37 x 21 on a 64 x 32 one).  FP64: a thread per
+        //    cell.  FP32: a thread per two cells, k and k + ceil(n/2) of the
+        //    colour's list, so a warp's lanes still read consecutive cells of the
+        //    colour (two-way bank conflicts, as one cell per thread).
+        if constexpr (sizeof(T) == 4) {
+            const float2 idx2 = make_float2(idx, idx), idy2 = make_float2(idy, idy);
+            const float2 om2 = make_float2(om, om), om12 = make_float2(om1, om1);
+    #pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int nh = (cn[c] + 1) >> 1;
+                for (int k = threadIdx.x; k < nh; k += blockDim.x) {
+                    const int kb = (k + nh < cn[c]) ? k + nh : k;
+                    const int ja = fastdiv24(k, cm[c]), jb = fastdiv24(kb, cm[c]);
+                    const int ia = ci0[c] + 2 * (k - ja * ccw[c]), ib = ci0[c] + 2 * (kb - jb * ccw[c]);
+                    T* ca = t.s + (cj0[c] + 2 * ja - t.poy) * W::PW + (ia - t.pox);
+                    T* cb = t.s + (cj0[c] + 2 * jb - t.poy) * W::PW + (ib - t.pox);
+                    float2 f2, d2;
+                    if constexpr (W::kRI) {
+                        f2 = make_float2(ca[W::oF], cb[W::oF]);
+                        d2 = make_float2(ca[W::oD], cb[W::oD]);
+                    } else {
+                        const long ra = cj0[c] + 2 * ja, rb = cj0[c] + 2 * jb;
+                        const long ga = ra * rhs.ld + ia, gb = rb * rhs.ld + ib;
+                        const long ha = ra * invd.ld + ia, hb = rb * invd.ld + ib;
+                        f2 = make_float2(__ldg(rhs.p + ga), __ldg(rhs.p + gb));
+                        d2 = make_float2(__ldg(invd.p + ha), __ldg(invd.p + hb));
+                    }
+                    gs9_pair<W>(ca, cb, kb != k, f2, d2, idx2, idy2, om2, om12);
+                }
+                __syncthreads();
+            }
+        } else {
+    #pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                for (int k = threadIdx.x; k < cn[c]; k += blockDim.x) {
+                    const int kj = fastdiv24(k, cm[c]);
+                    const int i = ci0[c] + 2 * (k - kj * ccw[c]), j = cj0[c] + 2 * kj;
+                    gs(i, j, RMID, RMID);
+                }
+                __syncthreads();
+            }
+        }
+
+        // 4. boundary pass (edge tiles only; uniform per CTA): per colour, the
+        //    edge cells of that colour along each non-periodic side within the
+        //    tile grown by G + 1, then the corners in turn
+        if (edge_tile) {
+            const int ei0 = max(X0 - 1 - G, mi0), ei1 = min(X1 + 1 + G, mi1);
+            const int ej0 = max(Y0 - 1 - G, mj0), ej1 = min(Y1 + 1 + G, mj1);
+            const bool sxl = !pr.xl && X0 == 0, sxh = !pr.xh && X1 >= nx;
+            const bool syl = !pr.yl && Y0 == 0, syh = !pr.yh && Y1 >= ny;
+            for (int c = 0; c < 4; ++c) {
+                const int ci = colour_ci(c), cj = colour_cj(c);
+                const int ia = ei0 + ((ei0 & 1) != ci), ja = ej0 + ((ej0 & 1) != cj);
+                const int ni = (ei1 > ia) ? (ei1 - ia + 1) / 2 : 0, nj = (ej1 > ja) ? (ej1 - ja + 1) / 2 : 0;
+                const int n0 = (syl && cj == 0) ? ni : 0;
+                const int n1 = n0 + ((syh && ((ny - 1) & 1) == cj) ? ni : 0);
+                const int n2 = n1 + ((sxl && ci == 0) ? nj : 0);
+                const int n3 = n2 + ((sxh && ((nx - 1) & 1) == ci) ? nj : 0);
+                for (int k = threadIdx.x; k < n3; k += blockDim.x) {
+                    if (k < n0) gs(ia + 2 * k, 0, RMID, RLO);
+                    else if (k < n1) gs(ia + 2 * (k - n0), ny - 1, RMID, RHI);
+                    else if (k < n2) gs(0, ja + 2 * (k - n1), RLO, RMID);
+                    else gs(nx - 1, ja + 2 * (k - n2), RHI, RMID);
+                }
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) {
+                for (int c = 0; c < 4; ++c) {
+                    const int i = (c & 1) ? nx - 1 : 0, j = (c & 2) ? ny - 1 : 0;
+                    if (i < X0 - G || i >= X1 + G || j < Y0 - G || j >= Y1 + G) continue;
+                    const int xr = region(i, nx, pr.xl, pr.xh), yr = region(j, ny, pr.yl, pr.yh);
+                    if (xr != RMID && yr != RMID) gs(i, j, xr, yr);
+                }
+            }
+            __syncthreads();
+        }
+    }   // sweeps
 
     // 5. write the tile, and the ghost cells next to it (the state fill_ghosts
     //    leaves: filled at the start of the sweep)
@@ -579,13 +596,15 @@ bool prepare_maps(SweepMaps* m, const DFT<T>& e, const DFT<T>& rhs, const DFT<T>
            encode<W>(&m->yy, g.yy.p, nx, ny + 1, g.yy.ld);
 }
 
-template <class T, int TX>
+template <class T, int TX, int K = 1>
 cudaError_t set_attr() {
-    cudaError_t e = cudaFuncSetAttribute(k_sweep9<true, T, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)Win<T, TX>::kSmemBytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_sweep9<false, T, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)Win<T, TX>::kSmemBytes);
+    cudaError_t e = cudaFuncSetAttribute(k_sweep9<true, T, TX, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)Win<T, TX, K>::kSmemBytes);
+    if constexpr (K == 1) {   // several sweeps per launch: the solver's own arrays (TMA) only
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_sweep9<false, T, TX, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)Win<T, TX, K>::kSmemBytes);
+    }
     return e;
 }
 
@@ -626,6 +645,15 @@ void tma_prepare(SweepTma* t, const DFT<T>& ea, const DFT<T>& eb, const DFT<T>& 
     if (!wide)
         t->ok = prepare_maps<Win<T, 32>>(&t->ma, ea, rhs, invd, g, nx, ny) &&
                 prepare_maps<Win<T, 32>>(&t->mb, eb, rhs, invd, g, nx, ny);
+    // two sweeps per launch: FP32 levels of 32-wide tiles that one wave of the
+    // two-sweep CTAs covers (their sweeps last about one CTA's latency)
+    t->ok2 = false;
+    if constexpr (sizeof(T) == 4) {
+        const long tiles = (long)((nx + 31) / 32) * ((ny + kTY - 1) / kTY);
+        if (t->ok && !wide && tiles <= (long)Win<float, 32, 2>::kMinBlocks * sm_count())
+            t->ok2 = prepare_maps<Win<T, 32, 2>>(&t->ma2, ea, rhs, invd, g, nx, ny) &&
+                     prepare_maps<Win<T, 32, 2>>(&t->mb2, eb, rhs, invd, g, nx, ny);
+    }
     t->pa = ea.p;
     t->pb = eb.p;
     t->rhs = rhs.p;
@@ -633,11 +661,11 @@ void tma_prepare(SweepTma* t, const DFT<T>& ea, const DFT<T>& eb, const DFT<T>& 
     t->xx = g.xx.p;
 }
 
-template <class T, int TX>
+template <class T, int TX, int K = 1>
 cudaError_t launch_tiles(const SweepMaps* m, const DFT<T>& pin, const DFT<T>& pout, const DFT<T>& rhs,
                          const DFT<T>& invd, const GeoT<T>& g, const BCd& b, int homog, int nx, int ny, double omega,
                          int* status, cudaStream_t st) {
-    using W = Win<T, TX>;
+    using W = Win<T, TX, K>;
     dim3 grd((nx + TX - 1) / TX, (ny + kTY - 1) / kTY);
     const int4 part = make_int4(nx / (int)grd.x, nx % (int)grd.x, ny / (int)grd.y, ny % (int)grd.y);
     if (m) {
@@ -652,13 +680,16 @@ cudaError_t launch_tiles(const SweepMaps* m, const DFT<T>& pin, const DFT<T>& po
         at[0].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = at;
         cfg.numAttrs = 1;
-        return cudaLaunchKernelEx(&cfg, k_sweep9<true, T, TX>, *m, pin, pout, rhs, invd, g, b, homog, nx, ny, part,
-                                  omega, status);
+        return cudaLaunchKernelEx(&cfg, k_sweep9<true, T, TX, K>, *m, pin, pout, rhs, invd, g, b, homog, nx, ny,
+                                  part, omega, status);
     }
-    static const SweepMaps none{};
-    k_sweep9<false, T, TX><<<grd, W::kThreads, W::kSmemBytes, st>>>(none, pin, pout, rhs, invd, g, b, homog, nx, ny,
-                                                                    part, omega, status);
-    return cudaGetLastError();
+    if constexpr (K == 1) {
+        static const SweepMaps none{};
+        k_sweep9<false, T, TX><<<grd, W::kThreads, W::kSmemBytes, st>>>(none, pin, pout, rhs, invd, g, b, homog, nx,
+                                                                        ny, part, omega, status);
+        return cudaGetLastError();
+    }
+    return cudaErrorNotSupported;
 }
 
 template <class T>
@@ -696,6 +727,7 @@ cudaError_t sweep_kernels_init() {
     e = set_attr<double, 32>();
     if (e == cudaSuccess) e = set_attr<float, 32>();
     if (e == cudaSuccess) e = set_attr<float, 64>();
+    if (e == cudaSuccess) e = set_attr<float, 32, 2>();
     if (e == cudaSuccess && dev < 64) done |= 1ull << dev;
     return e;
 }
@@ -718,6 +750,29 @@ cudaError_t launch_sweep9(const DF32& pin, const DF32& pout, const DF32& rhs, co
                           const BCd& b, int homog, int nx, int ny, double omega, const SweepTma* tma, int* status,
                           cudaStream_t st) {
     return sweep_impl(pin, pout, rhs, invd, g, b, homog, nx, ny, omega, tma, status, st);
+}
+
+bool sweep_pair_ok(const SweepTma* tma, const BCd& b) {
+    if (!tma || !tma->ok2 || !sweep_fusable(b)) return false;
+    for (int s = 0; s < 4; ++s)   // a periodic ghost would be read from global memory, one sweep stale
+        if (b.type[s] == T_PERIODIC) return false;
+    return true;
+}
+
+cudaError_t launch_sweep9_pair(const DF32& pin, const DF32& pout, const DF32& rhs, const DF32& invd, const Geo32& g,
+                               const BCd& b, int homog, int nx, int ny, double omega, const SweepTma* tma,
+                               int* status, cudaStream_t st) {
+    if (!sweep_pair_ok(tma, b) || (const void*)rhs.p != tma->rhs || (const void*)invd.p != tma->invd ||
+        (const void*)g.xx.p != tma->xx)
+        return cudaErrorNotSupported;
+    const SweepMaps* m =
+        ((const void*)pin.p == tma->pa) ? &tma->ma2 : ((const void*)pin.p == tma->pb) ? &tma->mb2 : nullptr;
+    if (!m) return cudaErrorNotSupported;
+    cudaError_t e = sweep_kernels_init();
+    if (e == cudaSuccess) e = launch_tiles<float, 32, 2>(m, pin, pout, rhs, invd, g, b, homog, nx, ny, omega, status,
+                                                         st);
+    count_launch();
+    return e;
 }
 
 }  // namespace mgp
