@@ -703,8 +703,19 @@ int smooth_body(mgp_solver* s, int d, int nu) {
             CK(launch_dd_colour(L.e, L.w, L.invd, L.g, L.nx, L.ny, 4.0 / 5.0, 1, st));
         }
     } else if (L.e2.p && sweep_fusable(L.bc)) {
-        for (int k = 0; k < nu; ++k) {
-            CK(launch_sweep9(L.e, L.e2, L.r, L.invd, L.g, L.bc, 1, L.nx, L.ny, 1.0, &s->tma[d], s->d_status, st));
+        // on small levels two sweeps per launch where the level allows it
+        // (the same bits as two launches)
+        const bool pairs = sweep_pair_ok(&s->tma[d], L.bc);
+        for (int k = 0; k < nu;) {
+            if (pairs && nu - k >= 2) {
+                CK(launch_sweep9_pair(L.e, L.e2, L.r, L.invd, L.g, L.bc, 1, L.nx, L.ny, 1.0, &s->tma[d], s->d_status,
+                                      st));
+                k += 2;
+            } else {
+                CK(launch_sweep9(L.e, L.e2, L.r, L.invd, L.g, L.bc, 1, L.nx, L.ny, 1.0, &s->tma[d], s->d_status,
+                                 st));
+                k += 1;
+            }
             const DF t = L.e;
             L.e = L.e2;
             L.e2 = t;

@@ -122,11 +122,14 @@ cudaError_t launch_sweep9(const DF& pin, const DF& pout, const DF& rhs, const DF
 cudaError_t launch_sweep9(const DF32& pin, const DF32& pout, const DF32& rhs, const DF32& invd, const Geo32& g,
                           const BCd& b, int homog, int nx, int ny, double omega, const SweepTma* tma, int* status,
                           cudaStream_t st);
-// Two sweeps in one launch on an FP32 level whose descriptors allow it
+// Two sweeps in one launch on a level whose descriptors allow it
 // (sweep_pair_ok: small levels of 32-wide tiles, no periodic side): the
 // result of two launch_sweep9 calls, bit for bit, written to pout.
 bool sweep_pair_ok(const SweepTma* tma, const BCd& b);
 cudaError_t launch_sweep9_pair(const DF32& pin, const DF32& pout, const DF32& rhs, const DF32& invd, const Geo32& g,
+                               const BCd& b, int homog, int nx, int ny, double omega, const SweepTma* tma,
+                               int* status, cudaStream_t st);
+cudaError_t launch_sweep9_pair(const DF& pin, const DF& pout, const DF& rhs, const DF& invd, const Geo& g,
                                const BCd& b, int homog, int nx, int ny, double omega, const SweepTma* tma,
                                int* status, cudaStream_t st);
 cudaError_t launch_invdiag(const DF& invd, const Geo& g, const BCd& b, int homog, int nx, int ny, int coupled,

@@ -91,7 +91,7 @@ struct Win {
     // 389 on tiles at the domain edge), so 12 warps cover them, and three
     // CTAs of 384 threads leave 56 registers a thread
     static constexpr int kThreads = kRI ? 512 : 384;
-    static_assert(K_ == 1 || (sizeof(T) == 4 && TX_ == 32), "two sweeps per launch: 32-wide FP32 tiles only");
+    static_assert(K_ == 1 || TX_ == 32, "two sweeps per launch: 32-wide tiles only");
     // CTAs per SM the window and the thread count allow
     static constexpr int kMinBlocks = (int)((228 * 1024) / (kSmemBytes + 1024)) < 2048 / kThreads
                                           ? (int)((228 * 1024) / (kSmemBytes + 1024))
@@ -103,6 +103,7 @@ static_assert(Win<double, 32>::kMinBlocks == 2 && Win<float, 32>::kMinBlocks == 
               "CTAs per SM");
 static_assert(Win<float, 32, 2>::PW == 60 && Win<float, 32, 2>::PH == 56 && Win<float, 32, 2>::kMinBlocks == 2,
               "two-sweep window");
+static_assert(Win<double, 32, 2>::PW == 58 && Win<double, 32, 2>::kMinBlocks == 1, "two-sweep FP64 window");
 
 template <class T>
 struct SLoadT {
@@ -645,15 +646,12 @@ void tma_prepare(SweepTma* t, const DFT<T>& ea, const DFT<T>& eb, const DFT<T>& 
     if (!wide)
         t->ok = prepare_maps<Win<T, 32>>(&t->ma, ea, rhs, invd, g, nx, ny) &&
                 prepare_maps<Win<T, 32>>(&t->mb, eb, rhs, invd, g, nx, ny);
-    // two sweeps per launch: FP32 levels of 32-wide tiles that one wave of the
+    // two sweeps per launch: levels of 32-wide tiles that one wave of the
     // two-sweep CTAs covers (their sweeps last about one CTA's latency)
-    t->ok2 = false;
-    if constexpr (sizeof(T) == 4) {
-        const long tiles = (long)((nx + 31) / 32) * ((ny + kTY - 1) / kTY);
-        if (t->ok && !wide && tiles <= (long)Win<float, 32, 2>::kMinBlocks * sm_count())
-            t->ok2 = prepare_maps<Win<T, 32, 2>>(&t->ma2, ea, rhs, invd, g, nx, ny) &&
-                     prepare_maps<Win<T, 32, 2>>(&t->mb2, eb, rhs, invd, g, nx, ny);
-    }
+    const long tiles = (long)((nx + 31) / 32) * ((ny + kTY - 1) / kTY);
+    t->ok2 = t->ok && !wide && tiles <= (long)Win<T, 32, 2>::kMinBlocks * sm_count() &&
+             prepare_maps<Win<T, 32, 2>>(&t->ma2, ea, rhs, invd, g, nx, ny) &&
+             prepare_maps<Win<T, 32, 2>>(&t->mb2, eb, rhs, invd, g, nx, ny);
     t->pa = ea.p;
     t->pb = eb.p;
     t->rhs = rhs.p;
@@ -728,6 +726,7 @@ cudaError_t sweep_kernels_init() {
     if (e == cudaSuccess) e = set_attr<float, 32>();
     if (e == cudaSuccess) e = set_attr<float, 64>();
     if (e == cudaSuccess) e = set_attr<float, 32, 2>();
+    if (e == cudaSuccess) e = set_attr<double, 32, 2>();
     if (e == cudaSuccess && dev < 64) done |= 1ull << dev;
     return e;
 }
@@ -759,9 +758,10 @@ bool sweep_pair_ok(const SweepTma* tma, const BCd& b) {
     return true;
 }
 
-cudaError_t launch_sweep9_pair(const DF32& pin, const DF32& pout, const DF32& rhs, const DF32& invd, const Geo32& g,
-                               const BCd& b, int homog, int nx, int ny, double omega, const SweepTma* tma,
-                               int* status, cudaStream_t st) {
+template <class T>
+cudaError_t sweep_pair_impl(const DFT<T>& pin, const DFT<T>& pout, const DFT<T>& rhs, const DFT<T>& invd,
+                            const GeoT<T>& g, const BCd& b, int homog, int nx, int ny, double omega,
+                            const SweepTma* tma, int* status, cudaStream_t st) {
     if (!sweep_pair_ok(tma, b) || (const void*)rhs.p != tma->rhs || (const void*)invd.p != tma->invd ||
         (const void*)g.xx.p != tma->xx)
         return cudaErrorNotSupported;
@@ -769,10 +769,20 @@ cudaError_t launch_sweep9_pair(const DF32& pin, const DF32& pout, const DF32& rh
         ((const void*)pin.p == tma->pa) ? &tma->ma2 : ((const void*)pin.p == tma->pb) ? &tma->mb2 : nullptr;
     if (!m) return cudaErrorNotSupported;
     cudaError_t e = sweep_kernels_init();
-    if (e == cudaSuccess) e = launch_tiles<float, 32, 2>(m, pin, pout, rhs, invd, g, b, homog, nx, ny, omega, status,
-                                                         st);
+    if (e == cudaSuccess) e = launch_tiles<T, 32, 2>(m, pin, pout, rhs, invd, g, b, homog, nx, ny, omega, status, st);
     count_launch();
     return e;
+}
+
+cudaError_t launch_sweep9_pair(const DF32& pin, const DF32& pout, const DF32& rhs, const DF32& invd, const Geo32& g,
+                               const BCd& b, int homog, int nx, int ny, double omega, const SweepTma* tma,
+                               int* status, cudaStream_t st) {
+    return sweep_pair_impl(pin, pout, rhs, invd, g, b, homog, nx, ny, omega, tma, status, st);
+}
+cudaError_t launch_sweep9_pair(const DF& pin, const DF& pout, const DF& rhs, const DF& invd, const Geo& g,
+                               const BCd& b, int homog, int nx, int ny, double omega, const SweepTma* tma,
+                               int* status, cudaStream_t st) {
+    return sweep_pair_impl(pin, pout, rhs, invd, g, b, homog, nx, ny, omega, tma, status, st);
 }
 
 }  // namespace mgp
