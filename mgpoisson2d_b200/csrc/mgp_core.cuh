@@ -1,9 +1,10 @@
 // mgp_core.cuh -- device-side building blocks of the B200 multigrid solver.
 //
-// Everything here is FP64 and is compiled with -fmad=false, so each product
-// and sum is rounded on its own in the order the Fortran routines write them:
-// a cell computed here is bit-identical to the same cell computed by the
-// Fortran code (and by the CPU oracle).
+// Compiled with -fmad=false, so each product and sum is rounded on its own
+// in the order the Fortran routines write them: a cell computed here in FP64
+// is bit-identical to the same cell computed by the Fortran code (and by the
+// CPU oracle).  The templates are also instantiated for FP32 fields, the grid
+// levels of the mixed-precision V-cycle.
 //
 // Citations: AU = arrayutils.f90, P2 = poisson2d.f90, MG = MGPoisson2D.f90,
 // DD = MGPoisson2D_DD.f90 (EdSantilli/MGPoisson2D, src/).

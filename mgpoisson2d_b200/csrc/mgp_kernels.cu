@@ -1,12 +1,15 @@
-// mgp_kernels.cu -- CUDA kernels of the B200 multigrid solver (sm_100a, FP64).
+// mgp_kernels.cu -- CUDA kernels of the B200 multigrid solver (sm_100a).
 //
-// Two execution shapes:
-//  * grid kernels, one thread per cell, for the large levels;
-//  * one 1024-thread CTA that runs a whole coarse sub-V-cycle, bottom
-//    BiCGStab included (vcycle_noinit from a given depth down, MG:675-854 and
-//    DD:867-1045), so the latency-bound small levels cost one launch.
-// Both call the same cell functions of mgp_core.cuh, so they produce the same
-// bits as each other and as the Fortran loop bodies.
+// Three execution shapes:
+//  * grid kernels, one thread per cell, for the large levels (FP64, and FP32
+//    for the grid levels of the mixed-precision V-cycle);
+//  * one 256-thread CTA that runs a whole coarse sub-V-cycle, bottom solve
+//    included (vcycle_noinit from a given depth down, MG:675-854 and
+//    DD:867-1045), so the latency-bound small levels cost one launch;
+//  * the same sub-cycle as a cooperative grid of CTAs when the coarsest
+//    level is too large for one CTA (the schedule stopped at an odd side).
+// All call the same cell functions of mgp_core.cuh, so the FP64 ones produce
+// the same bits as each other and as the Fortran loop bodies.
 #include <atomic>
 
 #include <mutex>
@@ -897,7 +900,8 @@ cudaError_t launch_dd_colour(const DF32& phi, const DF32& modrhs, const DF32& in
 }
 
 // ---------------------------------------------------------------------------
-// Single-CTA building blocks (every thread of the block calls them)
+// Building blocks of the coarse cycle (every thread of the scope calls them;
+// BLOOP is a block-stride loop for the single-CTA kernels' own staging)
 // ---------------------------------------------------------------------------
 #define BLOOP(k, n) for (int k = threadIdx.x; k < (n); k += blockDim.x)
 
