@@ -23,7 +23,11 @@
 //     halo suffices, E = 2), then the four corners in turn.
 // The halo cells are recomputed by every CTA that needs them, with the same
 // operations in the same order, so the result is bit-identical to running the
-// sub-passes over the whole grid one after another.
+// sub-passes over the whole grid one after another.  The same argument lets
+// one launch run K sweeps (K = 2 on small levels, whose sweeps last about
+// one CTA's latency): with a halo of K times the one-sweep halo, sweep s of K
+// works on the tile grown by (K - 1 - s)(4 + E) cells, and the tile comes out
+// as after K launches, bit for bit.
 //
 // Staging: on the solver's own arrays (aligned, with spare columns) one
 // thread issues seven TMA tile loads (five on the wide FP32 tiles;
