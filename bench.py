@@ -6,12 +6,14 @@ x sides, Neumann y sides; seeded 16-mode Fourier rhs, J-weighted mean removed).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 One step = one full solve (until |r|/|r0| <= 1e-10) of that problem.  The
-default solver is the V-cycle accelerated by BiCGStab (MGP_FLAG_KRYLOV: one
-V-cycle per preconditioner application) with the V-cycle's grid levels in
-FP32 inside the FP64 outer iteration (MGP_FLAG_MIXED) and its bottom solved
-exactly on the 8 x 8 level (MGP_FLAG_DIRECT_COARSE); --solver vcycle,
---precision fp64 and --coarse reference select the reference's stationary
-iteration, plain FP64 and the reference's bottom solver.  The line also carries one timed solve of the same
+default solver is the V-cycle accelerated by restarted GMRES(64)
+(MGP_FLAG_GMRES: one V-cycle per preconditioner application) with the
+V-cycle's grid levels in FP32 inside the FP64 outer iteration
+(MGP_FLAG_MIXED) and its bottom solved exactly on the 8 x 8 level
+(MGP_FLAG_DIRECT_COARSE); --solver krylov selects BiCGStab(V-cycle)
+(MGP_FLAG_KRYLOV), and --solver vcycle, --precision fp64 and --coarse
+reference the reference's stationary iteration, plain FP64 and the
+reference's bottom solver.  The line also carries one timed solve of the same
 solver in FP64 ("fp64_same_solver") and of the plain FP64 V-cycle iteration
 ("plain_vcycle"), and the headline solution's error against both.  Under
 torchrun every rank solves its own copy (replicas; the solve does not shard)
@@ -20,8 +22,9 @@ and rank 0 prints one JSON line.
 At N=1 the line also carries two legs on many independent problems (the
 batched workload: sides log-uniform in [64,1024]): "batched" (all problems as
 one mgp_batch on 16 streams vs one after another) and "served" (Poisson
-arrivals into an mgp_server with resident hierarchies; p50/p99 latency), and
-"precision_study": mixed precision against FP64 and against the exact solution
+arrivals into an mgp_server with resident hierarchies; p50/p99 latency), both
+with BiCGStab(V-cycle), whose work vectors are 8 per problem where GMRES(64)
+keeps 129, and "precision_study": mixed precision against FP64 and against the exact solution
 of a manufactured problem on the skewed, stretched grid at 512..4096, for the
 BiCGStab(V-cycle) solve and the deferred-correction solve, with the observed
 order of the discretisation error.  --serve-sweep adds "served_sweep" (the
@@ -67,11 +70,11 @@ def parse():
     p.add_argument("--cpu-vcycles", type=int, default=2, help="V-cycles in the bounded CPU sample")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--solver", default="krylov", choices=["krylov", "vcycle"])
+    p.add_argument("--solver", default="gmres", choices=["gmres", "krylov", "vcycle"])
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                    help="mixed: FP32 grid levels inside the FP64 outer iteration (MGP_FLAG_MIXED)")
     p.add_argument("--coarse", default="direct", choices=["direct", "reference"],
-                   help="bottom of the BiCGStab solver's V-cycle: exact (MGP_FLAG_DIRECT_COARSE) or the reference's")
+                   help="bottom of the Krylov solvers' V-cycle: exact (MGP_FLAG_DIRECT_COARSE) or the reference's")
     p.add_argument("--no-plain", action="store_true", help="skip the extra plain V-cycle solve")
     p.add_argument("--no-batch", action="store_true", help="skip the batched and served legs")
     p.add_argument("--batch", type=int, default=512, help="problems in the batched leg")
@@ -544,8 +547,8 @@ def main():
 
     v, geo, rhs, bc, _ = workload(args.n)
     base_flags = M.FLAG_DIRICHLET_COUPLED_DIAG
-    fp64_flags = base_flags | (M.FLAG_KRYLOV if args.solver == "krylov" else 0)
-    if args.solver == "krylov" and args.coarse == "direct":
+    fp64_flags = base_flags | {"krylov": M.FLAG_KRYLOV, "gmres": M.FLAG_GMRES, "vcycle": 0}[args.solver]
+    if args.solver != "vcycle" and args.coarse == "direct":
         fp64_flags |= M.FLAG_DIRECT_COARSE
     flags = fp64_flags | (M.FLAG_MIXED if args.precision == "mixed" else 0)
     solver = M.Solver(v, geo, bc, M.KIND_MG, flags)
@@ -662,10 +665,10 @@ def main():
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64+f32" if args.precision == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n": args.n, "tol": TOL, "nu": list(NU),
-                   "solver": "bicgstab(vcycle)" if args.solver == "krylov" else "vcycle",
+                   "solver": {"krylov": "bicgstab(vcycle)", "gmres": "gmres(vcycle)", "vcycle": "vcycle"}[args.solver],
                    "precision": ("FP32 grid levels, FP64 outer iteration / residual / update / coarse levels"
                                  if args.precision == "mixed" else "FP64"),
-                   "flags": "dirichlet_coupled_diag" + ("|krylov" if args.solver == "krylov" else "") +
+                   "flags": "dirichlet_coupled_diag" + ("" if args.solver == "vcycle" else "|" + args.solver) +
                             ("|mixed" if args.precision == "mixed" else "") +
                             ("|direct_coarse" if fp64_flags & M.FLAG_DIRECT_COARSE else ""),
                    "bottom": ("exact solve of the first level <= 64 cells" if fp64_flags & M.FLAG_DIRECT_COARSE

@@ -156,6 +156,16 @@ typedef struct mgp_report {
  * reference bottom runs.  No reference counterpart: the V-cycle is then a
  * different (stronger) preconditioner, for use with MGP_FLAG_KRYLOV. */
 #define MGP_FLAG_DIRECT_COARSE 16
+/* vcycle only: accelerate the V-cycle with restarted GMRES instead of
+ * BiCGStab (takes precedence over MGP_FLAG_KRYLOV): right-preconditioned
+ * GMRES(m) on L_h e = r0 with one V-cycle per preconditioner application,
+ * one pass of classical Gram-Schmidt, m = 64 (fewer if the 2m + 1 stored
+ * vectors would take more than a quarter of the free device memory).
+ * report.iterations and the relres history count V-cycles (the GMRES
+ * residual estimate); final_relres is the true residual recomputed at the
+ * end, and the solve restarts from it if it has not passed.  No reference
+ * counterpart. */
+#define MGP_FLAG_GMRES 32
 
 /* Solver kinds for the resident-hierarchy handle. */
 #define MGP_KIND_MG 0   /* module MGPoisson2D (vcycle, fmg)                  */

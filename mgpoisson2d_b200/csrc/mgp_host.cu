@@ -49,6 +49,10 @@ int set_err(int code, const char* fmt, ...) {
         if (r_) return r_;      \
     } while (0)
 
+// GMRES restart length and the blocks of its many-vector reductions.
+constexpr int kGmresRestart = 64;
+constexpr int kGmresBlocks = 296;
+
 // Levels with at most this many cells run inside the single-CTA coarse cycle.
 constexpr long kCoarseCells = 1024;
 // When the schedule stops above that (an odd side), the coarse cycle runs on
@@ -275,6 +279,14 @@ struct mgp_solver {
     // MGP_FLAG_KRYLOV: BiCGStab vectors on level 0 (residual, shadow residual,
     // search direction, A*y and A*z)
     DF kr{}, krh{}, kp{}, kv{}, kt{};
+    // MGP_FLAG_GMRES: 2m + 1 level-0 vectors (basis v_0..v_m, then the
+    // preconditioned z_0..z_{m-1}), each (nx + 2) x (ny + 2) with a ghost
+    // layer, and the reduction scratch (partials, two Gram-Schmidt columns,
+    // a norm, the update coefficients)
+    double* gm_base = nullptr;
+    double* gm_red = nullptr;
+    int gm_m = 0;
+    size_t gm_vec = 0, gm_ld = 0;
     std::vector<SweepTma> tma;   // per level, for the fused sweep
     // MGP_FLAG_MIXED: FP32 copies of the grid-path levels 0 .. dc-1
     struct Lv32 {
@@ -317,6 +329,8 @@ void solver_free(mgp_solver* s) {
     if (s->d_lv) cudaFree(s->d_lv);
     if (s->d_shadow) cudaFree(s->d_shadow);
     if (s->d_ainv) cudaFree(s->d_ainv);
+    if (s->gm_base) cudaFree(s->gm_base);
+    if (s->gm_red) cudaFree(s->gm_red);
     if (s->gctl.bar) cudaFree(s->gctl.bar);
     if (s->gctl.part) cudaFree(s->gctl.part);
     if (s->d_ref) cudaFree(s->d_ref);
@@ -594,6 +608,21 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
                                st));                                                      // P2:16-388
     }
     if ((s->flags & MGP_FLAG_DIRECT_COARSE) && s->kind == MGP_KIND_MG) RC(build_direct_coarse(s, st));
+    if ((s->flags & MGP_FLAG_GMRES) && s->kind == MGP_KIND_MG) {
+        s->gm_ld = (size_t)valid->nx + 2;
+        s->gm_vec = s->gm_ld * (valid->ny + 2);
+        size_t freeb = 0, totalb = 0;
+        CK(cudaMemGetInfo(&freeb, &totalb));
+        int m = kGmresRestart;
+        while (m > 8 && (size_t)(2 * m + 1) * s->gm_vec * sizeof(double) > freeb / 4) m /= 2;
+        s->gm_m = m;
+        if (cudaMalloc(&s->gm_base, (size_t)(2 * m + 1) * s->gm_vec * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&s->gm_red, sizeof(double) * ((size_t)kGmresBlocks * (m + 1) + 2 * (m + 1))) !=
+                cudaSuccess) {
+            cudaGetLastError();
+            return set_err(MGP_ENOMEM, "device allocation failed");
+        }
+    }
     // (one CTA per 256 cells, at most one per SM and at most what the device
     // keeps resident; a device without cooperative launch keeps one CTA)
     const int grid_max = coarse_grid_ctas_max();
@@ -1091,6 +1120,104 @@ int krylov_loop(mgp_solver* s, const BCd& ubc, int homog, double tol, int maxite
     }
 }
 
+// MGP_FLAG_GMRES: restarted, right-preconditioned GMRES(m) (Saad and Schultz,
+// SIAM J. Sci. Stat. Comput. 7, 1986) on L_h e = r0, with L_h and the V-cycle
+// preconditioner as in krylov_loop.  Each step: z_j = M^-1 v_j (one V-cycle),
+// w = L_h z_j, w orthogonalised against v_0..v_j by one pass of classical
+// Gram-Schmidt (the coefficients stay on the device; one host
+// synchronisation per step fetches them with |w|), and Givens rotations on
+// the host give the residual norm.  At convergence, breakdown or m steps,
+// phi0 += Z y and the true residual is recomputed with the caller's BCs;
+// the solve restarts from it if it has not passed, so a residual estimate
+// that drifted with lost orthogonality ends in a restart, not in a wrong
+// answer.  (A second pass, taken whenever |w| fell below half its norm
+// before, ran on every step with the V-cycle preconditioner, since
+// L_h M^-1 is close to the identity, and left the V-cycle count unchanged.)  Inner products are
+// unweighted; the weighted norms of the history differ by sqrt(dx dy).
+int gmres_loop(mgp_solver* s, const BCd& ubc, int homog, double tol, int maxiters, int numcycles, int nd, int nu,
+               int nb, double rscale, std::vector<double>& relres, int* iters_out, int verbosity) {
+    Lv& L0 = s->lv[0];
+    const int nx = s->valid.nx, ny = s->valid.ny, m = s->gm_m, ld = (int)s->gm_ld;
+    const double vol = s->valid.dx * s->valid.dy, sv = std::sqrt(vol);
+    cudaStream_t st = s->stream;
+    auto V = [&](int k) { return DF{s->gm_base + (size_t)k * s->gm_vec + ld + 1, ld}; };
+    auto Z = [&](int k) { return DF{s->gm_base + (size_t)(m + 1 + k) * s->gm_vec + ld + 1, ld}; };
+    const MVec mv{V(0).p, ld, (long)s->gm_vec}, mz{Z(0).p, ld, (long)s->gm_vec};
+    double* part = s->gm_red;
+    double* h1 = part + (size_t)kGmresBlocks * (m + 1);   // h1[m + 1], |w|^2, then y[m]
+    double* nrm = h1 + (m + 1);
+    double* dy = nrm + 1;
+    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), hc(m + 2), y(m);
+    int k = 0;
+    auto record = [&](double res) -> int {
+        relres[k] = res / rscale;
+        *iters_out = k;
+        if (verbosity >= 1) printf("GMRES V-Cycle %d: rel |res| = %.16e\n", k, relres[k]);
+        return std::isfinite(relres[k]) ? MGP_OK : MGP_EDIVERGED;
+    };
+    *iters_out = 0;
+    if (relres[0] <= tol) return MGP_OK;
+    for (;;) {   // one pass per (re)start; L0.r holds the residual
+        CK(launch_mdot(L0.r, MVec{L0.r.p, L0.r.ld, 0}, 1, nx, ny, part, kGmresBlocks, nrm, st));
+        CK(cudaMemcpyAsync(hc.data(), nrm, sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        const double beta = std::sqrt(hc[0]);
+        if (!(beta > 0.0) || !std::isfinite(beta)) return std::isfinite(beta) ? MGP_OK : MGP_EDIVERGED;
+        CK(launch_axpby(V(0), L0.r, 0.0, 1.0 / beta, nx, ny, 0, 0, st));
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int jend = 0;
+        for (int j = 0; j < m && k < maxiters; ++j) {
+            RC(vcycle_top(s, V(j), numcycles, nd, nu, nb));   // M^-1 v_j in L0.e
+            CK(launch_axpby(Z(j), L0.e, 0.0, 1.0, nx, ny, 1, 1, st));
+            CK(launch_fill(Z(j), L0.g, L0.bc, 1, 0, nx, ny, st));
+            CK(launch_apply(V(j + 1), Z(j), L0.r, L0.g, L0.bc, 1, nx, ny, 0, 0, st));
+            ++k;
+            CK(launch_mdot(V(j + 1), mv, j + 1, nx, ny, part, kGmresBlocks, h1, st));
+            CK(launch_maxpy(V(j + 1), mv, j + 1, h1, -1.0, nx, ny, st));
+            CK(launch_mdot(V(j + 1), MVec{V(j + 1).p, ld, 0}, 1, nx, ny, part, kGmresBlocks, nrm, st));
+            CK(cudaMemcpyAsync(hc.data(), h1, sizeof(double) * (m + 2), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            double* col = &H[(size_t)j * (m + 1)];   // column j of the Hessenberg matrix
+            for (int i = 0; i <= j; ++i) col[i] = hc[i];
+            const double hn = std::sqrt(hc[m + 1]);
+            col[j + 1] = hn;
+            for (int i = 0; i < j; ++i) {   // earlier rotations
+                const double t = cs[i] * col[i] + sn[i] * col[i + 1];
+                col[i + 1] = -sn[i] * col[i] + cs[i] * col[i + 1];
+                col[i] = t;
+            }
+            const double den = std::hypot(col[j], col[j + 1]);
+            cs[j] = den > 0.0 ? col[j] / den : 1.0;
+            sn[j] = den > 0.0 ? col[j + 1] / den : 0.0;
+            col[j] = den;
+            col[j + 1] = 0.0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            jend = j + 1;
+            RC(record(std::fabs(g[j + 1]) * sv));
+            if (relres[k] <= tol || !(hn > 0.0) || !(den > 0.0)) break;   // converged, or the space is exhausted
+            CK(launch_axpby(V(j + 1), V(j + 1), 1.0 / hn, 0.0, nx, ny, 0, 0, st));
+        }
+        if (jend == 0) return MGP_OK;   // maxiters reached before a step
+        for (int i = jend - 1; i >= 0; --i) {   // H y = g, upper triangular
+            double t = g[i];
+            for (int l = i + 1; l < jend; ++l) t -= H[(size_t)l * (m + 1) + i] * y[l];
+            y[i] = t / H[(size_t)i * (m + 1) + i];
+        }
+        CK(cudaMemcpyAsync(dy, y.data(), sizeof(double) * jend, cudaMemcpyHostToDevice, st));
+        CK(launch_maxpy(s->phi0, mz, jend, dy, 1.0, nx, ny, st));
+        CK(cudaStreamSynchronize(st));   // y's host copy is read by the transfer above
+        // true residual with the caller's BCs (MG:579)
+        CK(launch_fill(s->phi0, L0.g, ubc, homog, 0, nx, ny, st));
+        CK(launch_apply(L0.r, s->phi0, s->rhs0, L0.g, ubc, homog, nx, ny, 1, 0, st));
+        CK(launch_reduce(RED_SUMSQ, L0.r, L0.r, nx, ny, vol, red_partials(s), red_out(s), st));
+        RC(fetch_reductions(s, 1));
+        RC(record(s->h_red[0]));
+        if (relres[k] <= tol || k >= maxiters) return MGP_OK;
+    }
+}
+
 // 0 = vcycle (MG:400-670), 1 = fmg (MG:860-1122), 2 = DD vcycle (DD:589-862)
 int solver_solve(mgp_solver* s, int which, mgp_array* phi, mgp_array* rhs, const mgp_bdry* bc, int homog, double tol,
                  int maxiters, int numcycles, int nd, int nu, int nb, int zerophi, int verbosity, mgp_report* rep) {
@@ -1134,14 +1261,17 @@ int solver_solve(mgp_solver* s, int which, mgp_array* phi, mgp_array* rhs, const
     else relres[0] = 1.0;
     if (verbosity >= 1) printf("max MG depth = %d\nV-Cycle iter 0: rel |res| = %.16e\n", s->maxdepth, relres[0]);
     if (!std::isfinite(rscale)) status = MGP_EDIVERGED;
-    const bool krylov = which == 0 && (s->flags & MGP_FLAG_KRYLOV) && s->kr.p;
-    if (krylov && status == MGP_OK) {
-        const int rc = krylov_loop(s, ubc, homog, tol, maxiters, numcycles, nd, nu, nb, rscale, relres, &iters,
-                                   verbosity);
+    const bool gmres = which == 0 && (s->flags & MGP_FLAG_GMRES) && s->gm_base;
+    const bool krylov = which == 0 && !gmres && (s->flags & MGP_FLAG_KRYLOV) && s->kr.p;
+    if ((krylov || gmres) && status == MGP_OK) {
+        const int rc = gmres ? gmres_loop(s, ubc, homog, tol, maxiters, numcycles, nd, nu, nb, rscale, relres, &iters,
+                                          verbosity)
+                             : krylov_loop(s, ubc, homog, tol, maxiters, numcycles, nd, nu, nb, rscale, relres,
+                                           &iters, verbosity);
         if (rc == MGP_EDIVERGED) status = rc;
         else if (rc) return rc;
     }
-    for (int iter = 1; !krylov && iter <= maxiters && status == MGP_OK; ++iter) {
+    for (int iter = 1; !krylov && !gmres && iter <= maxiters && status == MGP_OK; ++iter) {
         if (which == 0) RC(vcycle_top(s, L0.r, numcycles, nd, nu, nb));   // MG:600-606
         else if (which == 1) RC(fmg_noinit(s, 0, numcycles, nd, nu, nb));
         else if (!mixed(s)) RC(vcycle_run(s, 0, numcycles, nd, nu, nb, false));

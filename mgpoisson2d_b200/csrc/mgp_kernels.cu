@@ -662,6 +662,70 @@ cudaError_t launch_axpby(const DF& y, const DF& x, double a, double b, int nx, i
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Many-vector kernels of the GMRES outer iteration (MGP_FLAG_GMRES).  Vector k
+// of a set is at V.p + k * V.stride, cell (i,j) at [i + j * V.ld]; valid cells
+// only.  Deterministic: fixed per-block trees, blocks combined in order.
+// ---------------------------------------------------------------------------
+constexpr int kMdotThreads = 256;
+
+// partials[k * gridDim.x + b] = sum over block b's cells of w * v_k (k = blockIdx.y).
+__global__ void __launch_bounds__(kMdotThreads) k_mdot(DF w, MVec V, int nx, int ny, double* partials) {
+    __shared__ double sh[kMdotThreads];
+    const double* v = V.p + (long)blockIdx.y * V.stride;
+    const long n = (long)nx * ny;
+    double acc = 0.0;
+    for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % nx), j = (int)(c / nx);
+        acc = acc + AT(w, i, j) * v[i + (long)j * V.ld];
+    }
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = kMdotThreads / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) sh[threadIdx.x] = sh[threadIdx.x] + sh[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partials[(long)blockIdx.y * gridDim.x + blockIdx.x] = sh[0];
+}
+
+// out[k] = sum of partials[k * nb .. k * nb + nb) (k = blockIdx.x), in block order.
+__global__ void __launch_bounds__(kMdotThreads) k_mdot_final(const double* partials, int nb, double* out) {
+    __shared__ double sh[kMdotThreads];
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) acc = acc + partials[(long)blockIdx.x * nb + b];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = kMdotThreads / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) sh[threadIdx.x] = sh[threadIdx.x] + sh[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
+}
+
+cudaError_t launch_mdot(const DF& w, const MVec& V, int nv, int nx, int ny, double* partials, int nb, double* out,
+                        cudaStream_t st) {
+    k_mdot<<<dim3(nb, nv), kMdotThreads, 0, st>>>(w, V, nx, ny, partials);
+    k_mdot_final<<<nv, kMdotThreads, 0, st>>>(partials, nb, out);
+    count_launch(2);
+    return cudaGetLastError();
+}
+
+// w += sign * sum_{k < nv} coef[k] v_k over the valid cells (coef in device memory).
+__global__ void k_maxpy(DF w, MVec V, int nv, const double* coef, double sign, int nx, int ny) {
+    CELL_IJ
+    if (i >= nx || j >= ny) return;
+    double acc = AT(w, i, j);
+    for (int k = 0; k < nv; ++k) acc = acc + (sign * coef[k]) * V.p[(long)k * V.stride + i + (long)j * V.ld];
+    AT(w, i, j) = acc;
+}
+
+cudaError_t launch_maxpy(const DF& w, const MVec& V, int nv, const double* coef, double sign, int nx, int ny,
+                         cudaStream_t st) {
+    k_maxpy<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(w, V, nv, coef, sign, nx, ny);
+    count_launch();
+    return cudaGetLastError();
+}
+
 __global__ void k_muldiv(DF y, DF x, int mul, int nx, int ny) {
     CELL_IJ
     if (i >= nx || j >= ny) return;

@@ -144,6 +144,18 @@ cudaError_t launch_prolong_cross(const DF& fine, const DF& crse, int ncx, int nc
 cudaError_t launch_set_guess(const DF& e, const DF& r, const DF& invd, int nx, int ny, cudaStream_t st);
 cudaError_t launch_jacobi(const DF& phi, const DF& r, const DF& invd, double omega, int nx, int ny, cudaStream_t st);
 // y[i,j] = a*y + b*x over i in [-gx, nx+gx), j in [-gy, ny+gy).
+// A set of vectors for GMRES: vector k at p + k * stride, cell (i,j) at [i + j * ld].
+struct MVec {
+    double* p;
+    int ld;
+    long stride;
+};
+// out[k] = sum over valid cells of w * v_k, k < nv (partials: nb * nv doubles).
+cudaError_t launch_mdot(const DF& w, const MVec& V, int nv, int nx, int ny, double* partials, int nb, double* out,
+                        cudaStream_t st);
+// w += sign * sum_{k < nv} coef[k] v_k (coef in device memory).
+cudaError_t launch_maxpy(const DF& w, const MVec& V, int nv, const double* coef, double sign, int nx, int ny,
+                         cudaStream_t st);
 cudaError_t launch_axpby(const DF& y, const DF& x, double a, double b, int nx, int ny, int gx, int gy,
                          cudaStream_t st);
 // y = y * x (mul=1) or y / x (mul=0) over the valid region.

@@ -489,6 +489,60 @@ def test_mixed_dc_vcycle_converges_to_fp64_solution(M, which):
     assert np.abs(err).max() / np.abs(sols[0].interior()).max() < 1e-7
 
 
+# ---------------------------------------------------------------------------
+# GMRES-accelerated V-cycle (MGP_FLAG_GMRES; no reference counterpart)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("mixed", [False, True])
+def test_gmres_vcycle_converges_to_oracle_solution(M, mixed):
+    """Right-preconditioned GMRES(m) with one V-cycle per application reaches
+    1e-10 and the oracle's FP64 solution, in no more V-cycles than BiCGStab
+    with the same preconditioner, and repeats bit for bit."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, _ = W.wavy_stretched(128)
+    base = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_DIRECT_COARSE | (M.FLAG_MIXED if mixed else 0)
+    old = _set_coupled(M, True)
+    try:
+        po = BoxData(v, 1, 1)
+        O.vcycle(po, rhs, geo, bc, True, 1e-11, 3000, gs_order=1)
+    finally:
+        _set_coupled(M, old)
+    with M.Solver(v, geo, bc, KIND_MG, base | M.FLAG_KRYLOV) as s:
+        pk = BoxData(v, 1, 1)
+        rk = s.vcycle(pk, rhs, bc, True, 1e-10, 3000)
+    with M.Solver(v, geo, bc, KIND_MG, base | M.FLAG_GMRES) as s:
+        pg = BoxData(v, 1, 1)
+        rg = s.vcycle(pg, rhs, bc, True, 1e-10, 3000)
+        pg2 = BoxData(v, 1, 1)
+        rg2 = s.vcycle(pg2, rhs, bc, True, 1e-10, 3000)
+    assert rg.status == 0 and not rg.diverged and rg.final_relres <= 1e-10, (rg.iterations, rg.final_relres)
+    assert rg.iterations <= rk.iterations, (rg.iterations, rk.iterations)
+    assert same(pg.data, pg2.data) and np.array_equal(rg.relres, rg2.relres)
+    err = pg.interior() - po.interior()
+    assert np.linalg.norm(err) / np.linalg.norm(po.interior()) < 1e-8
+    assert np.abs(err).max() / np.abs(po.interior()).max() < 1e-7
+
+
+def test_gmres_restarts(M):
+    """One sweep down and up per V-cycle on 256^2: the solve needs more V-cycles
+    than the restart length (64), so it restarts from the true residual and
+    still reaches the oracle's solution."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, _ = W.wavy_stretched(256)
+    old = _set_coupled(M, True)
+    try:
+        po = BoxData(v, 1, 1)
+        O.vcycle(po, rhs, geo, bc, True, 1e-11, 5000, gs_order=1)
+    finally:
+        _set_coupled(M, old)
+    with M.Solver(v, geo, bc, KIND_MG, M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_GMRES) as s:
+        pg = BoxData(v, 1, 1)
+        rg = s.vcycle(pg, rhs, bc, True, 1e-10, 2000, 1, 1, 1, 8)
+    assert rg.status == 0 and rg.final_relres <= 1e-10, (rg.iterations, rg.final_relres)
+    assert rg.iterations > 64, rg.iterations
+    err = pg.interior() - po.interior()
+    assert np.linalg.norm(err) / np.linalg.norm(po.interior()) < 1e-8
+
+
 def test_mixed_all_neumann_and_identity(M):
     """Mixed precision with the mean removal of an all-Neumann hierarchy (the
     terrain solver test) and on the identity map with Dirichlet sides."""
