@@ -11,9 +11,11 @@ default solver is the V-cycle accelerated by restarted GMRES(64)
 V-cycle's grid levels in FP32 inside the FP64 outer iteration
 (MGP_FLAG_MIXED) and its bottom solved exactly on the 8 x 8 level
 (MGP_FLAG_DIRECT_COARSE); --solver krylov selects BiCGStab(V-cycle)
-(MGP_FLAG_KRYLOV), and --solver vcycle, --precision fp64 and --coarse
-reference the reference's stationary iteration, plain FP64 and the
-reference's bottom solver.  The line also carries one timed solve of the same
+(MGP_FLAG_KRYLOV), --coarse large an exact bottom on the 32 x 32 level
+(MGP_FLAG_DIRECT_LARGE: its inverse built on the device when the solver is
+created), and --solver vcycle, --precision fp64 and --coarse reference the
+reference's stationary iteration, plain FP64 and the reference's bottom
+solver.  The line also carries one timed solve of the same
 solver in FP64 ("fp64_same_solver") and of the plain FP64 V-cycle iteration
 ("plain_vcycle"), and the headline solution's error against both.  Under
 torchrun every rank solves its own copy (replicas; the solve does not shard)
@@ -73,8 +75,9 @@ def parse():
     p.add_argument("--solver", default="gmres", choices=["gmres", "krylov", "vcycle"])
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                    help="mixed: FP32 grid levels inside the FP64 outer iteration (MGP_FLAG_MIXED)")
-    p.add_argument("--coarse", default="direct", choices=["direct", "reference"],
-                   help="bottom of the Krylov solvers' V-cycle: exact (MGP_FLAG_DIRECT_COARSE) or the reference's")
+    p.add_argument("--coarse", default="direct", choices=["direct", "large", "reference"],
+                   help="bottom of the Krylov solvers' V-cycle: exact on the first level of at most 64 cells "
+                        "(MGP_FLAG_DIRECT_COARSE), of at most 1024 (with MGP_FLAG_DIRECT_LARGE), or the reference's")
     p.add_argument("--no-plain", action="store_true", help="skip the extra plain V-cycle solve")
     p.add_argument("--no-batch", action="store_true", help="skip the batched and served legs")
     p.add_argument("--batch", type=int, default=512, help="problems in the batched leg")
@@ -439,14 +442,16 @@ def pinned(bd):
     return out
 
 
-def vcycle_bytes(M, v, mixed, direct, nu=NU):
+def vcycle_bytes(M, v, mixed, direct, nu=NU, large=False):
     """Algorithmic bytes of one V-cycle: per level with N cells and word size
     w, N w [8 (nu1 + nu2) + 6 + rho + 2 + rho + 3] (sweeps; residual fused
     with restriction; prolongation; the coarse guess r invdiag; rho = coarse
     cells per fine cell), plus 11 FP64 words per finest cell for the outer
     residual, norm and update.  Levels of at most 1024 cells (the coarse CTA)
-    are FP64; with FP32 grid levels the others take 4 B.  The bottom solve
-    is counted as time, not bytes."""
+    are FP64; with FP32 grid levels the others take 4 B.  The bottom is the
+    first level of at most 64 cells with `direct`, of at most 1024 with
+    `large` as well; its solve is counted as time, except the large bottom's
+    product with the inverse, 8 N (N + 2) bytes."""
     md = M.estimate_maxdepth(1000, v)
     rx, ry, md = M.create_mgschedule(md, v)
     nx, ny, levels = v.nx, v.ny, []
@@ -455,9 +460,16 @@ def vcycle_bytes(M, v, mixed, direct, nu=NU):
         if d < md:
             nx, ny = nx // rx[d], ny // ry[d]
     bottom = len(levels) - 1
+    total = 11 * 8 * v.nx * v.ny
+    if direct and large:
+        dc = next((d for d, (a, b) in enumerate(levels) if a * b <= 1024), bottom)
+        if 64 < levels[dc][0] * levels[dc][1] <= 1024:
+            bottom = dc
+            nb = levels[dc][0] * levels[dc][1]
+            total += 8 * nb * (nb + 2)
+            direct = False
     if direct:
         bottom = next((d for d, (a, b) in enumerate(levels) if a * b <= 64), bottom)
-    total = 11 * 8 * v.nx * v.ny
     for d in range(bottom):
         n = levels[d][0] * levels[d][1]
         w = 4 if (mixed and n > 1024) else 8
@@ -548,8 +560,8 @@ def main():
     v, geo, rhs, bc, _ = workload(args.n)
     base_flags = M.FLAG_DIRICHLET_COUPLED_DIAG
     fp64_flags = base_flags | {"krylov": M.FLAG_KRYLOV, "gmres": M.FLAG_GMRES, "vcycle": 0}[args.solver]
-    if args.solver != "vcycle" and args.coarse == "direct":
-        fp64_flags |= M.FLAG_DIRECT_COARSE
+    if args.solver != "vcycle" and args.coarse != "reference":
+        fp64_flags |= M.FLAG_DIRECT_COARSE | (M.FLAG_DIRECT_LARGE if args.coarse == "large" else 0)
     flags = fp64_flags | (M.FLAG_MIXED if args.precision == "mixed" else 0)
     solver = M.Solver(v, geo, bc, M.KIND_MG, flags)
     phi_d = BoxData(v, 1, 1).to_device()
@@ -653,11 +665,13 @@ def main():
                 "peak_kind": peak_kind, "traffic": (tr or {}).get("bytes_per_sweep"),
                 "alg_bytes_per_sweep": alg_bytes, "sweep_us": sweep_s * 1e6}
 
-    vb = vcycle_bytes(M, v, args.precision == "mixed", bool(fp64_flags & M.FLAG_DIRECT_COARSE))
+    vb = vcycle_bytes(M, v, args.precision == "mixed", bool(fp64_flags & M.FLAG_DIRECT_COARSE),
+                      large=bool(fp64_flags & M.FLAG_DIRECT_LARGE))
     vc_s = (total_ms / args.steps) * 1e-3 / max(last.iterations, 1)
     vcycle_roofline = {"bytes_per_vcycle": vb, "s_per_vcycle": vc_s, "achieved": vb / vc_s / 1e9, "peak": peak,
                        "unit": "GB/s", "frac": vb / vc_s / 1e9 / peak,
-                       "note": "whole V-cycle, algorithmic bytes of every level (bottom solve as time); the time is "
+                       "note": "whole V-cycle, algorithmic bytes of every level (bottom solve as time, the large bottom's "
+                               "product with its inverse as bytes); the time is "
                                "the solve's divided by its V-cycles, Krylov vector work included"}
 
     line = {
@@ -670,8 +684,11 @@ def main():
                                  if args.precision == "mixed" else "FP64"),
                    "flags": "dirichlet_coupled_diag" + ("" if args.solver == "vcycle" else "|" + args.solver) +
                             ("|mixed" if args.precision == "mixed" else "") +
-                            ("|direct_coarse" if fp64_flags & M.FLAG_DIRECT_COARSE else ""),
-                   "bottom": ("exact solve of the first level <= 64 cells" if fp64_flags & M.FLAG_DIRECT_COARSE
+                            ("|direct_coarse" if fp64_flags & M.FLAG_DIRECT_COARSE else "") +
+                            ("|direct_large" if fp64_flags & M.FLAG_DIRECT_LARGE else ""),
+                   "bottom": ("exact solve of the first level <= 1024 cells (inverse built on the device)"
+                              if fp64_flags & M.FLAG_DIRECT_LARGE else
+                              "exact solve of the first level <= 64 cells" if fp64_flags & M.FLAG_DIRECT_COARSE
                               else "relax + BiCGStab to 1e-6 (reference)"),
                    "vcycles_per_solve": last.iterations, "final_relres": last.final_relres,
                    "maxdepth": last.maxdepth, "l2": "flushed between steps (256 MiB write, outside step events)",

@@ -166,6 +166,15 @@ typedef struct mgp_report {
  * end, and the solve restarts from it if it has not passed.  No reference
  * counterpart. */
 #define MGP_FLAG_GMRES 32
+/* with MGP_FLAG_DIRECT_COARSE: the exact bottom is the first level of at
+ * most 1024 cells (the level where the single-CTA coarse cycle would start)
+ * instead of 64, so no coarse cycle runs: its operator's inverse is built by
+ * Gauss-Jordan elimination with partial pivoting on the device when the
+ * solver is created (n + 3 launches, 40 n^2 bytes of scratch) and applied by
+ * one kernel over many CTAs, one warp per row.  Where that level has more
+ * than 1024 cells, or lies below a level of at most 64, MGP_FLAG_DIRECT_COARSE
+ * alone applies.  No reference counterpart. */
+#define MGP_FLAG_DIRECT_LARGE 64
 
 /* Solver kinds for the resident-hierarchy handle. */
 #define MGP_KIND_MG 0   /* module MGPoisson2D (vcycle, fmg)                  */

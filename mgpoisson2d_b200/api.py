@@ -27,6 +27,7 @@ FLAG_KRYLOV = 4
 FLAG_MIXED = 8
 FLAG_DIRECT_COARSE = 16
 FLAG_GMRES = 32
+FLAG_DIRECT_LARGE = 64
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libmgp2d.so")
@@ -493,5 +494,5 @@ class Server:
 __all__ = ["vcycle", "fmg", "dc_vcycle", "Solver", "fill_ghosts", "extrapolate_ghosts", "compute_invdiags",
            "compute_laplacian", "compute_residual", "compute_pd", "compute_grad", "fill_boundary_fluxes", "compute_div", "relax_gs", "relax_jacobi", "solve_bicgstab2", "solve_bicgstab2_noalloc", "NOALLOC_MAX_SIDE", "restrict", "prolong", "pnorm",
            "inner_prod", "estimate_maxdepth", "create_mgschedule", "MGPError", "library_path", "kernel_launch_count",
-           "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV", "FLAG_MIXED", "FLAG_DIRECT_COARSE", "FLAG_GMRES", "Batch", "Server", "map_geometry", "map_fourier_rhs",
+           "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV", "FLAG_MIXED", "FLAG_DIRECT_COARSE", "FLAG_GMRES", "FLAG_DIRECT_LARGE", "Batch", "Server", "map_geometry", "map_fourier_rhs",
            "MAP_IDENTITY", "MAP_WAVY_EXP", "MAP_SKEW_LAYER", "EXPORTS", "KIND_MG", "KIND_DD"]

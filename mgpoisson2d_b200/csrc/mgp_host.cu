@@ -265,9 +265,11 @@ struct mgp_solver {
     Lv* d_shadow = nullptr; // coarse levels' shared-memory layout (offsets), or nullptr
     int shadow_bytes = 0;
     // MGP_FLAG_DIRECT_COARSE: level db (>= dc) is the V-cycle's bottom, solved
-    // with d_ainv, its operator's inverse (transposed); db = -1 without
+    // with d_ainv, its operator's inverse (transposed); db = -1 without.
+    // direct_large: db == dc, d_ainv row-major, applied by launch_direct_apply
     int db = -1;
     double* d_ainv = nullptr;
+    bool direct_large = false;
     // coarse cycle as a cooperative grid of grid_ctas CTAs (0: one CTA)
     int grid_ctas = 0;
     GridCtl gctl{};
@@ -398,6 +400,44 @@ bool invert_dense(std::vector<double> a, int n, std::vector<double>* inv) {
     return true;
 }
 
+// MGP_FLAG_DIRECT_LARGE: level dc (at most kDirectLargeCells cells) becomes
+// the bottom.  Its operator is assembled as in build_direct_coarse and
+// inverted on the device (launch_invert); a pivot below 1e-13 of the largest
+// entry keeps the reference bottom, as the host inversion does.
+int build_direct_large(mgp_solver* s, cudaStream_t st) {
+    const Lv& L = s->lv[s->dc];
+    const int n = L.nx * L.ny;
+    const size_t sz = (size_t)(L.nx + 2) * (L.ny + 2);
+    double *scratch = nullptr, *A = nullptr;
+    int* iw = nullptr;
+    // scratch: the columns' 2 n fields, later the elimination's 4 n^2 + 1 doubles
+    const size_t ns = std::max(2 * sz * n, 4 * (size_t)n * n + 1);
+    if (cudaMalloc(&scratch, sizeof(double) * ns) != cudaSuccess ||
+        cudaMalloc(&A, sizeof(double) * n * n) != cudaSuccess ||
+        cudaMalloc(&iw, sizeof(int) * (2 * n + 1)) != cudaSuccess) {
+        cudaGetLastError();
+        if (scratch) cudaFree(scratch);
+        if (A) cudaFree(A);
+        return set_err(MGP_ENOMEM, "device allocation failed");
+    }
+    int fail = 1;
+    cudaError_t e = launch_direct_columns(L, scratch, A, st);
+    if (e == cudaSuccess) e = launch_invert(A, n, A, scratch, iw, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&fail, iw + 2 * n, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(scratch);
+    cudaFree(iw);
+    if (e != cudaSuccess || fail) {
+        cudaFree(A);
+        if (e != cudaSuccess) return set_err(MGP_ECUDA, "direct coarse operator: %s", cudaGetErrorString(e));
+        return MGP_OK;   // singular to working precision: keep the reference bottom
+    }
+    s->d_ainv = A;
+    s->db = s->dc;
+    s->direct_large = true;
+    return MGP_OK;
+}
+
 // MGP_FLAG_DIRECT_COARSE: the first level from dc down with at most
 // kDirectCells cells becomes the bottom, solved with its operator's inverse.
 // The operator (homogeneous BCs) is assembled on the device column by column,
@@ -407,6 +447,9 @@ int build_direct_coarse(mgp_solver* s, cudaStream_t st) {
     bool diri = false;
     for (int k = 0; k < 4; ++k) diri = diri || s->types[k] == MGP_BCTYPE_DIRI;
     if (!diri) return MGP_OK;
+    if ((s->flags & MGP_FLAG_DIRECT_LARGE) && (long)s->lv[s->dc].nx * s->lv[s->dc].ny <= kDirectLargeCells &&
+        (long)s->lv[s->dc].nx * s->lv[s->dc].ny > kDirectCells)
+        return build_direct_large(s, st);
     int db = -1;
     for (int d = s->dc; d <= s->maxdepth; ++d)
         if ((long)s->lv[d].nx * s->lv[d].ny <= kDirectCells) {
@@ -791,12 +834,17 @@ int prolong_level(mgp_solver* s, int d, int order) {
 }
 
 int coarse_cycle(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
+    if (s->direct_large && d == s->db) {   // the exact bottom at dc
+        const Lv& L = s->lv[d];
+        CK(launch_direct_apply(L.e, L.r, s->d_ainv, L.nx, L.ny, s->stream));
+        return MGP_OK;
+    }
     CoarseArgs a;
     a.lv = s->d_lv;
     a.d0 = d;
     // the exact bottom serves cycles that reach it from above (fmg's cycles
     // that start below it keep the reference bottom)
-    const bool direct = s->d_ainv && d <= s->db;
+    const bool direct = s->d_ainv && !s->direct_large && d <= s->db;
     a.maxdepth = direct ? s->db : s->maxdepth;
     a.ainv = direct ? s->d_ainv : nullptr;
     a.numcycles = numcycles;

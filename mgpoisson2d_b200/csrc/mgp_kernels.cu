@@ -1525,6 +1525,162 @@ cudaError_t launch_direct_columns(const Lv& L, double* scratch, double* A, cudaS
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Gauss-Jordan inversion on the device (the exact bottom of
+// MGP_FLAG_DIRECT_LARGE).  X = [A | I], n x 2n row-major, is reduced one
+// pivot per launch, each launch reading one buffer and writing the other.
+// Step c's pivot is the unused row with the largest |X[r][c]| (the lowest
+// such row on ties), found by every CTA alike; rows are never swapped:
+// mark[r] records the step that took row r, prow[c] the pivot row of step c,
+// and at the end row prow[c] of the right half is row c of A^-1.  Each
+// update is X[r][k] - X[r][c] * (X[p][k] * (1 / X[p][c])), the pivot row
+// scaled first, as in the textbook elimination.
+// ---------------------------------------------------------------------------
+constexpr int kGjThreads = 256;
+constexpr int kGjRows = 32;   // rows of X per CTA and step
+
+// X = [A | I]; mark[r] = n (unused); fail = 0; amax = max |A| (CTA 0, in order of threads, then a tree).
+__global__ void __launch_bounds__(kGjThreads) k_gj_init(const double* A, int n, double* X, int* mark, int* fail,
+                                                        double* amax) {
+    const long nn = (long)n * n;
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < nn; q += (long)gridDim.x * blockDim.x) {
+        const long r = q / n, k = q - r * n;
+        X[r * 2 * n + k] = A[q];
+        X[r * 2 * n + n + k] = (r == k) ? 1.0 : 0.0;
+    }
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) mark[r] = n;
+    if (blockIdx.x == 0) {
+        __shared__ double sh[kGjThreads];
+        double m = 0.0;
+        for (long q = threadIdx.x; q < nn; q += blockDim.x) m = fmax(m, fabs(A[q]));
+        sh[threadIdx.x] = m;
+        __syncthreads();
+        for (int h = kGjThreads / 2; h > 0; h >>= 1) {
+            if (threadIdx.x < h) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + h]);
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            *amax = sh[0];
+            *fail = !(sh[0] > 0.0);
+        }
+    }
+}
+
+// One elimination step c: grid (2n / kGjThreads columns, n / kGjRows rows).
+__global__ void __launch_bounds__(kGjThreads) k_gj_step(const double* __restrict__ X, double* __restrict__ Y, int n,
+                                                        int c, int* mark, int* prow, const double* amax, int* fail) {
+    if (*fail) return;
+    __shared__ double sv[kGjThreads];
+    __shared__ int sr[kGjThreads];
+    __shared__ double sf[kGjRows];
+    // this CTA's rows' entries in column c, loaded while the pivot is searched
+    const int r0 = blockIdx.y * kGjRows, r1 = min(n, r0 + kGjRows);
+    if (threadIdx.x < r1 - r0) sf[threadIdx.x] = X[(long)(r0 + threadIdx.x) * 2 * n + c];
+    // pivot search over the rows no earlier step took (mark[r] >= c: step c's
+    // own mark, set below by CTA (0,0), leaves the predicate unchanged); the
+    // mark and the entry are loaded independently
+    double best = -1.0;
+    int br = n;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        const int mk = mark[r];
+        const double v = fabs(X[(long)r * 2 * n + c]);
+        if (mk >= c && v > best) { best = v; br = r; }   // rows ascend per thread: the first maximum stays
+    }
+    sv[threadIdx.x] = best;
+    sr[threadIdx.x] = br;
+    __syncthreads();
+    for (int h = kGjThreads / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            const double o = sv[threadIdx.x + h];
+            const int orr = sr[threadIdx.x + h];
+            if (o > sv[threadIdx.x] || (o == sv[threadIdx.x] && orr < sr[threadIdx.x])) {
+                sv[threadIdx.x] = o;
+                sr[threadIdx.x] = orr;
+            }
+        }
+        __syncthreads();
+    }
+    const int p = sr[0];
+    if (p >= n) {   // no unused row (cannot happen for c < n)
+        if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *fail = 1;
+        return;
+    }
+    const double piv = X[(long)p * 2 * n + c];
+    if (!(fabs(piv) > 1e-13 * *amax)) {
+        if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *fail = 1;
+        return;
+    }
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+        mark[p] = c;
+        prow[c] = p;
+    }
+    const double ip = 1.0 / piv;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 2 * n || (k <= c)) return;   // the left half's columns up to c are never read again
+    const double sk = X[(long)p * 2 * n + k] * ip;
+    if (r1 - r0 == kGjRows) {   // all rows' loads issued before the stores
+        double x[kGjRows];
+#pragma unroll
+        for (int t = 0; t < kGjRows; ++t) x[t] = X[(long)(r0 + t) * 2 * n + k];
+#pragma unroll
+        for (int t = 0; t < kGjRows; ++t) Y[(long)(r0 + t) * 2 * n + k] = (r0 + t == p) ? sk : x[t] - sf[t] * sk;
+    } else {
+        for (int r = r0; r < r1; ++r) {
+            const long q = (long)r * 2 * n + k;
+            Y[q] = (r == p) ? sk : X[q] - sf[r - r0] * sk;
+        }
+    }
+}
+
+// ainv[c][m] = X[prow[c]][n + m] (nothing after a failed step: prow is then incomplete).
+__global__ void k_gj_extract(const double* X, const int* prow, const int* fail, int n, double* ainv) {
+    if (*fail) return;
+    const long nn = (long)n * n;
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < nn; q += (long)gridDim.x * blockDim.x) {
+        const long c = q / n, m = q - c * n;
+        ainv[q] = X[(long)prow[c] * 2 * n + n + m];
+    }
+}
+
+cudaError_t launch_invert(const double* A, int n, double* ainv, double* work, int* iwork, cudaStream_t st) {
+    double *X0 = work, *X1 = work + 2L * n * n, *amax = work + 4L * n * n;
+    int *mark = iwork, *prow = iwork + n, *fail = iwork + 2 * n;
+    const int nb = std::min(1184, (int)((2L * n * n + kGjThreads - 1) / kGjThreads));
+    k_gj_init<<<nb, kGjThreads, 0, st>>>(A, n, X0, mark, fail, amax);
+    const dim3 grid((2 * n + kGjThreads - 1) / kGjThreads, (n + kGjRows - 1) / kGjRows);
+    for (int c = 0; c < n; ++c) {
+        k_gj_step<<<grid, kGjThreads, 0, st>>>((c & 1) ? X1 : X0, (c & 1) ? X0 : X1, n, c, mark, prow, amax, fail);
+    }
+    k_gj_extract<<<nb, kGjThreads, 0, st>>>((n & 1) ? X1 : X0, prow, fail, n, ainv);
+    count_launch(n + 2);
+    return cudaGetLastError();
+}
+
+// e_k = sum_m ainv[k][m] r_m: r staged in shared memory, one warp per row k,
+// lanes over m in steps of 32, then a butterfly of shuffles (a fixed order).
+constexpr int kDirectApplyThreads = 256;
+__global__ void __launch_bounds__(kDirectApplyThreads) k_direct_apply(DF e, DF r, const double* ainv, int nx,
+                                                                      int n) {
+    __shared__ double rs[kDirectLargeCells];
+    for (int m = threadIdx.x; m < n; m += blockDim.x) rs[m] = AT(r, m % nx, m / nx);
+    __syncthreads();
+    const int k = blockIdx.x * (kDirectApplyThreads / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (k >= n) return;
+    const double* row = ainv + (long)k * n;
+    double s = 0.0;
+#pragma unroll 8
+    for (int m = lane; m < n; m += 32) s = s + row[m] * rs[m];
+    for (int o = 16; o > 0; o >>= 1) s = s + __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) AT(e, k % nx, k / nx) = s;
+}
+
+cudaError_t launch_direct_apply(const DF& e, const DF& r, const double* ainv, int nx, int ny, cudaStream_t st) {
+    const int n = nx * ny, w = kDirectApplyThreads / 32;
+    k_direct_apply<<<(n + w - 1) / w, kDirectApplyThreads, 0, st>>>(e, r, ainv, nx, n);
+    count_launch();
+    return cudaGetLastError();
+}
+
 // Per device: opt the shared-memory coarse kernel into its largest window.
 cudaError_t coarse_kernels_init() {
     static std::mutex mu;

@@ -39,6 +39,9 @@ struct CoarseArgs {
 // Largest bottom level solved by its precomputed inverse (cells); b_direct
 // gives each row four threads of the coarse CTA.
 constexpr int kDirectCells = 64;
+// Largest bottom of MGP_FLAG_DIRECT_LARGE (cells): the coarse-cycle level,
+// solved by launch_direct_apply.
+constexpr int kDirectLargeCells = 1024;
 
 constexpr int kMaxCoarseLevels = 16;
 // Largest staged coarse hierarchy (bytes of dynamic shared memory).
@@ -201,6 +204,15 @@ int coarse_grid_ctas_max();
 // (n = nx * ny columns, one CTA each; scratch holds 2 n fields of
 // (nx + 2) x (ny + 2)).
 cudaError_t launch_direct_columns(const Lv& L, double* scratch, double* A, cudaStream_t st);
+// Inverse of the n x n row-major A by Gauss-Jordan elimination with partial
+// pivoting on the device, into ainv (row-major, may alias A).  work holds
+// 4 n^2 + 1 doubles, iwork 2 n + 1 ints; *fail (in iwork) ends nonzero when a
+// pivot fell below 1e-13 of the largest |A| entry (singular to working
+// precision).  Launches n + 3 kernels.
+cudaError_t launch_invert(const double* A, int n, double* ainv, double* work, int* iwork, cudaStream_t st);
+// e = ainv r on the level's cells (n = nx * ny <= kDirectLargeCells; cells
+// numbered i fastest), one warp per row.
+cudaError_t launch_direct_apply(const DF& e, const DF& r, const double* ainv, int nx, int ny, cudaStream_t st);
 cudaError_t launch_bicgstab(const BicgArgs& a, cudaStream_t st);
 cudaError_t launch_relax_block(const Lv& L, const DF& phi, const DF& rhs, int homog, double omega, int sweeps,
                                int dd, int* status, cudaStream_t st);

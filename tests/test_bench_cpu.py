@@ -30,6 +30,9 @@ def test_vcycle_bytes_bench_grid():
     assert bench.vcycle_bytes(M, v, True, True) == _by_hand(sides, 7, True)
     # the reference bottom (4 x 4, level 8) in plain FP64
     assert bench.vcycle_bytes(M, v, False, False) == _by_hand(sides, 8, False)
+    # exact bottom on the first level of at most 1024 cells (32 x 32, level
+    # 5), plus one read of its 1024 x 1024 inverse and of r and e
+    assert bench.vcycle_bytes(M, v, True, True, large=True) == _by_hand(sides, 5, True) + 8 * 1024 * 1026
 
 
 def test_vcycle_bytes_scales_with_word_size():

@@ -663,6 +663,91 @@ def test_direct_coarse_with_fmg(M):
     assert np.abs(sols[1] - sols[0]).max() <= 1e-7 * np.abs(sols[0]).max()
 
 
+# MGP_FLAG_DIRECT_LARGE: the bottom is the first level of at most 1024 cells,
+# inverted on the device by Gauss-Jordan elimination
+@pytest.mark.parametrize("case", ["DDDD-U", "DNND-mixed", "PPDD", "DDNN-U"])
+@pytest.mark.parametrize("nx,ny", [(32, 32), (64, 16), (12, 20)])
+def test_direct_large_solves_a_coarse_sized_grid_in_one_cycle(M, case, nx, ny):
+    """A grid of 240..1024 cells is its own bottom level: one V-cycle is the
+    exact solve, against numpy's dense solve of the oracle's operator."""
+    v, geo, rhs, bc, _ = _problem(case, nx, ny, 5)
+    res = BoxData(v)
+    O.compute_residual(res, rhs, BoxData(v, 1, 1), geo, bc, False)
+    A = _oracle_operator(v, geo, bc)
+    want = np.linalg.solve(A, res.interior().reshape(-1, order="F")).reshape((nx, ny), order="F")
+    fl = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_DIRECT_COARSE | M.FLAG_DIRECT_LARGE
+    with M.Solver(v, geo, bc, KIND_MG, fl) as s:
+        phi = BoxData(v, 1, 1)
+        r = s.vcycle(phi, rhs, bc, False, 1e-11, 5)
+    assert r.status == 0 and r.iterations == 1 and r.final_relres <= 1e-11, (r.iterations, r.final_relres)
+    assert np.abs(phi.interior() - want).max() <= 1e-10 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("solver", ["krylov", "gmres"])
+@pytest.mark.parametrize("mixed", [False, True])
+def test_direct_large_vcycle_converges_to_oracle_solution(M, solver, mixed):
+    """On the stretched grid the bottom is 32 x 32 instead of 8 x 8: the
+    Krylov(V-cycle) solve reaches 1e-10, deterministically, and the oracle's
+    FP64 solution.  The coarse operators are restrictions of the geometry,
+    not Galerkin products, so the exact 32 x 32 solve is not always the
+    better preconditioner: BiCGStab took 64 V-cycles against 57 with the 8 x 8
+    bottom (71 against 55 in mixed precision); GMRES no more."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, _ = W.wavy_stretched(128)
+    base = (M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_DIRECT_COARSE | (M.FLAG_MIXED if mixed else 0) |
+            (M.FLAG_KRYLOV if solver == "krylov" else M.FLAG_GMRES))
+    old = _set_coupled(M, True)
+    try:
+        po = BoxData(v, 1, 1)
+        O.vcycle(po, rhs, geo, bc, True, 1e-11, 3000, gs_order=1)
+    finally:
+        _set_coupled(M, old)
+    with M.Solver(v, geo, bc, KIND_MG, base) as s:
+        ps = BoxData(v, 1, 1)
+        rs = s.vcycle(ps, rhs, bc, True, 1e-10, 3000)
+    with M.Solver(v, geo, bc, KIND_MG, base | M.FLAG_DIRECT_LARGE) as s:
+        pd = BoxData(v, 1, 1)
+        rd = s.vcycle(pd, rhs, bc, True, 1e-10, 3000)
+        pd2 = BoxData(v, 1, 1)
+        rd2 = s.vcycle(pd2, rhs, bc, True, 1e-10, 3000)
+    assert rd.status == 0 and not rd.diverged and rd.final_relres <= 1e-10
+    assert rd.iterations <= (rs.iterations if solver == "gmres" else 1.5 * rs.iterations), (rd.iterations,
+                                                                                         rs.iterations)
+    assert same(pd.data, pd2.data) and np.array_equal(rd.relres, rd2.relres)   # deterministic
+    err = pd.interior() - po.interior()
+    assert np.linalg.norm(err) / np.linalg.norm(po.interior()) < 1e-8
+    assert np.abs(err).max() / np.abs(po.interior()).max() < 1e-7
+
+
+def test_direct_large_keeps_the_reference_bottom_when_singular(M):
+    """All-Neumann: the bottom operator is singular, the flags change nothing."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, _ = W.terrain_neumann(64, O.boundary_fluxes, O.compute_laplacian)
+    out = []
+    for fl in (0, M.FLAG_DIRECT_COARSE | M.FLAG_DIRECT_LARGE):
+        with M.Solver(v, geo, bc, KIND_MG, fl) as s:
+            p = BoxData(v, 1, 1)
+            r = s.vcycle(p, rhs, bc, False, 1e-9, 200)
+        out.append((p, r))
+    assert same(out[0][0].data, out[1][0].data) and np.array_equal(out[0][1].relres, out[1][1].relres)
+
+
+def test_direct_large_with_fmg(M):
+    """fmg's cycles that start below the 32 x 32 level keep the reference
+    bottom; the solve reaches the same solution as without the flags."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, _ = W.wavy_stretched(128)
+    sols = []
+    for fl in (M.FLAG_DIRICHLET_COUPLED_DIAG,
+               M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_DIRECT_COARSE | M.FLAG_DIRECT_LARGE):
+        with M.Solver(v, geo, bc, KIND_MG, fl) as s:
+            p = BoxData(v, 1, 1)
+            r = s.fmg(p, rhs, bc, True, 1e-10, 2000)
+        assert r.status == 0 and r.final_relres <= 1e-10
+        sols.append(p.interior())
+    assert np.abs(sols[1] - sols[0]).max() <= 1e-7 * np.abs(sols[0]).max()
+
+
 # ---------------------------------------------------------------------------
 # Batches and the solve server: every result identical to solving alone
 # ---------------------------------------------------------------------------
