@@ -377,3 +377,102 @@ def krylov_vcycle(phi: BoxData, rhs: BoxData, geo: GeoData, bc: BdryData, homog:
         if (passed and relres[k] <= tol) or k >= maxiters:
             fill_ghosts(phi, bc, geo, homog, False)
             return relres
+
+
+def gmres_vcycle(phi: BoxData, rhs: BoxData, geo: GeoData, bc: BdryData, homog: bool, tol: float,
+                 maxiters: int, restart: int = 64, numcycles: int = 1, smooth_down: int = 8, smooth_up: int = 8,
+                 smooth_bottom: int = 8, gs_order: int = 1):
+    """Oracle for the solver's MGP_FLAG_GMRES mode (no Fortran counterpart).
+
+    Restarted, right-preconditioned GMRES(restart) (Saad and Schultz, SIAM J.
+    Sci. Stat. Comput. 7, 1986) on L_h e = r0, L_h and the V-cycle
+    preconditioner as in ``krylov_vcycle``, the preconditioned vectors kept
+    (flexible form).  Each step: one V-cycle, w = L_h z_j, one pass of
+    classical Gram-Schmidt (every coefficient from the same w), Givens
+    rotations.  At convergence of the rotated residual, a breakdown or
+    ``restart`` steps: phi += Z y, the true residual rhs - L[phi] replaces the
+    last history entry, and the solve restarts from it if it has not passed.
+    Inner products are unweighted; the history is weighted like the
+    reference's norms (sqrt(dx dy)).  Returns the relative-residual history,
+    one entry per V-cycle; it agrees with the device's to rounding.
+    """
+    v = rhs.valid
+    vol = v.dx * v.dy
+    sv = float(np.sqrt(vol))
+
+    def true_residual():
+        rb = BoxData(v)
+        compute_residual(rb, rhs, phi, geo, bc, homog)
+        return rb.interior().copy()
+
+    def precond(x):
+        e, f = BoxData(v, 1, 1), BoxData(v)
+        f.interior()[:] = x
+        rep = vcycle(e, f, geo, bc, True, 0.0, 1, numcycles=numcycles, smooth_down=smooth_down,
+                     smooth_up=smooth_up, smooth_bottom=smooth_bottom, zerophi=True, gs_order=gs_order)
+        if rep.diverged:
+            raise RuntimeError("preconditioning V-cycle raised the residual")
+        lap = BoxData(v)
+        compute_laplacian(lap, e, geo, bc, True)
+        return e.interior().copy(), lap.interior().copy()
+
+    m = restart
+    r = true_residual()
+    rscale = sv * float(np.sqrt(np.sum(r * r)))
+    relres = [1.0]
+    if rscale == 0.0:
+        relres, rscale = [0.0], 1.0
+    if relres[0] <= tol:
+        return relres
+    x = phi.interior()
+    k = 0
+    while True:
+        beta = float(np.sqrt(np.sum(r * r)))
+        if not (beta > 0.0) or not np.isfinite(beta):
+            return relres
+        V, Z = [r / beta], []
+        H = np.zeros((m + 1, m))
+        cs, sn, g = np.zeros(m), np.zeros(m), np.zeros(m + 1)
+        g[0] = beta
+        jend = 0
+        for j in range(m):
+            if k >= maxiters:
+                break
+            z, w = precond(V[j])
+            k += 1
+            Z.append(z)
+            h = np.array([float(np.sum(w * V[i])) for i in range(j + 1)])
+            for i in range(j + 1):
+                w = w - h[i] * V[i]
+            hn = float(np.sqrt(np.sum(w * w)))
+            col = np.zeros(m + 1)
+            col[:j + 1] = h
+            col[j + 1] = hn
+            for i in range(j):   # earlier rotations
+                t = cs[i] * col[i] + sn[i] * col[i + 1]
+                col[i + 1] = -sn[i] * col[i] + cs[i] * col[i + 1]
+                col[i] = t
+            den = float(np.hypot(col[j], col[j + 1]))
+            cs[j] = col[j] / den if den > 0.0 else 1.0
+            sn[j] = col[j + 1] / den if den > 0.0 else 0.0
+            col[j], col[j + 1] = den, 0.0
+            H[:, j] = col
+            g[j + 1] = -sn[j] * g[j]
+            g[j] = cs[j] * g[j]
+            jend = j + 1
+            relres.append(float(abs(g[j + 1]) * sv / rscale))
+            if relres[-1] <= tol or not (hn > 0.0) or not (den > 0.0):
+                break
+            V.append(w * (1.0 / hn))
+        if jend == 0:
+            return relres
+        y = np.zeros(jend)
+        for i in range(jend - 1, -1, -1):   # H y = g, upper triangular
+            y[i] = (g[i] - float(np.dot(H[i, i + 1:jend], y[i + 1:jend]))) / H[i, i]
+        for i in range(jend):
+            x[:] = x + y[i] * Z[i]
+        r = true_residual()
+        relres[k] = sv * float(np.sqrt(np.sum(r * r))) / rscale
+        if relres[k] <= tol or k >= maxiters:
+            fill_ghosts(phi, bc, geo, homog, False)
+            return relres

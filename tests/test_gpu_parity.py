@@ -522,6 +522,34 @@ def test_gmres_vcycle_converges_to_oracle_solution(M, mixed):
     assert np.abs(err).max() / np.abs(po.interior()).max() < 1e-7
 
 
+@pytest.mark.parametrize("n", [64, 128])
+def test_gmres_vcycle_matches_oracle(M, n):
+    """Same V-cycles as the oracle's GMRES restatement (bit-exact in the device
+    order, the reference bottom); inner products are summed in a different
+    order, so the histories agree to rounding.  The converged solution
+    matches the oracle's GMRES and plain V-cycle solutions."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, _ = W.wavy_stretched(n)
+    old = _set_coupled(M, True)
+    try:
+        pa, pc = BoxData(v, 1, 1), BoxData(v, 1, 1)
+        ra = O.gmres_vcycle(pa, rhs, geo, bc, True, 1e-10, 400)
+        O.vcycle(pc, rhs, geo, bc, True, 1e-10, 2000, gs_order=1)
+    finally:
+        _set_coupled(M, old)
+    with M.Solver(v, geo, bc, KIND_MG, M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_GMRES) as s:
+        pb = BoxData(v, 1, 1)
+        rb = s.vcycle(pb, rhs, bc, True, 1e-10, 400)
+    assert rb.status == 0 and rb.final_relres <= 1e-10 and rb.relres[-1] == rb.final_relres
+    assert abs(rb.iterations - (len(ra) - 1)) <= 2, (rb.iterations, len(ra) - 1)
+    k = min(12, len(ra), len(rb.relres))
+    np.testing.assert_allclose(rb.relres[:k], ra[:k], rtol=1e-6)
+    for ref in (pa, pc):
+        err = pb.interior() - ref.interior()
+        assert np.linalg.norm(err) / np.linalg.norm(ref.interior()) < 1e-8
+    np.testing.assert_allclose(pb.data, pa.data, rtol=0, atol=1e-9 * np.abs(pa.data).max())   # ghosts too
+
+
 def test_gmres_restarts(M):
     """One sweep down and up per V-cycle on 256^2: the solve needs more V-cycles
     than the restart length (64), so it restarts from the true residual and
