@@ -31,6 +31,28 @@ def test_library_exports_every_declared_symbol():
     assert set(syms) == set(api.EXPORTS)
 
 
+def test_header_constants_match_the_python_binding():
+    """Every MGP_FLAG_*, MGP_KIND_*, MGP_BCTYPE_*, MGP_MAP_* and the no-alloc
+    side limit of include/mgp2d.h has the same value in the Python binding,
+    and the flags are distinct powers of two."""
+    import mgpoisson2d_b200 as pkg
+    import mgpoisson2d_b200.api as api
+    import mgpoisson2d_b200.types as T
+    src = open(os.path.join(ROOT, "include", "mgp2d.h")).read()
+    defs = dict(re.findall(r"^#define MGP_(\w+)\s+\(?(-?\d+)\)?", src, flags=re.M))
+    flags = {k: int(v) for k, v in defs.items() if k.startswith("FLAG_")}
+    assert len(flags) >= 7
+    for k, v in flags.items():
+        assert getattr(api, k) == v and getattr(pkg, k) == v, k
+        assert v > 0 and v & (v - 1) == 0, k
+    assert len(set(flags.values())) == len(flags)
+    for k, v in defs.items():
+        if k.startswith(("KIND_", "MAP_")) or k == "NOALLOC_MAX_SIDE":
+            assert getattr(api, k) == int(v), k
+        elif k.startswith("BCTYPE_"):
+            assert getattr(T, k) == int(v), k
+
+
 def test_version_and_error_strings():
     import mgpoisson2d_b200.api as api
     assert b"sm_100a" in api._lib.mgp_version()
