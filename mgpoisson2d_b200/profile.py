@@ -1,7 +1,7 @@
 """A short, fixed run of the benchmark workload for profilers:
 
-    python -m mgpoisson2d_b200.profile [--n 1024] [--vcycles 2] [--warmup 1] [--mixed] [--krylov]
-                                       [--workload wavy|skew] [--direct]
+    python -m mgpoisson2d_b200.profile [--n 1024] [--vcycles 2] [--warmup 1] [--mixed] [--krylov | --gmres]
+                                       [--workload wavy|skew] [--direct [--direct-large]]
 
 Builds the resident solver for the stretched mapped grid (wavy: the bench
 workload; skew: the skewed boundary-layer manufactured problem), runs `warmup` solves capped at `vcycles` V-cycles, then one more,
@@ -22,7 +22,11 @@ def main():
     p.add_argument("--dd", action="store_true", help="deferred-correction driver")
     p.add_argument("--mixed", action="store_true", help="FP32 grid levels (MGP_FLAG_MIXED)")
     p.add_argument("--krylov", action="store_true", help="BiCGStab acceleration (MGP_FLAG_KRYLOV)")
+    p.add_argument("--gmres", action="store_true", help="GMRES acceleration (MGP_FLAG_GMRES)")
     p.add_argument("--direct", action="store_true", help="exact bottom solve (MGP_FLAG_DIRECT_COARSE)")
+    p.add_argument("--direct-large", action="store_true",
+                   help="with --direct: the exact bottom on the first level of at most 1024 cells "
+                        "(MGP_FLAG_DIRECT_LARGE)")
     p.add_argument("--workload", default="wavy", choices=["wavy", "skew"])
     p.add_argument("--time-smoother", action="store_true", help="also report the finest level's time per sweep")
     a = p.parse_args()
@@ -43,7 +47,9 @@ def main():
     kind = M.KIND_DD if a.dd else M.KIND_MG
     flags = M.FLAG_DIRICHLET_COUPLED_DIAG | (M.FLAG_MIXED if a.mixed else 0) | (M.FLAG_KRYLOV if a.krylov else 0)
     flags |= M.FLAG_TIME_SMOOTHER if a.time_smoother else 0
+    flags |= M.FLAG_GMRES if a.gmres else 0
     flags |= M.FLAG_DIRECT_COARSE if a.direct else 0
+    flags |= M.FLAG_DIRECT_LARGE if a.direct_large else 0
     s = M.Solver(v, geo, bc, kind, flags)
     phi, f = BoxData.device_zeros(v, 1, 1), (rhs.to_device() if a.workload == "wavy" else rhs)
     if a.dd:
