@@ -69,7 +69,9 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--n", type=int, default=N_GRID)
-    p.add_argument("--cpu-vcycles", type=int, default=2, help="V-cycles in the bounded CPU sample")
+    p.add_argument("--cpu-vcycles", type=int, default=4,
+                   help="V-cycles per core in each bounded sample of --impl reference")
+    p.add_argument("--cpu-vcycles-1core", type=int, default=8, help="V-cycles in each cpu_baseline sample")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--solver", default="gmres", choices=["gmres", "krylov", "vcycle"])
@@ -168,71 +170,130 @@ def committed_traffic():
 # --------------------------------------------------------------------------- #
 # CPU legs
 # --------------------------------------------------------------------------- #
-def cpu_sample(n, vcycles):
-    """Time `vcycles` V-cycles of the oracle (lexicographic, as the reference)
-    on this workload, single thread.  Returns seconds per V-cycle."""
+# The oracle (a C restatement of the reference's FP64 solve) is built with
+# -march=native on the host that times it: the same arithmetic (no contraction,
+# no reassociation), tuned for that CPU.
+_CPU = {}
+
+
+def _cpu_oracle():
+    os.environ["MGP_ORACLE_NATIVE"] = "1"
     import ctypes
-    from mgpoisson2d_b200.types import BoxData
     from oracle import oracle as O
     O.lib().or_set_dirichlet_coupled_diagonal.argtypes = [ctypes.c_int]
     O.lib().or_set_dirichlet_coupled_diagonal(1)
+    return O
+
+
+def _cpu_init(n):
+    """Per CPU worker: the workload's inputs and the time of the solve's
+    set-up half (hierarchy, inverse diagonals, first residual: a call with no
+    V-cycle)."""
+    from mgpoisson2d_b200.types import BoxData
+    O = _cpu_oracle()
     v, geo, rhs, bc, _ = workload(n)
-    phi = BoxData(v, 1, 1)
     t0 = time.perf_counter()
-    rep = O.vcycle(phi, rhs, geo, bc, True, TOL, vcycles, smooth_down=NU[0], smooth_up=NU[1], smooth_bottom=NU[2],
-                   gs_order=0)
-    dt = time.perf_counter() - t0
-    return dt / max(rep.iterations, 1), rep.iterations
+    O.vcycle(BoxData(v, 1, 1), rhs, geo, bc, True, TOL, 0, smooth_down=NU[0], smooth_up=NU[1], smooth_bottom=NU[2],
+             gs_order=0)
+    _CPU.update(O=O, prob=(v, geo, rhs, bc), t_setup=time.perf_counter() - t0)
 
 
-def _ref_worker(args):
-    n, vc = args
-    return cpu_sample(n, vc)
+def _cpu_step(vcycles):
+    """One bounded sample: a fresh solve of the workload on the oracle
+    (lexicographic Gauss-Seidel, the reference's stationary V-cycle), stopped
+    after `vcycles` V-cycles.  Returns (seconds, V-cycles run, set-up seconds)."""
+    from mgpoisson2d_b200.types import BoxData
+    O = _CPU["O"]
+    v, geo, rhs, bc = _CPU["prob"]
+    t0 = time.perf_counter()
+    rep = O.vcycle(BoxData(v, 1, 1), rhs, geo, bc, True, TOL, vcycles, smooth_down=NU[0], smooth_up=NU[1],
+                   smooth_bottom=NU[2], gs_order=0)
+    return time.perf_counter() - t0, rep.iterations, _CPU["t_setup"]
+
+
+def solve_fraction(sec, vcycles, t_setup, vsolve):
+    """Fraction of a full solve (set-up + vsolve V-cycles) that a sample of
+    `vcycles` V-cycles taking `sec` seconds (set-up included) completed."""
+    tvc = max(sec - t_setup, 1e-12) / max(vcycles, 1)
+    return sec / (t_setup + vsolve * tvc)
+
+
+def oracle_vcycles_per_solve(n):
+    """V-cycles of the oracle's full lexicographic solve of this workload: the
+    committed fixture of that solve (tests/golden/make_fixtures.py) at 1024^2,
+    else the count recorded in profiles/vcycles.json."""
+    fx = os.path.join(ROOT, "tests", "golden", "config2_wavy1024.npz")
+    if n == 1024 and os.path.exists(fx):
+        import numpy as np
+        return int(np.load(fx)["iterations"]), "tests/golden/config2_wavy1024.npz (full oracle solve, 1 core)"
+    try:
+        return int(json.load(open(os.path.join(ROOT, "profiles", "vcycles.json")))[str(n)]), "profiles/vcycles.json"
+    except Exception:
+        return 1000, "default"
+
+
+def cpu_baseline_1core(n, vcycles, runs=3):
+    """cpu_baseline: the native oracle on one core, `runs` bounded samples of
+    `vcycles` V-cycles each (in a spawned process, so the timed work shares no
+    interpreter with the GPU process); the median sample's solve fraction per
+    second is the solves/s."""
+    import multiprocessing as mp
+    vsolve, src = oracle_vcycles_per_solve(n)
+    _cpu_oracle().build(force=True)
+    with mp.get_context("spawn").Pool(1, initializer=_cpu_init, initargs=(n,)) as pool:
+        res = [pool.apply(_cpu_step, (vcycles,)) for _ in range(runs)]
+    rates = sorted(solve_fraction(sec, vc, ts, vsolve) / sec for sec, vc, ts in res)
+    med = rates[len(rates) // 2]
+    sec, vc, ts = res[0]
+    return {"value": med, "unit": "solves/s", "cores": 1, "kind": "port",
+            "sample": f"median of {runs} samples of {vcycles} V-cycles of a fresh {n}^2 solve (set-up included) on "
+                      f"the oracle built with -march=native on this host (lexicographic Gauss-Seidel, the "
+                      f"reference's stationary iteration, FP64); a solve = set-up + {vsolve} V-cycles ({src}); "
+                      f"samples {', '.join(f'{r[0]:.2f}' for r in res)} s, set-up {ts:.3f} s",
+            "vcycles_per_solve": vsolve, "s_per_vcycle": (sec - ts) / max(vc, 1)}
 
 
 def run_reference(args):
+    """--impl reference: the reference's algorithm on the CPU, on every host
+    core the process may use.  Each step is one bounded sample per core (a
+    fresh solve stopped after --cpu-vcycles V-cycles, all cores at once); the
+    step's work is the sum over cores of the solve fraction each sample
+    completed, and value = that work over the steps' wall time."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     import multiprocessing as mp
-    cores = os.cpu_count() or 1
-    iters = solve_vcycles_estimate(args.n)
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        cores = os.cpu_count() or 1
+    vsolve, src = oracle_vcycles_per_solve(args.n)
+    _cpu_oracle().build(force=True)
     ctx = mp.get_context("spawn")
-    times = []
-    with ctx.Pool(cores) as pool:
+    walls, work = [], []
+    with ctx.Pool(cores, initializer=_cpu_init, initargs=(args.n,)) as pool:
         for step in range(args.warmup + args.steps):
-            res = pool.map(_ref_worker, [(args.n, args.cpu_vcycles)] * cores)
+            t0 = time.perf_counter()
+            res = pool.map(_cpu_step, [args.cpu_vcycles] * cores, chunksize=1)
+            wall = time.perf_counter() - t0
             if step >= args.warmup:
-                times.append(res)
-    per_vc = [t for step in times for (t, _) in step]
-    tvc = sum(per_vc) / len(per_vc)
-    value = cores / (tvc * iters)
+                walls.append(wall)
+                work.append(sum(solve_fraction(sec, vc, ts, vsolve) for sec, vc, ts in res))
+    value = sum(work) / sum(walls)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tvc * iters * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n": args.n, "tol": TOL, "nu": list(NU), "solver": "vcycle",
-                   "vcycles_per_solve": iters},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(walls) / len(walls),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": args.n, "tol": TOL, "nu": list(NU)},
+        "solver": "vcycle (the reference's stationary iteration, lexicographic Gauss-Seidel)",
+        "solves_per_step": sum(work) / len(work), "vcycles_per_solve": vsolve, "vcycles_per_solve_source": src,
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
-                         "sample": f"{args.cpu_vcycles} V-cycles per core per step of the {args.n}^2 solve "
-                                   f"(oracle, lexicographic Gauss-Seidel); solves/s = cores / "
-                                   f"(s per V-cycle x {iters} V-cycles per solve)"},
+                         "sample": f"per step, {cores} processes each run a fresh {args.n}^2 solve on the oracle "
+                                   f"(-march=native, FP64) for {args.cpu_vcycles} V-cycles at once; a solve = set-up "
+                                   f"+ {vsolve} V-cycles ({src})"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
-
-
-# V-cycles the 1e-10 solve of this workload takes (the device solve reports
-# its own count in every bench line; the CPU legs cannot afford a full solve).
-_VCYCLES = {}
-
-
-def solve_vcycles_estimate(n):
-    path = os.path.join(ROOT, "profiles", "vcycles.json")
-    try:
-        return int(json.load(open(path))[str(n)])
-    except Exception:
-        return _VCYCLES.get(n, 1000)
 
 
 # --------------------------------------------------------------------------- #
@@ -679,7 +740,9 @@ def main():
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64+f32" if args.precision == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n": args.n, "tol": TOL, "nu": list(NU),
-                   "solver": {"krylov": "bicgstab(vcycle)", "gmres": "gmres(vcycle)", "vcycle": "vcycle"}[args.solver],
+                   "l2": "flushed between steps (256 MiB write, outside step events)",
+                   "parallelism": f"replicas{world}"},
+        "solver": {"method": {"krylov": "bicgstab(vcycle)", "gmres": "gmres(vcycle)", "vcycle": "vcycle"}[args.solver],
                    "precision": ("FP32 grid levels, FP64 outer iteration / residual / update / coarse levels"
                                  if args.precision == "mixed" else "FP64"),
                    "flags": "dirichlet_coupled_diag" + ("" if args.solver == "vcycle" else "|" + args.solver) +
@@ -691,8 +754,7 @@ def main():
                               "exact solve of the first level <= 64 cells" if fp64_flags & M.FLAG_DIRECT_COARSE
                               else "relax + BiCGStab to 1e-6 (reference)"),
                    "vcycles_per_solve": last.iterations, "final_relres": last.final_relres,
-                   "maxdepth": last.maxdepth, "l2": "flushed between steps (256 MiB write, outside step events)",
-                   "parallelism": f"replicas{world}"},
+                   "maxdepth": last.maxdepth},
         "latency_ms": latency, "fp64_same_solver": fp64, "plain_vcycle": plain, "accuracy": accuracy,
         "roofline": roofline, "vcycle_roofline": vcycle_roofline, "clocks": clocks, "gpu_launches": launches,
         "unknowns_vcycles_per_s": value * last.iterations * v.nx * v.ny,
@@ -742,12 +804,13 @@ def main():
     if rank == 0 and world == 1 and not args.no_study:
         line["precision_study"] = precision_study(M, [int(x) for x in args.study_sizes.split(",") if x])
     if rank == 0 and world == 1 and not args.no_cpu:
-        tvc, nvc = cpu_sample(args.n, args.cpu_vcycles)
-        iters = solve_vcycles_estimate(args.n)
-        line["cpu_baseline"] = {"value": 1.0 / (tvc * iters), "unit": "solves/s", "cores": 1, "kind": "port",
-                                "sample": f"{nvc} V-cycles of the {args.n}^2 solve on the oracle (lexicographic "
-                                          f"Gauss-Seidel, the reference's stationary iteration), {tvc:.2f} s per "
-                                          f"V-cycle x {iters} V-cycles per solve"}
+        cb = cpu_baseline_1core(args.n, args.cpu_vcycles_1core)
+        line["cpu_baseline"] = cb
+        if plain:   # the same algorithm on both sides: the stationary FP64 V-cycle
+            line["same_algorithm"] = {"gpu_fp64_vcycle_solves_per_s": plain["solves_per_s"],
+                                      "cpu_1core_solves_per_s": cb["value"],
+                                      "ratio": plain["solves_per_s"] / cb["value"],
+                                      "gpu_vcycles": plain["vcycles"], "cpu_vcycles": cb["vcycles_per_solve"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     solver.close()

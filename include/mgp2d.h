@@ -192,6 +192,15 @@ const char *mgp_last_error(void);
 int mgp_set_flags(int flags);
 /* Number of CUDA kernels this process has launched through the library. */
 long long mgp_kernel_launch_count(void);
+/* Diagnostic with no reference counterpart (the Fortran library has no
+ * device waits).  Runs one cooperative grid of nctas CTAs through nbarriers
+ * of the grid barrier that the coarse cycle uses on large bottoms, with every
+ * wait bounded by wait_s seconds; CTA skip_cta (-1: none) exits before the
+ * first barrier, so the other CTAs' waits run out.  Returns MGP_OK when every
+ * barrier opened, MGP_ETIMEOUT when a wait ran out (the kernel still ends:
+ * after the first timeout no barrier waits again), MGP_ENOTSUP without
+ * cooperative launch.  seconds (nullable) receives the kernel's device time. */
+int mgp_selftest_grid_barrier(int nctas, int skip_cta, int nbarriers, double wait_s, double *seconds);
 
 /* ------------------------------------------------------------------------ */
 /* Schedule (MGPoisson2D.f90:38-129)                                          */

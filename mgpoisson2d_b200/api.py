@@ -84,6 +84,7 @@ _SIGS = {
                           _P(C.c_longlong)],
     "mgp_server_wait": [_vp, C.c_longlong, _R, _P(_d), _P(_d)],
     "mgp_server_destroy": [_vp],
+    "mgp_selftest_grid_barrier": [_i, _i, _i, _d, _P(_d)],
 }
 for _name, _args in _SIGS.items():
     _f = getattr(_lib, _name)
@@ -119,6 +120,14 @@ def library_path() -> str:
 
 def kernel_launch_count() -> int:
     return int(_lib.mgp_kernel_launch_count())
+
+
+def selftest_grid_barrier(nctas: int, skip_cta: int = -1, nbarriers: int = 64, wait_s: float = 0.05):
+    """Run the coarse cycle's bounded grid barrier (mgp_selftest_grid_barrier).
+    Returns (status, device seconds); the status is not raised."""
+    sec = C.c_double(0.0)
+    rc = _lib.mgp_selftest_grid_barrier(nctas, skip_cta, nbarriers, wait_s, _r(sec))
+    return int(rc), sec.value
 
 
 def set_flags(flags: int) -> int:

@@ -185,7 +185,8 @@ struct mgp_server {
     int flags = 0;
     size_t budget = 0;
     size_t used = 0;   // bytes of hierarchies alive (running or cached)
-    int running = 0;
+    int running = 0;   // requests taken off the queue and not yet finished
+    int holding = 0;   // of them, those whose hierarchy is admitted (its bytes count in `used`)
     bool stop = false;
     long long next_ticket = 1;
     std::mutex mu;
@@ -249,16 +250,29 @@ void serve(mgp_server* S) {
             }
             if (!sv) {   // admission by device memory
                 bytes = estimate_bytes(&r->valid, S->flags);
-                while (S->used + bytes > S->budget) {
-                    if (evict_one(S, doomed)) continue;
-                    if (S->running <= 1) break;   // nothing else will free memory: try anyway
-                    S->cv_mem.wait(lock);
+                if (bytes > S->budget) {   // could never fit, even with every other hierarchy gone
+                    rc = record_error(MGP_ENOMEM, "server: the request's hierarchy is larger than the memory budget");
+                } else {
+                    // wait for memory only while some admitted request will
+                    // release some; a worker waiting here holds none itself
+                    while (S->used + bytes > S->budget && !S->stop) {
+                        if (evict_one(S, doomed)) continue;
+                        if (S->holding == 0) break;   // nothing left to free: the accounting is all there is
+                        S->cv_mem.wait(lock);
+                    }
+                    if (S->stop) rc = record_error(MGP_EINVAL, "server: stopped before the request was admitted");
                 }
-                S->used += bytes;
+                if (!rc) {
+                    S->used += bytes;
+                    ++S->holding;
+                }
+            } else {
+                ++S->holding;
             }
         }
+        const bool held = !rc;
         for (mgp_solver* d : doomed) mgp_solver_destroy(d);
-        if (!sv) {
+        if (!sv && !rc) {
             rc = solver_create_on(&r->valid, &r->geo, &r->bc, MGP_KIND_MG, S->flags, -1, st, &sv);
             const size_t actual = rc ? 0 : solver_device_bytes(sv);
             std::lock_guard<std::mutex> lock(S->mu);
@@ -293,6 +307,7 @@ void serve(mgp_server* S) {
             r->status = rc;
             r->done = true;
             --S->running;
+            if (held) --S->holding;
         }
         if (drop) mgp_solver_destroy(drop);
         S->cv_done.notify_all();

@@ -680,6 +680,7 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
             return set_err(MGP_ENOMEM, "device allocation failed");
         }
         s->gctl.status = s->d_status;
+        s->gctl.wait_ns = kGridWaitNsDefault;
     }
     // shared-memory layout of the coarse levels for k_coarse_cycle_smem
     {
@@ -1242,9 +1243,13 @@ int gmres_loop(mgp_solver* s, const BCd& ubc, int homog, double tol, int maxiter
             col[j + 1] = 0.0;
             g[j + 1] = -sn[j] * g[j];
             g[j] = cs[j] * g[j];
+            if (!(den > 0.0)) {   // breakdown: column j is singular and stays out of H y = g; restart
+                if (jend == 0) RC(record(beta * sv));   // nothing to add: phi0 and its residual stand
+                break;
+            }
             jend = j + 1;
             RC(record(std::fabs(g[j + 1]) * sv));
-            if (relres[k] <= tol || !(hn > 0.0) || !(den > 0.0)) break;   // converged, or the space is exhausted
+            if (relres[k] <= tol || !(hn > 0.0)) break;   // converged, or the space is exhausted
             CK(launch_axpby(V(j + 1), V(j + 1), 1.0 / hn, 0.0, nx, ny, 0, 0, st));
         }
         if (jend == 0) return MGP_OK;   // maxiters reached before a step
@@ -1355,7 +1360,8 @@ int solver_solve(mgp_solver* s, int which, mgp_array* phi, mgp_array* rhs, const
     }
     CK(cudaEventRecord(s->ev1, st));
     CK(cudaStreamSynchronize(st));
-    if (status == MGP_OK && dstat) status = (dstat == 2) ? MGP_ETIMEOUT : (dstat == 3) ? MGP_ECUDA : MGP_EDIVERGED;
+    if (status == MGP_OK && dstat)
+        status = (dstat == DST_TIMEOUT) ? MGP_ETIMEOUT : (dstat == DST_MISALIGNED) ? MGP_ECUDA : MGP_EDIVERGED;
     if (rep) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, s->ev0, s->ev1);
@@ -1531,6 +1537,46 @@ extern "C" {
 const char* mgp_version(void) { return "mgp2d-b200 0.1 (sm_100a, FP64)"; }
 const char* mgp_last_error(void) { return g_err.c_str(); }
 long long mgp_kernel_launch_count(void) { return launch_count(); }
+
+int mgp_selftest_grid_barrier(int nctas, int skip_cta, int nbarriers, double wait_s, double* seconds) {
+    if (nctas < 2 || nbarriers < 1 || nbarriers > (1 << 20) || !(wait_s > 0.0) || wait_s > 10.0 ||
+        skip_cta >= nctas)
+        return set_err(MGP_EINVAL, "selftest_grid_barrier: bad argument");
+    const int cap = barrier_selftest_ctas_max();
+    if (cap < 2) return set_err(MGP_ENOTSUP, "selftest_grid_barrier: no cooperative launch on this device");
+    if (nctas > cap) return set_err(MGP_EINVAL, "selftest_grid_barrier: more CTAs than the device keeps resident");
+    GridCtl g{};
+    unsigned* bar = nullptr;
+    int* status = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = MGP_OK, dstat = 0;
+    if (cudaMalloc(&bar, 2 * sizeof(unsigned)) != cudaSuccess || cudaMalloc(&status, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        rc = set_err(MGP_ENOMEM, "cudaMalloc failed");
+    }
+    float ms = 0.f;
+    if (!rc) {
+        g.bar = bar;
+        g.status = status;
+        g.wait_ns = (unsigned long long)(wait_s * 1e9);
+        if (cudaMemset(bar, 0, 2 * sizeof(unsigned)) != cudaSuccess || cudaMemset(status, 0, sizeof(int)) != cudaSuccess ||
+            cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess ||
+            cudaEventRecord(e0, 0) != cudaSuccess || launch_barrier_selftest(g, nctas, skip_cta, nbarriers, 0) != cudaSuccess ||
+            cudaEventRecord(e1, 0) != cudaSuccess || cudaMemcpy(&dstat, status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            rc = set_err(MGP_ECUDA, cudaGetErrorString(cudaGetLastError()));
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (bar) cudaFree(bar);
+    if (status) cudaFree(status);
+    if (seconds) *seconds = ms * 1e-3;
+    if (rc) return rc;
+    if (dstat == DST_TIMEOUT) return set_err(MGP_ETIMEOUT, "a grid barrier wait ran out of its limit");
+    if (dstat) return set_err(MGP_ECUDA, "unexpected device status");
+    return MGP_OK;
+}
 
 int mgp_set_flags(int flags) {
     const int old = g_flags;
@@ -1875,7 +1921,11 @@ int mgp_solve_bicgstab2(const mgp_box* valid, mgp_array* phi, const mgp_array* r
     a.dd = 0;
     CK(launch_bicgstab(a, c.st));
     RC(stage_out(a.phi, phi, nx, ny, 1, c.st));
-    return c.finish();
+    int dstat = 0;
+    CK(cudaMemcpyAsync(&dstat, a.status, sizeof(int), cudaMemcpyDeviceToHost, c.st));
+    RC(c.finish());
+    if (dstat) return set_err(MGP_EDIVERGED, "solve_bicgstab2: non-finite residual");
+    return MGP_OK;
 }
 
 int mgp_restrict(const mgp_box* fine_valid, const mgp_array* fine, const mgp_box* crse_valid, mgp_array* crse,

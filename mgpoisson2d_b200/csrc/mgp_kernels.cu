@@ -323,33 +323,48 @@ __device__ __forceinline__ void perimeter_cell(int k, int nx, int ny, int& i, in
 __shared__ GridCtl s_gctl;   // the grid kernel's barrier and partials (set on entry)
 __shared__ int s_gred;       // grid reductions so far (parity of the partials buffer)
 
-// A CTA gives up on a grid barrier after kGridWaitLimit polls (each sleeps up
-// to 256 ns: seconds, far above any real wait) and reports status 2.
+// A CTA gives up on a grid barrier after s_gctl.wait_ns of %globaltimer or
+// kGridWaitLimit polls (each sleeps up to 256 ns), whichever comes first, and
+// records DST_TIMEOUT.  From then on the grid's barriers are out of step, so
+// every CTA that finds the status word set -- on entering a barrier or while
+// polling one -- stops waiting at once: the kernel runs to its end in
+// bounded time (its results are void and the host reports MGP_ETIMEOUT).
 constexpr long kGridWaitLimit = 1L << 24;
+
+__device__ __forceinline__ unsigned long long grid_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ void grid_barrier() {
     __syncthreads();
     if (threadIdx.x == 0) {
-        unsigned* bar = s_gctl.bar;
-        volatile unsigned* gen = bar + 1;
-        const unsigned g0 = *gen;
-        __threadfence();
-        if (atomicAdd(bar, 1u) == gridDim.x - 1) {   // the last to arrive opens the next generation
-            atomicExch(bar, 0u);
+        volatile int* stv = s_gctl.status;
+        if (*stv == DST_OK) {
+            unsigned* bar = s_gctl.bar;
+            volatile unsigned* gen = bar + 1;
+            const unsigned g0 = *gen;
             __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            unsigned nap = 32;
-            for (long k = 0; *gen == g0; ++k) {
-                if (k > kGridWaitLimit) {
-                    atomicExch(s_gctl.status, 2);
-                    break;
+            if (atomicAdd(bar, 1u) == gridDim.x - 1) {   // the last to arrive opens the next generation
+                atomicExch(bar, 0u);
+                __threadfence();
+                atomicAdd(bar + 1, 1u);
+            } else {
+                const unsigned long long t0 = grid_ns();
+                unsigned nap = 32;
+                for (long k = 0; *gen == g0; ++k) {
+                    if (*stv != DST_OK) break;   // another CTA gave up
+                    if (k > kGridWaitLimit || grid_ns() - t0 > s_gctl.wait_ns) {
+                        set_status(s_gctl.status, DST_TIMEOUT);
+                        break;
+                    }
+                    __nanosleep(nap);
+                    nap = nap < 256 ? 2 * nap : nap;
                 }
-                __nanosleep(nap);
-                nap = nap < 256 ? 2 * nap : nap;
             }
+            __threadfence();
         }
-        __threadfence();
     }
     __syncthreads();
 }
@@ -1240,7 +1255,7 @@ __device__ void b_relax(const Lv& L, const DF& phi, const DF& rhs, int homog, do
     else b_relax9<S>(L, phi, rhs, homog, omega, sweeps);
 }
 
-// solve_bicgstab2 (P2:2253-2477; DD:339-566 with dd = 1).  Status: 0 or 3 (non-finite).
+// solve_bicgstab2 (P2:2253-2477; DD:339-566 with dd = 1).  Status: DST_OK or DST_NONFINITE.
 template <class S>
 __device__ int b_bicgstab(const Lv& L, const DF& phi, const DF& rhs, int homog, double tol, int max_iters,
                           int max_restarts, int zerophi, int dd, double* sh) {
@@ -1330,7 +1345,7 @@ __device__ int b_bicgstab(const Lv& L, const DF& phi, const DF& rhs, int homog, 
         }
     }
     b_axpby<S>(phi, e, 1.0, 1.0, nx, ny, 1);
-    return isfinite(norm[0]) ? 0 : 3;
+    return isfinite(norm[0]) ? DST_OK : DST_NONFINITE;
 }
 
 // ---------------------------------------------------------------------------
@@ -1450,7 +1465,7 @@ finish:
 __global__ void __launch_bounds__(kCoarseThreads, 1) k_coarse_cycle(CoarseArgs a) {
     __shared__ double sh[kCoarseThreads];
     const int s = coarse_body<BlockScope>(a.lv, a, sh);
-    if (threadIdx.x == 0 && s) *a.status = s;
+    if (threadIdx.x == 0) set_status(a.status, s);
 }
 
 __device__ void b_copy(const DF& dst, const DF& src, int i0, int i1, int j0, int j1) {
@@ -1504,7 +1519,7 @@ __global__ void __launch_bounds__(kCoarseThreads, 1) k_coarse_cycle_smem(CoarseA
         const Lv &S = sl[k], &G = a.lv[a.d0 + k];
         b_copy(G.e, S.e, -1, S.nx + 1, -1, S.ny + 1);
     }
-    if (threadIdx.x == 0 && s) *a.status = s;
+    if (threadIdx.x == 0) set_status(a.status, s);
 }
 
 __global__ void __launch_bounds__(kCoarseThreads) k_direct_columns(Lv L, double* scratch, double* A) {
@@ -1706,7 +1721,7 @@ __global__ void __launch_bounds__(kCoarseThreads, 1) k_coarse_cycle_grid(CoarseA
     }
     __syncthreads();
     const int s = coarse_body<GridScope>(a.lv, a, sh);
-    if (GridScope::rank() == 0 && s) *a.status = s;
+    if (GridScope::rank() == 0) set_status(a.status, s);
 }
 
 // How many CTAs of k_coarse_cycle_grid the current device can keep resident
@@ -1722,6 +1737,43 @@ int coarse_grid_ctas_max() {
         return 0;
     }
     return coop ? nsm * per_sm : 0;
+}
+
+__global__ void __launch_bounds__(32) k_barrier_selftest(GridCtl g, int skip, int nbar) {
+    if (threadIdx.x == 0) {
+        s_gctl = g;
+        s_gred = 0;
+    }
+    __syncthreads();
+    if ((int)blockIdx.x == skip) return;   // this CTA never arrives
+    for (int k = 0; k < nbar; ++k) grid_barrier();
+}
+
+int barrier_selftest_ctas_max() {
+    int dev = 0, coop = 0, nsm = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_barrier_selftest, 32, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return coop ? nsm * per_sm : 0;
+}
+
+cudaError_t launch_barrier_selftest(const GridCtl& g, int nctas, int skip, int nbar, cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nctas);
+    cfg.blockDim = dim3(32);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, k_barrier_selftest, g, skip, nbar);
+    count_launch();
+    return e;
 }
 
 cudaError_t launch_coarse_cycle(const CoarseArgs& a, cudaStream_t st) {
@@ -1754,7 +1806,7 @@ __global__ void __launch_bounds__(kCoarseThreads, 1) k_bicgstab(BicgArgs a) {
     __shared__ double sh[kCoarseThreads];
     const int s = b_bicgstab<BlockScope>(a.L, a.phi, a.rhs, a.homog, a.tol, a.max_iters, a.max_restarts, a.zerophi,
                                          a.dd, sh);
-    if (threadIdx.x == 0 && s) *a.status = s;
+    if (threadIdx.x == 0) set_status(a.status, s);
 }
 
 cudaError_t launch_bicgstab(const BicgArgs& a, cudaStream_t st) {

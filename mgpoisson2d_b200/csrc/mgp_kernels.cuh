@@ -10,13 +10,33 @@ namespace mgp {
 // Reduction kinds of launch_reduce.
 enum RedKind { RED_SUMSQ = 0, RED_MAXABS = 1, RED_DOT = 2, RED_JSUM = 3, RED_ABSSUM = 4 };
 
-// Parameters of the single-CTA coarse cycle.
+// Values of a solver's device status word.  A kernel records the first error
+// it meets and never overwrites one already there (set_status), so the host
+// sees the cause, not a later consequence.
+enum DevStatus {
+    DST_OK = 0,
+    DST_TIMEOUT = 2,      // a bounded device wait (TMA tile barrier, grid barrier) ran out
+    DST_NONFINITE = 3,    // a non-finite residual in a device-side solve (bottom BiCGStab)
+    DST_MISALIGNED = 4,   // the sweep's shared-memory window was not 128-byte aligned
+};
+#ifdef __CUDACC__
+__device__ __forceinline__ void set_status(int* s, int v) {
+    if (s && v) atomicCAS(s, 0, v);
+}
+#endif
+
+// A grid barrier gives up after this long by default (%globaltimer
+// nanoseconds): far above any real wait between two barriers of the coarse
+// cycle (milliseconds at most).
+constexpr unsigned long long kGridWaitNsDefault = 1000000000ull;
+
 // Barrier and reduction partials of a cooperative grid running the
 // coarse cycle (k_coarse_cycle_grid).
 struct GridCtl {
     unsigned* bar;   // [0] arrivals, [1] generation; arrivals 0 at launch
     double* part;    // 2 x (CTAs) partial sums
-    int* status;     // set to 2 if a barrier wait gives up
+    int* status;     // DST_TIMEOUT if a barrier wait gives up; once nonzero, barriers stop waiting
+    unsigned long long wait_ns;   // a CTA's longest wait at one barrier
 };
 
 struct CoarseArgs {
@@ -117,8 +137,9 @@ void sweep_tma_prepare(SweepTma* t, const DF& ea, const DF& eb, const DF& rhs, c
                        int ny);
 void sweep_tma_prepare(SweepTma* t, const DF32& ea, const DF32& eb, const DF32& rhs, const DF32& invd,
                        const Geo32& g, int nx, int ny);
-// status (nullable) receives 2 if a CTA's staging never completed, 3 if the
-// shared-memory window was not 128-byte aligned (neither is expected).
+// status (nullable) receives DST_TIMEOUT if a CTA's staging never completed,
+// DST_MISALIGNED if the shared-memory window was not 128-byte aligned
+// (neither is expected).
 cudaError_t launch_sweep9(const DF& pin, const DF& pout, const DF& rhs, const DF& invd, const Geo& g, const BCd& b,
                           int homog, int nx, int ny, double omega, const SweepTma* tma, int* status,
                           cudaStream_t st);
@@ -200,6 +221,11 @@ cudaError_t coarse_kernels_init();
 cudaError_t launch_coarse_cycle(const CoarseArgs& a, cudaStream_t st);
 // Largest cooperative grid of the coarse cycle the current device keeps resident (0: none).
 int coarse_grid_ctas_max();
+// A cooperative grid of nctas CTAs (all resident) passing nbar grid barriers;
+// CTA `skip` (if >= 0) exits before the first one, so the others' waits run
+// out.  Exercises the bounded wait of the coarse cycle's grid barrier.
+cudaError_t launch_barrier_selftest(const GridCtl& g, int nctas, int skip, int nbar, cudaStream_t st);
+int barrier_selftest_ctas_max();
 // A[m * n + k] = (L e_k)_m for the level's operator with homogeneous BCs
 // (n = nx * ny columns, one CTA each; scratch holds 2 n fields of
 // (nx + 2) x (ny + 2)).

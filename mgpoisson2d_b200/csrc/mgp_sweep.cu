@@ -371,7 +371,7 @@ __global__ void __launch_bounds__((Win<T, TX, K>::kThreads), (Win<T, TX, K>::kMi
         const unsigned sb = (unsigned)__cvta_generic_to_shared(smem), bar = sb + W::oBarBytes;
         constexpr unsigned kS = sizeof(T);
         if (sb & 127) {   // TMA destinations must be 128-byte aligned
-            if (threadIdx.x == 0 && status) atomicExch(status, 3);
+            if (threadIdx.x == 0) set_status(status, DST_MISALIGNED);
             return;
         }
         if (threadIdx.x == 0) mbar_init(bar, 1);
@@ -400,7 +400,7 @@ __global__ void __launch_bounds__((Win<T, TX, K>::kThreads), (Win<T, TX, K>::kMi
         const bool landed = threadIdx.x >= 32 || mbar_wait0(bar);
         if (!__syncthreads_and(landed)) {   // never seen; leave the tile unwritten and report
             if (threadIdx.x == 0) {
-                if (status) atomicExch(status, 2);
+                set_status(status, DST_TIMEOUT);
                 mbar_wait0(bar);   // let copies still in flight land before the CTA exits
             }
             return;

@@ -21,14 +21,18 @@ from mgpoisson2d_b200.types import (BdryData, Box, BoxData, GeoData, MgpArray, M
                                     MgpBox, MgpGeo, MgpReport, make_report, read_report)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_SO = os.path.join(_HERE, "_build", "libmgp_oracle.so")
+# MGP_ORACLE_NATIVE=1 selects the copy built with -march=native for this host
+# (the timed CPU baseline; same arithmetic, same bits)
+_NATIVE = os.environ.get("MGP_ORACLE_NATIVE", "0") == "1"
+_SO = os.path.join(_HERE, "_build", "libmgp_oracle_native.so" if _NATIVE else "libmgp_oracle.so")
 
 
 def build(force: bool = False) -> str:
     src = [os.path.join(_HERE, f) for f in ("mgp_oracle.c", "mgp_oracle.h")]
     stale = not os.path.exists(_SO) or any(os.path.getmtime(s) > os.path.getmtime(_SO) for s in src)
     if force or stale:
-        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+        subprocess.run(["make", "-s", "-C", _HERE] + (["-B"] if force else []) + (["native"] if _NATIVE else []),
+                       check=True)
     return _SO
 
 

@@ -40,3 +40,30 @@ def test_vcycle_bytes_scales_with_word_size():
     b64 = bench.vcycle_bytes(M, v, False, False)
     b32 = bench.vcycle_bytes(M, v, True, False)
     assert b32 < b64 < 2 * b32 + 11 * 8 * 512 * 512
+
+
+def test_solve_fraction():
+    # a sample of 4 V-cycles of 1 s each after a 0.5 s set-up, in a solve of 100 V-cycles
+    f = bench.solve_fraction(4.5, 4, 0.5, 100)
+    assert abs(f - 4.5 / 100.5) < 1e-12
+    # a whole solve is one solve
+    assert abs(bench.solve_fraction(0.5 + 100 * 0.2, 100, 0.5, 100) - 1.0) < 1e-12
+
+
+def test_reference_arm_is_measured_not_projected():
+    """--impl reference on a small grid: one JSON line whose ms_per_step times
+    the steps fits inside the run's own wall time (the steps' time is measured,
+    not a projection of a whole solve), with the solve fractions it counted."""
+    import json
+    import subprocess
+    import time
+    t0 = time.time()
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--n", "64",
+                          "--steps", "2", "--warmup", "1", "--cpu-vcycles", "2"],
+                         capture_output=True, text=True, check=True, timeout=300).stdout
+    wall = time.time() - t0
+    line = json.loads(out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "solves/s"
+    assert line["ms_per_step"] * line["steps"] / 1e3 <= wall
+    assert abs(line["value"] - line["solves_per_step"] / (line["ms_per_step"] / 1e3)) <= 1e-9 * line["value"]
+    assert line["cpu_baseline"]["cores"] >= 1 and line["e2e"]["h2d_bytes_per_step"] == 0

@@ -231,7 +231,7 @@ def _set_coupled(M, on):
     return M.set_flags(int(on))
 
 
-@pytest.mark.parametrize("n", [32, 64, 256])
+@pytest.mark.parametrize("n", [32, 64, 128, 256])
 def test_vcycle_matches_oracle(M, n):
     from mgpoisson2d_b200 import workloads as W
     old = _set_coupled(M, True)

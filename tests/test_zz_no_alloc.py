@@ -32,23 +32,37 @@ def _problem(nx=40, ny=32, seed=21):
     return v, geo, rhs, bc
 
 
-def test_noalloc_matches_allocating_entry_point_on_two_calls():
-    assert torch.cuda.is_available(), "needs a CUDA device"
-    import mgpoisson2d_b200.api as M
-    v, geo, rhs, bc = _problem()
+def _allocating(v, geo, rhs, bc, M):
     inv = BoxData(v)
     M.compute_invdiags(inv, geo, bc, True)
     ref = BoxData(v, 1, 1)
     M.solve_bicgstab2(ref, rhs, geo, bc, False, inv, 1e-10, 80, 5, False)
-    geo_d, rhs_d, inv_d = geo.to_device(), rhs.to_device(), inv.to_device()
+    return inv, ref
+
+
+def _noalloc(v, geo, rhs, bc, inv, M):
+    phi_d = BoxData(v, 1, 1).to_device()
+    M.solve_bicgstab2_noalloc(phi_d, rhs.to_device(), geo.to_device(), bc, False, inv.to_device(), 1e-10, 80, 5,
+                              False)
+    return phi_d.to_host().interior().copy()
+
+
+def test_noalloc_matches_allocating_entry_point_on_two_calls():
+    """Problem A, then a different problem B (another size and data), then A
+    again: each no-allocation result matches the allocating entry point's, so
+    no call reads what the previous one left in the shared scratch array."""
+    assert torch.cuda.is_available(), "needs a CUDA device"
+    import mgpoisson2d_b200.api as M
+    pa = _problem()
+    pb = _problem(24, 36, seed=5)
+    inv_a, ref_a = _allocating(*pa, M)
+    inv_b, ref_b = _allocating(*pb, M)
     outs = []
-    for _ in range(2):
-        phi_d = BoxData(v, 1, 1).to_device()
-        M.solve_bicgstab2_noalloc(phi_d, rhs_d, geo_d, bc, False, inv_d, 1e-10, 80, 5, False)
-        got = phi_d.to_host()
-        np.testing.assert_allclose(got.interior(), ref.interior(), rtol=1e-9, atol=1e-12)
-        outs.append(got.interior().copy())
-    np.testing.assert_array_equal(outs[0], outs[1])
+    for (v, geo, rhs, bc), inv, ref in ((pa, inv_a, ref_a), (pb, inv_b, ref_b), (pa, inv_a, ref_a)):
+        got = _noalloc(v, geo, rhs, bc, inv, M)
+        np.testing.assert_allclose(got, ref.interior(), rtol=1e-9, atol=1e-12)
+        outs.append(got)
+    np.testing.assert_array_equal(outs[0], outs[2])
 
 
 def test_noalloc_rejects_oversized_grid_and_host_arrays():
