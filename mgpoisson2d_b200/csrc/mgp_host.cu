@@ -1222,9 +1222,15 @@ int gmres_loop(mgp_solver* s, const BCd& ubc, int homog, double tol, int maxiter
             CK(launch_fill(Z(j), L0.g, L0.bc, 1, 0, nx, ny, st));
             CK(launch_apply(V(j + 1), Z(j), L0.r, L0.g, L0.bc, 1, nx, ny, 0, 0, st));
             ++k;
-            CK(launch_mdot(V(j + 1), mv, j + 1, nx, ny, part, kGmresBlocks, h1, st));
-            CK(launch_maxpy(V(j + 1), mv, j + 1, h1, -1.0, nx, ny, st));
-            CK(launch_mdot(V(j + 1), MVec{V(j + 1).p, ld, 0}, 1, nx, ny, part, kGmresBlocks, nrm, st));
+            const cudaError_t gse =
+                launch_gs_pass(V(j + 1), mv, j + 1, nx, ny, part, (long)kGmresBlocks * (m + 1), kGmresBlocks, h1, nrm, st);
+            if (gse == cudaErrorNotSupported) {   // more blocks of cells than partial sums: a pass per step
+                CK(launch_mdot(V(j + 1), mv, j + 1, nx, ny, part, kGmresBlocks, h1, st));
+                CK(launch_maxpy(V(j + 1), mv, j + 1, h1, -1.0, nx, ny, st));
+                CK(launch_mdot(V(j + 1), MVec{V(j + 1).p, ld, 0}, 1, nx, ny, part, kGmresBlocks, nrm, st));
+            } else {
+                CK(gse);
+            }
             CK(cudaMemcpyAsync(hc.data(), h1, sizeof(double) * (m + 2), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             double* col = &H[(size_t)j * (m + 1)];   // column j of the Hessenberg matrix

@@ -26,6 +26,7 @@ static inline dim3 cells_grid(int nx, int ny, dim3 blk) {
     return dim3((unsigned)((nx + blk.x - 1) / blk.x), (unsigned)((ny + blk.y - 1) / blk.y));
 }
 static const dim3 kBlk2(32, 8);
+constexpr int kBlk2N = 256;   // threads of a kBlk2 block (a power of two: the per-block reduction trees)
 
 #define CELL_IJ                                              \
     const int i = blockIdx.x * blockDim.x + threadIdx.x;   \
@@ -722,6 +723,76 @@ cudaError_t launch_mdot(const DF& w, const MVec& V, int nv, int nx, int ny, doub
     k_mdot<<<dim3(nb, nv), kMdotThreads, 0, st>>>(w, V, nx, ny, partials);
     k_mdot_final<<<nv, kMdotThreads, 0, st>>>(partials, nb, out);
     count_launch(2);
+    return cudaGetLastError();
+}
+
+// The multi-dot with kDotVecs basis vectors per launch row: a thread reads
+// w at a cell once for all of its row's vectors, so a pass reads w
+// ceil(nv / kDotVecs) times and each v_k once, where one row per vector read
+// w nv times.  partials[k * gridDim.x + b] = block b's sum of w * v_k.
+constexpr int kDotVecs = 8;
+
+__global__ void __launch_bounds__(kMdotThreads) k_mdot8(DF w, MVec V, int nv, int nx, int ny, double* partials) {
+    __shared__ double sh[kDotVecs][kMdotThreads];
+    const int k0 = blockIdx.y * kDotVecs, kn = min(kDotVecs, nv - k0);
+    const long n = (long)nx * ny;
+    double acc[kDotVecs];
+#pragma unroll
+    for (int q = 0; q < kDotVecs; ++q) acc[q] = 0.0;
+    for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(c % nx), j = (int)(c / nx);
+        const double wv = AT(w, i, j);
+        const double* v = V.p + (long)k0 * V.stride + i + (long)j * V.ld;
+#pragma unroll
+        for (int q = 0; q < kDotVecs; ++q)
+            if (q < kn) acc[q] = acc[q] + wv * v[(long)q * V.stride];
+    }
+#pragma unroll
+    for (int q = 0; q < kDotVecs; ++q) sh[q][threadIdx.x] = acc[q];
+    __syncthreads();
+    for (int h = kMdotThreads / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h)
+#pragma unroll
+            for (int q = 0; q < kDotVecs; ++q) sh[q][threadIdx.x] = sh[q][threadIdx.x] + sh[q][threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x < kn) partials[(long)(k0 + threadIdx.x) * gridDim.x + blockIdx.x] = sh[threadIdx.x][0];
+}
+
+// w -= sum_{k < nv} h[k] v_k (the k_maxpy update, bit for bit) and, per
+// block of cells, the sum of the new w^2 into partials[block] (blocks in
+// row-major order of the launch grid).
+__global__ void k_maxpy_nrm(DF w, MVec V, int nv, const double* h, int nx, int ny, double* partials) {
+    __shared__ double sh[kBlk2N];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int t = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+    double sq = 0.0;
+    if (i < nx && j < ny) {
+        double acc = AT(w, i, j);
+        for (int k = 0; k < nv; ++k) acc = acc + (-1.0 * h[k]) * V.p[(long)k * V.stride + i + (long)j * V.ld];
+        AT(w, i, j) = acc;
+        sq = acc * acc;
+    }
+    sh[t] = sq;
+    __syncthreads();
+    for (int s = nt / 2; s > 0; s >>= 1) {
+        if (t < s) sh[t] = sh[t] + sh[t + s];
+        __syncthreads();
+    }
+    if (t == 0) partials[(long)blockIdx.y * gridDim.x + blockIdx.x] = sh[0];
+}
+
+cudaError_t launch_gs_pass(const DF& w, const MVec& V, int nv, int nx, int ny, double* partials, long cap, int nb,
+                           double* h, double* hnorm, cudaStream_t st) {
+    const dim3 gu = cells_grid(nx, ny, kBlk2);
+    const long nbu = (long)gu.x * gu.y;
+    if (nv < 1 || (long)nb * nv > cap || nbu > cap || kBlk2.x * kBlk2.y != kBlk2N) return cudaErrorNotSupported;
+    k_mdot8<<<dim3(nb, (nv + kDotVecs - 1) / kDotVecs), kMdotThreads, 0, st>>>(w, V, nv, nx, ny, partials);
+    k_mdot_final<<<nv, kMdotThreads, 0, st>>>(partials, nb, h);
+    // the coefficients are summed; their partials are free for the norm's
+    k_maxpy_nrm<<<gu, kBlk2, 0, st>>>(w, V, nv, h, nx, ny, partials);
+    k_mdot_final<<<1, kMdotThreads, 0, st>>>(partials, (int)nbu, hnorm);
+    count_launch(4);
     return cudaGetLastError();
 }
 

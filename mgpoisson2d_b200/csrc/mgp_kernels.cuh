@@ -177,6 +177,12 @@ struct MVec {
 // out[k] = sum over valid cells of w * v_k, k < nv (partials: nb * nv doubles).
 cudaError_t launch_mdot(const DF& w, const MVec& V, int nv, int nx, int ny, double* partials, int nb, double* out,
                         cudaStream_t st);
+// One classical Gram-Schmidt pass: h[k] = w . v_k (k < nv), w -= sum_k h[k] v_k,
+// then *hnorm = |w|^2.  partials holds cap doubles; cudaErrorNotSupported
+// when the pass's partial sums would not fit (the caller then uses
+// launch_mdot and launch_maxpy).
+cudaError_t launch_gs_pass(const DF& w, const MVec& V, int nv, int nx, int ny, double* partials, long cap, int nb,
+                           double* h, double* hnorm, cudaStream_t st);
 // w += sign * sum_{k < nv} coef[k] v_k (coef in device memory).
 cudaError_t launch_maxpy(const DF& w, const MVec& V, int nv, const double* coef, double sign, int nx, int ny,
                          cudaStream_t st);

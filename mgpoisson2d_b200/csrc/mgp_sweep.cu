@@ -506,6 +506,7 @@ __global__ void __launch_bounds__((Win<T, TX, K>::kThreads), (Win<T, TX, K>::kMi
                 const int n1 = n0 + ((syh && ((ny - 1) & 1) == cj) ? ni : 0);
                 const int n2 = n1 + ((sxl && ci == 0) ? nj : 0);
                 const int n3 = n2 + ((sxh && ((nx - 1) & 1) == ci) ? nj : 0);
+                if (n3 == 0) continue;   // no cell of this colour on the tile's sides (uniform per CTA): no barrier
                 for (int k = threadIdx.x; k < n3; k += blockDim.x) {
                     if (k < n0) gs(ia + 2 * k, 0, RMID, RLO);
                     else if (k < n1) gs(ia + 2 * (k - n0), ny - 1, RMID, RHI);
@@ -514,15 +515,25 @@ __global__ void __launch_bounds__((Win<T, TX, K>::kThreads), (Win<T, TX, K>::kMi
                 }
                 __syncthreads();
             }
-            if (threadIdx.x == 0) {
-                for (int c = 0; c < 4; ++c) {
-                    const int i = (c & 1) ? nx - 1 : 0, j = (c & 2) ? ny - 1 : 0;
-                    if (i < X0 - G || i >= X1 + G || j < Y0 - G || j >= Y1 + G) continue;
-                    const int xr = region(i, nx, pr.xl, pr.xh), yr = region(j, ny, pr.yl, pr.yh);
-                    if (xr != RMID && yr != RMID) gs(i, j, xr, yr);
-                }
+            // the corners inside the tile grown by G, in turn (uniform per CTA;
+            // most edge tiles hold none and skip the phase and its barrier)
+            unsigned corners = 0;
+            for (int c = 0; c < 4; ++c) {
+                const int i = (c & 1) ? nx - 1 : 0, j = (c & 2) ? ny - 1 : 0;
+                if (i < X0 - G || i >= X1 + G || j < Y0 - G || j >= Y1 + G) continue;
+                const int xr = region(i, nx, pr.xl, pr.xh), yr = region(j, ny, pr.yl, pr.yh);
+                if (xr != RMID && yr != RMID) corners |= 1u << c;
             }
-            __syncthreads();
+            if (corners) {
+                if (threadIdx.x == 0) {
+                    for (int c = 0; c < 4; ++c) {
+                        if (!((corners >> c) & 1u)) continue;
+                        const int i = (c & 1) ? nx - 1 : 0, j = (c & 2) ? ny - 1 : 0;
+                        gs(i, j, region(i, nx, pr.xl, pr.xh), region(j, ny, pr.yl, pr.yh));
+                    }
+                }
+                __syncthreads();
+            }
         }
     }   // sweeps
 
