@@ -77,7 +77,7 @@ def parse():
     p.add_argument("--solver", default="gmres", choices=["gmres", "krylov", "vcycle"])
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                    help="mixed: FP32 grid levels inside the FP64 outer iteration (MGP_FLAG_MIXED)")
-    p.add_argument("--coarse", default="direct", choices=["direct", "large", "reference"],
+    p.add_argument("--coarse", default="large", choices=["direct", "large", "reference"],
                    help="bottom of the Krylov solvers' V-cycle: exact on the first level of at most 64 cells "
                         "(MGP_FLAG_DIRECT_COARSE), of at most 1024 (with MGP_FLAG_DIRECT_LARGE), or the reference's")
     p.add_argument("--no-plain", action="store_true", help="skip the extra plain V-cycle solve")

@@ -550,6 +550,51 @@ __device__ __forceinline__ T restrict_cc(const DFT<T>& f, int ci, int cj, int re
     return acc;
 }
 
+// Fine += constant + linear (+ second-difference) terms for one coarse cell.
+// The adds happen in the Fortran order: all constant adds (MG:304-314), then
+// the linear ones (MG:316-333), then the quadratic ones (MG:335-352).  Each
+// fine cell belongs to one coarse cell, so doing them per cell in sequence
+// gives the same bits.
+template <class TF, class TC>
+__device__ __forceinline__ void prolong_cell(const DFT<TF>& fine, const DFT<TC>& crse, int ci, int cj, int refx, int refy,
+                                             int order) {
+    using R = TC;   // arithmetic in the coarse field's type
+    const R half = R(0.5), quarter = R(0.25), two = R(2.0), eighth = R(0.125);
+    const R c = AT(crse, ci, cj);
+    const int fi = refx * ci, fj = refy * cj;
+    R f00 = R(AT(fine, fi, fj));
+    R f10 = refx == 2 ? R(AT(fine, fi + 1, fj)) : R(0.0);
+    R f01 = refy == 2 ? R(AT(fine, fi, fj + 1)) : R(0.0);
+    R f11 = (refx == 2 && refy == 2) ? R(AT(fine, fi + 1, fj + 1)) : R(0.0);
+    f00 = f00 + c; f10 = f10 + c; f01 = f01 + c; f11 = f11 + c;
+    if (order >= 1) {
+        const R mx = half * (AT(crse, ci + 1, cj) - AT(crse, ci - 1, cj));
+        const R my = half * (AT(crse, ci, cj + 1) - AT(crse, ci, cj - 1));
+        if (refx == 2 && refy == 2) {
+            f00 = f00 + quarter * (-mx - my);
+            f10 = f10 + quarter * (mx - my);
+            f01 = f01 + quarter * (-mx + my);
+            f11 = f11 + quarter * (mx + my);
+        } else if (refx == 2) {
+            f00 = f00 + quarter * (-mx);
+            f10 = f10 + quarter * (mx);
+        } else {
+            f00 = f00 + quarter * (-my);
+            f01 = f01 + quarter * (my);
+        }
+    }
+    if (order >= 2) {
+        const R mx = quarter * (AT(crse, ci + 1, cj) - two * AT(crse, ci, cj) + AT(crse, ci - 1, cj));
+        const R my = quarter * (AT(crse, ci, cj + 1) - two * AT(crse, ci, cj) + AT(crse, ci, cj - 1));
+        const R q = (refx == 2 && refy == 2) ? eighth * (mx + my) : (refx == 2 ? eighth * mx : eighth * my);
+        f00 = f00 + q; f10 = f10 + q; f01 = f01 + q; f11 = f11 + q;
+    }
+    AT(fine, fi, fj) = TF(f00);
+    if (refx == 2) AT(fine, fi + 1, fj) = TF(f10);
+    if (refy == 2) AT(fine, fi, fj + 1) = TF(f01);
+    if (refx == 2 && refy == 2) AT(fine, fi + 1, fj + 1) = TF(f11);
+}
+
 // ---------------------------------------------------------------------------
 // Deferred-correction operators, DD:45-334
 // ---------------------------------------------------------------------------

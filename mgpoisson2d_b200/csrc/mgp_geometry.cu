@@ -239,7 +239,7 @@ int mgp_map_fourier_rhs(const mgp_box* valid, int map, const double* params, int
     const int nx = valid->nx, ny = valid->ny;
     double* dbuf = nullptr;   // amplitudes, then reduction partials and outputs
     int* ibuf = nullptr;
-    const size_t nd = (size_t)nmodes + 2 * 296 + 8;
+    const size_t nd = (size_t)nmodes + 2 * kRedBlocksMax + 8;
     if (cudaMalloc(&dbuf, nd * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&ibuf, (2 * (size_t)nmodes + 1) * sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
@@ -262,7 +262,7 @@ int mgp_map_fourier_rhs(const mgp_box* valid, int map, const double* params, int
                                     ibuf + nmodes);
             count_launch();
             double* partials = dbuf + nmodes;
-            double* out = partials + 2 * 296;
+            double* out = partials + 2 * kRedBlocksMax;
             if (launch_reduce(RED_JSUM, f, jd, nx, ny, valid->dx * valid->dy, partials, out, 0) != cudaSuccess)
                 return record_error(MGP_ECUDA, "map_fourier_rhs: reduction failed");
             k_center_scale<<<grd, blk>>>(f, jd, out, nx, ny);

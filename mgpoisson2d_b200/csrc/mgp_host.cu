@@ -14,6 +14,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
@@ -61,6 +62,93 @@ constexpr long kCoarseCells = 1024;
 constexpr long kGridCoarseCells = 8192;
 
 // ---------------------------------------------------------------------------
+// Device memory of solvers comes from a stream-ordered pool per device, owned
+// by this library, that keeps up to kPoolKeepBytes of freed memory for the
+// next solver instead of handing it back to the driver.  The Fortran-signature
+// drivers build and free a whole hierarchy in every call (as MG:469-533 and
+// MG:646-668 allocate and deallocate it); cudaMalloc and cudaFree of it cost
+// milliseconds, a reuse from the pool microseconds.  Where the device has no
+// memory pools the plain calls are used.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kPoolKeepBytes = 4ull << 30;
+
+cudaMemPool_t solver_pool() {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    static bool tried[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!tried[dev]) {
+        tried[dev] = true;
+        int supported = 0;
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        unsigned long long keep = kPoolKeepBytes;
+        if (cudaDeviceGetAttribute(&supported, cudaDevAttrMemoryPoolsSupported, dev) == cudaSuccess && supported &&
+            cudaMemPoolCreate(&p, &props) == cudaSuccess &&
+            cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep) == cudaSuccess)
+            pools[dev] = p;
+        else
+            cudaGetLastError();
+    }
+    return pools[dev];
+}
+
+// Allocation ordered on stream st (usable there at once, elsewhere after st is synchronised).
+cudaError_t dmalloc(void** p, size_t bytes, cudaStream_t st) {
+    if (cudaMemPool_t pool = solver_pool()) return cudaMallocFromPoolAsync(p, bytes, pool, st);
+    return cudaMalloc(p, bytes);
+}
+template <class T>
+cudaError_t dmalloc(T** p, size_t bytes, cudaStream_t st) {
+    return dmalloc(reinterpret_cast<void**>(p), bytes, st);
+}
+// The caller has synchronised every stream that used p.
+void dfree(void* p, cudaStream_t st) {
+    if (!p) return;
+    if (solver_pool()) cudaFreeAsync(p, st);
+    else cudaFree(p);
+}
+
+// Small pinned host buffers (a solver's reduction read-back) from 4 KB slabs
+// that are never returned: page-locking costs far more than the buffer.
+constexpr size_t kPinnedSlot = 64;
+struct PinnedSlots {
+    std::mutex mu;
+    std::vector<void*> free_slots;
+    void* get() {
+        std::lock_guard<std::mutex> lock(mu);
+        if (free_slots.empty()) {
+            char* slab = nullptr;
+            if (cudaMallocHost(&slab, 4096) != cudaSuccess) {
+                cudaGetLastError();
+                return nullptr;
+            }
+            for (size_t k = 0; k < 4096 / kPinnedSlot; ++k) free_slots.push_back(slab + k * kPinnedSlot);
+        }
+        void* p = free_slots.back();
+        free_slots.pop_back();
+        return p;
+    }
+    void put(void* p) {
+        if (!p) return;
+        std::lock_guard<std::mutex> lock(mu);
+        free_slots.push_back(p);
+    }
+};
+PinnedSlots& pinned_slots() {
+    static PinnedSlots* slots = new PinnedSlots();   // never destroyed: solvers may outlive static teardown
+    return *slots;
+}
+
+// ---------------------------------------------------------------------------
 // Device memory: every field of a solver comes out of one allocation.
 // ---------------------------------------------------------------------------
 template <class T>
@@ -90,10 +178,10 @@ struct ArenaT {
     }
     int commit(cudaStream_t st) {
         if (elems == 0) return MGP_OK;
-        if (cudaMalloc(&base, elems * sizeof(T)) != cudaSuccess) {
+        if (dmalloc(&base, elems * sizeof(T), st) != cudaSuccess) {
             cudaGetLastError();
             base = nullptr;
-            return set_err(MGP_ENOMEM, "cudaMalloc of %zu bytes failed", elems * sizeof(T));
+            return set_err(MGP_ENOMEM, "device allocation of %zu bytes failed", elems * sizeof(T));
         }
         for (auto& s : specs) {
             const size_t pad = s.g ? 32 : 0;
@@ -102,8 +190,8 @@ struct ArenaT {
         CK(cudaMemsetAsync(base, 0, elems * sizeof(T), st));   // fresh arrays start at zero
         return MGP_OK;
     }
-    void release() {
-        if (base) cudaFree(base);
+    void release() {   // after a device synchronisation (solver_free)
+        dfree(base, nullptr);
         base = nullptr;
         specs.clear();
         elems = 0;
@@ -324,22 +412,19 @@ struct mgp_solver {
 
 namespace {
 
-constexpr int kRedSlots = 2 * 296 + 8;
+constexpr int kRedSlots = 2 * kRedBlocksMax + 8;   // two partials per reduction block, then the outputs
 
 void solver_free(mgp_solver* s) {
     if (!s) return;
-    if (s->d_lv) cudaFree(s->d_lv);
-    if (s->d_shadow) cudaFree(s->d_shadow);
-    if (s->d_ainv) cudaFree(s->d_ainv);
-    if (s->gm_base) cudaFree(s->gm_base);
-    if (s->gm_red) cudaFree(s->gm_red);
-    if (s->gctl.bar) cudaFree(s->gctl.bar);
-    if (s->gctl.part) cudaFree(s->gctl.part);
-    if (s->d_ref) cudaFree(s->d_ref);
-    if (s->d_status) cudaFree(s->d_status);
-    if (s->d_bcbuf) cudaFree(s->d_bcbuf);
-    if (s->d_red) cudaFree(s->d_red);
-    if (s->h_red) cudaFreeHost(s->h_red);
+    // nothing of the solver's may still run when its memory goes back to the
+    // pool (its stream may already be gone: a server worker's, say), as
+    // cudaFree would have waited for the device
+    cudaDeviceSynchronize();
+    for (void* p : {(void*)s->d_lv, (void*)s->d_shadow, (void*)s->d_ainv, (void*)s->gm_base, (void*)s->gm_red,
+                    (void*)s->gctl.bar, (void*)s->gctl.part, (void*)s->d_ref, (void*)s->d_status,
+                    (void*)s->d_bcbuf, (void*)s->d_red})
+        dfree(p, nullptr);
+    pinned_slots().put(s->h_red);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     for (cudaEvent_t e : s->tev) cudaEventDestroy(e);
@@ -353,7 +438,7 @@ void solver_free(mgp_solver* s) {
 }
 
 double* red_partials(mgp_solver* s) { return s->d_red; }
-double* red_out(mgp_solver* s) { return s->d_red + 2 * 296; }
+double* red_out(mgp_solver* s) { return s->d_red + 2 * kRedBlocksMax; }
 
 // The mixed-precision V-cycle: MGP_FLAG_MIXED on a vcycle/fmg solver whose
 // grid path has at least one level.
@@ -410,14 +495,14 @@ int build_direct_large(mgp_solver* s, cudaStream_t st) {
     const size_t sz = (size_t)(L.nx + 2) * (L.ny + 2);
     double *scratch = nullptr, *A = nullptr;
     int* iw = nullptr;
-    // scratch: the columns' 2 n fields, later the elimination's 4 n^2 + 1 doubles
-    const size_t ns = std::max(2 * sz * n, 4 * (size_t)n * n + 1);
-    if (cudaMalloc(&scratch, sizeof(double) * ns) != cudaSuccess ||
-        cudaMalloc(&A, sizeof(double) * n * n) != cudaSuccess ||
-        cudaMalloc(&iw, sizeof(int) * (2 * n + 1)) != cudaSuccess) {
+    // scratch: the columns' 2 n fields, later the elimination's 4 n^2 + 1 + (n + 1) kGjPanel doubles
+    const size_t ns = std::max(2 * sz * n, 4 * (size_t)n * n + 1 + (size_t)(n + 1) * kGjPanel);
+    if (dmalloc(&scratch, sizeof(double) * ns, st) != cudaSuccess ||
+        dmalloc(&A, sizeof(double) * n * n, st) != cudaSuccess ||
+        dmalloc(&iw, sizeof(int) * (2 * n + 1), st) != cudaSuccess) {
         cudaGetLastError();
-        if (scratch) cudaFree(scratch);
-        if (A) cudaFree(A);
+        dfree(scratch, st);
+        dfree(A, st);
         return set_err(MGP_ENOMEM, "device allocation failed");
     }
     int fail = 1;
@@ -425,10 +510,10 @@ int build_direct_large(mgp_solver* s, cudaStream_t st) {
     if (e == cudaSuccess) e = launch_invert(A, n, A, scratch, iw, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&fail, iw + 2 * n, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    cudaFree(scratch);
-    cudaFree(iw);
+    dfree(scratch, st);
+    dfree(iw, st);
     if (e != cudaSuccess || fail) {
-        cudaFree(A);
+        dfree(A, st);
         if (e != cudaSuccess) return set_err(MGP_ECUDA, "direct coarse operator: %s", cudaGetErrorString(e));
         return MGP_OK;   // singular to working precision: keep the reference bottom
     }
@@ -461,23 +546,23 @@ int build_direct_coarse(mgp_solver* s, cudaStream_t st) {
     const int n = L.nx * L.ny;
     const size_t sz = (size_t)(L.nx + 2) * (L.ny + 2);
     double *scratch = nullptr, *A = nullptr;
-    if (cudaMalloc(&scratch, sizeof(double) * 2 * sz * n) != cudaSuccess ||
-        cudaMalloc(&A, sizeof(double) * n * n) != cudaSuccess) {
+    if (dmalloc(&scratch, sizeof(double) * 2 * sz * n, st) != cudaSuccess ||
+        dmalloc(&A, sizeof(double) * n * n, st) != cudaSuccess) {
         cudaGetLastError();
-        if (scratch) cudaFree(scratch);
+        dfree(scratch, st);
         return set_err(MGP_ENOMEM, "device allocation failed");
     }
     std::vector<double> h((size_t)n * n), inv;
     cudaError_t e = launch_direct_columns(L, scratch, A, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), A, sizeof(double) * n * n, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    cudaFree(scratch);
+    dfree(scratch, st);
     if (e != cudaSuccess) {
-        cudaFree(A);
+        dfree(A, st);
         return set_err(MGP_ECUDA, "direct coarse operator: %s", cudaGetErrorString(e));
     }
     if (!invert_dense(h, n, &inv)) {   // singular to working precision: keep the reference bottom
-        cudaFree(A);
+        dfree(A, st);
         return MGP_OK;
     }
     for (int k = 0; k < n; ++k)
@@ -485,7 +570,7 @@ int build_direct_coarse(mgp_solver* s, cudaStream_t st) {
     e = cudaMemcpyAsync(A, h.data(), sizeof(double) * n * n, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
-        cudaFree(A);
+        dfree(A, st);
         return set_err(MGP_ECUDA, "direct coarse operator: %s", cudaGetErrorString(e));
     }
     s->d_ainv = A;
@@ -617,12 +702,13 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
         for (DF* f : {&s->kr, &s->krh, &s->kp, &s->kv, &s->kt}) s->state.add(f, valid->nx, valid->ny, 0);
     RC(s->fixed.commit(st));
     RC(s->state.commit(st));
-    if (cudaMalloc(&s->d_bcbuf, sizeof(double) * 2 * (valid->nx + valid->ny + 2)) != cudaSuccess ||
-        cudaMalloc(&s->d_red, sizeof(double) * kRedSlots) != cudaSuccess ||
-        cudaMalloc(&s->d_lv, sizeof(Lv) * (md + 1)) != cudaSuccess ||
-        cudaMalloc(&s->d_ref, sizeof(int) * 2 * (md + 1)) != cudaSuccess ||
-        cudaMalloc(&s->d_status, sizeof(int)) != cudaSuccess ||
-        cudaMallocHost(&s->h_red, sizeof(double) * 8) != cudaSuccess) {
+    s->h_red = static_cast<double*>(pinned_slots().get());
+    static_assert(sizeof(double) * 8 <= kPinnedSlot, "reduction read-back slot");
+    if (dmalloc(&s->d_bcbuf, sizeof(double) * 2 * (valid->nx + valid->ny + 2), st) != cudaSuccess ||
+        dmalloc(&s->d_red, sizeof(double) * kRedSlots, st) != cudaSuccess ||
+        dmalloc(&s->d_lv, sizeof(Lv) * (md + 1), st) != cudaSuccess ||
+        dmalloc(&s->d_ref, sizeof(int) * 2 * (md + 1), st) != cudaSuccess ||
+        dmalloc(&s->d_status, sizeof(int), st) != cudaSuccess || !s->h_red) {
         cudaGetLastError();
         return set_err(MGP_ENOMEM, "device allocation failed");
     }
@@ -659,8 +745,8 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
         int m = kGmresRestart;
         while (m > 8 && (size_t)(2 * m + 1) * s->gm_vec * sizeof(double) > freeb / 4) m /= 2;
         s->gm_m = m;
-        if (cudaMalloc(&s->gm_base, (size_t)(2 * m + 1) * s->gm_vec * sizeof(double)) != cudaSuccess ||
-            cudaMalloc(&s->gm_red, sizeof(double) * ((size_t)kGmresBlocks * (m + 1) + 2 * (m + 1))) !=
+        if (dmalloc(&s->gm_base, (size_t)(2 * m + 1) * s->gm_vec * sizeof(double), st) != cudaSuccess ||
+            dmalloc(&s->gm_red, sizeof(double) * ((size_t)kGmresBlocks * (m + 1) + 2 * (m + 1)), st) !=
                 cudaSuccess) {
             cudaGetLastError();
             return set_err(MGP_ENOMEM, "device allocation failed");
@@ -674,8 +760,8 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         s->grid_ctas = (int)std::min<long>(std::min(std::max(nsm, 1), grid_max), std::max<long>(2, cells / 256));
-        if (cudaMalloc(&s->gctl.bar, 2 * sizeof(unsigned)) != cudaSuccess ||
-            cudaMalloc(&s->gctl.part, 2 * sizeof(double) * s->grid_ctas) != cudaSuccess) {
+        if (dmalloc(&s->gctl.bar, 2 * sizeof(unsigned), st) != cudaSuccess ||
+            dmalloc(&s->gctl.part, 2 * sizeof(double) * s->grid_ctas, st) != cudaSuccess) {
             cudaGetLastError();
             return set_err(MGP_ENOMEM, "device allocation failed");
         }
@@ -715,7 +801,7 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
         }
         const size_t bytes = off * sizeof(double);
         if (md - s->dc + 1 <= kMaxCoarseLevels && bytes <= (size_t)kCoarseSmemMax) {
-            if (cudaMalloc(&s->d_shadow, sizeof(Lv) * (md + 1)) != cudaSuccess) {
+            if (dmalloc(&s->d_shadow, sizeof(Lv) * (md + 1), st) != cudaSuccess) {
                 cudaGetLastError();
                 return set_err(MGP_ENOMEM, "device allocation failed");
             }
@@ -871,9 +957,14 @@ int vcycle_noinit(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
     const bool dd = (s->kind == MGP_KIND_DD);
     if (dd) CK(launch_set_guess(L.e, L.r, L.invd, L.nx, L.ny, st));   // DD:971
     RC(smooth(s, d, nd));
-    RC(residual_level(s, d));
-    CK(launch_restrict(L.w, Cl.r, Cl.nx, Cl.ny, s->refx[d], s->refy[d], 0, st));
-    if (!dd) CK(launch_set_guess(Cl.e, Cl.r, Cl.invd, Cl.nx, Cl.ny, st));   // MG:805-806
+    if (dd) {
+        RC(residual_level(s, d));
+        CK(launch_restrict(L.w, Cl.r, Cl.nx, Cl.ny, s->refx[d], s->refy[d], 0, st));
+    } else {   // residual (MG:793-795), restriction and the coarse guess (MG:805-806) in one pass
+        CK(launch_fill(L.e, L.g, L.bc, 1, 0, L.nx, L.ny, st));
+        CK(launch_resid_restrict(L.e, L.r, L.g, L.bc, 1, L.nx, L.ny, Cl.r, Cl.e, Cl.invd, Cl.nx, Cl.ny, s->refx[d],
+                                 s->refy[d], 1, st));
+    }
     for (int c = 1; c <= numcycles; ++c) RC(vcycle_noinit(s, d + 1, numcycles, nd, nu, nb));
     RC(prolong_level(s, d, 1));
     RC(smooth(s, d, nu));
@@ -923,26 +1014,29 @@ int vcycle32(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
         });
     };
     RC(smooth32(nd));
-    if (dd) {
-        CK(launch_dd_apply(L.w, L.e, L.r, L.g, F.bc, L.nx, L.ny, 1, st));
-        CK(launch_fill(L.e, L.g, F.bc, 1, 1, L.nx, L.ny, st));
-    } else {
-        CK(launch_fill(L.e, L.g, F.bc, 1, 0, L.nx, L.ny, st));
-        CK(launch_apply(L.w, L.e, L.r, L.g, F.bc, 1, L.nx, L.ny, 1, 0, st));
-    }
     const int rx = s->refx[d], ry = s->refy[d];
     const bool fine_next = d + 1 < s->dc;
     Lv& C = s->lv[d + 1];
+    if (dd) {
+        CK(launch_dd_apply(L.w, L.e, L.r, L.g, F.bc, L.nx, L.ny, 1, st));
+        CK(launch_fill(L.e, L.g, F.bc, 1, 1, L.nx, L.ny, st));
+        if (fine_next) CK(launch_restrict(L.w, s->lv32[d + 1].r, s->lv32[d + 1].nx, s->lv32[d + 1].ny, rx, ry, st));
+        else CK(launch_restrict(L.w, C.r, C.nx, C.ny, rx, ry, st));
+    } else {   // residual (MG:793-795), restriction and the coarse guess (MG:805-806) in one pass
+        CK(launch_fill(L.e, L.g, F.bc, 1, 0, L.nx, L.ny, st));
+        if (fine_next) {
+            auto& N = s->lv32[d + 1];
+            CK(launch_resid_restrict(L.e, L.r, L.g, F.bc, 1, L.nx, L.ny, N.r, N.e, N.invd, N.nx, N.ny, rx, ry, 1, st));
+        } else {
+            CK(launch_resid_restrict(L.e, L.r, L.g, F.bc, 1, L.nx, L.ny, C.r, C.e, C.invd, C.nx, C.ny, rx, ry, 1, st));
+        }
+    }
     if (fine_next) {
         auto& N = s->lv32[d + 1];
-        CK(launch_restrict(L.w, N.r, N.nx, N.ny, rx, ry, st));
-        if (!dd) CK(launch_set_guess(N.e, N.r, N.invd, N.nx, N.ny, st));   // MG:805-806
         for (int c = 1; c <= numcycles; ++c) RC(vcycle32(s, d + 1, numcycles, nd, nu, nb));
         CK(launch_fill(N.e, N.g, C.bc, 1, 1, N.nx, N.ny, st));    // MG:318
         CK(launch_prolong(L.e, N.e, N.nx, N.ny, rx, ry, 1, st));
     } else {
-        CK(launch_restrict(L.w, C.r, C.nx, C.ny, rx, ry, st));
-        if (!dd) CK(launch_set_guess(C.e, C.r, C.invd, C.nx, C.ny, st));
         for (int c = 1; c <= numcycles; ++c) RC(vcycle_noinit(s, d + 1, numcycles, nd, nu, nb));
         CK(launch_fill(C.e, C.g, C.bc, 1, 1, C.nx, C.ny, st));
         CK(launch_prolong(L.e, C.e, C.nx, C.ny, rx, ry, 1, st));
@@ -1805,8 +1899,8 @@ int mgp_relax_jacobi(const mgp_box* valid, mgp_array* phi, const mgp_array* rhs,
         return MGP_OK;
     };
     auto norm = [&](double* out) -> int {
-        CK(launch_reduce(RED_SUMSQ, r, r, nx, ny, vol, red, red + 2 * 296, c.st));
-        CK(cudaMemcpyAsync(out, red + 2 * 296, 8, cudaMemcpyDeviceToHost, c.st));
+        CK(launch_reduce(RED_SUMSQ, r, r, nx, ny, vol, red, red + 2 * kRedBlocksMax, c.st));
+        CK(cudaMemcpyAsync(out, red + 2 * kRedBlocksMax, 8, cudaMemcpyDeviceToHost, c.st));
         CK(cudaStreamSynchronize(c.st));
         return MGP_OK;
     };
@@ -1858,8 +1952,8 @@ int mgp_relax_gs(const mgp_box* valid, mgp_array* phi, const mgp_array* rhs, con
     auto resnorm = [&](double* out) -> int {
         CK(launch_fill(p, g, b, homog, 0, nx, ny, c.st));
         CK(launch_apply(r, p, f, g, b, homog, nx, ny, 1, 0, c.st));
-        CK(launch_reduce(RED_SUMSQ, r, r, nx, ny, vol, red, red + 2 * 296, c.st));
-        CK(cudaMemcpyAsync(out, red + 2 * 296, 8, cudaMemcpyDeviceToHost, c.st));
+        CK(launch_reduce(RED_SUMSQ, r, r, nx, ny, vol, red, red + 2 * kRedBlocksMax, c.st));
+        CK(cudaMemcpyAsync(out, red + 2 * kRedBlocksMax, 8, cudaMemcpyDeviceToHost, c.st));
         CK(cudaStreamSynchronize(c.st));
         return MGP_OK;
     };
@@ -1990,8 +2084,8 @@ int mgp_prolong(const mgp_box* fine_valid, mgp_array* fine, const mgp_box* crse_
     if (rax && ray) {
         const int gx = fine->ngx > 0 ? 1 : 0, gy = fine->ngy > 0 ? 1 : 0;
         CK(launch_reduce(RED_JSUM, f, fg.J, fine_valid->nx, fine_valid->ny, fine_geo->dx * fine_geo->dy, red,
-                         red + 2 * 296, c.st));
-        CK(launch_sub_mean(f, red + 2 * 296, fine_valid->nx, fine_valid->ny, gx, gy, c.st));
+                         red + 2 * kRedBlocksMax, c.st));
+        CK(launch_sub_mean(f, red + 2 * kRedBlocksMax, fine_valid->nx, fine_valid->ny, gx, gy, c.st));
     }
     RC(stage_out(f, fine, fine_valid->nx, fine_valid->ny, 1, c.st));
     RC(stage_out(cr, crse, crse_valid->nx, crse_valid->ny, 1, c.st));
@@ -2008,8 +2102,8 @@ int mgp_pnorm(const mgp_box* valid, const mgp_array* bd, int p, double* out) {
     RC(c.in(bd, valid->nx, valid->ny, 0, &a, "bd"));
     RC(c.dbuf(&red, kRedSlots));
     const int kind = p == 0 ? RED_MAXABS : p == 1 ? RED_ABSSUM : RED_SUMSQ;
-    CK(launch_reduce(kind, a, a, valid->nx, valid->ny, valid->dx * valid->dy, red, red + 2 * 296, c.st));
-    CK(cudaMemcpyAsync(out, red + 2 * 296, 8, cudaMemcpyDeviceToHost, c.st));
+    CK(launch_reduce(kind, a, a, valid->nx, valid->ny, valid->dx * valid->dy, red, red + 2 * kRedBlocksMax, c.st));
+    CK(cudaMemcpyAsync(out, red + 2 * kRedBlocksMax, 8, cudaMemcpyDeviceToHost, c.st));
     return c.finish();
 }
 
@@ -2022,8 +2116,8 @@ int mgp_inner_prod(const mgp_box* valid, const mgp_array* a, const mgp_array* b,
     RC(c.in(a, valid->nx, valid->ny, 0, &x, "a"));
     RC(c.in(b, valid->nx, valid->ny, 0, &y, "b"));
     RC(c.dbuf(&red, kRedSlots));
-    CK(launch_reduce(RED_DOT, x, y, valid->nx, valid->ny, valid->dx * valid->dy, red, red + 2 * 296, c.st));
-    CK(cudaMemcpyAsync(out, red + 2 * 296, 8, cudaMemcpyDeviceToHost, c.st));
+    CK(launch_reduce(RED_DOT, x, y, valid->nx, valid->ny, valid->dx * valid->dy, red, red + 2 * kRedBlocksMax, c.st));
+    CK(cudaMemcpyAsync(out, red + 2 * kRedBlocksMax, 8, cudaMemcpyDeviceToHost, c.st));
     return c.finish();
 }
 

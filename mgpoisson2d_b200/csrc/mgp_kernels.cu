@@ -483,6 +483,64 @@ cudaError_t launch_restrict(const DF& f, const DF& c, int ncx, int ncy, int refx
     return cudaGetLastError();
 }
 
+// The V-cycle's residual, restriction and coarse initial guess in one pass
+// (MG:793-795 then MG:805-806): a thread per fine cell computes its residual
+// rhs - L[phi] (k_apply's operations) into shared memory; the threads of
+// the block's coarse cells then sum their refx x refy fine residuals in
+// restrict_cc's order and type, write the coarse right-hand side and, with
+// guess, e = r * invdiag on the coarse level.  The fine residual never goes
+// to global memory: 6 words per fine cell instead of 9, one launch instead of
+// three, the same bits as k_apply, k_restrict_cc and k_set_guess in turn.
+// Blocks are kBlk2 (32 x 8) fine cells, so refx, refy in {1, 2} tile them.
+template <class T, class TC>
+__global__ void __launch_bounds__(kBlk2N) k_resid_restrict(DFT<T> phi, DFT<T> rhs, GeoT<T> g, BCd b, int homog, int nx,
+                                                           int ny, DFT<TC> rc, DFT<TC> ec, DFT<TC> invdc, int ncx,
+                                                           int ncy, int refx, int refy, int guess) {
+    __shared__ T w[8][33];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int i = blockIdx.x * 32 + tx, j = blockIdx.y * 8 + ty;
+    T v = T(0.0);
+    if (i < nx && j < ny) v = AT(rhs, i, j) - apply9(phi, g, b, homog, nx, ny, i, j);
+    w[ty][tx] = v;
+    __syncthreads();
+    if ((tx % refx) || (ty % refy)) return;
+    const int ci = i / refx, cj = j / refy;
+    if (ci >= ncx || cj >= ncy) return;
+    T acc = T(0.0);
+    const T sc = T(1.0 / (refx * refy));
+    for (int a = 0; a < refy; ++a)
+        for (int c = 0; c < refx; ++c) acc = acc + sc * w[ty + a][tx + c];
+    const TC r = TC(acc);
+    AT(rc, ci, cj) = r;
+    if (guess) AT(ec, ci, cj) = r * AT(invdc, ci, cj);
+}
+
+template <class T, class TC>
+cudaError_t resid_restrict_impl(const DFT<T>& phi, const DFT<T>& rhs, const GeoT<T>& g, const BCd& b, int homog,
+                                int nx, int ny, const DFT<TC>& rc, const DFT<TC>& ec, const DFT<TC>& invdc, int ncx,
+                                int ncy, int refx, int refy, int guess, cudaStream_t st) {
+    if (kBlk2.x != 32 || kBlk2.y != 8 || refx < 1 || refx > 2 || refy < 1 || refy > 2) return cudaErrorInvalidValue;
+    k_resid_restrict<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(phi, rhs, g, b, homog, nx, ny, rc, ec, invdc, ncx,
+                                                                   ncy, refx, refy, guess);
+    count_launch();
+    return cudaGetLastError();
+}
+cudaError_t launch_resid_restrict(const DF& phi, const DF& rhs, const Geo& g, const BCd& b, int homog, int nx, int ny,
+                                  const DF& rc, const DF& ec, const DF& invdc, int ncx, int ncy, int refx, int refy,
+                                  int guess, cudaStream_t st) {
+    return resid_restrict_impl(phi, rhs, g, b, homog, nx, ny, rc, ec, invdc, ncx, ncy, refx, refy, guess, st);
+}
+cudaError_t launch_resid_restrict(const DF32& phi, const DF32& rhs, const Geo32& g, const BCd& b, int homog, int nx,
+                                  int ny, const DF32& rc, const DF32& ec, const DF32& invdc, int ncx, int ncy, int refx,
+                                  int refy, int guess, cudaStream_t st) {
+    return resid_restrict_impl(phi, rhs, g, b, homog, nx, ny, rc, ec, invdc, ncx, ncy, refx, refy, guess, st);
+}
+cudaError_t launch_resid_restrict(const DF32& phi, const DF32& rhs, const Geo32& g, const BCd& b, int homog, int nx,
+                                  int ny, const DF& rc, const DF& ec, const DF& invdc, int ncx, int ncy, int refx,
+                                  int refy, int guess, cudaStream_t st) {
+    return resid_restrict_impl(phi, rhs, g, b, homog, nx, ny, rc, ec, invdc, ncx, ncy, refx, refy, guess, st);
+}
+
 // Cell-centred restriction of an FP32 field, into FP32 or (for the FP64
 // coarse levels) FP64; the sum runs in the fine field's type.
 template <class TF, class TC>
@@ -503,50 +561,6 @@ cudaError_t launch_restrict(const DF32& f, const DF& c, int ncx, int ncy, int re
     return cudaGetLastError();
 }
 
-// Fine += constant + linear (+ second-difference) terms for one coarse cell.
-// The adds happen in the Fortran order: all constant adds (MG:304-314), then
-// the linear ones (MG:316-333), then the quadratic ones (MG:335-352).  Each
-// fine cell belongs to one coarse cell, so doing them per cell in sequence
-// gives the same bits.
-template <class TF, class TC>
-__device__ __forceinline__ void prolong_cell(const DFT<TF>& fine, const DFT<TC>& crse, int ci, int cj, int refx, int refy,
-                                             int order) {
-    using R = TC;   // arithmetic in the coarse field's type
-    const R half = R(0.5), quarter = R(0.25), two = R(2.0), eighth = R(0.125);
-    const R c = AT(crse, ci, cj);
-    const int fi = refx * ci, fj = refy * cj;
-    R f00 = R(AT(fine, fi, fj));
-    R f10 = refx == 2 ? R(AT(fine, fi + 1, fj)) : R(0.0);
-    R f01 = refy == 2 ? R(AT(fine, fi, fj + 1)) : R(0.0);
-    R f11 = (refx == 2 && refy == 2) ? R(AT(fine, fi + 1, fj + 1)) : R(0.0);
-    f00 = f00 + c; f10 = f10 + c; f01 = f01 + c; f11 = f11 + c;
-    if (order >= 1) {
-        const R mx = half * (AT(crse, ci + 1, cj) - AT(crse, ci - 1, cj));
-        const R my = half * (AT(crse, ci, cj + 1) - AT(crse, ci, cj - 1));
-        if (refx == 2 && refy == 2) {
-            f00 = f00 + quarter * (-mx - my);
-            f10 = f10 + quarter * (mx - my);
-            f01 = f01 + quarter * (-mx + my);
-            f11 = f11 + quarter * (mx + my);
-        } else if (refx == 2) {
-            f00 = f00 + quarter * (-mx);
-            f10 = f10 + quarter * (mx);
-        } else {
-            f00 = f00 + quarter * (-my);
-            f01 = f01 + quarter * (my);
-        }
-    }
-    if (order >= 2) {
-        const R mx = quarter * (AT(crse, ci + 1, cj) - two * AT(crse, ci, cj) + AT(crse, ci - 1, cj));
-        const R my = quarter * (AT(crse, ci, cj + 1) - two * AT(crse, ci, cj) + AT(crse, ci, cj - 1));
-        const R q = (refx == 2 && refy == 2) ? eighth * (mx + my) : (refx == 2 ? eighth * mx : eighth * my);
-        f00 = f00 + q; f10 = f10 + q; f01 = f01 + q; f11 = f11 + q;
-    }
-    AT(fine, fi, fj) = TF(f00);
-    if (refx == 2) AT(fine, fi + 1, fj) = TF(f10);
-    if (refy == 2) AT(fine, fi, fj + 1) = TF(f01);
-    if (refx == 2 && refy == 2) AT(fine, fi + 1, fj + 1) = TF(f11);
-}
 
 // Cross term of the order-2 prolongation (MG:354-369); crse ghosts hold the
 // order-3 extrapolation.
@@ -863,7 +877,7 @@ cudaError_t launch_fillval(const DF& y, double v, int nx, int ny, int gx, int gy
 // threads and a fixed tree, so the result does not depend on scheduling.
 // ---------------------------------------------------------------------------
 constexpr int kRedThreads = 256;
-constexpr int kRedBlocks = 296;   // 2 x 148 SMs
+constexpr int kRedBlocks = kRedBlocksMax;
 
 template <class T>
 __device__ __forceinline__ double red_term(int kind, const DFT<T>& a, const DFT<T>& b, int i, int j, double& w) {
@@ -877,21 +891,39 @@ __device__ __forceinline__ double red_term(int kind, const DFT<T>& a, const DFT<
     }
 }
 
+// Block b sums cells [b * per, (b + 1) * per) of the n = nx * ny valid cells
+// in column-major order: consecutive threads on consecutive cells of a row
+// (coalesced), each thread four independent partial sums (loads in flight),
+// combined in a fixed order, then a fixed tree over the block.
 template <class T>
-__global__ void k_reduce_partial(int kind, DFT<T> a, DFT<T> b, int nx, int ny, double* partials) {
+__global__ void __launch_bounds__(kRedThreads) k_reduce_partial(int kind, DFT<T> a, DFT<T> b, int nx, int ny,
+                                                                int per, double* partials) {
     __shared__ double s0[kRedThreads], s1[kRedThreads];
-    const long n = (long)nx * ny;
-    double acc = 0.0, accw = 0.0;
-    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(k % nx), j = (int)(k / nx);
+    const int n = nx * ny, c0 = blockIdx.x * per, m = max(0, min(n, c0 + per) - c0);
+    const int step = blockDim.x;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0}, accw[4] = {0.0, 0.0, 0.0, 0.0};
+    int i = (c0 + (int)threadIdx.x) % nx, j = (c0 + (int)threadIdx.x) / nx;
+    int q = threadIdx.x;
+    for (; q + 3 * step < m; q += 4 * step) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            double w = 0.0;
+            const double t = red_term(kind, a, b, i, j, w);
+            acc[u] = (kind == RED_MAXABS) ? fmax(acc[u], t) : acc[u] + t;
+            accw[u] = accw[u] + w;
+            for (i += step; i >= nx; i -= nx) ++j;
+        }
+    }
+    for (; q < m; q += step) {
         double w = 0.0;
         const double t = red_term(kind, a, b, i, j, w);
-        if (kind == RED_MAXABS) acc = fmax(acc, t);
-        else acc = acc + t;
-        accw = accw + w;
+        acc[0] = (kind == RED_MAXABS) ? fmax(acc[0], t) : acc[0] + t;
+        accw[0] = accw[0] + w;
+        for (i += step; i >= nx; i -= nx) ++j;
     }
-    s0[threadIdx.x] = acc;
-    s1[threadIdx.x] = accw;
+    s0[threadIdx.x] = (kind == RED_MAXABS) ? fmax(fmax(acc[0], acc[1]), fmax(acc[2], acc[3]))
+                                           : (acc[0] + acc[1]) + (acc[2] + acc[3]);
+    s1[threadIdx.x] = (accw[0] + accw[1]) + (accw[2] + accw[3]);
     __syncthreads();
     for (int s = blockDim.x / 2; s > 0; s >>= 1) {
         if (threadIdx.x < s) {
@@ -933,27 +965,28 @@ __global__ void k_reduce_final(int kind, const double* partials, int nb, double 
     }
 }
 
-cudaError_t launch_reduce(int kind, const DF& a, const DF& b, int nx, int ny, double vol, double* partials,
-                          double* out, cudaStream_t st) {
+template <class T>
+cudaError_t reduce_impl(int kind, const DFT<T>& a, const DFT<T>& b, int nx, int ny, double vol, double* partials,
+                        double* out, cudaStream_t st) {
     const long n = (long)nx * ny;
-    int nb = (int)((n + kRedThreads - 1) / kRedThreads);
+    if (n >= (1L << 31)) return cudaErrorInvalidValue;
+    // at least four cells a thread, so the four partial sums all fill
+    int nb = (int)((n + 4 * kRedThreads - 1) / (4 * kRedThreads));
     if (nb > kRedBlocks) nb = kRedBlocks;
     if (nb < 1) nb = 1;
-    k_reduce_partial<<<nb, kRedThreads, 0, st>>>(kind, a, b, nx, ny, partials);
+    const int per = (int)((n + nb - 1) / nb);
+    k_reduce_partial<<<nb, kRedThreads, 0, st>>>(kind, a, b, nx, ny, per, partials);
     k_reduce_final<<<1, 512, 0, st>>>(kind, partials, nb, vol, out);
     count_launch(2);
     return cudaGetLastError();
 }
+cudaError_t launch_reduce(int kind, const DF& a, const DF& b, int nx, int ny, double vol, double* partials,
+                          double* out, cudaStream_t st) {
+    return reduce_impl(kind, a, b, nx, ny, vol, partials, out, st);
+}
 cudaError_t launch_reduce(int kind, const DF32& a, const DF32& b, int nx, int ny, double vol, double* partials,
                           double* out, cudaStream_t st) {
-    const long n = (long)nx * ny;
-    int nb = (int)((n + kRedThreads - 1) / kRedThreads);
-    if (nb > kRedBlocks) nb = kRedBlocks;
-    if (nb < 1) nb = 1;
-    k_reduce_partial<<<nb, kRedThreads, 0, st>>>(kind, a, b, nx, ny, partials);
-    k_reduce_final<<<1, 512, 0, st>>>(kind, partials, nb, vol, out);
-    count_launch(2);
-    return cudaGetLastError();
+    return reduce_impl(kind, a, b, nx, ny, vol, partials, out, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -1555,7 +1588,7 @@ __device__ __forceinline__ void rebase(DF& f, double* base) { f.p = base + (size
 // The same cycle with every coarse level held in shared memory: the levels'
 // arrays are copied in (the corrections with their ghosts, the operands, the
 // finest level's right-hand side), the cycle runs, the corrections go back.
-__global__ void __launch_bounds__(kCoarseThreads, 1) k_coarse_cycle_smem(CoarseArgs a) {
+__device__ __forceinline__ void coarse_cycle_smem(const CoarseArgs& a) {
     extern __shared__ double smem[];
     __shared__ double sh[kCoarseThreads];
     __shared__ Lv sl[kMaxCoarseLevels];
@@ -1593,6 +1626,41 @@ __global__ void __launch_bounds__(kCoarseThreads, 1) k_coarse_cycle_smem(CoarseA
     if (threadIdx.x == 0) set_status(a.status, s);
 }
 
+__global__ void __launch_bounds__(kCoarseThreads, 1) k_coarse_cycle_smem(CoarseArgs a) { coarse_cycle_smem(a); }
+
+// The coarse cycles of a lockstep batch: a CTA per problem, each with its own
+// arguments (staged in shared memory when its levels fit, else in place).
+__global__ void __launch_bounds__(kCoarseThreads, 1) k_coarse_jobs(const CoarseJob* __restrict__ jobs) {
+    const CoarseArgs& a = jobs[blockIdx.x].a;
+    if (a.shadow && a.smem_bytes > 0) {
+        coarse_cycle_smem(a);
+    } else {
+        __shared__ double sh[kCoarseThreads];
+        const int s = coarse_body<BlockScope>(a.lv, a, sh);
+        if (threadIdx.x == 0) set_status(a.status, s);
+    }
+}
+
+cudaError_t launch_coarse_jobs(const CoarseJob* jobs, int njobs, int smem_bytes, cudaStream_t st) {
+    if (njobs < 1) return cudaSuccess;
+    static std::mutex mu;
+    static unsigned long long done = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (dev >= 64 || !((done >> dev) & 1ull)) {
+            e = cudaFuncSetAttribute(k_coarse_jobs, cudaFuncAttributeMaxDynamicSharedMemorySize, kCoarseSmemMax);
+            if (e != cudaSuccess) return e;
+            if (dev < 64) done |= 1ull << dev;
+        }
+    }
+    k_coarse_jobs<<<njobs, kCoarseThreads, smem_bytes, st>>>(jobs);
+    count_launch();
+    return cudaGetLastError();
+}
+
 __global__ void __launch_bounds__(kCoarseThreads) k_direct_columns(Lv L, double* scratch, double* A) {
     const int nx = L.nx, ny = L.ny, n = nx * ny, k = blockIdx.x;
     const int ld = nx + 2;
@@ -1614,13 +1682,12 @@ cudaError_t launch_direct_columns(const Lv& L, double* scratch, double* A, cudaS
 // ---------------------------------------------------------------------------
 // Gauss-Jordan inversion on the device (the exact bottom of
 // MGP_FLAG_DIRECT_LARGE).  X = [A | I], n x 2n row-major, is reduced one
-// pivot per launch, each launch reading one buffer and writing the other.
-// Step c's pivot is the unused row with the largest |X[r][c]| (the lowest
-// such row on ties), found by every CTA alike; rows are never swapped:
-// mark[r] records the step that took row r, prow[c] the pivot row of step c,
-// and at the end row prow[c] of the right half is row c of A^-1.  Each
-// update is X[r][k] - X[r][c] * (X[p][k] * (1 / X[p][c])), the pivot row
-// scaled first, as in the textbook elimination.
+// pivot at a time.  Step c's pivot is the unused row with the largest
+// |X[r][c]| (the lowest such row on ties); rows are never swapped: mark[r]
+// records the step that took row r, prow[c] the pivot row of step c, and at
+// the end row prow[c] of the right half is row c of A^-1.  Each update is
+// X[r][k] - X[r][c] * (X[p][k] * (1 / X[p][c])), the pivot row scaled first,
+// as in the textbook elimination; columns up to c are not read again.
 // ---------------------------------------------------------------------------
 constexpr int kGjThreads = 256;
 constexpr int kGjRows = 32;   // rows of X per CTA and step
@@ -1652,72 +1719,6 @@ __global__ void __launch_bounds__(kGjThreads) k_gj_init(const double* A, int n, 
     }
 }
 
-// One elimination step c: grid (2n / kGjThreads columns, n / kGjRows rows).
-__global__ void __launch_bounds__(kGjThreads) k_gj_step(const double* __restrict__ X, double* __restrict__ Y, int n,
-                                                        int c, int* mark, int* prow, const double* amax, int* fail) {
-    if (*fail) return;
-    __shared__ double sv[kGjThreads];
-    __shared__ int sr[kGjThreads];
-    __shared__ double sf[kGjRows];
-    // this CTA's rows' entries in column c, loaded while the pivot is searched
-    const int r0 = blockIdx.y * kGjRows, r1 = min(n, r0 + kGjRows);
-    if (threadIdx.x < r1 - r0) sf[threadIdx.x] = X[(long)(r0 + threadIdx.x) * 2 * n + c];
-    // pivot search over the rows no earlier step took (mark[r] >= c: step c's
-    // own mark, set below by CTA (0,0), leaves the predicate unchanged); the
-    // mark and the entry are loaded independently
-    double best = -1.0;
-    int br = n;
-    for (int r = threadIdx.x; r < n; r += blockDim.x) {
-        const int mk = mark[r];
-        const double v = fabs(X[(long)r * 2 * n + c]);
-        if (mk >= c && v > best) { best = v; br = r; }   // rows ascend per thread: the first maximum stays
-    }
-    sv[threadIdx.x] = best;
-    sr[threadIdx.x] = br;
-    __syncthreads();
-    for (int h = kGjThreads / 2; h > 0; h >>= 1) {
-        if (threadIdx.x < h) {
-            const double o = sv[threadIdx.x + h];
-            const int orr = sr[threadIdx.x + h];
-            if (o > sv[threadIdx.x] || (o == sv[threadIdx.x] && orr < sr[threadIdx.x])) {
-                sv[threadIdx.x] = o;
-                sr[threadIdx.x] = orr;
-            }
-        }
-        __syncthreads();
-    }
-    const int p = sr[0];
-    if (p >= n) {   // no unused row (cannot happen for c < n)
-        if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *fail = 1;
-        return;
-    }
-    const double piv = X[(long)p * 2 * n + c];
-    if (!(fabs(piv) > 1e-13 * *amax)) {
-        if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *fail = 1;
-        return;
-    }
-    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
-        mark[p] = c;
-        prow[c] = p;
-    }
-    const double ip = 1.0 / piv;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= 2 * n || (k <= c)) return;   // the left half's columns up to c are never read again
-    const double sk = X[(long)p * 2 * n + k] * ip;
-    if (r1 - r0 == kGjRows) {   // all rows' loads issued before the stores
-        double x[kGjRows];
-#pragma unroll
-        for (int t = 0; t < kGjRows; ++t) x[t] = X[(long)(r0 + t) * 2 * n + k];
-#pragma unroll
-        for (int t = 0; t < kGjRows; ++t) Y[(long)(r0 + t) * 2 * n + k] = (r0 + t == p) ? sk : x[t] - sf[t] * sk;
-    } else {
-        for (int r = r0; r < r1; ++r) {
-            const long q = (long)r * 2 * n + k;
-            Y[q] = (r == p) ? sk : X[q] - sf[r - r0] * sk;
-        }
-    }
-}
-
 // ainv[c][m] = X[prow[c]][n + m] (nothing after a failed step: prow is then incomplete).
 __global__ void k_gj_extract(const double* X, const int* prow, const int* fail, int n, double* ainv) {
     if (*fail) return;
@@ -1728,17 +1729,159 @@ __global__ void k_gj_extract(const double* X, const int* prow, const int* fail, 
     }
 }
 
+// The elimination runs blocked: kGjPanel pivots per pair of launches, each
+// launch reading one buffer and writing the other, with every operation of
+// the one-pivot steps above in its order (so the same bits as a launch per
+// pivot).  k_gj_panel (one CTA, a
+// thread per row) runs the steps on the panel's columns only: the pivot
+// search, the pivot row scaled by 1 / pivot, the other rows' entries updated
+// x - f * s; it records f[r][j] (row r's entry in the step's pivot column:
+// the multiplier of step j) and 1 / pivot.  k_gj_trailing then replays the
+// steps on the columns right of the panel: per column the pivot rows' new
+// values s_j (the recurrence the steps apply to the pivot rows), then per row
+// x = (r == p_j) ? s_j : x - f[r][j] * s_j for j in order.
+constexpr int kGjPanelThreads = 1024;   // the largest bottom: a thread per row
+static_assert(kGjPanelThreads >= kDirectLargeCells, "a panel thread per row of the largest bottom");
+
+__global__ void __launch_bounds__(kGjPanelThreads) k_gj_panel(const double* __restrict__ X, int n, int c0, int b,
+                                                              int* mark, int* prow, const double* amax, int* fail,
+                                                              double* f, double* ipiv) {
+    __shared__ double sv[kGjPanelThreads / 32];
+    __shared__ int sr[kGjPanelThreads / 32];
+    __shared__ double prowv[kGjPanel];
+    __shared__ int sp;
+    if (*fail) return;
+    const int r = threadIdx.x;
+    const bool live = r < n;
+    double x[kGjPanel];
+#pragma unroll
+    for (int j = 0; j < kGjPanel; ++j) x[j] = (live && j < b) ? X[(long)r * 2 * n + c0 + j] : 0.0;
+    int mk = live ? mark[r] : -1;
+    const int lane = r & 31, wid = r >> 5;
+#pragma unroll
+    for (int j = 0; j < kGjPanel; ++j) {
+        if (j >= b) break;
+        const int c = c0 + j;
+        // pivot: the unused row with the largest |x[j]|, the lowest on ties
+        double best = (live && mk >= c) ? fabs(x[j]) : -1.0;
+        int br = (live && mk >= c) ? r : n;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_down_sync(0xffffffffu, best, o);
+            const int orr = __shfl_down_sync(0xffffffffu, br, o);
+            if (ob > best || (ob == best && orr < br)) { best = ob; br = orr; }
+        }
+        if (lane == 0) { sv[wid] = best; sr[wid] = br; }
+        __syncthreads();
+        if (wid == 0) {
+            best = lane < kGjPanelThreads / 32 ? sv[lane] : -1.0;
+            br = lane < kGjPanelThreads / 32 ? sr[lane] : n;
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_down_sync(0xffffffffu, best, o);
+                const int orr = __shfl_down_sync(0xffffffffu, br, o);
+                if (ob > best || (ob == best && orr < br)) { best = ob; br = orr; }
+            }
+            if (lane == 0) sp = br;
+        }
+        __syncthreads();
+        const int p = sp;
+        if (p >= n) {
+            if (r == 0) *fail = 1;
+            return;
+        }
+        if (r == p) {
+#pragma unroll
+            for (int q = 0; q < kGjPanel; ++q) prowv[q] = x[q];
+        }
+        __syncthreads();
+        const double piv = prowv[j];
+        if (!(fabs(piv) > 1e-13 * *amax)) {
+            if (r == 0) *fail = 1;
+            return;
+        }
+        const double ip = 1.0 / piv;
+        if (r == p) {
+            mk = c;
+            mark[p] = c;
+            prow[c] = p;
+        }
+        if (r == 0) ipiv[j] = ip;
+        if (live) f[(long)r * kGjPanel + j] = x[j];
+        const double fj = x[j];
+#pragma unroll
+        for (int q = 0; q < kGjPanel; ++q) {
+            if (q <= j || q >= b) continue;
+            const double sk = prowv[q] * ip;
+            x[q] = (r == p) ? sk : x[q] - fj * sk;
+        }
+        __syncthreads();   // prowv is rewritten by the next step's pivot row
+    }
+}
+
+// Columns [c0 + b, 2n) of rows [r0, r0 + kGjRows): grid (columns / kGjThreads, rows / kGjRows).
+__global__ void __launch_bounds__(kGjThreads) k_gj_trailing(const double* __restrict__ X, double* __restrict__ Y,
+                                                            int n, int c0, int b, const int* prow, const double* f,
+                                                            const double* ipiv, const int* fail) {
+    __shared__ double fp[kGjPanel][kGjPanel];   // f[p_j][i]
+    __shared__ double fr[kGjRows][kGjPanel];    // f[r][j] of this CTA's rows
+    __shared__ int pr[kGjPanel];
+    __shared__ double ip[kGjPanel];
+    if (*fail) return;
+    const int r0 = blockIdx.y * kGjRows, r1 = min(n, r0 + kGjRows);
+    for (int q = threadIdx.x; q < b; q += blockDim.x) {
+        pr[q] = prow[c0 + q];
+        ip[q] = ipiv[q];
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < b * b; q += blockDim.x) fp[q / b][q % b] = f[(long)pr[q / b] * kGjPanel + q % b];
+    for (int q = threadIdx.x; q < (r1 - r0) * b; q += blockDim.x) fr[q / b][q % b] = f[(long)(r0 + q / b) * kGjPanel + q % b];
+    __syncthreads();
+    const int k = c0 + b + blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 2 * n) return;
+    double sj[kGjPanel];
+#pragma unroll
+    for (int j = 0; j < kGjPanel; ++j) {
+        if (j >= b) break;
+        double x = X[(long)pr[j] * 2 * n + k];
+#pragma unroll
+        for (int i = 0; i < kGjPanel; ++i)
+            if (i < j) x = x - fp[j][i] * sj[i];
+        sj[j] = x * ip[j];
+    }
+    for (int r = r0; r < r1; ++r) {
+        double x = X[(long)r * 2 * n + k];
+#pragma unroll
+        for (int j = 0; j < kGjPanel; ++j) {
+            if (j >= b) break;
+            x = (r == pr[j]) ? sj[j] : x - fr[r - r0][j] * sj[j];
+        }
+        Y[(long)r * 2 * n + k] = x;
+    }
+}
+
 cudaError_t launch_invert(const double* A, int n, double* ainv, double* work, int* iwork, cudaStream_t st) {
     double *X0 = work, *X1 = work + 2L * n * n, *amax = work + 4L * n * n;
+    double *f = amax + 1, *ipiv = f + (long)n * kGjPanel;
     int *mark = iwork, *prow = iwork + n, *fail = iwork + 2 * n;
+    if (n > kGjPanelThreads) return cudaErrorNotSupported;
     const int nb = std::min(1184, (int)((2L * n * n + kGjThreads - 1) / kGjThreads));
     k_gj_init<<<nb, kGjThreads, 0, st>>>(A, n, X0, mark, fail, amax);
-    const dim3 grid((2 * n + kGjThreads - 1) / kGjThreads, (n + kGjRows - 1) / kGjRows);
-    for (int c = 0; c < n; ++c) {
-        k_gj_step<<<grid, kGjThreads, 0, st>>>((c & 1) ? X1 : X0, (c & 1) ? X0 : X1, n, c, mark, prow, amax, fail);
+    int launches = 2, cur = 0;
+    for (int c0 = 0; c0 < n; c0 += kGjPanel) {
+        const int b = std::min(kGjPanel, n - c0);
+        double* Xc = cur ? X1 : X0;
+        double* Xn = cur ? X0 : X1;
+        k_gj_panel<<<1, kGjPanelThreads, 0, st>>>(Xc, n, c0, b, mark, prow, amax, fail, f, ipiv);
+        const int ncols = 2 * n - (c0 + b);
+        if (ncols > 0) {
+            const dim3 grid((ncols + kGjThreads - 1) / kGjThreads, (n + kGjRows - 1) / kGjRows);
+            k_gj_trailing<<<grid, kGjThreads, 0, st>>>(Xc, Xn, n, c0, b, prow, f, ipiv, fail);
+            cur ^= 1;
+            ++launches;
+        }
+        ++launches;
     }
-    k_gj_extract<<<nb, kGjThreads, 0, st>>>((n & 1) ? X1 : X0, prow, fail, n, ainv);
-    count_launch(n + 2);
+    k_gj_extract<<<nb, kGjThreads, 0, st>>>(cur ? X1 : X0, prow, fail, n, ainv);
+    count_launch(launches);
     return cudaGetLastError();
 }
 

@@ -7,6 +7,10 @@
 
 namespace mgp {
 
+// Most blocks a reduction uses (4 per SM of a B200): launch_reduce's partials
+// take two doubles per block.
+constexpr int kRedBlocksMax = 592;
+
 // Reduction kinds of launch_reduce.
 enum RedKind { RED_SUMSQ = 0, RED_MAXABS = 1, RED_DOT = 2, RED_JSUM = 3, RED_ABSSUM = 4 };
 
@@ -62,6 +66,9 @@ constexpr int kDirectCells = 64;
 // Largest bottom of MGP_FLAG_DIRECT_LARGE (cells): the coarse-cycle level,
 // solved by launch_direct_apply.
 constexpr int kDirectLargeCells = 1024;
+// Pivots per panel of the blocked device Gauss-Jordan (launch_invert); its
+// scratch is 4 n^2 + 1 + (n + 1) kGjPanel doubles.
+constexpr int kGjPanel = 16;
 
 constexpr int kMaxCoarseLevels = 16;
 // Largest staged coarse hierarchy (bytes of dynamic shared memory).
@@ -101,6 +108,18 @@ cudaError_t launch_prolong(const DF32& fine, const DF32& crse, int ncx, int ncy,
 cudaError_t launch_prolong(const DF32& fine, const DF& crse, int ncx, int ncy, int refx, int refy, int order,
                            cudaStream_t st);
 cudaError_t launch_set_guess(const DF32& e, const DF32& r, const DF32& invd, int nx, int ny, cudaStream_t st);
+// rc = restrict(rhs - L[phi]) onto the coarse cells, and with guess
+// ec = rc * invdc: k_apply (mode 1), the cell restriction and k_set_guess in
+// one pass, the same bits.  phi's ghosts must be filled.
+cudaError_t launch_resid_restrict(const DF& phi, const DF& rhs, const Geo& g, const BCd& b, int homog, int nx, int ny,
+                                  const DF& rc, const DF& ec, const DF& invdc, int ncx, int ncy, int refx, int refy,
+                                  int guess, cudaStream_t st);
+cudaError_t launch_resid_restrict(const DF32& phi, const DF32& rhs, const Geo32& g, const BCd& b, int homog, int nx,
+                                  int ny, const DF32& rc, const DF32& ec, const DF32& invdc, int ncx, int ncy, int refx,
+                                  int refy, int guess, cudaStream_t st);
+cudaError_t launch_resid_restrict(const DF32& phi, const DF32& rhs, const Geo32& g, const BCd& b, int homog, int nx,
+                                  int ny, const DF& rc, const DF& ec, const DF& invdc, int ncx, int ncy, int refx,
+                                  int refy, int guess, cudaStream_t st);
 cudaError_t launch_sub_mean(const DF32& y, const double* out, int nx, int ny, int gx, int gy, cudaStream_t st);
 cudaError_t launch_reduce(int kind, const DF32& a, const DF32& b, int nx, int ny, double vol, double* partials,
                           double* out, cudaStream_t st);
@@ -121,6 +140,67 @@ struct SweepMaps {
     CUtensorMap pin, rhs, invd, xx, xy, yx, yy;
     int pcb, prb;
 };
+// ---- lockstep batches -------------------------------------------------- //
+// One launch runs the same phase of many problems.  Each launch has a job
+// table and pre[0..njobs]: job k owns blocks [pre[k], pre[k + 1]) of a 1-D
+// grid of pre[njobs] blocks (a block finds its job by binary search).
+// One level's sweep: phi in buf[s0 ^ flip] (descriptors m[s0 ^ flip]),
+// written to the other buffer.
+template <class T>
+struct alignas(64) SweepJobT {
+    SweepMaps m[2];
+    DFT<T> buf[2], rhs, invd;
+    GeoT<T> g;
+    BCd b;
+    int4 part;   // (nx / gx, nx % gx, ny / gy, ny % gy)
+    int nx, ny, gx, gy, s0;
+};
+// fill_ghosts of one field.
+template <class T>
+struct FillJob {
+    DFT<T> p;
+    GeoT<T> g;
+    BCd b;
+    int nx, ny, homog, do_neum;
+};
+// rc = restrict(rhs - L[phi]), ec = rc * invdc (k_resid_restrict); gbx blocks of 32 x 8 fine cells along x.
+template <class T, class TC>
+struct ResidJob {
+    DFT<T> phi, rhs;
+    GeoT<T> g;
+    BCd b;
+    DFT<TC> rc, ec, invdc;
+    int nx, ny, ncx, ncy, refx, refy, gbx;
+};
+// fine += prolong(crse), order 1 (k_prolong); gbx blocks of 32 x 8 coarse cells along x.
+template <class TF, class TC>
+struct ProlongJob {
+    DFT<TF> fine;
+    DFT<TC> crse;
+    int ncx, ncy, refx, refy, gbx;
+};
+// Cell-wise work on the valid region plus g ghost layers (k_cell_jobs: y + x,
+// x converted to y's type, y - x, x * z).  gbx blocks of 32 x 8 along x.
+template <class TD, class TS>
+struct CellJob {
+    DFT<TD> y;
+    DFT<TS> x;
+    DFT<TD> z;
+    int nx, ny, g, gbx;
+};
+// r = rhs - L[phi] on level 0 (caller BCs) and the block's sum of r^2 into
+// partials[block]; gbx blocks of 32 x 8 along x.
+struct NormJob {
+    DF phi, rhs, r;
+    Geo g;
+    BCd b;
+    int nx, ny, homog, gbx;
+};
+// The coarse cycle of one problem (one CTA each; CoarseArgs with its shadow layout).
+struct CoarseJob {
+    CoarseArgs a;
+};
+
 // Descriptors for sweeping one level with phi in either of its two buffers.
 struct SweepTma {
     SweepMaps ma, mb;
@@ -156,6 +236,26 @@ cudaError_t launch_sweep9_pair(const DF32& pin, const DF32& pout, const DF32& rh
 cudaError_t launch_sweep9_pair(const DF& pin, const DF& pout, const DF& rhs, const DF& invd, const Geo& g,
                                const BCd& b, int homog, int nx, int ny, double omega, const SweepTma* tma,
                                int* status, cudaStream_t st);
+// Lockstep launches: jobs and pre in device memory (pre[njobs] blocks in all).
+template <class T>
+cudaError_t launch_sweep9_jobs(const SweepJobT<T>* jobs, const int* pre, int njobs, int nblocks, int tx, int k,
+                               int flip, int* status, cudaStream_t st);
+template <class T>
+cudaError_t launch_fill_jobs(const FillJob<T>* jobs, const int* pre, int njobs, int nblocks, int phases,
+                             cudaStream_t st);
+template <class T, class TC>
+cudaError_t launch_resid_jobs(const ResidJob<T, TC>* jobs, const int* pre, int njobs, int nblocks, cudaStream_t st);
+template <class TF, class TC>
+cudaError_t launch_prolong_jobs(const ProlongJob<TF, TC>* jobs, const int* pre, int njobs, int nblocks,
+                                cudaStream_t st);
+// kind 0: y = y + x; 1: y = x converted; 2: y = y - x; 3: y = x * z
+template <class TD, class TS>
+cudaError_t launch_cell_jobs(const CellJob<TD, TS>* jobs, const int* pre, int njobs, int nblocks, int kind,
+                             cudaStream_t st);
+// r = rhs - L[phi], then norms[k] = sqrt(vol_k * sum of job k's r^2) in block order (vol in volk).
+cudaError_t launch_norm_jobs(const NormJob* jobs, const int* pre, int njobs, int nblocks, double* partials,
+                             const double* volk, double* norms, cudaStream_t st);
+cudaError_t launch_coarse_jobs(const CoarseJob* jobs, int njobs, int smem_bytes, cudaStream_t st);
 cudaError_t launch_invdiag(const DF& invd, const Geo& g, const BCd& b, int homog, int nx, int ny, int coupled,
                            cudaStream_t st);
 // kind: 0 cell, 1 x-face, 2 y-face, 3 node.  ncx/ncy = coarse cell counts.
