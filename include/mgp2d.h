@@ -175,6 +175,20 @@ typedef struct mgp_report {
  * than 1024 cells, or lies below a level of at most 64, MGP_FLAG_DIRECT_COARSE
  * alone applies.  No reference counterpart. */
 #define MGP_FLAG_DIRECT_LARGE 64
+/* mgp_batch only: solve the batch in lockstep.  Every phase of the V-cycle --
+ * a level's smoothing sweeps, its ghost fill, the residual restricted to the
+ * next level, the coarse cycles, the prolongations, the update and the
+ * residual norms -- runs as one launch over the job table of every problem
+ * not yet converged (one job per problem: the tiles or cell blocks of its
+ * level), with one host synchronisation per V-cycle for all the norms.  The
+ * solver is the stationary V-cycle (MGPoisson2D.f90:565-645, FP64 or with
+ * MGP_FLAG_MIXED), each problem stopping on its own test; each solution has
+ * the bits of solving that problem alone.  Applies when every problem is MG
+ * kind without MGP_FLAG_KRYLOV or MGP_FLAG_GMRES, numcycles is 1, the
+ * smoothing counts are even, every problem has a Dirichlet side and no
+ * periodic one, and its bottom fits one CTA; otherwise the batch runs its
+ * problems concurrently as without the flag.  No reference counterpart. */
+#define MGP_FLAG_LOCKSTEP 128
 
 /* Solver kinds for the resident-hierarchy handle. */
 #define MGP_KIND_MG 0   /* module MGPoisson2D (vcycle, fmg)                  */

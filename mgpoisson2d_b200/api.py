@@ -28,6 +28,7 @@ FLAG_MIXED = 8
 FLAG_DIRECT_COARSE = 16
 FLAG_GMRES = 32
 FLAG_DIRECT_LARGE = 64
+FLAG_LOCKSTEP = 128
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libmgp2d.so")

@@ -15,7 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 LIB = os.path.join(HERE, "libmgp2d.so")
-SOURCES = ["mgp_kernels.cu", "mgp_sweep.cu", "mgp_host.cu", "mgp_noalloc.cu", "mgp_batch.cu", "mgp_geometry.cu"]
+SOURCES = ["mgp_kernels.cu", "mgp_sweep.cu", "mgp_host.cu", "mgp_noalloc.cu", "mgp_batch.cu", "mgp_geometry.cu",
+           "mgp_lockstep.cu"]
 HEADERS = ["mgp_core.cuh", "mgp_kernels.cuh"]
 
 NVCC_FLAGS = [

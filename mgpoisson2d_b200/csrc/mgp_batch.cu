@@ -32,6 +32,13 @@ int record_error(int code, const char* msg);
 int solver_create_on(const mgp_box* valid, const mgp_geo* geo, const mgp_bdry* bc, int kind, int flags,
                      int maxdepth_user, cudaStream_t st, mgp_solver** out);
 size_t solver_device_bytes(const mgp_solver* s);
+struct Lockstep;
+Lockstep* lockstep_new();
+void lockstep_free(Lockstep* ls);
+bool lockstep_ok(const std::vector<mgp_solver*>& ss, int numcycles, int nd, int nu);
+int lockstep_vcycle(const std::vector<mgp_solver*>& ss, Lockstep* ls, mgp_array* phi, mgp_array* rhs,
+                    const mgp_bdry* bc, int homog, double tol, int maxiters, int nd, int nu, int nb, int zerophi,
+                    mgp_report* reports, cudaStream_t st);
 }  // namespace mgp
 
 using namespace mgp;
@@ -60,8 +67,10 @@ size_t estimate_bytes(const mgp_box* v, int flags) {
 struct mgp_batch {
     int dev = 0;
     int nstreams = 1;
+    int flags = 0;
     std::vector<mgp_solver*> solvers;
     std::vector<cudaStream_t> streams;
+    Lockstep* lockstep = nullptr;   // MGP_FLAG_LOCKSTEP: the phase-by-phase engine's buffers
 };
 
 extern "C" {
@@ -77,6 +86,7 @@ int mgp_batch_create(int nprob, const mgp_box* valid, const mgp_geo* geo, const 
         return record_error(MGP_ECUDA, "batch_create: no CUDA device");
     }
     b->nstreams = std::max(1, std::min(nstreams, nprob));
+    b->flags = flags;
     for (int k = 0; k < b->nstreams; ++k) {
         cudaStream_t st;
         if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
@@ -101,6 +111,7 @@ int mgp_batch_create(int nprob, const mgp_box* valid, const mgp_geo* geo, const 
 
 int mgp_batch_destroy(mgp_batch* b) {
     if (!b) return MGP_OK;
+    if (b->lockstep) lockstep_free(b->lockstep);
     for (mgp_solver* s : b->solvers) mgp_solver_destroy(s);
     for (cudaStream_t st : b->streams) cudaStreamDestroy(st);
     delete b;
@@ -118,6 +129,12 @@ int mgp_batch_vcycle(mgp_batch* b, mgp_array* phi, mgp_array* rhs, const mgp_bdr
                      mgp_report* reports) {
     if (!b || !phi || !rhs || !bc) return record_error(MGP_EINVAL, "batch_vcycle: null argument");
     const int n = (int)b->solvers.size();
+    if ((b->flags & MGP_FLAG_LOCKSTEP) && lockstep_ok(b->solvers, numcycles, smooth_down, smooth_up)) {
+        cudaSetDevice(b->dev);
+        if (!b->lockstep) b->lockstep = lockstep_new();
+        return lockstep_vcycle(b->solvers, b->lockstep, phi, rhs, bc, homog, tol, maxiters, smooth_down, smooth_up,
+                               smooth_bottom, zerophi, reports, b->streams[0]);
+    }
     std::atomic<int> next{0};
     std::vector<int> status(n, MGP_OK);
     std::vector<std::string> msg(n);

@@ -1627,6 +1627,520 @@ size_t solver_device_bytes(const mgp_solver* s) {
     return (s->fixed.elems + s->state.elems) * sizeof(double) +
            (s->fixed32.elems + s->state32.elems) * sizeof(float) + (size_t)s->shadow_bytes;
 }
+
+// ===========================================================================
+// Lockstep batches (mgp_batch_* with MGP_FLAG_LOCKSTEP): the stationary
+// V-cycle of MG:565-645 for many resident hierarchies at once.  Every phase of
+// the cycle -- a level's smoothing sweeps, its ghost fill, the fused
+// residual-restriction, the coarse cycles, the fills and prolongations on the
+// way up, the update, the residual norm -- is one launch over the phase's job
+// table, one job per unconverged problem (tiles or cell blocks of its level),
+// instead of a launch per problem.  Each job does what the single-problem
+// kernel does for its cells, so each problem's solution has the bits of its
+// own stationary V-cycle; only the residual norms are summed in another (fixed)
+// order.  One host synchronisation per V-cycle reads every problem's norm,
+// and the job tables are rebuilt when a problem leaves.
+// ===========================================================================
+struct Lockstep {
+    char* dev = nullptr;   // job tables and their block prefixes
+    size_t cap = 0;
+    double* part = nullptr;   // norm partials, one per cell block
+    size_t part_cap = 0;
+    double* norms = nullptr;  // per job
+    double* vols = nullptr;
+    double* h_norms = nullptr;   // pinned
+    int ncap = 0;
+    int* status = nullptr;    // the sweeps' status word
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+
+namespace {
+
+struct Packer {
+    std::vector<char> host;
+    size_t add(const void* p, size_t bytes) {
+        const size_t off = (host.size() + 255) / 256 * 256;
+        host.resize(off + bytes);
+        if (bytes) std::memcpy(host.data() + off, p, bytes);
+        return off;
+    }
+};
+
+// One launch's jobs: the host copy until upload, then device pointers.
+template <class J>
+struct Table {
+    std::vector<J> jobs;
+    std::vector<int> pre{0};
+    size_t oj = 0, op = 0;
+    const J* dj = nullptr;
+    const int* dp = nullptr;
+    void push(const J& j, int blocks) {
+        jobs.push_back(j);
+        pre.push_back(pre.back() + blocks);
+    }
+    int n() const { return (int)jobs.size(); }
+    int blocks() const { return pre.back(); }
+    void pack(Packer& pk) {
+        oj = pk.add(jobs.data(), jobs.size() * sizeof(J));
+        op = pk.add(pre.data(), pre.size() * sizeof(int));
+    }
+    void bind(char* base) {
+        dj = reinterpret_cast<const J*>(base + oj);
+        dp = reinterpret_cast<const int*>(base + op);
+    }
+};
+
+int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
+
+bool fill_one_phase(const BCd& b, int do_neum) {   // no side's fill reads another side's ghosts
+    for (int k = 0; k < 4; ++k) {
+        const int t = b.type[k];
+        if (t == T_DIRI || t == T_NONE || (t == T_NEUM && !do_neum)) continue;
+        return false;
+    }
+    return true;
+}
+
+template <class T>
+struct SweepGroups {   // a level's sweep jobs by tile width
+    Table<SweepJobT<T>> w32, w64;
+};
+
+template <class T>
+void add_sweep_job(SweepGroups<T>& sg, const SweepTma& t, const DFT<T>& e, const DFT<T>& e2, const DFT<T>& r,
+                   const DFT<T>& invd, const GeoT<T>& g, const BCd& b, int nx, int ny) {
+    SweepJobT<T> J;
+    std::memset(&J, 0, sizeof J);
+    const bool a_is_e = (const void*)e.p == t.pa;
+    J.m[0] = a_is_e ? t.ma : t.mb;
+    J.m[1] = a_is_e ? t.mb : t.ma;
+    J.buf[0] = e;
+    J.buf[1] = e2;
+    J.rhs = r;
+    J.invd = invd;
+    J.g = g;
+    J.b = b;
+    J.nx = nx;
+    J.ny = ny;
+    J.gx = cdiv(nx, t.tx);
+    J.gy = cdiv(ny, 32);
+    J.part = make_int4(nx / J.gx, nx % J.gx, ny / J.gy, ny % J.gy);
+    J.s0 = 0;
+    (t.tx == 64 ? sg.w64 : sg.w32).push(J, J.gx * J.gy);
+}
+
+// Everything one V-cycle iteration launches, for one set of active problems.
+struct Plan {
+    int D = 0;        // levels with sweeps (max grid-path depth)
+    bool mix = false;
+    std::vector<SweepGroups<double>> sw64;
+    std::vector<SweepGroups<float>> sw32;
+    std::vector<Table<FillJob<double>>> fpre64, fpost64;
+    std::vector<Table<FillJob<float>>> fpre32, fpost32;
+    std::vector<int> fpre_ph, fpost_ph;
+    std::vector<Table<ResidJob<double, double>>> res64;
+    std::vector<Table<ResidJob<float, float>>> res32;
+    std::vector<Table<ResidJob<float, double>>> res3264;
+    std::vector<Table<ProlongJob<double, double>>> pro64;
+    std::vector<Table<ProlongJob<float, float>>> pro32;
+    std::vector<Table<ProlongJob<float, double>>> pro3264;
+    Table<CoarseJob> coarse;
+    int coarse_smem = 0;
+    Table<DirectJob> direct;   // problems whose bottom is the coarse-cycle level, solved by its inverse
+    Table<CellJob<float, double>> r_to32;   // mixed: level-0 rhs rounded to FP32
+    Table<CellJob<float, float>> guess32;   // e = r invd on FP32 level 0
+    Table<CellJob<double, double>> guess64; // e = r invd on FP64 level 0
+    Table<CellJob<double, float>> e_to64;   // mixed: the correction widened
+    Table<CellJob<double, double>> update;  // phi += e (valid cells and ghosts)
+    Table<FillJob<double>> fill_phi;        // caller BCs
+    int fill_phi_ph = 1;
+    Table<NormJob> norm;
+    std::vector<double> vol;
+};
+
+CoarseArgs coarse_args_of(mgp_solver* s, int d, int nd, int nu, int nb) {
+    CoarseArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.lv = s->d_lv;
+    a.d0 = d;
+    const bool direct = s->d_ainv && !s->direct_large && d <= s->db;
+    a.maxdepth = direct ? s->db : s->maxdepth;
+    a.ainv = direct ? s->d_ainv : nullptr;
+    a.numcycles = 1;
+    a.nd = nd;
+    a.nu = nu;
+    a.nb = nb;
+    a.dd = 0;
+    a.refx = s->d_ref;
+    a.refy = s->d_ref + s->maxdepth + 1;
+    a.status = s->d_status;
+    a.shadow = s->d_shadow;
+    a.smem_bytes = s->shadow_bytes;
+    a.grid_ctas = 0;
+    return a;
+}
+
+void build_plan(Plan& P, const std::vector<mgp_solver*>& ss, const std::vector<int>& act, const std::vector<BCd>& ubc,
+                int homog, int nd, int nu, int nb) {
+    P = Plan();
+    for (int p : act) P.D = std::max(P.D, ss[p]->dc);
+    P.mix = !act.empty() && mixed(ss[act[0]]);
+    const int D = P.D;
+    P.sw64.resize(D); P.sw32.resize(D);
+    P.fpre64.resize(D); P.fpre32.resize(D); P.fpost64.resize(D); P.fpost32.resize(D);
+    P.fpre_ph.assign(D, 1); P.fpost_ph.assign(D, 1);
+    P.res64.resize(D); P.res32.resize(D); P.res3264.resize(D);
+    P.pro64.resize(D); P.pro32.resize(D); P.pro3264.resize(D);
+    for (int p : act) {
+        mgp_solver* s = ss[p];
+        const bool mx = mixed(s);
+        for (int d = 0; d < s->dc; ++d) {
+            const Lv& F = s->lv[d];
+            Lv& C = s->lv[d + 1];
+            const int rx = s->refx[d], ry = s->refy[d];
+            const bool next_grid = d + 1 < s->dc;
+            if (!fill_one_phase(F.bc, 0)) P.fpre_ph[d] = 3;
+            if (!fill_one_phase(C.bc, 1)) P.fpost_ph[d] = 3;
+            const int fblk = cdiv(2 * (F.nx + F.ny) + 12, 256), cblk = cdiv(2 * (C.nx + C.ny) + 12, 256);
+            const int gbx = cdiv(F.nx, 32), gby = cdiv(F.ny, 8);
+            const int cbx = cdiv(C.nx, 32), cby = cdiv(C.ny, 8);
+            if (mx) {
+                auto& L = s->lv32[d];
+                add_sweep_job(P.sw32[d], s->tma32[d], L.e, L.e2, L.r, L.invd, L.g, F.bc, L.nx, L.ny);
+                P.fpre32[d].push(FillJob<float>{L.e, L.g, F.bc, L.nx, L.ny, 1, 0}, fblk);
+                if (next_grid) {
+                    auto& N = s->lv32[d + 1];
+                    P.res32[d].push(ResidJob<float, float>{L.e, L.r, L.g, F.bc, N.r, N.e, N.invd, L.nx, L.ny, N.nx, N.ny,
+                                                           rx, ry, gbx},
+                                    gbx * gby);
+                    P.fpost32[d].push(FillJob<float>{N.e, N.g, C.bc, N.nx, N.ny, 1, 1}, cblk);
+                    P.pro32[d].push(ProlongJob<float, float>{L.e, N.e, N.nx, N.ny, rx, ry, cbx}, cbx * cby);
+                } else {
+                    P.res3264[d].push(ResidJob<float, double>{L.e, L.r, L.g, F.bc, C.r, C.e, C.invd, L.nx, L.ny, C.nx,
+                                                              C.ny, rx, ry, gbx},
+                                      gbx * gby);
+                    P.fpost64[d].push(FillJob<double>{C.e, C.g, C.bc, C.nx, C.ny, 1, 1}, cblk);
+                    P.pro3264[d].push(ProlongJob<float, double>{L.e, C.e, C.nx, C.ny, rx, ry, cbx}, cbx * cby);
+                }
+            } else {
+                add_sweep_job(P.sw64[d], s->tma[d], F.e, F.e2, F.r, F.invd, F.g, F.bc, F.nx, F.ny);
+                P.fpre64[d].push(FillJob<double>{F.e, F.g, F.bc, F.nx, F.ny, 1, 0}, fblk);
+                P.res64[d].push(ResidJob<double, double>{F.e, F.r, F.g, F.bc, C.r, C.e, C.invd, F.nx, F.ny, C.nx, C.ny,
+                                                         rx, ry, gbx},
+                                gbx * gby);
+                P.fpost64[d].push(FillJob<double>{C.e, C.g, C.bc, C.nx, C.ny, 1, 1}, cblk);
+                P.pro64[d].push(ProlongJob<double, double>{F.e, C.e, C.nx, C.ny, rx, ry, cbx}, cbx * cby);
+            }
+        }
+        if (s->direct_large && s->db == s->dc) {
+            const Lv& B = s->lv[s->dc];
+            P.direct.push(DirectJob{B.e, B.r, s->d_ainv, B.nx, B.ny}, direct_apply_blocks(B.nx, B.ny));
+        } else {
+            CoarseJob cj;
+            cj.a = coarse_args_of(s, s->dc, nd, nu, nb);
+            P.coarse.push(cj, 1);
+            if (s->d_shadow) P.coarse_smem = std::max(P.coarse_smem, s->shadow_bytes);
+        }
+        const Lv& L0 = s->lv[0];
+        const int nx = L0.nx, ny = L0.ny;
+        const int bx0 = cdiv(nx, 32), by0 = cdiv(ny, 8), bxg = cdiv(nx + 2, 32), byg = cdiv(ny + 2, 8);
+        if (mx) {
+            auto& M = s->lv32[0];
+            P.r_to32.push(CellJob<float, double>{M.r, L0.r, DF32{}, nx, ny, 0, bx0}, bx0 * by0);
+            P.guess32.push(CellJob<float, float>{M.e, M.r, M.invd, nx, ny, 0, bx0}, bx0 * by0);
+            P.e_to64.push(CellJob<double, float>{L0.e, M.e, DF{}, nx, ny, 1, bxg}, bxg * byg);
+        } else {
+            P.guess64.push(CellJob<double, double>{L0.e, L0.r, L0.invd, nx, ny, 0, bx0}, bx0 * by0);
+        }
+        P.update.push(CellJob<double, double>{s->phi0, L0.e, DF{}, nx, ny, 1, bxg}, bxg * byg);
+        if (!fill_one_phase(ubc[p], 0)) P.fill_phi_ph = 3;
+        P.fill_phi.push(FillJob<double>{s->phi0, L0.g, ubc[p], nx, ny, homog, 0}, cdiv(2 * (nx + ny) + 12, 256));
+        P.norm.push(NormJob{s->phi0, s->rhs0, L0.r, L0.g, ubc[p], nx, ny, homog, bx0}, bx0 * by0);
+        P.vol.push_back(s->valid.dx * s->valid.dy);
+    }
+}
+
+template <class F>
+void for_tables(Plan& P, F f) {
+    for (auto& g : P.sw64) { f(g.w32); f(g.w64); }
+    for (auto& g : P.sw32) { f(g.w32); f(g.w64); }
+    for (auto& t : P.fpre64) f(t);
+    for (auto& t : P.fpre32) f(t);
+    for (auto& t : P.fpost64) f(t);
+    for (auto& t : P.fpost32) f(t);
+    for (auto& t : P.res64) f(t);
+    for (auto& t : P.res32) f(t);
+    for (auto& t : P.res3264) f(t);
+    for (auto& t : P.pro64) f(t);
+    for (auto& t : P.pro32) f(t);
+    for (auto& t : P.pro3264) f(t);
+    f(P.coarse); f(P.direct); f(P.r_to32); f(P.guess32); f(P.guess64); f(P.e_to64); f(P.update); f(P.fill_phi); f(P.norm);
+}
+
+int upload_plan(Plan& P, Lockstep* ls, cudaStream_t st) {
+    Packer pk;
+    for_tables(P, [&](auto& t) { t.pack(pk); });
+    const size_t ov = pk.add(P.vol.data(), P.vol.size() * sizeof(double));
+    if (pk.host.size() > ls->cap) {
+        CK(cudaStreamSynchronize(st));
+        dfree(ls->dev, st);
+        ls->dev = nullptr;
+        ls->cap = 0;
+        const size_t cap = pk.host.size() + pk.host.size() / 2;
+        if (dmalloc(&ls->dev, cap, st) != cudaSuccess) {
+            cudaGetLastError();
+            return set_err(MGP_ENOMEM, "lockstep: device allocation failed");
+        }
+        ls->cap = cap;
+    }
+    // the tables the previous iteration's kernels read are no longer in use
+    // (the host synchronised on its norms); stream order covers the rest
+    CK(cudaMemcpyAsync(ls->dev, pk.host.data(), pk.host.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));   // the pageable source must stay valid until copied
+    for_tables(P, [&](auto& t) { t.bind(ls->dev); });
+    const size_t nb = (size_t)P.norm.blocks();
+    if (nb > ls->part_cap) {
+        dfree(ls->part, st);
+        ls->part = nullptr;
+        ls->part_cap = 0;
+        if (dmalloc(&ls->part, nb * sizeof(double), st) != cudaSuccess) {
+            cudaGetLastError();
+            return set_err(MGP_ENOMEM, "lockstep: device allocation failed");
+        }
+        ls->part_cap = nb;
+    }
+    ls->vols = reinterpret_cast<double*>(ls->dev + ov);
+    return MGP_OK;
+}
+
+template <class T>
+int sweeps(SweepGroups<T>& g, int n, Lockstep* ls, cudaStream_t st) {
+    for (int k = 0; k < n; ++k) {
+        CK(launch_sweep9_jobs<T>(g.w32.dj, g.w32.dp, g.w32.n(), g.w32.blocks(), 32, 1, k & 1, ls->status, st));
+        CK(launch_sweep9_jobs<T>(g.w64.dj, g.w64.dp, g.w64.n(), g.w64.blocks(), 64, 1, k & 1, ls->status, st));
+    }
+    return MGP_OK;
+}
+
+// One V-cycle iteration of every problem in the plan: vcycle_top, the cycle, phi += e, the new residual and its norm.
+int lockstep_iteration(Plan& P, Lockstep* ls, int nd, int nu, cudaStream_t st) {
+    CK(launch_cell_jobs(P.r_to32.dj, P.r_to32.dp, P.r_to32.n(), P.r_to32.blocks(), 1, st));
+    CK(launch_cell_jobs(P.guess32.dj, P.guess32.dp, P.guess32.n(), P.guess32.blocks(), 3, st));
+    CK(launch_cell_jobs(P.guess64.dj, P.guess64.dp, P.guess64.n(), P.guess64.blocks(), 3, st));
+    for (int d = 0; d < P.D; ++d) {   // down: smooth, fill, residual-restriction-guess (MG:784-806)
+        RC(sweeps(P.sw64[d], nd, ls, st));
+        RC(sweeps(P.sw32[d], nd, ls, st));
+        CK(launch_fill_jobs(P.fpre64[d].dj, P.fpre64[d].dp, P.fpre64[d].n(), P.fpre64[d].blocks(), P.fpre_ph[d], st));
+        CK(launch_fill_jobs(P.fpre32[d].dj, P.fpre32[d].dp, P.fpre32[d].n(), P.fpre32[d].blocks(), P.fpre_ph[d], st));
+        CK(launch_resid_jobs(P.res64[d].dj, P.res64[d].dp, P.res64[d].n(), P.res64[d].blocks(), st));
+        CK(launch_resid_jobs(P.res32[d].dj, P.res32[d].dp, P.res32[d].n(), P.res32[d].blocks(), st));
+        CK(launch_resid_jobs(P.res3264[d].dj, P.res3264[d].dp, P.res3264[d].n(), P.res3264[d].blocks(), st));
+    }
+    CK(launch_coarse_jobs(P.coarse.dj, P.coarse.n(), P.coarse_smem, st));
+    CK(launch_direct_jobs(P.direct.dj, P.direct.dp, P.direct.n(), P.direct.blocks(), st));
+    for (int d = P.D - 1; d >= 0; --d) {   // up: fill the coarse correction, prolong, smooth (MG:818-845)
+        CK(launch_fill_jobs(P.fpost64[d].dj, P.fpost64[d].dp, P.fpost64[d].n(), P.fpost64[d].blocks(), P.fpost_ph[d],
+                            st));
+        CK(launch_fill_jobs(P.fpost32[d].dj, P.fpost32[d].dp, P.fpost32[d].n(), P.fpost32[d].blocks(), P.fpost_ph[d],
+                            st));
+        CK(launch_prolong_jobs(P.pro64[d].dj, P.pro64[d].dp, P.pro64[d].n(), P.pro64[d].blocks(), st));
+        CK(launch_prolong_jobs(P.pro32[d].dj, P.pro32[d].dp, P.pro32[d].n(), P.pro32[d].blocks(), st));
+        CK(launch_prolong_jobs(P.pro3264[d].dj, P.pro3264[d].dp, P.pro3264[d].n(), P.pro3264[d].blocks(), st));
+        RC(sweeps(P.sw64[d], nu, ls, st));
+        RC(sweeps(P.sw32[d], nu, ls, st));
+    }
+    CK(launch_cell_jobs(P.e_to64.dj, P.e_to64.dp, P.e_to64.n(), P.e_to64.blocks(), 1, st));
+    CK(launch_cell_jobs(P.update.dj, P.update.dp, P.update.n(), P.update.blocks(), 0, st));   // MG:611
+    CK(launch_fill_jobs(P.fill_phi.dj, P.fill_phi.dp, P.fill_phi.n(), P.fill_phi.blocks(), P.fill_phi_ph, st));
+    CK(launch_norm_jobs(P.norm.dj, P.norm.dp, P.norm.n(), P.norm.blocks(), ls->part, ls->vols, ls->norms, st));
+    return MGP_OK;
+}
+
+}  // namespace
+
+Lockstep* lockstep_new() { return new Lockstep(); }
+
+void lockstep_free(Lockstep* ls) {
+    if (!ls) return;
+    cudaDeviceSynchronize();
+    dfree(ls->dev, nullptr);
+    dfree(ls->part, nullptr);
+    dfree(ls->norms, nullptr);
+    dfree(ls->status, nullptr);
+    if (ls->h_norms) cudaFreeHost(ls->h_norms);
+    if (ls->e0) cudaEventDestroy(ls->e0);
+    if (ls->e1) cudaEventDestroy(ls->e1);
+    delete ls;
+}
+
+// Whether the lockstep path serves these solvers with these counts: the MG
+// stationary V-cycle (no Krylov or GMRES flags), one coarse visit per level,
+// even smoothing counts (so every phase but the sweeps finds each level's
+// correction in its first buffer), every level swept with TMA descriptors, no
+// periodic side and a Dirichlet side (no mean removal), bottoms that fit one
+// CTA, and one precision for all.
+bool lockstep_ok(const std::vector<mgp_solver*>& ss, int numcycles, int nd, int nu) {
+    if (ss.empty() || numcycles != 1 || (nd & 1) || (nu & 1) || nd < 0 || nu < 0) return false;
+    const bool mx = mixed(ss[0]);
+    for (mgp_solver* s : ss) {
+        if (s->kind != MGP_KIND_MG || (s->flags & (MGP_FLAG_KRYLOV | MGP_FLAG_GMRES)) ||
+            (s->direct_large && s->db != s->dc) || s->grid_ctas > 1 || mixed(s) != mx)
+            return false;
+        bool diri = false;
+        for (int k = 0; k < 4; ++k) {
+            if (s->types[k] == MGP_BCTYPE_PERIODIC) return false;
+            diri = diri || s->types[k] == MGP_BCTYPE_DIRI;
+        }
+        if (!diri) return false;
+        for (int d = 0; d < s->dc; ++d) {
+            const SweepTma& t = mx ? s->tma32[d] : s->tma[d];
+            if (!t.ok || !s->lv[d].e2.p || !sweep_fusable(s->lv[d].bc)) return false;
+        }
+    }
+    return true;
+}
+
+int lockstep_vcycle(const std::vector<mgp_solver*>& ss, Lockstep* ls, mgp_array* phi, mgp_array* rhs,
+                    const mgp_bdry* bc, int homog, double tol, int maxiters, int nd, int nu, int nb, int zerophi,
+                    mgp_report* reports, cudaStream_t st) {
+    const int n = (int)ss.size();
+    if (maxiters < 0 || nb < 0) return set_err(MGP_EINVAL, "negative count");
+    if (ls->ncap < n) {
+        dfree(ls->norms, st);
+        if (ls->h_norms) cudaFreeHost(ls->h_norms);
+        ls->norms = nullptr;
+        ls->h_norms = nullptr;
+        if (dmalloc(&ls->norms, sizeof(double) * n, st) != cudaSuccess ||
+            cudaMallocHost(&ls->h_norms, sizeof(double) * n) != cudaSuccess) {
+            cudaGetLastError();
+            ls->ncap = 0;
+            return set_err(MGP_ENOMEM, "lockstep: allocation failed");
+        }
+        ls->ncap = n;
+    }
+    if (!ls->status && dmalloc(&ls->status, sizeof(int), st) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(MGP_ENOMEM, "lockstep: allocation failed");
+    }
+    if (!ls->e0) CK(cudaEventCreate(&ls->e0));
+    if (!ls->e1) CK(cudaEventCreate(&ls->e1));
+    CK(sweep_kernels_init());
+    CK(coarse_kernels_init());
+    CK(cudaEventRecord(ls->e0, st));
+    CK(cudaMemsetAsync(ls->status, 0, sizeof(int), st));
+    std::vector<BCd> ubc(n);
+    for (int p = 0; p < n; ++p) {   // solver_solve's set-up, per problem
+        mgp_solver* s = ss[p];
+        const int nx = s->valid.nx, ny = s->valid.ny;
+        RC(check_array(&phi[p], nx, "phi"));
+        RC(check_array(&rhs[p], nx, "rhs"));
+        for (int k = 0; k < 4; ++k)
+            if (bc[p].type[k] != s->types[k]) return set_err(MGP_EINVAL, "BC types differ from the solver's");
+        RC(make_bc(&bc[p], &s->valid, homog, s->d_bcbuf, &ubc[p], st));
+        CK(cudaMemsetAsync(s->state.base, 0, s->state.elems * sizeof(double), st));
+        if (s->state32.base) CK(cudaMemsetAsync(s->state32.base, 0, s->state32.elems * sizeof(float), st));
+        CK(cudaMemsetAsync(s->d_status, 0, sizeof(int), st));
+        RC(stage_in(&phi[p], nx, ny, s->phi0, 1, st));
+        RC(stage_in(&rhs[p], nx, ny, s->rhs0, 0, st));
+        if (zerophi) CK(launch_fillval(s->phi0, 0.0, nx, ny, 1, 1, st));
+    }
+    std::vector<std::vector<double>> hist(n, std::vector<double>((size_t)maxiters + 1, 0.0));
+    std::vector<double> rscale(n, 1.0);
+    std::vector<int> iters(n, 0), diverged(n, 0), status(n, MGP_OK);
+    std::vector<int> act(n);
+    for (int p = 0; p < n; ++p) act[p] = p;
+    Plan P;
+    // r(0) = rhs - L[phi] with the caller's BCs (MG:579) and its norm
+    build_plan(P, ss, act, ubc, homog, nd, nu, nb);
+    RC(upload_plan(P, ls, st));
+    CK(launch_fill_jobs(P.fill_phi.dj, P.fill_phi.dp, P.fill_phi.n(), P.fill_phi.blocks(), P.fill_phi_ph, st));
+    CK(launch_norm_jobs(P.norm.dj, P.norm.dp, P.norm.n(), P.norm.blocks(), ls->part, ls->vols, ls->norms, st));
+    CK(cudaMemcpyAsync(ls->h_norms, ls->norms, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::vector<int> next;
+    for (int p = 0; p < n; ++p) {
+        double r = ls->h_norms[p];
+        if (r == 0.0) { hist[p][0] = 0.0; r = 1.0; }
+        else hist[p][0] = 1.0;
+        rscale[p] = r;
+        if (!std::isfinite(r)) status[p] = MGP_EDIVERGED;
+        else if (hist[p][0] > tol && maxiters > 0) next.push_back(p);
+    }
+    act.swap(next);
+    for (int iter = 1; iter <= maxiters && !act.empty(); ++iter) {
+        build_plan(P, ss, act, ubc, homog, nd, nu, nb);
+        RC(upload_plan(P, ls, st));
+        RC(lockstep_iteration(P, ls, nd, nu, st));
+        CK(cudaMemcpyAsync(ls->h_norms, ls->norms, sizeof(double) * act.size(), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        next.clear();
+        std::vector<int> undo;
+        for (size_t k = 0; k < act.size(); ++k) {
+            const int p = act[k];
+            const double rr = ls->h_norms[k] / rscale[p];
+            hist[p][iter] = rr;
+            iters[p] = iter;
+            if (!std::isfinite(rr)) { status[p] = MGP_EDIVERGED; continue; }
+            if (rr <= tol) continue;
+            if (rr > hist[p][iter - 1]) {   // MG:630-639: undo the correction and stop
+                diverged[p] = 1;
+                undo.push_back(p);
+                continue;
+            }
+            next.push_back(p);
+        }
+        if (!undo.empty()) {
+            Table<CellJob<double, double>> t;
+            for (int p : undo) {
+                mgp_solver* s = ss[p];
+                const int nx = s->valid.nx, ny = s->valid.ny, bx = cdiv(nx + 2, 32), by = cdiv(ny + 2, 8);
+                t.push(CellJob<double, double>{s->phi0, s->lv[0].e, DF{}, nx, ny, 1, bx}, bx * by);
+            }
+            Packer pk;
+            t.pack(pk);
+            CK(cudaMemcpyAsync(ls->dev, pk.host.data(), pk.host.size(), cudaMemcpyHostToDevice, st));
+            t.bind(ls->dev);
+            CK(launch_cell_jobs(t.dj, t.dp, t.n(), t.blocks(), 2, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        act.swap(next);
+    }
+    for (int p = 0; p < n; ++p) RC(stage_out(ss[p]->phi0, &phi[p], ss[p]->valid.nx, ss[p]->valid.ny, 1, st));
+    CK(cudaEventRecord(ls->e1, st));
+    CK(cudaStreamSynchronize(st));
+    int sweep_status = 0;
+    CK(cudaMemcpy(&sweep_status, ls->status, sizeof(int), cudaMemcpyDeviceToHost));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ls->e0, ls->e1);
+    int first = MGP_OK;
+    for (int p = 0; p < n; ++p) {
+        int dstat = 0;
+        CK(cudaMemcpy(&dstat, ss[p]->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+        if (!dstat) dstat = sweep_status;
+        if (status[p] == MGP_OK && dstat)
+            status[p] = (dstat == DST_TIMEOUT) ? MGP_ETIMEOUT : (dstat == DST_MISALIGNED) ? MGP_ECUDA : MGP_EDIVERGED;
+        if (reports) {
+            mgp_report& r = reports[p];
+            double* dst = r.relres;
+            std::memset(&r, 0, sizeof r);
+            r.relres = dst;
+            r.status = status[p];
+            r.iterations = iters[p];
+            r.maxdepth = ss[p]->maxdepth;
+            r.diverged = diverged[p];
+            r.rscale = rscale[p];
+            r.final_relres = hist[p][iters[p]];
+            r.seconds = ms * 1e-3;
+            if (dst)
+                for (int k = 0; k <= iters[p]; ++k) dst[k] = hist[p][k];
+        }
+        if (status[p] && !first) first = status[p];
+    }
+    if (first == MGP_ETIMEOUT) return set_err(first, "a device wait ran out of its iteration limit");
+    if (first == MGP_ECUDA) return set_err(first, "misaligned shared-memory window in the sweep");
+    if (first) return set_err(first, "non-finite residual");
+    return MGP_OK;
+}
 }  // namespace mgp
 
 // ===========================================================================

@@ -1910,6 +1910,43 @@ cudaError_t launch_direct_apply(const DF& e, const DF& r, const double* ainv, in
     return cudaGetLastError();
 }
 
+// The exact bottoms of a lockstep batch (MGP_FLAG_DIRECT_LARGE): job k owns
+// blocks [pre[k], pre[k+1]), each k_direct_apply's rows of the job's level.
+__global__ void __launch_bounds__(kDirectApplyThreads) k_direct_jobs(const DirectJob* __restrict__ jobs,
+                                                                     const int* __restrict__ pre, int njobs) {
+    __shared__ double rs[kDirectLargeCells];
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(pre + mid) <= (int)blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    const DirectJob& J = jobs[lo];
+    const int n = J.nx * J.ny;
+    for (int m = threadIdx.x; m < n; m += blockDim.x) rs[m] = AT(J.r, m % J.nx, m / J.nx);
+    __syncthreads();
+    const int k = ((int)blockIdx.x - pre[lo]) * (kDirectApplyThreads / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (k >= n) return;
+    const double* row = J.ainv + (long)k * n;
+    double sacc = 0.0;
+#pragma unroll 8
+    for (int m = lane; m < n; m += 32) sacc = sacc + row[m] * rs[m];
+    for (int o = 16; o > 0; o >>= 1) sacc = sacc + __shfl_xor_sync(0xffffffffu, sacc, o);
+    if (lane == 0) AT(J.e, k % J.nx, k / J.nx) = sacc;
+}
+
+int direct_apply_blocks(int nx, int ny) {
+    const int w = kDirectApplyThreads / 32;
+    return (nx * ny + w - 1) / w;
+}
+
+cudaError_t launch_direct_jobs(const DirectJob* jobs, const int* pre, int njobs, int nblocks, cudaStream_t st) {
+    if (njobs < 1 || nblocks < 1) return cudaSuccess;
+    k_direct_jobs<<<nblocks, kDirectApplyThreads, 0, st>>>(jobs, pre, njobs);
+    count_launch();
+    return cudaGetLastError();
+}
+
 // Per device: opt the shared-memory coarse kernel into its largest window.
 cudaError_t coarse_kernels_init() {
     static std::mutex mu;

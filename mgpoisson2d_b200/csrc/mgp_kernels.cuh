@@ -200,6 +200,12 @@ struct NormJob {
 struct CoarseJob {
     CoarseArgs a;
 };
+// e = A^-1 r on a problem's exact bottom (MGP_FLAG_DIRECT_LARGE; k_direct_apply's blocks).
+struct DirectJob {
+    DF e, r;
+    const double* ainv;
+    int nx, ny;
+};
 
 // Descriptors for sweeping one level with phi in either of its two buffers.
 struct SweepTma {
@@ -256,6 +262,8 @@ cudaError_t launch_cell_jobs(const CellJob<TD, TS>* jobs, const int* pre, int nj
 cudaError_t launch_norm_jobs(const NormJob* jobs, const int* pre, int njobs, int nblocks, double* partials,
                              const double* volk, double* norms, cudaStream_t st);
 cudaError_t launch_coarse_jobs(const CoarseJob* jobs, int njobs, int smem_bytes, cudaStream_t st);
+int direct_apply_blocks(int nx, int ny);
+cudaError_t launch_direct_jobs(const DirectJob* jobs, const int* pre, int njobs, int nblocks, cudaStream_t st);
 cudaError_t launch_invdiag(const DF& invd, const Geo& g, const BCd& b, int homog, int nx, int ny, int coupled,
                            cudaStream_t st);
 // kind: 0 cell, 1 x-face, 2 y-face, 3 node.  ncx/ncy = coarse cell counts.

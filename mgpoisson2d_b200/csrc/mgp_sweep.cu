@@ -317,17 +317,19 @@ __device__ __forceinline__ void gs9_pair(float* a, float* b, bool write_b, float
     if (write_b) b[0] = r.y;
 }
 
-template <bool kTma, class T, int TX, int K = 1>
-__global__ void __launch_bounds__((Win<T, TX, K>::kThreads), (Win<T, TX, K>::kMinBlocks))
-    k_sweep9(const __grid_constant__ SweepMaps m, DFT<T> pin, DFT<T> pout, DFT<T> rhs, DFT<T> invd, GeoT<T> g,
-             const __grid_constant__ BCd b, int homog, int nx, int ny, int4 part, double omega, int* status) {
+// The sweep of tile (bx, by) of a level, by one CTA (the body of k_sweep9
+// and of the lockstep batch's k_sweep9_jobs).  m and b may live in kernel
+// parameter space or in global memory.
+template <bool kTma, class T, int TX, int K>
+__device__ __forceinline__ void sweep_tile(const SweepMaps& m, const DFT<T>& pin, const DFT<T>& pout,
+                                           const DFT<T>& rhs, const DFT<T>& invd, const GeoT<T>& g, const BCd& b,
+                                           int homog, int nx, int ny, int4 part, double omega, int* status, int bx,
+                                           int by) {
     using W = Win<T, TX, K>;
-    allow_dependents();
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     T* smem = reinterpret_cast<T*>(smem_raw);
     // tile bounds: part = (nx / gx, nx % gx, ny / gy, ny % gy); the first
     // nx % gx columns of tiles are one cell wider
-    const int bx = blockIdx.x, by = blockIdx.y;
     const int X0 = bx * part.x + min(bx, part.y), X1 = X0 + part.x + (bx < part.y ? 1 : 0);
     const int Y0 = by * part.z + min(by, part.w), Y1 = Y0 + part.z + (by < part.w ? 1 : 0);
     const Per pr = periodic_of(b);
@@ -549,6 +551,47 @@ __global__ void __launch_bounds__((Win<T, TX, K>::kThreads), (Win<T, TX, K>::kMi
     }
 }
 
+template <bool kTma, class T, int TX, int K = 1>
+__global__ void __launch_bounds__((Win<T, TX, K>::kThreads), (Win<T, TX, K>::kMinBlocks))
+    k_sweep9(const __grid_constant__ SweepMaps m, DFT<T> pin, DFT<T> pout, DFT<T> rhs, DFT<T> invd, GeoT<T> g,
+             const __grid_constant__ BCd b, int homog, int nx, int ny, int4 part, double omega, int* status) {
+    allow_dependents();
+    sweep_tile<kTma, T, TX, K>(m, pin, pout, rhs, invd, g, b, homog, nx, ny, part, omega, status, blockIdx.x,
+                               blockIdx.y);
+}
+
+// Lockstep batches: one launch sweeps the same level of many problems.  Job
+// k owns blocks [pre[k], pre[k + 1]) of the grid, one per tile of its level
+// (row-major over its gx x gy tiles); a block finds its job by binary
+// search.  flip selects the buffer each job's phi is read from (the job's s0
+// xor flip), so one job table serves every sweep of a smoothing call.
+// Descriptors in a job table may have been rewritten since the last launch
+// that read them (tables are rebuilt when the set of unconverged problems
+// changes): the tensor-map proxy is made to see the new ones before use.
+template <class T, int TX, int K>
+__global__ void __launch_bounds__((Win<T, TX, K>::kThreads), (Win<T, TX, K>::kMinBlocks))
+    k_sweep9_jobs(const SweepJobT<T>* __restrict__ jobs, const int* __restrict__ pre, int njobs, int flip,
+                  double omega, int* status) {
+    allow_dependents();
+    const int blk = blockIdx.x;
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {   // the last job with pre[job] <= blk
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(pre + mid) <= blk) lo = mid;
+        else hi = mid - 1;
+    }
+    const SweepJobT<T>& J = jobs[lo];
+    const int q = blk - __ldg(pre + lo), side = J.s0 ^ flip;
+    const SweepMaps& m = J.m[side];
+    if (threadIdx.x == 0) {
+        for (const CUtensorMap* d : {&m.pin, &m.rhs, &m.invd, &m.xx, &m.xy, &m.yx, &m.yy})
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(d) : "memory");
+    }
+    __syncthreads();
+    sweep_tile<true, T, TX, K>(m, J.buf[side], J.buf[side ^ 1], J.rhs, J.invd, J.g, J.b, 1, J.nx, J.ny, J.part, omega,
+                               status, q % J.gx, q / J.gx);
+}
+
 }  // namespace
 
 bool sweep_fusable(const BCd& b) {
@@ -610,6 +653,12 @@ bool prepare_maps(SweepMaps* m, const DFT<T>& e, const DFT<T>& rhs, const DFT<T>
            encode<W>(&m->invd, invd.p, nx, ny, invd.ld) && encode<W>(&m->xx, g.xx.p, nx + 1, ny, g.xx.ld) &&
            encode<W>(&m->xy, g.xy.p, nx + 1, ny, g.xy.ld) && encode<W>(&m->yx, g.yx.p, nx, ny + 1, g.yx.ld) &&
            encode<W>(&m->yy, g.yy.p, nx, ny + 1, g.yy.ld);
+}
+
+template <class T, int TX, int K>
+cudaError_t set_attr_jobs() {
+    return cudaFuncSetAttribute(k_sweep9_jobs<T, TX, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)Win<T, TX, K>::kSmemBytes);
 }
 
 template <class T, int TX, int K = 1>
@@ -742,6 +791,11 @@ cudaError_t sweep_kernels_init() {
     if (e == cudaSuccess) e = set_attr<float, 64>();
     if (e == cudaSuccess) e = set_attr<float, 32, 2>();
     if (e == cudaSuccess) e = set_attr<double, 32, 2>();
+    if (e == cudaSuccess) e = set_attr_jobs<double, 32, 1>();
+    if (e == cudaSuccess) e = set_attr_jobs<double, 32, 2>();
+    if (e == cudaSuccess) e = set_attr_jobs<float, 32, 1>();
+    if (e == cudaSuccess) e = set_attr_jobs<float, 64, 1>();
+    if (e == cudaSuccess) e = set_attr_jobs<float, 32, 2>();
     if (e == cudaSuccess && dev < 64) done |= 1ull << dev;
     return e;
 }
@@ -799,5 +853,43 @@ cudaError_t launch_sweep9_pair(const DF& pin, const DF& pout, const DF& rhs, con
                                int* status, cudaStream_t st) {
     return sweep_pair_impl(pin, pout, rhs, invd, g, b, homog, nx, ny, omega, tma, status, st);
 }
+
+namespace {
+template <class T, int TX, int K>
+cudaError_t jobs_launch(const SweepJobT<T>* jobs, const int* pre, int njobs, int nblocks, int flip, int* status,
+                        cudaStream_t st) {
+    using W = Win<T, TX, K>;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nblocks);
+    cfg.blockDim = dim3(W::kThreads);
+    cfg.dynamicSmemBytes = W::kSmemBytes;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_sweep9_jobs<T, TX, K>, jobs, pre, njobs, flip, 1.0, status);
+}
+}  // namespace
+
+template <class T>
+cudaError_t launch_sweep9_jobs(const SweepJobT<T>* jobs, const int* pre, int njobs, int nblocks, int tx, int k,
+                               int flip, int* status, cudaStream_t st) {
+    if (njobs < 1 || nblocks < 1) return cudaSuccess;
+    cudaError_t e = sweep_kernels_init();
+    if (e != cudaSuccess) return e;
+    if (tx == 32 && k == 1) e = jobs_launch<T, 32, 1>(jobs, pre, njobs, nblocks, flip, status, st);
+    else if (tx == 32 && k == 2) e = jobs_launch<T, 32, 2>(jobs, pre, njobs, nblocks, flip, status, st);
+    else if (sizeof(T) == 4 && tx == 64 && k == 1) e = jobs_launch<float, 64, 1>(
+        reinterpret_cast<const SweepJobT<float>*>(jobs), pre, njobs, nblocks, flip, status, st);
+    else return cudaErrorInvalidValue;
+    count_launch();
+    return e;
+}
+template cudaError_t launch_sweep9_jobs<double>(const SweepJobT<double>*, const int*, int, int, int, int, int, int*,
+                                                cudaStream_t);
+template cudaError_t launch_sweep9_jobs<float>(const SweepJobT<float>*, const int*, int, int, int, int, int, int*,
+                                               cudaStream_t);
 
 }  // namespace mgp

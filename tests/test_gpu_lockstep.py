@@ -1,0 +1,117 @@
+"""Lockstep batches (MGP_FLAG_LOCKSTEP): every V-cycle phase of all unconverged
+problems in one launch.  Each problem's solution must have the bits of its own
+stationary V-cycle (the resident solver without the flag), whatever else is in
+the batch and whenever the others converge; the V-cycle counts must be the
+same; and the solutions must agree with the CPU oracle in both sweep orders
+(config 4's problems, whose uneven sides give (2,1) and (1,2) levels)."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from mgpoisson2d_b200 import workloads as W
+from mgpoisson2d_b200.types import BoxData
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+# problems of the batched workload: 2, 5, 6, 8 coarsen (2,1) first, 7 and 13 (1,2); sides 64..1008
+PROBS = [0, 1, 2, 5, 6, 7, 8, 13, 14, 20]
+
+
+@pytest.fixture(scope="module")
+def M():
+    assert torch.cuda.is_available(), "needs a CUDA device"
+    import mgpoisson2d_b200.api as api
+    return api
+
+
+@pytest.fixture(scope="module")
+def probs():
+    return [W.batch_problem(i) for i in PROBS]
+
+
+def _alone(M, prob, flags, maxiters=60):
+    v, geo, rhs, bc = prob
+    with M.Solver(v, geo, bc, M.KIND_MG, flags) as s:
+        phi = BoxData(v, 1, 1)
+        rep = s.vcycle(phi, rhs, bc, True, 1e-10, maxiters)
+    return rep, phi.interior().copy()
+
+
+def _lockstep(M, probs, flags, maxiters=60):
+    phis = [BoxData(p[0], 1, 1) for p in probs]
+    with M.Batch([(p[0], p[1], p[3]) for p in probs], M.KIND_MG, flags | M.FLAG_LOCKSTEP, nstreams=2) as b:
+        reps = b.vcycle(phis, [p[2] for p in probs], [p[3] for p in probs], True, 1e-10, maxiters)
+    return reps, [p.interior().copy() for p in phis]
+
+
+@pytest.mark.parametrize("mixed,bottom", [(False, "reference"), (True, "reference"), (True, "large")])
+def test_lockstep_same_bits_as_each_problem_alone(M, probs, mixed, bottom):
+    flags = M.FLAG_DIRICHLET_COUPLED_DIAG | (M.FLAG_MIXED if mixed else 0)
+    if bottom == "large":   # the exact bottom on the coarse-cycle level, a batched matrix-vector product
+        flags |= M.FLAG_DIRECT_COARSE | M.FLAG_DIRECT_LARGE
+    reps, sols = _lockstep(M, probs, flags)
+    its = set()
+    for k, prob in enumerate(probs):
+        ra, sa = _alone(M, prob, flags)
+        assert reps[k].iterations == ra.iterations, (PROBS[k], reps[k].iterations, ra.iterations)
+        assert reps[k].final_relres <= 1e-10 and not reps[k].diverged
+        np.testing.assert_allclose(reps[k].relres, ra.relres, rtol=1e-12, atol=0)
+        assert np.array_equal(sols[k].view(np.uint64), sa.view(np.uint64)), PROBS[k]
+        its.add(ra.iterations)
+    assert len(its) > 1   # the problems leave the batch at different V-cycles
+
+
+def test_lockstep_same_alone_and_in_the_mix(M, probs):
+    flags = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_MIXED
+    _, mix = _lockstep(M, probs, flags)
+    for k in (0, 3, 7):
+        _, one = _lockstep(M, [probs[k]], flags)
+        assert np.array_equal(one[0].view(np.uint64), mix[k].view(np.uint64))
+
+
+@pytest.mark.parametrize("mixed,large", [(False, False), (True, False), (True, True)])
+def test_lockstep_against_oracle(M, probs, mixed, large):
+    flags = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_DIRECT_COARSE | (M.FLAG_MIXED if mixed else 0)
+    flags |= M.FLAG_DIRECT_LARGE if large else 0
+    reps, sols = _lockstep(M, probs, flags)
+    O.lib().or_set_dirichlet_coupled_diagonal.argtypes = [ctypes.c_int]
+    O.lib().or_set_dirichlet_coupled_diagonal(1)
+    try:
+        for k, (v, geo, rhs, bc) in enumerate(probs):
+            assert reps[k].final_relres <= 1e-10
+            for order in (1, 0):
+                po = BoxData(v, 1, 1)
+                ro = O.vcycle(po, rhs, geo, bc, True, 1e-10, 200, gs_order=order)
+                ref = po.interior()
+                rel_l2 = np.linalg.norm(sols[k] - ref) / np.linalg.norm(ref)
+                rel_max = np.abs(sols[k] - ref).max() / np.abs(ref).max()
+                assert rel_l2 <= 1e-8 and rel_max <= 1e-7, (PROBS[k], order, rel_l2, rel_max)
+    finally:
+        O.lib().or_set_dirichlet_coupled_diagonal(0)
+
+
+def test_lockstep_falls_back_for_krylov_and_odd_counts(M, probs):
+    """Flags or counts the lockstep path does not serve run the concurrent
+    per-problem path: same answers as solving alone."""
+    sub = probs[:3]
+    flags = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV
+    reps, sols = _lockstep(M, sub, flags)
+    for k, prob in enumerate(sub):
+        ra, sa = _alone(M, prob, flags)
+        assert np.array_equal(sols[k], sa)
+    flags = M.FLAG_DIRICHLET_COUPLED_DIAG
+    phis = [BoxData(p[0], 1, 1) for p in sub]
+    with M.Batch([(p[0], p[1], p[3]) for p in sub], M.KIND_MG, flags | M.FLAG_LOCKSTEP) as b:
+        reps = b.vcycle(phis, [p[2] for p in sub], [p[3] for p in sub], True, 1e-10, 60, 1, 7, 7, 7)
+    for k, prob in enumerate(sub):
+        v, geo, rhs, bc = prob
+        with M.Solver(v, geo, bc, M.KIND_MG, flags) as s:
+            phi = BoxData(v, 1, 1)
+            s.vcycle(phi, rhs, bc, True, 1e-10, 60, 1, 7, 7, 7)
+        assert np.array_equal(phis[k].interior(), phi.interior())
