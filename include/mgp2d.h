@@ -408,6 +408,15 @@ int mgp_batch_size(const mgp_batch *b, int *nprob);
 int mgp_batch_vcycle(mgp_batch *b, mgp_array *phi, mgp_array *rhs, const mgp_bdry *bc, int homog,
                      double tol, int maxiters, int numcycles, int smooth_down, int smooth_up,
                      int smooth_bottom, int zerophi, mgp_report *reports);
+/* Knobs of the lockstep path (MGP_FLAG_LOCKSTEP), which change speed and never
+ * results: groups = how many groups of problems run their lockstep loops
+ * concurrently, each on its own stream (1 .. nstreams; 0 restores the
+ * default, min(4, nstreams)); pairs = 1 runs two sweeps per launch on the
+ * levels whose descriptors allow it (when the smoothing counts are multiples
+ * of 4).  mgpoisson2d_b200.api.Batch.autotune times the combinations and
+ * caches the fastest.  No reference counterpart. */
+int mgp_batch_set_tuning(mgp_batch *b, int groups, int pairs);
+int mgp_batch_get_tuning(const mgp_batch *b, int *groups, int *pairs);
 
 typedef struct mgp_server mgp_server;
 /* A solve server with nworkers slots.  Requests start in arrival order as a

@@ -80,6 +80,8 @@ _SIGS = {
     "mgp_batch_destroy": [_vp],
     "mgp_batch_size": [_vp, _P(_i)],
     "mgp_batch_vcycle": [_vp, _A, _A, _BC, _i, _d, _i, _i, _i, _i, _i, _i, _R],
+    "mgp_batch_set_tuning": [_vp, _i, _i],
+    "mgp_batch_get_tuning": [_vp, _P(_i), _P(_i)],
     "mgp_server_create": [_i, C.c_size_t, _i, _P(_vp)],
     "mgp_server_submit": [_vp, C.c_ulonglong, _B, _G, _BC, _A, _A, _i, _d, _i, _i, _i, _i, _i, _i,
                           _P(C.c_longlong)],
@@ -420,6 +422,7 @@ class Batch:
         _ck(_lib.mgp_batch_create(n, self._boxes, self._geos, self._bcs, kind, flags, maxdepth_user, nstreams,
                                   _r(self._h)), "batch_create")
         self.n = n
+        self._nstreams = max(1, min(nstreams, n))
 
     def close(self):
         if self._h:
@@ -437,6 +440,69 @@ class Batch:
 
     def __exit__(self, *a):
         self.close()
+
+    def set_tuning(self, groups: int = 0, pairs: int = 0):
+        """Lockstep knobs (mgp_batch_set_tuning): concurrent groups, two sweeps per launch."""
+        _ck(_lib.mgp_batch_set_tuning(self._h, groups, pairs), "batch_set_tuning")
+
+    def tuning(self):
+        g, p = C.c_int(), C.c_int()
+        _ck(_lib.mgp_batch_get_tuning(self._h, _r(g), _r(p)), "batch_get_tuning")
+        return {"groups": g.value, "pairs": p.value}
+
+    def autotune(self, phis, rhss, bcs, homog, tol, maxiters, cache_path=None, key=None, groups=(1, 2, 4),
+                 pairs=(0, 1), numcycles=1, smooth_down=8, smooth_up=8, smooth_bottom=8):
+        """Time the lockstep knobs (every combination of `groups` and `pairs`,
+        one solve each, device-timed) and keep the fastest.  Every combination
+        gives the same bits, so the search changes nothing but speed.  With
+        `cache_path` the choice is stored under `key` in that JSON file and read
+        back instead of searching.  Returns the chosen knobs with the timings."""
+        import json
+        import os
+        import time
+        if cache_path and key and os.path.exists(cache_path):
+            try:
+                hit = json.load(open(cache_path)).get(key)
+            except (OSError, ValueError):
+                hit = None
+            if hit:
+                self.set_tuning(hit["groups"], hit["pairs"])
+                return dict(hit, cached=True)
+        sync = None
+        try:
+            import torch
+            if torch.cuda.is_available():
+                sync = torch.cuda.synchronize
+        except ImportError:
+            pass
+        times = {}
+        for g in groups:
+            for p in pairs:
+                if g > self._nstreams:
+                    continue
+                self.set_tuning(g, p)
+                for x in phis:
+                    x.data[...] = 0.0
+                if sync:
+                    sync()
+                t0 = time.perf_counter()
+                self.vcycle(phis, rhss, bcs, homog, tol, maxiters, numcycles, smooth_down, smooth_up, smooth_bottom)
+                if sync:
+                    sync()
+                times[f"{g},{p}"] = time.perf_counter() - t0
+        best = min(times, key=times.get)
+        g, p = (int(x) for x in best.split(","))
+        self.set_tuning(g, p)
+        out = {"groups": g, "pairs": p, "seconds": times}
+        if cache_path and key:
+            try:
+                cache = json.load(open(cache_path)) if os.path.exists(cache_path) else {}
+            except (OSError, ValueError):
+                cache = {}
+            cache[key] = out
+            with open(cache_path, "w") as f:
+                json.dump(cache, f, indent=1, sort_keys=True)
+        return dict(out, cached=False)
 
     def vcycle(self, phis, rhss, bcs, homog, tol, maxiters, numcycles=1, smooth_down=8, smooth_up=8,
                smooth_bottom=8, zerophi=False):

@@ -38,7 +38,7 @@ void lockstep_free(Lockstep* ls);
 bool lockstep_ok(const std::vector<mgp_solver*>& ss, int numcycles, int nd, int nu);
 int lockstep_vcycle(const std::vector<mgp_solver*>& ss, Lockstep* ls, mgp_array* phi, mgp_array* rhs,
                     const mgp_bdry* bc, int homog, double tol, int maxiters, int nd, int nu, int nb, int zerophi,
-                    mgp_report* reports, cudaStream_t st);
+                    mgp_report* reports, cudaStream_t st, int pairs);
 }  // namespace mgp
 
 using namespace mgp;
@@ -70,8 +70,74 @@ struct mgp_batch {
     int flags = 0;
     std::vector<mgp_solver*> solvers;
     std::vector<cudaStream_t> streams;
-    Lockstep* lockstep = nullptr;   // MGP_FLAG_LOCKSTEP: the phase-by-phase engine's buffers
+    std::vector<Lockstep*> lockstep;   // MGP_FLAG_LOCKSTEP: each group's phase-by-phase engine buffers
+    // lockstep tuning (mgp_batch_set_tuning): groups (0: the default) and two sweeps per launch on small levels
+    int lock_groups = 0;
+    int lock_pairs = 0;
 };
+
+namespace {
+
+// The lockstep path over up to kLockstepGroups groups of problems, each with
+// its own stream, host thread and job tables, so that one group's coarse
+// cycles (a CTA per problem, latency-bound) overlap another group's sweeps.
+// Problems go to groups round-robin in decreasing order of cells, which
+// balances the groups' work; a problem's kernels and their order are those
+// of its group alone, so its bits do not depend on the grouping.
+constexpr int kLockstepGroups = 4;
+
+int batch_lockstep(mgp_batch* b, mgp_array* phi, mgp_array* rhs, const mgp_bdry* bc, int homog, double tol,
+                   int maxiters, int nd, int nu, int nb, int zerophi, mgp_report* reports) {
+    const int n = (int)b->solvers.size();
+    const int want = b->lock_groups > 0 ? b->lock_groups : kLockstepGroups;
+    const int ng = std::max(1, std::min({want, b->nstreams, n}));
+    while ((int)b->lockstep.size() < ng) b->lockstep.push_back(lockstep_new());
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const mgp_solver* sx = b->solvers[x];
+        const mgp_solver* sy = b->solvers[y];
+        return solver_device_bytes(sx) > solver_device_bytes(sy);
+    });
+    std::vector<std::vector<int>> groups(ng);
+    for (int k = 0; k < n; ++k) groups[k % ng].push_back(order[k]);
+    std::vector<int> status(ng, MGP_OK);
+    std::vector<std::string> msg(ng);
+    auto run = [&](int g) {
+        cudaSetDevice(b->dev);
+        const std::vector<int>& ids = groups[g];
+        std::vector<mgp_solver*> ss;
+        std::vector<mgp_array> ph, rh;
+        std::vector<mgp_bdry> bb;
+        std::vector<mgp_report> rp;
+        for (int i : ids) {
+            ss.push_back(b->solvers[i]);
+            ph.push_back(phi[i]);
+            rh.push_back(rhs[i]);
+            bb.push_back(bc[i]);
+            mgp_report r{};
+            if (reports) r.relres = reports[i].relres;
+            rp.push_back(r);
+        }
+        status[g] = lockstep_vcycle(ss, b->lockstep[g], ph.data(), rh.data(), bb.data(), homog, tol, maxiters, nd, nu,
+                                    nb, zerophi, rp.data(), b->streams[g], b->lock_pairs);
+        if (status[g]) msg[g] = mgp_last_error();
+        if (reports)
+            for (size_t k = 0; k < ids.size(); ++k) reports[ids[k]] = rp[k];
+    };
+    std::vector<std::thread> pool;
+    for (int g = 1; g < ng; ++g) pool.emplace_back(run, g);
+    run(0);
+    for (auto& t : pool) t.join();
+    for (int g = 0; g < ng; ++g)
+        if (status[g]) {
+            record_error(status[g], msg[g].c_str());
+            return status[g];
+        }
+    return MGP_OK;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -111,10 +177,25 @@ int mgp_batch_create(int nprob, const mgp_box* valid, const mgp_geo* geo, const 
 
 int mgp_batch_destroy(mgp_batch* b) {
     if (!b) return MGP_OK;
-    if (b->lockstep) lockstep_free(b->lockstep);
+    for (Lockstep* ls : b->lockstep) lockstep_free(ls);
     for (mgp_solver* s : b->solvers) mgp_solver_destroy(s);
     for (cudaStream_t st : b->streams) cudaStreamDestroy(st);
     delete b;
+    return MGP_OK;
+}
+
+int mgp_batch_set_tuning(mgp_batch* b, int groups, int pairs) {
+    if (!b || groups < 0 || groups > b->nstreams || pairs < 0 || pairs > 1)
+        return record_error(MGP_EINVAL, "batch_set_tuning: bad argument");
+    b->lock_groups = groups;
+    b->lock_pairs = pairs;
+    return MGP_OK;
+}
+
+int mgp_batch_get_tuning(const mgp_batch* b, int* groups, int* pairs) {
+    if (!b || !groups || !pairs) return record_error(MGP_EINVAL, "batch_get_tuning: null argument");
+    *groups = b->lock_groups > 0 ? b->lock_groups : std::min({kLockstepGroups, b->nstreams, (int)b->solvers.size()});
+    *pairs = b->lock_pairs;
     return MGP_OK;
 }
 
@@ -129,12 +210,9 @@ int mgp_batch_vcycle(mgp_batch* b, mgp_array* phi, mgp_array* rhs, const mgp_bdr
                      mgp_report* reports) {
     if (!b || !phi || !rhs || !bc) return record_error(MGP_EINVAL, "batch_vcycle: null argument");
     const int n = (int)b->solvers.size();
-    if ((b->flags & MGP_FLAG_LOCKSTEP) && lockstep_ok(b->solvers, numcycles, smooth_down, smooth_up)) {
-        cudaSetDevice(b->dev);
-        if (!b->lockstep) b->lockstep = lockstep_new();
-        return lockstep_vcycle(b->solvers, b->lockstep, phi, rhs, bc, homog, tol, maxiters, smooth_down, smooth_up,
-                               smooth_bottom, zerophi, reports, b->streams[0]);
-    }
+    if ((b->flags & MGP_FLAG_LOCKSTEP) && lockstep_ok(b->solvers, numcycles, smooth_down, smooth_up))
+        return batch_lockstep(b, phi, rhs, bc, homog, tol, maxiters, smooth_down, smooth_up, smooth_bottom, zerophi,
+                              reports);
     std::atomic<int> next{0};
     std::vector<int> status(n, MGP_OK);
     std::vector<std::string> msg(n);

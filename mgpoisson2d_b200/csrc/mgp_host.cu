@@ -1652,6 +1652,13 @@ struct Lockstep {
     int ncap = 0;
     int* status = nullptr;    // the sweeps' status word
     cudaEvent_t e0 = nullptr, e1 = nullptr;
+    // the iteration captured as a CUDA graph for one set of active problems
+    // (replayed while that set does not change; re-captured when the set has
+    // stayed the same for two iterations in a row)
+    cudaStream_t capture = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<int> exec_act;
+    long long exec_launches = 0;
 };
 
 namespace {
@@ -1702,18 +1709,19 @@ bool fill_one_phase(const BCd& b, int do_neum) {   // no side's fill reads anoth
 }
 
 template <class T>
-struct SweepGroups {   // a level's sweep jobs by tile width
-    Table<SweepJobT<T>> w32, w64;
+struct SweepGroups {   // a level's sweep jobs by tile width, and those that sweep twice per launch
+    Table<SweepJobT<T>> w32, w64, w32k2;
 };
 
 template <class T>
 void add_sweep_job(SweepGroups<T>& sg, const SweepTma& t, const DFT<T>& e, const DFT<T>& e2, const DFT<T>& r,
-                   const DFT<T>& invd, const GeoT<T>& g, const BCd& b, int nx, int ny) {
+                   const DFT<T>& invd, const GeoT<T>& g, const BCd& b, int nx, int ny, bool pairs) {
     SweepJobT<T> J;
     std::memset(&J, 0, sizeof J);
     const bool a_is_e = (const void*)e.p == t.pa;
-    J.m[0] = a_is_e ? t.ma : t.mb;
-    J.m[1] = a_is_e ? t.mb : t.ma;
+    const bool k2 = pairs && t.ok2;   // the level's two-sweep descriptors exist
+    J.m[0] = k2 ? (a_is_e ? t.ma2 : t.mb2) : (a_is_e ? t.ma : t.mb);
+    J.m[1] = k2 ? (a_is_e ? t.mb2 : t.ma2) : (a_is_e ? t.mb : t.ma);
     J.buf[0] = e;
     J.buf[1] = e2;
     J.rhs = r;
@@ -1726,7 +1734,7 @@ void add_sweep_job(SweepGroups<T>& sg, const SweepTma& t, const DFT<T>& e, const
     J.gy = cdiv(ny, 32);
     J.part = make_int4(nx / J.gx, nx % J.gx, ny / J.gy, ny % J.gy);
     J.s0 = 0;
-    (t.tx == 64 ? sg.w64 : sg.w32).push(J, J.gx * J.gy);
+    (k2 ? sg.w32k2 : t.tx == 64 ? sg.w64 : sg.w32).push(J, J.gx * J.gy);
 }
 
 // Everything one V-cycle iteration launches, for one set of active problems.
@@ -1781,7 +1789,7 @@ CoarseArgs coarse_args_of(mgp_solver* s, int d, int nd, int nu, int nb) {
 }
 
 void build_plan(Plan& P, const std::vector<mgp_solver*>& ss, const std::vector<int>& act, const std::vector<BCd>& ubc,
-                int homog, int nd, int nu, int nb) {
+                int homog, int nd, int nu, int nb, bool pairs) {
     P = Plan();
     for (int p : act) P.D = std::max(P.D, ss[p]->dc);
     P.mix = !act.empty() && mixed(ss[act[0]]);
@@ -1806,7 +1814,7 @@ void build_plan(Plan& P, const std::vector<mgp_solver*>& ss, const std::vector<i
             const int cbx = cdiv(C.nx, 32), cby = cdiv(C.ny, 8);
             if (mx) {
                 auto& L = s->lv32[d];
-                add_sweep_job(P.sw32[d], s->tma32[d], L.e, L.e2, L.r, L.invd, L.g, F.bc, L.nx, L.ny);
+                add_sweep_job(P.sw32[d], s->tma32[d], L.e, L.e2, L.r, L.invd, L.g, F.bc, L.nx, L.ny, pairs);
                 P.fpre32[d].push(FillJob<float>{L.e, L.g, F.bc, L.nx, L.ny, 1, 0}, fblk);
                 if (next_grid) {
                     auto& N = s->lv32[d + 1];
@@ -1823,7 +1831,7 @@ void build_plan(Plan& P, const std::vector<mgp_solver*>& ss, const std::vector<i
                     P.pro3264[d].push(ProlongJob<float, double>{L.e, C.e, C.nx, C.ny, rx, ry, cbx}, cbx * cby);
                 }
             } else {
-                add_sweep_job(P.sw64[d], s->tma[d], F.e, F.e2, F.r, F.invd, F.g, F.bc, F.nx, F.ny);
+                add_sweep_job(P.sw64[d], s->tma[d], F.e, F.e2, F.r, F.invd, F.g, F.bc, F.nx, F.ny, pairs);
                 P.fpre64[d].push(FillJob<double>{F.e, F.g, F.bc, F.nx, F.ny, 1, 0}, fblk);
                 P.res64[d].push(ResidJob<double, double>{F.e, F.r, F.g, F.bc, C.r, C.e, C.invd, F.nx, F.ny, C.nx, C.ny,
                                                          rx, ry, gbx},
@@ -1862,8 +1870,8 @@ void build_plan(Plan& P, const std::vector<mgp_solver*>& ss, const std::vector<i
 
 template <class F>
 void for_tables(Plan& P, F f) {
-    for (auto& g : P.sw64) { f(g.w32); f(g.w64); }
-    for (auto& g : P.sw32) { f(g.w32); f(g.w64); }
+    for (auto& g : P.sw64) { f(g.w32); f(g.w64); f(g.w32k2); }
+    for (auto& g : P.sw32) { f(g.w32); f(g.w64); f(g.w32k2); }
     for (auto& t : P.fpre64) f(t);
     for (auto& t : P.fpre32) f(t);
     for (auto& t : P.fpost64) f(t);
@@ -1913,12 +1921,17 @@ int upload_plan(Plan& P, Lockstep* ls, cudaStream_t st) {
     return MGP_OK;
 }
 
+// n sweeps of every job of a level (n even; with two-sweep jobs a multiple of
+// 4, so every job's correction ends in its first buffer).
 template <class T>
 int sweeps(SweepGroups<T>& g, int n, Lockstep* ls, cudaStream_t st) {
     for (int k = 0; k < n; ++k) {
         CK(launch_sweep9_jobs<T>(g.w32.dj, g.w32.dp, g.w32.n(), g.w32.blocks(), 32, 1, k & 1, ls->status, st));
         CK(launch_sweep9_jobs<T>(g.w64.dj, g.w64.dp, g.w64.n(), g.w64.blocks(), 64, 1, k & 1, ls->status, st));
     }
+    for (int k = 0; k < n / 2; ++k)
+        CK(launch_sweep9_jobs<T>(g.w32k2.dj, g.w32k2.dp, g.w32k2.n(), g.w32k2.blocks(), 32, 2, k & 1, ls->status,
+                                 st));
     return MGP_OK;
 }
 
@@ -1963,6 +1976,8 @@ Lockstep* lockstep_new() { return new Lockstep(); }
 void lockstep_free(Lockstep* ls) {
     if (!ls) return;
     cudaDeviceSynchronize();
+    if (ls->exec) cudaGraphExecDestroy(ls->exec);
+    if (ls->capture) cudaStreamDestroy(ls->capture);
     dfree(ls->dev, nullptr);
     dfree(ls->part, nullptr);
     dfree(ls->norms, nullptr);
@@ -2002,8 +2017,9 @@ bool lockstep_ok(const std::vector<mgp_solver*>& ss, int numcycles, int nd, int 
 
 int lockstep_vcycle(const std::vector<mgp_solver*>& ss, Lockstep* ls, mgp_array* phi, mgp_array* rhs,
                     const mgp_bdry* bc, int homog, double tol, int maxiters, int nd, int nu, int nb, int zerophi,
-                    mgp_report* reports, cudaStream_t st) {
+                    mgp_report* reports, cudaStream_t st, int pairs_wanted) {
     const int n = (int)ss.size();
+    const bool pairs = pairs_wanted && nd % 4 == 0 && nu % 4 == 0;
     if (maxiters < 0 || nb < 0) return set_err(MGP_EINVAL, "negative count");
     if (ls->ncap < n) {
         dfree(ls->norms, st);
@@ -2051,7 +2067,7 @@ int lockstep_vcycle(const std::vector<mgp_solver*>& ss, Lockstep* ls, mgp_array*
     for (int p = 0; p < n; ++p) act[p] = p;
     Plan P;
     // r(0) = rhs - L[phi] with the caller's BCs (MG:579) and its norm
-    build_plan(P, ss, act, ubc, homog, nd, nu, nb);
+    build_plan(P, ss, act, ubc, homog, nd, nu, nb, pairs);
     RC(upload_plan(P, ls, st));
     CK(launch_fill_jobs(P.fill_phi.dj, P.fill_phi.dp, P.fill_phi.n(), P.fill_phi.blocks(), P.fill_phi_ph, st));
     CK(launch_norm_jobs(P.norm.dj, P.norm.dp, P.norm.n(), P.norm.blocks(), ls->part, ls->vols, ls->norms, st));
@@ -2067,10 +2083,51 @@ int lockstep_vcycle(const std::vector<mgp_solver*>& ss, Lockstep* ls, mgp_array*
         else if (hist[p][0] > tol && maxiters > 0) next.push_back(p);
     }
     act.swap(next);
+    std::vector<int> prev;
+    if (ls->exec) {   // a graph of an earlier call holds that call's tables and BC values
+        cudaGraphExecDestroy(ls->exec);
+        ls->exec = nullptr;
+        ls->exec_act.clear();
+    }
     for (int iter = 1; iter <= maxiters && !act.empty(); ++iter) {
-        build_plan(P, ss, act, ubc, homog, nd, nu, nb);
-        RC(upload_plan(P, ls, st));
-        RC(lockstep_iteration(P, ls, nd, nu, st));
+        if (ls->exec && act == ls->exec_act) {   // the same problems as the captured iteration
+            CK(cudaGraphLaunch(ls->exec, st));
+            count_launch((int)ls->exec_launches);
+        } else {
+            if (ls->exec) {
+                cudaGraphExecDestroy(ls->exec);
+                ls->exec = nullptr;
+                ls->exec_act.clear();
+            }
+            build_plan(P, ss, act, ubc, homog, nd, nu, nb, pairs);
+            RC(upload_plan(P, ls, st));
+            if (act == prev) {   // the set held for an iteration: capture it for the ones to come
+                if (!ls->capture) CK(cudaStreamCreateWithFlags(&ls->capture, cudaStreamNonBlocking));
+                const long long l0 = launch_count();
+                CK(cudaStreamBeginCapture(ls->capture, cudaStreamCaptureModeThreadLocal));
+                const int rc = lockstep_iteration(P, ls, nd, nu, ls->capture);
+                cudaGraph_t graph = nullptr;
+                const cudaError_t ce = cudaStreamEndCapture(ls->capture, &graph);
+                const long long nl = launch_count() - l0;
+                count_launch((int)-nl);
+                cudaGraphExec_t ex = nullptr;
+                if (!rc && ce == cudaSuccess && cudaGraphInstantiate(&ex, graph, 0) == cudaSuccess) {
+                    ls->exec = ex;
+                    ls->exec_act = act;
+                    ls->exec_launches = nl;
+                }
+                if (graph) cudaGraphDestroy(graph);
+                cudaGetLastError();
+                if (rc) return rc;
+            }
+            if (ls->exec) {
+                CK(cudaGraphLaunch(ls->exec, st));
+                count_launch((int)ls->exec_launches);
+            } else {
+                RC(lockstep_iteration(P, ls, nd, nu, st));
+            }
+        }
+        prev = act;
         CK(cudaMemcpyAsync(ls->h_norms, ls->norms, sizeof(double) * act.size(), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         next.clear();

@@ -115,3 +115,42 @@ def test_lockstep_falls_back_for_krylov_and_odd_counts(M, probs):
             phi = BoxData(v, 1, 1)
             s.vcycle(phi, rhs, bc, True, 1e-10, 60, 1, 7, 7, 7)
         assert np.array_equal(phis[k].interior(), phi.interior())
+
+
+def _solve_with(M, probs, flags, groups, pairs):
+    phis = [BoxData(p[0], 1, 1) for p in probs]
+    with M.Batch([(p[0], p[1], p[3]) for p in probs], M.KIND_MG, flags | M.FLAG_LOCKSTEP, nstreams=4) as b:
+        b.set_tuning(groups, pairs)
+        assert b.tuning() == {"groups": groups, "pairs": pairs}
+        reps = b.vcycle(phis, [p[2] for p in probs], [p[3] for p in probs], True, 1e-10, 60)
+    return [r.iterations for r in reps], [p.interior().copy() for p in phis]
+
+
+def test_lockstep_tuning_changes_no_bits(M, probs):
+    """Concurrent groups and two sweeps per launch change speed only: the
+    same V-cycle counts and the same bits for every setting."""
+    flags = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_MIXED | M.FLAG_DIRECT_COARSE
+    its0, sols0 = _solve_with(M, probs, flags, 1, 0)
+    for groups, pairs in ((2, 0), (4, 1), (1, 1), (3, 1)):
+        its, sols = _solve_with(M, probs, flags, groups, pairs)
+        assert its == its0
+        for a, b in zip(sols, sols0):
+            assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+def test_lockstep_autotune_keeps_fastest_and_caches(M, probs, tmp_path):
+    import json
+    flags = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_MIXED
+    cache = str(tmp_path / "tune.json")
+    sub = probs[:6]
+    phis = [BoxData(p[0], 1, 1) for p in sub]
+    args = ([p[2] for p in sub], [p[3] for p in sub], True, 1e-10, 60)
+    with M.Batch([(p[0], p[1], p[3]) for p in sub], M.KIND_MG, flags | M.FLAG_LOCKSTEP, nstreams=4) as b:
+        got = b.autotune(phis, *args, cache_path=cache, key="six")
+        assert not got["cached"] and len(got["seconds"]) == 6
+        best = min(got["seconds"], key=got["seconds"].get)
+        assert best == f"{got['groups']},{got['pairs']}" and b.tuning() == {"groups": got["groups"], "pairs": got["pairs"]}
+    assert json.load(open(cache))["six"]["groups"] == got["groups"]
+    with M.Batch([(p[0], p[1], p[3]) for p in sub], M.KIND_MG, flags | M.FLAG_LOCKSTEP, nstreams=4) as b:
+        again = b.autotune(phis, *args, cache_path=cache, key="six")
+        assert again["cached"] and b.tuning() == {"groups": got["groups"], "pairs": got["pairs"]}
