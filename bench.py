@@ -21,16 +21,22 @@ solver in FP64 ("fp64_same_solver") and of the plain FP64 V-cycle iteration
 torchrun every rank solves its own copy (replicas; the solve does not shard)
 and rank 0 prints one JSON line.
 
-At N=1 the line also carries two legs on many independent problems (the
-batched workload: sides log-uniform in [64,1024]): "batched" (all problems as
-one mgp_batch on 16 streams vs one after another) and "served" (Poisson
-arrivals into an mgp_server with resident hierarchies; p50/p99 latency), both
-with BiCGStab(V-cycle), whose work vectors are 8 per problem where GMRES(64)
-keeps 129, and "precision_study": mixed precision against FP64 and against the exact solution
-of a manufactured problem on the skewed, stretched grid at 512..4096, for the
-BiCGStab(V-cycle) solve and the deferred-correction solve, with the observed
-order of the discretisation error.  --serve-sweep adds "served_sweep" (the
-served workload over arrival rates 10..3000/s, sides 32..2048; minutes).
+At N=1 the line also carries:
+  * "batched" (512 independent problems, sides
+    log-uniform in [64,1024]): the lockstep batch (MGP_FLAG_LOCKSTEP, every
+    V-cycle phase of all unconverged problems in one launch per group, knobs
+    chosen by the autotuner) in mixed precision and in FP64, each against
+    the same problems one at a time, and the per-problem concurrent
+    BiCGStab(V-cycle) path; "batched_headline" is the metric's own
+    comparison, mixed against plain FP64 with the served p50/p99;
+  * "served" (config 5: Poisson arrivals of solves drawn from 64 problems
+    with sides log-uniform in [32,2048] rounded to 8, hierarchies resident,
+    tolerance 1e-8 or 1e-10) at 10, 30 and 100 requests/s, stopping once p99
+    diverges; --serve-sweep extends the rates to 3000/s;
+  * "precision_study": mixed precision against FP64 and against the exact
+    solution of a manufactured problem on the skewed, stretched grid at
+    512..4096, for the BiCGStab(V-cycle) solve and the deferred-correction
+    solve, with the observed order of the discretisation error.
 
 --impl reference times the CPU restatement of the reference algorithm (the
 reference is Fortran and no Fortran compiler exists on these hosts) on all
@@ -86,7 +92,7 @@ def parse():
     p.add_argument("--streams", type=int, default=16, help="concurrent solves in the batched and served legs")
     p.add_argument("--no-study", action="store_true", help="skip the precision/convergence study leg")
     p.add_argument("--serve-sweep", action="store_true",
-                   help="add the served workload swept over arrival rates (several minutes)")
+                   help="extend the served leg's arrival rates to 3000/s (several minutes)")
     p.add_argument("--study-sizes", default="512,1024,2048,4096",
                    help="grid sides of the precision/convergence study")
     return p.parse_args()
@@ -299,26 +305,42 @@ def run_reference(args):
 # --------------------------------------------------------------------------- #
 # Batched and served legs (many independent problems)
 # --------------------------------------------------------------------------- #
-def batched_leg(M, args, flags_list):
+def batched_leg(M, args):
     """`args.batch` problems of the batched workload (sides log-uniform in
-    [64, 1024], rounded to 16; random stretch and skew; Dirichlet), solved to
-    1e-10 one after another on one stream and as one batch on `args.streams`
-    streams, for each flag set.  Inputs and hierarchies resident."""
+    [64, 1024], rounded to 16; random stretch and skew; Dirichlet), inputs and
+    hierarchies resident, solved to 1e-10:
+      * lockstep (MGP_FLAG_LOCKSTEP: every V-cycle phase of all unconverged
+        problems in one launch per group; groups and two-sweep launches chosen
+        by Batch.autotune, which changes no bit) in mixed precision and in
+        FP64, the exact bottom on the coarse-cycle level;
+      * the same problems one at a time (the same solver, one stream);
+      * the per-problem concurrent path (BiCGStab(V-cycle), `args.streams`
+        streams), the batched form without lockstep.
+    Device-synchronised wall time around each batch call."""
     import numpy as np
     import torch
     from mgpoisson2d_b200 import workloads as W
     from mgpoisson2d_b200.types import BoxData
     probs = [W.batch_problem_device(i) for i in range(args.batch)]   # geometry and rhs made on the device
     rhs_d = [p[2] for p in probs]
+    bcs = [p[3] for p in probs]
     cells = sum(p[0].nx * p[0].ny for p in probs)
+    base = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_DIRECT_COARSE | M.FLAG_DIRECT_LARGE
+    legs = [("mixed", base | M.FLAG_LOCKSTEP | M.FLAG_MIXED, True),
+            ("fp64", base | M.FLAG_LOCKSTEP, True),
+            ("concurrent_bicgstab_mixed", base | M.FLAG_KRYLOV | M.FLAG_MIXED, False)]
     out = {"problems": args.batch, "cells": cells, "streams": args.streams,
            "workload": "sides log-uniform [64,1024] rounded to 16, stretch U[1,1.08] in a min(64,ny/4)-cell layer, "
-                       "skew U[0,25] deg, 16-mode rhs, Dirichlet; seeds 4e6+i; geometry and rhs generated on the device"}
-    for name, fl in flags_list:
+                       "skew U[0,25] deg, 16-mode rhs, Dirichlet; seeds 4e6+i; geometry and rhs generated on the device",
+           "timing": "device-synchronised wall time around one batch call, after an autotuning / warm-up call"}
+    for name, fl, lock in legs:
+        phis = [BoxData.device_zeros(p[0], 1, 1) for p in probs]
         with M.Batch([(v, g, bc) for v, g, _, bc in probs], M.KIND_MG, fl, nstreams=args.streams) as b:
-            phis = [BoxData(p[0], 1, 1).to_device() for p in probs]
-            bcs = [p[3] for p in probs]
-            b.vcycle(phis, rhs_d, bcs, True, TOL, MAXITERS)   # warm-up (graph capture)
+            tune = None
+            if lock:
+                tune = b.autotune(phis, rhs_d, bcs, True, TOL, MAXITERS, groups=(1, 2, 4, 8, 16))
+            else:
+                b.vcycle(phis, rhs_d, bcs, True, TOL, MAXITERS)   # warm-up (graph capture)
             for p in phis:
                 p.data.zero_()
             torch.cuda.synchronize()
@@ -327,23 +349,32 @@ def batched_leg(M, args, flags_list):
             torch.cuda.synchronize()
             tb = time.perf_counter() - t0
         assert all(r.final_relres <= TOL for r in reps), "batched solve did not converge"
-        # the same problems one at a time on one stream
-        solvers = [M.Solver(v, g, bc, M.KIND_MG, fl) for v, g, _, bc in probs]
-        for s, p, f, (v, g, _, bc) in zip(solvers, phis, rhs_d, probs):
-            p.data.zero_()
-            s.vcycle(p, f, bc, True, TOL, MAXITERS)   # warm-up
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for s, p, f, (v, g, _, bc) in zip(solvers, phis, rhs_d, probs):
-            p.data.zero_()
-            s.vcycle(p, f, bc, True, TOL, MAXITERS)
-        torch.cuda.synchronize()
-        ts = time.perf_counter() - t0
-        for s in solvers:
-            s.close()
-        out[name] = {"batched_solves_per_s": args.batch / tb, "sequential_solves_per_s": args.batch / ts,
-                     "speedup": ts / tb, "vcycles_mean": float(np.mean([r.iterations for r in reps]))}
-    return out, probs, rhs_d
+        row = {"solves_per_s": args.batch / tb, "seconds": tb,
+               "vcycles_mean": float(np.mean([r.iterations for r in reps])),
+               "vcycles_max": int(max(r.iterations for r in reps)),
+               "solver": "stationary V-cycle, lockstep" if lock else "BiCGStab(V-cycle), a stream per problem"}
+        if tune:
+            row["tuning"] = {"groups": tune["groups"], "two_sweep_launches": tune["pairs"],
+                             "searched_s": {k: round(v, 4) for k, v in tune["seconds"].items()}}
+        if lock:   # the same problems one at a time, same solver
+            solvers = [M.Solver(v, g, bc, M.KIND_MG, fl) for v, g, _, bc in probs]
+            for s_, p, f, (v, g, _, bc) in zip(solvers, phis, rhs_d, probs):
+                p.data.zero_()
+                s_.vcycle(p, f, bc, True, TOL, MAXITERS)   # warm-up
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for s_, p, f, (v, g, _, bc) in zip(solvers, phis, rhs_d, probs):
+                p.data.zero_()
+                s_.vcycle(p, f, bc, True, TOL, MAXITERS)
+            torch.cuda.synchronize()
+            ts = time.perf_counter() - t0
+            for s_ in solvers:
+                s_.close()
+            row["sequential_solves_per_s"] = args.batch / ts
+        out[name] = row
+    out["mixed_over_fp64"] = out["mixed"]["solves_per_s"] / out["fp64"]["solves_per_s"]
+    out["lockstep_over_concurrent"] = out["mixed"]["solves_per_s"] / out["concurrent_bicgstab_mixed"]["solves_per_s"]
+    return out
 
 
 def batched_multi(M, args, flags, rank, world):
@@ -386,54 +417,7 @@ def batched_multi(M, args, flags, rank, world):
             "timing": "device events around each rank's batch, max over ranks"}
 
 
-def served_leg(M, args, probs, rhs_d, flags_list, nreq=240, seed=5):
-    """Poisson arrivals of solves drawn from the batched workload's problems
-    (hierarchies resident per problem), tolerance 1e-8 or 1e-10 with
-    probability 1/2 each; `args.streams` slots.  Offered load: 0.5x and 2x the
-    batched throughput.  Reports p50/p99 latency (submit to done) and the
-    achieved solves/s."""
-    import numpy as np
-    from mgpoisson2d_b200.types import BoxData
-    out = {"requests": nreq, "slots": args.streams, "tolerances": [1e-8, 1e-10]}
-    for name, fl, cap in flags_list:
-        res = {}
-        for load in (0.5, 2.0):
-            rng = np.random.default_rng(seed)
-            rate = load * cap
-            gaps = rng.exponential(1.0 / rate, nreq)
-            which = rng.integers(0, len(probs), nreq)
-            tols = np.where(rng.random(nreq) < 0.5, 1e-8, 1e-10)
-            with M.Server(nworkers=args.streams, flags=fl) as srv:
-                # warm the resident hierarchies (one request per problem)
-                warm = [srv.submit(v, g, bc, BoxData(v, 1, 1).to_device(), rhs_d[k], True, 1e-10, MAXITERS,
-                                   key=k + 1) for k, (v, g, _, bc) in enumerate(probs)]
-                for t in warm:
-                    srv.wait(t)
-                outs = [BoxData(probs[k][0], 1, 1).to_device() for k in which]
-                tickets = []
-                t0 = time.perf_counter()
-                t_next = t0
-                for n in range(nreq):
-                    t_next += gaps[n]
-                    while time.perf_counter() < t_next:
-                        time.sleep(max(0.0, min(0.001, t_next - time.perf_counter())))
-                    v, g, _, bc = probs[which[n]]
-                    tickets.append(srv.submit(v, g, bc, outs[n], rhs_d[which[n]], True, float(tols[n]), MAXITERS,
-                                              key=int(which[n]) + 1))
-                lats = []
-                for t in tickets:
-                    rep, lat, qt = srv.wait(t)
-                    lats.append(lat)
-                span = time.perf_counter() - t0
-            lats = np.sort(np.array(lats)) * 1e3
-            res[f"offered_{load}x"] = {"offered_per_s": rate, "solves_per_s": nreq / span,
-                                       "p50_ms": float(lats[len(lats) // 2]),
-                                       "p99_ms": float(lats[min(len(lats) - 1, int(math.ceil(0.99 * len(lats))) - 1)])}
-        out[name] = res
-    return out
-
-
-def served_sweep(M, args, flags_list, pool=64, seed=5, rates=(10, 30, 100, 300, 1000, 3000)):
+def served_leg(M, args, flags_list, pool=64, seed=5, rates=(10, 30, 100)):
     """The served workload swept over arrival rates: a pool of `pool` problems
     (sides log-uniform in [32, 2048] rounded to a multiple of 8, maps as the
     batched workload, seed 5), requests drawn from the pool with Poisson
@@ -792,15 +776,19 @@ def main():
         if rank == 0:
             line["batched"] = batched_n
     if rank == 0 and world == 1 and not args.no_batch:
-        kry = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV | M.FLAG_DIRECT_COARSE
-        fls = [("mixed", kry | M.FLAG_MIXED), ("fp64", kry)]
-        batched, probs, rhs_b = batched_leg(M, args, fls)
+        batched = batched_leg(M, args)
         line["batched"] = batched
-        line["served"] = served_leg(M, args, probs, rhs_b,
-                                    [(n, f, batched[n]["batched_solves_per_s"]) for n, f in fls])
-    if rank == 0 and world == 1 and args.serve_sweep:
         kry = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV | M.FLAG_DIRECT_COARSE
-        line["served_sweep"] = served_sweep(M, args, [("mixed", kry | M.FLAG_MIXED), ("fp64", kry)])
+        rates = (10, 30, 100, 300, 1000, 3000) if args.serve_sweep else (10, 30, 100)
+        served = served_leg(M, args, [("mixed", kry | M.FLAG_MIXED), ("fp64", kry)], rates=rates)
+        line["served"] = served
+        # the metric's own comparison: mixed against plain FP64, batched and served
+        line["batched_headline"] = {
+            "mixed_solves_per_s": batched["mixed"]["solves_per_s"], "fp64_solves_per_s": batched["fp64"]["solves_per_s"],
+            "mixed_over_fp64": batched["mixed_over_fp64"], "problems": batched["problems"],
+            "served_mixed_p50_ms": served["mixed"][0]["p50_ms"], "served_mixed_p99_ms": served["mixed"][0]["p99_ms"],
+            "served_fp64_p50_ms": served["fp64"][0]["p50_ms"], "served_fp64_p99_ms": served["fp64"][0]["p99_ms"],
+            "served_rate_per_s": served["mixed"][0]["offered_per_s"]}
     if rank == 0 and world == 1 and not args.no_study:
         line["precision_study"] = precision_study(M, [int(x) for x in args.study_sizes.split(",") if x])
     if rank == 0 and world == 1 and not args.no_cpu:
