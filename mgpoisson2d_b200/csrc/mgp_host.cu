@@ -1107,14 +1107,14 @@ int vcycle_run(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb, bool
     CK(coarse_kernels_init());
     if (!s->cap) CK(cudaStreamCreateWithFlags(&s->cap, cudaStreamNonBlocking));
     const cudaStream_t saved = s->stream;
-    const long long l0 = launch_count();
+    const long long l0 = thread_launch_count();   // other threads' solvers may be launching meanwhile
     s->stream = s->cap;
     CK(cudaStreamBeginCapture(s->cap, cudaStreamCaptureModeThreadLocal));
     const int rc = run();
     cudaGraph_t graph = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(s->cap, &graph);
     s->stream = saved;
-    mgp_solver::VGraph g{d, mix, numcycles, nd, nu, nb, cur, state(), nullptr, launch_count() - l0};
+    mgp_solver::VGraph g{d, mix, numcycles, nd, nu, nb, cur, state(), nullptr, thread_launch_count() - l0};
     set_state(cur);   // the capture ran nothing: put the buffers back as they were
     count_launch((int)-g.launches);
     if (rc || ce != cudaSuccess) {
@@ -2103,12 +2103,12 @@ int lockstep_vcycle(const std::vector<mgp_solver*>& ss, Lockstep* ls, mgp_array*
             RC(upload_plan(P, ls, st));
             if (act == prev) {   // the set held for an iteration: capture it for the ones to come
                 if (!ls->capture) CK(cudaStreamCreateWithFlags(&ls->capture, cudaStreamNonBlocking));
-                const long long l0 = launch_count();
+                const long long l0 = thread_launch_count();
                 CK(cudaStreamBeginCapture(ls->capture, cudaStreamCaptureModeThreadLocal));
                 const int rc = lockstep_iteration(P, ls, nd, nu, ls->capture);
                 cudaGraph_t graph = nullptr;
                 const cudaError_t ce = cudaStreamEndCapture(ls->capture, &graph);
-                const long long nl = launch_count() - l0;
+                const long long nl = thread_launch_count() - l0;
                 count_launch((int)-nl);
                 cudaGraphExec_t ex = nullptr;
                 if (!rc && ce == cudaSuccess && cudaGraphInstantiate(&ex, graph, 0) == cudaSuccess) {

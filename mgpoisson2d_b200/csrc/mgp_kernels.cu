@@ -19,8 +19,13 @@
 namespace mgp {
 
 static std::atomic<long long> g_launches{0};
+thread_local long long t_launches = 0;   // this thread's launches (a capture counts its own)
 long long launch_count() { return g_launches.load(); }
-void count_launch(int n) { g_launches += n; }
+long long thread_launch_count() { return t_launches; }
+void count_launch(int n) {
+    g_launches += n;
+    t_launches += n;
+}
 
 static inline dim3 cells_grid(int nx, int ny, dim3 blk) {
     return dim3((unsigned)((nx + blk.x - 1) / blk.x), (unsigned)((ny + blk.y - 1) / blk.y));

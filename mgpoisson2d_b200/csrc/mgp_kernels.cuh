@@ -88,6 +88,7 @@ struct BicgArgs {
 constexpr int kCoarseThreads = 256;
 
 long long launch_count();
+long long thread_launch_count();   // launches the calling thread made (count_launch on it)
 void count_launch(int n = 1);
 
 cudaError_t launch_fill(const DF& p, const Geo& g, const BCd& b, int homog, int do_neum, int nx, int ny,

@@ -29,7 +29,13 @@ def main():
                         "(MGP_FLAG_DIRECT_LARGE)")
     p.add_argument("--workload", default="wavy", choices=["wavy", "skew"])
     p.add_argument("--time-smoother", action="store_true", help="also report the finest level's time per sweep")
+    p.add_argument("--batch", type=int, default=0,
+                   help="instead: a lockstep batch of this many problems of the batched workload "
+                        "(MGP_FLAG_LOCKSTEP, exact bottoms; --mixed for FP32 grid levels)")
+    p.add_argument("--groups", type=int, default=8, help="with --batch: lockstep groups")
     a = p.parse_args()
+    if a.batch:
+        return run_batch(a)
 
     import torch
 
@@ -72,6 +78,36 @@ def main():
         print(f"finest-level sweep {rep.smooth0_seconds / max(rep.smooth0_sweeps, 1) * 1e6:.2f} us "
               f"({rep.smooth0_sweeps} sweeps)")
     s.close()
+
+
+def run_batch(a):
+    """`warmup` + 1 lockstep solves of the first `batch` problems of the
+    batched workload (sides log-uniform in [64, 1024]) to 1e-10."""
+    import torch
+
+    import mgpoisson2d_b200.api as M
+    from mgpoisson2d_b200 import workloads as W
+    from mgpoisson2d_b200.types import BoxData
+
+    torch.cuda.set_device(0)
+    probs = [W.batch_problem_device(i) for i in range(a.batch)]
+    flags = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_LOCKSTEP | M.FLAG_DIRECT_COARSE | M.FLAG_DIRECT_LARGE
+    flags |= M.FLAG_MIXED if a.mixed else 0
+    with M.Batch([(p[0], p[1], p[3]) for p in probs], M.KIND_MG, flags, nstreams=max(1, a.groups)) as b:
+        b.set_tuning(a.groups, 1)
+        phis = [BoxData.device_zeros(p[0], 1, 1) for p in probs]
+        for k in range(a.warmup + 1):
+            for ph in phis:
+                ph.data.zero_()
+            torch.cuda.synchronize()
+            l0 = M.kernel_launch_count()
+            t0 = time.perf_counter()
+            reps = b.vcycle(phis, [p[2] for p in probs], [p[3] for p in probs], True, 1e-10, 200)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+    print(f"batch={a.batch} wall {dt * 1e3:.1f} ms ({a.batch / dt:.1f} solves/s), "
+          f"V-cycles mean {sum(r.iterations for r in reps) / len(reps):.2f} max {max(r.iterations for r in reps)}, "
+          f"{M.kernel_launch_count() - l0} launches")
 
 
 if __name__ == "__main__":
