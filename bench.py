@@ -9,12 +9,12 @@ One step = one full solve (until |r|/|r0| <= 1e-10) of that problem.  The
 default solver is the V-cycle accelerated by restarted GMRES(64)
 (MGP_FLAG_GMRES: one V-cycle per preconditioner application) with the
 V-cycle's grid levels in FP32 inside the FP64 outer iteration
-(MGP_FLAG_MIXED) and its bottom solved exactly on the 8 x 8 level
-(MGP_FLAG_DIRECT_COARSE); --solver krylov selects BiCGStab(V-cycle)
-(MGP_FLAG_KRYLOV), --coarse large an exact bottom on the 32 x 32 level
-(MGP_FLAG_DIRECT_LARGE: its inverse built on the device when the solver is
-created), and --solver vcycle, --precision fp64 and --coarse reference the
-reference's stationary iteration, plain FP64 and the reference's bottom
+(MGP_FLAG_MIXED) and its bottom solved exactly on the 32 x 32 level
+(MGP_FLAG_DIRECT_COARSE | MGP_FLAG_DIRECT_LARGE: the inverse built on the
+device when the solver is created); --solver krylov selects
+BiCGStab(V-cycle) (MGP_FLAG_KRYLOV), --coarse direct an exact bottom on the
+8 x 8 level, and --solver vcycle, --precision fp64 and --coarse reference
+the reference's stationary iteration, plain FP64 and the reference's bottom
 solver.  The line also carries one timed solve of the same
 solver in FP64 ("fp64_same_solver") and of the plain FP64 V-cycle iteration
 ("plain_vcycle"), and the headline solution's error against both.  Under
@@ -36,7 +36,10 @@ At N=1 the line also carries:
   * "precision_study": mixed precision against FP64 and against the exact
     solution of a manufactured problem on the skewed, stretched grid at
     512..4096, for the BiCGStab(V-cycle) solve and the deferred-correction
-    solve, with the observed order of the discretisation error.
+    solve, with the observed order of the discretisation error, and the same
+    solvers with BF16 values on the levels below the finest;
+  * "config1": the 128^2 identity-map Dirichlet problem (V-cycles, ms per
+    solve, error) for the FP64 V-cycle, the headline solver and the oracle.
 
 --impl reference times the CPU restatement of the reference algorithm (the
 reference is Fortran and no Fortran compiler exists on these hosts) on all
@@ -259,6 +262,62 @@ def cpu_baseline_1core(n, vcycles, runs=3):
             "vcycles_per_solve": vsolve, "s_per_vcycle": (sec - ts) / max(vc, 1)}
 
 
+def _cpu_config1(runs):
+    """Full oracle solves of the 128^2 identity-map Dirichlet problem on one
+    core (lexicographic Gauss-Seidel, FP64): median seconds and V-cycles."""
+    from mgpoisson2d_b200 import workloads as W
+    from mgpoisson2d_b200.types import BoxData
+    O = _cpu_oracle()
+    v, geo, rhs, bc, u = W.identity_dirichlet(128)
+    secs = []
+    for _ in range(runs):
+        phi = BoxData(v, 1, 1)
+        t0 = time.perf_counter()
+        rep = O.vcycle(phi, rhs, geo, bc, True, TOL, 100, smooth_down=NU[0], smooth_up=NU[1], smooth_bottom=NU[2],
+                       gs_order=0)
+        secs.append(time.perf_counter() - t0)
+    return sorted(secs)[len(secs) // 2], rep.iterations, float(abs(phi.interior() - u).max())
+
+
+def config1_leg(M, cpu, runs=20):
+    """The 128^2 identity-map Dirichlet problem (u = sin 2 pi x sin 3 pi y plus
+    1e-3 noise in the rhs): V-cycles, ms per solve and the error against u for
+    the reference's FP64 V-cycle and the headline solver, on the device (median
+    of `runs` solves with device arrays) and, with `cpu`, on the oracle."""
+    import torch
+    from mgpoisson2d_b200 import workloads as W
+    from mgpoisson2d_b200.types import BoxData
+    v, geo, rhs, bc, u = W.identity_dirichlet(128)
+    rhs_d = rhs.to_device()
+    stream = torch.cuda.current_stream()
+    base = M.FLAG_DIRICHLET_COUPLED_DIAG
+    out = {"workload": "identity_dirichlet_128", "tol": TOL, "nu": list(NU), "timing": f"median of {runs} solves"}
+    for name, fl in (("fp64_vcycle", base),
+                     ("mixed_gmres", base | M.FLAG_GMRES | M.FLAG_MIXED | M.FLAG_DIRECT_COARSE | M.FLAG_DIRECT_LARGE)):
+        with M.Solver(v, geo, bc, M.KIND_MG, fl) as s:
+            phi = BoxData(v, 1, 1).to_device()
+            ms = []
+            for k in range(runs + 3):
+                phi.data.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                r = s.vcycle(phi, rhs_d, bc, True, TOL, 200, 1, *NU)
+                e1.record(stream)
+                e1.synchronize()
+                if k >= 3:
+                    ms.append(e0.elapsed_time(e1))
+        out[name] = {"vcycles": r.iterations, "final_relres": r.final_relres, "ms_per_solve": sorted(ms)[len(ms) // 2],
+                     "err_max": float(abs(phi.to_host().interior() - u).max())}
+    if cpu:
+        import multiprocessing as mp
+        _cpu_oracle().build(force=False)
+        with mp.get_context("spawn").Pool(1) as pool:
+            sec, its, e = pool.apply(_cpu_config1, (5,))
+        out["cpu_1core"] = {"vcycles": its, "ms_per_solve": sec * 1e3, "err_max": e, "kind": "port",
+                            "sample": "median of 5 full oracle solves (-march=native, FP64, lexicographic GS)"}
+    return out
+
+
 def run_reference(args):
     """--impl reference: the reference's algorithm on the CPU, on every host
     core the process may use.  Each step is one bounded sample per core (a
@@ -424,7 +483,9 @@ def served_leg(M, args, flags_list, pool=64, seed=5, rates=(10, 30, 100)):
     arrivals at each rate, tolerance 1e-8 or 1e-10 with probability 1/2,
     min(2000, 8 x rate) requests per rate (at least 100), hierarchies resident
     per problem; stops after the first rate whose p99 has diverged (above 10x
-    the lowest rate's p99, or fewer than 0.7 of the offered solves/s)."""
+    the lowest rate's p99, or fewer than 0.7 of the offered solves/s).  The
+    solver is the headline's, GMRES(V-cycle) with the exact bottom, mixed and
+    FP64."""
     import numpy as np
     import torch
     from mgpoisson2d_b200 import workloads as W
@@ -529,7 +590,8 @@ def precision_study(M, sizes):
     Dirichlet data at the face centres, metric generated on the device), for
     two solvers: BiCGStab(V-cycle) with the exact bottom ("mixed", "fp64") and
     the deferred-correction solve, DD V-cycles inside the FP64 9-point
-    residual loop, nu = 8/8/8 ("dc_mixed", "dc_fp64").  Per solve: V-cycles
+    residual loop, nu = 8/8/8 ("dc_mixed", "dc_fp64"), each also with BF16
+    values on the levels below the finest ("bf16", "dc_bf16").  Per solve: V-cycles
     (DC iterations), time, relative max / L2 error against u; per pair the
     mixed solution's distance from the FP64 one; per size step the observed
     order log2(e_n / e_2n) of the discretisation error."""
@@ -538,7 +600,9 @@ def precision_study(M, sizes):
     from mgpoisson2d_b200.types import BoxData
     kry = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV | M.FLAG_DIRECT_COARSE
     solvers = (("mixed", M.KIND_MG, kry | M.FLAG_MIXED), ("fp64", M.KIND_MG, kry),
-               ("dc_mixed", M.KIND_DD, M.FLAG_MIXED), ("dc_fp64", M.KIND_DD, 0))
+               ("bf16", M.KIND_MG, kry | M.FLAG_MIXED | M.FLAG_BF16_COARSE),
+               ("dc_mixed", M.KIND_DD, M.FLAG_MIXED), ("dc_fp64", M.KIND_DD, 0),
+               ("dc_bf16", M.KIND_DD, M.FLAG_MIXED | M.FLAG_BF16_COARSE))
     stream = torch.cuda.current_stream()
     rows = []
     for n in sizes:
@@ -566,7 +630,8 @@ def precision_study(M, sizes):
             row[name] = {"vcycles": r.iterations, "final_relres": r.final_relres, "ms": e0.elapsed_time(e1),
                          "err_max": float((p - u).abs().max() / u.abs().max()),
                          "err_l2": float(torch.linalg.norm(p - u) / torch.linalg.norm(u))}
-        for a, b, key in (("mixed", "fp64", "mixed_vs_fp64"), ("dc_mixed", "dc_fp64", "dc_mixed_vs_fp64")):
+        for a, b, key in (("mixed", "fp64", "mixed_vs_fp64"), ("dc_mixed", "dc_fp64", "dc_mixed_vs_fp64"),
+                          ("bf16", "fp64", "bf16_vs_fp64"), ("dc_bf16", "dc_fp64", "dc_bf16_vs_fp64")):
             d = sol[a] - sol[b]
             row[key] = {"rel_l2": float(torch.linalg.norm(d) / torch.linalg.norm(sol[b])),
                         "rel_max": float(d.abs().max() / sol[b].abs().max())}
@@ -578,7 +643,11 @@ def precision_study(M, sizes):
     torch.cuda.empty_cache()
     return {"workload": "skew_stretched (30 deg skew, 1.05 boundary-layer stretch, u = e^x cos 4 pi y)",
             "tol": TOL, "solvers": {"mixed / fp64": "bicgstab(vcycle), exact bottom",
-                                    "dc_mixed / dc_fp64": "deferred correction (dc_vcycle), nu 8/8/8"},
+                                    "dc_mixed / dc_fp64": "deferred correction (dc_vcycle), nu 8/8/8",
+                                    "bf16 / dc_bf16": "the mixed solvers with the levels below the finest holding "
+                                                      "BF16 values (MGP_FLAG_BF16_COARSE: a numerics study; the "
+                                                      "storage stays FP32, so its times include the rounding "
+                                                      "launches and no saved bytes)"},
             "rows": rows}
 
 
@@ -778,9 +847,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_batch:
         batched = batched_leg(M, args)
         line["batched"] = batched
-        kry = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV | M.FLAG_DIRECT_COARSE
+        gm = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_GMRES | M.FLAG_DIRECT_COARSE | M.FLAG_DIRECT_LARGE
         rates = (10, 30, 100, 300, 1000, 3000) if args.serve_sweep else (10, 30, 100)
-        served = served_leg(M, args, [("mixed", kry | M.FLAG_MIXED), ("fp64", kry)], rates=rates)
+        served = served_leg(M, args, [("mixed", gm | M.FLAG_MIXED), ("fp64", gm)], rates=rates)
         line["served"] = served
         # the metric's own comparison: mixed against plain FP64, batched and served
         line["batched_headline"] = {
@@ -791,6 +860,7 @@ def main():
             "served_rate_per_s": served["mixed"][0]["offered_per_s"]}
     if rank == 0 and world == 1 and not args.no_study:
         line["precision_study"] = precision_study(M, [int(x) for x in args.study_sizes.split(",") if x])
+        line["config1"] = config1_leg(M, not args.no_cpu)
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline_1core(args.n, args.cpu_vcycles_1core)
         line["cpu_baseline"] = cb

@@ -62,7 +62,7 @@ typedef enum mgp_status {
     MGP_EINVAL    = 1,  /* bad argument: the Fortran code would print and stop  */
     MGP_ENOMEM    = 2,  /* device or host allocation failed                     */
     MGP_EDIVERGED = 3,  /* non-finite residual (NaN/Inf in the data)            */
-    MGP_EMAXITER  = 4,  /* reserved: iteration cap reached (solves return OK)    */
+    MGP_EMAXITER  = 4,  /* maxiters reached (only with MGP_FLAG_REPORT_MAXITER) */
     MGP_ETIMEOUT  = 5,  /* a bounded device wait ran out                         */
     MGP_ECUDA     = 6,  /* a CUDA runtime call failed                            */
     MGP_ENOTSUP   = 7   /* a path the Fortran library also stops on              */
@@ -189,6 +189,26 @@ typedef struct mgp_report {
  * periodic one, and its bottom fits one CTA; otherwise the batch runs its
  * problems concurrently as without the flag.  No reference counterpart. */
 #define MGP_FLAG_LOCKSTEP 128
+/* vcycle, fmg, dc_vcycle (one-shot, resident, batch and server): a solve that
+ * stops because it ran maxiters V-cycles without reaching tol returns
+ * MGP_EMAXITER instead of MGP_OK (the report and phi are filled as usual).
+ * Without the flag such a solve returns MGP_OK, as the Fortran drivers do
+ * (MGPoisson2D.f90:596-645 leave the loop and return), and the caller reads
+ * report.final_relres.  A solve stopped by a growing residual (report.diverged)
+ * still returns MGP_OK.  No reference counterpart. */
+#define MGP_FLAG_REPORT_MAXITER 256
+/* with MGP_FLAG_MIXED: a numerics study of BF16 storage on the coarse grid
+ * levels.  The FP32 copies of every level below the finest -- the operator's
+ * face coefficients, J and the inverse diagonal when the solver is created,
+ * the correction and right-hand side each time a kernel writes them -- are
+ * rounded to the nearest BF16 value (round to nearest even), so the V-cycle
+ * computes in FP32 on the values a BF16 copy would hold.  The storage stays
+ * FP32, so the flag adds launches and saves no bytes: it measures the
+ * V-cycle counts and the error of that variant, not its speed.  The finest
+ * level, the FP64 outer iteration and the FP64 coarse levels (the single-CTA
+ * cycle and the exact bottom) are unchanged.  Not used by lockstep batches.
+ * No reference counterpart. */
+#define MGP_FLAG_BF16_COARSE 512
 
 /* Solver kinds for the resident-hierarchy handle. */
 #define MGP_KIND_MG 0   /* module MGPoisson2D (vcycle, fmg)                  */

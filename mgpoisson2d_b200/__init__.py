@@ -15,7 +15,7 @@ _API_NAMES = {
     "compute_div", "relax_gs", "relax_jacobi", "solve_bicgstab2", "solve_bicgstab2_noalloc", "restrict", "prolong",
     "pnorm", "inner_prod", "estimate_maxdepth", "create_mgschedule", "MGPError", "library_path",
     "kernel_launch_count", "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV", "FLAG_MIXED",
-    "FLAG_DIRECT_COARSE", "FLAG_GMRES", "FLAG_DIRECT_LARGE", "FLAG_LOCKSTEP",
+    "FLAG_DIRECT_COARSE", "FLAG_GMRES", "FLAG_DIRECT_LARGE", "FLAG_LOCKSTEP", "FLAG_REPORT_MAXITER", "FLAG_BF16_COARSE",
     "NOALLOC_MAX_SIDE", "EXPORTS",
 }
 

@@ -29,6 +29,8 @@ FLAG_DIRECT_COARSE = 16
 FLAG_GMRES = 32
 FLAG_DIRECT_LARGE = 64
 FLAG_LOCKSTEP = 128
+FLAG_REPORT_MAXITER = 256
+FLAG_BF16_COARSE = 512
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libmgp2d.so")
@@ -422,6 +424,7 @@ class Batch:
         _ck(_lib.mgp_batch_create(n, self._boxes, self._geos, self._bcs, kind, flags, maxdepth_user, nstreams,
                                   _r(self._h)), "batch_create")
         self.n = n
+        self._statuses = []
         self._nstreams = max(1, min(nstreams, n))
 
     def close(self):
@@ -512,9 +515,15 @@ class Batch:
         parr = (MgpArray * n)(*[p.c() for p in phis])
         farr = (MgpArray * n)(*[f.c() for f in rhss])
         barr = (MgpBdry * n)(*[b.c() for b in bcs])
-        _ck(_lib.mgp_batch_vcycle(self._h, parr, farr, barr, int(homog), tol, maxiters, numcycles, smooth_down,
-                                  smooth_up, smooth_bottom, int(zerophi), rarr), "batch_vcycle")
+        rc = _lib.mgp_batch_vcycle(self._h, parr, farr, barr, int(homog), tol, maxiters, numcycles, smooth_down,
+                                   smooth_up, smooth_bottom, int(zerophi), rarr)
+        self._statuses = [int(rarr[k].status) for k in range(n)]
+        _ck(rc, "batch_vcycle")
         return [read_report(rarr[k], bufs[k]) for k in range(n)]
+
+    def last_statuses(self):
+        """Each problem's status from the last vcycle call (also after it raised)."""
+        return list(self._statuses)
 
 
 class Server:
@@ -570,5 +579,5 @@ class Server:
 __all__ = ["vcycle", "fmg", "dc_vcycle", "Solver", "fill_ghosts", "extrapolate_ghosts", "compute_invdiags",
            "compute_laplacian", "compute_residual", "compute_pd", "compute_grad", "fill_boundary_fluxes", "compute_div", "relax_gs", "relax_jacobi", "solve_bicgstab2", "solve_bicgstab2_noalloc", "NOALLOC_MAX_SIDE", "restrict", "prolong", "pnorm",
            "inner_prod", "estimate_maxdepth", "create_mgschedule", "MGPError", "library_path", "kernel_launch_count",
-           "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV", "FLAG_MIXED", "FLAG_DIRECT_COARSE", "FLAG_GMRES", "FLAG_DIRECT_LARGE", "Batch", "Server", "map_geometry", "map_fourier_rhs",
+           "set_flags", "FLAG_DIRICHLET_COUPLED_DIAG", "FLAG_TIME_SMOOTHER", "FLAG_KRYLOV", "FLAG_MIXED", "FLAG_DIRECT_COARSE", "FLAG_GMRES", "FLAG_DIRECT_LARGE", "FLAG_LOCKSTEP", "FLAG_REPORT_MAXITER", "FLAG_BF16_COARSE", "Batch", "Server", "map_geometry", "map_fourier_rhs",
            "MAP_IDENTITY", "MAP_WAVY_EXP", "MAP_SKEW_LAYER", "EXPORTS", "KIND_MG", "KIND_DD"]

@@ -51,11 +51,13 @@ double now_s() {
 
 // Device bytes a hierarchy of nx x ny cells takes, before it exists: FP64
 // fields ~21 per cell over all levels (geometry, inverse diagonal,
-// corrections, residuals, the BiCGStab vectors), FP32 copies ~14, plus
-// padding and the small buffers.
+// corrections, residuals, the BiCGStab vectors), FP32 copies ~14, with
+// MGP_FLAG_GMRES the 2m + 1 = 129 stored fields of GMRES(64), plus padding
+// and the small buffers.
 size_t estimate_bytes(const mgp_box* v, int flags) {
     const double n = (double)v->nx * (double)v->ny;
-    const double per = 8.0 * 21.0 + ((flags & MGP_FLAG_MIXED) ? 4.0 * 14.0 : 0.0);
+    const double per = 8.0 * 21.0 + ((flags & MGP_FLAG_MIXED) ? 4.0 * 14.0 : 0.0) +
+                       ((flags & MGP_FLAG_GMRES) ? 8.0 * 129.0 : 0.0);
     return (size_t)(n * per) + ((size_t)8 << 20);
 }
 

@@ -60,6 +60,8 @@ constexpr long kCoarseCells = 1024;
 // the coarsest level alone; beyond this many cells it runs as a cooperative
 // grid of one CTA per 256 cells (at most one per SM) instead of one CTA.
 constexpr long kGridCoarseCells = 8192;
+// Largest coarse-cycle level run by one thread-block cluster (cells).
+constexpr long kClusterCoarseCells = 1L << 17;
 
 // ---------------------------------------------------------------------------
 // Device memory of solvers comes from a stream-ordered pool per device, owned
@@ -360,6 +362,7 @@ struct mgp_solver {
     bool direct_large = false;
     // coarse cycle as a cooperative grid of grid_ctas CTAs (0: one CTA)
     int grid_ctas = 0;
+    int coarse_cluster = 0;   // the grid_ctas CTAs form one thread-block cluster (2: one-CTA reduction order)
     GridCtl gctl{};
     int* d_ref = nullptr;   // refx then refy
     int* d_status = nullptr;
@@ -616,6 +619,14 @@ int build_fp32_levels(mgp_solver* s) {
         CK(launch_convert(M.g.yx, L.g.yx, L.nx, L.ny + 1, 0, 0, st));
         CK(launch_convert(M.g.yy, L.g.yy, L.nx, L.ny + 1, 0, 0, st));
         CK(launch_convert(M.invd, L.invd, L.nx, L.ny, 0, 0, st));
+        if (d >= 1 && (s->flags & MGP_FLAG_BF16_COARSE)) {
+            CK(launch_round_bf16(M.g.J, L.nx, L.ny, 0, st));
+            CK(launch_round_bf16(M.g.xx, L.nx + 1, L.ny, 0, st));
+            CK(launch_round_bf16(M.g.xy, L.nx + 1, L.ny, 0, st));
+            CK(launch_round_bf16(M.g.yx, L.nx, L.ny + 1, 0, st));
+            CK(launch_round_bf16(M.g.yy, L.nx, L.ny + 1, 0, st));
+            CK(launch_round_bf16(M.invd, L.nx, L.ny, 0, st));
+        }
         sweep_tma_prepare(&s->tma32[d], M.e, M.e2, M.r, M.invd, M.g, M.nx, M.ny);
     }
     return MGP_OK;
@@ -752,22 +763,6 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
             return set_err(MGP_ENOMEM, "device allocation failed");
         }
     }
-    // (one CTA per 256 cells, at most one per SM and at most what the device
-    // keeps resident; a device without cooperative launch keeps one CTA)
-    const int grid_max = coarse_grid_ctas_max();
-    if (const long cells = (long)s->lv[s->dc].nx * s->lv[s->dc].ny; cells > kGridCoarseCells && grid_max > 1) {
-        int dev = 0, nsm = 0;
-        CK(cudaGetDevice(&dev));
-        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        s->grid_ctas = (int)std::min<long>(std::min(std::max(nsm, 1), grid_max), std::max<long>(2, cells / 256));
-        if (dmalloc(&s->gctl.bar, 2 * sizeof(unsigned), st) != cudaSuccess ||
-            dmalloc(&s->gctl.part, 2 * sizeof(double) * s->grid_ctas, st) != cudaSuccess) {
-            cudaGetLastError();
-            return set_err(MGP_ENOMEM, "device allocation failed");
-        }
-        s->gctl.status = s->d_status;
-        s->gctl.wait_ns = kGridWaitNsDefault;
-    }
     // shared-memory layout of the coarse levels for k_coarse_cycle_smem
     {
         std::vector<Lv> sh(s->lv);
@@ -807,6 +802,39 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
             }
             CK(cudaMemcpyAsync(s->d_shadow, sh.data(), sizeof(Lv) * (md + 1), cudaMemcpyHostToDevice, st));
             s->shadow_bytes = (int)bytes;
+        }
+    }
+    // Coarse levels that one CTA cannot stage in shared memory: up to
+    // kClusterCoarseCells, one thread-block cluster of 16 (or 8) CTAs with
+    // hardware barriers; above that, or where no such cluster fits and the
+    // level has more than kGridCoarseCells cells, a cooperative grid, one CTA
+    // per 256 cells, at most one per SM and at most what the device keeps
+    // resident; otherwise one CTA on global memory.
+    {
+        const int grid_max = coarse_grid_ctas_max();
+        const long coarse_cells = (long)s->lv[s->dc].nx * s->lv[s->dc].ny;
+        const bool staged = s->shadow_bytes > 0;
+        const int cluster_max = !staged && coarse_cells <= kClusterCoarseCells ? coarse_cluster_ctas_max() : 0;
+        if (cluster_max > 1) {
+            // levels a lockstep batch also serves (one CTA there) keep the
+            // one-CTA reduction order, so a problem has the same bits in both
+            s->grid_ctas = cluster_max;
+            s->coarse_cluster = coarse_cells <= kGridCoarseCells ? 2 : 1;
+        } else if (!staged && coarse_cells > kGridCoarseCells && grid_max > 1) {
+            int dev = 0, nsm = 0;
+            CK(cudaGetDevice(&dev));
+            CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+            s->grid_ctas = (int)std::min<long>(std::min(std::max(nsm, 1), grid_max),
+                                               std::max<long>(2, coarse_cells / 256));
+        }
+        if (s->grid_ctas > 1) {
+            if (dmalloc(&s->gctl.bar, 2 * sizeof(unsigned), st) != cudaSuccess ||
+                dmalloc(&s->gctl.part, 2 * sizeof(double) * s->grid_ctas, st) != cudaSuccess) {
+                cudaGetLastError();
+                return set_err(MGP_ENOMEM, "device allocation failed");
+            }
+            s->gctl.status = s->d_status;
+            s->gctl.wait_ns = kGridWaitNsDefault;
         }
     }
     s->tma.assign(md + 1, SweepTma{});
@@ -943,8 +971,9 @@ int coarse_cycle(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
     a.shadow = s->d_shadow;
     a.smem_bytes = s->shadow_bytes;
     a.grid_ctas = s->grid_ctas;
+    a.cluster = s->coarse_cluster;
     a.gctl = s->gctl;
-    if (a.grid_ctas > 1) CK(cudaMemsetAsync(s->gctl.bar, 0, 2 * sizeof(unsigned), s->stream));
+    if (a.grid_ctas > 1 && !a.cluster) CK(cudaMemsetAsync(s->gctl.bar, 0, 2 * sizeof(unsigned), s->stream));
     CK(launch_coarse_cycle(a, s->stream));
     return MGP_OK;
 }
@@ -982,6 +1011,12 @@ int vcycle32(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
     const Lv& F = s->lv[d];   // BCs of the level
     cudaStream_t st = s->stream;
     const bool dd = (s->kind == MGP_KIND_DD);
+    // MGP_FLAG_BF16_COARSE: the fields of levels >= 1 take BF16 values each
+    // time a kernel writes them to memory
+    const bool b16 = (s->flags & MGP_FLAG_BF16_COARSE) != 0;
+    auto round16 = [&](const DF32& f, int lvl, int nx_, int ny_, int g) -> cudaError_t {
+        return (b16 && lvl >= 1) ? launch_round_bf16(f, nx_, ny_, g, st) : cudaSuccess;
+    };
     if (dd) CK(launch_set_guess(L.e, L.r, L.invd, L.nx, L.ny, st));   // DD:971
     auto smooth32 = [&](int nu_) -> int {
         return timed_smooth(s, d, nu_, [&]() -> int {
@@ -992,6 +1027,7 @@ int vcycle32(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
                     CK(launch_fill(L.e, L.g, F.bc, 1, 1, L.nx, L.ny, st));   // DD:259
                     CK(launch_dd_colour(L.e, L.w, L.invd, L.g, L.nx, L.ny, 4.0 / 5.0, 0, st));
                     CK(launch_dd_colour(L.e, L.w, L.invd, L.g, L.nx, L.ny, 4.0 / 5.0, 1, st));
+                    CK(round16(L.e, d, L.nx, L.ny, 1));
                 }
                 return MGP_OK;
             }
@@ -1009,6 +1045,7 @@ int vcycle32(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
                     k += 1;
                 }
                 std::swap(L.e, L.e2);
+                CK(round16(L.e, d, L.nx, L.ny, 1));
             }
             return MGP_OK;
         });
@@ -1020,13 +1057,20 @@ int vcycle32(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
     if (dd) {
         CK(launch_dd_apply(L.w, L.e, L.r, L.g, F.bc, L.nx, L.ny, 1, st));
         CK(launch_fill(L.e, L.g, F.bc, 1, 1, L.nx, L.ny, st));
-        if (fine_next) CK(launch_restrict(L.w, s->lv32[d + 1].r, s->lv32[d + 1].nx, s->lv32[d + 1].ny, rx, ry, st));
-        else CK(launch_restrict(L.w, C.r, C.nx, C.ny, rx, ry, st));
+        if (fine_next) {
+            auto& N = s->lv32[d + 1];
+            CK(launch_restrict(L.w, N.r, N.nx, N.ny, rx, ry, st));
+            CK(round16(N.r, d + 1, N.nx, N.ny, 0));
+        } else {
+            CK(launch_restrict(L.w, C.r, C.nx, C.ny, rx, ry, st));
+        }
     } else {   // residual (MG:793-795), restriction and the coarse guess (MG:805-806) in one pass
         CK(launch_fill(L.e, L.g, F.bc, 1, 0, L.nx, L.ny, st));
         if (fine_next) {
             auto& N = s->lv32[d + 1];
             CK(launch_resid_restrict(L.e, L.r, L.g, F.bc, 1, L.nx, L.ny, N.r, N.e, N.invd, N.nx, N.ny, rx, ry, 1, st));
+            CK(round16(N.r, d + 1, N.nx, N.ny, 0));
+            CK(round16(N.e, d + 1, N.nx, N.ny, 1));
         } else {
             CK(launch_resid_restrict(L.e, L.r, L.g, F.bc, 1, L.nx, L.ny, C.r, C.e, C.invd, C.nx, C.ny, rx, ry, 1, st));
         }
@@ -1035,11 +1079,14 @@ int vcycle32(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
         auto& N = s->lv32[d + 1];
         for (int c = 1; c <= numcycles; ++c) RC(vcycle32(s, d + 1, numcycles, nd, nu, nb));
         CK(launch_fill(N.e, N.g, C.bc, 1, 1, N.nx, N.ny, st));    // MG:318
+        CK(round16(N.e, d + 1, N.nx, N.ny, 1));
         CK(launch_prolong(L.e, N.e, N.nx, N.ny, rx, ry, 1, st));
+        CK(round16(L.e, d, L.nx, L.ny, 1));
     } else {
         for (int c = 1; c <= numcycles; ++c) RC(vcycle_noinit(s, d + 1, numcycles, nd, nu, nb));
         CK(launch_fill(C.e, C.g, C.bc, 1, 1, C.nx, C.ny, st));
         CK(launch_prolong(L.e, C.e, C.nx, C.ny, rx, ry, 1, st));
+        CK(round16(L.e, d, L.nx, L.ny, 1));
     }
     const bool rax = (C.bc.type[0] == T_PERIODIC && C.bc.type[1] == T_PERIODIC) ||
                      (C.bc.type[0] == T_NEUM && C.bc.type[1] == T_NEUM);
@@ -1048,6 +1095,7 @@ int vcycle32(mgp_solver* s, int d, int numcycles, int nd, int nu, int nb) {
     if (rax && ray) {   // MG:371-383
         CK(launch_reduce(RED_JSUM, L.e, L.g.J, L.nx, L.ny, L.g.dx * L.g.dy, red_partials(s), red_out(s), st));
         CK(launch_sub_mean(L.e, red_out(s), L.nx, L.ny, 1, 1, st));
+        CK(round16(L.e, d, L.nx, L.ny, 1));
     }
     RC(smooth32(nu));
     return MGP_OK;
@@ -1462,6 +1510,8 @@ int solver_solve(mgp_solver* s, int which, mgp_array* phi, mgp_array* rhs, const
     CK(cudaStreamSynchronize(st));
     if (status == MGP_OK && dstat)
         status = (dstat == DST_TIMEOUT) ? MGP_ETIMEOUT : (dstat == DST_MISALIGNED) ? MGP_ECUDA : MGP_EDIVERGED;
+    if (status == MGP_OK && (s->flags & MGP_FLAG_REPORT_MAXITER) && !diverged && !(relres[iters] <= tol))
+        status = MGP_EMAXITER;
     if (rep) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, s->ev0, s->ev1);
@@ -1485,6 +1535,7 @@ int solver_solve(mgp_solver* s, int which, mgp_array* phi, mgp_array* rhs, const
     }
     if (status == MGP_ETIMEOUT) return set_err(status, "a device wait ran out of its iteration limit");
     if (status == MGP_ECUDA) return set_err(status, "misaligned shared-memory window in the sweep");
+    if (status == MGP_EMAXITER) return set_err(status, "maxiters reached before the tolerance");
     if (status) return set_err(status, "non-finite residual");
     return MGP_OK;
 }
@@ -1785,6 +1836,7 @@ CoarseArgs coarse_args_of(mgp_solver* s, int d, int nd, int nu, int nb) {
     a.shadow = s->d_shadow;
     a.smem_bytes = s->shadow_bytes;
     a.grid_ctas = 0;
+    a.cluster = 0;
     return a;
 }
 
@@ -1998,8 +2050,9 @@ bool lockstep_ok(const std::vector<mgp_solver*>& ss, int numcycles, int nd, int 
     if (ss.empty() || numcycles != 1 || (nd & 1) || (nu & 1) || nd < 0 || nu < 0) return false;
     const bool mx = mixed(ss[0]);
     for (mgp_solver* s : ss) {
-        if (s->kind != MGP_KIND_MG || (s->flags & (MGP_FLAG_KRYLOV | MGP_FLAG_GMRES)) ||
-            (s->direct_large && s->db != s->dc) || s->grid_ctas > 1 || mixed(s) != mx)
+        if (s->kind != MGP_KIND_MG || (s->flags & (MGP_FLAG_KRYLOV | MGP_FLAG_GMRES | MGP_FLAG_BF16_COARSE)) ||
+            (s->direct_large && s->db != s->dc) || (long)s->lv[s->dc].nx * s->lv[s->dc].ny > kGridCoarseCells ||
+            mixed(s) != mx)
             return false;
         bool diri = false;
         for (int k = 0; k < 4; ++k) {
@@ -2176,6 +2229,9 @@ int lockstep_vcycle(const std::vector<mgp_solver*>& ss, Lockstep* ls, mgp_array*
         if (!dstat) dstat = sweep_status;
         if (status[p] == MGP_OK && dstat)
             status[p] = (dstat == DST_TIMEOUT) ? MGP_ETIMEOUT : (dstat == DST_MISALIGNED) ? MGP_ECUDA : MGP_EDIVERGED;
+        if (status[p] == MGP_OK && (ss[p]->flags & MGP_FLAG_REPORT_MAXITER) && !diverged[p] &&
+            !(hist[p][iters[p]] <= tol))
+            status[p] = MGP_EMAXITER;
         if (reports) {
             mgp_report& r = reports[p];
             double* dst = r.relres;
@@ -2195,6 +2251,7 @@ int lockstep_vcycle(const std::vector<mgp_solver*>& ss, Lockstep* ls, mgp_array*
     }
     if (first == MGP_ETIMEOUT) return set_err(first, "a device wait ran out of its iteration limit");
     if (first == MGP_ECUDA) return set_err(first, "misaligned shared-memory window in the sweep");
+    if (first == MGP_EMAXITER) return set_err(first, "maxiters reached before the tolerance");
     if (first) return set_err(first, "non-finite residual");
     return MGP_OK;
 }

@@ -14,6 +14,8 @@
 
 #include <mutex>
 
+#include <cuda_bf16.h>
+
 #include "mgp_kernels.cuh"
 
 namespace mgp {
@@ -375,19 +377,60 @@ __device__ void grid_barrier() {
     __syncthreads();
 }
 
+// rrank / rsize / ractive: the loop that accumulates a reduction's
+// per-thread partial sums (RLOOP).
 struct BlockScope {
     static constexpr bool kGrid = false;
+    static constexpr bool kCluster = false;
     __device__ static int rank() { return threadIdx.x; }
     __device__ static int size() { return blockDim.x; }
     __device__ static void sync() { __syncthreads(); }
+    __device__ static int rrank() { return threadIdx.x; }
+    __device__ static int rsize() { return blockDim.x; }
+    __device__ static bool ractive() { return true; }
 };
 struct GridScope {
     static constexpr bool kGrid = true;
+    static constexpr bool kCluster = false;
     __device__ static int rank() { return blockIdx.x * blockDim.x + threadIdx.x; }
     __device__ static int size() { return gridDim.x * blockDim.x; }
     __device__ static void sync() { grid_barrier(); }
+    __device__ static int rrank() { return rank(); }
+    __device__ static int rsize() { return size(); }
+    __device__ static bool ractive() { return true; }
+};
+// The CTAs of one thread-block cluster that is the whole grid (co-scheduled
+// on one GPC by the hardware): GridScope's loops and CTA-ordered reductions,
+// with the cluster's hardware barrier (release / acquire at cluster scope,
+// which orders the global-memory accesses of every thread of the cluster) in
+// place of the polled global-memory barrier.  Like __syncthreads it needs no
+// time limit: every CTA of a cluster is resident before any runs, and the
+// coarse cycle's control flow is the same in every CTA (each one combines
+// the reductions' partials in the same order).
+__device__ __forceinline__ void cluster_barrier() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// kOrdered: its reductions are accumulated by the first CTA alone, thread t
+// summing cells t, t + blockDim, ... as BlockScope's thread t does, and
+// combined by the same block tree (the CTAs have BlockScope's kCoarseThreads
+// threads), so every result -- the sweeps, whose colour passes do not depend
+// on which thread updates a cell, and the reductions -- has the bits of the
+// one-CTA kernel; the result reaches the other CTAs through global memory.
+// Otherwise every CTA accumulates its share and the CTAs' partials are
+// combined in CTA order, as in GridScope.
+template <bool kOrdered>
+struct ClusterScope {
+    static constexpr bool kGrid = true;
+    static constexpr bool kCluster = kOrdered;
+    __device__ static int rank() { return blockIdx.x * blockDim.x + threadIdx.x; }
+    __device__ static int size() { return gridDim.x * blockDim.x; }
+    __device__ static void sync() { cluster_barrier(); }
+    __device__ static int rrank() { return kOrdered ? (int)threadIdx.x : rank(); }
+    __device__ static int rsize() { return kOrdered ? (int)blockDim.x : size(); }
+    __device__ static bool ractive() { return !kOrdered || blockIdx.x == 0; }
 };
 #define SLOOP(k, n) for (int k = S::rank(); k < (n); k += S::size())
+#define RLOOP(k, n) for (int k = S::rrank(); S::ractive() && k < (n); k += S::rsize())
 
 // Step 3 of the sweep; every thread of the scope calls it.
 template <class S>
@@ -656,6 +699,21 @@ cudaError_t launch_convert(const DF32& dst, const DF& src, int nx, int ny, int g
 }
 cudaError_t launch_convert(const DF& dst, const DF32& src, int nx, int ny, int gx, int gy, cudaStream_t st) {
     k_convert<<<cells_grid(nx + 2 * gx, ny + 2 * gy, kBlk2), kBlk2, 0, st>>>(dst, src, nx, ny, gx, gy);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// Every value of an FP32 field (ghosts included) replaced by the nearest
+// BF16 value (round to nearest even): the values a BF16 copy of the field
+// would hold, read back into FP32 arithmetic.
+__global__ void k_round_bf16(DF32 f, int nx, int ny, int g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x - g;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y - g;
+    if (i >= nx + g || j >= ny + g) return;
+    AT(f, i, j) = __bfloat162float(__float2bfloat16_rn(AT(f, i, j)));
+}
+cudaError_t launch_round_bf16(const DF32& f, int nx, int ny, int g, cudaStream_t st) {
+    k_round_bf16<<<cells_grid(nx + 2 * g, ny + 2 * g, kBlk2), kBlk2, 0, st>>>(f, nx, ny, g);
     count_launch();
     return cudaGetLastError();
 }
@@ -1136,10 +1194,20 @@ __device__ double b_reduce(double v, double* sh) {
     __syncthreads();
     if constexpr (!S::kGrid) {
         return sh[32];
+    } else if constexpr (S::kCluster) {
+        volatile double* part = s_gctl.part + (s_gred & 1) * gridDim.x;
+        if (blockIdx.x == 0 && threadIdx.x == 0) part[0] = sh[32];
+        S::sync();
+        if (threadIdx.x == 0) {
+            sh[33] = part[0];
+            s_gred = s_gred + 1;
+        }
+        __syncthreads();
+        return sh[33];
     } else {
         volatile double* part = s_gctl.part + (s_gred & 1) * gridDim.x;
         if (threadIdx.x == 0) part[blockIdx.x] = sh[32];
-        grid_barrier();
+        S::sync();
         if (threadIdx.x == 0) {
             double t = part[0];
             for (int c = 1; c < (int)gridDim.x; ++c) t = kMax ? fmax(t, part[c]) : t + part[c];
@@ -1155,22 +1223,64 @@ __device__ double b_sum(double v, double* sh) { return b_reduce<S, false>(v, sh)
 template <class S>
 __device__ double b_max(double v, double* sh) { return b_reduce<S, true>(v, sh); }
 
+// A thread's partial of a reduction over the cells k = rrank, rrank + rsize,
+// ... (k = i + j nx), combined in that order: acc = op(acc, f(i, j)).  Four
+// cells' values are loaded before they are combined, and the cell index
+// advances by addition, so the loads overlap; the order of the combines, and
+// so the result, is the plain loop's.
+template <class S, bool kMax, class F>
+__device__ __forceinline__ double r_accum(int nx, int ny, F f) {
+    double acc = 0.0;
+    if (!S::ractive()) return acc;
+    const int n = nx * ny, step = S::rsize();
+    const int di = step % nx, dj = step / nx;
+    int k = S::rrank(), i = k % nx, j = k / nx;
+    auto adv = [&](int& ii, int& jj) {
+        ii += di;
+        jj += dj;
+        if (ii >= nx) {
+            ii -= nx;
+            ++jj;
+        }
+    };
+    auto op = [](double x, double v) { return kMax ? fmax(x, v) : x + v; };
+    for (; k + 3 * step < n; k += 4 * step) {
+        int i1 = i, j1 = j;
+        adv(i1, j1);
+        int i2 = i1, j2 = j1;
+        adv(i2, j2);
+        int i3 = i2, j3 = j2;
+        adv(i3, j3);
+        const double v0 = f(i, j), v1 = f(i1, j1), v2 = f(i2, j2), v3 = f(i3, j3);
+        acc = op(acc, v0);
+        acc = op(acc, v1);
+        acc = op(acc, v2);
+        acc = op(acc, v3);
+        i = i3;
+        j = j3;
+        adv(i, j);
+    }
+    for (; k < n; k += step) {
+        acc = op(acc, f(i, j));
+        adv(i, j);
+    }
+    return acc;
+}
+
 // pnorm (AU:753-796) with p = 2 or 0.
 template <class S>
 __device__ double b_pnorm(const DF& a, int nx, int ny, int p, double vol, double* sh) {
-    double acc = 0.0;
-    SLOOP(k, nx * ny) {
-        const double v = AT(a, k % nx, k / nx);
-        acc = (p == 0) ? fmax(acc, fabs(v)) : acc + v * v;
-    }
-    if (p == 0) return b_max<S>(acc, sh);
+    if (p == 0) return b_max<S>(r_accum<S, true>(nx, ny, [&](int i, int j) { return fabs(AT(a, i, j)); }), sh);
+    const double acc = r_accum<S, false>(nx, ny, [&](int i, int j) {
+        const double v = AT(a, i, j);
+        return v * v;
+    });
     return sqrt(vol * b_sum<S>(acc, sh));
 }
 
 template <class S>
 __device__ double b_dot(const DF& a, const DF& c, int nx, int ny, double vol, double* sh) {
-    double acc = 0.0;
-    SLOOP(k, nx * ny) acc = acc + AT(a, k % nx, k / nx) * AT(c, k % nx, k / nx);
+    const double acc = r_accum<S, false>(nx, ny, [&](int i, int j) { return AT(a, i, j) * AT(c, i, j); });
     return vol * b_sum<S>(acc, sh);
 }
 
@@ -1473,7 +1583,7 @@ __device__ void b_prolong(const Lv& F, const Lv& Cl, int refx, int refy, int ord
     if (rax && ray) {   // MG:371-383
         const double dxprod = F.g.dx * F.g.dy;
         double s = 0.0, vv = 0.0;
-        SLOOP(k, F.nx * F.ny) {
+        RLOOP(k, F.nx * F.ny) {
             const double jj = AT(F.g.J, k % F.nx, k / F.nx);
             s = s + jj * AT(F.e, k % F.nx, k / F.nx);
             vv = vv + jj;
@@ -1980,6 +2090,71 @@ __global__ void __launch_bounds__(kCoarseThreads, 1) k_coarse_cycle_grid(CoarseA
     if (GridScope::rank() == 0) set_status(a.status, s);
 }
 
+// The coarse sub-cycle over one thread-block cluster of a.grid_ctas CTAs
+// (a.cluster set): the same body as k_coarse_cycle_grid with hardware
+// cluster barriers, for coarsest levels that one CTA cannot stage in shared
+// memory, where the grid version's time is its barriers.  kOrdered
+// (a.cluster == 2): the one-CTA kernel's reduction order and bits.
+static_assert(kClusterThreads == kCoarseThreads, "the cluster CTAs reduce in the one-CTA kernel's order");
+template <bool kOrdered>
+__global__ void __launch_bounds__(kClusterThreads, 1) k_coarse_cycle_cluster(CoarseArgs a) {
+    __shared__ double sh[64];
+    if (threadIdx.x == 0) {
+        s_gctl = a.gctl;
+        s_gred = 0;
+    }
+    __syncthreads();
+    const int s = coarse_body<ClusterScope<kOrdered>>(a.lv, a, sh);
+    if (ClusterScope<kOrdered>::rank() == 0) set_status(a.status, s);
+}
+
+// Largest cluster of k_coarse_cycle_cluster (16, else 8) that the current
+// device can place at least once, or 0.
+int coarse_cluster_ctas_max() {
+    static std::mutex mu;
+    static int cached[64];
+    static unsigned long long known = 0;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev < 64 && ((known >> dev) & 1ull)) return cached[dev];
+    int best = 0;
+    if (cudaFuncSetAttribute(k_coarse_cycle_cluster<true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+            cudaSuccess &&
+        cudaFuncSetAttribute(k_coarse_cycle_cluster<false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+            cudaSuccess) {
+        for (int n : {16, 8}) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(n);
+            cfg.blockDim = dim3(kClusterThreads);
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = n;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            int nclusters = 0;
+            int nclusters2 = 0;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, k_coarse_cycle_cluster<true>, &cfg) == cudaSuccess &&
+                cudaOccupancyMaxActiveClusters(&nclusters2, k_coarse_cycle_cluster<false>, &cfg) == cudaSuccess &&
+                nclusters >= 1 && nclusters2 >= 1) {
+                best = n;
+                break;
+            }
+        }
+    }
+    cudaGetLastError();
+    if (dev < 64) {
+        cached[dev] = best;
+        known |= 1ull << dev;
+    }
+    return best;
+}
+
 // How many CTAs of k_coarse_cycle_grid the current device can keep resident
 // at once (0 if it cannot launch cooperative grids).
 int coarse_grid_ctas_max() {
@@ -2033,6 +2208,23 @@ cudaError_t launch_barrier_selftest(const GridCtl& g, int nctas, int skip, int n
 }
 
 cudaError_t launch_coarse_cycle(const CoarseArgs& a, cudaStream_t st) {
+    if (a.grid_ctas > 1 && a.cluster) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(a.grid_ctas);
+        cfg.blockDim = dim3(kClusterThreads);
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = a.grid_ctas;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        const cudaError_t e = a.cluster == 2 ? cudaLaunchKernelEx(&cfg, k_coarse_cycle_cluster<true>, a)
+                                             : cudaLaunchKernelEx(&cfg, k_coarse_cycle_cluster<false>, a);
+        count_launch();
+        return e;
+    }
     if (a.grid_ctas > 1) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(a.grid_ctas);

@@ -57,6 +57,8 @@ struct CoarseArgs {
     int smem_bytes;      // dynamic shared memory the staged levels need
     const double* ainv;  // MGP_FLAG_DIRECT_COARSE: inverse of level maxdepth's operator, transposed, or nullptr
     int grid_ctas;       // > 1: run as a cooperative grid of this many CTAs (gctl set)
+    int cluster;         // with grid_ctas > 1: the grid is one thread-block cluster (hardware barriers);
+                         // 2: its reductions in the one-CTA kernel's order (the same bits)
     GridCtl gctl;
 };
 
@@ -86,6 +88,7 @@ struct BicgArgs {
 };
 
 constexpr int kCoarseThreads = 256;
+constexpr int kClusterThreads = 256;   // threads per CTA of the cluster coarse cycle
 
 long long launch_count();
 long long thread_launch_count();   // launches the calling thread made (count_launch on it)
@@ -127,6 +130,7 @@ cudaError_t launch_reduce(int kind, const DF32& a, const DF32& b, int nx, int ny
 // dst = src rounded to dst's type, over i in [-gx, nx+gx), j in [-gy, ny+gy).
 cudaError_t launch_convert(const DF32& dst, const DF& src, int nx, int ny, int gx, int gy, cudaStream_t st);
 cudaError_t launch_convert(const DF& dst, const DF32& src, int nx, int ny, int gx, int gy, cudaStream_t st);
+cudaError_t launch_round_bf16(const DF32& f, int nx, int ny, int g, cudaStream_t st);
 // mode: 0 lap, 1 rhs - lap; jscale divides lap by J first.
 cudaError_t launch_apply(const DF& out, const DF& phi, const DF& rhs, const Geo& g, const BCd& b, int homog,
                          int nx, int ny, int mode, int jscale, cudaStream_t st);
@@ -336,6 +340,7 @@ cudaError_t coarse_kernels_init();
 cudaError_t launch_coarse_cycle(const CoarseArgs& a, cudaStream_t st);
 // Largest cooperative grid of the coarse cycle the current device keeps resident (0: none).
 int coarse_grid_ctas_max();
+int coarse_cluster_ctas_max();
 // A cooperative grid of nctas CTAs (all resident) passing nbar grid barriers;
 // CTA `skip` (if >= 0) exits before the first one, so the others' waits run
 // out.  Exercises the bounded wait of the coarse cycle's grid barrier.

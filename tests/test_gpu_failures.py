@@ -30,7 +30,7 @@ pytestmark = pytest.mark.gpu
 
 torch = pytest.importorskip("torch")
 
-MGP_OK, MGP_ENOMEM, MGP_EDIVERGED, MGP_ETIMEOUT = 0, 2, 3, 5
+MGP_OK, MGP_ENOMEM, MGP_EDIVERGED, MGP_EMAXITER, MGP_ETIMEOUT = 0, 2, 3, 4, 5
 
 
 @pytest.fixture(scope="module")
@@ -174,3 +174,46 @@ def test_grid_barrier_selftest_rejects_bad_arguments(M):
     assert M.selftest_grid_barrier(4, 4, 4, 0.05)[0] == 1           # skip index out of range
     assert M.selftest_grid_barrier(4, -1, 4, 0.0)[0] == 1           # no limit
     assert M.selftest_grid_barrier(100000, -1, 4, 0.05)[0] == 1     # more CTAs than stay resident
+
+
+@pytest.mark.parametrize("flags", [0, 4 | 8, 32 | 8 | 16 | 64])   # plain; BiCGStab + mixed; GMRES + exact bottom
+def test_maxiter_status_only_with_the_flag(M, flags):
+    """A solve capped by maxiters returns OK as the Fortran drivers do, and
+    MGP_EMAXITER with MGP_FLAG_REPORT_MAXITER; the iterate is the same either way,
+    and a solve that reaches tol under the flag still returns OK."""
+    v, geo, rhs, bc, _ = W.wavy_stretched(128)
+    base = M.FLAG_DIRICHLET_COUPLED_DIAG | flags
+    with M.Solver(v, geo, bc, M.KIND_MG, base) as s:
+        phi0 = BoxData(v, 1, 1)
+        rep0 = s.vcycle(phi0, rhs, bc, True, 1e-10, 2)
+    assert rep0.iterations == 2 and rep0.final_relres > 1e-10
+    with M.Solver(v, geo, bc, M.KIND_MG, base | M.FLAG_REPORT_MAXITER) as s:
+        phi1 = BoxData(v, 1, 1)
+        with pytest.raises(M.MGPError) as ei:
+            s.vcycle(phi1, rhs, bc, True, 1e-10, 2)
+        assert ei.value.status == MGP_EMAXITER
+        assert np.array_equal(phi1.interior(), phi0.interior())
+        rep = s.vcycle(BoxData(v, 1, 1), rhs, bc, True, 1e-10, 400)
+        assert rep.final_relres <= 1e-10
+
+
+def test_maxiter_status_in_a_lockstep_batch(M):
+    """Under lockstep each report carries its own status: the problems that
+    reach tol within maxiters report OK, the rest MGP_EMAXITER, and the call
+    returns MGP_EMAXITER."""
+    probs = [W.batch_problem(i) for i in (0, 1, 2, 5, 6, 7, 8, 13, 14, 20)]
+    phis = [BoxData(p[0], 1, 1) for p in probs]
+    fl = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_LOCKSTEP
+    with M.Batch([(p[0], p[1], p[3]) for p in probs], M.KIND_MG, fl) as b:
+        reps = b.vcycle(phis, [p[2] for p in probs], [p[3] for p in probs], True, 1e-10, 60)
+    its = sorted(r.iterations for r in reps)
+    cap = its[len(its) // 2]
+    assert its[0] <= cap < its[-1]
+    phis = [BoxData(p[0], 1, 1) for p in probs]
+    with M.Batch([(p[0], p[1], p[3]) for p in probs], M.KIND_MG, fl | M.FLAG_REPORT_MAXITER) as b:
+        with pytest.raises(M.MGPError) as ei:
+            b.vcycle(phis, [p[2] for p in probs], [p[3] for p in probs], True, 1e-10, cap)
+        assert ei.value.status == MGP_EMAXITER
+        st = b.last_statuses()
+    for r, s in zip(reps, st):
+        assert s == (MGP_OK if r.iterations <= cap else MGP_EMAXITER)

@@ -489,6 +489,40 @@ def test_mixed_dc_vcycle_converges_to_fp64_solution(M, which):
     assert np.abs(err).max() / np.abs(sols[0].interior()).max() < 1e-7
 
 
+@pytest.mark.parametrize("kind", ["krylov", "dc"])
+def test_bf16_coarse_values_converge_to_fp64_solution(M, kind):
+    """MGP_FLAG_BF16_COARSE (a numerics study of BF16 storage below the
+    finest level): the FP64 outer iteration still reaches 1e-10 and the FP64
+    solution; the flag changes the iterates (the coarse levels hold other
+    values) and stays deterministic."""
+    from mgpoisson2d_b200 import workloads as W
+    v, geo, rhs, bc, _ = W.skew_stretched(128)
+    f = rhs.copy()
+    f.interior()[:] /= geo.J.interior()
+
+    def run(fl):
+        if kind == "dc":
+            with M.Solver(v, geo, bc, KIND_DD, fl) as s:
+                p = BoxData(v, 1, 1)
+                r = s.dc_vcycle(p, f.copy(), bc, False, 1e-10, 400, 1, 8, 8, 8)
+        else:
+            with M.Solver(v, geo, bc, KIND_MG, fl | M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV) as s:
+                p = BoxData(v, 1, 1)
+                r = s.vcycle(p, rhs, bc, False, 1e-10, 400)
+        assert r.status == 0 and not r.diverged and r.final_relres <= 1e-10, (fl, r.iterations, r.final_relres)
+        return p, r
+    p64, r64 = run(0)
+    p32, r32 = run(M.FLAG_MIXED)
+    pb, rb = run(M.FLAG_MIXED | M.FLAG_BF16_COARSE)
+    pb2, _ = run(M.FLAG_MIXED | M.FLAG_BF16_COARSE)
+    assert same(pb.data, pb2.data)
+    assert not same(pb.data, p32.data)
+    assert rb.iterations <= 2 * r64.iterations + 2
+    err = pb.interior() - p64.interior()
+    assert np.linalg.norm(err) / np.linalg.norm(p64.interior()) < 1e-8
+    assert np.abs(err).max() / np.abs(p64.interior()).max() < 1e-7
+
+
 # ---------------------------------------------------------------------------
 # GMRES-accelerated V-cycle (MGP_FLAG_GMRES; no reference counterpart)
 # ---------------------------------------------------------------------------
