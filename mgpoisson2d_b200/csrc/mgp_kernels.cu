@@ -390,6 +390,8 @@ struct BlockScope {
     __device__ static bool ractive() { return true; }
 };
 struct GridScope {
+    __device__ static int cta() { return blockIdx.x; }
+    __device__ static int ncta() { return gridDim.x; }
     static constexpr bool kGrid = true;
     static constexpr bool kCluster = false;
     __device__ static int rank() { return blockIdx.x * blockDim.x + threadIdx.x; }
@@ -418,16 +420,28 @@ __device__ __forceinline__ void cluster_barrier() {
 // one-CTA kernel; the result reaches the other CTAs through global memory.
 // Otherwise every CTA accumulates its share and the CTAs' partials are
 // combined in CTA order, as in GridScope.
+// Ranks count within the cluster (%cluster_ctarank), so a grid of several
+// clusters runs one coarse cycle per cluster.
 template <bool kOrdered>
 struct ClusterScope {
     static constexpr bool kGrid = true;
     static constexpr bool kCluster = kOrdered;
-    __device__ static int rank() { return blockIdx.x * blockDim.x + threadIdx.x; }
-    __device__ static int size() { return gridDim.x * blockDim.x; }
+    __device__ static int cta() {
+        unsigned r;
+        asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+        return (int)r;
+    }
+    __device__ static int ncta() {
+        unsigned r;
+        asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+        return (int)r;
+    }
+    __device__ static int rank() { return cta() * blockDim.x + threadIdx.x; }
+    __device__ static int size() { return ncta() * blockDim.x; }
     __device__ static void sync() { cluster_barrier(); }
     __device__ static int rrank() { return kOrdered ? (int)threadIdx.x : rank(); }
     __device__ static int rsize() { return kOrdered ? (int)blockDim.x : size(); }
-    __device__ static bool ractive() { return !kOrdered || blockIdx.x == 0; }
+    __device__ static bool ractive() { return !kOrdered || cta() == 0; }
 };
 #define SLOOP(k, n) for (int k = S::rank(); k < (n); k += S::size())
 #define RLOOP(k, n) for (int k = S::rrank(); S::ractive() && k < (n); k += S::rsize())
@@ -1195,8 +1209,8 @@ __device__ double b_reduce(double v, double* sh) {
     if constexpr (!S::kGrid) {
         return sh[32];
     } else if constexpr (S::kCluster) {
-        volatile double* part = s_gctl.part + (s_gred & 1) * gridDim.x;
-        if (blockIdx.x == 0 && threadIdx.x == 0) part[0] = sh[32];
+        volatile double* part = s_gctl.part + (s_gred & 1) * S::ncta();
+        if (S::cta() == 0 && threadIdx.x == 0) part[0] = sh[32];
         S::sync();
         if (threadIdx.x == 0) {
             sh[33] = part[0];
@@ -1205,12 +1219,12 @@ __device__ double b_reduce(double v, double* sh) {
         __syncthreads();
         return sh[33];
     } else {
-        volatile double* part = s_gctl.part + (s_gred & 1) * gridDim.x;
-        if (threadIdx.x == 0) part[blockIdx.x] = sh[32];
+        volatile double* part = s_gctl.part + (s_gred & 1) * S::ncta();
+        if (threadIdx.x == 0) part[S::cta()] = sh[32];
         S::sync();
         if (threadIdx.x == 0) {
             double t = part[0];
-            for (int c = 1; c < (int)gridDim.x; ++c) t = kMax ? fmax(t, part[c]) : t + part[c];
+            for (int c = 1; c < S::ncta(); ++c) t = kMax ? fmax(t, part[c]) : t + part[c];
             sh[33] = t;
             s_gred = s_gred + 1;
         }
