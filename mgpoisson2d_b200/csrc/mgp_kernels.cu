@@ -13,6 +13,7 @@
 #include <atomic>
 
 #include <mutex>
+#include <utility>
 
 #include <cuda_bf16.h>
 
@@ -35,6 +36,34 @@ static inline dim3 cells_grid(int nx, int ny, dim3 blk) {
 static const dim3 kBlk2(32, 8);
 constexpr int kBlk2N = 256;   // threads of a kBlk2 block (a power of two: the per-block reduction trees)
 
+// Programmatic dependent launch for the V-cycle's small kernels (the sweeps
+// do the same in mgp_sweep.cu): launched with the programmatic serialization
+// attribute, a kernel may be scheduled while the kernel ahead of it in the
+// stream is still running; pdl_wait() at its start returns once that kernel
+// has completed and its writes are visible (at once when nothing is
+// pending), before this kernel reads or writes anything that kernel may
+// touch, so the semantics are those of plain stream order and the gain is
+// the launch and scheduling latency.  pdl_allow() lets the next kernel be
+// scheduled in turn.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_allow() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <class... KArgs, class... Args>
+static cudaError_t launch_dep(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+}
+
 #define CELL_IJ                                              \
     const int i = blockIdx.x * blockDim.x + threadIdx.x;   \
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -46,6 +75,8 @@ constexpr int kBlk2N = 256;   // threads of a kBlk2 block (a power of two: the p
 // (used when no side's fill reads another side's ghosts).
 template <class T>
 __global__ void k_fill(DFT<T> p, GeoT<T> g, BCd b, int homog, int do_neum, int nx, int ny, int phase) {
+    pdl_wait();
+    pdl_allow();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     int lo[4], cnt[4];
     for (int s = 0; s < 4; ++s) side_range(b, s, nx, ny, do_neum, lo[s], cnt[s]);
@@ -58,6 +89,27 @@ __global__ void k_fill(DFT<T> p, GeoT<T> g, BCd b, int homog, int do_neum, int n
         }
     }
     if (phase >= 2 && k < 4) fill_corner(p, b, nx, ny, k);
+}
+
+// The three phases of k_fill (x sides, y sides, corners) in one CTA, a
+// barrier between them: the same element operations in the same phase order.
+constexpr int kFill3Threads = 1024;
+template <class T>
+__global__ void __launch_bounds__(kFill3Threads) k_fill3(DFT<T> p, GeoT<T> g, BCd b, int homog, int do_neum, int nx,
+                                                          int ny) {
+    pdl_wait();
+    pdl_allow();
+    int lo[4], cnt[4];
+    for (int s = 0; s < 4; ++s) side_range(b, s, nx, ny, do_neum, lo[s], cnt[s]);
+    for (int ph = 0; ph < 2; ++ph) {
+        const int s0 = 2 * ph, n = cnt[s0] + cnt[s0 + 1];
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            if (k < cnt[s0]) fill_side_elem(p, g, b, homog, s0, nx, ny, lo[s0] + k);
+            else fill_side_elem(p, g, b, homog, s0 + 1, nx, ny, lo[s0 + 1] + k - cnt[s0]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) fill_corner(p, b, nx, ny, threadIdx.x);
 }
 
 static bool fill_single_phase(const BCd& b, int do_neum) {
@@ -75,14 +127,19 @@ cudaError_t fill_impl(const DFT<T>& p, const GeoT<T>& g, const BCd& b, int homog
                       cudaStream_t st) {
     const int n = 2 * (nx + ny) + 12;
     const int blk = 256, grd = (n + blk - 1) / blk;
+    cudaError_t e = cudaSuccess;
     if (fill_single_phase(b, do_neum)) {
-        k_fill<<<grd, blk, 0, st>>>(p, g, b, homog, do_neum, nx, ny, 3);
+        e = launch_dep(k_fill<T>, dim3(grd), dim3(blk), 0, st, p, g, b, homog, do_neum, nx, ny, 3);
+        count_launch();
+    } else if (n <= 8 * kFill3Threads) {
+        e = launch_dep(k_fill3<T>, dim3(1), dim3(kFill3Threads), 0, st, p, g, b, homog, do_neum, nx, ny);
         count_launch();
     } else {
-        for (int ph = 0; ph < 3; ++ph) k_fill<<<grd, blk, 0, st>>>(p, g, b, homog, do_neum, nx, ny, ph);
+        for (int ph = 0; ph < 3 && e == cudaSuccess; ++ph)
+            e = launch_dep(k_fill<T>, dim3(grd), dim3(blk), 0, st, p, g, b, homog, do_neum, nx, ny, ph);
         count_launch(3);
     }
-    return cudaGetLastError();
+    return e;
 }
 cudaError_t launch_fill(const DF& p, const Geo& g, const BCd& b, int homog, int do_neum, int nx, int ny,
                         cudaStream_t st) {
@@ -559,6 +616,8 @@ __global__ void __launch_bounds__(kBlk2N) k_resid_restrict(DFT<T> phi, DFT<T> rh
                                                            int ny, DFT<TC> rc, DFT<TC> ec, DFT<TC> invdc, int ncx,
                                                            int ncy, int refx, int refy, int guess) {
     __shared__ T w[8][33];
+    pdl_wait();
+    pdl_allow();
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int i = blockIdx.x * 32 + tx, j = blockIdx.y * 8 + ty;
     T v = T(0.0);
@@ -582,10 +641,10 @@ cudaError_t resid_restrict_impl(const DFT<T>& phi, const DFT<T>& rhs, const GeoT
                                 int nx, int ny, const DFT<TC>& rc, const DFT<TC>& ec, const DFT<TC>& invdc, int ncx,
                                 int ncy, int refx, int refy, int guess, cudaStream_t st) {
     if (kBlk2.x != 32 || kBlk2.y != 8 || refx < 1 || refx > 2 || refy < 1 || refy > 2) return cudaErrorInvalidValue;
-    k_resid_restrict<<<cells_grid(nx, ny, kBlk2), kBlk2, 0, st>>>(phi, rhs, g, b, homog, nx, ny, rc, ec, invdc, ncx,
-                                                                   ncy, refx, refy, guess);
+    const cudaError_t e = launch_dep(k_resid_restrict<T, TC>, cells_grid(nx, ny, kBlk2), kBlk2, 0, st, phi, rhs, g, b,
+                                     homog, nx, ny, rc, ec, invdc, ncx, ncy, refx, refy, guess);
     count_launch();
-    return cudaGetLastError();
+    return e;
 }
 cudaError_t launch_resid_restrict(const DF& phi, const DF& rhs, const Geo& g, const BCd& b, int homog, int nx, int ny,
                                   const DF& rc, const DF& ec, const DF& invdc, int ncx, int ncy, int refx, int refy,
@@ -638,6 +697,8 @@ __device__ __forceinline__ void prolong_cross_cell(const DF& fine, const DF& crs
 
 template <class TF, class TC>
 __global__ void k_prolong(DFT<TF> fine, DFT<TC> crse, int ncx, int ncy, int refx, int refy, int order) {
+    pdl_wait();
+    pdl_allow();
     const int ci = blockIdx.x * blockDim.x + threadIdx.x;
     const int cj = blockIdx.y * blockDim.y + threadIdx.y;
     if (ci >= ncx || cj >= ncy) return;
@@ -653,22 +714,25 @@ __global__ void k_prolong_cross(DF fine, DF crse, int ncx, int ncy) {
 
 cudaError_t launch_prolong(const DF& fine, const DF& crse, int ncx, int ncy, int refx, int refy, int order,
                            cudaStream_t st) {
-    k_prolong<<<cells_grid(ncx, ncy, kBlk2), kBlk2, 0, st>>>(fine, crse, ncx, ncy, refx, refy, order);
+    const cudaError_t e = launch_dep(k_prolong<double, double>, cells_grid(ncx, ncy, kBlk2), kBlk2, 0, st, fine, crse, ncx,
+                                     ncy, refx, refy, order);
     count_launch();
-    return cudaGetLastError();
+    return e;
 }
 
 cudaError_t launch_prolong(const DF32& fine, const DF32& crse, int ncx, int ncy, int refx, int refy, int order,
                            cudaStream_t st) {
-    k_prolong<<<cells_grid(ncx, ncy, kBlk2), kBlk2, 0, st>>>(fine, crse, ncx, ncy, refx, refy, order);
+    const cudaError_t e = launch_dep(k_prolong<float, float>, cells_grid(ncx, ncy, kBlk2), kBlk2, 0, st, fine, crse, ncx,
+                                     ncy, refx, refy, order);
     count_launch();
-    return cudaGetLastError();
+    return e;
 }
 cudaError_t launch_prolong(const DF32& fine, const DF& crse, int ncx, int ncy, int refx, int refy, int order,
                            cudaStream_t st) {
-    k_prolong<<<cells_grid(ncx, ncy, kBlk2), kBlk2, 0, st>>>(fine, crse, ncx, ncy, refx, refy, order);
+    const cudaError_t e = launch_dep(k_prolong<float, double>, cells_grid(ncx, ncy, kBlk2), kBlk2, 0, st, fine, crse, ncx,
+                                     ncy, refx, refy, order);
     count_launch();
-    return cudaGetLastError();
+    return e;
 }
 
 cudaError_t launch_prolong_cross(const DF& fine, const DF& crse, int ncx, int ncy, cudaStream_t st) {
@@ -2020,6 +2084,15 @@ constexpr int kDirectApplyThreads = 256;
 __global__ void __launch_bounds__(kDirectApplyThreads) k_direct_apply(DF e, DF r, const double* ainv, int nx,
                                                                       int n) {
     __shared__ double rs[kDirectLargeCells];
+    // the inverse is fixed: its rows go to L2 while the kernel ahead finishes
+    {
+        const char* base = reinterpret_cast<const char*>(ainv + (long)blockIdx.x * (kDirectApplyThreads / 32) * n);
+        const long bytes = (long)min(kDirectApplyThreads / 32, n - (int)blockIdx.x * (kDirectApplyThreads / 32)) * n * 8;
+        for (long o = (long)threadIdx.x * 128; o < bytes; o += (long)blockDim.x * 128)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(base + o));
+    }
+    pdl_wait();
+    pdl_allow();
     for (int m = threadIdx.x; m < n; m += blockDim.x) rs[m] = AT(r, m % nx, m / nx);
     __syncthreads();
     const int k = blockIdx.x * (kDirectApplyThreads / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
@@ -2034,9 +2107,10 @@ __global__ void __launch_bounds__(kDirectApplyThreads) k_direct_apply(DF e, DF r
 
 cudaError_t launch_direct_apply(const DF& e, const DF& r, const double* ainv, int nx, int ny, cudaStream_t st) {
     const int n = nx * ny, w = kDirectApplyThreads / 32;
-    k_direct_apply<<<(n + w - 1) / w, kDirectApplyThreads, 0, st>>>(e, r, ainv, nx, n);
+    const cudaError_t err = launch_dep(k_direct_apply, dim3((n + w - 1) / w), dim3(kDirectApplyThreads), 0, st, e, r,
+                                       ainv, nx, n);
     count_launch();
-    return cudaGetLastError();
+    return err;
 }
 
 // The exact bottoms of a lockstep batch (MGP_FLAG_DIRECT_LARGE): job k owns

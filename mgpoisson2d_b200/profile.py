@@ -1,10 +1,12 @@
 """A short, fixed run of the benchmark workload for profilers:
 
     python -m mgpoisson2d_b200.profile [--n 1024] [--vcycles 2] [--warmup 1] [--mixed] [--krylov | --gmres]
-                                       [--workload wavy|skew] [--direct [--direct-large]]
+                                       [--workload wavy|skew|served] [--served-index K] [--direct [--direct-large]]
 
 Builds the resident solver for the stretched mapped grid (wavy: the bench
-workload; skew: the skewed boundary-layer manufactured problem), runs `warmup` solves capped at `vcycles` V-cycles, then one more,
+workload; skew: the skewed boundary-layer manufactured problem; served:
+problem K of the served pool, sides log-uniform in [32, 2048] rounded to 8,
+seed 5, e.g. K = 44, 1160 x 1720, whose coarse cycle starts at 145 x 215), runs `warmup` solves capped at `vcycles` V-cycles, then one more,
 and prints the device time per V-cycle.  Under ncu, the kernels of the last
 solve follow those of the warm-up solves in launch order.
 """
@@ -27,7 +29,8 @@ def main():
     p.add_argument("--direct-large", action="store_true",
                    help="with --direct: the exact bottom on the first level of at most 1024 cells "
                         "(MGP_FLAG_DIRECT_LARGE)")
-    p.add_argument("--workload", default="wavy", choices=["wavy", "skew"])
+    p.add_argument("--workload", default="wavy", choices=["wavy", "skew", "served"])
+    p.add_argument("--served-index", type=int, default=44, help="with --workload served: the pool problem")
     p.add_argument("--time-smoother", action="store_true", help="also report the finest level's time per sweep")
     p.add_argument("--batch", type=int, default=0,
                    help="instead: a lockstep batch of this many problems of the batched workload "
@@ -47,6 +50,9 @@ def main():
     if a.workload == "wavy":
         v, geo, rhs, bc, _ = W.wavy_stretched(a.n)
         homog = True
+    elif a.workload == "served":
+        v, geo, rhs, bc = W.batch_problem_device(a.served_index, seed=5, nmin=32, nmax=2048, round_to=8)
+        homog = True
     else:
         v, geo, rhs, bc, _ = W.skew_stretched_device(a.n)
         homog = False
@@ -58,6 +64,8 @@ def main():
     flags |= M.FLAG_DIRECT_LARGE if a.direct_large else 0
     s = M.Solver(v, geo, bc, kind, flags)
     phi, f = BoxData.device_zeros(v, 1, 1), (rhs.to_device() if a.workload == "wavy" else rhs)
+    if a.workload == "served":
+        a.n = f"{v.nx}x{v.ny}"
     if a.dd:
         f.data /= geo.J.to_device().data[1:-1, 1:-1]
     run = (lambda: s.dc_vcycle(phi, f, bc, homog, 1e-10, a.vcycles, 1, 8, 8, 8)) if a.dd else \
