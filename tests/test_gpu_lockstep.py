@@ -154,3 +154,25 @@ def test_lockstep_autotune_keeps_fastest_and_caches(M, probs, tmp_path):
     with M.Batch([(p[0], p[1], p[3]) for p in sub], M.KIND_MG, flags | M.FLAG_LOCKSTEP, nstreams=4) as b:
         again = b.autotune(phis, *args, cache_path=cache, key="six")
         assert again["cached"] and b.tuning() == {"groups": got["groups"], "pairs": got["pairs"]}
+
+
+def test_cluster_coarse_cycle_same_bits_as_lockstep(M):
+    """A coarse level of 2 K - 8 K cells that one CTA cannot stage (sides
+    8 x 61 and 8 x 45 stop the schedule at 61 x 45) runs on a thread-block
+    cluster when the problem is solved alone and on one CTA in a lockstep
+    batch; the cluster keeps the one-CTA reduction order, so the bits agree."""
+    probs = [W.skew_stretched(360, nx=488), W.skew_stretched(488, nx=360)]
+    flags = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_MIXED
+    alone = []
+    for v, geo, rhs, bc, _ in probs:
+        with M.Solver(v, geo, bc, M.KIND_MG, flags) as s:
+            phi = BoxData(v, 1, 1)
+            rep = s.vcycle(phi, rhs, bc, False, 1e-10, 60)
+        assert rep.final_relres <= 1e-10
+        alone.append((rep.iterations, phi.interior().copy()))
+    phis = [BoxData(p[0], 1, 1) for p in probs]
+    with M.Batch([(p[0], p[1], p[3]) for p in probs], M.KIND_MG, flags | M.FLAG_LOCKSTEP) as b:
+        reps = b.vcycle(phis, [p[2] for p in probs], [p[3] for p in probs], False, 1e-10, 60)
+    for k in range(2):
+        assert reps[k].iterations == alone[k][0]
+        assert np.array_equal(phis[k].interior().view(np.uint64), alone[k][1].view(np.uint64))
