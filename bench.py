@@ -6,7 +6,7 @@ x sides, Neumann y sides; seeded 16-mode Fourier rhs, J-weighted mean removed).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 One step = one full solve (until |r|/|r0| <= 1e-10) of that problem.  The
-default solver is the V-cycle accelerated by restarted GMRES(64)
+default solver is the V-cycle accelerated by restarted GMRES(128)
 (MGP_FLAG_GMRES: one V-cycle per preconditioner application) with the
 V-cycle's grid levels in FP32 inside the FP64 outer iteration
 (MGP_FLAG_MIXED) and its bottom solved exactly on the 32 x 32 level

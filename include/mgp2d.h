@@ -159,7 +159,7 @@ typedef struct mgp_report {
 /* vcycle only: accelerate the V-cycle with restarted GMRES instead of
  * BiCGStab (takes precedence over MGP_FLAG_KRYLOV): right-preconditioned
  * GMRES(m) on L_h e = r0 with one V-cycle per preconditioner application,
- * one pass of classical Gram-Schmidt, m = 64 (fewer if the 2m + 1 stored
+ * one pass of classical Gram-Schmidt, m = 128 (fewer if the 2m + 1 stored
  * vectors would take more than a quarter of the free device memory).
  * report.iterations and the relres history count V-cycles (the GMRES
  * residual estimate); final_relres is the true residual recomputed at the

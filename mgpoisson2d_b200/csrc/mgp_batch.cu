@@ -32,6 +32,7 @@ int record_error(int code, const char* msg);
 int solver_create_on(const mgp_box* valid, const mgp_geo* geo, const mgp_bdry* bc, int kind, int flags,
                      int maxdepth_user, cudaStream_t st, mgp_solver** out);
 size_t solver_device_bytes(const mgp_solver* s);
+size_t solver_pool_cached_bytes();
 struct Lockstep;
 Lockstep* lockstep_new();
 void lockstep_free(Lockstep* ls);
@@ -52,12 +53,12 @@ double now_s() {
 // Device bytes a hierarchy of nx x ny cells takes, before it exists: FP64
 // fields ~21 per cell over all levels (geometry, inverse diagonal,
 // corrections, residuals, the BiCGStab vectors), FP32 copies ~14, with
-// MGP_FLAG_GMRES the 2m + 1 = 129 stored fields of GMRES(64), plus padding
+// MGP_FLAG_GMRES the 2m + 1 = 257 stored fields of GMRES(128), plus padding
 // and the small buffers.
 size_t estimate_bytes(const mgp_box* v, int flags) {
     const double n = (double)v->nx * (double)v->ny;
     const double per = 8.0 * 21.0 + ((flags & MGP_FLAG_MIXED) ? 4.0 * 14.0 : 0.0) +
-                       ((flags & MGP_FLAG_GMRES) ? 8.0 * 129.0 : 0.0);
+                       ((flags & MGP_FLAG_GMRES) ? 8.0 * 257.0 : 0.0);
     return (size_t)(n * per) + ((size_t)8 << 20);
 }
 
@@ -434,6 +435,7 @@ int mgp_server_create(int nworkers, size_t mem_budget, int flags, mgp_server** o
             delete S;
             return record_error(MGP_ECUDA, "server_create: cudaMemGetInfo failed");
         }
+        fr += solver_pool_cached_bytes();   // freed solver memory the pool keeps serves new solvers too
         mem_budget = fr / 10 * 9;
     }
     S->budget = mem_budget;

@@ -51,7 +51,7 @@ int set_err(int code, const char* fmt, ...) {
     } while (0)
 
 // GMRES restart length and the blocks of its many-vector reductions.
-constexpr int kGmresRestart = 64;
+constexpr int kGmresRestart = 128;
 constexpr int kGmresBlocks = 296;
 
 // Levels with at most this many cells run inside the single-CTA coarse cycle.
@@ -72,7 +72,11 @@ constexpr long kClusterCoarseCells = 1L << 17;
 // milliseconds, a reuse from the pool microseconds.  Where the device has no
 // memory pools the plain calls are used.
 // ---------------------------------------------------------------------------
-constexpr unsigned long long kPoolKeepBytes = 4ull << 30;
+// The pool keeps an eighth of the device's memory (at least 4 GB) once
+// freed: enough for a resident hierarchy with GMRES's stored vectors and a
+// one-shot call's own beside it (2.7 GB each at 1024^2), so the one-shot
+// drivers reuse memory instead of returning and re-mapping it per call.
+constexpr unsigned long long kPoolKeepMinBytes = 4ull << 30;
 
 cudaMemPool_t solver_pool() {
     static std::mutex mu;
@@ -92,7 +96,12 @@ cudaMemPool_t solver_pool() {
         props.location.type = cudaMemLocationTypeDevice;
         props.location.id = dev;
         cudaMemPool_t p = nullptr;
-        unsigned long long keep = kPoolKeepBytes;
+        size_t freeb = 0, totalb = 0;
+        if (cudaMemGetInfo(&freeb, &totalb) != cudaSuccess) {
+            cudaGetLastError();
+            totalb = 0;
+        }
+        unsigned long long keep = std::max<unsigned long long>(kPoolKeepMinBytes, totalb / 8);
         if (cudaDeviceGetAttribute(&supported, cudaDevAttrMemoryPoolsSupported, dev) == cudaSuccess && supported &&
             cudaMemPoolCreate(&p, &props) == cudaSuccess &&
             cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep) == cudaSuccess)
@@ -1675,8 +1684,27 @@ int solver_create_on(const mgp_box* valid, const mgp_geo* geo, const mgp_bdry* b
 }
 size_t solver_device_bytes(const mgp_solver* s) {
     if (!s) return 0;
-    return (s->fixed.elems + s->state.elems) * sizeof(double) +
-           (s->fixed32.elems + s->state32.elems) * sizeof(float) + (size_t)s->shadow_bytes;
+    size_t bytes = (s->fixed.elems + s->state.elems) * sizeof(double) +
+                   (s->fixed32.elems + s->state32.elems) * sizeof(float) + (size_t)s->shadow_bytes;
+    if (s->gm_base) bytes += (size_t)(2 * s->gm_m + 1) * s->gm_vec * sizeof(double);   // GMRES's stored vectors
+    if (s->d_ainv && s->db >= 0) {   // the exact bottom's inverse
+        const size_t n = (size_t)s->lv[s->db].nx * s->lv[s->db].ny;
+        bytes += n * n * sizeof(double);
+    }
+    return bytes;
+}
+// Memory the solvers' pool on the current device holds but no solver uses
+// (freed, kept for reuse; see solver_pool): free for the next solver.
+size_t solver_pool_cached_bytes() {
+    cudaMemPool_t p = solver_pool();
+    if (!p) return 0;
+    unsigned long long reserved = 0, used = 0;
+    if (cudaMemPoolGetAttribute(p, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
+        cudaMemPoolGetAttribute(p, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return reserved > used ? (size_t)(reserved - used) : 0;
 }
 
 // ===========================================================================

@@ -2184,8 +2184,13 @@ __global__ void __launch_bounds__(kCoarseThreads, 1) k_coarse_cycle_grid(CoarseA
 // memory, where the grid version's time is its barriers.  kOrdered
 // (a.cluster == 2): the one-CTA kernel's reduction order and bits.
 static_assert(kClusterThreads == kCoarseThreads, "the cluster CTAs reduce in the one-CTA kernel's order");
+// Two CTAs an SM (128 registers, some spilled): a cluster CTA fits beside a
+// sweep CTA of another stream, so under a server's concurrent solves a
+// cluster does not wait for sixteen idle SMs in one GPC (served p99 at 10
+// requests/s 156-1162 ms over four runs with one CTA an SM, 158-207 ms with
+// two); alone it is 6 % slower on a 145 x 215 level.
 template <bool kOrdered>
-__global__ void __launch_bounds__(kClusterThreads, 1) k_coarse_cycle_cluster(CoarseArgs a) {
+__global__ void __launch_bounds__(kClusterThreads, 2) k_coarse_cycle_cluster(CoarseArgs a) {
     __shared__ double sh[64];
     if (threadIdx.x == 0) {
         s_gctl = a.gctl;

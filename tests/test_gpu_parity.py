@@ -834,12 +834,17 @@ def test_batch_matches_individual_solves(M):
         assert same(phis[k].data, pa.data) and np.array_equal(reps[k].relres, ra.relres)
 
 
-def test_server_results_same_alone_and_in_the_mix(M):
+@pytest.mark.parametrize("solver", ["krylov", "gmres_mixed"])
+def test_server_results_same_alone_and_in_the_mix(M, solver):
     """Requests overlap on the device (3 slots, 7 requests, two keys reused);
-    each result must equal the same solve run alone."""
+    each result must equal the same solve run alone (BiCGStab, and the
+    served leg's GMRES mixed with the exact bottom)."""
     from mgpoisson2d_b200 import workloads as W
     probs = [W.batch_problem(i, nmax=160) for i in range(4)]
     flags = M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV
+    if solver == "gmres_mixed":
+        flags = (M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_GMRES | M.FLAG_MIXED | M.FLAG_DIRECT_COARSE |
+                 M.FLAG_DIRECT_LARGE)
     order = [0, 1, 2, 3, 0, 1, 0]
     with M.Server(nworkers=3, flags=flags) as srv:
         outs, tickets = [], []
