@@ -112,6 +112,37 @@ cudaMemPool_t solver_pool() {
     return pools[dev];
 }
 
+// Memory the pool holds but no solver uses (freed, kept for reuse).
+size_t pool_cached_bytes() {
+    cudaMemPool_t p = solver_pool();
+    if (!p) return 0;
+    unsigned long long reserved = 0, used = 0;
+    if (cudaMemPoolGetAttribute(p, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
+        cudaMemPoolGetAttribute(p, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return reserved > used ? (size_t)(reserved - used) : 0;
+}
+
+// The current device's total memory, queried once per device.
+size_t device_total_bytes() {
+    static std::mutex mu;
+    static size_t total[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return 0;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!total[dev]) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) total[dev] = tot;
+        else cudaGetLastError();
+    }
+    return total[dev];
+}
+
 // Allocation ordered on stream st (usable there at once, elsewhere after st is synchronised).
 cudaError_t dmalloc(void** p, size_t bytes, cudaStream_t st) {
     if (cudaMemPool_t pool = solver_pool()) return cudaMallocFromPoolAsync(p, bytes, pool, st);
@@ -760,10 +791,18 @@ int solver_build(mgp_solver* s, const mgp_box* valid, const mgp_geo* geo, const 
     if ((s->flags & MGP_FLAG_GMRES) && s->kind == MGP_KIND_MG) {
         s->gm_ld = (size_t)valid->nx + 2;
         s->gm_vec = s->gm_ld * (valid->ny + 2);
-        size_t freeb = 0, totalb = 0;
-        CK(cudaMemGetInfo(&freeb, &totalb));
+        // m = kGmresRestart unless the 2m + 1 vectors would take more than a
+        // quarter of the memory free for solvers (the device's free memory
+        // and what the pool keeps); a request of at most 1/16 of the device
+        // skips the query
         int m = kGmresRestart;
-        while (m > 8 && (size_t)(2 * m + 1) * s->gm_vec * sizeof(double) > freeb / 4) m /= 2;
+        const size_t want = (size_t)(2 * m + 1) * s->gm_vec * sizeof(double);
+        if (want > device_total_bytes() / 16) {
+            size_t freeb = 0, totalb = 0;
+            CK(cudaMemGetInfo(&freeb, &totalb));
+            freeb += pool_cached_bytes();
+            while (m > 8 && (size_t)(2 * m + 1) * s->gm_vec * sizeof(double) > freeb / 4) m /= 2;
+        }
         s->gm_m = m;
         if (dmalloc(&s->gm_base, (size_t)(2 * m + 1) * s->gm_vec * sizeof(double), st) != cudaSuccess ||
             dmalloc(&s->gm_red, sizeof(double) * ((size_t)kGmresBlocks * (m + 1) + 2 * (m + 1)), st) !=
@@ -1695,17 +1734,7 @@ size_t solver_device_bytes(const mgp_solver* s) {
 }
 // Memory the solvers' pool on the current device holds but no solver uses
 // (freed, kept for reuse; see solver_pool): free for the next solver.
-size_t solver_pool_cached_bytes() {
-    cudaMemPool_t p = solver_pool();
-    if (!p) return 0;
-    unsigned long long reserved = 0, used = 0;
-    if (cudaMemPoolGetAttribute(p, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
-        cudaMemPoolGetAttribute(p, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
-    return reserved > used ? (size_t)(reserved - used) : 0;
-}
+size_t solver_pool_cached_bytes() { return pool_cached_bytes(); }
 
 // ===========================================================================
 // Lockstep batches (mgp_batch_* with MGP_FLAG_LOCKSTEP): the stationary

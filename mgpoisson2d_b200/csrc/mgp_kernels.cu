@@ -1885,31 +1885,31 @@ cudaError_t launch_direct_columns(const Lv& L, double* scratch, double* A, cudaS
 constexpr int kGjThreads = 256;
 constexpr int kGjRows = 32;   // rows of X per CTA and step
 
-// X = [A | I]; mark[r] = n (unused); fail = 0; amax = max |A| (CTA 0, in order of threads, then a tree).
-__global__ void __launch_bounds__(kGjThreads) k_gj_init(const double* A, int n, double* X, int* mark, int* fail,
-                                                        double* amax) {
+// X = [A | I]; mark[r] = n (unused); amax = max |A| over the entries that are
+// not NaN (fmax's rule), as the bit pattern of a non-negative double, whose
+// integer order is its numeric order: every CTA's maximum goes in by an
+// atomic max on a word zeroed before the launch, which gives the exact
+// maximum whatever the order.  An amax of 0 fails the first pivot test.
+__global__ void __launch_bounds__(kGjThreads) k_gj_init(const double* A, int n, double* X, int* mark,
+                                                        unsigned long long* amax_bits) {
     const long nn = (long)n * n;
+    double m = 0.0;
     for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < nn; q += (long)gridDim.x * blockDim.x) {
         const long r = q / n, k = q - r * n;
-        X[r * 2 * n + k] = A[q];
+        const double a = A[q];
+        X[r * 2 * n + k] = a;
         X[r * 2 * n + n + k] = (r == k) ? 1.0 : 0.0;
+        m = fmax(m, fabs(a));
     }
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) mark[r] = n;
-    if (blockIdx.x == 0) {
-        __shared__ double sh[kGjThreads];
-        double m = 0.0;
-        for (long q = threadIdx.x; q < nn; q += blockDim.x) m = fmax(m, fabs(A[q]));
-        sh[threadIdx.x] = m;
+    __shared__ double sh[kGjThreads];
+    sh[threadIdx.x] = m;
+    __syncthreads();
+    for (int h = kGjThreads / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + h]);
         __syncthreads();
-        for (int h = kGjThreads / 2; h > 0; h >>= 1) {
-            if (threadIdx.x < h) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + h]);
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) {
-            *amax = sh[0];
-            *fail = !(sh[0] > 0.0);
-        }
     }
+    if (threadIdx.x == 0) atomicMax(amax_bits, (unsigned long long)__double_as_longlong(sh[0]));
 }
 
 // ainv[c][m] = X[prow[c]][n + m] (nothing after a failed step: prow is then incomplete).
@@ -1942,8 +1942,8 @@ __global__ void __launch_bounds__(kGjPanelThreads) k_gj_panel(const double* __re
     __shared__ double sv[kGjPanelThreads / 32];
     __shared__ int sr[kGjPanelThreads / 32];
     __shared__ double prowv[kGjPanel];
-    __shared__ int sp;
     if (*fail) return;
+    const double amx = *amax;   // read once: the stores below may alias it as far as the compiler knows
     const int r = threadIdx.x;
     const bool live = r < n;
     double x[kGjPanel];
@@ -1965,18 +1965,18 @@ __global__ void __launch_bounds__(kGjPanelThreads) k_gj_panel(const double* __re
         }
         if (lane == 0) { sv[wid] = best; sr[wid] = br; }
         __syncthreads();
-        if (wid == 0) {
-            best = lane < kGjPanelThreads / 32 ? sv[lane] : -1.0;
-            br = lane < kGjPanelThreads / 32 ? sr[lane] : n;
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ob = __shfl_down_sync(0xffffffffu, best, o);
-                const int orr = __shfl_down_sync(0xffffffffu, br, o);
-                if (ob > best || (ob == best && orr < br)) { best = ob; br = orr; }
-            }
-            if (lane == 0) sp = br;
+        // every warp combines the warps' candidates by the same tree, so all
+        // agree on the pivot without another barrier (the next writes of
+        // sv / sr come after the barrier below, which every warp reaches
+        // only when done reading them)
+        best = lane < kGjPanelThreads / 32 ? sv[lane] : -1.0;
+        br = lane < kGjPanelThreads / 32 ? sr[lane] : n;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_down_sync(0xffffffffu, best, o);
+            const int orr = __shfl_down_sync(0xffffffffu, br, o);
+            if (ob > best || (ob == best && orr < br)) { best = ob; br = orr; }
         }
-        __syncthreads();
-        const int p = sp;
+        const int p = __shfl_sync(0xffffffffu, br, 0);
         if (p >= n) {
             if (r == 0) *fail = 1;
             return;
@@ -1987,7 +1987,7 @@ __global__ void __launch_bounds__(kGjPanelThreads) k_gj_panel(const double* __re
         }
         __syncthreads();
         const double piv = prowv[j];
-        if (!(fabs(piv) > 1e-13 * *amax)) {
+        if (!(fabs(piv) > 1e-13 * amx)) {
             if (r == 0) *fail = 1;
             return;
         }
@@ -2006,7 +2006,8 @@ __global__ void __launch_bounds__(kGjPanelThreads) k_gj_panel(const double* __re
             const double sk = prowv[q] * ip;
             x[q] = (r == p) ? sk : x[q] - fj * sk;
         }
-        __syncthreads();   // prowv is rewritten by the next step's pivot row
+        // prowv is rewritten by the next step's pivot row only after the
+        // next step's first barrier, which every thread reaches after this read
     }
 }
 
@@ -2057,7 +2058,10 @@ cudaError_t launch_invert(const double* A, int n, double* ainv, double* work, in
     int *mark = iwork, *prow = iwork + n, *fail = iwork + 2 * n;
     if (n > kGjPanelThreads) return cudaErrorNotSupported;
     const int nb = std::min(1184, (int)((2L * n * n + kGjThreads - 1) / kGjThreads));
-    k_gj_init<<<nb, kGjThreads, 0, st>>>(A, n, X0, mark, fail, amax);
+    cudaError_t e = cudaMemsetAsync(amax, 0, sizeof(double), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(fail, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    k_gj_init<<<nb, kGjThreads, 0, st>>>(A, n, X0, mark, reinterpret_cast<unsigned long long*>(amax));
     int launches = 2, cur = 0;
     for (int c0 = 0; c0 < n; c0 += kGjPanel) {
         const int b = std::min(kGjPanel, n - c0);
