@@ -38,6 +38,8 @@ At N=1 the line also carries:
     512..4096, for the BiCGStab(V-cycle) solve and the deferred-correction
     solve, with the observed order of the discretisation error, and the same
     solvers with BF16 values on the levels below the finest;
+  * "roofline_4096": the level-0 FP32 sweep timed live at 4096^2, beside the
+    headline's 1024^2 "roofline";
   * "config1": the 128^2 identity-map Dirichlet problem (V-cycles, ms per
     solve, error) for the FP64 V-cycle, the headline solver and the oracle.
 
@@ -584,6 +586,33 @@ def vcycle_bytes(M, v, mixed, direct, nu=NU, large=False):
     return total
 
 
+def roofline_large(M, n=4096):
+    """The level-0 FP32 sweep at n^2 (the skewed, stretched grid of the
+    precision study), timed live as the bench's own roofline: one mixed
+    BiCGStab(V-cycle) solve with the finest level's smoothing bracketed by
+    CUDA events (MGP_FLAG_TIME_SMOOTHER), algorithmic bytes 8 words of 4 B a
+    cell per sweep."""
+    import torch
+    from mgpoisson2d_b200 import workloads as W
+    from mgpoisson2d_b200.types import BoxData
+    v, geo, rhs, bc, _ = W.skew_stretched_device(n)
+    fl = (M.FLAG_DIRICHLET_COUPLED_DIAG | M.FLAG_KRYLOV | M.FLAG_MIXED | M.FLAG_DIRECT_COARSE |
+          M.FLAG_TIME_SMOOTHER)
+    with M.Solver(v, geo, bc, M.KIND_MG, fl) as s:
+        phi = BoxData.device_zeros(v, 1, 1)
+        s.vcycle(phi, rhs, bc, False, TOL, 4)   # warm-up
+        phi.data.zero_()
+        r = s.vcycle(phi, rhs, bc, False, TOL, MAXITERS)
+    sweep_s = r.smooth0_seconds / max(r.smooth0_sweeps, 1)
+    peak, kind = measured_peak()
+    alg = SWEEP_WORDS * 4 * v.nx * v.ny
+    del v, geo, rhs, bc, phi
+    torch.cuda.empty_cache()
+    return {"kernel": f"k_sweep9 level 0 (FP32 fields, TMA staging), {n}^2", "achieved": alg / sweep_s / 1e9,
+            "peak": peak, "peak_kind": kind, "unit": "GB/s", "frac": alg / sweep_s / 1e9 / peak,
+            "alg_bytes_per_sweep": alg, "sweep_us": sweep_s * 1e6, "sweeps": r.smooth0_sweeps}
+
+
 def precision_study(M, sizes):
     """Mixed precision against FP64 and against the exact solution on the
     skewed, boundary-layer-stretched manufactured problem (u = e^x cos 4 pi y,
@@ -860,6 +889,7 @@ def main():
             "served_rate_per_s": served["mixed"][0]["offered_per_s"]}
     if rank == 0 and world == 1 and not args.no_study:
         line["precision_study"] = precision_study(M, [int(x) for x in args.study_sizes.split(",") if x])
+        line["roofline_4096"] = roofline_large(M)
         line["config1"] = config1_leg(M, not args.no_cpu)
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline_1core(args.n, args.cpu_vcycles_1core)
