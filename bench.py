@@ -22,14 +22,14 @@ torchrun every rank solves its own copy (replicas; the solve does not shard)
 and rank 0 prints one JSON line.
 
 At N=1 the line also carries:
-  * "batched" (BASELINE config 4: 512 independent problems, sides
+  * "batched" (512 independent problems, sides
     log-uniform in [64,1024]): the lockstep batch (MGP_FLAG_LOCKSTEP, every
     V-cycle phase of all unconverged problems in one launch per group, knobs
     chosen by the autotuner) in mixed precision and in FP64, each against
     the same problems one at a time, and the per-problem concurrent
     BiCGStab(V-cycle) path; "batched_headline" is the metric's own
     comparison, mixed against plain FP64 with the served p50/p99;
-  * "served" (config 5: Poisson arrivals of solves drawn from 64 problems
+  * "served" (Poisson arrivals of solves drawn from 64 problems
     with sides log-uniform in [32,2048] rounded to 8, hierarchies resident,
     tolerance 1e-8 or 1e-10) at 10, 30 and 100 requests/s, stopping once p99
     diverges; --serve-sweep extends the rates to 3000/s;
@@ -40,7 +40,7 @@ At N=1 the line also carries:
     solvers with BF16 values on the levels below the finest;
   * "roofline_4096": the level-0 FP32 sweep timed live at 4096^2, beside the
     headline's 1024^2 "roofline";
-  * "config1": the 128^2 identity-map Dirichlet problem (V-cycles, ms per
+  * "identity128": the 128^2 identity-map Dirichlet problem (V-cycles, ms per
     solve, error) for the FP64 V-cycle, the headline solver and the oracle.
 
 --impl reference times the CPU restatement of the reference algorithm (the
@@ -233,10 +233,10 @@ def oracle_vcycles_per_solve(n):
     """V-cycles of the oracle's full lexicographic solve of this workload: the
     committed fixture of that solve (tests/golden/make_fixtures.py) at 1024^2,
     else the count recorded in profiles/vcycles.json."""
-    fx = os.path.join(ROOT, "tests", "golden", "config2_wavy1024.npz")
+    fx = os.path.join(ROOT, "tests", "golden", "wavy1024.npz")
     if n == 1024 and os.path.exists(fx):
         import numpy as np
-        return int(np.load(fx)["iterations"]), "tests/golden/config2_wavy1024.npz (full oracle solve, 1 core)"
+        return int(np.load(fx)["iterations"]), "tests/golden/wavy1024.npz (full oracle solve, 1 core)"
     try:
         return int(json.load(open(os.path.join(ROOT, "profiles", "vcycles.json")))[str(n)]), "profiles/vcycles.json"
     except Exception:
@@ -264,7 +264,7 @@ def cpu_baseline_1core(n, vcycles, runs=3):
             "vcycles_per_solve": vsolve, "s_per_vcycle": (sec - ts) / max(vc, 1)}
 
 
-def _cpu_config1(runs):
+def _cpu_identity128(runs):
     """Full oracle solves of the 128^2 identity-map Dirichlet problem on one
     core (lexicographic Gauss-Seidel, FP64): median seconds and V-cycles."""
     from mgpoisson2d_b200 import workloads as W
@@ -281,7 +281,7 @@ def _cpu_config1(runs):
     return sorted(secs)[len(secs) // 2], rep.iterations, float(abs(phi.interior() - u).max())
 
 
-def config1_leg(M, cpu, runs=20):
+def identity128_leg(M, cpu, runs=20):
     """The 128^2 identity-map Dirichlet problem (u = sin 2 pi x sin 3 pi y plus
     1e-3 noise in the rhs): V-cycles, ms per solve and the error against u for
     the reference's FP64 V-cycle and the headline solver, on the device (median
@@ -314,7 +314,7 @@ def config1_leg(M, cpu, runs=20):
         import multiprocessing as mp
         _cpu_oracle().build(force=False)
         with mp.get_context("spawn").Pool(1) as pool:
-            sec, its, e = pool.apply(_cpu_config1, (5,))
+            sec, its, e = pool.apply(_cpu_identity128, (5,))
         out["cpu_1core"] = {"vcycles": its, "ms_per_solve": sec * 1e3, "err_max": e, "kind": "port",
                             "sample": "median of 5 full oracle solves (-march=native, FP64, lexicographic GS)"}
     return out
@@ -890,7 +890,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_study:
         line["precision_study"] = precision_study(M, [int(x) for x in args.study_sizes.split(",") if x])
         line["roofline_4096"] = roofline_large(M)
-        line["config1"] = config1_leg(M, not args.no_cpu)
+        line["identity128"] = identity128_leg(M, not args.no_cpu)
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline_1core(args.n, args.cpu_vcycles_1core)
         line["cpu_baseline"] = cb

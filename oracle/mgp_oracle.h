@@ -1,8 +1,8 @@
 /*
  * mgp_oracle.h -- CPU restatement of the MGPoisson2D multigrid hot path.
  *
- * TEST INFRASTRUCTURE ONLY.  This code is the checker for the CUDA library in
- * mgpoisson2d_b200/ and the timed CPU baseline in bench.py.  The product never
+ * TEST INFRASTRUCTURE ONLY.  The tests check the CUDA library in
+ * mgpoisson2d_b200/ against this code, and bench.py times it as the CPU baseline.  The product never
  * links, loads or calls it.
  *
  * It restates, in C, the Fortran 90 routines of EdSantilli/MGPoisson2D

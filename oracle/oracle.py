@@ -1,7 +1,7 @@
 """Python face of the CPU oracle (oracle/mgp_oracle.c).
 
-TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as
-the checker, and by bench.py's CPU-baseline and reference legs.  The product
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() to
+check the device result, and by bench.py's CPU-baseline and reference legs.  The product
 package never imports it.
 
 Function names and argument lists follow the Fortran routines they restate

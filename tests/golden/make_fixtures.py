@@ -1,24 +1,24 @@
-"""Generate the golden fixtures of the benchmark configurations from the CPU
+"""Generate the golden fixtures of the benchmark workloads from the CPU
 oracle (oracle/mgp_oracle.c, a restatement of the reference's FP64 solve).
 
 The reference (Fortran 90) cannot be compiled where these fixtures are made
 (no Fortran compiler), so the fixtures hold the oracle's own FP64 solutions at
-the configurations' full sizes, solved in the reference's lexicographic
+the workloads' full sizes, solved in the reference's lexicographic
 Gauss-Seidel order (MGPoisson2D.f90:596-640, poisson2d.f90:1702-1812) with the
 reference settings nu = 8/8/8, numcycles = 1 and the coupled Dirichlet
 diagonal (without it the reference iteration diverges on every problem with
 two adjacent Dirichlet sides).  The GPU tests compare the device's solutions
 with them; they never run this script.
 
-    python tests/golden/make_fixtures.py [config1] [config2] [config2_colour]
+    python tests/golden/make_fixtures.py [identity128] [wavy1024] [wavy1024_colour]
 
-config1  128^2 identity map, homogeneous Dirichlet (workloads.identity_dirichlet):
-         the whole solution, the relres history.
-config2  1024^2 wavy map with 64:1 stretching, Dirichlet x / Neumann y
-         (workloads.wavy_stretched): norms of the whole solution, every 8th
-         cell in each direction (16384 values), 16384 cells at seeded random
-         positions, the relres history.  About four minutes on one core.
-config2_colour  the same solve in the device's colour order.
+identity128  128^2 identity map, homogeneous Dirichlet (workloads.identity_dirichlet):
+             the whole solution, the relres history.
+wavy1024  1024^2 wavy map with 64:1 stretching, Dirichlet x / Neumann y
+          (workloads.wavy_stretched): norms of the whole solution, every 8th
+          cell in each direction (16384 values), 16384 cells at seeded random
+          positions, the relres history.  About four minutes on one core.
+wavy1024_colour  the same solve in the device's colour order.
 
 Each fixture also records checksums of its inputs, so a test can tell an
 input that drifted (a different libm) from a solver that did.
@@ -63,14 +63,14 @@ def solve(v, geo, rhs, bc, homog, maxiters, gs_order):
     return phi.interior().copy(), rep, dt
 
 
-def config1():
+def identity128():
     v, geo, rhs, bc, u = W.identity_dirichlet(128)
     sol, rep, dt = solve(v, geo, rhs, bc, True, 100, 0)
-    out = os.path.join(HERE, "config1_identity128.npz")
+    out = os.path.join(HERE, "identity128.npz")
     np.savez_compressed(out, solution=sol, relres=rep.relres, iterations=rep.iterations, maxdepth=rep.maxdepth,
                         diverged=rep.diverged, inputs=input_sums(geo, rhs), seconds=dt,
                         err_max=np.abs(sol - u).max())
-    print(f"config1: {rep.iterations} V-cycles, relres {rep.final_relres:.3e}, {dt:.1f} s -> {out}")
+    print(f"identity128: {rep.iterations} V-cycles, relres {rep.final_relres:.3e}, {dt:.1f} s -> {out}")
 
 
 def sample_points(n, count=16384, seed=8):
@@ -78,30 +78,30 @@ def sample_points(n, count=16384, seed=8):
     return rng.integers(0, n, count), rng.integers(0, n, count)
 
 
-def config2(gs_order=0):
+def wavy1024(gs_order=0):
     n = 1024
     v, geo, rhs, bc, _ = W.wavy_stretched(n)
     sol, rep, dt = solve(v, geo, rhs, bc, True, 2000, gs_order)
     si, sj = sample_points(n)
-    name = "config2_wavy1024.npz" if gs_order == 0 else "config2_wavy1024_colour.npz"
+    name = "wavy1024.npz" if gs_order == 0 else "wavy1024_colour.npz"
     out = os.path.join(HERE, name)
     np.savez_compressed(out, strided=sol[::8, ::8].copy(), sample_i=si, sample_j=sj, sample=sol[si, sj],
                         l2=np.linalg.norm(sol), maxabs=np.abs(sol).max(), total=sol.sum(), relres=rep.relres,
                         iterations=rep.iterations, maxdepth=rep.maxdepth, diverged=rep.diverged,
                         inputs=input_sums(geo, rhs), seconds=dt, gs_order=gs_order)
-    print(f"config2 (gs_order {gs_order}): {rep.iterations} V-cycles, relres {rep.final_relres:.3e}, "
+    print(f"wavy1024 (gs_order {gs_order}): {rep.iterations} V-cycles, relres {rep.final_relres:.3e}, "
           f"{dt:.1f} s -> {out}")
 
 
 if __name__ == "__main__":
     O.build()
-    which = sys.argv[1:] or ["config1", "config2"]
+    which = sys.argv[1:] or ["identity128", "wavy1024"]
     for w in which:
-        if w == "config1":
-            config1()
-        elif w == "config2":
-            config2(0)
-        elif w == "config2_colour":
-            config2(1)
+        if w == "identity128":
+            identity128()
+        elif w == "wavy1024":
+            wavy1024(0)
+        elif w == "wavy1024_colour":
+            wavy1024(1)
         else:
             raise SystemExit(f"unknown fixture {w}")

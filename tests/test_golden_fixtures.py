@@ -1,10 +1,10 @@
 """The committed golden fixtures (tests/golden/make_fixtures.py) against the
 oracle and the workload generators, on the CPU.
 
-* config 1's fixture is reproduced bit for bit by a fresh oracle solve (the
+* the 128^2 identity-map fixture is reproduced bit for bit by a fresh oracle solve (the
   oracle is deterministic), and its solution has the manufactured solution's
   discretisation error;
-* config 2's fixture was made from the same inputs the generators give now
+* the 1024^2 stretched wavy-map fixtures were made from the same inputs the generators give now
   (checksums), and records a converged, non-diverged lexicographic solve whose
   residual history falls monotonically (the stationary V-cycle, MG:630-639).
 """
@@ -30,8 +30,8 @@ def _coupled(on):
     O.lib().or_set_dirichlet_coupled_diagonal(int(on))
 
 
-def test_config1_fixture_reproduced_by_the_oracle():
-    fx = np.load(os.path.join(GOLDEN, "config1_identity128.npz"))
+def test_identity128_fixture_reproduced_by_the_oracle():
+    fx = np.load(os.path.join(GOLDEN, "identity128.npz"))
     v, geo, rhs, bc, u = W.identity_dirichlet(128)
     np.testing.assert_allclose(input_sums(geo, rhs), fx["inputs"], rtol=1e-12, atol=1e-12)
     _coupled(True)
@@ -47,8 +47,8 @@ def test_config1_fixture_reproduced_by_the_oracle():
     assert np.abs(fx["solution"] - u).max() < 2e-3
 
 
-@pytest.mark.parametrize("name", ["config2_wavy1024.npz", "config2_wavy1024_colour.npz"])
-def test_config2_fixture_inputs_and_history(name):
+@pytest.mark.parametrize("name", ["wavy1024.npz", "wavy1024_colour.npz"])
+def test_wavy1024_fixture_inputs_and_history(name):
     path = os.path.join(GOLDEN, name)
     if not os.path.exists(path):
         pytest.skip(f"{name} not generated")

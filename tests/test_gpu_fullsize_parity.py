@@ -1,19 +1,19 @@
-"""Parity at the benchmark configurations' own sizes.
+"""Parity at the benchmark workloads' own sizes.
 
 The reference pins its FP64 solve only by manufactured-solution rates, so the
 CPU oracle (a restatement of MGPoisson2D.f90:400-670 with poisson2d.f90's
-operator and lexicographic Gauss-Seidel) is the judge of the converged
-solution.  Its solutions at full size are committed fixtures
+operator and lexicographic Gauss-Seidel) decides what the converged
+solution is.  Its solutions at full size are committed fixtures
 (tests/golden/make_fixtures.py); the device solves must agree with them within
 the tolerance for two solutions converged to relres <= 1e-10 in different
 sweep orders: relative L2 <= 1e-8 and relative max <= 1e-7.
 
-* config 1: 128^2 identity map, homogeneous Dirichlet, nu = 8/8/8;
-* config 2: 1024^2 wavy map with 64:1 stretching, Dirichlet x / Neumann y:
+* 128^2 identity map, homogeneous Dirichlet, nu = 8/8/8;
+* 1024^2 wavy map with 64:1 stretching, Dirichlet x / Neumann y:
   the reference's stationary V-cycle, the GMRES-accelerated V-cycle in FP64
   and with FP32 grid levels (the bench's headline solver), all against the
   oracle's lexicographic solution;
-* config 4: problems of the batched workload with semicoarsened schedules
+* problems of the batched workload with semicoarsened schedules
   ((2,1) and (1,2) levels), solved through mgp_batch in FP64 and mixed
   precision, each against the oracle in both sweep orders.
 """
@@ -62,8 +62,8 @@ def _inputs_match(fx, geo, rhs):
     np.testing.assert_allclose(input_sums(geo, rhs), fx["inputs"], rtol=1e-12, atol=1e-12)
 
 
-def test_config1_identity128_against_fixture(M):
-    fx = np.load(os.path.join(GOLDEN, "config1_identity128.npz"))
+def test_identity128_against_fixture(M):
+    fx = np.load(os.path.join(GOLDEN, "identity128.npz"))
     v, geo, rhs, bc, u = W.identity_dirichlet(128)
     _inputs_match(fx, geo, rhs)
     ref = fx["solution"]
@@ -73,7 +73,7 @@ def test_config1_identity128_against_fixture(M):
             phi = BoxData(v, 1, 1)
             rep = s.vcycle(phi, rhs, bc, True, 1e-10, 100)
         assert rep.final_relres <= 1e-10
-        _close(phi.interior(), ref, f"config 1 {name}")
+        _close(phi.interior(), ref, f"identity128 {name}")
         if extra == 0:   # the stationary iteration: the oracle's V-cycle count within one
             assert abs(rep.iterations - int(fx["iterations"])) <= 1
     # the Fortran-signature driver as well
@@ -83,10 +83,10 @@ def test_config1_identity128_against_fixture(M):
         rep = M.vcycle(phi, rhs, geo, bc, True, 1e-10, 100)
     finally:
         _coupled(M, old)
-    _close(phi.interior(), ref, "config 1 mgp_vcycle")
+    _close(phi.interior(), ref, "identity128 mgp_vcycle")
 
 
-def _config2_compare(phi_int, fx, what):
+def _wavy1024_compare(phi_int, fx, what):
     si, sj = fx["sample_i"], fx["sample_j"]
     _close(phi_int[::8, ::8], fx["strided"], what + " (every 8th cell)")
     _close(phi_int[si, sj], fx["sample"], what + " (random cells)")
@@ -95,8 +95,8 @@ def _config2_compare(phi_int, fx, what):
 
 
 @pytest.mark.parametrize("solver", ["vcycle_fp64", "gmres_fp64", "gmres_mixed"])
-def test_config2_wavy1024_against_fixture(M, solver):
-    path = os.path.join(GOLDEN, "config2_wavy1024.npz")
+def test_wavy1024_against_fixture(M, solver):
+    path = os.path.join(GOLDEN, "wavy1024.npz")
     fx = np.load(path)
     v, geo, rhs, bc, _ = W.wavy_stretched(1024)
     _inputs_match(fx, geo, rhs)
@@ -109,15 +109,15 @@ def test_config2_wavy1024_against_fixture(M, solver):
         phi = BoxData.device_zeros(v, 1, 1)
         rep = s.vcycle(phi, rhs.to_device(), bc, True, 1e-10, 2000)
     assert rep.final_relres <= 1e-10 and not rep.diverged
-    _config2_compare(phi.to_host().interior(), fx, f"config 2 {solver}")
+    _wavy1024_compare(phi.to_host().interior(), fx, f"wavy1024 {solver}")
 
 
-def test_config2_colour_order_fixture_matches_lexicographic():
+def test_wavy1024_colour_order_fixture_matches_lexicographic():
     """The oracle run in the device's colour order (what the stationary GPU
     iteration follows) and in the reference's lexicographic order converge to
     the same solution: the sweep order changes the path, not the answer."""
-    a = np.load(os.path.join(GOLDEN, "config2_wavy1024.npz"))
-    b_path = os.path.join(GOLDEN, "config2_wavy1024_colour.npz")
+    a = np.load(os.path.join(GOLDEN, "wavy1024.npz"))
+    b_path = os.path.join(GOLDEN, "wavy1024_colour.npz")
     if not os.path.exists(b_path):
         pytest.skip("colour-order fixture not generated")
     b = np.load(b_path)
@@ -126,12 +126,12 @@ def test_config2_colour_order_fixture_matches_lexicographic():
 
 # problems of the batched workload (sides log-uniform in [64, 1024] rounded to
 # 16): 2, 5, 8 and 6 coarsen (2,1) first, 7 and 13 coarsen (1,2) first
-CONFIG4 = [0, 1, 2, 5, 6, 7, 8, 13]
+BATCH_PROBS = [0, 1, 2, 5, 6, 7, 8, 13]
 
 
 @pytest.mark.parametrize("mixed", [False, True])
-def test_config4_batch_against_oracle(M, mixed):
-    probs = [W.batch_problem(i) for i in CONFIG4]
+def test_batch_problems_against_oracle(M, mixed):
+    probs = [W.batch_problem(i) for i in BATCH_PROBS]
     flags = M.FLAG_DIRICHLET_COUPLED_DIAG | (M.FLAG_MIXED if mixed else 0)
     phis = [BoxData(p[0], 1, 1) for p in probs]
     with M.Batch([(p[0], p[1], p[3]) for p in probs], M.KIND_MG, flags, nstreams=4) as b:
@@ -144,7 +144,7 @@ def test_config4_batch_against_oracle(M, mixed):
                 po = BoxData(v, 1, 1)
                 ro = O.vcycle(po, rhs, geo, bc, True, 1e-10, 200, gs_order=order)
                 assert ro.final_relres <= 1e-10
-                _close(phis[k].interior(), po.interior(), f"problem {CONFIG4[k]} ({v.nx}x{v.ny}) order {order}")
+                _close(phis[k].interior(), po.interior(), f"problem {BATCH_PROBS[k]} ({v.nx}x{v.ny}) order {order}")
                 if order == 1 and not mixed:   # same sweep order: the same V-cycle count
                     assert reps[k].iterations == ro.iterations
     finally:

@@ -3,7 +3,8 @@ problems in one launch.  Each problem's solution must have the bits of its own
 stationary V-cycle (the resident solver without the flag), whatever else is in
 the batch and whenever the others converge; the V-cycle counts must be the
 same; and the solutions must agree with the CPU oracle in both sweep orders
-(config 4's problems, whose uneven sides give (2,1) and (1,2) levels)."""
+(problems of the batched workload, whose uneven sides give (2,1) and (1,2)
+levels)."""
 from __future__ import annotations
 
 import ctypes

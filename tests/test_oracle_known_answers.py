@@ -256,7 +256,7 @@ def test_reference_diagonal_diverges_on_dirichlet():
 
 @pytest.mark.parametrize("gs_order", [0, 1])
 def test_coupled_diagonal_converges_second_order(gs_order):
-    """config-1 style problem, coupled diagonal: converges to 1e-10 and the
+    """128^2 identity-map Dirichlet problem, coupled diagonal: converges to 1e-10 and the
     discretisation error vs u falls at second order."""
     _coupled(True)
     try:
