@@ -538,8 +538,8 @@ int build_direct_large(mgp_solver* s, cudaStream_t st) {
     const size_t sz = (size_t)(L.nx + 2) * (L.ny + 2);
     double *scratch = nullptr, *A = nullptr;
     int* iw = nullptr;
-    // scratch: the columns' 2 n fields, later the elimination's 4 n^2 + 1 + (n + 1) kGjPanel doubles
-    const size_t ns = std::max(2 * sz * n, 4 * (size_t)n * n + 1 + (size_t)(n + 1) * kGjPanel);
+    // scratch: the columns' 2 n fields, later the elimination's 4 n^2 + 2 + (n + 1) kGjPanel doubles
+    const size_t ns = std::max(2 * sz * n, 4 * (size_t)n * n + 2 + (size_t)(n + 1) * kGjPanel);
     if (dmalloc(&scratch, sizeof(double) * ns, st) != cudaSuccess ||
         dmalloc(&A, sizeof(double) * n * n, st) != cudaSuccess ||
         dmalloc(&iw, sizeof(int) * (2 * n + 1), st) != cudaSuccess) {

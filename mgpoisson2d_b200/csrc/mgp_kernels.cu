@@ -1998,8 +1998,7 @@ __global__ void __launch_bounds__(kGjPanelThreads) k_gj_panel(const double* __re
             prow[c] = p;
         }
         if (r == 0) ipiv[j] = ip;
-        if (live) f[(long)r * kGjPanel + j] = x[j];
-        const double fj = x[j];
+        const double fj = x[j];   // the multiplier; x[j] keeps it (only columns right of j change)
 #pragma unroll
         for (int q = 0; q < kGjPanel; ++q) {
             if (q <= j || q >= b) continue;
@@ -2008,6 +2007,14 @@ __global__ void __launch_bounds__(kGjPanelThreads) k_gj_panel(const double* __re
         }
         // prowv is rewritten by the next step's pivot row only after the
         // next step's first barrier, which every thread reaches after this read
+    }
+    // f[r][j] = row r's entry in step j's pivot column, written once for the
+    // panel as one 128-byte row a thread (16-byte stores) instead of an
+    // 8-byte store a step
+    if (live) {
+        double2* fr = reinterpret_cast<double2*>(f + (long)r * kGjPanel);
+#pragma unroll
+        for (int j = 0; j < kGjPanel; j += 2) fr[j / 2] = make_double2(x[j], x[j + 1]);
     }
 }
 
@@ -2054,7 +2061,7 @@ __global__ void __launch_bounds__(kGjThreads) k_gj_trailing(const double* __rest
 
 cudaError_t launch_invert(const double* A, int n, double* ainv, double* work, int* iwork, cudaStream_t st) {
     double *X0 = work, *X1 = work + 2L * n * n, *amax = work + 4L * n * n;
-    double *f = amax + 1, *ipiv = f + (long)n * kGjPanel;
+    double *f = amax + 2, *ipiv = f + (long)n * kGjPanel;   // f 16-byte aligned (the panel's double2 stores)
     int *mark = iwork, *prow = iwork + n, *fail = iwork + 2 * n;
     if (n > kGjPanelThreads) return cudaErrorNotSupported;
     const int nb = std::min(1184, (int)((2L * n * n + kGjThreads - 1) / kGjThreads));

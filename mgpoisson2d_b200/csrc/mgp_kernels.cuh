@@ -69,7 +69,7 @@ constexpr int kDirectCells = 64;
 // solved by launch_direct_apply.
 constexpr int kDirectLargeCells = 1024;
 // Pivots per panel of the blocked device Gauss-Jordan (launch_invert); its
-// scratch is 4 n^2 + 1 + (n + 1) kGjPanel doubles.
+// scratch is 4 n^2 + 2 + (n + 1) kGjPanel doubles.
 constexpr int kGjPanel = 16;
 
 constexpr int kMaxCoarseLevels = 16;
@@ -352,9 +352,10 @@ int barrier_selftest_ctas_max();
 cudaError_t launch_direct_columns(const Lv& L, double* scratch, double* A, cudaStream_t st);
 // Inverse of the n x n row-major A by Gauss-Jordan elimination with partial
 // pivoting on the device, into ainv (row-major, may alias A).  work holds
-// 4 n^2 + 1 doubles, iwork 2 n + 1 ints; *fail (in iwork) ends nonzero when a
-// pivot fell below 1e-13 of the largest |A| entry (singular to working
-// precision).  Launches n + 3 kernels.
+// 4 n^2 + 2 + (n + 1) kGjPanel doubles (16-byte aligned), iwork 2 n + 1 ints;
+// *fail (in iwork) ends nonzero when a pivot fell below 1e-13 of the largest
+// |A| entry (singular to working precision).  Launches 2 n / kGjPanel + 2
+// kernels.
 cudaError_t launch_invert(const double* A, int n, double* ainv, double* work, int* iwork, cudaStream_t st);
 // e = ainv r on the level's cells (n = nx * ny <= kDirectLargeCells; cells
 // numbered i fastest), one warp per row.
